@@ -1,0 +1,239 @@
+// Shared device/host helpers for the ddx library (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "../../include/ddx.h"
+
+namespace ddx {
+
+// ---------------------------------------------------------------------------
+// Error reporting: every C entry point returns a status and records a message
+// retrievable with ddx_last_error() (thread-local).
+// ---------------------------------------------------------------------------
+void set_error(const char* fmt, ...);
+
+#define DDX_REQUIRE(cond, ...)                 \
+  do {                                         \
+    if (!(cond)) {                             \
+      ::ddx::set_error(__VA_ARGS__);           \
+      return DDX_ERR_ARG;                      \
+    }                                          \
+  } while (0)
+
+#define DDX_LAUNCH_CHECK(name)                                                     \
+  do {                                                                             \
+    cudaError_t e_ = cudaGetLastError();                                           \
+    if (e_ != cudaSuccess) {                                                       \
+      ::ddx::set_error("%s: launch failed: %s", name, cudaGetErrorString(e_));     \
+      return DDX_ERR_CUDA;                                                         \
+    }                                                                              \
+  } while (0)
+
+constexpr int kThreads = 256;   // block size of every reducing kernel
+constexpr int kRedCtas = 592;   // 148 SMs x 4: max grid of a reducing kernel
+constexpr int kMaxNV = 4;       // max partial sums per RHS in one reduction
+
+// Device error word (bounded-wait timeouts); read by ddx_device_error().
+extern __device__ int g_device_error;
+enum { DEVERR_MBAR_TIMEOUT = 1, DEVERR_BAD_SIZE = 2 };
+
+__host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+inline bool valid_rhs_count(int R) {
+  return R == 1 || R == 2 || R == 4 || R == 8 || R == 16 || R == 32 || R == 64;
+}
+
+inline int red_grid(int64_t work_items) {
+  int64_t g = ceil_div(work_items, kThreads);
+  if (g < 1) g = 1;
+  if (g > kRedCtas) g = kRedCtas;
+  return (int)g;
+}
+
+// ---------------------------------------------------------------------------
+// Value conversions
+// ---------------------------------------------------------------------------
+template <typename T> __device__ __forceinline__ float to_f32(T v);
+template <> __device__ __forceinline__ float to_f32<float>(float v) { return v; }
+template <> __device__ __forceinline__ float to_f32<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+template <> __device__ __forceinline__ float to_f32<__half>(__half v) { return __half2float(v); }
+
+// ---------------------------------------------------------------------------
+// Deterministic reductions.
+//
+// A fused kernel accumulates NV per-RHS partial sums in fixed thread order,
+// reduces them inside the CTA in a fixed tree, and writes one partial per CTA
+// to partials[(cta * NV + v) * R + j]. The CTA that arrives last (ticket
+// counter) sums the per-CTA partials in a fixed order and runs the finalize
+// step. The order of every floating-point addition is fixed by the launch
+// shape, so repeated runs are bitwise identical. The ticket resets itself, so
+// the kernel can be replayed from a CUDA graph.
+// ---------------------------------------------------------------------------
+
+// Sum `val` over the threads of the CTA that share the column tid % R (R a
+// power of two dividing blockDim). Result valid in threads tid < R.
+__device__ __forceinline__ double block_sum_by_col(double val, double* red, int R) {
+  const int tid = threadIdx.x;
+  red[tid] = val;
+  __syncthreads();
+  for (int s = blockDim.x >> 1; s >= R; s >>= 1) {
+    if (tid < s) red[tid] += red[tid + s];
+    __syncthreads();
+  }
+  double out = red[tid];
+  __syncthreads();
+  return out;
+}
+
+template <int NV>
+__device__ __forceinline__ void write_cta_partials(const double (&v)[NV], double* red, int R,
+                                                   double* partials) {
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double s = block_sum_by_col(v[k], red, R);
+    if (threadIdx.x < R) partials[((size_t)blockIdx.x * NV + k) * R + threadIdx.x] = s;
+  }
+}
+
+// True in exactly one CTA, the last to arrive; it then sees all partials.
+__device__ __forceinline__ bool last_cta_arrival(unsigned int* ticket) {
+  __shared__ bool is_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int t = atomicAdd(ticket, 1u);
+    is_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (is_last) __threadfence();
+  return is_last;
+}
+
+// In the last CTA: totals over all CTAs, valid in threads tid < R (column tid).
+// Resets the ticket.
+template <int NV>
+__device__ __forceinline__ void final_sums(const double* partials, int R, double* red,
+                                           double (&out)[NV], unsigned int* ticket) {
+  const int t = threadIdx.x;
+  const int j = t % R, g = t / R, G = blockDim.x / R;
+  const int ncta = gridDim.x;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double acc = 0.0;
+    for (int c = g; c < ncta; c += G) acc += __ldcg(partials + ((size_t)c * NV + v) * R + j);
+    out[v] = block_sum_by_col(acc, red, R);
+  }
+  if (t == 0) *ticket = 0u;
+}
+
+// ---------------------------------------------------------------------------
+// PCG state accessors (layout documented in ddx.h)
+// ---------------------------------------------------------------------------
+struct PcgState {
+  double* st;
+  int* ist;
+  double* hist;
+  int R;
+  __device__ __forceinline__ double& s(int slot, int j) const { return st[slot * R + j]; }
+  __device__ __forceinline__ int& a(int slot, int j) const { return ist[slot * R + j]; }
+  __device__ __forceinline__ int& g(int slot) const { return ist[DDX_IST_COUNT * R + slot]; }
+};
+
+__device__ __forceinline__ int n_active(const int* ist, int R) {
+  return ist == nullptr ? 1 : *((volatile const int*)ist + DDX_IST_COUNT * R + DDX_G_NACTIVE);
+}
+
+// Count active RHS into the global counter (all threads of the CTA call it;
+// threads tid < R pass their flag).
+__device__ __forceinline__ void publish_nactive(PcgState S, int flag) {
+  __shared__ int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  if (threadIdx.x < S.R && flag) atomicAdd(&cnt, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) S.g(DDX_G_NACTIVE) = cnt;
+}
+
+// Finalize steps shared by the fused kernels (threads tid < R, column tid).
+__device__ __forceinline__ void fin_rz(PcgState S, int j, double rho, double zq) {
+  if (!S.a(DDX_IST_ACTIVE, j)) return;
+  S.s(DDX_ST_RHO, j) = rho;
+  S.s(DDX_ST_ZQ, j) = zq;
+  double beta = 0.0;
+  if (S.a(DDX_IST_ITERS, j) > 0) {
+    const double rho_prev = S.s(DDX_ST_RHO_PREV, j);
+    if (rho_prev != 0.0) {
+      beta = S.g(DDX_G_FLEXIBLE) ? -S.s(DDX_ST_ALPHA, j) * zq / rho_prev : rho / rho_prev;
+    }
+  }
+  S.s(DDX_ST_BETA, j) = beta;
+}
+
+__device__ __forceinline__ int fin_pq(PcgState S, int j, double pq) {
+  S.s(DDX_ST_PQ, j) = pq;
+  int act = S.a(DDX_IST_ACTIVE, j);
+  double alpha = 0.0;
+  if (act) {
+    if (pq > 0.0) {
+      alpha = S.s(DDX_ST_RHO, j) / pq;
+    } else {
+      act = 0;
+      S.a(DDX_IST_ACTIVE, j) = 0;
+      S.g(DDX_G_BREAKDOWN) = 1;
+    }
+    S.s(DDX_ST_RHO_PREV, j) = S.s(DDX_ST_RHO, j);
+  }
+  S.s(DDX_ST_ALPHA, j) = alpha;
+  return act;
+}
+
+__device__ __forceinline__ int fin_rr(PcgState S, int j, double rr) {
+  int act = S.a(DDX_IST_ACTIVE, j);
+  if (act) {
+    const int it = ++S.a(DDX_IST_ITERS, j);
+    const double rn = sqrt(rr);
+    S.s(DDX_ST_RR, j) = rr;
+    S.hist[(size_t)it * S.R + j] = rn;
+    if (rn < S.s(DDX_ST_ATOL, j) || it >= S.g(DDX_G_MAXITER)) {
+      act = 0;
+      S.a(DDX_IST_ACTIVE, j) = 0;
+    }
+  }
+  return act;
+}
+
+// r = b - A x at the start of a solve: tolerance from ||b||, first stop test.
+__device__ __forceinline__ int fin_init(PcgState S, int j, double bb, double rr) {
+  const double rtol = S.s(DDX_ST_BB, j);  // ddx_pcg_reset parks rtol here
+  const double atol = fmax(S.s(DDX_ST_ATOL, j), rtol * sqrt(bb));
+  S.s(DDX_ST_ATOL, j) = atol;
+  S.s(DDX_ST_BB, j) = bb;
+  S.s(DDX_ST_RR, j) = rr;
+  const double rn = sqrt(rr);
+  S.hist[j] = rn;
+  S.a(DDX_IST_ITERS, j) = 0;
+  // A zero right-hand side with a zero residual has nothing to solve.
+  const int act = !(rn < atol) && !(bb == 0.0 && rr == 0.0) && S.g(DDX_G_MAXITER) > 0;
+  S.a(DDX_IST_ACTIVE, j) = act;
+  return act;
+}
+
+// Residual replacement: r was recomputed as b - A x; redo the stop test.
+__device__ __forceinline__ int fin_replace(PcgState S, int j, double rr) {
+  int act = S.a(DDX_IST_ACTIVE, j);
+  if (!act) return 0;  // converged RHS keep their recorded history
+  const double rn = sqrt(rr);
+  S.s(DDX_ST_RR, j) = rr;
+  S.hist[(size_t)S.a(DDX_IST_ITERS, j) * S.R + j] = rn;
+  if (rn < S.s(DDX_ST_ATOL, j)) {
+    act = 0;
+    S.a(DDX_IST_ACTIVE, j) = 0;
+  }
+  return act;
+}
+
+}  // namespace ddx

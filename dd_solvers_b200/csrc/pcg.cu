@@ -1,0 +1,180 @@
+// PCG vector updates with fused deterministic reductions and a device-side
+// stop test. Replaces the per-iteration torch ops of CG.solve
+// (src/dd_solvers/dd_solvers/solvers.py:243-268): the norm + .item() host
+// sync (244), torch.dot (256, 265) and the compiled axpy updates (170-189).
+#include <stdarg.h>
+
+#include "common.cuh"
+
+namespace ddx {
+
+static thread_local char g_msg[512] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_msg, sizeof(g_msg), fmt, ap);
+  va_end(ap);
+}
+
+__device__ int g_device_error = 0;
+
+__global__ void k_pcg_reset(PcgState S, int maxiter, int flexible, double rtol, double atol) {
+  const int j = threadIdx.x;
+  if (j < S.R) {
+#pragma unroll
+    for (int s = 0; s < DDX_ST_COUNT; ++s) S.s(s, j) = 0.0;
+    S.s(DDX_ST_ATOL, j) = atol;
+    S.s(DDX_ST_BB, j) = rtol;
+    S.a(DDX_IST_ACTIVE, j) = 1;
+    S.a(DDX_IST_ITERS, j) = 0;
+  }
+  if (j == 0) {
+    S.g(DDX_G_NACTIVE) = S.R;
+    S.g(DDX_G_MAXITER) = maxiter;
+    S.g(DDX_G_FLEXIBLE) = flexible;
+    S.g(DDX_G_BREAKDOWN) = 0;
+  }
+}
+
+// p = z + beta p
+__global__ void k_update_p(int64_t n, int R, const double* __restrict__ z, double* __restrict__ p,
+                           const double* __restrict__ st, const int* __restrict__ ist) {
+  if (n_active(ist, R) == 0) return;
+  const int64_t total = n * R;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int j = threadIdx.x % R;  // stride is a multiple of R
+  const double beta = st[DDX_ST_BETA * R + j];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+    p[i] = fma(beta, p[i], z[i]);
+  }
+}
+
+// x += alpha p; r -= alpha q; rr = ||r||^2 -> stop test
+__global__ void __launch_bounds__(kThreads) k_update_xr(int64_t n, PcgState S, double* __restrict__ x,
+                                                        double* __restrict__ r, const double* __restrict__ p,
+                                                        const double* __restrict__ q, double* partials,
+                                                        unsigned int* ticket) {
+  __shared__ double red[kThreads];
+  const int R = S.R;
+  if (n_active(S.ist, R) == 0) return;
+  const int64_t total = n * R;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int j = threadIdx.x % R;
+  const double alpha = S.st[DDX_ST_ALPHA * R + j];
+  double acc[1] = {0.0};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+    const double xi = fma(alpha, p[i], x[i]);
+    const double ri = fma(-alpha, q[i], r[i]);
+    x[i] = xi;
+    r[i] = ri;
+    acc[0] = fma(ri, ri, acc[0]);
+  }
+  write_cta_partials<1>(acc, red, R, partials);
+  if (!last_cta_arrival(ticket)) return;
+  double tot[1];
+  final_sums<1>(partials, R, red, tot, ticket);
+  int act = 0;
+  if (threadIdx.x < R) act = fin_rr(S, threadIdx.x, tot[0]);
+  publish_nactive(S, act);
+}
+
+// rho = r.z, zq = z.q -> beta
+__global__ void __launch_bounds__(kThreads) k_dots_rz(int64_t n, PcgState S, const double* __restrict__ r,
+                                                      const double* __restrict__ z,
+                                                      const double* __restrict__ q, double* partials,
+                                                      unsigned int* ticket) {
+  __shared__ double red[kThreads];
+  const int R = S.R;
+  if (n_active(S.ist, R) == 0) return;
+  const int64_t total = n * R;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+    const double zi = z[i];
+    acc[0] = fma(r[i], zi, acc[0]);
+    if (q != nullptr) acc[1] = fma(zi, q[i], acc[1]);
+  }
+  write_cta_partials<2>(acc, red, R, partials);
+  if (!last_cta_arrival(ticket)) return;
+  double tot[2];
+  final_sums<2>(partials, R, red, tot, ticket);
+  if (threadIdx.x < R) fin_rz(S, threadIdx.x, tot[0], tot[1]);
+}
+
+}  // namespace ddx
+
+using namespace ddx;
+
+extern "C" {
+
+const char* ddx_last_error(void) { return g_msg; }
+
+int ddx_version(void) { return 100; }
+
+size_t ddx_partials_len(int R) { return (size_t)kRedCtas * kMaxNV * (size_t)R; }
+
+int ddx_device_error(int* code) {
+  int v = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&v, g_device_error, sizeof(int));
+  if (e != cudaSuccess) {
+    set_error("ddx_device_error: %s", cudaGetErrorString(e));
+    return DDX_ERR_CUDA;
+  }
+  int zero = 0;
+  e = cudaMemcpyToSymbol(g_device_error, &zero, sizeof(int));
+  if (e != cudaSuccess) {
+    set_error("ddx_device_error: %s", cudaGetErrorString(e));
+    return DDX_ERR_CUDA;
+  }
+  if (code) *code = v;
+  return DDX_OK;
+}
+
+int ddx_pcg_reset(int R, double* st, int* ist, int maxiter, int flexible, double rtol, double atol,
+                  ddx_stream_t stream) {
+  DDX_REQUIRE(valid_rhs_count(R), "ddx_pcg_reset: unsupported R=%d", R);
+  DDX_REQUIRE(st && ist, "ddx_pcg_reset: null state");
+  DDX_REQUIRE(maxiter >= 0, "ddx_pcg_reset: maxiter < 0");
+  PcgState S{st, ist, nullptr, R};
+  k_pcg_reset<<<1, 64, 0, (cudaStream_t)stream>>>(S, maxiter, flexible, rtol, atol);
+  DDX_LAUNCH_CHECK("ddx_pcg_reset");
+  return DDX_OK;
+}
+
+int ddx_pcg_update_p(int64_t n, int R, const double* z, double* p, const double* st, const int* ist,
+                     ddx_stream_t stream) {
+  DDX_REQUIRE(valid_rhs_count(R), "ddx_pcg_update_p: unsupported R=%d", R);
+  DDX_REQUIRE(n >= 0 && z && p && st && ist, "ddx_pcg_update_p: bad arguments");
+  if (n == 0) return DDX_OK;
+  int grid = (int)std::min<int64_t>(ceil_div(n * R, kThreads), 148 * 16);
+  k_update_p<<<grid, kThreads, 0, (cudaStream_t)stream>>>(n, R, z, p, st, ist);
+  DDX_LAUNCH_CHECK("ddx_pcg_update_p");
+  return DDX_OK;
+}
+
+int ddx_pcg_update_xr(int64_t n, int R, double* x, double* r, const double* p, const double* q,
+                      double* st, int* ist, double* hist, double* partials, unsigned int* tickets,
+                      ddx_stream_t stream) {
+  DDX_REQUIRE(valid_rhs_count(R), "ddx_pcg_update_xr: unsupported R=%d", R);
+  DDX_REQUIRE(n >= 0 && x && r && p && q && st && ist && hist && partials && tickets,
+              "ddx_pcg_update_xr: bad arguments");
+  PcgState S{st, ist, hist, R};
+  k_update_xr<<<red_grid(n * R), kThreads, 0, (cudaStream_t)stream>>>(n, S, x, r, p, q, partials,
+                                                                       tickets + 0);
+  DDX_LAUNCH_CHECK("ddx_pcg_update_xr");
+  return DDX_OK;
+}
+
+int ddx_pcg_dots_rz(int64_t n, int R, const double* r, const double* z, const double* q, double* st,
+                    int* ist, double* partials, unsigned int* tickets, ddx_stream_t stream) {
+  DDX_REQUIRE(valid_rhs_count(R), "ddx_pcg_dots_rz: unsupported R=%d", R);
+  DDX_REQUIRE(n >= 0 && r && z && st && ist && partials && tickets, "ddx_pcg_dots_rz: bad arguments");
+  PcgState S{st, ist, nullptr, R};
+  k_dots_rz<<<red_grid(n * R), kThreads, 0, (cudaStream_t)stream>>>(n, S, r, z, q, partials,
+                                                                     tickets + 1);
+  DDX_LAUNCH_CHECK("ddx_pcg_dots_rz");
+  return DDX_OK;
+}
+
+}  // extern "C"

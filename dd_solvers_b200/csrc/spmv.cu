@@ -1,0 +1,303 @@
+// Sparse matrix-vector products for the PCG loop.
+//
+// Replaces FastBSR's RPT-I kernel (src/dd_solvers/dd_solvers/bsr.py:40-76, one
+// thread per scalar row over a BSR matrix) and torch's CSR matvec
+// (solvers.py:264, 880). The continuous Q1/P1 matrices of the measured
+// problems are scalar (9/27/7-point rows), so the main kernel uses SELL-32:
+// each warp owns a 32-row slice whose entries are stored column by column, so
+// every value/column load of the warp is one contiguous 256/128-byte segment;
+// x is read through the read-only cache (its reuse across neighbouring rows is
+// served by L1/L2). The PCG epilogues (p.q, b - A x and its norms) are fused
+// with deterministic CTA partials and a last-CTA finalize.
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace ddx {
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads)
+    k_spmv_sell(int64_t n, int64_t nslices, const int64_t* __restrict__ slice_ptr,
+                const int* __restrict__ slice_width, const int* __restrict__ cols,
+                const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y,
+                const double* __restrict__ b, PcgState S, double* partials, unsigned int* ticket) {
+  __shared__ double red[kThreads];
+  if (MODE != DDX_SPMV_PLAIN && n_active(S.ist, 1) == 0) return;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int wpb = blockDim.x >> 5;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t s = (int64_t)blockIdx.x * wpb + warp; s < nslices; s += (int64_t)gridDim.x * wpb) {
+    const int64_t row = s * 32 + lane;
+    const int64_t base = slice_ptr[s] + lane;
+    const int w = slice_width[s];
+    double sum = 0.0;
+    if (row < n) {
+      int jj = 0;
+      for (; jj + 4 <= w; jj += 4) {
+        const int64_t o = base + (int64_t)jj * 32;
+        const double v0 = __ldcs(vals + o), v1 = __ldcs(vals + o + 32), v2 = __ldcs(vals + o + 64),
+                     v3 = __ldcs(vals + o + 96);
+        const int c0 = __ldcs(cols + o), c1 = __ldcs(cols + o + 32), c2 = __ldcs(cols + o + 64),
+                  c3 = __ldcs(cols + o + 96);
+        sum = fma(v0, __ldg(x + c0), sum);
+        sum = fma(v1, __ldg(x + c1), sum);
+        sum = fma(v2, __ldg(x + c2), sum);
+        sum = fma(v3, __ldg(x + c3), sum);
+      }
+      for (; jj < w; ++jj) {
+        const int64_t o = base + (int64_t)jj * 32;
+        sum = fma(__ldcs(vals + o), __ldg(x + __ldcs(cols + o)), sum);
+      }
+      if (MODE == DDX_SPMV_PLAIN || MODE == DDX_SPMV_PQ) {
+        y[row] = sum;
+        if (MODE == DDX_SPMV_PQ) acc[0] = fma(x[row], sum, acc[0]);
+      } else {
+        const double bi = b[row];
+        const double ri = bi - sum;
+        y[row] = ri;
+        if (MODE == DDX_SPMV_RES_INIT) acc[1] = fma(bi, bi, acc[1]);
+        acc[0] = fma(ri, ri, acc[0]);
+      }
+    }
+  }
+  if (MODE == DDX_SPMV_PLAIN) return;
+  constexpr int NV = (MODE == DDX_SPMV_RES_INIT) ? 2 : 1;
+  double part[NV];
+  part[0] = acc[0];
+  if (NV == 2) part[NV - 1] = acc[1];
+  write_cta_partials<NV>(part, red, 1, partials);
+  if (!last_cta_arrival(ticket)) return;
+  double tot[NV];
+  final_sums<NV>(partials, 1, red, tot, ticket);
+  int act = 0;
+  if (threadIdx.x == 0) {
+    if (MODE == DDX_SPMV_PQ) act = fin_pq(S, 0, tot[0]);
+    if (MODE == DDX_SPMV_RES_INIT) act = fin_init(S, 0, tot[NV - 1], tot[0]);
+    if (MODE == DDX_SPMV_RES_REPLACE) act = fin_replace(S, 0, tot[0]);
+  }
+  if (MODE != DDX_SPMV_PQ) publish_nactive(S, act);
+  else {
+    // alpha step can deactivate a RHS on breakdown; keep the counter exact.
+    publish_nactive(S, threadIdx.x == 0 ? act : 0);
+  }
+}
+
+// CSR, R threads per row (R in {1..64}, power of two), (n, R) vector layout.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads)
+    k_spmv_csr(int64_t n, const int* __restrict__ row_ptr, const int* __restrict__ cols,
+               const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y,
+               const double* __restrict__ b, PcgState S, double* partials, unsigned int* ticket) {
+  __shared__ double red[kThreads];
+  const int R = S.R;
+  if (MODE != DDX_SPMV_PLAIN && n_active(S.ist, R) == 0) return;
+  const int j = threadIdx.x % R;
+  const int rpb = blockDim.x / R;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t row = (int64_t)blockIdx.x * rpb + threadIdx.x / R; row < n; row += (int64_t)gridDim.x * rpb) {
+    const int k0 = row_ptr[row], k1 = row_ptr[row + 1];
+    double sum = 0.0;
+    for (int k = k0; k < k1; ++k) sum = fma(__ldg(vals + k), __ldg(x + (int64_t)__ldg(cols + k) * R + j), sum);
+    const int64_t o = row * R + j;
+    if (MODE == DDX_SPMV_PLAIN || MODE == DDX_SPMV_PQ) {
+      y[o] = sum;
+      if (MODE == DDX_SPMV_PQ) acc[0] = fma(x[o], sum, acc[0]);
+    } else {
+      const double bi = b[o];
+      const double ri = bi - sum;
+      y[o] = ri;
+      if (MODE == DDX_SPMV_RES_INIT) acc[1] = fma(bi, bi, acc[1]);
+      acc[0] = fma(ri, ri, acc[0]);
+    }
+  }
+  if (MODE == DDX_SPMV_PLAIN) return;
+  constexpr int NV = (MODE == DDX_SPMV_RES_INIT) ? 2 : 1;
+  double part[NV];
+  part[0] = acc[0];
+  if (NV == 2) part[NV - 1] = acc[1];
+  write_cta_partials<NV>(part, red, R, partials);
+  if (!last_cta_arrival(ticket)) return;
+  double tot[NV];
+  final_sums<NV>(partials, R, red, tot, ticket);
+  int act = 0;
+  if (threadIdx.x < R) {
+    const int jj = threadIdx.x;
+    if (MODE == DDX_SPMV_PQ) act = fin_pq(S, jj, tot[0]);
+    if (MODE == DDX_SPMV_RES_INIT) act = fin_init(S, jj, tot[NV - 1], tot[0]);
+    if (MODE == DDX_SPMV_RES_REPLACE) act = fin_replace(S, jj, tot[0]);
+  }
+  publish_nactive(S, act);
+}
+
+// One CTA per (long) row; threads stride over the row's entries.
+__global__ void __launch_bounds__(kThreads)
+    k_spmv_rowblock(int64_t n_rows, int R, const int* __restrict__ row_ptr, const int* __restrict__ cols,
+                    const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y) {
+  __shared__ double red[kThreads];
+  const int j = threadIdx.x % R;
+  const int G = blockDim.x / R;
+  for (int64_t row = blockIdx.x; row < n_rows; row += gridDim.x) {
+    const int k0 = row_ptr[row], k1 = row_ptr[row + 1];
+    double sum = 0.0;
+    for (int k = k0 + threadIdx.x / R; k < k1; k += G)
+      sum = fma(__ldg(vals + k), __ldg(x + (int64_t)__ldg(cols + k) * R + j), sum);
+    sum = block_sum_by_col(sum, red, R);
+    if (threadIdx.x < R) y[row * R + threadIdx.x] = sum;
+  }
+}
+
+// BSR with column-major (bs x bs) blocks; one warp per block row. Lane l walks
+// the row's stored values e = l, l+32, ...; entry e of the block row is block
+// e / bs^2, column (e % bs^2) / bs, row e % bs.
+template <typename T, int BS>
+__global__ void k_spmv_bsr(int64_t nbr, const int* __restrict__ row_ptr, const int* __restrict__ cols,
+                           const T* __restrict__ vals, const T* __restrict__ x, T* __restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  const int64_t br = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (br >= nbr) return;
+  constexpr int B2 = BS * BS;
+  T acc[BS];
+#pragma unroll
+  for (int r = 0; r < BS; ++r) acc[r] = T(0);
+  const int64_t e0 = (int64_t)row_ptr[br] * B2, e1 = (int64_t)row_ptr[br + 1] * B2;
+  for (int64_t e = e0 + lane; e < e1; e += 32) {
+    const int64_t blk = e / B2;
+    const int w = (int)(e - blk * B2);
+    const int c = w / BS, r = w - c * BS;
+    const T v = vals[e] * x[(int64_t)cols[blk] * BS + c];
+#pragma unroll
+    for (int rr = 0; rr < BS; ++rr)
+      if (rr == r) acc[rr] += v;
+  }
+#pragma unroll
+  for (int r = 0; r < BS; ++r) {
+    T v = acc[r];
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if (lane == r) y[br * BS + r] = v;
+  }
+}
+
+template <typename T>
+static int launch_bsr(int64_t nbr, int bs, const int* rp, const int* ci, const T* v, const T* x, T* y,
+                      cudaStream_t s) {
+  const int wpb = 8;
+  const int grid = (int)ceil_div(nbr, wpb);
+  switch (bs) {
+#define DDX_BSR_CASE(B) \
+  case B: k_spmv_bsr<T, B><<<grid, wpb * 32, 0, s>>>(nbr, rp, ci, v, x, y); break;
+    DDX_BSR_CASE(1) DDX_BSR_CASE(2) DDX_BSR_CASE(3) DDX_BSR_CASE(4)
+    DDX_BSR_CASE(5) DDX_BSR_CASE(6) DDX_BSR_CASE(7) DDX_BSR_CASE(8)
+#undef DDX_BSR_CASE
+    default: set_error("ddx_spmv_bsr: block size %d not in 1..8", bs); return DDX_ERR_UNSUPPORTED;
+  }
+  DDX_LAUNCH_CHECK("ddx_spmv_bsr");
+  return DDX_OK;
+}
+
+}  // namespace ddx
+
+using namespace ddx;
+
+extern "C" {
+
+int ddx_spmv_sell_f64(int64_t n, int64_t nslices, const int64_t* slice_ptr, const int* slice_width,
+                      const int* cols, const double* vals, const double* x, double* y, const double* b,
+                      int mode, double* st, int* ist, double* hist, double* partials,
+                      unsigned int* tickets, ddx_stream_t stream) {
+  DDX_REQUIRE(n >= 0 && nslices == ceil_div(n, 32), "ddx_spmv_sell_f64: nslices must be ceil(n/32)");
+  DDX_REQUIRE(slice_ptr && slice_width && x && y, "ddx_spmv_sell_f64: null pointer");
+  DDX_REQUIRE(mode >= 0 && mode <= 3, "ddx_spmv_sell_f64: bad mode %d", mode);
+  if (mode != DDX_SPMV_PLAIN)
+    DDX_REQUIRE(st && ist && hist && partials && tickets, "ddx_spmv_sell_f64: PCG mode needs state");
+  if (mode >= DDX_SPMV_RES_INIT) DDX_REQUIRE(b, "ddx_spmv_sell_f64: residual mode needs b");
+  if (n == 0) return DDX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  PcgState S{st, ist, hist, 1};
+  const int wpb = kThreads / 32;
+  const int grid = (int)std::min<int64_t>(ceil_div(nslices, wpb), kRedCtas);
+  unsigned int* t = tickets ? tickets + 2 : nullptr;
+  switch (mode) {
+    case DDX_SPMV_PLAIN:
+      k_spmv_sell<DDX_SPMV_PLAIN><<<(int)ceil_div(nslices, wpb), kThreads, 0, s>>>(
+          n, nslices, slice_ptr, slice_width, cols, vals, x, y, b, S, partials, t);
+      break;
+    case DDX_SPMV_PQ:
+      k_spmv_sell<DDX_SPMV_PQ><<<grid, kThreads, 0, s>>>(n, nslices, slice_ptr, slice_width, cols, vals,
+                                                         x, y, b, S, partials, t);
+      break;
+    case DDX_SPMV_RES_INIT:
+      k_spmv_sell<DDX_SPMV_RES_INIT><<<grid, kThreads, 0, s>>>(n, nslices, slice_ptr, slice_width, cols,
+                                                               vals, x, y, b, S, partials, t);
+      break;
+    default:
+      k_spmv_sell<DDX_SPMV_RES_REPLACE><<<grid, kThreads, 0, s>>>(n, nslices, slice_ptr, slice_width,
+                                                                  cols, vals, x, y, b, S, partials, t);
+  }
+  DDX_LAUNCH_CHECK("ddx_spmv_sell_f64");
+  return DDX_OK;
+}
+
+int ddx_spmv_csr_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols, const double* vals,
+                     const double* x, double* y, const double* b, int mode, double* st, int* ist,
+                     double* hist, double* partials, unsigned int* tickets, ddx_stream_t stream) {
+  DDX_REQUIRE(valid_rhs_count(R), "ddx_spmv_csr_f64: unsupported R=%d", R);
+  DDX_REQUIRE(n_rows >= 0 && row_ptr && x && y, "ddx_spmv_csr_f64: bad arguments");
+  DDX_REQUIRE(mode >= 0 && mode <= 3, "ddx_spmv_csr_f64: bad mode %d", mode);
+  if (mode != DDX_SPMV_PLAIN)
+    DDX_REQUIRE(st && ist && hist && partials && tickets, "ddx_spmv_csr_f64: PCG mode needs state");
+  if (mode >= DDX_SPMV_RES_INIT) DDX_REQUIRE(b, "ddx_spmv_csr_f64: residual mode needs b");
+  if (n_rows == 0) return DDX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  PcgState S{st, ist, hist, R};
+  const int rpb = kThreads / R;
+  const int64_t need = ceil_div(n_rows, rpb);
+  const int grid = (int)std::min<int64_t>(need, kRedCtas);
+  unsigned int* t = tickets ? tickets + 3 : nullptr;
+  switch (mode) {
+    case DDX_SPMV_PLAIN:
+      k_spmv_csr<DDX_SPMV_PLAIN><<<(int)std::min<int64_t>(need, 148 * 64), kThreads, 0, s>>>(
+          n_rows, row_ptr, cols, vals, x, y, b, S, partials, t);
+      break;
+    case DDX_SPMV_PQ:
+      k_spmv_csr<DDX_SPMV_PQ><<<grid, kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S, partials, t);
+      break;
+    case DDX_SPMV_RES_INIT:
+      k_spmv_csr<DDX_SPMV_RES_INIT><<<grid, kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S,
+                                                              partials, t);
+      break;
+    default:
+      k_spmv_csr<DDX_SPMV_RES_REPLACE><<<grid, kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S,
+                                                                 partials, t);
+  }
+  DDX_LAUNCH_CHECK("ddx_spmv_csr_f64");
+  return DDX_OK;
+}
+
+int ddx_spmv_csr_rowblock_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols,
+                              const double* vals, const double* x, double* y, ddx_stream_t stream) {
+  DDX_REQUIRE(valid_rhs_count(R), "ddx_spmv_csr_rowblock_f64: unsupported R=%d", R);
+  DDX_REQUIRE(n_rows >= 0 && row_ptr && x && y, "ddx_spmv_csr_rowblock_f64: bad arguments");
+  if (n_rows == 0) return DDX_OK;
+  const int grid = (int)std::min<int64_t>(n_rows, 148 * 8);
+  k_spmv_rowblock<<<grid, kThreads, 0, (cudaStream_t)stream>>>(n_rows, R, row_ptr, cols, vals, x, y);
+  DDX_LAUNCH_CHECK("ddx_spmv_csr_rowblock_f64");
+  return DDX_OK;
+}
+
+int ddx_spmv_bsr(int64_t n_block_rows, int bs, const int* row_ptr, const int* cols, const void* vals,
+                 const void* x, void* y, int dtype, ddx_stream_t stream) {
+  DDX_REQUIRE(n_block_rows >= 0 && row_ptr && x && y, "ddx_spmv_bsr: bad arguments");
+  if (n_block_rows == 0) return DDX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == DDX_F64)
+    return launch_bsr<double>(n_block_rows, bs, row_ptr, cols, (const double*)vals, (const double*)x,
+                              (double*)y, s);
+  if (dtype == DDX_F32)
+    return launch_bsr<float>(n_block_rows, bs, row_ptr, cols, (const float*)vals, (const float*)x,
+                             (float*)y, s);
+  set_error("ddx_spmv_bsr: dtype %d not supported (F64 or F32)", dtype);
+  return DDX_ERR_UNSUPPORTED;
+}
+
+}  // extern "C"

@@ -1,0 +1,85 @@
+"""SPD factorisation with the interface of ``dd_solvers.cudss``
+(src/dd_solvers/dd_solvers/cudss.py:1-44; src/dd_solvers/cpp/cudss.cpp:34-105).
+
+cuDSS is absent from this image. ``spd_factorize`` instead factors the (small,
+coarse) matrix densely in FP64 with cuSOLVER's Cholesky (``torch.linalg.cholesky``),
+forms the explicit symmetric inverse once, and ``solve`` applies it with the
+HBM-bound ``ddx_coarse_gemv_f64`` kernel. The batched variant factors each
+matrix of a block-diagonal batch the same way.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import _lib as L
+
+__all__ = ["CudssSolver", "spd_factorize", "CudssBatchSolver", "spd_batch_factorize"]
+
+
+def _dense_inverse(A: torch.Tensor) -> torch.Tensor:
+    dense = A.to_dense().to(torch.float64) if A.layout != torch.strided else A.to(torch.float64)
+    Lc, info = torch.linalg.cholesky_ex(dense)
+    if int(info.max() if info.dim() else info) != 0:
+        raise RuntimeError("spd_factorize: matrix is not positive definite")
+    inv = torch.cholesky_inverse(Lc)
+    return 0.5 * (inv + inv.transpose(-1, -2))
+
+
+class CudssSolver:
+    def __init__(self, inverse: torch.Tensor, dtype: torch.dtype):
+        self.inverse = inverse.contiguous()
+        self.dtype = dtype
+        self.n = inverse.shape[0]
+
+    def solve(self, rhs: torch.Tensor) -> torch.Tensor:
+        L.require_cuda(rhs, "rhs")
+        R = 1 if rhs.dim() == 1 else rhs.shape[1]
+        w = rhs.to(torch.float64).contiguous()
+        y = torch.empty_like(w)
+        if R in (1, 2, 4, 8, 16, 32, 64):
+            L.call("ddx_coarse_gemv_f64", self.n, R, L.ptr(self.inverse), L.ptr(w), L.ptr(y), None, L.stream_ptr())
+        else:
+            for j in range(R):
+                wj = w[:, j].contiguous()
+                yj = torch.empty_like(wj)
+                L.call("ddx_coarse_gemv_f64", self.n, 1, L.ptr(self.inverse), L.ptr(wj), L.ptr(yj), None,
+                       L.stream_ptr())
+                y[:, j] = yj
+        return y.to(rhs.dtype)
+
+
+def spd_factorize(A: torch.Tensor) -> CudssSolver:
+    L.require_cuda(A, "A")
+    return CudssSolver(_dense_inverse(A), A.dtype)
+
+
+class CudssBatchSolver:
+    def __init__(self, solvers, sizes):
+        self.solvers = solvers
+        self.sizes = sizes
+
+    def solve(self, rhs: torch.Tensor) -> torch.Tensor:
+        outs, o = [], 0
+        for s, n in zip(self.solvers, self.sizes):
+            outs.append(s.solve(rhs[o:o + n]))
+            o += n
+        return torch.cat(outs)
+
+
+def spd_batch_factorize(nrows, nnz, values, col_indices, row_start) -> CudssBatchSolver:
+    """Block-diagonal batch given as concatenated CSR pieces (src/dd_solvers/cpp/cudss.cpp:107-247)."""
+    solvers, sizes = [], []
+    vo = ro = 0
+    nrows_l = [int(v) for v in nrows.tolist()]
+    nnz_l = [int(v) for v in nnz.tolist()]
+    for n, z in zip(nrows_l, nnz_l):
+        crow = row_start[ro:ro + n + 1].to(torch.int64)
+        crow = crow - crow[0]
+        A = torch.sparse_csr_tensor(crow, col_indices[vo:vo + z].to(torch.int64), values[vo:vo + z], size=(n, n))
+        if not A.is_cuda:
+            A = A.cuda()
+        solvers.append(spd_factorize(A))
+        sizes.append(n)
+        vo += z
+        ro += n + 1
+    return CudssBatchSolver(solvers, sizes)

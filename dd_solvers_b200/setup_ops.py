@@ -1,0 +1,219 @@
+"""Setup-time data preparation (runs once per operator, outside the solve loop).
+
+Counterparts in the reference: ``SchwarzOperator.setup`` and its numba kernels
+(``src/dd_solvers/dd_solvers/solvers.py:571-771``, dense block extraction
+407-423, coarse matrix 426-481), ``Inv.setup`` (350-353) and ``csr_to_bsr``
+(``src/dd_solvers/cpp/cusparse.cpp:22-107``). These are written with torch
+tensor ops so they run on the GPU for large problems and on CPU tensors in
+the host-side tests; no kernel of the solve path is involved.
+
+HBM layouts produced here (all consumed by ``libddx.so``):
+
+* SELL-32 matrix: ``slice_ptr`` (int64, nslices+1), ``slice_width`` (int32),
+  ``cols`` (int32), ``vals`` (float64); entry ``j`` of row ``32 s + l`` at
+  ``slice_ptr[s] + 32 j + l``; padding has value 0 and the row's own column.
+* Inverse blocks: one flat buffer per precision; block ``i`` column-major with
+  leading dimension ``ld_i = round_up(k_i, 16 / elem_size)`` at element offset
+  ``blk_off[i]`` (16-byte aligned), rows ``k_i..ld_i-1`` zero; FP32 per-block
+  power-of-two scales for low-precision storage.
+* Transpose map: ``dof_ptr`` (int32, n+1), ``dof_src`` (int32): the positions of
+  DOF ``d`` in the subdomain-major concatenation ``sub_idx`` in ascending order.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import scipy.sparse as sps
+import torch
+
+ELEM_BYTES = {torch.float64: 8, torch.float32: 4, torch.bfloat16: 2, torch.float16: 2}
+# |Q| <= 2**TARGET_EXP after scaling (FP16 uses its range: largest power of two
+# below its maximum 65504 is 2**15; 2**14 keeps a factor-2 margin).
+TARGET_EXP = {torch.float64: None, torch.float32: 0, torch.bfloat16: 0, torch.float16: 14}
+
+
+# ---------------------------------------------------------------------------
+# SELL-32
+# ---------------------------------------------------------------------------
+
+def csr_to_sell32(crow: torch.Tensor, col: torch.Tensor, val: torch.Tensor):
+    """CSR -> SELL-32 (slice height 32, no row sorting)."""
+    dev = crow.device
+    n = crow.numel() - 1
+    nsl = (n + 31) // 32
+    lens = (crow[1:] - crow[:-1]).to(torch.int64)
+    lens_p = torch.zeros(nsl * 32, dtype=torch.int64, device=dev)
+    lens_p[:n] = lens
+    width = lens_p.view(nsl, 32).amax(dim=1)
+    slice_ptr = torch.zeros(nsl + 1, dtype=torch.int64, device=dev)
+    slice_ptr[1:] = torch.cumsum(width * 32, 0)
+    total = int(slice_ptr[-1])
+    rows_all = torch.arange(nsl * 32, device=dev)
+    # padding default: own row (clamped to a valid column), value 0
+    cols_s = torch.empty(total, dtype=torch.int32, device=dev)
+    vals_s = torch.zeros(total, dtype=torch.float64, device=dev)
+    # fill default columns slice by slice: position slice_ptr[s] + 32 j + l -> row 32 s + l
+    pos = torch.arange(total, device=dev)
+    sl = torch.searchsorted(slice_ptr, pos, right=True) - 1
+    lrow = (pos - slice_ptr[sl]) % 32
+    cols_s[:] = torch.clamp(sl * 32 + lrow, max=max(n - 1, 0)).to(torch.int32)
+    # scatter real entries
+    row_of = torch.repeat_interleave(torch.arange(n, device=dev), lens)
+    j_in_row = torch.arange(int(crow[-1]), device=dev) - crow[:-1].to(torch.int64)[row_of]
+    dst = slice_ptr[row_of // 32] + j_in_row * 32 + (row_of % 32)
+    cols_s[dst] = col.to(torch.int32)
+    vals_s[dst] = val.to(torch.float64)
+    del rows_all
+    return slice_ptr, width.to(torch.int32), cols_s, vals_s
+
+
+# ---------------------------------------------------------------------------
+# Subdomain maps
+# ---------------------------------------------------------------------------
+
+def transpose_map(sub_idx: torch.Tensor, n: int):
+    """DOF -> positions in the subdomain-major list, ascending (stable sort)."""
+    order = torch.argsort(sub_idx.to(torch.int64), stable=True)
+    counts = torch.bincount(sub_idx.to(torch.int64), minlength=n)
+    dof_ptr = torch.zeros(n + 1, dtype=torch.int64, device=sub_idx.device)
+    dof_ptr[1:] = torch.cumsum(counts, 0)
+    return dof_ptr.to(torch.int32), order.to(torch.int32)
+
+
+def extract_blocks(crow, col, val, sub_ptr, sub_idx, first: int, last: int, kpad: int) -> torch.Tensor:
+    """Dense local matrices ``A[idx_i][:, idx_i]`` for subdomains ``first..last-1``.
+
+    Returns ``(last-first, kpad, kpad)`` FP64 with the identity in the padding
+    rows/columns (so every block stays invertible). Entries are located with a
+    sorted-key search, the vectorised form of the reference's per-row scan
+    (``solvers.py:407-423``).
+    """
+    dev = crow.device
+    n = crow.numel() - 1
+    p0, p1 = int(sub_ptr[first]), int(sub_ptr[last])
+    B = last - first
+    out = torch.zeros(B, kpad, kpad, dtype=torch.float64, device=dev)
+    ks = (sub_ptr[first + 1:last + 1] - sub_ptr[first:last]).to(torch.int64)
+    # identity padding
+    ar = torch.arange(kpad, device=dev)
+    pad = ar[None, :] >= ks[:, None]
+    out.diagonal(dim1=1, dim2=2)[pad] = 1.0
+    if p1 == p0:
+        return out
+    pos = torch.arange(p0, p1, device=dev)
+    s_loc = torch.repeat_interleave(torch.arange(B, device=dev), ks)
+    lrow = pos - sub_ptr[first:last].to(torch.int64)[s_loc]
+    g = sub_idx[p0:p1].to(torch.int64)
+    mkey = s_loc * n + g  # sorted ascending
+    rs = crow[g].to(torch.int64)
+    cnt = crow[g + 1].to(torch.int64) - rs
+    e_row = torch.repeat_interleave(torch.arange(p1 - p0, device=dev), cnt)
+    e_off = torch.arange(int(cnt.sum()), device=dev) - torch.repeat_interleave(torch.cumsum(cnt, 0) - cnt, cnt)
+    e_idx = rs[e_row] + e_off
+    ecol = col[e_idx].to(torch.int64)
+    key = s_loc[e_row] * n + ecol
+    hit = torch.searchsorted(mkey, key)
+    hit_c = torch.clamp(hit, max=mkey.numel() - 1)
+    ok = mkey[hit_c] == key
+    lcol = hit_c - (sub_ptr[first:last].to(torch.int64)[s_loc[e_row]] - p0)
+    out[s_loc[e_row][ok], lrow[e_row][ok], lcol[ok]] = val[e_idx][ok].to(torch.float64)
+    return out
+
+
+def block_scales(inv: torch.Tensor, dtype: torch.dtype) -> torch.Tensor:
+    """Per-block power-of-two scales (FP32) for low-precision storage."""
+    t = TARGET_EXP[dtype]
+    B = inv.shape[0]
+    if t is None:
+        return torch.ones(B, dtype=torch.float32, device=inv.device)
+    amax = inv.abs().reshape(B, -1).amax(dim=1)
+    amax = torch.where(amax > 0, amax, torch.ones_like(amax))
+    m, e = torch.frexp(amax)  # amax = m * 2**e, m in [0.5, 1)
+    e = torch.where(m == 0.5, e - 1, e)  # exact powers of two
+    return torch.ldexp(torch.ones_like(amax), (e - t).to(torch.int32)).to(torch.float32)
+
+
+def quantize(inv: torch.Tensor, scales: torch.Tensor, dtype: torch.dtype) -> torch.Tensor:
+    """``Q = (B / s)`` rounded FP64 -> FP32 -> dtype (round to nearest even)."""
+    q = inv / scales.to(torch.float64)[:, None, None]
+    if dtype == torch.float64:
+        return q
+    return q.to(torch.float32).to(dtype)
+
+
+class BlockStore:
+    """Packed column-major inverse blocks of one precision."""
+
+    def __init__(self, ks: np.ndarray, dtype: torch.dtype, device):
+        self.dtype = dtype
+        self.V = 16 // ELEM_BYTES[dtype]
+        self.ks = ks.astype(np.int64)
+        self.lds = ((self.ks + self.V - 1) // self.V) * self.V
+        sizes = self.ks * self.lds
+        off = np.zeros(len(ks) + 1, dtype=np.int64)
+        np.cumsum(sizes, out=off[1:])
+        self.off_np = off
+        self.total = int(off[-1])
+        self.data = torch.zeros(max(self.total, self.V), dtype=dtype, device=device)
+        self.blk_off = torch.as_tensor(off[:-1], device=device)
+        self.scale = torch.ones(len(ks), dtype=torch.float32, device=device)
+
+    @property
+    def nbytes(self) -> int:
+        return self.total * ELEM_BYTES[self.dtype]
+
+    def put(self, first: int, inv: torch.Tensor) -> None:
+        """Stores blocks ``first..first+B-1`` from a padded (B, kpad, kpad) FP64 batch."""
+        B = inv.shape[0]
+        sc = block_scales(inv, self.dtype)
+        q = quantize(inv, sc, self.dtype)
+        self.scale[first:first + B] = sc
+        qt = q.transpose(1, 2)  # column-major: row c of qt is column c of q
+        for b in range(B):
+            i = first + b
+            k, ld = int(self.ks[i]), int(self.lds[i])
+            if k == 0:
+                continue
+            dst = self.data[self.off_np[i]:self.off_np[i] + k * ld].view(k, ld)
+            dst[:, :k] = qt[b, :k, :k]
+
+    def block(self, i: int) -> torch.Tensor:
+        """Dequantised FP64 block i (for tests)."""
+        k, ld = int(self.ks[i]), int(self.lds[i])
+        d = self.data[self.off_np[i]:self.off_np[i] + k * ld].view(k, ld)[:, :k]
+        return d.transpose(0, 1).to(torch.float64) * float(self.scale[i])
+
+
+def invert_blocks(blocks: torch.Tensor, ks: torch.Tensor) -> torch.Tensor:
+    """Inverse of each padded SPD block; padding rows/cols zeroed afterwards."""
+    inv = torch.linalg.inv(blocks)
+    kpad = blocks.shape[-1]
+    ar = torch.arange(kpad, device=blocks.device)
+    keep = ar[None, :] < ks[:, None]
+    mask = (keep[:, :, None] & keep[:, None, :]).to(inv.dtype)
+    return inv * mask
+
+
+def scipy_csr(A) -> sps.csr_matrix:
+    if isinstance(A, sps.spmatrix) or isinstance(A, sps.sparray):
+        return sps.csr_matrix(A)
+    crow = A.crow_indices().cpu().numpy()
+    col = A.col_indices().cpu().numpy()
+    val = A.values().cpu().numpy().astype(np.float64)
+    return sps.csr_matrix((val, col, crow), shape=tuple(A.shape))
+
+
+def round_up(x: int, m: int) -> int:
+    return (x + m - 1) // m * m
+
+
+def batch_for(kpad: int, budget_bytes: int = 2 << 30) -> int:
+    """Subdomains per setup batch so a padded FP64 batch (x3 for LU workspace)
+    stays within the budget."""
+    per = 3 * kpad * kpad * 8
+    return max(1, budget_bytes // max(per, 1))
+
+
+def ceil_log2(x: float) -> int:
+    return int(math.ceil(math.log2(x)))

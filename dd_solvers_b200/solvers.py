@@ -1,0 +1,807 @@
+"""Schwarz-preconditioned CG on B200: drop-in for the reference's ``dd_solvers.solvers``.
+
+Public names, constructor signatures, ``setup``/``solve``/``destroy`` and the
+metadata keys follow ``src/dd_solvers/dd_solvers/solvers.py`` of mgr0dzicki/dd-solvers:
+
+* ``CG`` (192-303): PCG with optional preconditioner; stops on
+  ``||r|| < max(atol, rtol ||b||)``; ``iterations = len(residual_norms) - 1``;
+  raises ``ConvergenceNotAchieved`` when the loop reaches ``maxiter - 1``.
+* ``AdditiveSchwarz`` (774-826), ``HybridSchwarz`` (829-906): two-level Schwarz
+  with explicit local inverses ``Inv`` (343-359) and a coarse solver ``CUDSS``
+  (85-113).
+* helpers ``asm_permutation`` (541-551), ``permute_csr_tensor`` (125-167),
+  ``inverse_permutation`` (306-309), ``csr_to_torch`` (116-122), ``timeit`` (48-65),
+  ``collect`` (40-45).
+
+What runs where: every per-iteration operation is a kernel of ``libddx.so``
+(``include/ddx.h``) launched on the current torch stream: SELL-32 SpMV with the
+p.q / residual epilogues, the TMA-staged local-inverse apply, the transpose-map
+prolongation with the coarse correction and the r.z dots, and the fused x/r/p
+updates. Step lengths, dot products and the stop test are evaluated on the
+device, so the loop needs no host synchronisation; the host polls the number
+of active right-hand sides every ``check_every`` iterations, and each chunk of
+iterations is replayed from a CUDA graph. There is no CPU path: CPU tensors
+are rejected.
+
+Extensions (keyword-only): several right-hand sides as an ``(n, R)`` block;
+overlapping/uneven subdomains (``subdomains=(sub_ptr, sub_idx)``) and a
+general coarse restriction (``coarse_restriction=R0``) in ``setup``; FP32/BF16/
+FP16 block storage with per-block power-of-two scales and FP32 accumulation;
+flexible (Polak-Ribiere) PCG and periodic residual replacement.
+"""
+from __future__ import annotations
+
+import gc
+import math
+from abc import ABC, abstractmethod
+from typing import Any, Tuple
+
+import numpy as np
+import scipy.sparse as sps
+import torch
+
+from . import _lib as L
+from . import setup_ops as so
+from .bsr import FastBSR
+from .cusparse import csr_to_bsr, gather_csr, sort_csr
+from .gemv import gemv_strided_batched
+from . import cudss
+
+Metadata = dict[str, Any]
+
+__all__ = [
+    "ConvergenceNotAchieved", "collect", "timeit", "SparseSolver", "CUDSS", "csr_to_torch",
+    "permute_csr_tensor", "CG", "inverse_permutation", "DenseBatchSolver", "Inv", "asm_permutation",
+    "SchwarzOperator", "AdditiveSchwarz", "HybridSchwarz", "FastBSR", "csr_to_bsr", "sort_csr",
+    "gather_csr", "gemv_strided_batched",
+]
+
+
+class ConvergenceNotAchieved(Exception):
+    def __init__(self, metadata: Metadata):
+        self.metadata = metadata
+        if "iterations" not in self.metadata:
+            msg = "Convergence not achieved."
+        else:
+            msg = f"Convergence not achieved in {self.metadata['iterations']} iterations."
+        super().__init__(msg)
+
+
+def collect():
+    """Collects garbage and clears the CUDA cache."""
+    gc.collect()
+    if torch.cuda.is_available():
+        torch.cuda.empty_cache()
+
+
+def timeit(fun, warmup_iters=10, iters=10, repetitions=20):
+    """Min over ``repetitions`` of the mean CUDA-event time of ``iters`` calls (ms)."""
+    times = []
+    for _ in range(repetitions):
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        for _ in range(warmup_iters):
+            fun()
+        start.record()
+        for _ in range(iters):
+            fun()
+        end.record()
+        torch.cuda.synchronize()
+        times.append(start.elapsed_time(end) / iters)
+    return min(times)
+
+
+class SparseSolver(ABC):
+    @abstractmethod
+    def setup(self, matrix: torch.Tensor, *args, **kwargs) -> Metadata | None:
+        """Setup the solver with the given matrix in CSR format."""
+
+    @abstractmethod
+    def solve(self, rhs: torch.Tensor) -> Tuple[torch.Tensor, Metadata]:
+        pass
+
+    @abstractmethod
+    def destroy(self) -> None:
+        pass
+
+
+# ---------------------------------------------------------------------------
+# Coarse solver
+# ---------------------------------------------------------------------------
+
+class CUDSS(SparseSolver):
+    """SPD coarse solver with the reference's ``CUDSS`` interface (85-113).
+
+    cuDSS is not installed in this image, so the factorisation is a dense FP64
+    Cholesky (cuSOLVER through ``torch.linalg.cholesky``) turned once into the
+    explicit inverse; each solve is one HBM-bound ``ddx_coarse_gemv_f64``
+    launch (coarse sizes here are at most a few thousand).
+    """
+
+    def __str__(self):
+        return "CUDSS"
+
+    def setup(self, matrix: torch.Tensor, *args, **kwargs) -> None:
+        assert matrix.is_cuda
+        assert matrix.dtype in [torch.float32, torch.float64]
+        assert matrix.values().shape[0] < 2 ** 31
+        self.solver = cudss.spd_factorize(matrix)
+        self.dtype = matrix.dtype
+
+    def solve(self, rhs: torch.Tensor) -> Tuple[torch.Tensor, Metadata]:
+        assert rhs.is_cuda
+        assert rhs.dtype == self.dtype
+        return self.solver.solve(rhs), {}
+
+    @property
+    def inverse(self) -> torch.Tensor:
+        return self.solver.inverse
+
+    def destroy(self):
+        self.solver = None
+
+
+def csr_to_torch(csr: sps.csr_matrix) -> torch.Tensor:
+    return torch.sparse_csr_tensor(
+        torch.as_tensor(csr.indptr), torch.as_tensor(csr.indices), torch.as_tensor(csr.data), csr.shape)
+
+
+def permute_csr_tensor(mat: torch.Tensor, perm: torch.Tensor) -> torch.Tensor:
+    """Returns CSR matrix ``Ap`` such that ``Ap[perm][:, perm] == A`` (solvers.py:125-167).
+
+    Row ``i`` of ``A`` becomes row ``perm[i]`` of ``Ap`` and column ``j`` becomes
+    ``perm[j]``; columns are then sorted within each row.
+    """
+    indptr = mat.crow_indices().to(torch.int64)
+    indices = mat.col_indices().to(torch.int64)
+    values = mat.values()
+    n = mat.shape[0]
+    perm = perm.to(device=indptr.device, dtype=torch.int64)
+    row_sizes = indptr[1:] - indptr[:-1]
+    new_sizes = torch.empty_like(row_sizes)
+    new_sizes[perm] = row_sizes
+    indptr2 = torch.zeros_like(indptr)
+    indptr2[1:] = torch.cumsum(new_sizes, 0)
+    rows = torch.repeat_interleave(torch.arange(n, device=indptr.device), row_sizes)
+    new_rows = perm[rows]
+    new_cols = perm[indices]
+    key = new_rows * mat.shape[1] + new_cols
+    order = torch.argsort(key)
+    return torch.sparse_csr_tensor(indptr2, new_cols[order].to(mat.col_indices().dtype),
+                                   values[order], mat.shape)
+
+
+def inverse_permutation(perm: torch.Tensor) -> torch.Tensor:
+    inv_perm = torch.empty_like(perm)
+    inv_perm[perm] = torch.arange(len(perm), device=perm.device, dtype=perm.dtype)
+    return inv_perm
+
+
+def asm_permutation(fine_to_solvers: torch.Tensor, solvers_to_coarse: torch.Tensor,
+                    fine_to_dofs: torch.Tensor) -> torch.Tensor:
+    """DOF permutation grouping DOFs by (coarse group, solver) (solvers.py:541-551)."""
+    n_solvers = solvers_to_coarse.shape[0]
+    solver_indices = fine_to_dofs[fine_to_solvers.argsort(stable=True)].reshape(n_solvers, -1)
+    return solver_indices[solvers_to_coarse.argsort(stable=True)].flatten()
+
+
+# ---------------------------------------------------------------------------
+# Dense local solvers
+# ---------------------------------------------------------------------------
+
+class DenseBatchSolver(ABC):
+    @abstractmethod
+    def setup(self, matrix_batch: torch.Tensor):
+        """matrix should have shape (batch_size, n, n)"""
+
+    @abstractmethod
+    def solve(self, rhs_batch: torch.Tensor) -> torch.Tensor:
+        pass
+
+
+class Inv(DenseBatchSolver):
+    """Explicit inverses applied by a batched GEMV (solvers.py:343-359).
+
+    ``precision`` is the storage type of the inverse blocks. Used standalone it
+    behaves like the reference (column-major ``torch.linalg.inv``, downcast,
+    ``gemv_strided_batched``). Inside the Schwarz operators the blocks are
+    inverted in FP64 and stored with a per-block power-of-two scale when
+    ``precision`` is FP32/BF16/FP16.
+    """
+
+    def __init__(self, precision: torch.dtype | None = None):
+        self.precision = precision
+
+    def __str__(self):
+        return f"Inv({self.precision or ''})"
+
+    def setup(self, matrix_batch: torch.Tensor):
+        inv = torch.linalg.inv(matrix_batch)
+        # column-major, like the reference's result of torch.linalg.inv
+        inv = inv.transpose(1, 2).contiguous().transpose(1, 2)
+        self.matrix_inv = inv.to(self.precision) if self.precision is not None else inv
+
+    def solve(self, rhs_batch: torch.Tensor) -> torch.Tensor:
+        return gemv_strided_batched(self.matrix_inv, rhs_batch.reshape(self.matrix_inv.shape[0], -1))
+
+
+# ---------------------------------------------------------------------------
+# Schwarz operators
+# ---------------------------------------------------------------------------
+
+def _to_scipy_R(R0, n: int) -> sps.csr_matrix:
+    if R0 is None:
+        return None
+    if isinstance(R0, torch.Tensor):
+        R0 = so.scipy_csr(R0)
+    R0 = sps.csr_matrix(R0, dtype=np.float64)
+    R0.sort_indices()
+    assert R0.shape[1] == n
+    return R0
+
+
+def _csr_dev(M: sps.csr_matrix, device):
+    M = sps.csr_matrix(M)
+    M.sort_indices()
+    return (torch.as_tensor(M.indptr.astype(np.int32), device=device),
+            torch.as_tensor(M.indices.astype(np.int32), device=device),
+            torch.as_tensor(M.data.astype(np.float64), device=device))
+
+
+class SchwarzOperator(SparseSolver):
+    """Two-level Schwarz with explicit local inverses (solvers.py:554-771).
+
+    ``setup(matrix, dofs_per_solver, solvers_per_coarse)`` reproduces the
+    reference layout (equal contiguous blocks, P0 coarse groups). Keyword-only
+    ``subdomains=(sub_ptr, sub_idx)`` gives overlapping/uneven index sets and
+    ``coarse_restriction=R0`` (``n_c x n``, SciPy or torch CSR) a general coarse
+    space (P0 aggregates of ``owner`` when ``owner=`` is given instead).
+    """
+
+    def __init__(self, preconditioner_precision: torch.dtype, local_solver: DenseBatchSolver,
+                 coarse_solver: SparseSolver | None, collect_timings: bool = False):
+        self.preconditioner_precision = preconditioner_precision
+        self.local_solver = local_solver
+        self.coarse_solver = coarse_solver
+        self.collect_timings = collect_timings
+        self._scratch = {}
+
+    # -- setup -------------------------------------------------------------
+    def setup(self, matrix: torch.Tensor, dofs_per_solver: int | None = None,
+              solvers_per_coarse: torch.Tensor | None = None, *args, subdomains=None,
+              coarse_restriction=None, owner=None, **kwargs):
+        assert matrix.is_sparse_csr
+        L.require_cuda(matrix, "matrix")
+        self.device = matrix.device
+        n = matrix.shape[0]
+        self.n = n
+        if self.collect_timings:
+            events = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            events[0].record()
+        A_sp = so.scipy_csr(matrix)
+        if subdomains is None:
+            assert dofs_per_solver is not None and solvers_per_coarse is not None
+            spc = solvers_per_coarse.to("cpu", torch.int64).numpy()
+            self.solvers_per_coarse = solvers_per_coarse
+            self.dofs_per_solver = int(dofs_per_solver)
+            self.n_solvers = int(spc.sum())
+            self.n_coarse = len(spc)
+            sub_ptr, sub_idx = np.arange(self.n_solvers + 1, dtype=np.int64) * self.dofs_per_solver, \
+                np.arange(n, dtype=np.int32)
+            assert sub_ptr[-1] == n, "dofs_per_solver * n_solvers must equal the matrix size"
+            solvers_to_coarse = np.repeat(np.arange(self.n_coarse), spc)
+            owner_np = np.repeat(np.arange(self.n_solvers), self.dofs_per_solver)
+            R0 = sps.csr_matrix((np.ones(n), (solvers_to_coarse[owner_np], np.arange(n))),
+                                shape=(self.n_coarse, n))
+            R0.sort_indices()
+        else:
+            sub_ptr, sub_idx = (np.asarray(t.cpu() if isinstance(t, torch.Tensor) else t) for t in subdomains)
+            sub_ptr = sub_ptr.astype(np.int64)
+            sub_idx = sub_idx.astype(np.int32)
+            self.n_solvers = len(sub_ptr) - 1
+            if coarse_restriction is not None:
+                R0 = _to_scipy_R(coarse_restriction, n)
+            elif owner is not None:
+                own = np.asarray(owner.cpu() if isinstance(owner, torch.Tensor) else owner)
+                R0 = sps.csr_matrix((np.ones(n), (own.astype(np.int64), np.arange(n))),
+                                    shape=(int(own.max()) + 1, n))
+                R0.sort_indices()
+            else:
+                R0 = None
+            self.n_coarse = 0 if R0 is None else R0.shape[0]
+        if self.coarse_solver is None:
+            R0 = None
+            self.n_coarse = 0
+        self._R0_sp = R0
+        if self.collect_timings:
+            events[1].record()
+
+        # coarse space
+        if R0 is not None:
+            Ac = (R0 @ A_sp @ R0.T).tocsr()
+            Ac.sort_indices()
+            Ac_t = torch.sparse_csr_tensor(torch.as_tensor(Ac.indptr), torch.as_tensor(Ac.indices),
+                                           torch.as_tensor(Ac.data), Ac.shape).to(self.device)
+            self.coarse_solver.setup(Ac_t)
+            self._R0 = _csr_dev(R0, self.device)
+            self._P = _csr_dev(R0.T.tocsr(), self.device)
+            self._fused_coarse = isinstance(self.coarse_solver, CUDSS)
+        if self.collect_timings:
+            events[2].record()
+
+        # local blocks
+        dev = self.device
+        ks = np.diff(sub_ptr)
+        self.ks = ks
+        self.kmax = int(ks.max()) if len(ks) else 0
+        block_dtype = (getattr(self.local_solver, "precision", None) or self.preconditioner_precision
+                       or matrix.dtype)
+        if not isinstance(self.local_solver, Inv):
+            raise NotImplementedError("only Inv local solvers are implemented on this path")
+        self.block_dtype = block_dtype
+        self.acc_dtype = torch.float64 if block_dtype == torch.float64 else torch.float32
+        self.sub_ptr = torch.as_tensor(sub_ptr, device=dev)
+        self.sub_idx = torch.as_tensor(sub_idx, device=dev)
+        self.order = torch.as_tensor(np.argsort(-ks, kind="stable").astype(np.int32), device=dev)
+        self.dof_ptr, self.dof_src = so.transpose_map(self.sub_idx, n)
+        self.store = so.BlockStore(ks, block_dtype, dev)
+        crow = torch.as_tensor(A_sp.indptr.astype(np.int64), device=dev)
+        col = torch.as_tensor(A_sp.indices.astype(np.int64), device=dev)
+        val = torch.as_tensor(A_sp.data, device=dev)
+        kpad = so.round_up(max(self.kmax, 1), 16)
+        # group subdomains of similar size to bound padding work
+        order_np = np.argsort(ks, kind="stable")
+        bsz = so.batch_for(kpad)
+        i = 0
+        N = self.n_solvers
+        # process in index order in batches; kpad per batch from the batch's max k
+        while i < N:
+            j = min(N, i + bsz)
+            kb = so.round_up(max(int(ks[i:j].max()), 1), 16)
+            blocks = so.extract_blocks(crow, col, val, self.sub_ptr, self.sub_idx, i, j, kb)
+            inv = so.invert_blocks(blocks, torch.as_tensor(ks[i:j], device=dev))
+            del blocks
+            self.store.put(i, inv)
+            del inv
+            i = j
+        del order_np
+        if self.collect_timings:
+            events[3].record()
+            torch.cuda.synchronize()
+            timings = {
+                "preprocessing time": events[0].elapsed_time(events[1]),
+                "coarse solver setup time": events[1].elapsed_time(events[2]),
+                "local solver setup time": events[2].elapsed_time(events[3]),
+            }
+            if self.n_coarse:
+                x_c = torch.rand(self.n_coarse, device=dev, dtype=torch.float64)
+                timings["coarse solver solve time"] = timeit(lambda: self.coarse_solver.solve(x_c))
+            x_i = torch.rand(n, device=dev, dtype=torch.float64)
+            timings["local solver solve time"] = timeit(lambda: self._local(x_i.view(n, 1), 1))
+            return timings
+        return None
+
+    def destroy(self) -> None:
+        if self.coarse_solver is not None:
+            self.coarse_solver.destroy()
+        self._scratch = {}
+
+    # -- kernels -----------------------------------------------------------
+    @property
+    def local_bytes(self) -> int:
+        return self.store.nbytes
+
+    def scratch(self, R: int) -> dict:
+        s = self._scratch.get(R)
+        if s is None:
+            dev = self.device
+            nloc = int(self.sub_idx.numel())
+            s = {"ylocal": torch.empty(max(nloc, 1) * R, dtype=self.acc_dtype, device=dev),
+                 "y": torch.empty(self.n * R, dtype=torch.float64, device=dev)}
+            if self.n_coarse:
+                s["w"] = torch.empty(self.n_coarse * R, dtype=torch.float64, device=dev)
+                s["yc"] = torch.empty(self.n_coarse * R, dtype=torch.float64, device=dev)
+            self._scratch[R] = s
+        return s
+
+    def _local(self, r: torch.Tensor, R: int, ist: torch.Tensor | None = None) -> torch.Tensor:
+        s = self.scratch(R)
+        L.call("ddx_schwarz_local_apply", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
+               L.ptr(self.order), L.ptr(self.store.blk_off), L.ptr(self.store.data),
+               L.DTYPE_CODE[self.block_dtype], L.ptr(self.store.scale), self.kmax, L.ptr(r),
+               L.ptr(s["ylocal"]), L.DTYPE_CODE[self.acc_dtype], L.ptr(ist), L.stream_ptr())
+        return s["ylocal"]
+
+    def _restrict(self, rowptr, col, val, x, out, R):
+        L.call("ddx_spmv_csr_rowblock_f64", rowptr.numel() - 1, R, L.ptr(rowptr), L.ptr(col), L.ptr(val),
+               L.ptr(x), L.ptr(out), L.stream_ptr())
+
+    def _coarse(self, w, yc, R, ist=None):
+        if self._fused_coarse:
+            L.call("ddx_coarse_gemv_f64", self.n_coarse, R, L.ptr(self.coarse_solver.inverse), L.ptr(w),
+                   L.ptr(yc), L.ptr(ist), L.stream_ptr())
+        else:
+            out, _ = self.coarse_solver.solve(w.view(self.n_coarse, R).squeeze(-1) if R == 1 else
+                                              w.view(self.n_coarse, R))
+            yc.copy_(out.reshape(-1))
+
+    def _combine(self, z, R, ylocal=None, u=None, prolong=False, sign=1.0, pcg=None, r=None, q=None):
+        s = self.scratch(R)
+        p_ptr = p_col = p_val = yc = None
+        if prolong:
+            p_ptr, p_col, p_val = self._P
+            yc = s["yc"]
+        st = ist = partials = tickets = None
+        dots = 0
+        if pcg is not None:
+            st, ist, partials, tickets = pcg.st, pcg.ist, pcg.partials, pcg.tickets
+            dots = 1
+        L.call("ddx_schwarz_combine", self.n, R, L.ptr(self.dof_ptr), L.ptr(self.dof_src), L.ptr(ylocal),
+               L.DTYPE_CODE[self.acc_dtype], L.ptr(u), L.ptr(p_ptr), L.ptr(p_col), L.ptr(p_val), L.ptr(yc),
+               float(sign), L.ptr(z), dots, L.ptr(r), L.ptr(q), L.ptr(st), L.ptr(ist), L.ptr(partials),
+               L.ptr(tickets), L.stream_ptr())
+
+    # Applied by the fused PCG loop: z = M r with rho = r.z (and z.q) -> beta.
+    def _apply_fused(self, r, z, R, pcg, q):
+        raise NotImplementedError
+
+    def _apply(self, rhs: torch.Tensor) -> torch.Tensor:
+        L.require_cuda(rhs, "rhs")
+        R = 1 if rhs.dim() == 1 else rhs.shape[1]
+        x = rhs.to(torch.float64).contiguous()
+        z = torch.empty(self.n * R, dtype=torch.float64, device=rhs.device)
+        self._apply_fused(x.view(-1), z, R, None, None)
+        return z.view(rhs.shape).to(rhs.dtype)
+
+    def solve(self, rhs: torch.Tensor) -> tuple[torch.Tensor, Metadata]:
+        return self._apply(rhs), {}
+
+
+class AdditiveSchwarz(SchwarzOperator):
+    """``y = sum_i R_i^T A_i^{-1} R_i x + R_0^T A_0^{-1} R_0 x`` (solvers.py:774-826)."""
+
+    def __init__(self, preconditioner_precision: torch.dtype, local_solver: DenseBatchSolver,
+                 coarse_solver: SparseSolver | None, number_of_dofs_per_coarse_is_const: bool = False,
+                 collect_timings: bool = False):
+        super().__init__(preconditioner_precision, local_solver, coarse_solver, collect_timings)
+        self.number_of_dofs_per_coarse_is_const = number_of_dofs_per_coarse_is_const
+
+    def __str__(self):
+        return (f"AdditiveSchwarz({self.preconditioner_precision}, {self.local_solver}, {self.coarse_solver}, "
+                f"const_dofs_per_coarse={self.number_of_dofs_per_coarse_is_const})")
+
+    def setup(self, matrix, dofs_per_solver=None, solvers_per_coarse=None, *args, **kwargs):
+        timings = super().setup(matrix, dofs_per_solver, solvers_per_coarse, *args, **kwargs)
+        if self.number_of_dofs_per_coarse_is_const and solvers_per_coarse is not None:
+            self.dofs_per_coarse = dofs_per_solver * int(self.solvers_per_coarse[0].item())
+        return timings
+
+    def _apply_fused(self, r, z, R, pcg, q):
+        s = self.scratch(R)
+        ist = None if pcg is None else pcg.ist
+        if self.n_coarse:
+            self._restrict(*self._R0, r, s["w"], R)
+            self._coarse(s["w"], s["yc"], R, ist)
+        ylocal = self._local(r, R, ist)
+        self._combine(z, R, ylocal=ylocal, prolong=bool(self.n_coarse), sign=1.0, pcg=pcg, r=r, q=q)
+
+
+class HybridSchwarz(SchwarzOperator):
+    """Projected local solves ``z = (I - R_0^T A_0^{-1} R_0 A) y`` (solvers.py:829-906)."""
+
+    def __str__(self):
+        return f"HybridSchwarz({self.preconditioner_precision}, {self.local_solver}, {self.coarse_solver})"
+
+    def setup(self, matrix, dofs_per_solver=None, solvers_per_coarse=None, *args, **kwargs):
+        timings = super().setup(matrix, dofs_per_solver, solvers_per_coarse, *args, **kwargs)
+        if self.n_coarse:
+            A_sp = so.scipy_csr(matrix)
+            AR = (self._R0_sp @ A_sp).tocsr()
+            AR.sum_duplicates()
+            self._AR = _csr_dev(AR, self.device)
+        return timings
+
+    def T0(self, rhs: torch.Tensor) -> torch.Tensor:
+        """``R_0^T A_0^{-1} R_0 b`` (solvers.py:861-872)."""
+        R = 1 if rhs.dim() == 1 else rhs.shape[1]
+        out = torch.zeros(self.n * R, dtype=torch.float64, device=rhs.device)
+        self._T0_into(rhs.to(torch.float64).contiguous().view(-1), out, R)
+        return out.view(rhs.shape).to(rhs.dtype)
+
+    def _T0_into(self, b, x, R, ist=None):
+        """x += R_0^T A_0^{-1} R_0 b."""
+        if not self.n_coarse:
+            return
+        s = self.scratch(R)
+        self._restrict(*self._R0, b, s["w"], R)
+        self._coarse(s["w"], s["yc"], R, ist)
+        self._combine(x, R, u=x, prolong=True, sign=1.0)
+
+    def _apply_fused(self, r, z, R, pcg, q):
+        s = self.scratch(R)
+        ist = None if pcg is None else pcg.ist
+        ylocal = self._local(r, R, ist)
+        if not self.n_coarse:
+            self._combine(z, R, ylocal=ylocal, pcg=pcg, r=r, q=q)
+            return
+        y = s["y"]
+        self._combine(y, R, ylocal=ylocal)
+        self._restrict(*self._AR, y, s["w"], R)
+        self._coarse(s["w"], s["yc"], R, ist)
+        self._combine(z, R, u=y, prolong=True, sign=-1.0, pcg=pcg, r=r, q=q)
+
+
+# ---------------------------------------------------------------------------
+# PCG
+# ---------------------------------------------------------------------------
+
+class _PcgWork:
+    """Device buffers of one solve shape (n, R)."""
+
+    def __init__(self, n: int, R: int, maxiter: int, device):
+        f = dict(dtype=torch.float64, device=device)
+        self.n, self.R = n, R
+        self.b = torch.empty(n * R, **f)
+        self.x = torch.empty(n * R, **f)
+        self.r = torch.empty(n * R, **f)
+        self.z = torch.empty(n * R, **f)
+        self.p = torch.zeros(n * R, **f)
+        self.q = torch.zeros(n * R, **f)
+        self.st = torch.zeros(L.ST_COUNT * R, **f)
+        self.ist = torch.zeros(L.IST_COUNT * R + L.G_COUNT, dtype=torch.int32, device=device)
+        self.maxiter = maxiter
+        self.hist = torch.zeros((maxiter + 1) * R, **f)
+        self.partials = torch.zeros(int(L.lib().ddx_partials_len(R)), **f)
+        self.tickets = torch.zeros(L.TICKETS, dtype=torch.int32, device=device)
+        self.graphs = {}
+        self.warm = False
+
+
+class _SellMatrix:
+    """The system matrix in SELL-32 (bsr_matmul=True) or CSR (R > 1) form."""
+
+    def __init__(self, matrix: torch.Tensor):
+        crow = matrix.crow_indices()
+        col = matrix.col_indices()
+        val = matrix.values().to(torch.float64)
+        self.n = matrix.shape[0]
+        self.crow32 = crow.to(torch.int32)
+        self.col32 = col.to(torch.int32)
+        self.val = val
+        self.sell = so.csr_to_sell32(crow.to(torch.int64), col, val)
+        self.nnz = int(col.numel())
+
+    def launch(self, x, y, R, mode, w: _PcgWork | None = None, b=None, use_sell=True):
+        st = ist = hist = partials = tickets = None
+        if w is not None:
+            st, ist, hist, partials, tickets = w.st, w.ist, w.hist, w.partials, w.tickets
+        if R == 1 and use_sell:
+            sp, sw, sc, sv = self.sell
+            L.call("ddx_spmv_sell_f64", self.n, sw.numel(), L.ptr(sp), L.ptr(sw), L.ptr(sc), L.ptr(sv), L.ptr(x),
+                   L.ptr(y), L.ptr(b), mode, L.ptr(st), L.ptr(ist), L.ptr(hist), L.ptr(partials), L.ptr(tickets),
+                   L.stream_ptr())
+        else:
+            L.call("ddx_spmv_csr_f64", self.n, R, L.ptr(self.crow32), L.ptr(self.col32), L.ptr(self.val), L.ptr(x),
+                   L.ptr(y), L.ptr(b), mode, L.ptr(st), L.ptr(ist), L.ptr(hist), L.ptr(partials), L.ptr(tickets),
+                   L.stream_ptr())
+
+    def __matmul__(self, x: torch.Tensor) -> torch.Tensor:
+        R = 1 if x.dim() == 1 else x.shape[1]
+        xx = x.to(torch.float64).contiguous()
+        y = torch.empty_like(xx)
+        self.launch(xx, y, R, L.SPMV_PLAIN)
+        return y.to(x.dtype)
+
+
+class CG(SparseSolver):
+    """Preconditioned conjugate gradients (solvers.py:192-303).
+
+    Keyword-only extensions: ``flexible`` (Polak-Ribiere beta; default: on when
+    the preconditioner stores its blocks below FP64), ``replace_every``
+    (recompute r = b - A x every so many iterations), ``check_every``
+    (iterations per host poll), ``use_graph`` (replay chunks from CUDA graphs).
+    """
+
+    def __init__(self, preconditioner: SparseSolver | None = None, rtol: float = 1e-7, atol: float = 0,
+                 maxiter: int | None = 1000, bsr_matmul: bool = True, estimate_cond: bool = False, *,
+                 flexible: bool | None = None, replace_every: int = 0, check_every: int = 8,
+                 use_graph: bool = True):
+        self.preconditioner = preconditioner
+        self.rtol = rtol
+        self.atol = atol
+        self.maxiter = maxiter
+        self.bsr_matmul = bsr_matmul
+        self.estimate_cond = estimate_cond
+        self.flexible = flexible
+        self.replace_every = replace_every
+        self.check_every = check_every
+        self.use_graph = use_graph
+        self._work = {}
+
+    def __str__(self):
+        return f"CG({self.preconditioner or ''}, bsr_matmul={self.bsr_matmul})"
+
+    def setup(self, matrix: torch.Tensor, *args, **kwargs) -> None:
+        L.require_cuda(matrix, "matrix")
+        if matrix.layout != torch.sparse_csr:
+            matrix = matrix.to_sparse_csr()
+        timings = None
+        if self.preconditioner is not None:
+            timings = self.preconditioner.setup(matrix, *args, **kwargs)
+        if self.bsr_matmul and "block_size" not in kwargs:
+            raise ValueError("Unable to determine block size for BSR matrix multiplication.")
+        self.block_size = kwargs.get("block_size", 1)
+        self.matrix = _SellMatrix(matrix)
+        self.n = matrix.shape[0]
+        self._work = {}
+        return timings
+
+    # -- helpers -------------------------------------------------------------
+    def _is_flexible(self) -> bool:
+        if self.flexible is not None:
+            return bool(self.flexible)
+        pc = self.preconditioner
+        return isinstance(pc, SchwarzOperator) and pc.block_dtype != torch.float64
+
+    def _work_for(self, R: int, maxiter: int) -> _PcgWork:
+        w = self._work.get(R)
+        if w is None or w.maxiter < maxiter:
+            w = _PcgWork(self.n, R, maxiter, self.matrix.val.device)
+            self._work[R] = w
+        return w
+
+    def _precondition(self, w: _PcgWork):
+        pc = self.preconditioner
+        R = w.R
+        if pc is None:
+            L.call("ddx_pcg_dots_rz", self.n, R, L.ptr(w.r), L.ptr(w.r), L.ptr(w.q), L.ptr(w.st), L.ptr(w.ist),
+                   L.ptr(w.partials), L.ptr(w.tickets), L.stream_ptr())
+            return w.r
+        if isinstance(pc, SchwarzOperator):
+            pc._apply_fused(w.r, w.z, R, w, w.q)
+            return w.z
+        # generic preconditioner: Python-level solve, then the fused dots
+        rr = w.r.view(self.n, R) if R > 1 else w.r
+        z, _ = pc.solve(rr)
+        w.z.copy_(z.reshape(-1).to(torch.float64))
+        L.call("ddx_pcg_dots_rz", self.n, R, L.ptr(w.r), L.ptr(w.z), L.ptr(w.q), L.ptr(w.st), L.ptr(w.ist),
+               L.ptr(w.partials), L.ptr(w.tickets), L.stream_ptr())
+        return w.z
+
+    def _iteration(self, w: _PcgWork, replace: bool):
+        R = w.R
+        z = self._precondition(w)
+        L.call("ddx_pcg_update_p", self.n, R, L.ptr(z), L.ptr(w.p), L.ptr(w.st), L.ptr(w.ist), L.stream_ptr())
+        self.matrix.launch(w.p, w.q, R, L.SPMV_PQ, w, use_sell=self.bsr_matmul)
+        L.call("ddx_pcg_update_xr", self.n, R, L.ptr(w.x), L.ptr(w.r), L.ptr(w.p), L.ptr(w.q), L.ptr(w.st),
+               L.ptr(w.ist), L.ptr(w.hist), L.ptr(w.partials), L.ptr(w.tickets), L.stream_ptr())
+        if replace:
+            self.matrix.launch(w.x, w.r, R, L.SPMV_RES_REPLACE, w, b=w.b, use_sell=self.bsr_matmul)
+
+    def _chunk(self, w: _PcgWork, k: int, start: int):
+        re = self.replace_every
+        plan = tuple(bool(re) and ((start + i + 1) % re == 0) for i in range(k))
+        graphable = self.use_graph and (self.preconditioner is None or isinstance(self.preconditioner, SchwarzOperator))
+        if not graphable:
+            for rep in plan:
+                self._iteration(w, rep)
+            return
+        g = w.graphs.get(plan)
+        if g is None:
+            if not w.warm:
+                # first chunk runs eagerly: kernel attributes and scratch buffers
+                # are set up outside any capture
+                for rep in plan:
+                    self._iteration(w, rep)
+                w.warm = True
+                return
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                for rep in plan:
+                    self._iteration(w, rep)
+            w.graphs[plan] = g
+        g.replay()
+
+    # -- solve ---------------------------------------------------------------
+    def solve(self, rhs: torch.Tensor, x0=None) -> Tuple[torch.Tensor, Metadata]:
+        L.require_cuda(rhs, "rhs")
+        n = self.n
+        R = 1 if rhs.dim() == 1 else rhs.shape[1]
+        Rp = 1 << max(0, (R - 1).bit_length())
+        if Rp > 64:
+            raise ValueError("at most 64 right-hand sides per solve")
+        maxiter = self.maxiter or n * 10
+        w = self._work_for(Rp, maxiter)
+        flexible = self._is_flexible()
+        if isinstance(self.preconditioner, SchwarzOperator):
+            self.preconditioner.scratch(Rp)
+        # stage b and x (padded RHS columns are zero: inactive from the start)
+        bmat = w.b.view(n, Rp)
+        xmat = w.x.view(n, Rp)
+        bmat.zero_()
+        bmat[:, :R] = rhs.view(n, R).to(torch.float64)
+        xmat.zero_()
+        if x0 is not None:
+            xmat[:, :R] = x0.view(n, R).to(torch.float64)
+        w.p.zero_()
+        w.q.zero_()
+        L.call("ddx_pcg_reset", Rp, L.ptr(w.st), L.ptr(w.ist), maxiter, int(flexible), float(self.rtol),
+               float(self.atol), L.stream_ptr())
+        pc = self.preconditioner
+        if pc is not None and hasattr(pc, "T0"):
+            if isinstance(pc, HybridSchwarz):
+                pc._T0_into(w.b, w.x, Rp)
+            else:
+                xmat[:, :R] += pc.T0(rhs).view(n, R).to(torch.float64)
+        self.matrix.launch(w.x, w.r, Rp, L.SPMV_RES_INIT, w, b=w.b, use_sell=self.bsr_matmul)
+
+        alphas, betas = [], []
+        done = 0
+        k = max(1, int(self.check_every))
+        if self.replace_every:
+            k = math.gcd(k, int(self.replace_every))
+        if self.estimate_cond:
+            k = 1
+        active = int(w.ist[L.IST_COUNT * Rp + L.G_NACTIVE].item())
+        while active > 0 and done < maxiter:
+            kk = min(k, maxiter - done)
+            if kk != k or self.estimate_cond:
+                for i in range(kk):
+                    self._iteration(w, bool(self.replace_every) and (done + i + 1) % self.replace_every == 0)
+                    if self.estimate_cond:
+                        st = w.st.view(L.ST_COUNT, Rp)
+                        alphas.append(float(st[L.ST_ALPHA, 0]))
+                        betas.append(float(st[L.ST_BETA, 0]))
+            else:
+                self._chunk(w, kk, done)
+            done += kk
+            active = int(w.ist[L.IST_COUNT * Rp + L.G_NACTIVE].item())
+
+        # results and reference-compatible metadata
+        ist = w.ist[: L.IST_COUNT * Rp].view(L.IST_COUNT, Rp).cpu()
+        st = w.st.view(L.ST_COUNT, Rp).cpu()
+        hist = w.hist.view(-1, Rp)[: maxiter + 1].cpu()
+        x = xmat[:, :R].clone()
+        out = x.view(rhs.shape).to(rhs.dtype)
+        if x0 is not None:
+            x0.copy_(out.view(x0.shape))
+            out = x0
+        its, norms, failed = [], [], False
+        for j in range(R):
+            it = int(ist[L.IST_ITERS, j])
+            atol_j = float(st[L.ST_ATOL, j])
+            conv = float(hist[it, j]) < atol_j or (float(st[L.ST_BB, j]) == 0.0 and it == 0)
+            if conv:
+                its.append(it)
+                norms.append([float(v) for v in hist[: it + 1, j]])
+                if it + 1 >= maxiter:
+                    failed = True
+            else:
+                its.append(maxiter - 1)
+                norms.append([float(v) for v in hist[:maxiter, j]])
+                failed = True
+        if R == 1 and rhs.dim() == 1:
+            metadata = {"iterations": its[0], "residual norms": norms[0],
+                        "preconditioner metadata": [{} for _ in range(its[0])]}
+        else:
+            metadata = {"iterations": its, "residual norms": norms,
+                        "preconditioner metadata": [{} for _ in range(max(its) if its else 0)]}
+        if self.estimate_cond:
+            nal = len(alphas)
+            lmat = torch.zeros((nal, nal), dtype=torch.float64)
+            for i in range(nal):
+                lmat[i, i] = 1 / alphas[i]
+                if i > 0:
+                    lmat[i, i] += betas[i] / alphas[i - 1]
+                    lmat[i - 1, i] = lmat[i, i - 1] = betas[i] ** 0.5 / alphas[i - 1]
+            metadata["condition number estimate"] = torch.linalg.cond(lmat, p=2).item()
+        if failed:
+            raise ConvergenceNotAchieved(metadata)
+        return out, metadata
+
+    def destroy(self) -> None:
+        if self.preconditioner is not None:
+            self.preconditioner.destroy()
+            self.preconditioner = None
+        self.matrix = None
+        self._work = {}

@@ -1,0 +1,171 @@
+/*
+ * ddx.h - C ABI of the B200 (sm_100a) Schwarz-preconditioned CG kernels.
+ *
+ * Every entry point takes raw device pointers, sizes and a CUDA stream, never
+ * allocates device memory, launches asynchronously on `stream`, and returns a
+ * ddx_status (0 = success). The message of the last failure on the calling
+ * thread is returned by ddx_last_error().
+ *
+ * Vector blocks of several right-hand sides use the layout (n, R) with the R
+ * values of one DOF contiguous ("DOF-major"); R = 1 is a plain vector. The
+ * fused PCG kernels support R in {1, 2, 4, 8, 16, 32, 64}.
+ *
+ * References (paths within mgr0dzicki/dd-solvers) name the interface of the
+ * reference that each entry point replaces.
+ */
+#ifndef DDX_H
+#define DDX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* ddx_stream_t; /* same type as cudaStream_t */
+
+enum ddx_status {
+  DDX_OK = 0,
+  DDX_ERR_ARG = 1,         /* invalid argument (shape, alignment, dtype) */
+  DDX_ERR_CUDA = 2,        /* CUDA launch or runtime error */
+  DDX_ERR_UNSUPPORTED = 3  /* valid request this build does not implement */
+};
+
+enum ddx_dtype { DDX_F64 = 0, DDX_F32 = 1, DDX_BF16 = 2, DDX_F16 = 3 };
+
+/* ---- PCG state (device memory owned by the caller) ----------------------
+ * st   : double[DDX_ST_COUNT * R], slot s of RHS j at st[s*R + j]
+ * ist  : int[DDX_IST_COUNT * R + DDX_G_COUNT], slot s of RHS j at ist[s*R + j],
+ *        global g at ist[DDX_IST_COUNT*R + g]
+ * hist : double[(maxiter + 1) * R], residual norm after k updates of RHS j at
+ *        hist[k*R + j]
+ * partials / tickets: reduction scratch, sized by ddx_partials_len(R) doubles
+ *        and DDX_TICKETS unsigned ints (zero-initialised once by the caller;
+ *        every kernel leaves its ticket at zero again).
+ */
+enum {
+  DDX_ST_RHO = 0, DDX_ST_RHO_PREV = 1, DDX_ST_ZQ = 2, DDX_ST_PQ = 3, DDX_ST_ALPHA = 4,
+  DDX_ST_BETA = 5, DDX_ST_RR = 6, DDX_ST_ATOL = 7, DDX_ST_BB = 8, DDX_ST_COUNT = 9
+};
+enum { DDX_IST_ACTIVE = 0, DDX_IST_ITERS = 1, DDX_IST_COUNT = 2 };
+enum {
+  DDX_G_NACTIVE = 0,   /* number of RHS still iterating */
+  DDX_G_MAXITER = 1,   /* update limit per RHS */
+  DDX_G_FLEXIBLE = 2,  /* 1: Polak-Ribiere beta, 0: Fletcher-Reeves */
+  DDX_G_BREAKDOWN = 3, /* set when p.q <= 0 stopped a RHS */
+  DDX_G_COUNT = 4
+};
+enum { DDX_TICKETS = 16 };
+
+const char* ddx_last_error(void);
+int ddx_version(void);
+/* doubles needed for the `partials` scratch of the fused reductions */
+size_t ddx_partials_len(int R);
+/* Reads and clears the device-side error word (bounded-wait timeouts).
+ * Synchronous. 0 = no error. */
+int ddx_device_error(int* code);
+
+/* ---- PCG state and vector updates ---------------------------------------
+ * Replace CG.solve's torch ops: fused_add / fused_sub / fused_mul_add
+ * (src/dd_solvers/dd_solvers/solvers.py:170-189), torch.dot (256, 265) and
+ * torch.linalg.norm(r).item() (244), which become device-side deterministic
+ * reductions with the stop test evaluated on the device. */
+
+/* Initialise st/ist for a new solve: iterations 0, every RHS active,
+ * maxiter and flexible flags, tolerance constants. */
+int ddx_pcg_reset(int R, double* st, int* ist, int maxiter, int flexible, double rtol, double atol,
+                  ddx_stream_t stream);
+/* p = z + beta p (beta = 0 on a RHS's first iteration). */
+int ddx_pcg_update_p(int64_t n, int R, const double* z, double* p, const double* st, const int* ist,
+                     ddx_stream_t stream);
+/* x += alpha p; r -= alpha q; then rr = ||r||^2 per RHS, stop test, history. */
+int ddx_pcg_update_xr(int64_t n, int R, double* x, double* r, const double* p, const double* q,
+                      double* st, int* ist, double* hist, double* partials, unsigned int* tickets,
+                      ddx_stream_t stream);
+/* rho = r.z (and z.q when flexible) -> beta; for preconditioners that write z
+ * themselves (generic path). q may be NULL on the first iteration. */
+int ddx_pcg_dots_rz(int64_t n, int R, const double* r, const double* z, const double* q, double* st,
+                    int* ist, double* partials, unsigned int* tickets, ddx_stream_t stream);
+/* Residual replacement without SpMV fusion: recompute the stop test from r. */
+
+/* ---- Sparse matrix-vector products --------------------------------------
+ * Replace FastBSR.__matmul__ (src/dd_solvers/dd_solvers/bsr.py:24-25, RPT-I
+ * kernel 40-76) and torch's CSR matvec (solvers.py:264, 880).
+ *
+ * SELL-32 (R = 1): slice s holds rows [32s, 32s+32); entry j of row 32s+l is
+ * at slice_ptr[s] + 32*j + l (padding: value 0, column = own row).
+ * mode: 0 y = A x
+ *       1 y = A x, then p.q -> alpha (x is p, y is q; PCG step)
+ *       2 y = b - A x, then ||b||, ||y|| -> tolerance and active flags (PCG start)
+ *       3 y = b - A x, then ||y|| -> stop test (residual replacement)
+ */
+enum { DDX_SPMV_PLAIN = 0, DDX_SPMV_PQ = 1, DDX_SPMV_RES_INIT = 2, DDX_SPMV_RES_REPLACE = 3 };
+int ddx_spmv_sell_f64(int64_t n, int64_t nslices, const int64_t* slice_ptr, const int* slice_width,
+                      const int* cols, const double* vals, const double* x, double* y,
+                      const double* b, int mode, double* st, int* ist, double* hist,
+                      double* partials, unsigned int* tickets, ddx_stream_t stream);
+/* CSR, R right-hand sides in (n, R) layout (R threads per row). Same modes. */
+int ddx_spmv_csr_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols, const double* vals,
+                     const double* x, double* y, const double* b, int mode, double* st, int* ist,
+                     double* hist, double* partials, unsigned int* tickets, ddx_stream_t stream);
+/* CSR with long rows, one CTA per row, deterministic block reduction:
+ * y[row, j] = sum_k vals[k] x[cols[k], j] (coarse restriction A_R y or R0 r). */
+int ddx_spmv_csr_rowblock_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols,
+                              const double* vals, const double* x, double* y, ddx_stream_t stream);
+/* BSR, block size bs (1..8), blocks column-major (bs, bs) as produced by the
+ * reference's csr_to_bsr (src/dd_solvers/cpp/cusparse.cpp:22-107); dtype F64
+ * or F32 for vals/x/y. One warp per block row. */
+int ddx_spmv_bsr(int64_t n_block_rows, int bs, const int* row_ptr, const int* cols, const void* vals,
+                 const void* x, void* y, int dtype, ddx_stream_t stream);
+
+/* ---- Batched GEMV (reference op) ----------------------------------------
+ * Replaces dd_solvers_gemv::gemv_strided_batched
+ * (src/dd_solvers/cpp/gemv.cpp:9-53, kernels gemv_kernels.cu:31-139):
+ * out[b] = M_b v_b, M (N, k, k) column-major in mat_dtype, v/out (N, k) in
+ * vec_dtype (F32/F64); matrix entries are converted to the vector type and
+ * accumulated in it. mat F64 with vec F32 is rejected as in the reference. */
+int ddx_gemv_strided_batched(int64_t N, int k, const void* mat, int mat_dtype, const void* vec,
+                             void* out, int vec_dtype, ddx_stream_t stream);
+
+/* ---- Schwarz preconditioner ---------------------------------------------
+ * Replace AdditiveSchwarz.solve (solvers.py:811-826), HybridSchwarz.solve /
+ * T0 (861-888) and Inv.solve (355-359).
+ *
+ * Subdomain i has k_i = sub_ptr[i+1] - sub_ptr[i] DOFs sub_idx[sub_ptr[i]..].
+ * Its inverse block is stored column-major with leading dimension
+ * ld_i = round_up(k_i, 16 / sizeof(block element)) at element offset
+ * blk_off[i] (16-byte aligned); entry (row, col) at blk_off[i] + col*ld_i + row.
+ * Low-precision blocks carry a per-block scale: A_i^{-1} ~= scale[i] * Q_i.
+ * `order` lists subdomains by decreasing k (work distribution).
+ *
+ * local_apply: ylocal[sub_ptr[i] + t, j] = scale[i] * sum_c Q_i[t, c] r[sub_idx[sub_ptr[i]+c], j]
+ *   blocks are streamed through shared memory by bulk asynchronous copies
+ *   (TMA engine); accumulation in FP32 for F32/BF16/F16 blocks, FP64 for F64.
+ *   ylocal has element type acc (F32 or F64) and layout (sum k_i, R).
+ */
+int ddx_schwarz_local_apply(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
+                            const int* order, const int64_t* blk_off, const void* blocks,
+                            int block_dtype, const float* scale, int kmax, const double* r,
+                            void* ylocal, int acc_dtype, const int* ist, ddx_stream_t stream);
+/* combine: z[d, j] = sum_{t in T(d)} ylocal[src[t], j]      (if ylocal)
+ *                  + u[d, j]                                (if u)
+ *                  + sign * sum_c P[d, c] yc[c, j]          (if p_ptr)
+ * where T(d) = dof_ptr[d]..dof_ptr[d+1] lists the positions of DOF d in the
+ * subdomain-major ylocal (ascending subdomain order, so the sum order is
+ * fixed). With dots != 0 it also forms rho = r.z (and z.q when flexible) and
+ * beta on the device. u may alias z. */
+int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src, const void* ylocal,
+                        int acc_dtype, const double* u, const int* p_ptr, const int* p_col,
+                        const double* p_val, const double* yc, double sign, double* z, int dots,
+                        const double* r, const double* q, double* st, int* ist, double* partials,
+                        unsigned int* tickets, ddx_stream_t stream);
+/* Dense coarse solve with the explicit FP64 inverse (row-major, symmetric):
+ * yc[c, j] = sum_d Ainv[c, d] w[d, j]. */
+int ddx_coarse_gemv_f64(int n_c, int R, const double* Ainv, const double* w, double* yc,
+                        const int* ist, ddx_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DDX_H */

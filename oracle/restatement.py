@@ -1,0 +1,245 @@
+"""ORACLE (test infrastructure only): FP64 CPU restatement of Schwarz-PCG.
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this module, and only as the checker or the timed CPU
+baseline. The product path (``dd_solvers_b200``) never imports it.
+
+It restates the reference's algorithm with NumPy/SciPy in FP64 and generalises
+it to the cases the reference cannot express (overlapping and uneven
+subdomains, a general coarse restriction, several right-hand sides,
+low-precision block storage with per-block power-of-two scales):
+
+* ``pcg``                 - ``CG.solve`` (``src/dd_solvers/dd_solvers/solvers.py:228-297``):
+                            stop on ``||r|| < max(atol, rtol ||b||)`` checked at the top of
+                            each iteration, Fletcher-Reeves beta, ``iterations =
+                            len(residual_norms) - 1`` (276), ``ConvergenceNotAchieved``
+                            when the loop index reaches ``maxiter - 1`` (294-295).
+                            ``flexible=True`` swaps in the Polak-Ribiere beta.
+* ``Schwarz.local``       - ``sum_i R_i^T A_i^{-1} R_i r`` (``Inv.solve``, 355-359, on the
+                            ``reshape(n_solvers, -1)`` blocks of 814/878, generalised to
+                            index sets).
+* ``Schwarz.additive``    - ``AdditiveSchwarz.solve`` (811-826).
+* ``Schwarz.hybrid``      - ``HybridSchwarz.solve`` (874-888): ``y - R0^T A_C^{-1} (R0 A) y``.
+* ``Schwarz.T0``          - ``HybridSchwarz.T0`` (861-872).
+* ``coarse_matrix``       - ``R0 A R0^T`` (``_construct_coarse_solver_matrix``, 721-771).
+* ``quantize``            - ``Inv.setup`` downcast (350-353) plus the per-block
+                            power-of-two scale of this package's low-precision storage.
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.linalg as sla
+import scipy.sparse as sps
+
+
+class ConvergenceNotAchieved(Exception):
+    def __init__(self, metadata):
+        self.metadata = metadata
+        super().__init__(f"Convergence not achieved in {metadata.get('iterations')} iterations.")
+
+
+# ---------------------------------------------------------------------------
+# Low-precision emulation
+# ---------------------------------------------------------------------------
+
+def round_to_bf16(x: np.ndarray) -> np.ndarray:
+    """FP64 -> FP32 (nearest even) -> BF16 (nearest even), returned as FP64.
+
+    Matches ``tensor.to(torch.float32).to(torch.bfloat16)`` for finite values.
+    """
+    f = np.asarray(x, dtype=np.float32)
+    b = f.view(np.uint32).astype(np.uint64)
+    rounding = ((b >> 16) & 1) + 0x7FFF
+    b = ((b + rounding) & 0xFFFF0000).astype(np.uint32)
+    return b.view(np.float32).astype(np.float64)
+
+
+def round_to(x: np.ndarray, dtype: str) -> np.ndarray:
+    if dtype == "f64":
+        return np.asarray(x, dtype=np.float64)
+    if dtype == "f32":
+        return np.asarray(x, dtype=np.float32).astype(np.float64)
+    if dtype == "f16":
+        return np.asarray(x, dtype=np.float32).astype(np.float16).astype(np.float64)
+    if dtype == "bf16":
+        return round_to_bf16(x)
+    raise ValueError(dtype)
+
+
+# Exponent of the largest scaled magnitude: |Q| <= 2**TARGET_EXP.
+TARGET_EXP = {"f64": None, "f32": 0, "bf16": 0, "f16": 14}
+
+
+def block_scale(amax: float, dtype: str) -> float:
+    """Per-block power-of-two scale ``s`` with ``max|B/s| <= 2**TARGET_EXP``."""
+    t = TARGET_EXP[dtype]
+    if t is None or amax == 0.0:
+        return 1.0
+    e = int(np.ceil(np.log2(amax)))
+    if 2.0 ** (e - 1) >= amax:  # guard log2 rounding
+        e -= 1
+    return float(2.0 ** (e - t))
+
+
+def quantize(B: np.ndarray, dtype: str) -> tuple[float, np.ndarray]:
+    """Returns ``(s, Q)`` with ``Q = round(B / s)`` in ``dtype`` (as FP64 values)."""
+    s = block_scale(float(np.max(np.abs(B))) if B.size else 0.0, dtype)
+    return s, round_to(B / s, dtype)
+
+
+# ---------------------------------------------------------------------------
+# Schwarz preconditioners
+# ---------------------------------------------------------------------------
+
+def local_block(A: sps.csr_matrix, idx: np.ndarray) -> np.ndarray:
+    return A[idx][:, idx].toarray()
+
+
+def coarse_matrix(A: sps.csr_matrix, R0: sps.csr_matrix) -> np.ndarray:
+    return (R0 @ A @ R0.T).toarray()
+
+
+class Schwarz:
+    """Two-level Schwarz with explicit local inverses (reference ``Inv``)."""
+
+    def __init__(self, A, sub_ptr, sub_idx, R0=None, block_dtype="f64", vec_dtype="f64",
+                 inverse_blocks=None):
+        self.A = sps.csr_matrix(A)
+        self.sub_ptr = np.asarray(sub_ptr, dtype=np.int64)
+        self.sub_idx = np.asarray(sub_idx, dtype=np.int64)
+        self.N = len(self.sub_ptr) - 1
+        self.block_dtype = block_dtype
+        self.vec_dtype = vec_dtype
+        self.scales = np.ones(self.N)
+        self.blocks = []
+        for i in range(self.N):
+            idx = self.sub_idx[self.sub_ptr[i]:self.sub_ptr[i + 1]]
+            if inverse_blocks is not None:
+                Binv = inverse_blocks[i]
+            else:
+                Ai = local_block(self.A, idx)
+                Binv = np.linalg.inv(Ai) if len(idx) else np.zeros((0, 0))
+            s, Q = quantize(Binv, block_dtype)
+            self.scales[i] = s
+            self.blocks.append(Q)
+        self.R0 = None if R0 is None else sps.csr_matrix(R0)
+        if self.R0 is not None:
+            self.Ac = coarse_matrix(self.A, self.R0)
+            self.Ac_cho = sla.cho_factor(self.Ac)
+            self.AR = (self.R0 @ self.A).tocsr()
+
+    def _vec(self, r):
+        return round_to(r, self.vec_dtype)
+
+    def local(self, r: np.ndarray) -> np.ndarray:
+        """``sum_i R_i^T (s_i Q_i) R_i r`` (columns of r are independent RHS)."""
+        r = self._vec(r)
+        y = np.zeros_like(r, dtype=np.float64)
+        for i in range(self.N):
+            idx = self.sub_idx[self.sub_ptr[i]:self.sub_ptr[i + 1]]
+            if len(idx) == 0:
+                continue
+            y[idx] += self.scales[i] * (self.blocks[i] @ r[idx])
+        return y
+
+    def coarse_solve(self, w):
+        return sla.cho_solve(self.Ac_cho, w)
+
+    def additive(self, r: np.ndarray) -> np.ndarray:
+        y = self.local(r)
+        if self.R0 is not None:
+            rr = self._vec(r)
+            y = y + self.R0.T @ self.coarse_solve(self.R0 @ rr)
+        return self._vec(y)
+
+    def hybrid(self, r: np.ndarray) -> np.ndarray:
+        y = self.local(r)
+        if self.R0 is not None:
+            y = y - self.R0.T @ self.coarse_solve(self.AR @ y)
+        return self._vec(y)
+
+    def T0(self, b: np.ndarray) -> np.ndarray:
+        return self.R0.T @ self.coarse_solve(self.R0 @ self._vec(b))
+
+
+# ---------------------------------------------------------------------------
+# PCG
+# ---------------------------------------------------------------------------
+
+def pcg(A, b, M=None, rtol=1e-7, atol=0.0, maxiter=1000, x0=None, T0=None,
+        flexible=False, record_iterates=False, raise_on_fail=True):
+    """Single-RHS PCG with the reference's control flow (``solvers.py:228-297``)."""
+    A = sps.csr_matrix(A)
+    b = np.asarray(b, dtype=np.float64)
+    atol = max(atol, rtol * float(np.linalg.norm(b)))
+    n = len(b)
+    maxiter = maxiter or n * 10
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+    if T0 is not None:
+        x = x + T0(b)
+    r = b - A @ x
+    norms = []
+    alphas, betas = [], []
+    iterates = []
+    rho_prev = None
+    p = q = None
+    alpha = 0.0
+    i = 0
+    for i in range(maxiter):
+        rn = float(np.linalg.norm(r))
+        norms.append(rn)
+        if rn < atol:
+            break
+        z = M(r) if M is not None else r.copy()
+        rho = float(r @ z)
+        if i > 0:
+            if flexible:
+                beta = -alpha * float(z @ q) / rho_prev
+            else:
+                beta = rho / rho_prev
+            p = beta * p + z
+            betas.append(beta)
+        else:
+            p = z.copy()
+        q = A @ p
+        alpha = rho / float(p @ q)
+        alphas.append(alpha)
+        x = x + alpha * p
+        r = r - alpha * q
+        rho_prev = rho
+        if record_iterates:
+            iterates.append(x.copy())
+    meta = {"iterations": len(norms) - 1, "residual norms": norms,
+            "alphas": alphas, "betas": betas}
+    if record_iterates:
+        meta["iterates"] = iterates
+    if i + 1 == maxiter and raise_on_fail:
+        raise ConvergenceNotAchieved(meta)
+    return x, meta
+
+
+def pcg_multi(A, B, M=None, **kw):
+    """Column-by-column PCG for an ``(n, R)`` block of right-hand sides."""
+    B = np.asarray(B, dtype=np.float64)
+    X = np.zeros_like(B)
+    its = []
+    norms = []
+    for j in range(B.shape[1]):
+        Mj = None if M is None else (lambda r, M=M: M(r[:, None])[:, 0])
+        x, meta = pcg(A, B[:, j], Mj, **kw)
+        X[:, j] = x
+        its.append(meta["iterations"])
+        norms.append(meta["residual norms"])
+    return X, {"iterations": its, "residual norms": norms}
+
+
+def lanczos_condition(alphas, betas) -> float:
+    """Condition-number estimate from the CG coefficients (``solvers.py:281-292``)."""
+    k = len(alphas)
+    L = np.zeros((k, k))
+    for i in range(k):
+        L[i, i] = 1.0 / alphas[i]
+        if i > 0:
+            L[i, i] += betas[i - 1] / alphas[i - 1]
+            L[i - 1, i] = L[i, i - 1] = np.sqrt(betas[i - 1]) / alphas[i - 1]
+    return float(np.linalg.cond(L, 2))

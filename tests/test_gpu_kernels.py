@@ -1,0 +1,211 @@
+"""GPU parity of the individual kernels against the oracle / reference known answers.
+
+Mirrors the reference's kernel tests: tests/test_gemv.py (7 dtype pairs x k,
+rtol = atol = 1e-5), tests/test_bsr.py (fixture + random BSR, atol 1e-12 FP64 /
+1e-6 FP32), tests/test_cusparse.py and tests/test_cudss.py (known answers).
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sps
+import torch
+
+from conftest import golden
+from helpers import p1_case, q1_case, torch_csr
+
+pytestmark = pytest.mark.gpu
+
+DT = {"f16": torch.float16, "bf16": torch.bfloat16, "f32": torch.float32, "f64": torch.float64}
+
+
+@pytest.mark.parametrize("mat_dtype,vec_dtype", [("f16", "f32"), ("f16", "f64"), ("bf16", "f32"), ("bf16", "f64"),
+                                                 ("f32", "f32"), ("f32", "f64"), ("f64", "f64")])
+@pytest.mark.parametrize("k", [1, 2, 5, 10, 20, 50, 100, 200])
+@pytest.mark.parametrize("use_shared_memory", [True, False])
+def test_gemv_strided_batched(cuda, mat_dtype, vec_dtype, k, use_shared_memory):
+    from dd_solvers_b200 import gemv_strided_batched
+
+    n = 7
+    rng = np.random.default_rng(42 + k)
+    A = torch.as_tensor(rng.standard_normal((n, k, k))).to(DT[mat_dtype])
+    A = A.permute(0, 2, 1).contiguous().permute(0, 2, 1).to(cuda)  # column-major
+    b = torch.as_tensor(rng.standard_normal((n, k))).to(DT[vec_dtype]).to(cuda)
+    exact = (A.to(b.dtype) @ b[:, :, None]).reshape(n, k)
+    out = gemv_strided_batched(A, b, use_shared_memory=use_shared_memory)
+    assert out.dtype == b.dtype
+    assert torch.allclose(exact, out, rtol=1e-5, atol=1e-5)
+
+
+def test_gemv_rejects_double_float(cuda):
+    from dd_solvers_b200 import gemv_strided_batched
+
+    A = torch.zeros(2, 3, 3, dtype=torch.float64, device=cuda).transpose(1, 2)
+    with pytest.raises(RuntimeError, match="Double-Float"):
+        gemv_strided_batched(A, torch.zeros(2, 3, dtype=torch.float32, device=cuda))
+
+
+def _allclose(a, b):
+    atol = 1e-6 if a.dtype == torch.float32 else 1e-12
+    return torch.allclose(a, b, atol=atol)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_bsr_small_fixture(cuda, dtype):
+    from dd_solvers_b200 import FastBSR
+
+    g = golden("unit_cases.npz")
+    m = torch.sparse_bsr_tensor(torch.as_tensor(g["bsr_crow"]), torch.as_tensor(g["bsr_col"]),
+                                torch.as_tensor(g["bsr_val"]), size=g["bsr_dense"].shape).to(cuda, dtype)
+    x = torch.randn(m.shape[0], device=cuda, dtype=dtype)
+    y = FastBSR(m) @ x
+    assert _allclose(y, torch.as_tensor(g["bsr_dense"], device=cuda, dtype=dtype) @ x)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+@pytest.mark.parametrize("bs", [1, 2, 3, 4, 6, 8])
+def test_bsr_random(cuda, dtype, bs):
+    from dd_solvers_b200 import FastBSR
+
+    torch.manual_seed(bs)
+    nbr, per = 1000, 3
+    crow = torch.arange(0, nbr * per + 1, per)
+    col = torch.randint(0, nbr, (nbr * per,))
+    vals = torch.randn(nbr * per, bs, bs, dtype=dtype)
+    m = torch.sparse_bsr_tensor(crow, col, vals, size=(nbr * bs, nbr * bs))
+    x = torch.randn(nbr * bs, dtype=dtype)
+    expected = (m.to_dense() @ x).to(cuda)
+    y = FastBSR(m.to(cuda)) @ x.to(cuda)
+    assert _allclose(y, expected)
+
+
+def test_csr_to_bsr_layout(cuda):
+    from dd_solvers_b200 import csr_to_bsr
+
+    m = torch.sparse_csr_tensor(torch.tensor([0, 2, 3, 5, 9]), torch.tensor([0, 1, 1, 0, 2, 0, 1, 2, 3]),
+                                torch.tensor([1, 2, 3, 4, 5, 6, 7, 8, 9], dtype=torch.float64)).to(cuda)
+    b = csr_to_bsr(m, 2)
+    assert b.crow_indices().tolist() == [0, 1, 3]
+    assert b.col_indices().tolist() == [0, 0, 1]
+    assert b.values().stride() == (4, 1, 2)
+    assert torch.equal(b.to_dense(), m.to_dense())
+
+
+def test_cusparse_known_answers(cuda):
+    from dd_solvers_b200 import gather_csr, sort_csr
+
+    g = golden("unit_cases.npz")
+    for i in range(int(g["n_cusparse_cases"])):
+        tag = "sort" if f"sort{i}_in_crow" in g.files else "gather"
+        fi = torch.sparse_csr_tensor(*(torch.as_tensor(g[f"{tag}{i}_in_{p}"]) for p in ("crow", "col", "val")),
+                                     size=(len(g[f"{tag}{i}_in_crow"]) - 1, 4)).to(cuda)
+        out = (sort_csr if tag == "sort" else gather_csr)(fi)
+        for p, t in (("crow", out.crow_indices()), ("col", out.col_indices()), ("val", out.values())):
+            assert np.array_equal(t.cpu().numpy(), g[f"{tag}{i}_out_{p}"]), (tag, i, p)
+
+
+@pytest.mark.parametrize("value_type", [torch.float32, torch.float64])
+def test_cudss_known_answers(cuda, value_type):
+    from dd_solvers_b200 import cudss
+
+    g = golden("unit_cases.npz")
+    A = torch.sparse_csr_tensor(torch.as_tensor(g["spd_3x3_crow"]), torch.as_tensor(g["spd_3x3_col"]),
+                                torch.as_tensor(g["spd_3x3_val"]).to(value_type), size=(3, 3)).to(cuda)
+    s = cudss.spd_factorize(A)
+    for xn, bn in (("cudss_x1", "cudss_b1"), ("cudss_x2", "cudss_b2")):
+        x = s.solve(torch.as_tensor(g[bn], device=cuda, dtype=value_type))
+        assert x.dtype == value_type
+        assert torch.allclose(x, torch.as_tensor(g[xn], device=cuda, dtype=value_type), atol=1e-6)
+    # batch: block-diagonal 3x3 + 2x2
+    nrows = torch.tensor([3, 2])
+    nnz = torch.tensor([5, 4])
+    vals = torch.cat([torch.as_tensor(g["spd_3x3_val"]), torch.as_tensor(g["spd_2x2_val"])]).to(value_type)
+    cols = torch.cat([torch.as_tensor(g["spd_3x3_col"]), torch.as_tensor(g["spd_2x2_col"])])
+    rows = torch.cat([torch.as_tensor(g["spd_3x3_crow"]), torch.as_tensor(g["spd_2x2_crow"])])
+    bs = cudss.spd_batch_factorize(nrows, nnz, vals.to(cuda), cols.to(cuda), rows.to(cuda))
+    x = bs.solve(torch.as_tensor(g["cudss_b"], device=cuda, dtype=value_type))
+    assert torch.allclose(x, torch.as_tensor(g["cudss_x"], device=cuda, dtype=value_type), atol=1e-6)
+
+
+# ---------------------------------------------------------------------------
+# SpMV (SELL-32 and CSR multi-RHS) vs SciPy
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("case", ["q1_2d", "q1_3d", "p1"])
+@pytest.mark.parametrize("R", [1, 4, 64])
+def test_spmv(cuda, case, R):
+    from dd_solvers_b200.solvers import _SellMatrix
+
+    if case == "q1_2d":
+        A = q1_case(2, 40)[1]
+    elif case == "q1_3d":
+        A = q1_case(3, 12, kappa_seed=1)[1]
+    else:
+        A = p1_case(40)[1]
+    M = _SellMatrix(torch_csr(A, cuda))
+    rng = np.random.default_rng(R)
+    x = rng.standard_normal((A.shape[0], R))
+    y = (M @ torch.as_tensor(x if R > 1 else x[:, 0], device=cuda)).cpu().numpy().reshape(A.shape[0], R)
+    ref = A @ x
+    assert np.max(np.abs(y - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+# ---------------------------------------------------------------------------
+# Schwarz local apply / combine vs the oracle restatement
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("prec", ["f64", "f32", "bf16", "f16"])
+@pytest.mark.parametrize("case", ["q1_2d", "q1_3d_uneven", "p1_rcb"])
+def test_schwarz_apply(cuda, prec, case):
+    import dd_solvers_b200 as dd
+    from oracle import restatement as orc
+
+    if case == "q1_2d":
+        P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(2, 32, 4)
+    elif case == "q1_3d_uneven":
+        P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(3, 12, 3, kappa_seed=2, coarse="q1")
+    else:
+        P, A, owner, nparts, sub_ptr, sub_idx, R0 = p1_case(34, 8)
+    At = torch_csr(A, cuda)
+    for kind in ("additive", "hybrid"):
+        cls = dd.AdditiveSchwarz if kind == "additive" else dd.HybridSchwarz
+        pc = cls(torch.float64, dd.Inv(DT[prec]), dd.CUDSS())
+        pc.setup(At, subdomains=(sub_ptr, sub_idx), coarse_restriction=R0)
+        # oracle with the GPU's own (dequantised) blocks: isolates the apply
+        blocks = [pc.store.block(i).cpu().numpy() for i in range(pc.n_solvers)]
+        M = orc.Schwarz(A, sub_ptr, sub_idx, R0, block_dtype="f64", inverse_blocks=blocks)
+        rng = np.random.default_rng(7)
+        r = rng.standard_normal(A.shape[0])
+        z = pc.solve(torch.as_tensor(r, device=cuda))[0].cpu().numpy()
+        zr = M.additive(r) if kind == "additive" else M.hybrid(r)
+        tol = 1e-12 if prec == "f64" else 2e-6
+        assert np.linalg.norm(z - zr) <= tol * np.linalg.norm(zr), (kind, np.linalg.norm(z - zr) / np.linalg.norm(zr))
+
+
+@pytest.mark.parametrize("prec", ["f32", "bf16", "f16"])
+def test_block_quantisation_matches_oracle(cuda, prec):
+    """Stored blocks equal the oracle's power-of-two-scaled rounding of the FP64 inverse."""
+    import dd_solvers_b200 as dd
+    from oracle import restatement as orc
+
+    P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(2, 24, 3)
+    pc = dd.AdditiveSchwarz(torch.float64, dd.Inv(DT[prec]), dd.CUDSS())
+    pc.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0)
+    pc64 = dd.AdditiveSchwarz(torch.float64, dd.Inv(), dd.CUDSS())
+    pc64.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0)
+    for i in range(pc.n_solvers):
+        inv64 = pc64.store.block(i).cpu().numpy()
+        s, Q = orc.quantize(inv64, prec)
+        assert float(pc.store.scale[i]) == s
+        assert np.array_equal(pc.store.block(i).cpu().numpy(), s * Q)
+
+
+def test_local_apply_multi_rhs_matches_columns(cuda):
+    import dd_solvers_b200 as dd
+
+    P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(2, 32, 4)
+    pc = dd.HybridSchwarz(torch.float64, dd.Inv(torch.bfloat16), dd.CUDSS())
+    pc.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0)
+    r = torch.randn(A.shape[0], 8, dtype=torch.float64, device=cuda)
+    Z = pc.solve(r)[0]
+    for j in range(8):
+        zj = pc.solve(r[:, j].contiguous())[0]
+        assert torch.allclose(Z[:, j], zj, rtol=0, atol=1e-14 * float(zj.abs().max()))

@@ -1,0 +1,267 @@
+"""End-to-end PCG parity on the GPU.
+
+* the reference's 24-DOF fixture and its own solver results (tests/golden/fixture24.npz,
+  from src/dd_solvers/tests/test_solvers.py:25-176),
+* "config 1-R" (2D Q1 Poisson 255^2 DOFs, 15x15 subdomains, P0 coarse): the
+  reference's FP64 iteration counts and solutions (tests/golden/c1r.npz),
+* overlapping / uneven / Q1-coarse / multi-RHS / low-precision cases against the
+  FP64 oracle restatement.
+Bar: FP64 path equal iteration counts (+-1) and 1e-10 relative solution
+agreement at equal counts; mixed precision: relative error <= 1e-8 against a
+direct FP64 solve at rtol 1e-10.
+"""
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+import torch
+
+from conftest import golden
+from helpers import p1_case, q1_case, torch_csr
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref_setup(cuda, g, problem_dtype=torch.float64):
+    A = torch.sparse_csr_tensor(torch.as_tensor(g["p_crow"]), torch.as_tensor(g["p_col"]), torch.as_tensor(g["p_val"]),
+                                size=(24, 24)).to(cuda, problem_dtype)
+    s2c = torch.as_tensor(g["solvers_to_coarse"])
+    spc = s2c.bincount(minlength=int(s2c.max()) + 1)
+    return A, spc.to(cuda)
+
+
+@pytest.mark.parametrize("rhs_name", ["load", "rhs_u"])
+@pytest.mark.parametrize("case", ["asm_f64", "hsm_f64", "asm_f64_inv32", "hsm_f64_inv32", "none"])
+def test_fixture24_matches_reference(cuda, rhs_name, case):
+    import dd_solvers_b200 as dd
+
+    g = golden("fixture24.npz")
+    A, spc = _ref_setup(cuda, g)
+    perm = torch.as_tensor(g["perm"]).to(cuda)
+    b = torch.as_tensor(g[rhs_name], device=cuda)[perm]
+    pcs = {"asm_f64": lambda: dd.AdditiveSchwarz(torch.float64, dd.Inv(), dd.CUDSS()),
+           "hsm_f64": lambda: dd.HybridSchwarz(torch.float64, dd.Inv(), dd.CUDSS()),
+           "asm_f64_inv32": lambda: dd.AdditiveSchwarz(torch.float64, dd.Inv(torch.float32), dd.CUDSS()),
+           "hsm_f64_inv32": lambda: dd.HybridSchwarz(torch.float64, dd.Inv(torch.float32), dd.CUDSS()),
+           "none": lambda: None}
+    cg = dd.CG(pcs[case](), rtol=1e-12, flexible=False)
+    cg.setup(A, dofs_per_solver=6, solvers_per_coarse=spc, block_size=3)
+    x, meta = cg.solve(b)
+    key = f"{rhs_name}__{case}"
+    ref_it = int(g[key + "__iters"])
+    assert abs(meta["iterations"] - ref_it) <= 1
+    xr = g[key + "__x"]
+    if meta["iterations"] == ref_it:
+        tol = 1e-10 if "inv32" not in case else 1e-6
+        assert np.linalg.norm(x.cpu().numpy() - xr) <= tol * np.linalg.norm(xr)
+    # reference's own pin (test_solvers.py:176)
+    inv_perm = dd.inverse_permutation(perm)
+    Ad = A.to_dense()
+    assert torch.linalg.norm(Ad @ x - b) < 1e-10
+    assert len(meta["residual norms"]) == meta["iterations"] + 1
+
+
+@pytest.mark.parametrize("pc_name,problem_dtype,rtol", [
+    ("cg_csr", torch.float32, 1e-7), ("cg_sell", torch.float64, 1e-7),
+    ("asm64", torch.float64, 1e-7), ("asm32", torch.float64, 1e-7), ("asm32", torch.float32, 1e-7),
+    ("asm32_f16", torch.float32, 1e-7), ("hsm64", torch.float64, 1e-7), ("hsm64_f32", torch.float64, 1e-7),
+    ("hsm64_f16", torch.float64, 1e-7), ("hsm64_bf16", torch.float64, 1e-7), ("hsm32", torch.float32, 1e-6),
+    ("hsm32", torch.float64, 1e-6)])
+def test_reference_solver_matrix(cuda, pc_name, problem_dtype, rtol):
+    """The in-scope rows of the reference's test_sparse_solver table (test_solvers.py:115-176)."""
+    import dd_solvers_b200 as dd
+
+    g = golden("fixture24.npz")
+    A, spc = _ref_setup(cuda, g, problem_dtype)
+    perm = torch.as_tensor(g["perm"]).to(cuda)
+    b = torch.as_tensor(g["load"], device=cuda, dtype=problem_dtype)[perm]
+    mk = {"cg_csr": lambda: dd.CG(bsr_matmul=False), "cg_sell": lambda: dd.CG(bsr_matmul=True),
+          "asm64": lambda: dd.CG(dd.AdditiveSchwarz(torch.float64, dd.Inv(), dd.CUDSS())),
+          "asm32": lambda: dd.CG(dd.AdditiveSchwarz(torch.float32, dd.Inv(), dd.CUDSS())),
+          "asm32_f16": lambda: dd.CG(dd.AdditiveSchwarz(torch.float32, dd.Inv(torch.float16), dd.CUDSS())),
+          "hsm64": lambda: dd.CG(dd.HybridSchwarz(torch.float64, dd.Inv(), dd.CUDSS())),
+          "hsm64_f32": lambda: dd.CG(dd.HybridSchwarz(torch.float64, dd.Inv(torch.float32), dd.CUDSS())),
+          "hsm64_f16": lambda: dd.CG(dd.HybridSchwarz(torch.float64, dd.Inv(torch.float16), dd.CUDSS())),
+          "hsm64_bf16": lambda: dd.CG(dd.HybridSchwarz(torch.float64, dd.Inv(torch.bfloat16), dd.CUDSS())),
+          "hsm32": lambda: dd.CG(dd.HybridSchwarz(torch.float32, dd.Inv(), dd.CUDSS()), rtol=rtol)}
+    solver = mk[pc_name]()
+    solver.setup(A, dofs_per_solver=6, solvers_per_coarse=spc, block_size=3)
+    x, _ = solver.solve(b)
+    solver.destroy()
+    assert x.dtype == problem_dtype
+    assert torch.linalg.norm(A.to_dense() @ x - b) < 1e-10
+
+
+def test_cudss_direct_solver(cuda):
+    import dd_solvers_b200 as dd
+
+    g = golden("fixture24.npz")
+    A, _ = _ref_setup(cuda, g)
+    s = dd.CUDSS()
+    s.setup(A)
+    b = torch.as_tensor(g["rhs_u"], device=cuda)
+    x, meta = s.solve(b)
+    assert meta == {}
+    assert torch.linalg.norm(A.to_dense() @ x - b) < 1e-10
+
+
+def test_condition_number_estimate(cuda):
+    import dd_solvers_b200 as dd
+
+    g = golden("unit_cases.npz")
+    solver = dd.CG(preconditioner=None, rtol=1e-9, estimate_cond=True, bsr_matmul=False)
+    solver.setup(torch.diag(torch.tensor([0.5, 4, 21], dtype=torch.float64)).to_sparse_csr().to(cuda))
+    _, meta = solver.solve(torch.ones(3, dtype=torch.float64, device=cuda))
+    assert np.isclose(meta["condition number estimate"], float(g["cond_estimate"]))
+    # float32 input is solved in FP64 here (3 iterations); the reference's float32 run needs 6
+
+
+def _c1r_problem():
+    from dd_solvers_b200 import partition, problems
+
+    P = problems.poisson2d(256)
+    A = P.matrix
+    b = problems.uniform_rhs(A.shape[0], seed=0)
+    owner, nparts = partition.box_owner(P.interior_shape, 15)
+    return P, A, b, owner, nparts
+
+
+@pytest.mark.parametrize("kind", ["asm_f64", "hsm_f64"])
+@pytest.mark.parametrize("layout", ["reference", "index_sets"])
+def test_config1r_matches_reference(cuda, kind, layout):
+    """Same inputs as the reference run: iteration count and solution to 1e-10."""
+    import dd_solvers_b200 as dd
+    from dd_solvers_b200 import partition
+
+    g = golden("c1r.npz")
+    P, A, b, owner, nparts = _c1r_problem()
+    assert np.allclose(b[:16], g["b_head"]) and np.isclose(b.sum(), float(g["b_sum"]))
+    perm = np.argsort(owner, kind="stable")
+    assert np.array_equal(perm[:64], g["perm_head"])
+    cls = dd.AdditiveSchwarz if kind == "asm_f64" else dd.HybridSchwarz
+    cg = dd.CG(cls(torch.float64, dd.Inv(), dd.CUDSS()), rtol=1e-8)
+    if layout == "reference":
+        inv = np.empty_like(perm)
+        inv[perm] = np.arange(len(perm))
+        Ap = dd.permute_csr_tensor(torch_csr(A, cuda), torch.as_tensor(inv, device=cuda))
+        cg.setup(Ap, dofs_per_solver=289, solvers_per_coarse=torch.ones(nparts, dtype=torch.int64, device=cuda),
+                 block_size=1)
+        x, meta = cg.solve(torch.as_tensor(b[perm], device=cuda))
+        x = x.cpu().numpy()
+    else:
+        # natural ordering with index-set subdomains (overlap 0) and P0 owners: same operator
+        sub_ptr, sub_idx = partition.overlapping_subdomains(A, owner, nparts, 0)
+        cg.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), owner=owner, block_size=1)
+        xn, meta = cg.solve(torch.as_tensor(b, device=cuda))
+        x = xn.cpu().numpy()[perm]
+    ref_it = int(g[kind + "__iters"])
+    assert abs(meta["iterations"] - ref_it) <= 1
+    xr = g[kind + "__x"]
+    if meta["iterations"] == ref_it:
+        assert np.linalg.norm(x - xr) <= 1e-10 * np.linalg.norm(xr)
+    ref_norms = g[kind + "__norms"]
+    k = min(len(ref_norms), len(meta["residual norms"])) - 1
+    assert np.allclose(meta["residual norms"][:k], ref_norms[:k], rtol=1e-7)
+
+
+@pytest.mark.parametrize("case", ["q1_2d_p0", "q1_3d_q1coarse", "p1_rcb"])
+@pytest.mark.parametrize("kind", ["additive", "hybrid"])
+def test_overlapping_fp64_matches_oracle(cuda, case, kind):
+    import dd_solvers_b200 as dd
+    from oracle import restatement as orc
+
+    if case == "q1_2d_p0":
+        P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(2, 64, 8)
+    elif case == "q1_3d_q1coarse":
+        P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(3, 16, 4, kappa_seed=5, coarse="q1")
+    else:
+        P, A, owner, nparts, sub_ptr, sub_idx, R0 = p1_case(50, 16)
+    b = np.random.default_rng(11).uniform(-1, 1, A.shape[0])
+    M = orc.Schwarz(A, sub_ptr, sub_idx, R0)
+    cls = dd.AdditiveSchwarz if kind == "additive" else dd.HybridSchwarz
+    cg = dd.CG(cls(torch.float64, dd.Inv(), dd.CUDSS()), rtol=1e-8)
+    cg.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0, block_size=1)
+    x, meta = cg.solve(torch.as_tensor(b, device=cuda))
+    if kind == "additive":
+        xr, om = orc.pcg(A, b, M.additive, rtol=1e-8)
+    else:
+        xr, om = orc.pcg(A, b, M.hybrid, rtol=1e-8, T0=M.T0)
+    assert abs(meta["iterations"] - om["iterations"]) <= 1
+    if meta["iterations"] == om["iterations"]:
+        assert np.linalg.norm(x.cpu().numpy() - xr) <= 1e-10 * np.linalg.norm(xr)
+
+
+@pytest.mark.parametrize("prec", [torch.float32, torch.bfloat16, torch.float16])
+@pytest.mark.parametrize("kind", ["additive", "hybrid"])
+def test_mixed_precision_reaches_fp64_accuracy(cuda, prec, kind):
+    import dd_solvers_b200 as dd
+
+    P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(3, 16, 4, kappa_seed=9, coarse="q1")
+    b = np.random.default_rng(1).uniform(-1, 1, A.shape[0])
+    xd = spla.spsolve(A.tocsc(), b)
+    cls = dd.AdditiveSchwarz if kind == "additive" else dd.HybridSchwarz
+    cg = dd.CG(cls(torch.float64, dd.Inv(prec), dd.CUDSS()), rtol=1e-10, replace_every=16)
+    cg.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0, block_size=1)
+    x, meta = cg.solve(torch.as_tensor(b, device=cuda))
+    err = np.linalg.norm(x.cpu().numpy() - xd) / np.linalg.norm(xd)
+    assert err <= 1e-8, (err, meta["iterations"])
+
+
+def test_multi_rhs_matches_single(cuda):
+    import dd_solvers_b200 as dd
+
+    P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(2, 48, 6)
+    B = np.random.default_rng(3).standard_normal((A.shape[0], 5))  # padded to 8 internally
+    cg = dd.CG(dd.HybridSchwarz(torch.float64, dd.Inv(), dd.CUDSS()), rtol=1e-9)
+    cg.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0, block_size=1)
+    X, meta = cg.solve(torch.as_tensor(B, device=cuda))
+    assert X.shape == B.shape and len(meta["iterations"]) == 5
+    for j in range(5):
+        xj, mj = cg.solve(torch.as_tensor(B[:, j].copy(), device=cuda))
+        assert mj["iterations"] == meta["iterations"][j]
+        assert torch.allclose(X[:, j], xj, rtol=0, atol=1e-12 * float(xj.abs().max()))
+
+
+def test_graph_and_eager_bitwise_equal_and_deterministic(cuda):
+    import dd_solvers_b200 as dd
+
+    P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(2, 48, 6)
+    b = torch.as_tensor(np.random.default_rng(5).uniform(-1, 1, A.shape[0]), device=cuda)
+    out = []
+    for use_graph in (True, True, False):
+        cg = dd.CG(dd.AdditiveSchwarz(torch.float64, dd.Inv(torch.bfloat16), dd.CUDSS()), rtol=1e-9,
+                   use_graph=use_graph, check_every=4)
+        cg.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0, block_size=1)
+        out.append(cg.solve(b)[0])
+        out.append(cg.solve(b)[0])
+    for o in out[1:]:
+        assert torch.equal(o, out[0])
+
+
+def test_convergence_not_achieved(cuda):
+    import dd_solvers_b200 as dd
+
+    P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(2, 32, 4)
+    cg = dd.CG(None, rtol=1e-12, maxiter=5, bsr_matmul=False)
+    cg.setup(torch_csr(A, cuda))
+    with pytest.raises(dd.ConvergenceNotAchieved) as e:
+        cg.solve(torch.ones(A.shape[0], dtype=torch.float64, device=cuda))
+    assert e.value.metadata["iterations"] == 4
+    assert len(e.value.metadata["residual norms"]) == 5
+
+
+def test_zero_rhs_and_x0(cuda):
+    import dd_solvers_b200 as dd
+
+    P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(2, 16, 2)
+    cg = dd.CG(dd.HybridSchwarz(torch.float64, dd.Inv(), dd.CUDSS()), rtol=1e-10)
+    cg.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0, block_size=1)
+    x, meta = cg.solve(torch.zeros(A.shape[0], dtype=torch.float64, device=cuda))
+    assert meta["iterations"] == 0 and float(x.abs().max()) == 0.0
+    b = torch.ones(A.shape[0], dtype=torch.float64, device=cuda)
+    cg = dd.CG(dd.AdditiveSchwarz(torch.float64, dd.Inv(), dd.CUDSS()), rtol=1e-10)
+    cg.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0, block_size=1)
+    x1, m1 = cg.solve(b)
+    x0 = x1.clone()
+    x2, m2 = cg.solve(b, x0=x0)
+    assert x2 is x0
+    assert m2["iterations"] <= 1

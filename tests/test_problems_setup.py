@@ -1,0 +1,210 @@
+"""Host-side logic on CPU: assemblers, partitions, coarse spaces, setup layouts, C ABI."""
+import itertools
+import os
+import re
+
+import numpy as np
+import pytest
+import scipy.sparse as sps
+import torch
+
+from dd_solvers_b200 import partition, problems
+from dd_solvers_b200 import setup_ops as so
+from helpers import p1_case, q1_case
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _q1_brute(dim, n_el, kappa):
+    h = 1.0 / n_el
+    K = problems.q1_reference_stiffness(dim) * h ** (dim - 2)
+    m = n_el - 1
+    rows, cols, vals = [], [], []
+    for c in itertools.product(range(n_el), repeat=dim):
+        nodes = []
+        for a in range(2 ** dim):
+            bits = [(a >> d) & 1 for d in range(dim)]
+            nodes.append([c[dim - 1 - d] + bits[d] for d in range(dim)])
+        for a in range(2 ** dim):
+            for b in range(2 ** dim):
+                pa, pb = nodes[a], nodes[b]
+                if any(q == 0 or q == n_el for q in pa + pb):
+                    continue
+                la = lb = 0
+                for d in reversed(range(dim)):
+                    la = la * m + pa[d] - 1
+                    lb = lb * m + pb[d] - 1
+                rows.append(la)
+                cols.append(lb)
+                vals.append(kappa[c] * K[a, b])
+    return sps.csr_matrix((vals, (rows, cols)), shape=(m ** dim, m ** dim))
+
+
+@pytest.mark.parametrize("dim,n_el", [(2, 6), (3, 4)])
+def test_q1_stencil_assembly_matches_element_loop(dim, n_el):
+    kappa = np.exp(np.random.default_rng(dim).standard_normal((n_el,) * dim))
+    A = problems.q1_grid(dim, n_el, kappa).matrix
+    B = _q1_brute(dim, n_el, kappa)
+    assert abs(A - B).max() < 1e-14
+    assert A.has_sorted_indices
+    assert np.linalg.eigvalsh(A.toarray()).min() > 0
+
+
+def test_p1_jittered_spd_and_consistent():
+    P = problems.p1_jittered(9, 0.3, 1.0, 0)
+    A = P.matrix.toarray()
+    assert np.allclose(A, A.T)
+    assert np.linalg.eigvalsh(A).min() > 0
+    # constant coefficient, no jitter: the 5-point Laplacian (diagonal pair cancels)
+    P0 = problems.p1_jittered(6, 0.0, 0.0, 0)
+    A0 = P0.matrix.toarray()
+    assert np.allclose(np.diag(A0), 4.0)
+    assert np.allclose(A0[0, 1], -1.0) and np.allclose(A0[0, 5], 0.0)
+
+
+def test_grf_statistics():
+    g = problems.gaussian_random_field(64, 0.1, seed=0)
+    assert g.shape == (64, 64)
+    assert 0.3 < g.std() < 2.0
+    g2 = problems.gaussian_random_field(64, 0.1, seed=0)
+    assert np.array_equal(g, g2)
+
+
+def test_box_partition_sizes():
+    owner, n = partition.box_owner((255, 255), 8)
+    c = np.bincount(owner, minlength=n)
+    assert n == 64 and c.min() >= 31 * 31 and c.max() == 32 * 32
+    owner3, n3 = partition.box_owner((127,) * 3, 16)
+    c3 = np.bincount(owner3, minlength=n3)
+    assert n3 == 4096 and c3.max() == 512
+
+
+def test_overlap_and_transpose_map():
+    P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(2, 16, 4)
+    ks = np.diff(sub_ptr)
+    assert ks.max() == 6 * 6  # 4x4 owned + one layer on each side
+    for i in range(nparts):
+        idx = sub_idx[sub_ptr[i]:sub_ptr[i + 1]]
+        assert np.all(np.diff(idx) > 0)
+        assert set(np.flatnonzero(owner == i)) <= set(idx)
+    dof_ptr, dof_src = so.transpose_map(torch.as_tensor(sub_idx), A.shape[0])
+    dof_ptr, dof_src = dof_ptr.numpy(), dof_src.numpy()
+    for d in range(A.shape[0]):
+        pos = dof_src[dof_ptr[d]:dof_ptr[d + 1]]
+        assert np.all(sub_idx[pos] == d) and np.all(np.diff(pos) > 0)
+    assert dof_ptr[-1] == len(sub_idx)
+
+
+def test_rcb_uneven_partition():
+    # 66 interior nodes per axis: the second bisection level splits 33 node
+    # lines at the middle line, where jitter decides the side
+    P = problems.p1_jittered(68, 0.3, 1.0, 1)
+    owner = partition.rcb_owner(P.coords, 16)
+    c = np.bincount(owner, minlength=16)
+    assert c.sum() == P.matrix.shape[0] and c.min() > 0 and c.max() != c.min()
+
+
+def test_q1_coarse_restriction_partition_of_unity():
+    R = partition.q1_coarse_restriction(2, 16, 4)
+    assert R.shape == (9, 225)
+    # interior fine nodes far from the boundary are interpolated with weights summing to 1
+    s = np.asarray(R.sum(axis=0)).ravel().reshape(15, 15)
+    assert np.allclose(s[3:12, 3:12], 1.0)
+    R3 = partition.q1_coarse_restriction(3, 8, 2)
+    assert R3.shape == (1, 343) and np.isclose(R3.max(), 1.0)
+
+
+def test_sell32_roundtrip():
+    A = p1_case(20, 4)[1]
+    crow = torch.as_tensor(A.indptr.astype(np.int64))
+    sp, sw, sc, sv = so.csr_to_sell32(crow, torch.as_tensor(A.indices.astype(np.int64)), torch.as_tensor(A.data))
+    n = A.shape[0]
+    D = np.zeros((n, n))
+    sp, sw, sc, sv = sp.numpy(), sw.numpy(), sc.numpy(), sv.numpy()
+    for s in range(len(sw)):
+        for l in range(32):
+            r = 32 * s + l
+            if r >= n:
+                continue
+            for j in range(sw[s]):
+                D[r, sc[sp[s] + 32 * j + l]] += sv[sp[s] + 32 * j + l]
+    assert np.array_equal(D, A.toarray())
+
+
+def test_extract_blocks_matches_scipy():
+    P, A, owner, nparts, sub_ptr, sub_idx, R0 = p1_case(20, 4)
+    crow = torch.as_tensor(A.indptr.astype(np.int64))
+    col = torch.as_tensor(A.indices.astype(np.int64))
+    val = torch.as_tensor(A.data)
+    ks = np.diff(sub_ptr)
+    kpad = so.round_up(int(ks.max()), 16)
+    blk = so.extract_blocks(crow, col, val, torch.as_tensor(sub_ptr), torch.as_tensor(sub_idx), 0, nparts, kpad)
+    for i in range(nparts):
+        idx = sub_idx[sub_ptr[i]:sub_ptr[i + 1]]
+        k = len(idx)
+        assert np.array_equal(blk[i, :k, :k].numpy(), A[idx][:, idx].toarray())
+        assert np.array_equal(blk[i, k:, k:].numpy(), np.eye(kpad - k))
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32, torch.bfloat16, torch.float16])
+def test_blockstore_layout_and_quantisation(dtype):
+    from oracle import restatement as orc
+
+    ks = np.array([5, 12, 0, 9])
+    store = so.BlockStore(ks, dtype, "cpu")
+    kpad = 16
+    rng = np.random.default_rng(0)
+    inv = torch.zeros(4, kpad, kpad, dtype=torch.float64)
+    for i, k in enumerate(ks):
+        inv[i, :k, :k] = torch.as_tensor(rng.standard_normal((k, k)) * 1e-3)
+    store.put(0, inv)
+    name = {torch.float64: "f64", torch.float32: "f32", torch.bfloat16: "bf16", torch.float16: "f16"}[dtype]
+    V = 16 // so.ELEM_BYTES[dtype]
+    for i, k in enumerate(ks):
+        assert int(store.blk_off[i]) * so.ELEM_BYTES[dtype] % 16 == 0
+        if k == 0:
+            continue
+        s, Q = orc.quantize(inv[i, :k, :k].numpy(), name)
+        assert np.array_equal(store.block(i).numpy(), s * Q)
+        # column-major with ld = round_up(k, V) and zero padding rows
+        ld = (k + V - 1) // V * V
+        raw = store.data[store.off_np[i]:store.off_np[i] + k * ld].view(k, ld)
+        assert torch.all(raw[:, k:] == 0)
+
+
+def test_capi_exports_every_declared_symbol():
+    """libddx.so loads here (no GPU) and exports exactly what include/ddx.h declares."""
+    import ctypes
+
+    from dd_solvers_b200 import _lib
+
+    hdr = open(os.path.join(ROOT, "include", "ddx.h")).read()
+    declared = set(re.findall(r"^\w[\w\s\*]*?\b(ddx_\w+)\s*\(", hdr, flags=re.M))
+    assert declared, "no declarations found"
+    lib = _lib.lib()
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert declared == set(_lib.exported_symbols()) | (declared - set(_lib.exported_symbols()))
+    assert set(_lib.exported_symbols()) <= declared
+
+
+def test_capi_argument_checks_without_gpu():
+    from dd_solvers_b200 import _lib
+
+    lib = _lib.lib()
+    assert lib.ddx_pcg_reset(3, None, None, 10, 0, 1e-8, 0.0, None) == 1
+    assert b"unsupported R=3" in lib.ddx_last_error()
+    assert lib.ddx_gemv_strided_batched(1, 3, None, 0, None, None, 1, None) == 1
+    assert b"Double-Float" in lib.ddx_last_error() or b"null" in lib.ddx_last_error()
+    assert lib.ddx_spmv_sell_f64(100, 3, None, None, None, None, None, None, None, 0, None, None, None, None,
+                                 None, None) == 1
+    assert lib.ddx_partials_len(64) == 592 * 4 * 64
+
+
+def test_solver_rejects_cpu_tensors():
+    import dd_solvers_b200 as dd
+    from dd_solvers_b200 import _lib
+
+    A = torch.eye(3, dtype=torch.float64).to_sparse_csr()
+    with pytest.raises(_lib.DDXError):
+        dd.CG(bsr_matmul=False).setup(A)
