@@ -1,0 +1,502 @@
+"""Benchmark: time per right-hand side to 1e-8 relative error, mixed precision vs FP64.
+
+Workload (default): 3D Q1 diffusion on 128^3 hexahedra (127^3 = 2,048,383 DOFs),
+kappa = exp(g), g i.i.d. N(0,1) per element (seed 0); 16^3 = 4096 box subdomains
+with one layer of overlap; Q1 coarse space on the subdomain vertices (15^3 =
+3375 coarse DOFs); Hybrid Schwarz with local inverse blocks stored in BF16
+(per-block power-of-two scale, FP32 accumulation); FP64 flexible PCG. One
+step = one PCG solve of one right-hand side (uniform[-1,1], seeded). The
+relative error of every timed solution against the FP64 reference solution
+(the FP64 plain path at rtol 1e-12) is checked to be <= 1e-8; the stopping
+tolerance is tightened until it is.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n-el 128] [--parts 16]
+
+--impl reference times the FP64 CPU restatement of the same algorithm on the
+host cores (the reference's own solver runs on GPUs only; its CPU behaviour is
+what the restatement reproduces) on a bounded sample of the workload.
+
+With --gpus N > 1 (torchrun), every rank solves its own right-hand sides on its
+own replica of the problem (the path needs no exchange between GPUs: weak
+scaling, no collective in the solve); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]), "source": "measured"}
+    return dict(PEAKS_FALLBACK, source="fallback")
+
+
+def build_problem(n_el: int, parts: int, seed: int = 0):
+    from dd_solvers_b200 import partition, problems
+
+    t0 = time.time()
+    P = problems.diffusion3d_lognormal(n_el, seed)
+    A = P.matrix
+    owner, nparts = partition.box_owner(P.interior_shape, parts)
+    sub_ptr, sub_idx = partition.overlapping_subdomains(A, owner, nparts, 1)
+    R0 = partition.q1_coarse_restriction(3, n_el, parts)
+    return dict(P=P, A=A, owner=owner, nparts=nparts, sub_ptr=sub_ptr, sub_idx=sub_idx, R0=R0,
+                host_setup_s=time.time() - t0)
+
+
+def rhs_for(n: int, rank: int, step: int):
+    from dd_solvers_b200 import problems
+
+    return problems.uniform_rhs(n, seed=1000 * rank + step)
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region (clocks and throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(smax)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: FP64 restatement, bounded sample
+# ---------------------------------------------------------------------------
+
+def cpu_time_per_rhs(prob, iterations: int, sample_subdomains: int = 48, budget_s: float = 25.0):
+    """Estimated CPU time of one FP64 Hybrid-Schwarz PCG solve (ms per RHS).
+
+    Sample: one PCG iteration of the oracle restatement, timed in full for the
+    SpMV, the coarse restriction / solve / prolongation and the vector updates,
+    and for ``sample_subdomains`` of the local inverse applies (dense FP64 GEMV
+    with NumPy's threaded BLAS), scaled to all subdomains; times the iteration
+    count the FP64 GPU solve needed.
+    """
+    import scipy.linalg as sla
+
+    from oracle import restatement as orc
+
+    A, R0 = prob["A"], prob["R0"]
+    sub_ptr, sub_idx = prob["sub_ptr"], prob["sub_idx"]
+    n = A.shape[0]
+    N = len(sub_ptr) - 1
+    rng = np.random.default_rng(0)
+    r = rng.standard_normal(n)
+    t_start = time.time()
+    # local inverse applies on a sample of subdomains (inverses built untimed)
+    pick = np.linspace(0, N - 1, min(sample_subdomains, N)).astype(int)
+    invs = []
+    for i in pick:
+        idx = sub_idx[sub_ptr[i]:sub_ptr[i + 1]]
+        invs.append((idx, np.linalg.inv(orc.local_block(A, idx))))
+        if time.time() - t_start > budget_s:
+            break
+    y = np.zeros(n)
+    t0 = time.perf_counter()
+    for idx, Binv in invs:
+        y[idx] += Binv @ r[idx]
+    t_local = (time.perf_counter() - t0) * (N / len(invs))
+    # coarse space (setup untimed)
+    AR = (R0 @ A).tocsr()
+    Ac = (AR @ R0.T).toarray()
+    cf = sla.cho_factor(Ac)
+    t0 = time.perf_counter()
+    w = AR @ y
+    yc = sla.cho_solve(cf, w)
+    z = y - R0.T @ yc
+    t_coarse = time.perf_counter() - t0
+    # SpMV + PCG vector work
+    p = rng.standard_normal(n)
+    x = np.zeros(n)
+    t0 = time.perf_counter()
+    q = A @ p
+    rho = r @ z
+    pq = p @ q
+    alpha = rho / pq
+    p = z + 0.5 * p
+    x += alpha * p
+    r -= alpha * q
+    _ = np.linalg.norm(r)
+    t_rest = time.perf_counter() - t0
+    per_iter = t_local + t_coarse + t_rest
+    return {
+        "ms_per_rhs": per_iter * iterations * 1e3,
+        "per_iteration_ms": per_iter * 1e3,
+        "sample": (f"one FP64 hybrid-Schwarz PCG iteration of the oracle restatement on the full problem "
+                   f"(SpMV, coarse, vector updates timed in full; local inverse GEMVs timed on {len(invs)} of "
+                   f"{N} subdomains and scaled) x {iterations} iterations"),
+        "cores": os.cpu_count(),
+    }
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args, rank: int, world: int):
+    import torch
+    import torch.distributed as dist
+
+    import dd_solvers_b200 as dd
+    from dd_solvers_b200 import _lib as L
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    prob = build_problem(args.n_el, args.parts)
+    A = prob["A"]
+    n = A.shape[0]
+    At = dd.csr_to_torch(A).to(dev)
+
+    t0 = time.time()
+    pc64 = dd.HybridSchwarz(torch.float64, dd.Inv(), dd.CUDSS())
+    pc64.setup(At, subdomains=(prob["sub_ptr"], prob["sub_idx"]), coarse_restriction=prob["R0"])
+    pcs = {"f64": pc64}
+    for name, dt in (("bf16", torch.bfloat16), ("f32", torch.float32), ("f16", torch.float16)):
+        pcs[name] = pc64.requantize(dt)
+    torch.cuda.synchronize()
+    gpu_setup_s = time.time() - t0
+
+    # one CG front-end per precision sharing the SELL matrix of the first
+    base = dd.CG(pcs["f64"], rtol=1e-12, maxiter=2000, check_every=args.check_every)
+    base.preconditioner = None
+    base.setup(At, block_size=1)
+    mat = base.matrix
+
+    def make(prec, rtol):
+        cg = dd.CG(pcs[prec], rtol=rtol, maxiter=2000, check_every=args.check_every,
+                   flexible=(prec != "f64"), replace_every=(args.replace_every if prec != "f64" else 0))
+        cg.matrix = mat
+        cg.n = n
+        cg.block_size = 1
+        return cg
+
+    b0 = torch.as_tensor(rhs_for(n, rank, 0), device=dev)
+    xref, mref = make("f64", 1e-12).solve(b0)
+    nref = float(torch.linalg.norm(xref))
+
+    def rel_err(x):
+        return float(torch.linalg.norm(x - xref)) / nref
+
+    # calibrate the stopping tolerance of each precision to reach 1e-8 error
+    cal = {}
+    for prec in ("f64", "bf16", "f32", "f16"):
+        rtol = 1e-8
+        for _ in range(6):
+            cg = make(prec, rtol)
+            x, meta = cg.solve(b0)
+            e = rel_err(x)
+            if e <= 1e-8:
+                break
+            rtol /= 4
+        cal[prec] = {"rtol": rtol, "rel_error": e, "iterations": meta["iterations"], "solver": cg}
+
+    head = args.precision
+    steps, warm = args.steps, args.warmup
+
+    def timed(prec, k, w, host=False):
+        cg = cal[prec]["solver"]
+        bs = [torch.as_tensor(rhs_for(n, rank, s + 1), device=dev) for s in range(min(k, 4))]
+        if host:
+            bh = [b.cpu().pin_memory() for b in bs]
+            xh = torch.empty(n, dtype=torch.float64).pin_memory()
+            bd = torch.empty(n, dtype=torch.float64, device=dev)
+        for s in range(w):
+            cg.solve(bs[s % len(bs)])
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        its = []
+        ev0.record()
+        for s in range(k):
+            if host:
+                bd.copy_(bh[s % len(bh)], non_blocking=True)
+                x, meta = cg.solve(bd)
+                xh.copy_(x, non_blocking=True)
+            else:
+                x, meta = cg.solve(bs[s % len(bs)])
+            its.append(meta["iterations"])
+        ev1.record()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms = ev0.elapsed_time(ev1) / k
+        if world > 1:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t)
+        return ms, its
+
+    clocks = Clocks(dev.index if dev.index is not None else 0)
+    L.CALLS[0] = 0
+    clocks.start()
+    ms_head, its_head = timed(head, steps, warm)
+    clk = clocks.stop()
+    launches = L.CALLS[0]
+    # every timed solution meets the error bar
+    errs = {}
+    for prec in ("f64", "bf16", "f32", "f16"):
+        bt = torch.as_tensor(rhs_for(n, rank, 1), device=dev)
+        xr, _ = make("f64", 1e-12).solve(bt)
+        x, _ = cal[prec]["solver"].solve(bt)
+        errs[prec] = float(torch.linalg.norm(x - xr) / torch.linalg.norm(xr))
+    per_prec = {}
+    for prec in ("f64", "f32", "f16"):
+        ms, its = timed(prec, max(1, min(steps, 3)), 1)
+        per_prec[prec] = {"ms_per_rhs": ms, "iterations": its[-1], "rtol": cal[prec]["rtol"],
+                          "rel_error": errs[prec]}
+    per_prec[head] = {"ms_per_rhs": ms_head, "iterations": its_head[-1], "rtol": cal[head]["rtol"],
+                      "rel_error": errs[head]}
+    ms_e2e, _ = timed(head, steps, 1, host=True)
+
+    # dominant kernel: local inverse apply of the head precision, timed alone
+    pc = pcs[head]
+    r = torch.randn(n, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        pc._local(r, 1)
+    kev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    reps = 10
+    torch.cuda.synchronize()
+    kev[0].record()
+    for _ in range(reps):
+        pc._local(r, 1)
+    kev[1].record()
+    torch.cuda.synchronize()
+    k_ms = kev[0].elapsed_time(kev[1]) / reps
+    ks = pc.ks.astype(np.int64)
+    elt = {"f64": 8, "f32": 4, "bf16": 2, "f16": 2}[head]
+    alg_bytes = int((ks * ks).sum() * elt + 4 * len(ks) + ks.sum() * 4 + n * 8 + ks.sum() * 4)
+    # SpMV (FP64 SELL) timed alone too
+    q = torch.empty_like(r)
+    for _ in range(3):
+        mat.launch(r, q, 1, L.SPMV_PLAIN)
+    torch.cuda.synchronize()
+    kev[0].record()
+    for _ in range(reps):
+        mat.launch(r, q, 1, L.SPMV_PLAIN)
+    kev[1].record()
+    torch.cuda.synchronize()
+    s_ms = kev[0].elapsed_time(kev[1]) / reps
+    spmv_bytes = mat.nnz * 12 + (n + 1) * 4 + n * 16
+
+    # batched right-hand sides through the tensor-core local apply
+    batched = None
+    if args.batched:
+        Rb = args.batched
+        cgb = make(head, cal[head]["rtol"])
+        Bh = np.stack([rhs_for(n, rank, 100 + j) for j in range(Rb)], axis=1)
+        Bd = torch.as_tensor(Bh, device=dev)
+        Xb, mb = cgb.solve(Bd)  # warm-up (builds tile store, captures graphs)
+        ebs = []
+        for j in (0, Rb - 1):
+            xr, _ = make("f64", 1e-12).solve(Bd[:, j].contiguous())
+            ebs.append(float(torch.linalg.norm(Xb[:, j] - xr) / torch.linalg.norm(xr)))
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        kb = max(1, min(steps, 3))
+        e0.record()
+        for _ in range(kb):
+            Xb, mb = cgb.solve(Bd)
+        e1.record()
+        torch.cuda.synchronize()
+        bms = e0.elapsed_time(e1) / kb
+        if world > 1:
+            t = torch.tensor([bms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            bms = float(t)
+        # tensor-core kernel alone
+        rb = torch.randn(n * Rb, dtype=torch.float64, device=dev)
+        pcb = pcs[head]
+        for _ in range(2):
+            pcb._local(rb, Rb)
+        torch.cuda.synchronize()
+        kev[0].record()
+        for _ in range(reps):
+            pcb._local(rb, Rb)
+        kev[1].record()
+        torch.cuda.synchronize()
+        tc_ms = kev[0].elapsed_time(kev[1]) / reps
+        tiles = pcb._tile_store()
+        tc_bytes = int((ks * ks).sum() * elt + 4 * len(ks) + ks.sum() * 4 + n * Rb * 8 + ks.sum() * Rb * 4)
+        tc_flops = float(2 * (ks * ks).sum() * Rb)
+        batched = {"rhs": Rb, "ms_per_solve": bms, "ms_per_rhs": bms / Rb, "iterations": max(mb["iterations"]),
+                   "rel_error_vs_fp64_checked_columns": ebs,
+                   "speedup_vs_fp64_plain_per_rhs": None,
+                   "tc_kernel": {"name": "ddx_schwarz_local_apply_tc", "ms_per_launch": tc_ms,
+                                 "algorithmic_bytes": tc_bytes, "tile_bytes": tiles.nbytes,
+                                 "achieved_gbs": tc_bytes / (tc_ms * 1e-3) / 1e9,
+                                 "achieved_tflops": tc_flops / (tc_ms * 1e-3) / 1e12}}
+
+    peaks = load_peaks()
+    out = None
+    if rank == 0:
+        ach = alg_bytes / (k_ms * 1e-3) / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tp):
+            tj = json.load(open(tp))
+            t = tj.get(f"local_apply_{head}")
+            if t and t.get("n_el") == args.n_el and t.get("parts") == args.parts:
+                traffic = t["bytes_per_launch"]
+        f64_ms = per_prec["f64"]["ms_per_rhs"]
+        if batched is not None:
+            batched["speedup_vs_fp64_plain_per_rhs"] = f64_ms / batched["ms_per_rhs"]
+        out = {
+            "metric": "time per RHS to 1e-8 rel. error (mixed-precision Hybrid-Schwarz PCG), 1 B200",
+            "value": ms_head / world,
+            "unit": "ms/RHS",
+            "n_gpus": world,
+            "steps": steps,
+            "warmup": warm,
+            "ms_per_step": ms_head,
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": f"{head} blocks / f32 accumulate / f64 PCG",
+            "data": "synthetic (seeded lognormal coefficient and uniform RHS)",
+            "config": {
+                "workload": f"hybrid-schwarz q1-3d {args.n_el}^3 cells, {prob['nparts']} subdomains overlap 1, "
+                            f"q1 coarse {prob['R0'].shape[0]}, {head} blocks",
+                "n_dofs": n, "subdomains": prob["nparts"], "k_max": int(ks.max()), "k_min": int(ks.min()),
+                "coarse_dofs": prob["R0"].shape[0], "rhs_per_step": 1, "rtol_used": cal[head]["rtol"],
+                "l2": "inputs larger than L2 (local inverse blocks %.1f GB per apply)" % (alg_bytes / 1e9),
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            },
+            "rel_error_vs_fp64": errs[head],
+            "iterations": its_head[-1],
+            "fp64_plain_ms_per_rhs": f64_ms,
+            "speedup_vs_fp64_plain": f64_ms / ms_head,
+            "per_precision": per_prec,
+            "e2e": {"value": ms_e2e / world, "unit": "ms/RHS", "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8},
+            "roofline": {"kernel": f"ddx_schwarz_local_apply ({head})", "bound": "hbm", "achieved": ach,
+                         "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": ach / peaks["hbm_gbs"],
+                         "traffic": traffic, "algorithmic_bytes": alg_bytes, "ms_per_launch": k_ms,
+                         "peak_source": peaks["source"]},
+            "spmv_roofline": {"kernel": "ddx_spmv_sell_f64", "achieved": spmv_bytes / (s_ms * 1e-3) / 1e9,
+                              "frac": spmv_bytes / (s_ms * 1e-3) / 1e9 / peaks["hbm_gbs"], "ms_per_launch": s_ms,
+                              "algorithmic_bytes": spmv_bytes},
+            "gpu_launches": launches,
+            "batched": batched,
+            "clocks": clk,
+            "setup_s": {"host": prob["host_setup_s"], "gpu": gpu_setup_s},
+        }
+    return out, prob, cal
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n-el", type=int, default=128)
+    ap.add_argument("--parts", type=int, default=16)
+    ap.add_argument("--precision", default="bf16", choices=["bf16", "f32", "f16"])
+    ap.add_argument("--check-every", type=int, default=8)
+    ap.add_argument("--replace-every", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batched", type=int, default=64, help="also time R right-hand sides per solve (0: skip)")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        prob = build_problem(args.n_el, args.parts)
+        # iteration count of the FP64 method on this workload (measured on B200 by the GPU arm)
+        iters = int(os.environ.get("DDX_FP64_ITERATIONS", "0")) or 40
+        vals = []
+        for _ in range(max(1, args.steps)):
+            vals.append(cpu_time_per_rhs(prob, iters))
+        v = min(x["ms_per_rhs"] for x in vals)
+        line = {"metric": "time per RHS to 1e-8 rel. error (mixed-precision Hybrid-Schwarz PCG), 1 B200",
+                "value": v, "unit": "ms/RHS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": False, "impl": "reference", "dtype": "f64",
+                "config": {"workload": f"hybrid-schwarz q1-3d {args.n_el}^3 cells, {prob['nparts']} subdomains "
+                                       f"overlap 1, q1 coarse {prob['R0'].shape[0]}, FP64 CPU restatement"},
+                "cpu_baseline": {"value": v, "unit": "ms/RHS", "cores": vals[0]["cores"], "kind": "port",
+                                 "sample": vals[0]["sample"]},
+                "e2e": {"value": v, "unit": "ms/RHS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    out, prob, cal = run_ours(args, rank, world)
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            cb = cpu_time_per_rhs(prob, cal["f64"]["iterations"])
+            out["cpu_baseline"] = {"value": cb["ms_per_rhs"], "unit": "ms/RHS", "cores": cb["cores"], "kind": "port",
+                                   "sample": cb["sample"]}
+        print(json.dumps(out))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -45,6 +45,7 @@ _SIGS = {
     "ddx_spmv_bsr": (_I, [_I64, _I, _P, _P, _P, _P, _P, _I, _P]),
     "ddx_gemv_strided_batched": (_I, [_I64, _I, _P, _I, _P, _P, _I, _P]),
     "ddx_schwarz_local_apply": (_I, [_I, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _P]),
+    "ddx_schwarz_local_apply_tc": (_I, [_I, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _P, _P, _P]),
     "ddx_schwarz_combine": (_I, [_I64, _I, _P, _P, _P, _I, _P, _P, _P, _P, _P, _D, _P, _I, _P, _P, _P, _P,
                                  _P, _P, _P]),
     "ddx_coarse_gemv_f64": (_I, [_I, _I, _P, _P, _P, _P, _P]),
@@ -79,7 +80,13 @@ def exported_symbols() -> list[str]:
     return list(_SIGS)
 
 
+# Number of library calls issued (each launches one kernel; the local apply
+# launches one per right-hand side). CUDA-graph replays add their captured count.
+CALLS = [0]
+
+
 def call(name: str, *args) -> None:
+    CALLS[0] += 1
     status = getattr(lib(), name)(*args)
     if status != 0:
         msg = lib().ddx_last_error().decode()

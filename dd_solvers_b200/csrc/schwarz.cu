@@ -115,6 +115,14 @@ __device__ __forceinline__ void fma_vec<float, float>(const void* p, float xv, f
   acc[3] = fmaf(v.w, xv, acc[3]);
 }
 template <>
+__device__ __forceinline__ void fma_vec<float, double>(const void* p, double xv, double* acc) {
+  const float4 v = *reinterpret_cast<const float4*>(p);
+  acc[0] = fma((double)v.x, xv, acc[0]);
+  acc[1] = fma((double)v.y, xv, acc[1]);
+  acc[2] = fma((double)v.z, xv, acc[2]);
+  acc[3] = fma((double)v.w, xv, acc[3]);
+}
+template <>
 __device__ __forceinline__ void fma_vec<__nv_bfloat16, float>(const void* p, float xv, float* acc) {
   const uint4 u = *reinterpret_cast<const uint4*>(p);
   const uint32_t w[4] = {u.x, u.y, u.z, u.w};
@@ -422,7 +430,10 @@ int ddx_schwarz_local_apply(int n_sub, int R, const int64_t* sub_ptr, const int*
       DDX_REQUIRE(acc_dtype == DDX_F64, "ddx_schwarz_local_apply: F64 blocks accumulate in F64");
       return launch_apply_typed<double, double>(a, s);
     case DDX_F32:
-      DDX_REQUIRE(acc_dtype == DDX_F32, "ddx_schwarz_local_apply: F32 blocks accumulate in F32");
+      // FP64 accumulation matches the reference's rule for FP32 blocks with
+      // FP64 vectors (accumulate in the vector type)
+      if (acc_dtype == DDX_F64) return launch_apply_typed<float, double>(a, s);
+      DDX_REQUIRE(acc_dtype == DDX_F32, "ddx_schwarz_local_apply: F32 blocks accumulate in F32 or F64");
       return launch_apply_typed<float, float>(a, s);
     case DDX_BF16:
       DDX_REQUIRE(acc_dtype == DDX_F32, "ddx_schwarz_local_apply: BF16 blocks accumulate in F32");

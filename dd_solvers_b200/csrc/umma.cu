@@ -1,0 +1,400 @@
+// Multi-RHS Schwarz local apply on the 5th-generation tensor cores (tcgen05).
+//
+// For many right-hand sides the local solve of subdomain i is a dense product
+// Y_i (k x R) = Q_i (k x k) * X_i (k x R), X_i = r[idx_i, :], i.e. a GEMM with
+// N = R, which the SIMT streaming kernel cannot feed at HBM speed. Layout per
+// persistent CTA (one per SM):
+//   warp 0      producer: streams 128x64 BF16/FP16 tiles of Q_i, stored in HBM
+//               already in the K-major 128-byte-swizzled UMMA layout, with one
+//               contiguous cp.async.bulk per tile into a 4-stage ring.
+//   warp 1      allocates TMEM; one lane issues tcgen05.mma (M=128, N=R, K=16)
+//               and tcgen05.commit to release ring stages / publish results.
+//   warps 2..5  gather X_i = r[idx_i, :] (FP64 -> 16-bit) into a resident
+//               K-major swizzled B buffer, then drain each 128-row accumulator
+//               from TMEM (tcgen05.ld), scale, and store ylocal (FP32).
+// Two TMEM accumulators (2 x R columns) let the epilogue of row tile m overlap
+// the MMAs of row tile m+1. Every wait is bounded (device error word).
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace ddx {
+namespace umma {
+
+constexpr int kM = 128;
+constexpr int kK = 64;              // 16-bit elements per 128-byte swizzle row
+constexpr int kStages = 4;
+constexpr int kTileBytes = kM * 128; // 16 KB
+constexpr int kThreads = 192;
+constexpr int kEpiThreads = 128;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ uint64_t gtimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait (2 s); false on timeout (recorded in the device error word).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t addr = smem_u32(bar);
+  uint64_t t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if ((it & 1023u) == 0) {
+      const uint64_t t = gtimer();
+      if (t0 == 0) t0 = t;
+      else if (t - t0 > 2000000000ull) {
+        atomicOr(&g_device_error, DEVERR_MBAR_TIMEOUT);
+        return false;
+      }
+    }
+  }
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 2, %0;" ::"n"(kEpiThreads) : "memory"); }
+
+// K-major, 128-byte swizzle shared-memory matrix descriptor (sm_100 format):
+// start address >> 4 in bits 0-13, leading byte offset (unused for swizzled
+// K-major, 16 B) in 16-29, stride byte offset 1024 B (8 rows x 128 B) in 32-45,
+// descriptor version 1 in 46-47, layout type 2 (128B swizzle) in 61-63.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1u << 16) | ((uint64_t)(1024u >> 4) << 32) |
+         ((uint64_t)1u << 46) | ((uint64_t)2u << 61);
+}
+
+// Instruction descriptor, kind::f16: D F32 (bits 4-5 = 1), A/B format in bits
+// 7-9 / 10-12 (F16 = 0, BF16 = 1), both K-major, N >> 3 in bits 17-22,
+// M >> 4 in bits 24-28.
+__host__ __device__ constexpr uint32_t idesc_f16(int ab_fmt, int N) {
+  return (1u << 4) | ((uint32_t)ab_fmt << 7) | ((uint32_t)ab_fmt << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(kM >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+// 32 lanes x 16 consecutive columns of FP32 from TMEM; the wait is tied to the
+// destination registers so no use can be scheduled before it.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t u0, u1, u2, u3, u4, u5, u6, u7, u8, u9, u10, u11, u12, u13, u14, u15;
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(u0), "=r"(u1), "=r"(u2), "=r"(u3), "=r"(u4), "=r"(u5), "=r"(u6), "=r"(u7), "=r"(u8), "=r"(u9),
+        "=r"(u10), "=r"(u11), "=r"(u12), "=r"(u13), "=r"(u14), "=r"(u15)
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(u0), "+r"(u1), "+r"(u2), "+r"(u3), "+r"(u4), "+r"(u5), "+r"(u6), "+r"(u7), "+r"(u8),
+                 "+r"(u9), "+r"(u10), "+r"(u11), "+r"(u12), "+r"(u13), "+r"(u14), "+r"(u15)
+               :
+               : "memory");
+  v[0] = __uint_as_float(u0); v[1] = __uint_as_float(u1); v[2] = __uint_as_float(u2); v[3] = __uint_as_float(u3);
+  v[4] = __uint_as_float(u4); v[5] = __uint_as_float(u5); v[6] = __uint_as_float(u6); v[7] = __uint_as_float(u7);
+  v[8] = __uint_as_float(u8); v[9] = __uint_as_float(u9); v[10] = __uint_as_float(u10);
+  v[11] = __uint_as_float(u11); v[12] = __uint_as_float(u12); v[13] = __uint_as_float(u13);
+  v[14] = __uint_as_float(u14); v[15] = __uint_as_float(u15);
+}
+
+template <typename T> __device__ __forceinline__ uint16_t to_bits(double v);
+template <> __device__ __forceinline__ uint16_t to_bits<__nv_bfloat16>(double v) {
+  return __bfloat16_as_ushort(__float2bfloat16_rn((float)v));
+}
+template <> __device__ __forceinline__ uint16_t to_bits<__half>(double v) {
+  return __half_as_ushort(__float2half_rn((float)v));
+}
+
+struct Args {
+  int n_sub;
+  const int64_t* sub_ptr;
+  const int* sub_idx;
+  const int* order;
+  const int64_t* tile_off;  // bytes
+  const unsigned char* tiles;
+  const float* scale;
+  const double* r;
+  float* ylocal;
+  const int* ist;
+  const double* st;  // PCG state (||r_j||^2 scales the 16-bit conversion); may be null
+  int kmax;
+};
+
+// Power-of-two scale that maps RHS j of r into [-1, 1] before the 16-bit
+// conversion (FP16 would flush small residual entries to zero otherwise),
+// from the PCG's current ||r_j||^2; 1 without PCG state.
+__device__ __forceinline__ float rhs_scale(const double* st, int R, int j) {
+  if (st == nullptr) return 1.0f;
+  const double rr = st[DDX_ST_RR * R + j];
+  if (!(rr > 0.0) || !(rr < 1e300)) return 1.0f;
+  int e;
+  frexp(sqrt(rr), &e);  // sqrt(rr) in [2^(e-1), 2^e)
+  e = max(-100, min(100, e));
+  return ldexpf(1.0f, -e);
+}
+
+template <typename T, int N>
+__global__ void __launch_bounds__(kThreads, 1) k_apply_tc(Args a) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1024-byte alignment for the swizzled tiles
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* ring = smem;                                  // kStages x 16 KB
+  unsigned char* bbuf = smem + kStages * kTileBytes;           // nK x (N x 128 B)
+  const int nk_max = (a.kmax + kK - 1) / kK;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(bbuf + (size_t)nk_max * N * 128);
+  uint64_t* a_full = bars;
+  uint64_t* a_empty = bars + kStages;
+  uint64_t* b_full = bars + 2 * kStages;
+  uint64_t* b_empty = b_full + 1;
+  uint64_t* acc_full = b_full + 2;   // [2]
+  uint64_t* acc_empty = b_full + 4;  // [2]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(b_full + 6);
+  __shared__ int abort_flag_s;
+  volatile int& abort_flag = abort_flag_s;
+  __shared__ float rhs_unscale[64];  // 1 / (per-RHS conversion scale)
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (a.ist != nullptr && n_active(a.ist, N) == 0) return;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&a_full[s], 1);
+      mbar_init(&a_empty[s], 1);
+    }
+    mbar_init(b_full, 1);
+    mbar_init(b_empty, 1);
+    for (int s = 0; s < 2; ++s) {
+      mbar_init(&acc_full[s], 1);
+      mbar_init(&acc_empty[s], kEpiThreads / 32);
+    }
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (threadIdx.x < N) rhs_unscale[threadIdx.x] = 1.0f / rhs_scale(a.st, N, threadIdx.x);
+  constexpr uint32_t kCols = (2 * N < 32) ? 32 : 2 * N;  // power of two >= 32
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------ producer ------------------------------
+    if (lane == 0) {
+      uint32_t g = 0;
+      for (int w = blockIdx.x; w < a.n_sub && !abort_flag; w += gridDim.x) {
+        const int i = a.order[w];
+        const int k = (int)(a.sub_ptr[i + 1] - a.sub_ptr[i]);
+        if (k == 0 || k > a.kmax) continue;
+        const int nK = (k + kK - 1) / kK;
+        const unsigned char* src = a.tiles + a.tile_off[i];
+        for (int m0 = 0; m0 < k; m0 += kM) {
+          const int rows = (min(kM, k - m0) + 7) / 8 * 8;
+          const uint32_t bytes = (uint32_t)rows * 128u;
+          for (int t = 0; t < nK; ++t, ++g) {
+            const int s = g % kStages;
+            if (!mbar_wait(&a_empty[s], ((g / kStages) & 1u) ^ 1u)) { abort_flag = 1; break; }
+            mbar_expect_tx(&a_full[s], bytes);
+            bulk_g2s(ring + (size_t)s * kTileBytes, src, bytes, &a_full[s]);
+            src += bytes;
+          }
+          if (abort_flag) break;
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------ MMA issuer -----------------------------
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_f16(std::is_same<T, __nv_bfloat16>::value ? 1 : 0, N);
+      uint32_t g = 0, acc_n = 0, sub_n = 0;
+      for (int w = blockIdx.x; w < a.n_sub && !abort_flag; w += gridDim.x) {
+        const int i = a.order[w];
+        const int k = (int)(a.sub_ptr[i + 1] - a.sub_ptr[i]);
+        if (k == 0 || k > a.kmax) continue;
+        const int nK = (k + kK - 1) / kK;
+        if (!mbar_wait(b_full, sub_n & 1u)) { abort_flag = 1; break; }
+        fence_after();
+        for (int m0 = 0; m0 < k; m0 += kM, ++acc_n) {
+          const uint32_t ab = acc_n & 1u;
+          if (!mbar_wait(&acc_empty[ab], ((acc_n >> 1) & 1u) ^ 1u)) { abort_flag = 1; break; }
+          fence_after();
+          const uint32_t d = tmem + ab * N;
+          for (int t = 0; t < nK; ++t, ++g) {
+            const int s = g % kStages;
+            if (!mbar_wait(&a_full[s], (g / kStages) & 1u)) { abort_flag = 1; break; }
+            fence_after();
+            const uint32_t sa = smem_u32(ring + (size_t)s * kTileBytes);
+            const uint32_t sb = smem_u32(bbuf + (size_t)t * N * 128);
+#pragma unroll
+            for (int kk = 0; kk < kK / 16; ++kk)
+              mma_f16(d, sw128_desc(sa + kk * 32), sw128_desc(sb + kk * 32), idesc, (t > 0 || kk > 0) ? 1u : 0u);
+            mma_commit(&a_empty[s]);
+          }
+          if (abort_flag) break;
+          mma_commit(&acc_full[ab]);
+        }
+        if (abort_flag) break;
+        mma_commit(b_empty);
+        ++sub_n;
+      }
+    }
+  } else {
+    // ------------------------- gather + epilogue --------------------------
+    const int e = threadIdx.x - 64;   // 0..127
+    const int quarter = warp & 3;     // TMEM lane quarter this warp may access
+    uint32_t acc_n = 0, sub_n = 0;
+    for (int w = blockIdx.x; w < a.n_sub && !abort_flag; w += gridDim.x) {
+      const int i = a.order[w];
+      const int64_t p0 = a.sub_ptr[i];
+      const int k = (int)(a.sub_ptr[i + 1] - p0);
+      if (k == 0) continue;
+      if (k > a.kmax) {
+        if (e == 0) atomicOr(&g_device_error, DEVERR_BAD_SIZE);
+        continue;
+      }
+      const int nK = (k + kK - 1) / kK;
+      // B buffer free once the MMAs of the previous subdomain completed
+      if (!mbar_wait(b_empty, (sub_n & 1u) ^ 1u)) { abort_flag = 1; break; }
+      // gather: unit = (K tile t, 16-byte chunk c8, rhs j); j fastest
+      const int units = nK * 8 * N;
+      const double rsc = (double)rhs_scale(a.st, N, e % N);  // this thread's RHS: j = e % N
+      for (int u = e; u < units; u += kEpiThreads) {
+        const int j = u % N;
+        const int rest = u / N;
+        const int c8 = rest & 7;
+        const int t = rest >> 3;
+        uint32_t packed[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          uint32_t lo = 0, hi = 0;
+          const int c0 = t * kK + c8 * 8 + 2 * q;
+          if (c0 < k) lo = to_bits<T>(rsc * a.r[(int64_t)a.sub_idx[p0 + c0] * N + j]);
+          if (c0 + 1 < k) hi = to_bits<T>(rsc * a.r[(int64_t)a.sub_idx[p0 + c0 + 1] * N + j]);
+          packed[q] = lo | (hi << 16);
+        }
+        unsigned char* row = bbuf + (size_t)t * N * 128 + (size_t)j * 128;
+        *reinterpret_cast<uint4*>(row + ((c8 ^ (j & 7)) * 16)) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      epi_sync();
+      if (e == 0) mbar_arrive(b_full);
+      ++sub_n;
+      // epilogue per 128-row tile
+      const float sc = a.scale ? a.scale[i] : 1.0f;
+      for (int m0 = 0; m0 < k; m0 += kM, ++acc_n) {
+        const uint32_t ab = acc_n & 1u;
+        if (!mbar_wait(&acc_full[ab], (acc_n >> 1) & 1u)) { abort_flag = 1; break; }
+        fence_after();
+        float v[N];
+#pragma unroll
+        for (int c = 0; c < N; c += 16) tmem_ld16(tmem + ab * N + c + ((uint32_t)(quarter * 32) << 16), v + c);
+        fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[ab]);
+        const int row = m0 + quarter * 32 + lane;
+        if (row < k) {
+          float4* dst = reinterpret_cast<float4*>(a.ylocal + (p0 + row) * N);
+#pragma unroll
+          for (int c = 0; c < N; c += 4)
+            dst[c / 4] = make_float4(sc * rhs_unscale[c] * v[c], sc * rhs_unscale[c + 1] * v[c + 1],
+                                     sc * rhs_unscale[c + 2] * v[c + 2], sc * rhs_unscale[c + 3] * v[c + 3]);
+        }
+      }
+    }
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+  }
+}
+
+template <typename T, int N>
+static int launch(const Args& a, cudaStream_t s) {
+  const int nk_max = (a.kmax + kK - 1) / kK;
+  const size_t smem = 1024 + (size_t)kStages * kTileBytes + (size_t)nk_max * N * 128 + 16 * 8 + 64;
+  if (smem > 227 * 1024) {
+    set_error("ddx_schwarz_local_apply_tc: k=%d with R=%d needs %zu bytes of shared memory", a.kmax, N, smem);
+    return DDX_ERR_UNSUPPORTED;
+  }
+  auto kern = k_apply_tc<T, N>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::max(1, std::min(a.n_sub, nsm));
+  kern<<<grid, kThreads, smem, s>>>(a);
+  DDX_LAUNCH_CHECK("ddx_schwarz_local_apply_tc");
+  return DDX_OK;
+}
+
+}  // namespace umma
+}  // namespace ddx
+
+using namespace ddx;
+
+extern "C" int ddx_schwarz_local_apply_tc(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
+                                          const int* order, const int64_t* tile_off, const void* tiles,
+                                          int block_dtype, const float* scale, int kmax, const double* r,
+                                          float* ylocal, const int* ist, const double* st,
+                                          ddx_stream_t stream) {
+  DDX_REQUIRE(R == 16 || R == 32 || R == 64, "ddx_schwarz_local_apply_tc: R must be 16, 32 or 64 (got %d)", R);
+  DDX_REQUIRE(n_sub >= 0 && kmax >= 0, "ddx_schwarz_local_apply_tc: bad sizes");
+  if (n_sub == 0 || kmax == 0) return DDX_OK;
+  DDX_REQUIRE(sub_ptr && sub_idx && order && tile_off && tiles && r && ylocal,
+              "ddx_schwarz_local_apply_tc: null pointer");
+  DDX_REQUIRE(((uintptr_t)tiles & 15u) == 0 && ((uintptr_t)ylocal & 15u) == 0,
+              "ddx_schwarz_local_apply_tc: tiles and ylocal must be 16-byte aligned");
+  umma::Args a{n_sub, sub_ptr, sub_idx, order, tile_off, (const unsigned char*)tiles, scale, r, ylocal, ist, st, kmax};
+  cudaStream_t s = (cudaStream_t)stream;
+  if (block_dtype == DDX_BF16) {
+    if (R == 16) return umma::launch<__nv_bfloat16, 16>(a, s);
+    if (R == 32) return umma::launch<__nv_bfloat16, 32>(a, s);
+    return umma::launch<__nv_bfloat16, 64>(a, s);
+  }
+  if (block_dtype == DDX_F16) {
+    if (R == 16) return umma::launch<__half, 16>(a, s);
+    if (R == 32) return umma::launch<__half, 32>(a, s);
+    return umma::launch<__half, 64>(a, s);
+  }
+  set_error("ddx_schwarz_local_apply_tc: block dtype must be BF16 or F16");
+  return DDX_ERR_ARG;
+}

@@ -185,6 +185,82 @@ class BlockStore:
         return d.transpose(0, 1).to(torch.float64) * float(self.scale[i])
 
 
+UMMA_M = 128  # rows per tensor-core tile
+UMMA_K = 64   # 16-bit columns per tile (one 128-byte swizzle row)
+
+
+def umma_tile_rows(k: int) -> list[int]:
+    """Rows stored for each 128-row tile of a k x k block (multiples of 8)."""
+    rows = []
+    for m0 in range(0, k, UMMA_M):
+        r = min(UMMA_M, k - m0)
+        rows.append((r + 7) // 8 * 8)
+    return rows
+
+
+def swizzle128_index(device) -> torch.Tensor:
+    """Position of element (r, c) of a (128, 64) 16-bit tile in the K-major
+    128-byte-swizzled layout: row r at byte 128 r, 16-byte chunk c // 8 stored
+    at chunk (c // 8) ^ (r % 8)."""
+    r = torch.arange(UMMA_M, device=device)[:, None]
+    c = torch.arange(UMMA_K, device=device)[None, :]
+    return (r * UMMA_K + (((c // 8) ^ (r % 8)) * 8) + (c % 8)).reshape(-1)
+
+
+class UmmaTileStore:
+    """16-bit inverse blocks pre-arranged as tensor-core A tiles.
+
+    Subdomain ``i`` (size ``k``) is cut into ``ceil(k/128)`` row tiles by
+    ``ceil(k/64)`` column tiles, stored row-tile-major at byte offset
+    ``tile_off[i]``. Tile ``(m, t)`` holds ``rows_m`` rows (``umma_tile_rows``)
+    of 64 columns in the K-major 128-byte-swizzled shared-memory layout, so one
+    contiguous bulk copy lands it ready for ``tcgen05.mma``. Columns ``>= k``
+    and padding rows are zero. Built from a column-major ``BlockStore`` of the
+    same type, so both hold identical values.
+    """
+
+    def __init__(self, src: "BlockStore"):
+        assert src.dtype in (torch.bfloat16, torch.float16)
+        dev = src.data.device
+        self.dtype = src.dtype
+        ks = src.ks
+        sizes = []
+        for k in ks:
+            k = int(k)
+            nK = (k + UMMA_K - 1) // UMMA_K
+            sizes.append(sum(umma_tile_rows(k)) * nK * UMMA_K)
+        off = np.zeros(len(ks) + 1, dtype=np.int64)
+        np.cumsum(np.asarray(sizes, dtype=np.int64), out=off[1:])
+        self.off_np = off
+        self.data = torch.zeros(max(int(off[-1]), 8), dtype=src.dtype, device=dev)
+        self.tile_off = torch.as_tensor(off[:-1] * 2, device=dev)  # bytes
+        self.scale = src.scale
+        sw = swizzle128_index(dev)
+        for i, k in enumerate(ks):
+            k = int(k)
+            if k == 0:
+                continue
+            nK = (k + UMMA_K - 1) // UMMA_K
+            rows = umma_tile_rows(k)
+            ld = int(src.lds[i])
+            colmaj = src.data[src.off_np[i]:src.off_np[i] + k * ld].view(k, ld)[:, :k]  # [col, row]
+            full = torch.zeros(len(rows) * UMMA_M, nK * UMMA_K, dtype=src.dtype, device=dev)
+            full[:k, :k] = colmaj.transpose(0, 1)  # [row, col]
+            tiles = full.view(len(rows), UMMA_M, nK, UMMA_K).permute(0, 2, 1, 3).reshape(len(rows), nK, -1)
+            sw_tiles = torch.empty_like(tiles)
+            sw_tiles[:, :, sw] = tiles
+            o = int(off[i])
+            for m, rm in enumerate(rows):
+                n_el = rm * UMMA_K
+                seg = sw_tiles[m, :, :n_el].reshape(-1)
+                self.data[o:o + seg.numel()] = seg
+                o += seg.numel()
+
+    @property
+    def nbytes(self) -> int:
+        return int(self.off_np[-1]) * 2
+
+
 def invert_blocks(blocks: torch.Tensor, ks: torch.Tensor) -> torch.Tensor:
     """Inverse of each padded SPD block; padding rows/cols zeroed afterwards."""
     inv = torch.linalg.inv(blocks)

@@ -265,6 +265,8 @@ class SchwarzOperator(SparseSolver):
         self.coarse_solver = coarse_solver
         self.collect_timings = collect_timings
         self._scratch = {}
+        self._tiles = None
+        self.use_tensor_cores = True
 
     # -- setup -------------------------------------------------------------
     def setup(self, matrix: torch.Tensor, dofs_per_solver: int | None = None,
@@ -339,7 +341,7 @@ class SchwarzOperator(SparseSolver):
         if not isinstance(self.local_solver, Inv):
             raise NotImplementedError("only Inv local solvers are implemented on this path")
         self.block_dtype = block_dtype
-        self.acc_dtype = torch.float64 if block_dtype == torch.float64 else torch.float32
+        self.acc_dtype = self._acc_for(block_dtype)
         self.sub_ptr = torch.as_tensor(sub_ptr, device=dev)
         self.sub_idx = torch.as_tensor(sub_idx, device=dev)
         self.order = torch.as_tensor(np.argsort(-ks, kind="stable").astype(np.int32), device=dev)
@@ -386,10 +388,62 @@ class SchwarzOperator(SparseSolver):
             self.coarse_solver.destroy()
         self._scratch = {}
 
+    def requantize(self, dtype: torch.dtype) -> "SchwarzOperator":
+        """Same operator with the inverse blocks re-stored in ``dtype``.
+
+        Needs FP64 blocks in ``self`` (the exact inverses); shares every other
+        buffer (index maps, coarse space) with ``self``.
+        """
+        import copy
+
+        assert self.block_dtype == torch.float64, "requantize from FP64 blocks"
+        other = copy.copy(self)
+        other.local_solver = Inv(dtype)
+        other.block_dtype = dtype
+        other.acc_dtype = self._acc_for(dtype)
+        other._tiles = None
+        other._scratch = {}
+        store = so.BlockStore(self.ks, dtype, self.device)
+        N = self.n_solvers
+        i = 0
+        while i < N:
+            j = min(N, i + 256)
+            kb = so.round_up(max(int(self.ks[i:j].max()), 1), 16)
+            batch = torch.zeros(j - i, kb, kb, dtype=torch.float64, device=self.device)
+            for b in range(i, j):
+                k = int(self.ks[b])
+                if k:
+                    batch[b - i, :k, :k] = self.store.block(b)
+            store.put(i, batch)
+            i = j
+        other.store = store
+        return other
+
     # -- kernels -----------------------------------------------------------
+    def _acc_for(self, block_dtype: torch.dtype) -> torch.dtype:
+        """FP64 blocks accumulate in FP64; FP32 blocks in the vector type (as the
+        reference's GEMV does, gemv_kernels.cu:45-54); BF16/FP16 blocks in FP32."""
+        if block_dtype == torch.float64:
+            return torch.float64
+        if block_dtype == torch.float32 and (self.preconditioner_precision or torch.float64) == torch.float64:
+            return torch.float64
+        return torch.float32
+
     @property
     def local_bytes(self) -> int:
         return self.store.nbytes
+
+    def _tc_ok(self, R: int) -> bool:
+        """The tensor-core path: BF16/FP16 blocks, R in {16, 32, 64}, B panel in shared memory."""
+        if R not in (16, 32, 64) or self.block_dtype not in (torch.bfloat16, torch.float16):
+            return False
+        nk = (self.kmax + so.UMMA_K - 1) // so.UMMA_K
+        return 1024 + 4 * 16384 + nk * R * 128 + 192 <= 227 * 1024
+
+    def _tile_store(self):
+        if getattr(self, "_tiles", None) is None:
+            self._tiles = so.UmmaTileStore(self.store)
+        return self._tiles
 
     def scratch(self, R: int) -> dict:
         s = self._scratch.get(R)
@@ -404,8 +458,16 @@ class SchwarzOperator(SparseSolver):
             self._scratch[R] = s
         return s
 
-    def _local(self, r: torch.Tensor, R: int, ist: torch.Tensor | None = None) -> torch.Tensor:
+    def _local(self, r: torch.Tensor, R: int, ist: torch.Tensor | None = None,
+               st: torch.Tensor | None = None) -> torch.Tensor:
         s = self.scratch(R)
+        if self._tc_ok(R) and self.use_tensor_cores:
+            t = self._tile_store()
+            L.call("ddx_schwarz_local_apply_tc", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
+                   L.ptr(self.order), L.ptr(t.tile_off), L.ptr(t.data), L.DTYPE_CODE[self.block_dtype],
+                   L.ptr(self.store.scale), self.kmax, L.ptr(r), L.ptr(s["ylocal"]), L.ptr(ist), L.ptr(st),
+                   L.stream_ptr())
+            return s["ylocal"]
         L.call("ddx_schwarz_local_apply", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
                L.ptr(self.order), L.ptr(self.store.blk_off), L.ptr(self.store.data),
                L.DTYPE_CODE[self.block_dtype], L.ptr(self.store.scale), self.kmax, L.ptr(r),
@@ -479,10 +541,11 @@ class AdditiveSchwarz(SchwarzOperator):
     def _apply_fused(self, r, z, R, pcg, q):
         s = self.scratch(R)
         ist = None if pcg is None else pcg.ist
+        st = None if pcg is None else pcg.st
         if self.n_coarse:
             self._restrict(*self._R0, r, s["w"], R)
             self._coarse(s["w"], s["yc"], R, ist)
-        ylocal = self._local(r, R, ist)
+        ylocal = self._local(r, R, ist, st)
         self._combine(z, R, ylocal=ylocal, prolong=bool(self.n_coarse), sign=1.0, pcg=pcg, r=r, q=q)
 
 
@@ -520,7 +583,8 @@ class HybridSchwarz(SchwarzOperator):
     def _apply_fused(self, r, z, R, pcg, q):
         s = self.scratch(R)
         ist = None if pcg is None else pcg.ist
-        ylocal = self._local(r, R, ist)
+        st = None if pcg is None else pcg.st
+        ylocal = self._local(r, R, ist, st)
         if not self.n_coarse:
             self._combine(z, R, ylocal=ylocal, pcg=pcg, r=r, q=q)
             return
@@ -554,6 +618,7 @@ class _PcgWork:
         self.partials = torch.zeros(int(L.lib().ddx_partials_len(R)), **f)
         self.tickets = torch.zeros(L.TICKETS, dtype=torch.int32, device=device)
         self.graphs = {}
+        self.graph_calls = {}
         self.warm = False
 
 
@@ -696,11 +761,15 @@ class CG(SparseSolver):
                 w.warm = True
                 return
             g = torch.cuda.CUDAGraph()
+            c0 = L.CALLS[0]
             with torch.cuda.graph(g):
                 for rep in plan:
                     self._iteration(w, rep)
+            w.graph_calls[plan] = L.CALLS[0] - c0
+            L.CALLS[0] = c0
             w.graphs[plan] = g
         g.replay()
+        L.CALLS[0] += w.graph_calls[plan]
 
     # -- solve ---------------------------------------------------------------
     def solve(self, rhs: torch.Tensor, x0=None) -> Tuple[torch.Tensor, Metadata]:

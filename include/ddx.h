@@ -148,6 +148,20 @@ int ddx_schwarz_local_apply(int n_sub, int R, const int64_t* sub_ptr, const int*
                             const int* order, const int64_t* blk_off, const void* blocks,
                             int block_dtype, const float* scale, int kmax, const double* r,
                             void* ylocal, int acc_dtype, const int* ist, ddx_stream_t stream);
+/* Tensor-core variant for R in {16, 32, 64} right-hand sides and BF16/FP16
+ * blocks: Y_i = Q_i X_i as tcgen05.mma (M = 128, N = R, K = 16, FP32
+ * accumulators in TMEM). `tiles` holds each block cut into 128-row x 64-column
+ * tiles in the K-major 128-byte-swizzled shared-memory layout (row r of a tile
+ * at byte 128 r, its 16-byte chunk c stored at chunk c ^ (r % 8)), row-tile
+ * major, the last row tile truncated to a multiple of 8 rows, columns >= k
+ * zero; subdomain i starts at byte tile_off[i]. r is converted to the block
+ * type after scaling RHS j by a power of two near 1 / ||r_j|| (from st, the
+ * PCG state, when given). ylocal is FP32, (sum k_i, R). Needs
+ * 66 KB + ceil(kmax / 64) * R * 128 bytes of shared memory (<= 227 KB). */
+int ddx_schwarz_local_apply_tc(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
+                               const int* order, const int64_t* tile_off, const void* tiles,
+                               int block_dtype, const float* scale, int kmax, const double* r,
+                               float* ylocal, const int* ist, const double* st, ddx_stream_t stream);
 /* combine: z[d, j] = sum_{t in T(d)} ylocal[src[t], j]      (if ylocal)
  *                  + u[d, j]                                (if u)
  *                  + sign * sum_c P[d, c] yc[c, j]          (if p_ptr)
