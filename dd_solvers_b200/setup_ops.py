@@ -37,8 +37,12 @@ TARGET_EXP = {torch.float64: None, torch.float32: 0, torch.bfloat16: 0, torch.fl
 # SELL-32
 # ---------------------------------------------------------------------------
 
-def csr_to_sell32(crow: torch.Tensor, col: torch.Tensor, val: torch.Tensor):
-    """CSR -> SELL-32 (slice height 32, no row sorting)."""
+def csr_to_sell32(crow: torch.Tensor, col: torch.Tensor, val: torch.Tensor, return_positions: bool = False):
+    """CSR -> SELL-32 (slice height 32, no row sorting).
+
+    With ``return_positions`` also returns the SELL position of every CSR
+    entry, so new values on the same pattern can be scattered in place.
+    """
     dev = crow.device
     n = crow.numel() - 1
     nsl = (n + 31) // 32
@@ -65,6 +69,8 @@ def csr_to_sell32(crow: torch.Tensor, col: torch.Tensor, val: torch.Tensor):
     cols_s[dst] = col.to(torch.int32)
     vals_s[dst] = val.to(torch.float64)
     del rows_all
+    if return_positions:
+        return slice_ptr, width.to(torch.int32), cols_s, vals_s, dst
     return slice_ptr, width.to(torch.int32), cols_s, vals_s
 
 

@@ -633,8 +633,15 @@ class _SellMatrix:
         self.crow32 = crow.to(torch.int32)
         self.col32 = col.to(torch.int32)
         self.val = val
-        self.sell = so.csr_to_sell32(crow.to(torch.int64), col, val)
+        *self.sell, self._sell_pos = so.csr_to_sell32(crow.to(torch.int64), col, val, return_positions=True)
         self.nnz = int(col.numel())
+
+    def set_values(self, vals: torch.Tensor) -> None:
+        """New CSR values on the same sparsity pattern (both layouts updated in place)."""
+        assert vals.numel() == self.nnz
+        v = vals.to(self.val.device, torch.float64)
+        self.val.copy_(v)
+        self.sell[3][self._sell_pos] = v
 
     def launch(self, x, y, R, mode, w: _PcgWork | None = None, b=None, use_sell=True):
         st = ist = hist = partials = tickets = None
@@ -700,6 +707,11 @@ class CG(SparseSolver):
         self.n = matrix.shape[0]
         self._work = {}
         return timings
+
+    def set_matrix_values(self, vals: torch.Tensor) -> None:
+        """Replaces the system matrix's values (same sparsity pattern) without
+        touching the preconditioner; used by the differentiable solve."""
+        self.matrix.set_values(vals)
 
     # -- helpers -------------------------------------------------------------
     def _is_flexible(self) -> bool:

@@ -179,6 +179,16 @@ int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src
 int ddx_coarse_gemv_f64(int n_c, int R, const double* Ainv, const double* w, double* yc,
                         const int* ist, ddx_stream_t stream);
 
+/* ---- Differentiable solve -----------------------------------------------
+ * No counterpart in the reference (it has no autograd). Per-cell coefficient
+ * gradient of a Q1 diffusion solve on a uniform n_el^dim grid:
+ * grad[e] = -h^(dim-2) lambda_e^T K_ref u_e, with u and lambda on the
+ * x-fastest interior nodes (zero on the Dirichlet boundary), kref the
+ * (2^dim)^2 unit-cell stiffness (device memory, row-major, local node bit d =
+ * offset along axis d), cells numbered x fastest. */
+int ddx_elem_grad_q1(int dim, int n_el, const double* u, const double* lam, const double* kref,
+                     double* grad, ddx_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
