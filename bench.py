@@ -59,9 +59,9 @@ def build_problem(n_el: int, parts: int, seed: int = 0):
 
 
 def rhs_for(n: int, rank: int, step: int):
-    from dd_solvers_b200 import problems
+    from dd_solvers_b200 import problems, replicas
 
-    return problems.uniform_rhs(n, seed=1000 * rank + step)
+    return problems.uniform_rhs(n, seed=replicas.rhs_seed(rank, step))
 
 
 class Clocks:
@@ -195,6 +195,7 @@ def run_ours(args, rank: int, world: int):
 
     import dd_solvers_b200 as dd
     from dd_solvers_b200 import _lib as L
+    from dd_solvers_b200 import replicas
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
@@ -278,11 +279,7 @@ def run_ours(args, rank: int, world: int):
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
-        ms = ev0.elapsed_time(ev1) / k
-        if world > 1:
-            t = torch.tensor([ms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t)
+        ms = replicas.max_over_ranks(ev0.elapsed_time(ev1) / k, dev)
         return ms, its
 
     clocks = Clocks(dev.index if dev.index is not None else 0)
@@ -359,11 +356,7 @@ def run_ours(args, rank: int, world: int):
             Xb, mb = cgb.solve(Bd)
         e1.record()
         torch.cuda.synchronize()
-        bms = e0.elapsed_time(e1) / kb
-        if world > 1:
-            t = torch.tensor([bms], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            bms = float(t)
+        bms = replicas.max_over_ranks(e0.elapsed_time(e1) / kb, dev)
         # tensor-core kernel alone
         rb = torch.randn(n * Rb, dtype=torch.float64, device=dev)
         pcb = pcs[head]

@@ -1,0 +1,111 @@
+"""Kernel micro-benchmarks (counterparts of the reference's
+experiments/benchmark_batched_gemv.py and experiments/benchmark_bsrmv.py).
+
+    python -m dd_solvers_b200.microbench apply --n-el 64 --parts 8 --precision bf16 --rhs 1
+    python -m dd_solvers_b200.microbench spmv --n-el 128 --rhs 1
+
+``apply`` times the Schwarz local-inverse apply (SIMT streaming kernel for
+R < 16, tensor-core kernel for R in {16, 32, 64} with BF16/FP16 blocks) on the
+3D Q1 box-partition problem; ``spmv`` times the FP64 SpMV. Each prints one
+JSON line with the mean CUDA-event time per launch, the algorithmic bytes and
+the achieved GB/s against the measured HBM peak.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+
+import numpy as np
+import torch
+
+DT = {"f64": torch.float64, "f32": torch.float32, "bf16": torch.bfloat16, "f16": torch.float16}
+ELT = {"f64": 8, "f32": 4, "bf16": 2, "f16": 2}
+
+
+def _peak() -> float:
+    p = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "MEASURED_PEAKS.json")
+    return float(json.load(open(p))["hbm_gbs"]) if os.path.exists(p) else 6650.0
+
+
+def _problem(n_el: int, parts: int, seed: int = 0):
+    from . import partition, problems
+
+    P = problems.diffusion3d_lognormal(n_el, seed)
+    owner, nparts = partition.box_owner(P.interior_shape, parts)
+    sub_ptr, sub_idx = partition.overlapping_subdomains(P.matrix, owner, nparts, 1)
+    return P.matrix, sub_ptr, sub_idx, partition.q1_coarse_restriction(3, n_el, parts)
+
+
+def _time(fn, reps: int, warm: int = 3) -> float:
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def bench_apply(args) -> dict:
+    import dd_solvers_b200 as dd
+
+    dev = torch.device("cuda")
+    A, sub_ptr, sub_idx, R0 = _problem(args.n_el, args.parts)
+    pc = dd.AdditiveSchwarz(torch.float64, dd.Inv(DT[args.precision]), None)
+    pc.setup(dd.csr_to_torch(A).to(dev), subdomains=(sub_ptr, sub_idx))
+    R = args.rhs
+    pc.use_tensor_cores = not args.simt
+    r = torch.randn(A.shape[0] * R, dtype=torch.float64, device=dev)
+    ms = _time(lambda: pc._local(r, R), args.reps)
+    ks = pc.ks.astype(np.int64)
+    n = A.shape[0]
+    acc = 8 if pc.acc_dtype == torch.float64 else 4
+    nbytes = int((ks * ks).sum() * ELT[args.precision] + 4 * len(ks) + ks.sum() * 4 + n * R * 8 + ks.sum() * R * acc)
+    tc = pc._tc_ok(R) and pc.use_tensor_cores
+    return {"kernel": "ddx_schwarz_local_apply_tc" if tc else "ddx_schwarz_local_apply", "precision": args.precision,
+            "rhs": R, "n_dofs": n, "subdomains": len(ks), "k_max": int(ks.max()), "ms_per_launch": ms,
+            "algorithmic_bytes": nbytes, "achieved_gbs": nbytes / ms / 1e6, "frac_of_peak": nbytes / ms / 1e6 / _peak(),
+            "tflops": 2.0 * float((ks * ks).sum()) * R / ms / 1e9}
+
+
+def bench_spmv(args) -> dict:
+    import dd_solvers_b200 as dd
+    from dd_solvers_b200 import _lib as L
+    from .solvers import _SellMatrix
+
+    from . import problems
+
+    dev = torch.device("cuda")
+    A = problems.diffusion3d_lognormal(args.n_el, 0).matrix
+    M = _SellMatrix(dd.csr_to_torch(A).to(dev))
+    R = args.rhs
+    x = torch.randn(A.shape[0] * R, dtype=torch.float64, device=dev)
+    y = torch.empty_like(x)
+    ms = _time(lambda: M.launch(x, y, R, L.SPMV_PLAIN), args.reps)
+    n = A.shape[0]
+    nbytes = A.nnz * 12 + (n + 1) * 4 + n * R * 16
+    return {"kernel": "ddx_spmv_sell_f64" if R == 1 else "ddx_spmv_csr_f64", "rhs": R, "n_dofs": n, "nnz": A.nnz,
+            "ms_per_launch": ms, "algorithmic_bytes": nbytes, "achieved_gbs": nbytes / ms / 1e6,
+            "frac_of_peak": nbytes / ms / 1e6 / _peak()}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("what", choices=["apply", "spmv"])
+    ap.add_argument("--n-el", type=int, default=64)
+    ap.add_argument("--parts", type=int, default=8)
+    ap.add_argument("--precision", default="bf16", choices=list(DT))
+    ap.add_argument("--rhs", type=int, default=1)
+    ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--simt", action="store_true", help="force the SIMT kernel for R >= 16")
+    args = ap.parse_args()
+    out = bench_apply(args) if args.what == "apply" else bench_spmv(args)
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

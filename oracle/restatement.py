@@ -218,7 +218,7 @@ def pcg(A, b, M=None, rtol=1e-7, atol=0.0, maxiter=1000, x0=None, T0=None,
     return x, meta
 
 
-def pcg_multi(A, B, M=None, **kw):
+def pcg_multi(A, B, M=None, T0=None, **kw):
     """Column-by-column PCG for an ``(n, R)`` block of right-hand sides."""
     B = np.asarray(B, dtype=np.float64)
     X = np.zeros_like(B)
@@ -226,7 +226,8 @@ def pcg_multi(A, B, M=None, **kw):
     norms = []
     for j in range(B.shape[1]):
         Mj = None if M is None else (lambda r, M=M: M(r[:, None])[:, 0])
-        x, meta = pcg(A, B[:, j], Mj, **kw)
+        Tj = None if T0 is None else (lambda b, T0=T0: T0(b[:, None])[:, 0])
+        x, meta = pcg(A, B[:, j], Mj, T0=Tj, **kw)
         X[:, j] = x
         its.append(meta["iterations"])
         norms.append(meta["residual norms"])
