@@ -13,6 +13,9 @@ The reference has no differentiable solve; this follows the standard adjoint
 method. The preconditioner is built once (for a representative kappa) and
 reused: PCG converges to ``A(kappa)^{-1} b`` for any SPD preconditioner, so
 only the matrix values are refreshed per call (``CG.set_matrix_values``).
+Use ``AdditiveSchwarz`` for a reused preconditioner: it is SPD whatever the
+current matrix, whereas ``HybridSchwarz`` projects with ``R0 A`` of the matrix
+it was built for and must be rebuilt when kappa changes.
 """
 from __future__ import annotations
 

@@ -54,7 +54,9 @@ def _setup(cuda, n_el, parts, kappa):
     P = problems.q1_grid(2, n_el)
     owner, nparts = partition.box_owner(P.interior_shape, parts)
     sub_ptr, sub_idx = partition.overlapping_subdomains(A, owner, nparts, 1)
-    cg = dd.CG(dd.HybridSchwarz(torch.float64, dd.Inv(), dd.CUDSS()), rtol=1e-13, maxiter=3000)
+    # The preconditioner is built once and reused for other kappa: it must stay
+    # SPD for any A, which the additive form is (the hybrid projection is not).
+    cg = dd.CG(dd.AdditiveSchwarz(torch.float64, dd.Inv(), dd.CUDSS()), rtol=1e-12, maxiter=5000)
     cg.setup(op.matrix(torch.as_tensor(kappa, device=cuda)), subdomains=(sub_ptr, sub_idx), owner=owner,
              block_size=1)
     return op, cg, A
@@ -69,8 +71,8 @@ def test_gradient_matches_dense_adjoint(cuda):
     f = rng.uniform(-1, 1, (n_el - 1) ** 2)
     ut = rng.standard_normal((n_el - 1) ** 2) * 1e-3
     op, cg, A = _setup(cuda, n_el, 4, kappa)
-    k_t = torch.as_tensor(kappa, device=cuda, requires_grad=True)
-    f_t = torch.as_tensor(f, device=cuda, requires_grad=True)
+    k_t = torch.tensor(kappa, device=cuda, requires_grad=True)
+    f_t = torch.tensor(f, device=cuda, requires_grad=True)
     u = dd.DiffusionSolve.apply(k_t, f_t, op, cg)
     loss = ((u - torch.as_tensor(ut, device=cuda)) ** 2).sum()
     loss.backward()
