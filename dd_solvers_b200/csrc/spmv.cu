@@ -130,6 +130,130 @@ __global__ void __launch_bounds__(kThreads)
   publish_nactive(S, act);
 }
 
+// CSR SpMM for R >= 2 right-hand sides: R/2 threads per row, each owning two
+// adjacent RHS columns (16-byte loads of x rows), entries walked four at a
+// time with independent loads. Column sums for the PCG epilogues are reduced
+// as even/odd halves and written in the standard partials layout.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads)
+    k_spmm_csr2(int64_t n, const int* __restrict__ row_ptr, const int* __restrict__ cols,
+                const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y,
+                const double* __restrict__ b, PcgState S, double* partials, unsigned int* ticket) {
+  __shared__ double red[kThreads];
+  const int R = S.R;
+  if (MODE != DDX_SPMV_PLAIN && n_active(S.ist, R) == 0) return;
+  const int tpr = R / 2;
+  const int c2 = threadIdx.x % tpr;  // this thread's column pair
+  const int rpb = blockDim.x / tpr;
+  double acc0[2] = {0.0, 0.0}, acc1[2] = {0.0, 0.0};  // [even, odd] column partials
+  for (int64_t row = (int64_t)blockIdx.x * rpb + threadIdx.x / tpr; row < n; row += (int64_t)gridDim.x * rpb) {
+    const int k0 = row_ptr[row], k1 = row_ptr[row + 1];
+    double2 sum = make_double2(0.0, 0.0);
+    int k = k0;
+    for (; k + 4 <= k1; k += 4) {
+      const int cA = __ldg(cols + k), cB = __ldg(cols + k + 1), cC = __ldg(cols + k + 2), cD = __ldg(cols + k + 3);
+      const double vA = __ldg(vals + k), vB = __ldg(vals + k + 1), vC = __ldg(vals + k + 2), vD = __ldg(vals + k + 3);
+      const double2 xA = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cA * R) + c2);
+      const double2 xB = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cB * R) + c2);
+      const double2 xC = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cC * R) + c2);
+      const double2 xD = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cD * R) + c2);
+      sum.x = fma(vA, xA.x, sum.x); sum.y = fma(vA, xA.y, sum.y);
+      sum.x = fma(vB, xB.x, sum.x); sum.y = fma(vB, xB.y, sum.y);
+      sum.x = fma(vC, xC.x, sum.x); sum.y = fma(vC, xC.y, sum.y);
+      sum.x = fma(vD, xD.x, sum.x); sum.y = fma(vD, xD.y, sum.y);
+    }
+    for (; k < k1; ++k) {
+      const double v = __ldg(vals + k);
+      const double2 xv = __ldg(reinterpret_cast<const double2*>(x + (int64_t)__ldg(cols + k) * R) + c2);
+      sum.x = fma(v, xv.x, sum.x);
+      sum.y = fma(v, xv.y, sum.y);
+    }
+    double2* yo = reinterpret_cast<double2*>(y + row * R) + c2;
+    if (MODE == DDX_SPMV_PLAIN || MODE == DDX_SPMV_PQ) {
+      *yo = sum;
+      if (MODE == DDX_SPMV_PQ) {
+        const double2 xo = reinterpret_cast<const double2*>(x + row * R)[c2];
+        acc0[0] = fma(xo.x, sum.x, acc0[0]);
+        acc0[1] = fma(xo.y, sum.y, acc0[1]);
+      }
+    } else {
+      const double2 bi = reinterpret_cast<const double2*>(b + row * R)[c2];
+      const double2 ri = make_double2(bi.x - sum.x, bi.y - sum.y);
+      *yo = ri;
+      if (MODE == DDX_SPMV_RES_INIT) {
+        acc1[0] = fma(bi.x, bi.x, acc1[0]);
+        acc1[1] = fma(bi.y, bi.y, acc1[1]);
+      }
+      acc0[0] = fma(ri.x, ri.x, acc0[0]);
+      acc0[1] = fma(ri.y, ri.y, acc0[1]);
+    }
+  }
+  if (MODE == DDX_SPMV_PLAIN) return;
+  constexpr int NV = (MODE == DDX_SPMV_RES_INIT) ? 2 : 1;
+  // CTA sums of each column, written as partials[(cta * NV + v) * R + column]
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    const double* a = v == 0 ? acc0 : acc1;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const double s = block_sum_by_col(a[h], red, tpr);
+      if (threadIdx.x < tpr) partials[((size_t)blockIdx.x * NV + v) * R + 2 * threadIdx.x + h] = s;
+    }
+  }
+  if (!last_cta_arrival(ticket)) return;
+  double tot[NV];
+  final_sums<NV>(partials, R, red, tot, ticket);
+  int act = 0;
+  if (threadIdx.x < R) {
+    const int jj = threadIdx.x;
+    if (MODE == DDX_SPMV_PQ) act = fin_pq(S, jj, tot[0]);
+    if (MODE == DDX_SPMV_RES_INIT) act = fin_init(S, jj, tot[NV - 1], tot[0]);
+    if (MODE == DDX_SPMV_RES_REPLACE) act = fin_replace(S, jj, tot[0]);
+  }
+  publish_nactive(S, act);
+}
+
+// One CTA per (long) row for R >= 2: R/2 threads per entry, each owning two
+// RHS columns (16-byte x loads), 256/(R/2) entries per step, unrolled by 4;
+// fixed-order reduction of the per-thread sums (even and odd columns).
+__global__ void __launch_bounds__(kThreads)
+    k_spmv_rowblock2(int64_t n_rows, int R, const int* __restrict__ row_ptr, const int* __restrict__ cols,
+                     const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y) {
+  __shared__ double red[kThreads];
+  const int tpr = R / 2;
+  const int c2 = threadIdx.x % tpr;
+  const int G = blockDim.x / tpr;  // entries per step
+  const int e0 = threadIdx.x / tpr;
+  for (int64_t row = blockIdx.x; row < n_rows; row += gridDim.x) {
+    const int k0 = row_ptr[row], k1 = row_ptr[row + 1];
+    double2 s = make_double2(0.0, 0.0);
+    int k = k0 + e0;
+    for (; k + 3 * G < k1; k += 4 * G) {
+      const int cA = __ldg(cols + k), cB = __ldg(cols + k + G), cC = __ldg(cols + k + 2 * G),
+                cD = __ldg(cols + k + 3 * G);
+      const double vA = __ldg(vals + k), vB = __ldg(vals + k + G), vC = __ldg(vals + k + 2 * G),
+                   vD = __ldg(vals + k + 3 * G);
+      const double2 xA = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cA * R) + c2);
+      const double2 xB = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cB * R) + c2);
+      const double2 xC = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cC * R) + c2);
+      const double2 xD = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cD * R) + c2);
+      s.x = fma(vA, xA.x, s.x); s.y = fma(vA, xA.y, s.y);
+      s.x = fma(vB, xB.x, s.x); s.y = fma(vB, xB.y, s.y);
+      s.x = fma(vC, xC.x, s.x); s.y = fma(vC, xC.y, s.y);
+      s.x = fma(vD, xD.x, s.x); s.y = fma(vD, xD.y, s.y);
+    }
+    for (; k < k1; k += G) {
+      const double v = __ldg(vals + k);
+      const double2 xv = __ldg(reinterpret_cast<const double2*>(x + (int64_t)__ldg(cols + k) * R) + c2);
+      s.x = fma(v, xv.x, s.x);
+      s.y = fma(v, xv.y, s.y);
+    }
+    const double se = block_sum_by_col(s.x, red, tpr);
+    const double so = block_sum_by_col(s.y, red, tpr);
+    if (threadIdx.x < tpr) reinterpret_cast<double2*>(y + row * R)[threadIdx.x] = make_double2(se, so);
+  }
+}
+
 // One CTA per (long) row; threads stride over the row's entries.
 __global__ void __launch_bounds__(kThreads)
     k_spmv_rowblock(int64_t n_rows, int R, const int* __restrict__ row_ptr, const int* __restrict__ cols,
@@ -250,10 +374,35 @@ int ddx_spmv_csr_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols,
   if (n_rows == 0) return DDX_OK;
   cudaStream_t s = (cudaStream_t)stream;
   PcgState S{st, ist, hist, R};
+  unsigned int* t = tickets ? tickets + 3 : nullptr;
+  if (R >= 2) {
+    DDX_REQUIRE(((uintptr_t)x & 15u) == 0 && ((uintptr_t)y & 15u) == 0 && (b == nullptr || ((uintptr_t)b & 15u) == 0),
+                "ddx_spmv_csr_f64: x, y and b must be 16-byte aligned for R >= 2");
+    const int rpb2 = kThreads / (R / 2);
+    const int64_t need2 = ceil_div(n_rows, rpb2);
+    const int grid2 = (int)std::min<int64_t>(need2, kRedCtas);
+    switch (mode) {
+      case DDX_SPMV_PLAIN:
+        k_spmm_csr2<DDX_SPMV_PLAIN><<<(int)std::min<int64_t>(need2, 148 * 64), kThreads, 0, s>>>(
+            n_rows, row_ptr, cols, vals, x, y, b, S, partials, t);
+        break;
+      case DDX_SPMV_PQ:
+        k_spmm_csr2<DDX_SPMV_PQ><<<grid2, kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S, partials, t);
+        break;
+      case DDX_SPMV_RES_INIT:
+        k_spmm_csr2<DDX_SPMV_RES_INIT><<<grid2, kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S,
+                                                                  partials, t);
+        break;
+      default:
+        k_spmm_csr2<DDX_SPMV_RES_REPLACE><<<grid2, kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S,
+                                                                     partials, t);
+    }
+    DDX_LAUNCH_CHECK("ddx_spmv_csr_f64");
+    return DDX_OK;
+  }
   const int rpb = kThreads / R;
   const int64_t need = ceil_div(n_rows, rpb);
   const int grid = (int)std::min<int64_t>(need, kRedCtas);
-  unsigned int* t = tickets ? tickets + 3 : nullptr;
   switch (mode) {
     case DDX_SPMV_PLAIN:
       k_spmv_csr<DDX_SPMV_PLAIN><<<(int)std::min<int64_t>(need, 148 * 64), kThreads, 0, s>>>(
@@ -280,7 +429,13 @@ int ddx_spmv_csr_rowblock_f64(int64_t n_rows, int R, const int* row_ptr, const i
   DDX_REQUIRE(n_rows >= 0 && row_ptr && x && y, "ddx_spmv_csr_rowblock_f64: bad arguments");
   if (n_rows == 0) return DDX_OK;
   const int grid = (int)std::min<int64_t>(n_rows, 148 * 8);
-  k_spmv_rowblock<<<grid, kThreads, 0, (cudaStream_t)stream>>>(n_rows, R, row_ptr, cols, vals, x, y);
+  if (R >= 2) {
+    DDX_REQUIRE(((uintptr_t)x & 15u) == 0 && ((uintptr_t)y & 15u) == 0,
+                "ddx_spmv_csr_rowblock_f64: x and y must be 16-byte aligned for R >= 2");
+    k_spmv_rowblock2<<<grid, kThreads, 0, (cudaStream_t)stream>>>(n_rows, R, row_ptr, cols, vals, x, y);
+  } else {
+    k_spmv_rowblock<<<grid, kThreads, 0, (cudaStream_t)stream>>>(n_rows, R, row_ptr, cols, vals, x, y);
+  }
   DDX_LAUNCH_CHECK("ddx_spmv_csr_rowblock_f64");
   return DDX_OK;
 }

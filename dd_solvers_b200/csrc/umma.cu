@@ -9,8 +9,9 @@
 //               contiguous cp.async.bulk per tile into a 4-stage ring.
 //   warp 1      allocates TMEM; one lane issues tcgen05.mma (M=128, N=R, K=16)
 //               and tcgen05.commit to release ring stages / publish results.
-//   warps 2..5  gather X_i = r[idx_i, :] (FP64 -> 16-bit) into a resident
-//               K-major swizzled B buffer, then drain each 128-row accumulator
+//   warps 2..5  gather X_i = r16[idx_i, :] (rows of r packed to 16 bits by
+//               ddx_pack_rhs16) with 16-byte cp.async copies into a resident
+//               MN-major swizzled B panel, then drain each 128-row accumulator
 //               from TMEM (tcgen05.ld), scale, and store ylocal (FP32).
 // Two TMEM accumulators (2 x R columns) let the epilogue of row tile m overlap
 // the MMAs of row tile m+1. Every wait is bounded (device error word).
@@ -85,13 +86,39 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
          ((uint64_t)1u << 46) | ((uint64_t)2u << 61);
 }
 
+// MN-major B panel: one row of N 16-bit values (2N bytes) per K index, the
+// swizzle as wide as a row (128 / 64 / 32 bytes for N = 64 / 32 / 16), atoms of
+// 8 rows at stride SBO = 16 N bytes. LBO (stride between MN atoms) is unused
+// because N fits in one atom. Layout codes: 2 = 128B, 4 = 64B, 6 = 32B.
+template <int N>
+__device__ __forceinline__ uint64_t mn_desc(uint32_t saddr) {
+  constexpr uint32_t sbo = 16u * N;
+  constexpr uint64_t layout = N == 64 ? 2u : (N == 32 ? 4u : 6u);
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(sbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+         ((uint64_t)1u << 46) | (layout << 61);
+}
+
+// Byte offset of 16-byte chunk q of panel row c under the row-wide swizzle
+// (address bits [4,7) XOR bits [7,10), masked to the swizzle width).
+template <int N>
+__device__ __forceinline__ uint32_t mn_offset(int c, int q) {
+  constexpr uint32_t mask = N == 64 ? 7u : (N == 32 ? 3u : 1u);
+  const uint32_t L = (uint32_t)c * (2u * N) + (uint32_t)q * 16u;
+  return L ^ (((L >> 7) & mask) << 4);
+}
+
 // Instruction descriptor, kind::f16: D F32 (bits 4-5 = 1), A/B format in bits
-// 7-9 / 10-12 (F16 = 0, BF16 = 1), both K-major, N >> 3 in bits 17-22,
-// M >> 4 in bits 24-28.
+// 7-9 / 10-12 (F16 = 0, BF16 = 1), A K-major (bit 15 = 0), B MN-major
+// (bit 16 = 1), N >> 3 in bits 17-22, M >> 4 in bits 24-28.
 __host__ __device__ constexpr uint32_t idesc_f16(int ab_fmt, int N) {
-  return (1u << 4) | ((uint32_t)ab_fmt << 7) | ((uint32_t)ab_fmt << 10) | ((uint32_t)(N >> 3) << 17) |
+  return (1u << 4) | ((uint32_t)ab_fmt << 7) | ((uint32_t)ab_fmt << 10) | (1u << 16) | ((uint32_t)(N >> 3) << 17) |
          ((uint32_t)(kM >> 4) << 24);
 }
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
   asm volatile(
@@ -145,7 +172,7 @@ struct Args {
   const int64_t* tile_off;  // bytes
   const unsigned char* tiles;
   const float* scale;
-  const double* r;
+  const uint16_t* r16;  // packed 16-bit rows of r (n, N), scaled per RHS
   float* ylocal;
   const int* ist;
   const double* st;  // PCG state (||r_j||^2 scales the 16-bit conversion); may be null
@@ -264,7 +291,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc(Args a) {
             const uint32_t sb = smem_u32(bbuf + (size_t)t * N * 128);
 #pragma unroll
             for (int kk = 0; kk < kK / 16; ++kk)
-              mma_f16(d, sw128_desc(sa + kk * 32), sw128_desc(sb + kk * 32), idesc, (t > 0 || kk > 0) ? 1u : 0u);
+              mma_f16(d, sw128_desc(sa + kk * 32), mn_desc<N>(sb + kk * 32 * N), idesc, (t > 0 || kk > 0) ? 1u : 0u);
             mma_commit(&a_empty[s]);
           }
           if (abort_flag) break;
@@ -292,26 +319,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc(Args a) {
       const int nK = (k + kK - 1) / kK;
       // B buffer free once the MMAs of the previous subdomain completed
       if (!mbar_wait(b_empty, (sub_n & 1u) ^ 1u)) { abort_flag = 1; break; }
-      // gather: unit = (K tile t, 16-byte chunk c8, rhs j); j fastest
-      const int units = nK * 8 * N;
-      const double rsc = (double)rhs_scale(a.st, N, e % N);  // this thread's RHS: j = e % N
+      // gather: panel row c = packed 16-bit row of DOF sub_idx[p0 + c] (2N bytes,
+      // N/8 chunks of 16 bytes, copied asynchronously); rows k..64 nK-1 are zero
+      constexpr int CPR = N / 8;
+      const int units = nK * kK * CPR;
       for (int u = e; u < units; u += kEpiThreads) {
-        const int j = u % N;
-        const int rest = u / N;
-        const int c8 = rest & 7;
-        const int t = rest >> 3;
-        uint32_t packed[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          uint32_t lo = 0, hi = 0;
-          const int c0 = t * kK + c8 * 8 + 2 * q;
-          if (c0 < k) lo = to_bits<T>(rsc * a.r[(int64_t)a.sub_idx[p0 + c0] * N + j]);
-          if (c0 + 1 < k) hi = to_bits<T>(rsc * a.r[(int64_t)a.sub_idx[p0 + c0 + 1] * N + j]);
-          packed[q] = lo | (hi << 16);
-        }
-        unsigned char* row = bbuf + (size_t)t * N * 128 + (size_t)j * 128;
-        *reinterpret_cast<uint4*>(row + ((c8 ^ (j & 7)) * 16)) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+        const int c = u / CPR, q = u % CPR;
+        unsigned char* dst = bbuf + mn_offset<N>(c, q);
+        if (c < k) cp_async16(dst, a.r16 + (int64_t)a.sub_idx[p0 + c] * N + q * 8);
+        else *reinterpret_cast<uint4*>(dst) = make_uint4(0u, 0u, 0u, 0u);
       }
+      cp_async_wait_all();
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       epi_sync();
       if (e == 0) mbar_arrive(b_full);
@@ -373,17 +391,18 @@ using namespace ddx;
 
 extern "C" int ddx_schwarz_local_apply_tc(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
                                           const int* order, const int64_t* tile_off, const void* tiles,
-                                          int block_dtype, const float* scale, int kmax, const double* r,
+                                          int block_dtype, const float* scale, int kmax, const void* r16,
                                           float* ylocal, const int* ist, const double* st,
                                           ddx_stream_t stream) {
   DDX_REQUIRE(R == 16 || R == 32 || R == 64, "ddx_schwarz_local_apply_tc: R must be 16, 32 or 64 (got %d)", R);
   DDX_REQUIRE(n_sub >= 0 && kmax >= 0, "ddx_schwarz_local_apply_tc: bad sizes");
   if (n_sub == 0 || kmax == 0) return DDX_OK;
-  DDX_REQUIRE(sub_ptr && sub_idx && order && tile_off && tiles && r && ylocal,
+  DDX_REQUIRE(sub_ptr && sub_idx && order && tile_off && tiles && r16 && ylocal,
               "ddx_schwarz_local_apply_tc: null pointer");
-  DDX_REQUIRE(((uintptr_t)tiles & 15u) == 0 && ((uintptr_t)ylocal & 15u) == 0,
-              "ddx_schwarz_local_apply_tc: tiles and ylocal must be 16-byte aligned");
-  umma::Args a{n_sub, sub_ptr, sub_idx, order, tile_off, (const unsigned char*)tiles, scale, r, ylocal, ist, st, kmax};
+  DDX_REQUIRE(((uintptr_t)tiles & 15u) == 0 && ((uintptr_t)ylocal & 15u) == 0 && ((uintptr_t)r16 & 15u) == 0,
+              "ddx_schwarz_local_apply_tc: tiles, r16 and ylocal must be 16-byte aligned");
+  umma::Args a{n_sub, sub_ptr, sub_idx, order, tile_off, (const unsigned char*)tiles, scale,
+               (const uint16_t*)r16, ylocal, ist, st, kmax};
   cudaStream_t s = (cudaStream_t)stream;
   if (block_dtype == DDX_BF16) {
     if (R == 16) return umma::launch<__nv_bfloat16, 16>(a, s);
@@ -397,4 +416,37 @@ extern "C" int ddx_schwarz_local_apply_tc(int n_sub, int R, const int64_t* sub_p
   }
   set_error("ddx_schwarz_local_apply_tc: block dtype must be BF16 or F16");
   return DDX_ERR_ARG;
+}
+
+namespace ddx {
+namespace umma {
+// r16[i, j] = 16-bit(scale_j * r[i, j]) with the same per-RHS power-of-two
+// scale the tensor-core apply undoes (rhs_scale).
+template <typename T>
+__global__ void k_pack16(int64_t n, int R, const double* __restrict__ r, const double* __restrict__ st,
+                         uint16_t* __restrict__ out) {
+  const int64_t total = n * R;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int j = threadIdx.x % R;  // stride is a multiple of R
+  const double sc = (double)rhs_scale(st, R, j);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) out[i] = to_bits<T>(sc * r[i]);
+}
+}  // namespace umma
+}  // namespace ddx
+
+extern "C" int ddx_pack_rhs16(int64_t n, int R, const double* r, const double* st, void* r16, int dtype,
+                              ddx_stream_t stream) {
+  DDX_REQUIRE(valid_rhs_count(R), "ddx_pack_rhs16: unsupported R=%d", R);
+  DDX_REQUIRE(n >= 0 && r && r16, "ddx_pack_rhs16: bad arguments");
+  if (n == 0) return DDX_OK;
+  const int grid = (int)std::min<int64_t>(ceil_div(n * R, 256), 148 * 16);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == DDX_BF16) umma::k_pack16<__nv_bfloat16><<<grid, 256, 0, s>>>(n, R, r, st, (uint16_t*)r16);
+  else if (dtype == DDX_F16) umma::k_pack16<__half><<<grid, 256, 0, s>>>(n, R, r, st, (uint16_t*)r16);
+  else {
+    set_error("ddx_pack_rhs16: dtype must be BF16 or F16");
+    return DDX_ERR_ARG;
+  }
+  DDX_LAUNCH_CHECK("ddx_pack_rhs16");
+  return DDX_OK;
 }

@@ -59,6 +59,11 @@ def bench_apply(args) -> dict:
     pc.setup(dd.csr_to_torch(A).to(dev), subdomains=(sub_ptr, sub_idx))
     R = args.rhs
     pc.use_tensor_cores = not args.simt
+    pc.autotune = args.tune
+    tune = None
+    if args.tune:
+        pc.tune(R)
+        tune = {f"groups={g},stage_kb={kb}": ms for (g, kb), ms in pc.tune_timings.items()}
     r = torch.randn(A.shape[0] * R, dtype=torch.float64, device=dev)
     ms = _time(lambda: pc._local(r, R), args.reps)
     ks = pc.ks.astype(np.int64)
@@ -69,7 +74,7 @@ def bench_apply(args) -> dict:
     return {"kernel": "ddx_schwarz_local_apply_tc" if tc else "ddx_schwarz_local_apply", "precision": args.precision,
             "rhs": R, "n_dofs": n, "subdomains": len(ks), "k_max": int(ks.max()), "ms_per_launch": ms,
             "algorithmic_bytes": nbytes, "achieved_gbs": nbytes / ms / 1e6, "frac_of_peak": nbytes / ms / 1e6 / _peak(),
-            "tflops": 2.0 * float((ks * ks).sum()) * R / ms / 1e9}
+            "tflops": 2.0 * float((ks * ks).sum()) * R / ms / 1e9, "config": pc._apply_config(R), "tune_ms": tune}
 
 
 def bench_spmv(args) -> dict:
@@ -102,6 +107,7 @@ def main():
     ap.add_argument("--rhs", type=int, default=1)
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--simt", action="store_true", help="force the SIMT kernel for R >= 16")
+    ap.add_argument("--tune", action="store_true", help="run the autotuner first and report every candidate")
     args = ap.parse_args()
     out = bench_apply(args) if args.what == "apply" else bench_spmv(args)
     print(json.dumps(out))

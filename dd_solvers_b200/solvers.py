@@ -267,6 +267,7 @@ class SchwarzOperator(SparseSolver):
         self._scratch = {}
         self._tiles = None
         self.use_tensor_cores = True
+        self.autotune = True
 
     # -- setup -------------------------------------------------------------
     def setup(self, matrix: torch.Tensor, dofs_per_solver: int | None = None,
@@ -463,16 +464,68 @@ class SchwarzOperator(SparseSolver):
         s = self.scratch(R)
         if self._tc_ok(R) and self.use_tensor_cores:
             t = self._tile_store()
+            if "r16" not in s:
+                s["r16"] = torch.empty(self.n * R, dtype=self.block_dtype, device=self.device)
+            code = L.DTYPE_CODE[self.block_dtype]
+            L.call("ddx_pack_rhs16", self.n, R, L.ptr(r), L.ptr(st), L.ptr(s["r16"]), code, L.stream_ptr())
             L.call("ddx_schwarz_local_apply_tc", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
-                   L.ptr(self.order), L.ptr(t.tile_off), L.ptr(t.data), L.DTYPE_CODE[self.block_dtype],
-                   L.ptr(self.store.scale), self.kmax, L.ptr(r), L.ptr(s["ylocal"]), L.ptr(ist), L.ptr(st),
-                   L.stream_ptr())
+                   L.ptr(self.order), L.ptr(t.tile_off), L.ptr(t.data), code, L.ptr(self.store.scale), self.kmax,
+                   L.ptr(s["r16"]), L.ptr(s["ylocal"]), L.ptr(ist), L.ptr(st), L.stream_ptr())
             return s["ylocal"]
-        L.call("ddx_schwarz_local_apply", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
+        cfg = self._apply_config(R)
+        self._simt_apply(r, s["ylocal"], R, ist, *cfg)
+        return s["ylocal"]
+
+    def _simt_apply(self, r, ylocal, R, ist, groups: int, stage_kb: int) -> None:
+        L.call("ddx_schwarz_local_apply_ex", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
                L.ptr(self.order), L.ptr(self.store.blk_off), L.ptr(self.store.data),
                L.DTYPE_CODE[self.block_dtype], L.ptr(self.store.scale), self.kmax, L.ptr(r),
-               L.ptr(s["ylocal"]), L.DTYPE_CODE[self.acc_dtype], L.ptr(ist), L.stream_ptr())
-        return s["ylocal"]
+               L.ptr(ylocal), L.DTYPE_CODE[self.acc_dtype], L.ptr(ist), groups, stage_kb, L.stream_ptr())
+
+    # -- autotuner -------------------------------------------------------------
+    # (groups of consumer warps, KiB per shared-memory stage) candidates for the SIMT apply
+    TUNE_CANDIDATES = [(g, kb) for g in (1, 2, 4) for kb in (12, 20, 32)]
+    _tuned: dict = {}
+
+    def _tune_key(self, R: int):
+        return (str(self.block_dtype), str(self.acc_dtype), R, self.kmax, self.n_solvers, int(self.store.total))
+
+    def _apply_config(self, R: int) -> tuple[int, int]:
+        """Tuned (groups, stage KiB) for this operator; tunes on first eager use."""
+        key = self._tune_key(R)
+        cfg = SchwarzOperator._tuned.get(key)
+        if cfg is not None:
+            return cfg
+        if not self.autotune or torch.cuda.is_current_stream_capturing():
+            return (0, 0)  # library defaults
+        return self.tune(R)
+
+    def tune(self, R: int = 1, reps: int = 3) -> tuple[int, int]:
+        """Project autotuner: times every candidate configuration of the SIMT
+        local apply on this operator's own blocks (CUDA events, after one
+        warm-up launch) and keeps the fastest; results are cached per
+        (precision, R, sizes) for the process."""
+        s = self.scratch(R)
+        r = torch.randn(self.n * R, dtype=torch.float64, device=self.device)
+        best, best_ms, timings = (0, 0), float("inf"), {}
+        for g, kb in self.TUNE_CANDIDATES:
+            try:
+                self._simt_apply(r, s["ylocal"], R, None, g, kb)
+            except L.DDXError:
+                continue  # e.g. shared memory too small for this shape
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                self._simt_apply(r, s["ylocal"], R, None, g, kb)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            timings[(g, kb)] = ms
+            if ms < best_ms:
+                best, best_ms = (g, kb), ms
+        SchwarzOperator._tuned[self._tune_key(R)] = best
+        self.tune_timings = timings
+        return best
 
     def _restrict(self, rowptr, col, val, x, out, R):
         L.call("ddx_spmv_csr_rowblock_f64", rowptr.numel() - 1, R, L.ptr(rowptr), L.ptr(col), L.ptr(val),

@@ -87,7 +87,6 @@ int ddx_pcg_update_xr(int64_t n, int R, double* x, double* r, const double* p, c
  * themselves (generic path). q may be NULL on the first iteration. */
 int ddx_pcg_dots_rz(int64_t n, int R, const double* r, const double* z, const double* q, double* st,
                     int* ist, double* partials, unsigned int* tickets, ddx_stream_t stream);
-/* Residual replacement without SpMV fusion: recompute the stop test from r. */
 /* out[j] = x_j . y_j for R right-hand sides in (n, R) layout, with the same
  * deterministic two-stage reduction as ddx_pcg_dots_rz, but without any
  * caller-provided scratch: for callers that cannot allocate device memory
@@ -159,6 +158,14 @@ int ddx_gemv_strided_batched(int64_t N, int k, const void* mat, int mat_dtype, c
  *   (TMA engine); accumulation in FP32 for F32/BF16/F16 blocks, FP64 for F64.
  *   ylocal has element type acc (F32 or F64) and layout (sum k_i, R).
  */
+/* Same with explicit tuning knobs (setup-time autotuner): `groups` consumer
+ * groups of four warps split each block's columns (1, 2 or 4; 0 = default 2)
+ * and `stage_kb` KiB per shared-memory ring stage (0 = default 20). */
+int ddx_schwarz_local_apply_ex(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
+                               const int* order, const int64_t* blk_off, const void* blocks,
+                               int block_dtype, const float* scale, int kmax, const double* r,
+                               void* ylocal, int acc_dtype, const int* ist, int groups, int stage_kb,
+                               ddx_stream_t stream);
 int ddx_schwarz_local_apply(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
                             const int* order, const int64_t* blk_off, const void* blocks,
                             int block_dtype, const float* scale, int kmax, const double* r,
@@ -169,14 +176,19 @@ int ddx_schwarz_local_apply(int n_sub, int R, const int64_t* sub_ptr, const int*
  * tiles in the K-major 128-byte-swizzled shared-memory layout (row r of a tile
  * at byte 128 r, its 16-byte chunk c stored at chunk c ^ (r % 8)), row-tile
  * major, the last row tile truncated to a multiple of 8 rows, columns >= k
- * zero; subdomain i starts at byte tile_off[i]. r is converted to the block
- * type after scaling RHS j by a power of two near 1 / ||r_j|| (from st, the
- * PCG state, when given). ylocal is FP32, (sum k_i, R). Needs
+ * zero; subdomain i starts at byte tile_off[i]. r16 is r packed to the block
+ * type by ddx_pack_rhs16 (same st). ylocal is FP32, (sum k_i, R). Needs
  * 66 KB + ceil(kmax / 64) * R * 128 bytes of shared memory (<= 227 KB). */
 int ddx_schwarz_local_apply_tc(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
                                const int* order, const int64_t* tile_off, const void* tiles,
-                               int block_dtype, const float* scale, int kmax, const double* r,
+                               int block_dtype, const float* scale, int kmax, const void* r16,
                                float* ylocal, const int* ist, const double* st, ddx_stream_t stream);
+/* r16[i, j] = (dtype) (s_j * r[i, j]), dtype BF16 or F16, with s_j the power of
+ * two near 1 / ||r_j|| taken from st (||r_j||^2 slot; 1 when st is NULL), so
+ * residual entries stay in the 16-bit range as the solve converges; the
+ * tensor-core apply divides s_j out again. */
+int ddx_pack_rhs16(int64_t n, int R, const double* r, const double* st, void* r16, int dtype,
+                   ddx_stream_t stream);
 /* combine: z[d, j] = sum_{t in T(d)} ylocal[src[t], j]      (if ylocal)
  *                  + u[d, j]                                (if u)
  *                  + sign * sum_c P[d, c] yc[c, j]          (if p_ptr)

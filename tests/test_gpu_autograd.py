@@ -125,4 +125,6 @@ def test_grf_gradient_central_differences(cuda):
         fd = (lp - lm) / (2 * h)
         ad = float((gk * dk).sum() + (gf * df).sum())
         worst = max(worst, abs(fd - ad) / max(abs(ad), 1e-30))
-    assert worst <= 1e-5, worst
+    # Error budget: each of the two solves per difference stops at rtol 1e-12,
+    # leaving ~1e-11 relative error in L, amplified by 1/(2h) = 5e5 -> ~1e-5.
+    assert worst <= 1e-4, worst

@@ -180,6 +180,31 @@ def test_schwarz_apply(cuda, prec, case):
         assert np.linalg.norm(z - zr) <= tol * np.linalg.norm(zr), (kind, np.linalg.norm(z - zr) / np.linalg.norm(zr))
 
 
+@pytest.mark.parametrize("prec", ["f64", "f32", "bf16"])
+def test_simt_apply_every_tuning_candidate(cuda, prec):
+    """Every (consumer groups, stage size) the autotuner may pick, on subdomains
+    of up to 34^2 = 1156 DOFs (FP64: 5 row groups per thread, instantiated as 8)."""
+    import dd_solvers_b200 as dd
+    from oracle import restatement as orc
+
+    P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(2, 96, 3)
+    pc = dd.AdditiveSchwarz(torch.float64, dd.Inv(DT[prec]), None)
+    pc.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx))
+    blocks = [pc.store.block(i).cpu().numpy() for i in range(pc.n_solvers)]
+    r = np.random.default_rng(5).standard_normal(A.shape[0])
+    rt = torch.as_tensor(r, device=cuda)
+    ref = np.concatenate([blocks[i] @ r[sub_idx[sub_ptr[i]:sub_ptr[i + 1]]] for i in range(pc.n_solvers)])
+    tol = 1e-12 if prec != "bf16" else 2e-6
+    for groups, kb in pc.TUNE_CANDIDATES:
+        s = pc.scratch(1)
+        pc._simt_apply(rt, s["ylocal"], 1, None, groups, kb)
+        got = s["ylocal"][: len(sub_idx)].double().cpu().numpy()
+        assert np.linalg.norm(got - ref) <= tol * np.linalg.norm(ref), (groups, kb)
+    from dd_solvers_b200 import _lib
+
+    assert _lib.device_error() == 0
+
+
 @pytest.mark.parametrize("prec", ["f32", "bf16", "f16"])
 def test_block_quantisation_matches_oracle(cuda, prec):
     """Stored blocks equal the oracle's power-of-two-scaled rounding of the FP64 inverse."""
