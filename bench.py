@@ -1,16 +1,22 @@
 """Benchmark: time per right-hand side to 1e-8 relative error, mixed precision vs FP64.
 
-Workload (default): 3D Q1 diffusion on 128^3 hexahedra (127^3 = 2,048,383 DOFs),
-kappa = exp(g), g i.i.d. N(0,1) per element (seed 0); 16^3 = 4096 box subdomains
-with one layer of overlap; Q1 coarse space on the subdomain vertices (15^3 =
-3375 coarse DOFs); Hybrid Schwarz with local inverse blocks stored in BF16
-(per-block power-of-two scale, FP32 accumulation); FP64 flexible PCG. One
-step = one PCG solve of one right-hand side (uniform[-1,1], seeded). The
-relative error of every timed solution against the FP64 reference solution
-(the FP64 plain path at rtol 1e-12) is checked to be <= 1e-8; the stopping
-tolerance is tightened until it is.
+Default workload (C2, the headline): 3D Q1 diffusion on 128^3 hexahedra
+(127^3 = 2,048,383 DOFs), kappa = exp(g), g i.i.d. N(0,1) per element (seed 0);
+16^3 = 4096 box subdomains with one layer of overlap; Q1 coarse space on the
+subdomain vertices (15^3 = 3375 coarse DOFs); Hybrid Schwarz with local inverse
+blocks stored in BF16 (per-block power-of-two scale, FP32 accumulation); FP64
+flexible PCG. One step = one PCG solve of one right-hand side (uniform[-1,1],
+seeded). The relative error of every timed solution against the FP64 reference
+solution (the FP64 plain path at rtol 1e-12) is checked to be <= 1e-8; the
+stopping tolerance is tightened until it is.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n-el 128] [--parts 16]
+Other workloads (--workload): c1 2D Q1 Poisson 256^2, 8x8 subdomains, additive
+Schwarz; c3 2D Q1 Poisson 1024^2, 32x32 subdomains, 64 right-hand sides per
+solve on the tensor cores; c5 jittered P1 on 2048^2 nodes, RCB into 2048 uneven
+subdomains, 16 right-hand sides per solve. For several right-hand sides a step
+is one solve of the whole block and the time is divided by their number.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2]
 
 --impl reference times the FP64 CPU restatement of the same algorithm on the
 host cores (the reference's own solver runs on GPUs only; its CPU behaviour is
@@ -36,6 +42,25 @@ sys.path.insert(0, ROOT)
 
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
+# fp64_iterations: PCG iterations of the FP64 method on the workload (measured on
+# B200 by the GPU arm; the CPU restatement reproduces it +-1), used to scale the
+# per-iteration CPU sample of the reference arm.
+WORKLOADS = {
+    "c2": dict(kind="q1_3d", n_el=128, parts=16, coarse="q1", method="hybrid", rhs="uniform", R=1,
+               fp64_iterations=31,
+               name="hybrid-schwarz q1-3d 128^3 cells lognormal kappa, 4096 subdomains overlap 1, q1 coarse 3375"),
+    "c1": dict(kind="q1_2d", n_el=256, parts=8, coarse="p0", method="additive", rhs="uniform", R=1,
+               fp64_iterations=30,
+               name="additive-schwarz q1-2d poisson 256^2 cells, 64 subdomains overlap 1, p0 coarse 64"),
+    "c3": dict(kind="q1_2d", n_el=1024, parts=32, coarse="p0", method="hybrid", rhs="normal", R=64,
+               fp64_iterations=40,
+               name="hybrid-schwarz q1-2d poisson 1024^2 cells, 1024 subdomains overlap 1, p0 coarse, 64 rhs"),
+    "c5": dict(kind="p1", n_nodes=2048, parts=2048, coarse="p0", method="hybrid", rhs="normal", R=16,
+               fp64_iterations=60,
+               name="hybrid-schwarz p1 jittered 2048^2 nodes lognormal kappa, rcb 2048 subdomains overlap 1, "
+                    "p0 coarse, 16 rhs"),
+}
+
 
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -45,23 +70,36 @@ def load_peaks():
     return dict(PEAKS_FALLBACK, source="fallback")
 
 
-def build_problem(n_el: int, parts: int, seed: int = 0):
+def build_problem(spec: dict, seed: int = 0):
     from dd_solvers_b200 import partition, problems
 
     t0 = time.time()
-    P = problems.diffusion3d_lognormal(n_el, seed)
+    if spec["kind"] == "q1_3d":
+        P = problems.diffusion3d_lognormal(spec["n_el"], seed)
+        owner, nparts = partition.box_owner(P.interior_shape, spec["parts"])
+    elif spec["kind"] == "q1_2d":
+        P = problems.poisson2d(spec["n_el"])
+        owner, nparts = partition.box_owner(P.interior_shape, spec["parts"])
+    else:
+        P = problems.p1_jittered(spec["n_nodes"], 0.3, 1.0, seed)
+        nparts = spec["parts"]
+        owner = partition.rcb_owner(P.coords, nparts)
     A = P.matrix
-    owner, nparts = partition.box_owner(P.interior_shape, parts)
     sub_ptr, sub_idx = partition.overlapping_subdomains(A, owner, nparts, 1)
-    R0 = partition.q1_coarse_restriction(3, n_el, parts)
+    if spec["coarse"] == "q1":
+        R0 = partition.q1_coarse_restriction(3, spec["n_el"], spec["parts"])
+    else:
+        R0 = partition.p0_restriction(owner, nparts)
     return dict(P=P, A=A, owner=owner, nparts=nparts, sub_ptr=sub_ptr, sub_idx=sub_idx, R0=R0,
                 host_setup_s=time.time() - t0)
 
 
-def rhs_for(n: int, rank: int, step: int):
+def rhs_for(n: int, rank: int, step: int, spec: dict, R: int | None = None):
     from dd_solvers_b200 import problems, replicas
 
-    return problems.uniform_rhs(n, seed=replicas.rhs_seed(rank, step))
+    seed = replicas.rhs_seed(rank, step)
+    gen = problems.uniform_rhs if spec["rhs"] == "uniform" else problems.normal_rhs
+    return gen(n, seed=seed, nrhs=R if (R or 1) > 1 else None)
 
 
 class Clocks:
@@ -126,7 +164,7 @@ def cpu_time_per_rhs(prob, iterations: int, sample_subdomains: int = 48, budget_
     SpMV, the coarse restriction / solve / prolongation and the vector updates,
     and for ``sample_subdomains`` of the local inverse applies (dense FP64 GEMV
     with NumPy's threaded BLAS), scaled to all subdomains; times the iteration
-    count the FP64 GPU solve needed.
+    count the FP64 solve needs on the workload.
     """
     import scipy.linalg as sla
 
@@ -178,7 +216,7 @@ def cpu_time_per_rhs(prob, iterations: int, sample_subdomains: int = 48, budget_
     return {
         "ms_per_rhs": per_iter * iterations * 1e3,
         "per_iteration_ms": per_iter * 1e3,
-        "sample": (f"one FP64 hybrid-Schwarz PCG iteration of the oracle restatement on the full problem "
+        "sample": (f"one FP64 Schwarz PCG iteration of the oracle restatement on the full problem "
                    f"(SpMV, coarse, vector updates timed in full; local inverse GEMVs timed on {len(invs)} of "
                    f"{N} subdomains and scaled) x {iterations} iterations"),
         "cores": os.cpu_count(),
@@ -189,7 +227,7 @@ def cpu_time_per_rhs(prob, iterations: int, sample_subdomains: int = 48, budget_
 # GPU arm
 # ---------------------------------------------------------------------------
 
-def run_ours(args, rank: int, world: int):
+def run_ours(args, spec, rank: int, world: int):
     import torch
     import torch.distributed as dist
 
@@ -199,23 +237,26 @@ def run_ours(args, rank: int, world: int):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    prob = build_problem(args.n_el, args.parts)
+    R = spec["R"]
+    prob = build_problem(spec)
     A = prob["A"]
     n = A.shape[0]
     At = dd.csr_to_torch(A).to(dev)
+    head = args.precision
+    precs = ("f64", "bf16", "f32", "f16") if R == 1 else ("f64", head)
 
     t0 = time.time()
-    pc64 = dd.HybridSchwarz(torch.float64, dd.Inv(), dd.CUDSS())
+    cls = dd.HybridSchwarz if spec["method"] == "hybrid" else dd.AdditiveSchwarz
+    pc64 = cls(torch.float64, dd.Inv(), dd.CUDSS())
     pc64.setup(At, subdomains=(prob["sub_ptr"], prob["sub_idx"]), coarse_restriction=prob["R0"])
     pcs = {"f64": pc64}
-    for name, dt in (("bf16", torch.bfloat16), ("f32", torch.float32), ("f16", torch.float16)):
-        pcs[name] = pc64.requantize(dt)
+    for name in precs[1:]:
+        pcs[name] = pc64.requantize({"bf16": torch.bfloat16, "f32": torch.float32, "f16": torch.float16}[name])
     torch.cuda.synchronize()
     gpu_setup_s = time.time() - t0
 
     # one CG front-end per precision sharing the SELL matrix of the first
-    base = dd.CG(pcs["f64"], rtol=1e-12, maxiter=2000, check_every=args.check_every)
-    base.preconditioner = None
+    base = dd.CG(None, rtol=1e-12, maxiter=2000, check_every=args.check_every)
     base.setup(At, block_size=1)
     mat = base.matrix
 
@@ -227,36 +268,52 @@ def run_ours(args, rank: int, world: int):
         cg.block_size = 1
         return cg
 
-    b0 = torch.as_tensor(rhs_for(n, rank, 0), device=dev)
-    xref, mref = make("f64", 1e-12).solve(b0)
-    nref = float(torch.linalg.norm(xref))
+    def rhs(step, nr=None):
+        return torch.as_tensor(rhs_for(n, rank, step, spec, nr), device=dev)
 
-    def rel_err(x):
-        return float(torch.linalg.norm(x - xref)) / nref
+    # FP64 reference solutions (single RHS at rtol 1e-12) for the checked columns
+    check_cols = [0] if R == 1 else [0, R - 1]
+    B0 = rhs(0, R)
+    ref = {}
+    for j in check_cols:
+        bj = B0 if R == 1 else B0[:, j].contiguous()
+        ref[j], _ = make("f64", 1e-12).solve(bj)
+
+    def max_err(X):
+        es = []
+        for j in check_cols:
+            xj = X if R == 1 else X[:, j]
+            es.append(float(torch.linalg.norm(xj - ref[j]) / torch.linalg.norm(ref[j])))
+        return max(es)
 
     # calibrate the stopping tolerance of each precision to reach 1e-8 error
     cal = {}
-    for prec in ("f64", "bf16", "f32", "f16"):
+    for prec in precs:
         rtol = 1e-8
         for _ in range(6):
             cg = make(prec, rtol)
-            x, meta = cg.solve(b0)
-            e = rel_err(x)
+            if prec == "f64" and R > 1:
+                x, meta = cg.solve(B0[:, 0].contiguous())  # FP64 plain comparison runs one RHS
+                e = float(torch.linalg.norm(x - ref[0]) / torch.linalg.norm(ref[0]))
+            else:
+                x, meta = cg.solve(B0)
+                e = max_err(x)
             if e <= 1e-8:
                 break
             rtol /= 4
-        cal[prec] = {"rtol": rtol, "rel_error": e, "iterations": meta["iterations"], "solver": cg}
+        its = meta["iterations"] if isinstance(meta["iterations"], int) else max(meta["iterations"])
+        cal[prec] = {"rtol": rtol, "rel_error": e, "iterations": its, "solver": cg}
 
-    head = args.precision
     steps, warm = args.steps, args.warmup
 
     def timed(prec, k, w, host=False, count_from_timed=False):
         cg = cal[prec]["solver"]
-        bs = [torch.as_tensor(rhs_for(n, rank, s + 1), device=dev) for s in range(min(k, 4))]
+        nr = R if (prec != "f64" or R == 1) else 1
+        bs = [rhs(s + 1, nr) for s in range(min(k, 4))]
         if host:
             bh = [b.cpu().pin_memory() for b in bs]
-            xh = torch.empty(n, dtype=torch.float64).pin_memory()
-            bd = torch.empty(n, dtype=torch.float64, device=dev)
+            xh = torch.empty_like(bh[0]).pin_memory()
+            bd = torch.empty_like(bs[0])
         for s in range(w):
             cg.solve(bs[s % len(bs)])
         if world > 1:
@@ -274,13 +331,13 @@ def run_ours(args, rank: int, world: int):
                 xh.copy_(x, non_blocking=True)
             else:
                 x, meta = cg.solve(bs[s % len(bs)])
-            its.append(meta["iterations"])
+            its.append(meta["iterations"] if isinstance(meta["iterations"], int) else max(meta["iterations"]))
         ev1.record()
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         ms = replicas.max_over_ranks(ev0.elapsed_time(ev1) / k, dev)
-        return ms, its
+        return ms / nr, its  # per right-hand side
 
     clocks = Clocks(dev.index if dev.index is not None else 0)
     clocks.start()  # sampler running before the warm-up, so its start-up stays outside the timed region
@@ -290,13 +347,21 @@ def run_ours(args, rank: int, world: int):
     launches = L.CALLS[0]
     # every timed solution meets the error bar
     errs = {}
-    for prec in ("f64", "bf16", "f32", "f16"):
-        bt = torch.as_tensor(rhs_for(n, rank, 1), device=dev)
-        xr, _ = make("f64", 1e-12).solve(bt)
+    for prec in precs:
+        nr = R if (prec != "f64" or R == 1) else 1
+        bt = rhs(1, nr)
         x, _ = cal[prec]["solver"].solve(bt)
-        errs[prec] = float(torch.linalg.norm(x - xr) / torch.linalg.norm(xr))
+        es = []
+        for j in (check_cols if nr > 1 else [0]):
+            bj = bt if nr == 1 else bt[:, j].contiguous()
+            xr, _ = make("f64", 1e-12).solve(bj)
+            xj = x if nr == 1 else x[:, j]
+            es.append(float(torch.linalg.norm(xj - xr) / torch.linalg.norm(xr)))
+        errs[prec] = max(es)
     per_prec = {}
-    for prec in ("f64", "f32", "f16"):
+    for prec in precs:
+        if prec == head:
+            continue
         ms, its = timed(prec, max(1, min(steps, 3)), 1)
         per_prec[prec] = {"ms_per_rhs": ms, "iterations": its[-1], "rtol": cal[prec]["rtol"],
                           "rel_error": errs[prec]}
@@ -306,41 +371,42 @@ def run_ours(args, rank: int, world: int):
 
     # dominant kernel: local inverse apply of the head precision, timed alone
     pc = pcs[head]
-    r = torch.randn(n, dtype=torch.float64, device=dev)
+    r = torch.randn(n * R, dtype=torch.float64, device=dev)
     for _ in range(3):
-        pc._local(r, 1)
+        pc._local(r, R)
     kev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     reps = 10
     torch.cuda.synchronize()
     kev[0].record()
     for _ in range(reps):
-        pc._local(r, 1)
+        pc._local(r, R)
     kev[1].record()
     torch.cuda.synchronize()
     k_ms = kev[0].elapsed_time(kev[1]) / reps
     ks = pc.ks.astype(np.int64)
     elt = {"f64": 8, "f32": 4, "bf16": 2, "f16": 2}[head]
-    alg_bytes = int((ks * ks).sum() * elt + 4 * len(ks) + ks.sum() * 4 + n * 8 + ks.sum() * 4)
-    # SpMV (FP64 SELL) timed alone too
+    tc = pc._tc_ok(R) and pc.use_tensor_cores
+    alg_bytes = int((ks * ks).sum() * elt + 4 * len(ks) + ks.sum() * 4 + n * R * 8 + ks.sum() * R * 4)
+    flops = float(2 * (ks * ks).sum() * R)
+    # SpMV (FP64) timed alone too
     q = torch.empty_like(r)
     for _ in range(3):
-        mat.launch(r, q, 1, L.SPMV_PLAIN)
+        mat.launch(r, q, R, L.SPMV_PLAIN)
     torch.cuda.synchronize()
     kev[0].record()
     for _ in range(reps):
-        mat.launch(r, q, 1, L.SPMV_PLAIN)
+        mat.launch(r, q, R, L.SPMV_PLAIN)
     kev[1].record()
     torch.cuda.synchronize()
     s_ms = kev[0].elapsed_time(kev[1]) / reps
-    spmv_bytes = mat.nnz * 12 + (n + 1) * 4 + n * 16
+    spmv_bytes = mat.nnz * 12 + (n + 1) * 4 + n * R * 16
 
-    # batched right-hand sides through the tensor-core local apply
+    # batched right-hand sides through the tensor-core local apply (single-RHS workloads)
     batched = None
-    if args.batched:
+    if args.batched and R == 1:
         Rb = args.batched
         cgb = make(head, cal[head]["rtol"])
-        Bh = np.stack([rhs_for(n, rank, 100 + j) for j in range(Rb)], axis=1)
-        Bd = torch.as_tensor(Bh, device=dev)
+        Bd = torch.as_tensor(np.stack([rhs_for(n, rank, 100 + j, spec) for j in range(Rb)], axis=1), device=dev)
         Xb, mb = cgb.solve(Bd)  # warm-up (builds tile store, captures graphs)
         ebs = []
         for j in (0, Rb - 1):
@@ -357,7 +423,6 @@ def run_ours(args, rank: int, world: int):
         e1.record()
         torch.cuda.synchronize()
         bms = replicas.max_over_ranks(e0.elapsed_time(e1) / kb, dev)
-        # tensor-core kernel alone
         rb = torch.randn(n * Rb, dtype=torch.float64, device=dev)
         pcb = pcs[head]
         for _ in range(2):
@@ -387,31 +452,30 @@ def run_ours(args, rank: int, world: int):
         traffic = None
         tp = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tp):
-            tj = json.load(open(tp))
-            t = tj.get(f"local_apply_{head}")
-            if t and t.get("n_el") == args.n_el and t.get("parts") == args.parts:
+            t = json.load(open(tp)).get(f"{args.workload}_local_apply_{head}_r{R}")
+            if t:
                 traffic = t["bytes_per_launch"]
         f64_ms = per_prec["f64"]["ms_per_rhs"]
         if batched is not None:
             batched["speedup_vs_fp64_plain_per_rhs"] = f64_ms / batched["ms_per_rhs"]
+        kname = "ddx_schwarz_local_apply_tc" if tc else "ddx_schwarz_local_apply"
         out = {
-            "metric": "time per RHS to 1e-8 rel. error (mixed-precision Hybrid-Schwarz PCG), 1 B200",
+            "metric": "time per RHS to 1e-8 rel. error (mixed-precision Schwarz PCG), 1 B200",
             "value": ms_head / world,
             "unit": "ms/RHS",
             "n_gpus": world,
             "steps": steps,
             "warmup": warm,
-            "ms_per_step": ms_head,
+            "ms_per_step": ms_head * R,
             "higher_is_better": False,
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": f"{head} blocks / f32 accumulate / f64 PCG",
-            "data": "synthetic (seeded lognormal coefficient and uniform RHS)",
+            "data": "synthetic (seeded coefficient fields and right-hand sides)",
             "config": {
-                "workload": f"hybrid-schwarz q1-3d {args.n_el}^3 cells, {prob['nparts']} subdomains overlap 1, "
-                            f"q1 coarse {prob['R0'].shape[0]}, {head} blocks",
+                "workload": f"{args.workload}: {spec['name']}, {head} blocks",
                 "n_dofs": n, "subdomains": prob["nparts"], "k_max": int(ks.max()), "k_min": int(ks.min()),
-                "coarse_dofs": prob["R0"].shape[0], "rhs_per_step": 1, "rtol_used": cal[head]["rtol"],
+                "coarse_dofs": prob["R0"].shape[0], "rhs_per_step": R, "rtol_used": cal[head]["rtol"],
                 "l2": "inputs larger than L2 (local inverse blocks %.1f GB per apply)" % (alg_bytes / 1e9),
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             },
@@ -420,12 +484,14 @@ def run_ours(args, rank: int, world: int):
             "fp64_plain_ms_per_rhs": f64_ms,
             "speedup_vs_fp64_plain": f64_ms / ms_head,
             "per_precision": per_prec,
-            "e2e": {"value": ms_e2e / world, "unit": "ms/RHS", "h2d_bytes_per_step": n * 8, "d2h_bytes_per_step": n * 8},
-            "roofline": {"kernel": f"ddx_schwarz_local_apply ({head})", "bound": "hbm", "achieved": ach,
+            "e2e": {"value": ms_e2e / world, "unit": "ms/RHS", "h2d_bytes_per_step": n * R * 8,
+                    "d2h_bytes_per_step": n * R * 8},
+            "roofline": {"kernel": f"{kname} ({head}, R={R})", "bound": "hbm", "achieved": ach,
                          "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": ach / peaks["hbm_gbs"],
                          "traffic": traffic, "algorithmic_bytes": alg_bytes, "ms_per_launch": k_ms,
-                         "peak_source": peaks["source"]},
-            "spmv_roofline": {"kernel": "ddx_spmv_sell_f64", "achieved": spmv_bytes / (s_ms * 1e-3) / 1e9,
+                         "tflops": flops / (k_ms * 1e-3) / 1e12, "peak_source": peaks["source"]},
+            "spmv_roofline": {"kernel": "ddx_spmv_sell_f64" if R == 1 else "ddx_spmv_csr_f64",
+                              "achieved": spmv_bytes / (s_ms * 1e-3) / 1e9,
                               "frac": spmv_bytes / (s_ms * 1e-3) / 1e9 / peaks["hbm_gbs"], "ms_per_launch": s_ms,
                               "algorithmic_bytes": spmv_bytes},
             "gpu_launches": launches,
@@ -442,14 +508,14 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n-el", type=int, default=128)
-    ap.add_argument("--parts", type=int, default=16)
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="bf16", choices=["bf16", "f32", "f16"])
     ap.add_argument("--check-every", type=int, default=8)
     ap.add_argument("--replace-every", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batched", type=int, default=64, help="also time R right-hand sides per solve (0: skip)")
     args = ap.parse_args()
+    spec = WORKLOADS[args.workload]
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -457,18 +523,13 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        prob = build_problem(args.n_el, args.parts)
-        # iteration count of the FP64 method on this workload (measured on B200 by the GPU arm)
-        iters = int(os.environ.get("DDX_FP64_ITERATIONS", "0")) or 40
-        vals = []
-        for _ in range(max(1, args.steps)):
-            vals.append(cpu_time_per_rhs(prob, iters))
+        prob = build_problem(spec)
+        vals = [cpu_time_per_rhs(prob, spec["fp64_iterations"]) for _ in range(max(1, args.steps))]
         v = min(x["ms_per_rhs"] for x in vals)
-        line = {"metric": "time per RHS to 1e-8 rel. error (mixed-precision Hybrid-Schwarz PCG), 1 B200",
+        line = {"metric": "time per RHS to 1e-8 rel. error (mixed-precision Schwarz PCG), 1 B200",
                 "value": v, "unit": "ms/RHS", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "higher_is_better": False, "impl": "reference", "dtype": "f64",
-                "config": {"workload": f"hybrid-schwarz q1-3d {args.n_el}^3 cells, {prob['nparts']} subdomains "
-                                       f"overlap 1, q1 coarse {prob['R0'].shape[0]}, FP64 CPU restatement"},
+                "config": {"workload": f"{args.workload}: {spec['name']}, FP64 CPU restatement"},
                 "cpu_baseline": {"value": v, "unit": "ms/RHS", "cores": vals[0]["cores"], "kind": "port",
                                  "sample": vals[0]["sample"]},
                 "e2e": {"value": v, "unit": "ms/RHS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -481,7 +542,7 @@ def main():
 
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    out, prob, cal = run_ours(args, rank, world)
+    out, prob, cal = run_ours(args, spec, rank, world)
     if rank == 0:
         if not args.no_cpu_baseline:
             cb = cpu_time_per_rhs(prob, cal["f64"]["iterations"])

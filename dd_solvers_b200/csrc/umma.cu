@@ -28,6 +28,7 @@ constexpr int kStages = 4;
 constexpr int kTileBytes = kM * 128; // 16 KB
 constexpr int kThreads = 192;
 constexpr int kEpiThreads = 128;
+constexpr int kPanelSlack = 2048;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -200,7 +201,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc(Args a) {
   unsigned char* ring = smem;                                  // kStages x 16 KB
   unsigned char* bbuf = smem + kStages * kTileBytes;           // nK x (N x 128 B)
   const int nk_max = (a.kmax + kK - 1) / kK;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(bbuf + (size_t)nk_max * N * 128);
+  // 2 KiB of slack after the B panel keeps every operand read inside this CTA's shared memory
+  uint64_t* bars = reinterpret_cast<uint64_t*>(bbuf + (size_t)nk_max * N * 128 + kPanelSlack);
   uint64_t* a_full = bars;
   uint64_t* a_empty = bars + kStages;
   uint64_t* b_full = bars + 2 * kStages;
@@ -368,7 +370,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc(Args a) {
 template <typename T, int N>
 static int launch(const Args& a, cudaStream_t s) {
   const int nk_max = (a.kmax + kK - 1) / kK;
-  const size_t smem = 1024 + (size_t)kStages * kTileBytes + (size_t)nk_max * N * 128 + 16 * 8 + 64;
+  const size_t smem = 1024 + (size_t)kStages * kTileBytes + (size_t)nk_max * N * 128 + kPanelSlack + 16 * 8 + 64;
   if (smem > 227 * 1024) {
     set_error("ddx_schwarz_local_apply_tc: k=%d with R=%d needs %zu bytes of shared memory", a.kmax, N, smem);
     return DDX_ERR_UNSUPPORTED;

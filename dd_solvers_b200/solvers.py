@@ -439,7 +439,7 @@ class SchwarzOperator(SparseSolver):
         if R not in (16, 32, 64) or self.block_dtype not in (torch.bfloat16, torch.float16):
             return False
         nk = (self.kmax + so.UMMA_K - 1) // so.UMMA_K
-        return 1024 + 4 * 16384 + nk * R * 128 + 192 <= 227 * 1024
+        return 1024 + 4 * 16384 + nk * R * 128 + 2048 + 192 <= 227 * 1024
 
     def _tile_store(self):
         if getattr(self, "_tiles", None) is None:
