@@ -12,9 +12,14 @@ stopping tolerance is tightened until it is.
 
 Other workloads (--workload): c1 2D Q1 Poisson 256^2, 8x8 subdomains, additive
 Schwarz; c3 2D Q1 Poisson 1024^2, 32x32 subdomains, 64 right-hand sides per
-solve on the tensor cores; c5 jittered P1 on 2048^2 nodes, RCB into 2048 uneven
-subdomains, 16 right-hand sides per solve. For several right-hand sides a step
-is one solve of the whole block and the time is divided by their number.
+solve on the tensor cores; c4 the gradient of ||u - u_t||^2 for 2D Q1 diffusion
+on 512^2 cells with kappa = exp(Gaussian random field) (one step = forward
+solve + adjoint solve + element-gradient kernel, checked against central
+differences along 16 seeded directions); c5 jittered P1 on 2048^2 nodes, RCB
+into 2048 uneven subdomains, 16 right-hand sides per solve (block terms from
+--precision: BF16 uses two 16-bit residual terms, FP16 one). For several
+right-hand sides a step is one solve of the whole block and the time is
+divided by their number.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2]
 
@@ -55,6 +60,10 @@ WORKLOADS = {
     "c3": dict(kind="q1_2d", n_el=1024, parts=32, coarse="p0", method="hybrid", rhs="normal", R=64,
                fp64_iterations=40,
                name="hybrid-schwarz q1-2d poisson 1024^2 cells, 1024 subdomains overlap 1, p0 coarse, 64 rhs"),
+    "c4": dict(kind="grad", n_el=512, parts=16, coarse="p0", method="additive", rhs="ones", R=1,
+               fp64_iterations=2 * 155,
+               name="differentiable q1-2d 512^2 cells, kappa = exp(GRF l=0.1), f = 1, loss ||u - u_t||^2, "
+                    "adjoint PCG + element gradient, additive schwarz 256 subdomains overlap 1, p0 coarse"),
     "c5": dict(kind="p1", n_nodes=2048, parts=2048, coarse="p0", method="hybrid", rhs="normal", R=16,
                fp64_iterations=60,
                name="hybrid-schwarz p1 jittered 2048^2 nodes lognormal kappa, rcb 2048 subdomains overlap 1, "
@@ -74,7 +83,11 @@ def build_problem(spec: dict, seed: int = 0):
     from dd_solvers_b200 import partition, problems
 
     t0 = time.time()
-    if spec["kind"] == "q1_3d":
+    if spec["kind"] == "grad":
+        g = problems.gaussian_random_field(spec["n_el"], 0.1, seed=seed)
+        P = problems.q1_grid(2, spec["n_el"], np.exp(g))
+        owner, nparts = partition.box_owner(P.interior_shape, spec["parts"])
+    elif spec["kind"] == "q1_3d":
         P = problems.diffusion3d_lognormal(spec["n_el"], seed)
         owner, nparts = partition.box_owner(P.interior_shape, spec["parts"])
     elif spec["kind"] == "q1_2d":
@@ -226,6 +239,161 @@ def cpu_time_per_rhs(prob, iterations: int, sample_subdomains: int = 48, budget_
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+
+def run_grad(args, spec, rank: int, world: int):
+    """c4: time per gradient of L = ||u(kappa, f) - u_t||^2 w.r.t. (kappa, f).
+
+    One step = forward PCG solve + loss + backward (adjoint PCG solve, mass
+    scaling, element-gradient kernel), FP64 vectors, local blocks of the head
+    precision (FP64 for comparison). The gradient is checked against central
+    differences (h = 1e-6) along 16 seeded directions in (kappa, f).
+    """
+    import torch
+    import torch.distributed as dist
+
+    import dd_solvers_b200 as dd
+    from dd_solvers_b200 import _lib as L
+    from dd_solvers_b200 import problems, replicas
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    prob = build_problem(spec)
+    n_el = spec["n_el"]
+    op = dd.Q1Diffusion(2, n_el, dev)
+    n = op.n
+    kappa = torch.as_tensor(np.exp(problems.gaussian_random_field(n_el, 0.1, seed=0)), device=dev)
+    kappa_t = torch.as_tensor(np.exp(problems.gaussian_random_field(n_el, 0.1, seed=1)), device=dev)
+    f = torch.ones(n, dtype=torch.float64, device=dev)
+    head = args.precision
+    dts = {"f64": torch.float64, "bf16": torch.bfloat16, "f32": torch.float32, "f16": torch.float16}
+    t0 = time.time()
+    cgs = {}
+    for prec in ("f64", head):
+        cg = dd.CG(dd.AdditiveSchwarz(torch.float64, dd.Inv(dts[prec]), dd.CUDSS()), rtol=1e-10, maxiter=5000,
+                   check_every=args.check_every, flexible=(prec != "f64"))
+        cg.setup(op.matrix(kappa), subdomains=(prob["sub_ptr"], prob["sub_idx"]), owner=prob["owner"],
+                 block_size=1)
+        cgs[prec] = cg
+    torch.cuda.synchronize()
+    gpu_setup_s = time.time() - t0
+    with torch.no_grad():
+        ut = dd.DiffusionSolve.apply(kappa_t, f, op, cgs["f64"])
+
+    def grad_step(cg, k, ff):
+        k = k.detach().requires_grad_(True)
+        ff = ff.detach().requires_grad_(True)
+        u = dd.DiffusionSolve.apply(k, ff, op, cg)
+        loss = ((u - ut) ** 2).sum()
+        loss.backward()
+        return loss.detach(), k.grad, ff.grad
+
+    def timed(prec, k_steps, w, host=False, count=False):
+        cg = cgs[prec]
+        if host:
+            kh, fh = kappa.cpu().pin_memory(), f.cpu().pin_memory()
+            gkh = torch.empty_like(kh).pin_memory()
+            gfh = torch.empty_like(fh).pin_memory()
+            lh = torch.empty((), dtype=torch.float64).pin_memory()
+            kd, fd = torch.empty_like(kappa), torch.empty_like(f)
+        for _ in range(w):
+            grad_step(cg, kappa, f)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        if count:
+            L.CALLS[0] = 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(k_steps):
+            if host:
+                kd.copy_(kh, non_blocking=True)
+                fd.copy_(fh, non_blocking=True)
+                loss, gk, gf = grad_step(cg, kd, fd)
+                gkh.copy_(gk, non_blocking=True)
+                gfh.copy_(gf, non_blocking=True)
+                lh.copy_(loss, non_blocking=True)
+            else:
+                grad_step(cg, kappa, f)
+        e1.record()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        return replicas.max_over_ranks(e0.elapsed_time(e1) / k_steps, dev)
+
+    steps, warm = args.steps, args.warmup
+    clocks = Clocks(dev.index if dev.index is not None else 0)
+    clocks.start()
+    ms_head = timed(head, steps, warm, count=True)
+    clk = clocks.stop()
+    launches = L.CALLS[0]
+    ms_f64 = timed("f64", max(1, min(steps, 3)), 1)
+    ms_e2e = timed(head, steps, 1, host=True)
+
+    # gradient check: central differences along 16 seeded directions (tight solves)
+    cgc = cgs[head]
+    rtol_run = cgc.rtol
+    cgc.rtol = 1e-12
+    _, gk, gf = grad_step(cgc, kappa, f)
+    rng = np.random.default_rng(123)
+    h = 1e-6
+    worst = 0.0
+    with torch.no_grad():
+        for _ in range(16):
+            dk = torch.as_tensor(rng.standard_normal(kappa.shape), device=dev) * kappa
+            df = torch.as_tensor(rng.standard_normal(n), device=dev)
+            lp = float(((dd.DiffusionSolve.apply(kappa + h * dk, f + h * df, op, cgc) - ut) ** 2).sum())
+            lm = float(((dd.DiffusionSolve.apply(kappa - h * dk, f - h * df, op, cgc) - ut) ** 2).sum())
+            fd_ = (lp - lm) / (2 * h)
+            ad = float((gk * dk).sum() + (gf * df).sum())
+            worst = max(worst, abs(fd_ - ad) / max(abs(ad), 1e-30))
+    cgc.rtol = rtol_run
+    # gradient agreement between the head precision and FP64 blocks at the run tolerance
+    _, gk64, gf64 = grad_step(cgs["f64"], kappa, f)
+    _, gkh_, gfh_ = grad_step(cgs[head], kappa, f)
+    grad_rel = float(torch.linalg.norm(gkh_ - gk64) / torch.linalg.norm(gk64))
+
+    # dominant kernel: the element gradient + local apply are small here; report the local apply
+    pc = cgs[head].preconditioner
+    r = torch.randn(n, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        pc._local(r, 1)
+    kev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    kev[0].record()
+    for _ in range(20):
+        pc._local(r, 1)
+    kev[1].record()
+    torch.cuda.synchronize()
+    k_ms = kev[0].elapsed_time(kev[1]) / 20
+    ks = pc.ks.astype(np.int64)
+    elt = {"f64": 8, "f32": 4, "bf16": 2, "f16": 2}[head]
+    alg_bytes = int((ks * ks).sum() * elt + 4 * len(ks) + ks.sum() * 4 + n * 8 + ks.sum() * 4)
+    peaks = load_peaks()
+    out = None
+    if rank == 0:
+        ach = alg_bytes / (k_ms * 1e-3) / 1e9
+        out = {
+            "metric": "time per gradient (forward + adjoint Schwarz PCG to rtol 1e-10 + element gradient), 1 B200",
+            "value": ms_head / world, "unit": "ms/gradient", "n_gpus": world, "steps": steps, "warmup": warm,
+            "ms_per_step": ms_head, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": f"{head} blocks / f64 PCG", "data": "synthetic (seeded Gaussian random fields)",
+            "config": {"workload": f"{args.workload}: {spec['name']}, {head} blocks", "n_dofs": n,
+                       "subdomains": prob["nparts"], "k_max": int(ks.max()),
+                       "l2": "inputs smaller than L2; every step re-assembles A(kappa) and solves twice",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "fp64_blocks_ms_per_gradient": ms_f64, "speedup_vs_fp64_blocks": ms_f64 / ms_head,
+            "gradient_check": {"directions": 16, "h": h, "max_rel_err_fd_vs_adjoint": worst,
+                               "head_vs_fp64_blocks_grad_rel_diff": grad_rel},
+            "e2e": {"value": ms_e2e / world, "unit": "ms/gradient", "h2d_bytes_per_step": (kappa.numel() + n) * 8,
+                    "d2h_bytes_per_step": (kappa.numel() + n + 1) * 8},
+            "roofline": {"kernel": f"ddx_schwarz_local_apply ({head}, R=1)", "bound": "hbm", "achieved": ach,
+                         "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": ach / peaks["hbm_gbs"], "traffic": None,
+                         "algorithmic_bytes": alg_bytes, "ms_per_launch": k_ms, "peak_source": peaks["source"]},
+            "gpu_launches": launches, "clocks": clk,
+            "setup_s": {"host": prob["host_setup_s"], "gpu": gpu_setup_s},
+        }
+    return out, prob, {"f64": {"iterations": spec["fp64_iterations"]}}
+
 
 def run_ours(args, spec, rank: int, world: int):
     import torch
@@ -542,12 +710,13 @@ def main():
 
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    out, prob, cal = run_ours(args, spec, rank, world)
+    runner = run_grad if spec["kind"] == "grad" else run_ours
+    out, prob, cal = runner(args, spec, rank, world)
     if rank == 0:
         if not args.no_cpu_baseline:
             cb = cpu_time_per_rhs(prob, cal["f64"]["iterations"])
-            out["cpu_baseline"] = {"value": cb["ms_per_rhs"], "unit": "ms/RHS", "cores": cb["cores"], "kind": "port",
-                                   "sample": cb["sample"]}
+            out["cpu_baseline"] = {"value": cb["ms_per_rhs"], "unit": out["unit"], "cores": cb["cores"],
+                                   "kind": "port", "sample": cb["sample"]}
         print(json.dumps(out))
     if world > 1:
         dist.barrier()

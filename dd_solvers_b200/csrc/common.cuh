@@ -54,6 +54,22 @@ inline int red_grid(int64_t work_items) {
   return (int)g;
 }
 
+// Grid for a grid-stride kernel: at most the CTAs that are resident at once on
+// this device (SM count x occupancy of `kernel` at kThreads threads), at most
+// `cap`, at least 1, at most `need`.
+template <typename Kernel>
+inline int resident_grid(Kernel kernel, int64_t need, int64_t cap) {
+  int dev = 0, nsm = 1, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  int64_t g = (int64_t)per_sm * nsm;
+  if (g > cap) g = cap;
+  if (g > need) g = need;
+  return (int)(g < 1 ? 1 : g);
+}
+
 // ---------------------------------------------------------------------------
 // Value conversions
 // ---------------------------------------------------------------------------

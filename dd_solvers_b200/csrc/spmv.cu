@@ -15,8 +15,10 @@
 
 namespace ddx {
 
+// 4 CTAs per SM (64 registers): twice the loads in flight of the unbounded
+// 84-92-register build, without spills.
 template <int MODE>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
     k_spmv_sell(int64_t n, int64_t nslices, const int64_t* __restrict__ slice_ptr,
                 const int* __restrict__ slice_width, const int* __restrict__ cols,
                 const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y,
@@ -131,10 +133,10 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // CSR SpMM for R >= 2 right-hand sides: R/2 threads per row, each owning two
-// adjacent RHS columns (16-byte loads of x rows), entries walked four at a
-// time with independent loads. Column sums for the PCG epilogues are reduced
+// adjacent RHS columns (16-byte loads of x rows), entries walked in predicated
+// chunks of eight with independent loads. Column sums for the PCG epilogues are reduced
 // as even/odd halves and written in the standard partials layout.
-template <int MODE>
+template <int MODE, int kChunk = 8>
 __global__ void __launch_bounds__(kThreads)
     k_spmm_csr2(int64_t n, const int* __restrict__ row_ptr, const int* __restrict__ cols,
                 const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y,
@@ -149,24 +151,26 @@ __global__ void __launch_bounds__(kThreads)
   for (int64_t row = (int64_t)blockIdx.x * rpb + threadIdx.x / tpr; row < n; row += (int64_t)gridDim.x * rpb) {
     const int k0 = row_ptr[row], k1 = row_ptr[row + 1];
     double2 sum = make_double2(0.0, 0.0);
-    int k = k0;
-    for (; k + 4 <= k1; k += 4) {
-      const int cA = __ldg(cols + k), cB = __ldg(cols + k + 1), cC = __ldg(cols + k + 2), cD = __ldg(cols + k + 3);
-      const double vA = __ldg(vals + k), vB = __ldg(vals + k + 1), vC = __ldg(vals + k + 2), vD = __ldg(vals + k + 3);
-      const double2 xA = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cA * R) + c2);
-      const double2 xB = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cB * R) + c2);
-      const double2 xC = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cC * R) + c2);
-      const double2 xD = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cD * R) + c2);
-      sum.x = fma(vA, xA.x, sum.x); sum.y = fma(vA, xA.y, sum.y);
-      sum.x = fma(vB, xB.x, sum.x); sum.y = fma(vB, xB.y, sum.y);
-      sum.x = fma(vC, xC.x, sum.x); sum.y = fma(vC, xC.y, sum.y);
-      sum.x = fma(vD, xD.x, sum.x); sum.y = fma(vD, xD.y, sum.y);
-    }
-    for (; k < k1; ++k) {
-      const double v = __ldg(vals + k);
-      const double2 xv = __ldg(reinterpret_cast<const double2*>(x + (int64_t)__ldg(cols + k) * R) + c2);
-      sum.x = fma(v, xv.x, sum.x);
-      sum.y = fma(v, xv.y, sum.y);
+    // predicated chunks of kChunk entries: one round of column/value loads and
+    // one round of x loads per chunk (a 7- or 9-entry P1/Q1 row is one or two
+    // chunks), entries accumulated in CSR order
+    for (int k = k0; k < k1; k += kChunk) {
+      int c[kChunk];
+      double v[kChunk];
+#pragma unroll
+      for (int e = 0; e < kChunk; ++e) {
+        const bool ok = k + e < k1;
+        c[e] = ok ? __ldg(cols + k + e) : -1;
+        v[e] = ok ? __ldg(vals + k + e) : 0.0;
+      }
+#pragma unroll
+      for (int e = 0; e < kChunk; ++e) {
+        if (c[e] >= 0) {
+          const double2 xv = __ldg(reinterpret_cast<const double2*>(x + (int64_t)c[e] * R) + c2);
+          sum.x = fma(v[e], xv.x, sum.x);
+          sum.y = fma(v[e], xv.y, sum.y);
+        }
+      }
     }
     double2* yo = reinterpret_cast<double2*>(y + row * R) + c2;
     if (MODE == DDX_SPMV_PLAIN || MODE == DDX_SPMV_PQ) {
@@ -378,24 +382,25 @@ int ddx_spmv_csr_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols,
   if (R >= 2) {
     DDX_REQUIRE(((uintptr_t)x & 15u) == 0 && ((uintptr_t)y & 15u) == 0 && (b == nullptr || ((uintptr_t)b & 15u) == 0),
                 "ddx_spmv_csr_f64: x, y and b must be 16-byte aligned for R >= 2");
+    // grid-stride kernels at ~75 registers: one wave of resident CTAs
     const int rpb2 = kThreads / (R / 2);
     const int64_t need2 = ceil_div(n_rows, rpb2);
-    const int grid2 = (int)std::min<int64_t>(need2, kRedCtas);
     switch (mode) {
       case DDX_SPMV_PLAIN:
-        k_spmm_csr2<DDX_SPMV_PLAIN><<<(int)std::min<int64_t>(need2, 148 * 64), kThreads, 0, s>>>(
+        k_spmm_csr2<DDX_SPMV_PLAIN><<<resident_grid(k_spmm_csr2<DDX_SPMV_PLAIN>, need2, 1 << 20), kThreads, 0, s>>>(
             n_rows, row_ptr, cols, vals, x, y, b, S, partials, t);
         break;
       case DDX_SPMV_PQ:
-        k_spmm_csr2<DDX_SPMV_PQ><<<grid2, kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S, partials, t);
+        k_spmm_csr2<DDX_SPMV_PQ><<<resident_grid(k_spmm_csr2<DDX_SPMV_PQ>, need2, kRedCtas), kThreads, 0, s>>>(
+            n_rows, row_ptr, cols, vals, x, y, b, S, partials, t);
         break;
       case DDX_SPMV_RES_INIT:
-        k_spmm_csr2<DDX_SPMV_RES_INIT><<<grid2, kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S,
-                                                                  partials, t);
+        k_spmm_csr2<DDX_SPMV_RES_INIT><<<resident_grid(k_spmm_csr2<DDX_SPMV_RES_INIT>, need2, kRedCtas), kThreads,
+                                         0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S, partials, t);
         break;
       default:
-        k_spmm_csr2<DDX_SPMV_RES_REPLACE><<<grid2, kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S,
-                                                                     partials, t);
+        k_spmm_csr2<DDX_SPMV_RES_REPLACE><<<resident_grid(k_spmm_csr2<DDX_SPMV_RES_REPLACE>, need2, kRedCtas),
+                                            kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S, partials, t);
     }
     DDX_LAUNCH_CHECK("ddx_spmv_csr_f64");
     return DDX_OK;

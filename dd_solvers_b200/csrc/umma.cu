@@ -4,17 +4,31 @@
 // Y_i (k x R) = Q_i (k x k) * X_i (k x R), X_i = r[idx_i, :], i.e. a GEMM with
 // N = R, which the SIMT streaming kernel cannot feed at HBM speed. Layout per
 // persistent CTA (one per SM):
-//   warp 0      producer: streams 128x64 BF16/FP16 tiles of Q_i, stored in HBM
-//               already in the K-major 128-byte-swizzled UMMA layout, with one
-//               contiguous cp.async.bulk per tile into a 4-stage ring.
+//   warp 0      producer: per subdomain, the B panel X_i (written by
+//               ddx_pack_panels16 already gathered, converted to 16 bits and
+//               in the MN-major swizzled UMMA layout) with one cp.async.bulk
+//               per 64-row chunk into the resident panel buffer, then the
+//               128x64 BF16/FP16 tiles of Q_i, stored in HBM already in the
+//               K-major 128-byte-swizzled layout, one cp.async.bulk per tile
+//               into a 4-stage ring.
 //   warp 1      allocates TMEM; one lane issues tcgen05.mma (M=128, N=R, K=16)
-//               and tcgen05.commit to release ring stages / publish results.
-//   warps 2..5  gather X_i = r16[idx_i, :] (rows of r packed to 16 bits by
-//               ddx_pack_rhs16) with 16-byte cp.async copies into a resident
-//               MN-major swizzled B panel, then drain each 128-row accumulator
-//               from TMEM (tcgen05.ld), scale, and store ylocal (FP32).
+//               and tcgen05.commit to release ring stages / the panel and to
+//               publish results.
+//   warps 2..5  drain each 128-row accumulator from TMEM (tcgen05.ld), scale,
+//               and store ylocal (FP32).
 // Two TMEM accumulators (2 x R columns) let the epilogue of row tile m overlap
-// the MMAs of row tile m+1. Every wait is bounded (device error word).
+// the MMAs of row tile m+1. Every wait is bounded (device error word). No
+// thread of this kernel issues a dependent global load on the B path: the
+// gather through the subdomain index map happens in the pack kernel, where
+// every thread has its own independent loads in flight.
+//
+// Residual terms. Rounding r to 16 bits perturbs Q_i r by up to
+// cond(A_i) * 2^-p relative (p = 8 for BF16, 11 for FP16), which stalls PCG
+// once the local blocks are ill conditioned (high-contrast coefficients,
+// large 2D subdomains). With TERMS = 2 the pack writes r ~ hi + lo (hi the
+// 16-bit rounding of r, lo that of r - hi) as two panels, and each K step
+// issues one MMA per panel into the same accumulator: the product sees r to
+// ~2^-2p, the A stream (the HBM cost) is read once.
 #include <algorithm>
 
 #include "common.cuh"
@@ -76,7 +90,6 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
-__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 2, %0;" ::"n"(kEpiThreads) : "memory"); }
 
 // K-major, 128-byte swizzle shared-memory matrix descriptor (sm_100 format):
 // start address >> 4 in bits 0-13, leading byte offset (unused for swizzled
@@ -116,10 +129,6 @@ __host__ __device__ constexpr uint32_t idesc_f16(int ab_fmt, int N) {
          ((uint32_t)(kM >> 4) << 24);
 }
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
   asm volatile(
@@ -164,25 +173,36 @@ template <> __device__ __forceinline__ uint16_t to_bits<__nv_bfloat16>(double v)
 template <> __device__ __forceinline__ uint16_t to_bits<__half>(double v) {
   return __half_as_ushort(__float2half_rn((float)v));
 }
+template <typename T> __device__ __forceinline__ double from_bits(uint16_t b);
+template <> __device__ __forceinline__ double from_bits<__nv_bfloat16>(uint16_t b) {
+  return (double)__bfloat162float(__ushort_as_bfloat16(b));
+}
+template <> __device__ __forceinline__ double from_bits<__half>(uint16_t b) {
+  return (double)__half2float(__ushort_as_half(b));
+}
 
 struct Args {
   int n_sub;
   const int64_t* sub_ptr;
-  const int* sub_idx;
   const int* order;
   const int64_t* tile_off;  // bytes
   const unsigned char* tiles;
   const float* scale;
-  const uint16_t* r16;  // packed 16-bit rows of r (n, N), scaled per RHS
+  const unsigned char* b16;    // per-subdomain B panels (ddx_pack_panels16)
+  const int64_t* panel_off;    // bytes
   float* ylocal;
   const int* ist;
   const double* st;  // PCG state (||r_j||^2 scales the 16-bit conversion); may be null
   int kmax;
 };
 
-// Power-of-two scale that maps RHS j of r into [-1, 1] before the 16-bit
-// conversion (FP16 would flush small residual entries to zero otherwise),
-// from the PCG's current ||r_j||^2; 1 without PCG state.
+// Power-of-two scale applied to RHS j of r before the 16-bit conversion, from
+// the PCG's current ||r_j||^2 (1 without PCG state): ||s r_j|| lands in
+// [2^(top-1), 2^top) with top = 14 for FP16 (every entry stays below 2^14, far
+// from the FP16 maximum 65504, while entries down to ~2^-10 ||r_j|| keep full
+// precision instead of falling into FP16 subnormals) and top = 0 for BF16,
+// whose exponent range needs no help.
+template <typename T>
 __device__ __forceinline__ float rhs_scale(const double* st, int R, int j) {
   if (st == nullptr) return 1.0f;
   const double rr = st[DDX_ST_RR * R + j];
@@ -190,19 +210,21 @@ __device__ __forceinline__ float rhs_scale(const double* st, int R, int j) {
   int e;
   frexp(sqrt(rr), &e);  // sqrt(rr) in [2^(e-1), 2^e)
   e = max(-100, min(100, e));
-  return ldexpf(1.0f, -e);
+  constexpr int top = std::is_same<T, __half>::value ? 14 : 0;
+  return ldexpf(1.0f, top - e);
 }
 
-template <typename T, int N>
+template <typename T, int N, int TERMS>
 __global__ void __launch_bounds__(kThreads, 1) k_apply_tc(Args a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte alignment for the swizzled tiles
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* ring = smem;                                  // kStages x 16 KB
-  unsigned char* bbuf = smem + kStages * kTileBytes;           // nK x (N x 128 B)
+  unsigned char* bbuf = smem + kStages * kTileBytes;           // TERMS x nK x (N x 128 B)
   const int nk_max = (a.kmax + kK - 1) / kK;
-  // 2 KiB of slack after the B panel keeps every operand read inside this CTA's shared memory
-  uint64_t* bars = reinterpret_cast<uint64_t*>(bbuf + (size_t)nk_max * N * 128 + kPanelSlack);
+  const uint32_t panel_bytes = (uint32_t)nk_max * N * 128;    // a multiple of 1024: every panel is atom aligned
+  // 2 KiB of slack after the B panels keeps every operand read inside this CTA's shared memory
+  uint64_t* bars = reinterpret_cast<uint64_t*>(bbuf + (size_t)TERMS * panel_bytes + kPanelSlack);
   uint64_t* a_full = bars;
   uint64_t* a_empty = bars + kStages;
   uint64_t* b_full = bars + 2 * kStages;
@@ -231,7 +253,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc(Args a) {
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (threadIdx.x < N) rhs_unscale[threadIdx.x] = 1.0f / rhs_scale(a.st, N, threadIdx.x);
+  if (threadIdx.x < N) rhs_unscale[threadIdx.x] = 1.0f / rhs_scale<T>(a.st, N, threadIdx.x);
   constexpr uint32_t kCols = (2 * N < 32) ? 32 : 2 * N;  // power of two >= 32
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -247,12 +269,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc(Args a) {
   if (warp == 0) {
     // ------------------------------ producer ------------------------------
     if (lane == 0) {
-      uint32_t g = 0;
+      uint32_t g = 0, sub_n = 0;
       for (int w = blockIdx.x; w < a.n_sub && !abort_flag; w += gridDim.x) {
         const int i = a.order[w];
         const int k = (int)(a.sub_ptr[i + 1] - a.sub_ptr[i]);
         if (k == 0 || k > a.kmax) continue;
         const int nK = (k + kK - 1) / kK;
+        // B panel: the previous subdomain's MMAs must have finished reading it
+        if (!mbar_wait(b_empty, (sub_n & 1u) ^ 1u)) { abort_flag = 1; break; }
+        ++sub_n;
+        constexpr uint32_t chunk_bytes = (uint32_t)kK * 2u * N;  // 64 panel rows
+        const unsigned char* psrc = a.b16 + a.panel_off[i];
+        mbar_expect_tx(b_full, (uint32_t)TERMS * (uint32_t)nK * chunk_bytes);
+        for (int tt = 0; tt < TERMS; ++tt)
+          for (int t = 0; t < nK; ++t, psrc += chunk_bytes)
+            bulk_g2s(bbuf + (size_t)tt * panel_bytes + (size_t)t * chunk_bytes, psrc, chunk_bytes, b_full);
         const unsigned char* src = a.tiles + a.tile_off[i];
         for (int m0 = 0; m0 < k; m0 += kM) {
           const int rows = (min(kM, k - m0) + 7) / 8 * 8;
@@ -293,7 +324,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc(Args a) {
             const uint32_t sb = smem_u32(bbuf + (size_t)t * N * 128);
 #pragma unroll
             for (int kk = 0; kk < kK / 16; ++kk)
-              mma_f16(d, sw128_desc(sa + kk * 32), mn_desc<N>(sb + kk * 32 * N), idesc, (t > 0 || kk > 0) ? 1u : 0u);
+#pragma unroll
+              for (int tt = 0; tt < TERMS; ++tt)
+                mma_f16(d, sw128_desc(sa + kk * 32), mn_desc<N>(sb + tt * panel_bytes + kk * 32 * N), idesc,
+                        (t > 0 || kk > 0 || tt > 0) ? 1u : 0u);
             mma_commit(&a_empty[s]);
           }
           if (abort_flag) break;
@@ -305,10 +339,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc(Args a) {
       }
     }
   } else {
-    // ------------------------- gather + epilogue --------------------------
+    // ------------------------------ epilogue --------------------------------
     const int e = threadIdx.x - 64;   // 0..127
     const int quarter = warp & 3;     // TMEM lane quarter this warp may access
-    uint32_t acc_n = 0, sub_n = 0;
+    uint32_t acc_n = 0;
     for (int w = blockIdx.x; w < a.n_sub && !abort_flag; w += gridDim.x) {
       const int i = a.order[w];
       const int64_t p0 = a.sub_ptr[i];
@@ -318,24 +352,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc(Args a) {
         if (e == 0) atomicOr(&g_device_error, DEVERR_BAD_SIZE);
         continue;
       }
-      const int nK = (k + kK - 1) / kK;
-      // B buffer free once the MMAs of the previous subdomain completed
-      if (!mbar_wait(b_empty, (sub_n & 1u) ^ 1u)) { abort_flag = 1; break; }
-      // gather: panel row c = packed 16-bit row of DOF sub_idx[p0 + c] (2N bytes,
-      // N/8 chunks of 16 bytes, copied asynchronously); rows k..64 nK-1 are zero
-      constexpr int CPR = N / 8;
-      const int units = nK * kK * CPR;
-      for (int u = e; u < units; u += kEpiThreads) {
-        const int c = u / CPR, q = u % CPR;
-        unsigned char* dst = bbuf + mn_offset<N>(c, q);
-        if (c < k) cp_async16(dst, a.r16 + (int64_t)a.sub_idx[p0 + c] * N + q * 8);
-        else *reinterpret_cast<uint4*>(dst) = make_uint4(0u, 0u, 0u, 0u);
-      }
-      cp_async_wait_all();
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      epi_sync();
-      if (e == 0) mbar_arrive(b_full);
-      ++sub_n;
       // epilogue per 128-row tile
       const float sc = a.scale ? a.scale[i] : 1.0f;
       for (int m0 = 0; m0 < k; m0 += kM, ++acc_n) {
@@ -367,15 +383,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc(Args a) {
   }
 }
 
-template <typename T, int N>
+template <typename T, int N, int TERMS>
 static int launch(const Args& a, cudaStream_t s) {
   const int nk_max = (a.kmax + kK - 1) / kK;
-  const size_t smem = 1024 + (size_t)kStages * kTileBytes + (size_t)nk_max * N * 128 + kPanelSlack + 16 * 8 + 64;
+  const size_t smem =
+      1024 + (size_t)kStages * kTileBytes + (size_t)TERMS * nk_max * N * 128 + kPanelSlack + 16 * 8 + 64;
   if (smem > 227 * 1024) {
-    set_error("ddx_schwarz_local_apply_tc: k=%d with R=%d needs %zu bytes of shared memory", a.kmax, N, smem);
+    set_error("ddx_schwarz_local_apply_tc: k=%d with R=%d and %d residual terms needs %zu bytes of shared memory",
+              a.kmax, N, TERMS, smem);
     return DDX_ERR_UNSUPPORTED;
   }
-  auto kern = k_apply_tc<T, N>;
+  auto kern = k_apply_tc<T, N, TERMS>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
@@ -391,64 +409,124 @@ static int launch(const Args& a, cudaStream_t s) {
 
 using namespace ddx;
 
-extern "C" int ddx_schwarz_local_apply_tc(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
-                                          const int* order, const int64_t* tile_off, const void* tiles,
-                                          int block_dtype, const float* scale, int kmax, const void* r16,
-                                          float* ylocal, const int* ist, const double* st,
-                                          ddx_stream_t stream) {
+template <typename T, int TERMS>
+static int launch_r(int R, const umma::Args& a, cudaStream_t s) {
+  if (R == 16) return umma::launch<T, 16, TERMS>(a, s);
+  if (R == 32) return umma::launch<T, 32, TERMS>(a, s);
+  return umma::launch<T, 64, TERMS>(a, s);
+}
+
+extern "C" int ddx_schwarz_local_apply_tc(int n_sub, int R, const int64_t* sub_ptr, const int* order,
+                                          const int64_t* tile_off, const void* tiles, int block_dtype,
+                                          const float* scale, int kmax, const void* b16,
+                                          const int64_t* panel_off, int terms, float* ylocal, const int* ist,
+                                          const double* st, ddx_stream_t stream) {
   DDX_REQUIRE(R == 16 || R == 32 || R == 64, "ddx_schwarz_local_apply_tc: R must be 16, 32 or 64 (got %d)", R);
+  DDX_REQUIRE(terms == 1 || terms == 2, "ddx_schwarz_local_apply_tc: terms must be 1 or 2 (got %d)", terms);
   DDX_REQUIRE(n_sub >= 0 && kmax >= 0, "ddx_schwarz_local_apply_tc: bad sizes");
   if (n_sub == 0 || kmax == 0) return DDX_OK;
-  DDX_REQUIRE(sub_ptr && sub_idx && order && tile_off && tiles && r16 && ylocal,
+  DDX_REQUIRE(sub_ptr && order && tile_off && tiles && b16 && panel_off && ylocal,
               "ddx_schwarz_local_apply_tc: null pointer");
-  DDX_REQUIRE(((uintptr_t)tiles & 15u) == 0 && ((uintptr_t)ylocal & 15u) == 0 && ((uintptr_t)r16 & 15u) == 0,
-              "ddx_schwarz_local_apply_tc: tiles, r16 and ylocal must be 16-byte aligned");
-  umma::Args a{n_sub, sub_ptr, sub_idx, order, tile_off, (const unsigned char*)tiles, scale,
-               (const uint16_t*)r16, ylocal, ist, st, kmax};
+  DDX_REQUIRE(((uintptr_t)tiles & 15u) == 0 && ((uintptr_t)ylocal & 15u) == 0 && ((uintptr_t)b16 & 15u) == 0,
+              "ddx_schwarz_local_apply_tc: tiles, b16 and ylocal must be 16-byte aligned");
+  umma::Args a{n_sub, sub_ptr, order, tile_off, (const unsigned char*)tiles, scale,
+               (const unsigned char*)b16, panel_off, ylocal, ist, st, kmax};
   cudaStream_t s = (cudaStream_t)stream;
-  if (block_dtype == DDX_BF16) {
-    if (R == 16) return umma::launch<__nv_bfloat16, 16>(a, s);
-    if (R == 32) return umma::launch<__nv_bfloat16, 32>(a, s);
-    return umma::launch<__nv_bfloat16, 64>(a, s);
-  }
-  if (block_dtype == DDX_F16) {
-    if (R == 16) return umma::launch<__half, 16>(a, s);
-    if (R == 32) return umma::launch<__half, 32>(a, s);
-    return umma::launch<__half, 64>(a, s);
-  }
+  if (block_dtype == DDX_BF16)
+    return terms == 1 ? launch_r<__nv_bfloat16, 1>(R, a, s) : launch_r<__nv_bfloat16, 2>(R, a, s);
+  if (block_dtype == DDX_F16) return terms == 1 ? launch_r<__half, 1>(R, a, s) : launch_r<__half, 2>(R, a, s);
   set_error("ddx_schwarz_local_apply_tc: block dtype must be BF16 or F16");
   return DDX_ERR_ARG;
 }
 
 namespace ddx {
 namespace umma {
-// r16[i, j] = 16-bit(scale_j * r[i, j]) with the same per-RHS power-of-two
-// scale the tensor-core apply undoes (rhs_scale).
-template <typename T>
-__global__ void k_pack16(int64_t n, int R, const double* __restrict__ r, const double* __restrict__ st,
-                         uint16_t* __restrict__ out) {
-  const int64_t total = n * R;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const int j = threadIdx.x % R;  // stride is a multiple of R
-  const double sc = (double)rhs_scale(st, R, j);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) out[i] = to_bits<T>(sc * r[i]);
+// B panels of the tensor-core apply. Subdomain i (k rows, nK = ceil(k / 64)
+// chunks) occupies TERMS x nK x 64 x 2N bytes at panel_off[i], term-major;
+// within a term, panel row c (= DOF sub_idx[sub_ptr[i] + c]) holds its N
+// 16-bit values at the MN-major swizzled offsets mn_offset<N>(c, q) (q = 16-byte
+// chunk), the layout the UMMA B descriptor reads. Term 0 = 16-bit(s_j r[d, j]),
+// term 1 = 16-bit(s_j r[d, j] - term 0), s_j = rhs_scale<T>. Rows k..64 nK - 1
+// are never written (the caller zeroes them once). One CTA walks subdomains;
+// each thread converts one 16-byte chunk (8 RHS) of one row per step.
+template <typename T, int N, int TERMS>
+__global__ void __launch_bounds__(256) k_pack_panels(int n_sub, const int64_t* __restrict__ sub_ptr,
+                                                     const int* __restrict__ sub_idx,
+                                                     const int64_t* __restrict__ panel_off,
+                                                     const double* __restrict__ r, const double* __restrict__ st,
+                                                     unsigned char* __restrict__ out) {
+  __shared__ double sc[N];
+  if (threadIdx.x < N) sc[threadIdx.x] = (double)rhs_scale<T>(st, N, threadIdx.x);
+  __syncthreads();
+  constexpr int CPR = N / 8;  // 16-byte chunks per row
+  for (int i = blockIdx.x; i < n_sub; i += gridDim.x) {
+    const int64_t p0 = sub_ptr[i];
+    const int k = (int)(sub_ptr[i + 1] - p0);
+    const int nK = (k + kK - 1) / kK;
+    unsigned char* base = out + panel_off[i];
+    const size_t term_bytes = (size_t)nK * kK * 2 * N;
+    for (int u = threadIdx.x; u < k * CPR; u += blockDim.x) {
+      const int c = u / CPR, q = u % CPR;
+      const double2* src = reinterpret_cast<const double2*>(r + (int64_t)sub_idx[p0 + c] * N + q * 8);
+      double v[8];
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const double2 d = __ldg(src + h);
+        v[2 * h] = d.x * sc[q * 8 + 2 * h];
+        v[2 * h + 1] = d.y * sc[q * 8 + 2 * h + 1];
+      }
+      uint16_t hi[8];
+#pragma unroll
+      for (int h = 0; h < 8; ++h) hi[h] = to_bits<T>(v[h]);
+      const uint32_t off = mn_offset<N>(c, q);
+      *reinterpret_cast<uint4*>(base + off) =
+          make_uint4(hi[0] | ((uint32_t)hi[1] << 16), hi[2] | ((uint32_t)hi[3] << 16), hi[4] | ((uint32_t)hi[5] << 16),
+                     hi[6] | ((uint32_t)hi[7] << 16));
+      if (TERMS == 2) {
+        uint16_t lo[8];
+#pragma unroll
+        for (int h = 0; h < 8; ++h) lo[h] = to_bits<T>(v[h] - from_bits<T>(hi[h]));
+        *reinterpret_cast<uint4*>(base + term_bytes + off) =
+            make_uint4(lo[0] | ((uint32_t)lo[1] << 16), lo[2] | ((uint32_t)lo[3] << 16),
+                       lo[4] | ((uint32_t)lo[5] << 16), lo[6] | ((uint32_t)lo[7] << 16));
+      }
+    }
+  }
+}
+
+template <typename T, int TERMS>
+static void launch_pack(int N, int grid, cudaStream_t s, int n_sub, const int64_t* sub_ptr, const int* sub_idx,
+                        const int64_t* panel_off, const double* r, const double* st, unsigned char* out) {
+  if (N == 16) k_pack_panels<T, 16, TERMS><<<grid, 256, 0, s>>>(n_sub, sub_ptr, sub_idx, panel_off, r, st, out);
+  else if (N == 32) k_pack_panels<T, 32, TERMS><<<grid, 256, 0, s>>>(n_sub, sub_ptr, sub_idx, panel_off, r, st, out);
+  else k_pack_panels<T, 64, TERMS><<<grid, 256, 0, s>>>(n_sub, sub_ptr, sub_idx, panel_off, r, st, out);
 }
 }  // namespace umma
 }  // namespace ddx
 
-extern "C" int ddx_pack_rhs16(int64_t n, int R, const double* r, const double* st, void* r16, int dtype,
-                              ddx_stream_t stream) {
-  DDX_REQUIRE(valid_rhs_count(R), "ddx_pack_rhs16: unsupported R=%d", R);
-  DDX_REQUIRE(n >= 0 && r && r16, "ddx_pack_rhs16: bad arguments");
-  if (n == 0) return DDX_OK;
-  const int grid = (int)std::min<int64_t>(ceil_div(n * R, 256), 148 * 16);
+extern "C" int ddx_pack_panels16(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
+                                 const int64_t* panel_off, const double* r, const double* st, void* b16,
+                                 int dtype, int terms, ddx_stream_t stream) {
+  DDX_REQUIRE(R == 16 || R == 32 || R == 64, "ddx_pack_panels16: R must be 16, 32 or 64 (got %d)", R);
+  DDX_REQUIRE(terms == 1 || terms == 2, "ddx_pack_panels16: terms must be 1 or 2 (got %d)", terms);
+  DDX_REQUIRE(n_sub >= 0, "ddx_pack_panels16: bad sizes");
+  if (n_sub == 0) return DDX_OK;
+  DDX_REQUIRE(sub_ptr && sub_idx && panel_off && r && b16, "ddx_pack_panels16: null pointer");
+  DDX_REQUIRE(((uintptr_t)r & 15u) == 0 && ((uintptr_t)b16 & 15u) == 0,
+              "ddx_pack_panels16: r and b16 must be 16-byte aligned");
+  const int grid = std::min(n_sub, 148 * 8);
   cudaStream_t s = (cudaStream_t)stream;
-  if (dtype == DDX_BF16) umma::k_pack16<__nv_bfloat16><<<grid, 256, 0, s>>>(n, R, r, st, (uint16_t*)r16);
-  else if (dtype == DDX_F16) umma::k_pack16<__half><<<grid, 256, 0, s>>>(n, R, r, st, (uint16_t*)r16);
-  else {
-    set_error("ddx_pack_rhs16: dtype must be BF16 or F16");
+  unsigned char* o = (unsigned char*)b16;
+  if (dtype == DDX_BF16) {
+    if (terms == 1) umma::launch_pack<__nv_bfloat16, 1>(R, grid, s, n_sub, sub_ptr, sub_idx, panel_off, r, st, o);
+    else umma::launch_pack<__nv_bfloat16, 2>(R, grid, s, n_sub, sub_ptr, sub_idx, panel_off, r, st, o);
+  } else if (dtype == DDX_F16) {
+    if (terms == 1) umma::launch_pack<__half, 1>(R, grid, s, n_sub, sub_ptr, sub_idx, panel_off, r, st, o);
+    else umma::launch_pack<__half, 2>(R, grid, s, n_sub, sub_ptr, sub_idx, panel_off, r, st, o);
+  } else {
+    set_error("ddx_pack_panels16: dtype must be BF16 or F16");
     return DDX_ERR_ARG;
   }
-  DDX_LAUNCH_CHECK("ddx_pack_rhs16");
+  DDX_LAUNCH_CHECK("ddx_pack_panels16");
   return DDX_OK;
 }

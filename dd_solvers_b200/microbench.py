@@ -59,6 +59,7 @@ def bench_apply(args) -> dict:
     pc.setup(dd.csr_to_torch(A).to(dev), subdomains=(sub_ptr, sub_idx))
     R = args.rhs
     pc.use_tensor_cores = not args.simt
+    pc.rhs_terms = args.terms
     pc.autotune = args.tune
     tune = None
     if args.tune:
@@ -72,7 +73,7 @@ def bench_apply(args) -> dict:
     nbytes = int((ks * ks).sum() * ELT[args.precision] + 4 * len(ks) + ks.sum() * 4 + n * R * 8 + ks.sum() * R * acc)
     tc = pc._tc_ok(R) and pc.use_tensor_cores
     return {"kernel": "ddx_schwarz_local_apply_tc" if tc else "ddx_schwarz_local_apply", "precision": args.precision,
-            "rhs": R, "n_dofs": n, "subdomains": len(ks), "k_max": int(ks.max()), "ms_per_launch": ms,
+            "rhs": R, "rhs_terms": pc._tc_terms(R) if tc else None, "n_dofs": n, "subdomains": len(ks), "k_max": int(ks.max()), "ms_per_launch": ms,
             "algorithmic_bytes": nbytes, "achieved_gbs": nbytes / ms / 1e6, "frac_of_peak": nbytes / ms / 1e6 / _peak(),
             "tflops": 2.0 * float((ks * ks).sum()) * R / ms / 1e9, "config": pc._apply_config(R), "tune_ms": tune}
 
@@ -107,6 +108,8 @@ def main():
     ap.add_argument("--rhs", type=int, default=1)
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--simt", action="store_true", help="force the SIMT kernel for R >= 16")
+    ap.add_argument("--terms", type=int, default=None, choices=[1, 2],
+                    help="16-bit residual terms of the tensor-core apply (default: automatic)")
     ap.add_argument("--tune", action="store_true", help="run the autotuner first and report every candidate")
     args = ap.parse_args()
     out = bench_apply(args) if args.what == "apply" else bench_spmv(args)

@@ -267,6 +267,10 @@ class SchwarzOperator(SparseSolver):
         self._scratch = {}
         self._tiles = None
         self.use_tensor_cores = True
+        # 16-bit residual terms per tensor-core product (1 or 2; None = 2 for
+        # BF16 blocks when both panels fit in shared memory, else 1): BF16's
+        # 8-bit significand on r stalls PCG once cond(A_i) is large
+        self.rhs_terms = None
         self.autotune = True
 
     # -- setup -------------------------------------------------------------
@@ -434,12 +438,27 @@ class SchwarzOperator(SparseSolver):
     def local_bytes(self) -> int:
         return self.store.nbytes
 
-    def _tc_ok(self, R: int) -> bool:
-        """The tensor-core path: BF16/FP16 blocks, R in {16, 32, 64}, B panel in shared memory."""
-        if R not in (16, 32, 64) or self.block_dtype not in (torch.bfloat16, torch.float16):
-            return False
+    def _tc_fits(self, R: int, terms: int) -> bool:
         nk = (self.kmax + so.UMMA_K - 1) // so.UMMA_K
-        return 1024 + 4 * 16384 + nk * R * 128 + 2048 + 192 <= 227 * 1024
+        return 1024 + 4 * 16384 + terms * nk * R * 128 + 2048 + 192 <= 227 * 1024
+
+    def _tc_terms(self, R: int) -> int:
+        """Residual terms of the tensor-core path for R right-hand sides; 0 = not usable.
+
+        The path needs BF16/FP16 blocks, R in {16, 32, 64} and the B panels of
+        the largest subdomain in shared memory.
+        """
+        if R not in (16, 32, 64) or self.block_dtype not in (torch.bfloat16, torch.float16):
+            return 0
+        if self.rhs_terms is not None:
+            return self.rhs_terms if self._tc_fits(R, self.rhs_terms) else 0
+        if self.block_dtype == torch.bfloat16 and self._tc_fits(R, 2):
+            return 2
+        return 1 if self._tc_fits(R, 1) else 0
+
+    def _tc_ok(self, R: int) -> bool:
+        """The tensor-core path: BF16/FP16 blocks, R in {16, 32, 64}, B panels in shared memory."""
+        return self._tc_terms(R) > 0
 
     def _tile_store(self):
         if getattr(self, "_tiles", None) is None:
@@ -462,19 +481,35 @@ class SchwarzOperator(SparseSolver):
     def _local(self, r: torch.Tensor, R: int, ist: torch.Tensor | None = None,
                st: torch.Tensor | None = None) -> torch.Tensor:
         s = self.scratch(R)
-        if self._tc_ok(R) and self.use_tensor_cores:
+        terms = self._tc_terms(R) if self.use_tensor_cores else 0
+        if terms:
             t = self._tile_store()
-            if "r16" not in s:
-                s["r16"] = torch.empty(self.n * R, dtype=self.block_dtype, device=self.device)
+            b16, panel_off = self._panels(R, terms)
             code = L.DTYPE_CODE[self.block_dtype]
-            L.call("ddx_pack_rhs16", self.n, R, L.ptr(r), L.ptr(st), L.ptr(s["r16"]), code, L.stream_ptr())
-            L.call("ddx_schwarz_local_apply_tc", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
-                   L.ptr(self.order), L.ptr(t.tile_off), L.ptr(t.data), code, L.ptr(self.store.scale), self.kmax,
-                   L.ptr(s["r16"]), L.ptr(s["ylocal"]), L.ptr(ist), L.ptr(st), L.stream_ptr())
+            L.call("ddx_pack_panels16", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
+                   L.ptr(panel_off), L.ptr(r), L.ptr(st), L.ptr(b16), code, terms, L.stream_ptr())
+            L.call("ddx_schwarz_local_apply_tc", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.order),
+                   L.ptr(t.tile_off), L.ptr(t.data), code, L.ptr(self.store.scale), self.kmax, L.ptr(b16),
+                   L.ptr(panel_off), terms, L.ptr(s["ylocal"]), L.ptr(ist), L.ptr(st), L.stream_ptr())
             return s["ylocal"]
         cfg = self._apply_config(R)
         self._simt_apply(r, s["ylocal"], R, ist, *cfg)
         return s["ylocal"]
+
+    def _panels(self, R: int, terms: int):
+        """Zero-initialised B-panel buffer and per-subdomain byte offsets for the
+        tensor-core path: subdomain i takes terms * ceil(k_i / 64) * 64 * 2R bytes."""
+        key = ("panels", R, terms)
+        got = self._scratch.get(key)
+        if got is None:
+            nk = (self.ks.astype(np.int64) + so.UMMA_K - 1) // so.UMMA_K
+            sizes = terms * nk * so.UMMA_K * 2 * R
+            off = np.zeros(len(sizes) + 1, dtype=np.int64)
+            np.cumsum(sizes, out=off[1:])
+            b16 = torch.zeros(max(int(off[-1]), 16), dtype=torch.uint8, device=self.device)
+            got = (b16, torch.as_tensor(off[:-1], device=self.device))
+            self._scratch[key] = got
+        return got
 
     def _simt_apply(self, r, ylocal, R, ist, groups: int, stage_kb: int) -> None:
         L.call("ddx_schwarz_local_apply_ex", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),

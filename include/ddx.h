@@ -176,19 +176,33 @@ int ddx_schwarz_local_apply(int n_sub, int R, const int64_t* sub_ptr, const int*
  * tiles in the K-major 128-byte-swizzled shared-memory layout (row r of a tile
  * at byte 128 r, its 16-byte chunk c stored at chunk c ^ (r % 8)), row-tile
  * major, the last row tile truncated to a multiple of 8 rows, columns >= k
- * zero; subdomain i starts at byte tile_off[i]. r16 is r packed to the block
- * type by ddx_pack_rhs16 (same st). ylocal is FP32, (sum k_i, R). Needs
- * 66 KB + ceil(kmax / 64) * R * 128 bytes of shared memory (<= 227 KB). */
-int ddx_schwarz_local_apply_tc(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
-                               const int* order, const int64_t* tile_off, const void* tiles,
-                               int block_dtype, const float* scale, int kmax, const void* r16,
-                               float* ylocal, const int* ist, const double* st, ddx_stream_t stream);
-/* r16[i, j] = (dtype) (s_j * r[i, j]), dtype BF16 or F16, with s_j the power of
- * two near 1 / ||r_j|| taken from st (||r_j||^2 slot; 1 when st is NULL), so
- * residual entries stay in the 16-bit range as the solve converges; the
- * tensor-core apply divides s_j out again. */
-int ddx_pack_rhs16(int64_t n, int R, const double* r, const double* st, void* r16, int dtype,
-                   ddx_stream_t stream);
+ * zero; subdomain i starts at byte tile_off[i]. X_i comes from b16 at byte
+ * panel_off[i], written by ddx_pack_panels16 (same st, same terms). With
+ * terms = 2 every K step multiplies the tile by both residual terms into one
+ * FP32 accumulator, so the product sees r to about twice the 16-bit precision
+ * (needed when the local blocks are ill conditioned; the block stream is read
+ * once either way). ylocal is FP32, (sum k_i, R). Needs 66 KB + terms *
+ * ceil(kmax / 64) * R * 128 bytes of shared memory (<= 227 KB). */
+int ddx_schwarz_local_apply_tc(int n_sub, int R, const int64_t* sub_ptr, const int* order,
+                               const int64_t* tile_off, const void* tiles, int block_dtype,
+                               const float* scale, int kmax, const void* b16, const int64_t* panel_off,
+                               int terms, float* ylocal, const int* ist, const double* st,
+                               ddx_stream_t stream);
+/* Gathers and packs the tensor-core B panels X_i = r[idx_i, :] (r FP64, (n, R),
+ * R in {16, 32, 64}) to 16-bit dtype (BF16 or F16). Subdomain i (k_i DOFs,
+ * nK_i = ceil(k_i / 64)) occupies terms * nK_i * 64 * 2R bytes at byte
+ * panel_off[i] (16-byte aligned), term-major; within a term, panel row c is DOF
+ * sub_idx[sub_ptr[i] + c], its 16-byte chunk q (RHS 8q..8q+7) stored at byte
+ * c * 2R + 16 q with bits [4,7) XORed by bits [7,10) masked to the row width
+ * (the MN-major swizzle of the UMMA B operand). Term 0 = (dtype) (s_j r[d, j]);
+ * for terms = 2, term 1 = (dtype) (s_j r[d, j] - term 0). s_j is a power of two
+ * from st (||r_j||^2 slot; 1 when st is NULL) putting ||s_j r_j|| just below
+ * 2^14 for F16 and 1 for BF16, so residual entries stay in the normal 16-bit
+ * range as the solve converges; the tensor-core apply divides s_j out again.
+ * Rows k_i..64 nK_i - 1 are not written: zero them once. */
+int ddx_pack_panels16(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
+                      const int64_t* panel_off, const double* r, const double* st, void* b16,
+                      int dtype, int terms, ddx_stream_t stream);
 /* combine: z[d, j] = sum_{t in T(d)} ylocal[src[t], j]      (if ylocal)
  *                  + u[d, j]                                (if u)
  *                  + sign * sum_c P[d, c] yc[c, j]          (if p_ptr)

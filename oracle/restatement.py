@@ -66,6 +66,38 @@ def round_to(x: np.ndarray, dtype: str) -> np.ndarray:
     raise ValueError(dtype)
 
 
+def rhs_scale(norm: float, dtype: str) -> float:
+    """Per-RHS power-of-two scale of the 16-bit residual pack: ``norm * s`` in
+    ``[2**(top-1), 2**top)``, top 14 for FP16 and 0 for BF16 (1 for a zero or
+    non-finite norm)."""
+    if not (norm > 0.0) or not np.isfinite(norm):
+        return 1.0
+    e = int(np.frexp(norm)[1])
+    e = max(-100, min(100, e))
+    return float(2.0 ** ((14 if dtype == "f16" else 0) - e))
+
+
+def rhs_terms(r: np.ndarray, dtype: str, terms: int, scaled: bool = False) -> np.ndarray:
+    """The residual a tensor-core apply multiplies: ``sum_t h_t / s_j`` with
+    ``h_0 = round(s_j r_j)``, ``h_1 = round(s_j r_j - h_0)`` in ``dtype``.
+
+    ``scaled`` applies the per-RHS scale from ``||r_j||`` (what the solver's
+    pack does with PCG state); without it ``s_j = 1``. Columns are RHS.
+    """
+    r = np.asarray(r, dtype=np.float64)
+    r2 = r.reshape(r.shape[0], -1)
+    out = np.zeros_like(r2)
+    for j in range(r2.shape[1]):
+        s = rhs_scale(float(np.linalg.norm(r2[:, j])), dtype) if scaled else 1.0
+        v = r2[:, j] * s
+        acc = np.zeros_like(v)
+        for _ in range(terms):
+            h = round_to(v - acc, dtype)
+            acc = acc + h
+        out[:, j] = acc / s
+    return out.reshape(r.shape)
+
+
 # Exponent of the largest scaled magnitude: |Q| <= 2**TARGET_EXP.
 TARGET_EXP = {"f64": None, "f32": 0, "bf16": 0, "f16": 14}
 
