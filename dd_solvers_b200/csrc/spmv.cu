@@ -133,10 +133,10 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // CSR SpMM for R >= 2 right-hand sides: R/2 threads per row, each owning two
-// adjacent RHS columns (16-byte loads of x rows), entries walked in predicated
-// chunks of eight with independent loads. Column sums for the PCG epilogues are reduced
+// adjacent RHS columns (16-byte loads of x rows), entries walked four at a
+// time with independent loads. Column sums for the PCG epilogues are reduced
 // as even/odd halves and written in the standard partials layout.
-template <int MODE, int kChunk = 8>
+template <int MODE>
 __global__ void __launch_bounds__(kThreads)
     k_spmm_csr2(int64_t n, const int* __restrict__ row_ptr, const int* __restrict__ cols,
                 const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y,
@@ -151,26 +151,24 @@ __global__ void __launch_bounds__(kThreads)
   for (int64_t row = (int64_t)blockIdx.x * rpb + threadIdx.x / tpr; row < n; row += (int64_t)gridDim.x * rpb) {
     const int k0 = row_ptr[row], k1 = row_ptr[row + 1];
     double2 sum = make_double2(0.0, 0.0);
-    // predicated chunks of kChunk entries: one round of column/value loads and
-    // one round of x loads per chunk (a 7- or 9-entry P1/Q1 row is one or two
-    // chunks), entries accumulated in CSR order
-    for (int k = k0; k < k1; k += kChunk) {
-      int c[kChunk];
-      double v[kChunk];
-#pragma unroll
-      for (int e = 0; e < kChunk; ++e) {
-        const bool ok = k + e < k1;
-        c[e] = ok ? __ldg(cols + k + e) : -1;
-        v[e] = ok ? __ldg(vals + k + e) : 0.0;
-      }
-#pragma unroll
-      for (int e = 0; e < kChunk; ++e) {
-        if (c[e] >= 0) {
-          const double2 xv = __ldg(reinterpret_cast<const double2*>(x + (int64_t)c[e] * R) + c2);
-          sum.x = fma(v[e], xv.x, sum.x);
-          sum.y = fma(v[e], xv.y, sum.y);
-        }
-      }
+    int k = k0;
+    for (; k + 4 <= k1; k += 4) {
+      const int cA = __ldg(cols + k), cB = __ldg(cols + k + 1), cC = __ldg(cols + k + 2), cD = __ldg(cols + k + 3);
+      const double vA = __ldg(vals + k), vB = __ldg(vals + k + 1), vC = __ldg(vals + k + 2), vD = __ldg(vals + k + 3);
+      const double2 xA = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cA * R) + c2);
+      const double2 xB = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cB * R) + c2);
+      const double2 xC = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cC * R) + c2);
+      const double2 xD = __ldg(reinterpret_cast<const double2*>(x + (int64_t)cD * R) + c2);
+      sum.x = fma(vA, xA.x, sum.x); sum.y = fma(vA, xA.y, sum.y);
+      sum.x = fma(vB, xB.x, sum.x); sum.y = fma(vB, xB.y, sum.y);
+      sum.x = fma(vC, xC.x, sum.x); sum.y = fma(vC, xC.y, sum.y);
+      sum.x = fma(vD, xD.x, sum.x); sum.y = fma(vD, xD.y, sum.y);
+    }
+    for (; k < k1; ++k) {
+      const double v = __ldg(vals + k);
+      const double2 xv = __ldg(reinterpret_cast<const double2*>(x + (int64_t)__ldg(cols + k) * R) + c2);
+      sum.x = fma(v, xv.x, sum.x);
+      sum.y = fma(v, xv.y, sum.y);
     }
     double2* yo = reinterpret_cast<double2*>(y + row * R) + c2;
     if (MODE == DDX_SPMV_PLAIN || MODE == DDX_SPMV_PQ) {
@@ -382,7 +380,7 @@ int ddx_spmv_csr_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols,
   if (R >= 2) {
     DDX_REQUIRE(((uintptr_t)x & 15u) == 0 && ((uintptr_t)y & 15u) == 0 && (b == nullptr || ((uintptr_t)b & 15u) == 0),
                 "ddx_spmv_csr_f64: x, y and b must be 16-byte aligned for R >= 2");
-    // grid-stride kernels at ~75 registers: one wave of resident CTAs
+    // grid-stride kernels: one wave of resident CTAs
     const int rpb2 = kThreads / (R / 2);
     const int64_t need2 = ceil_div(n_rows, rpb2);
     switch (mode) {
