@@ -367,7 +367,7 @@ def run_grad(args, spec, rank: int, world: int):
     k_ms = kev[0].elapsed_time(kev[1]) / 20
     ks = pc.ks.astype(np.int64)
     elt = {"f64": 8, "f32": 4, "bf16": 2, "f16": 2}[head]
-    alg_bytes = int((ks * ks).sum() * elt + 4 * len(ks) + ks.sum() * 4 + n * 8 + ks.sum() * 4)
+    alg_bytes = int(pc.store.nbytes + 4 * len(ks) + ks.sum() * 4 + n * 8 + ks.sum() * 4)
     peaks = load_peaks()
     out = None
     if rank == 0:
@@ -554,7 +554,10 @@ def run_ours(args, spec, rank: int, world: int):
     ks = pc.ks.astype(np.int64)
     elt = {"f64": 8, "f32": 4, "bf16": 2, "f16": 2}[head]
     tc = pc._tc_ok(R) and pc.use_tensor_cores
-    alg_bytes = int((ks * ks).sum() * elt + 4 * len(ks) + ks.sum() * 4 + n * R * 8 + ks.sum() * R * 4)
+    # block bytes the kernel must stream: the full blocks for the tensor-core
+    # path, the stored (upper-triangle tile) bytes for the SIMT path
+    blk_bytes = int((ks * ks).sum() * elt) if tc else pc.store.nbytes
+    alg_bytes = int(blk_bytes + 4 * len(ks) + ks.sum() * 4 + n * R * 8 + ks.sum() * R * 4)
     flops = float(2 * (ks * ks).sum() * R)
     # SpMV (FP64) timed alone too
     q = torch.empty_like(r)

@@ -70,10 +70,11 @@ def bench_apply(args) -> dict:
     ks = pc.ks.astype(np.int64)
     n = A.shape[0]
     acc = 8 if pc.acc_dtype == torch.float64 else 4
-    nbytes = int((ks * ks).sum() * ELT[args.precision] + 4 * len(ks) + ks.sum() * 4 + n * R * 8 + ks.sum() * R * acc)
     tc = pc._tc_ok(R) and pc.use_tensor_cores
+    blk_bytes = int((ks * ks).sum() * ELT[args.precision]) if tc else pc.store.nbytes
+    nbytes = int(blk_bytes + 4 * len(ks) + ks.sum() * 4 + n * R * 8 + ks.sum() * R * acc)
     return {"kernel": "ddx_schwarz_local_apply_tc" if tc else "ddx_schwarz_local_apply", "precision": args.precision,
-            "rhs": R, "rhs_terms": pc._tc_terms(R) if tc else None, "n_dofs": n, "subdomains": len(ks), "k_max": int(ks.max()), "ms_per_launch": ms,
+            "rhs": R, "rhs_terms": pc._tc_terms(R) if tc else None, "layout": pc.store.layout, "n_dofs": n, "subdomains": len(ks), "k_max": int(ks.max()), "ms_per_launch": ms,
             "algorithmic_bytes": nbytes, "achieved_gbs": nbytes / ms / 1e6, "frac_of_peak": nbytes / ms / 1e6 / _peak(),
             "tflops": 2.0 * float((ks * ks).sum()) * R / ms / 1e9, "config": pc._apply_config(R), "tune_ms": tune}
 

@@ -148,15 +148,53 @@ def quantize(inv: torch.Tensor, scales: torch.Tensor, dtype: torch.dtype) -> tor
     return q.to(torch.float32).to(dtype)
 
 
-class BlockStore:
-    """Packed column-major inverse blocks of one precision."""
+SYM_T = 32  # edge of the symmetric-layout tiles
 
-    def __init__(self, ks: np.ndarray, dtype: torch.dtype, device):
+
+def sym_chunk_swizzle(r: torch.Tensor, elem_bytes: int) -> torch.Tensor:
+    """XOR applied to the 16-byte chunk index of tile row ``r`` in the
+    symmetric layout, so that eight consecutive rows read at the same chunk
+    hit eight different 16-byte bank groups (rows of 64 B for 16-bit types:
+    ``(r >> 1) & 3``; rows of 128/256 B for FP32/FP64: ``r & 7``)."""
+    return ((r >> 1) & 3) if elem_bytes == 2 else (r & 7)
+
+
+def sym_tile_index(elem_bytes: int, device) -> torch.Tensor:
+    """Storage position of element (r, c) of a 32 x 32 tile: row-major rows of
+    32 elements, 16-byte chunk ``c // V`` of row r stored at chunk
+    ``(c // V) ^ sym_chunk_swizzle(r)`` (V = 16 / elem_bytes elements)."""
+    V = 16 // elem_bytes
+    r = torch.arange(SYM_T, device=device)[:, None]
+    c = torch.arange(SYM_T, device=device)[None, :]
+    return (r * SYM_T + ((c // V) ^ sym_chunk_swizzle(r, elem_bytes)) * V + (c % V)).reshape(-1)
+
+
+class BlockStore:
+    """Inverse blocks of one precision, quantised with a per-block power-of-two scale.
+
+    ``layout="sym"`` (the default of the Schwarz operators): the FP64 inverse
+    is symmetrised, ``(B + B^T) / 2``, before rounding, so the stored ``Q`` is
+    exactly symmetric and only its upper-triangle 32 x 32 tiles are kept:
+    block i (k rows, ``nt = ceil(k / 32)``) holds the ``nt (nt + 1) / 2`` tiles
+    ``(I, J), I <= J`` in row-major order of (I, J), each 1024 elements in the
+    swizzled row-major layout of ``sym_tile_index``, zero beyond k, starting at
+    element ``blk_off[i]`` (16-byte aligned). About half the bytes of the full
+    block. ``layout="colmajor"``: the full block column-major with leading
+    dimension ``round_up(k, 16 B / element)``.
+    """
+
+    def __init__(self, ks: np.ndarray, dtype: torch.dtype, device, layout: str = "colmajor"):
+        assert layout in ("colmajor", "sym")
         self.dtype = dtype
+        self.layout = layout
         self.V = 16 // ELEM_BYTES[dtype]
         self.ks = ks.astype(np.int64)
         self.lds = ((self.ks + self.V - 1) // self.V) * self.V
-        sizes = self.ks * self.lds
+        if layout == "sym":
+            nt = (self.ks + SYM_T - 1) // SYM_T
+            sizes = nt * (nt + 1) // 2 * (SYM_T * SYM_T)
+        else:
+            sizes = self.ks * self.lds
         off = np.zeros(len(ks) + 1, dtype=np.int64)
         np.cumsum(sizes, out=off[1:])
         self.off_np = off
@@ -164,6 +202,7 @@ class BlockStore:
         self.data = torch.zeros(max(self.total, self.V), dtype=dtype, device=device)
         self.blk_off = torch.as_tensor(off[:-1], device=device)
         self.scale = torch.ones(len(ks), dtype=torch.float32, device=device)
+        self._sw = sym_tile_index(ELEM_BYTES[dtype], device) if layout == "sym" else None
 
     @property
     def nbytes(self) -> int:
@@ -172,9 +211,27 @@ class BlockStore:
     def put(self, first: int, inv: torch.Tensor) -> None:
         """Stores blocks ``first..first+B-1`` from a padded (B, kpad, kpad) FP64 batch."""
         B = inv.shape[0]
+        if self.layout == "sym":
+            inv = 0.5 * (inv + inv.transpose(1, 2))
         sc = block_scales(inv, self.dtype)
         q = quantize(inv, sc, self.dtype)
         self.scale[first:first + B] = sc
+        if self.layout == "sym":
+            for b in range(B):
+                i = first + b
+                k = int(self.ks[i])
+                if k == 0:
+                    continue
+                nt = (k + SYM_T - 1) // SYM_T
+                full = torch.zeros(nt * SYM_T, nt * SYM_T, dtype=self.dtype, device=q.device)
+                full[:k, :k] = q[b, :k, :k]
+                tiles = full.view(nt, SYM_T, nt, SYM_T).permute(0, 2, 1, 3)  # [I, J, r, c]
+                I, J = torch.triu_indices(nt, nt, device=q.device)
+                up = tiles[I, J].reshape(-1, SYM_T * SYM_T)
+                sw = torch.empty_like(up)
+                sw[:, self._sw] = up
+                self.data[self.off_np[i]:self.off_np[i + 1]] = sw.reshape(-1)
+            return
         qt = q.transpose(1, 2)  # column-major: row c of qt is column c of q
         for b in range(B):
             i = first + b
@@ -184,11 +241,25 @@ class BlockStore:
             dst = self.data[self.off_np[i]:self.off_np[i] + k * ld].view(k, ld)
             dst[:, :k] = qt[b, :k, :k]
 
-    def block(self, i: int) -> torch.Tensor:
-        """Dequantised FP64 block i (for tests)."""
-        k, ld = int(self.ks[i]), int(self.lds[i])
+    def dense_q(self, i: int) -> torch.Tensor:
+        """Stored (quantised, unscaled) block i as a dense [row, col] k x k tensor."""
+        k = int(self.ks[i])
+        if self.layout == "sym":
+            nt = (k + SYM_T - 1) // SYM_T
+            sw = self.data[self.off_np[i]:self.off_np[i + 1]].view(-1, SYM_T * SYM_T)
+            up = sw[:, self._sw].view(-1, SYM_T, SYM_T)
+            full = torch.zeros(nt, nt, SYM_T, SYM_T, dtype=self.dtype, device=self.data.device)
+            I, J = torch.triu_indices(nt, nt, device=self.data.device)
+            full[I, J] = up
+            full[J, I] = up.transpose(1, 2)
+            return full.permute(0, 2, 1, 3).reshape(nt * SYM_T, nt * SYM_T)[:k, :k]
+        ld = int(self.lds[i])
         d = self.data[self.off_np[i]:self.off_np[i] + k * ld].view(k, ld)[:, :k]
-        return d.transpose(0, 1).to(torch.float64) * float(self.scale[i])
+        return d.transpose(0, 1)
+
+    def block(self, i: int) -> torch.Tensor:
+        """Dequantised FP64 block i (for tests and requantisation)."""
+        return self.dense_q(i).to(torch.float64) * float(self.scale[i])
 
 
 UMMA_M = 128  # rows per tensor-core tile
@@ -221,8 +292,8 @@ class UmmaTileStore:
     ``tile_off[i]``. Tile ``(m, t)`` holds ``rows_m`` rows (``umma_tile_rows``)
     of 64 columns in the K-major 128-byte-swizzled shared-memory layout, so one
     contiguous bulk copy lands it ready for ``tcgen05.mma``. Columns ``>= k``
-    and padding rows are zero. Built from a column-major ``BlockStore`` of the
-    same type, so both hold identical values.
+    and padding rows are zero. Built from a ``BlockStore`` of the same type
+    (either layout), so both hold identical values.
     """
 
     def __init__(self, src: "BlockStore"):
@@ -248,10 +319,8 @@ class UmmaTileStore:
                 continue
             nK = (k + UMMA_K - 1) // UMMA_K
             rows = umma_tile_rows(k)
-            ld = int(src.lds[i])
-            colmaj = src.data[src.off_np[i]:src.off_np[i] + k * ld].view(k, ld)[:, :k]  # [col, row]
             full = torch.zeros(len(rows) * UMMA_M, nK * UMMA_K, dtype=src.dtype, device=dev)
-            full[:k, :k] = colmaj.transpose(0, 1)  # [row, col]
+            full[:k, :k] = src.dense_q(i)  # [row, col]
             tiles = full.view(len(rows), UMMA_M, nK, UMMA_K).permute(0, 2, 1, 3).reshape(len(rows), nK, -1)
             sw_tiles = torch.empty_like(tiles)
             sw_tiles[:, :, sw] = tiles

@@ -267,6 +267,10 @@ class SchwarzOperator(SparseSolver):
         self._scratch = {}
         self._tiles = None
         self.use_tensor_cores = True
+        # store the (symmetrised) inverse blocks as upper-triangle tiles when
+        # that takes fewer bytes than the full blocks (the SIMT apply then
+        # streams about half the bytes)
+        self.symmetric_blocks = True
         # 16-bit residual terms per tensor-core product (1 or 2; None = 2 for
         # BF16 blocks when both panels fit in shared memory, else 1): BF16's
         # 8-bit significand on r stalls PCG once cond(A_i) is large
@@ -351,7 +355,7 @@ class SchwarzOperator(SparseSolver):
         self.sub_idx = torch.as_tensor(sub_idx, device=dev)
         self.order = torch.as_tensor(np.argsort(-ks, kind="stable").astype(np.int32), device=dev)
         self.dof_ptr, self.dof_src = so.transpose_map(self.sub_idx, n)
-        self.store = so.BlockStore(ks, block_dtype, dev)
+        self.store = so.BlockStore(ks, block_dtype, dev, layout=self._layout(ks))
         crow = torch.as_tensor(A_sp.indptr.astype(np.int64), device=dev)
         col = torch.as_tensor(A_sp.indices.astype(np.int64), device=dev)
         val = torch.as_tensor(A_sp.data, device=dev)
@@ -408,7 +412,7 @@ class SchwarzOperator(SparseSolver):
         other.acc_dtype = self._acc_for(dtype)
         other._tiles = None
         other._scratch = {}
-        store = so.BlockStore(self.ks, dtype, self.device)
+        store = so.BlockStore(self.ks, dtype, self.device, layout=self.store.layout)
         N = self.n_solvers
         i = 0
         while i < N:
@@ -423,6 +427,15 @@ class SchwarzOperator(SparseSolver):
             i = j
         other.store = store
         return other
+
+    def _layout(self, ks: np.ndarray) -> str:
+        """Upper-triangle tiles when they take fewer elements than the full
+        column-major blocks (they pad k to a multiple of 32: small blocks stay full)."""
+        if not self.symmetric_blocks:
+            return "colmajor"
+        ks = ks.astype(np.int64)
+        nt = (ks + so.SYM_T - 1) // so.SYM_T
+        return "sym" if int((nt * (nt + 1) // 2).sum()) * so.SYM_T ** 2 < int((ks * ks).sum()) else "colmajor"
 
     # -- kernels -----------------------------------------------------------
     def _acc_for(self, block_dtype: torch.dtype) -> torch.dtype:
@@ -512,38 +525,51 @@ class SchwarzOperator(SparseSolver):
         return got
 
     def _simt_apply(self, r, ylocal, R, ist, groups: int, stage_kb: int) -> None:
-        L.call("ddx_schwarz_local_apply_ex", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
+        """SIMT local apply; ``groups`` is the consumer-group count of the full-block
+        kernel or the consumer-warp count of the upper-triangle-tile kernel."""
+        entry = "ddx_schwarz_local_apply_sym" if self.store.layout == "sym" else "ddx_schwarz_local_apply_ex"
+        L.call(entry, self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
                L.ptr(self.order), L.ptr(self.store.blk_off), L.ptr(self.store.data),
                L.DTYPE_CODE[self.block_dtype], L.ptr(self.store.scale), self.kmax, L.ptr(r),
                L.ptr(ylocal), L.DTYPE_CODE[self.acc_dtype], L.ptr(ist), groups, stage_kb, L.stream_ptr())
 
     # -- autotuner -------------------------------------------------------------
-    # (groups of consumer warps, KiB per shared-memory stage) candidates for the SIMT apply
+    # (consumer groups of 4 warps, KiB per shared-memory stage): full-block kernel;
+    # (consumer warps, KiB per stage): upper-triangle-tile kernel
     TUNE_CANDIDATES = [(g, kb) for g in (1, 2, 4) for kb in (12, 20, 32)]
+    TUNE_CANDIDATES_SYM = [(w, kb) for w in (4, 8, 16) for kb in (8, 16, 32)]
     _tuned: dict = {}
 
-    def _tune_key(self, R: int):
-        return (str(self.block_dtype), str(self.acc_dtype), R, self.kmax, self.n_solvers, int(self.store.total))
+    @property
+    def tune_candidates(self):
+        return self.TUNE_CANDIDATES_SYM if self.store.layout == "sym" else self.TUNE_CANDIDATES
+
+    def _tune_key(self):
+        # The SIMT apply runs one right-hand side per launch, so one
+        # configuration serves every R (which also keeps the summation order,
+        # hence the bits of each column, the same for every R).
+        return (str(self.block_dtype), str(self.acc_dtype), self.store.layout, self.kmax, self.n_solvers,
+                int(self.store.total))
 
     def _apply_config(self, R: int) -> tuple[int, int]:
         """Tuned (groups, stage KiB) for this operator; tunes on first eager use."""
-        key = self._tune_key(R)
-        cfg = SchwarzOperator._tuned.get(key)
+        cfg = SchwarzOperator._tuned.get(self._tune_key())
         if cfg is not None:
             return cfg
         if not self.autotune or torch.cuda.is_current_stream_capturing():
             return (0, 0)  # library defaults
-        return self.tune(R)
+        return self.tune()
 
     def tune(self, R: int = 1, reps: int = 3) -> tuple[int, int]:
         """Project autotuner: times every candidate configuration of the SIMT
         local apply on this operator's own blocks (CUDA events, after one
-        warm-up launch) and keeps the fastest; results are cached per
-        (precision, R, sizes) for the process."""
+        warm-up launch, ``R`` right-hand sides per launch) and keeps the
+        fastest; results are cached per (precision, layout, sizes) for the
+        process and used for every R."""
         s = self.scratch(R)
         r = torch.randn(self.n * R, dtype=torch.float64, device=self.device)
         best, best_ms, timings = (0, 0), float("inf"), {}
-        for g, kb in self.TUNE_CANDIDATES:
+        for g, kb in self.tune_candidates:
             try:
                 self._simt_apply(r, s["ylocal"], R, None, g, kb)
             except L.DDXError:
@@ -558,7 +584,7 @@ class SchwarzOperator(SparseSolver):
             timings[(g, kb)] = ms
             if ms < best_ms:
                 best, best_ms = (g, kb), ms
-        SchwarzOperator._tuned[self._tune_key(R)] = best
+        SchwarzOperator._tuned[self._tune_key()] = best
         self.tune_timings = timings
         return best
 

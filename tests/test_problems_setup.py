@@ -208,3 +208,38 @@ def test_solver_rejects_cpu_tensors():
     A = torch.eye(3, dtype=torch.float64).to_sparse_csr()
     with pytest.raises(_lib.DDXError):
         dd.CG(bsr_matmul=False).setup(A)
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32, torch.bfloat16, torch.float16])
+def test_blockstore_symmetric_tiles(dtype):
+    """Upper-triangle tile layout: round trip equals the full layout of the
+    symmetrised blocks, and each element sits where the kernel reads it."""
+    ks = np.array([5, 40, 0, 70, 64])
+    rng = np.random.default_rng(1)
+    inv = torch.zeros(len(ks), 80, 80, dtype=torch.float64)
+    for i, k in enumerate(ks):
+        m = rng.standard_normal((k, k))
+        inv[i, :k, :k] = torch.as_tensor(m + 0.3 * m.T) * 1e-3  # not symmetric: put symmetrises
+    sym = so.BlockStore(ks, dtype, "cpu", layout="sym")
+    sym.put(0, inv)
+    full = so.BlockStore(ks, dtype, "cpu")
+    full.put(0, 0.5 * (inv + inv.transpose(1, 2)))
+    V = 16 // so.ELEM_BYTES[dtype]
+    for i, k in enumerate(ks):
+        if k == 0:
+            continue
+        assert torch.equal(sym.block(i), full.block(i))
+        Q = sym.dense_q(i)
+        nt = (k + 31) // 32
+        tau = 0
+        for I in range(nt):
+            for J in range(I, nt):
+                base = int(sym.off_np[i]) + tau * 1024
+                for r, c in ((0, 0), (1, 9), (7, 31), (30, 17)):
+                    sw = ((r >> 1) & 3) if so.ELEM_BYTES[dtype] == 2 else (r & 7)
+                    pos = base + r * 32 + (((c // V) ^ sw) * V) + c % V
+                    gr, gc = I * 32 + r, J * 32 + c
+                    want = Q[gr, gc] if gr < k and gc < k else 0
+                    assert sym.data[pos] == want, (i, I, J, r, c)
+                tau += 1
+        assert int(sym.off_np[i + 1]) - int(sym.off_np[i]) == tau * 1024
