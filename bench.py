@@ -554,9 +554,14 @@ def run_ours(args, spec, rank: int, world: int):
     ks = pc.ks.astype(np.int64)
     elt = {"f64": 8, "f32": 4, "bf16": 2, "f16": 2}[head]
     tc = pc._tc_ok(R) and pc.use_tensor_cores
-    # block bytes the kernel must stream: the full blocks for the tensor-core
-    # path, the stored (upper-triangle tile) bytes for the SIMT path
-    blk_bytes = int((ks * ks).sum() * elt) if tc else pc.store.nbytes
+    # block bytes the kernel must stream: the full blocks (tensor-core path on
+    # full blocks) or the stored upper-triangle tiles (SIMT path, symmetric
+    # tensor-core path)
+    tcsym = tc and pc._tc_sym_ok(R, pc._tc_terms(R))
+    if tc:
+        blk_bytes = pc._tile_store(True).nbytes if tcsym else int((ks * ks).sum() * elt)
+    else:
+        blk_bytes = pc.store.nbytes
     alg_bytes = int(blk_bytes + 4 * len(ks) + ks.sum() * 4 + n * R * 8 + ks.sum() * R * 4)
     flops = float(2 * (ks * ks).sum() * R)
     # SpMV (FP64) timed alone too
@@ -605,13 +610,16 @@ def run_ours(args, spec, rank: int, world: int):
         kev[1].record()
         torch.cuda.synchronize()
         tc_ms = kev[0].elapsed_time(kev[1]) / reps
-        tiles = pcb._tile_store()
-        tc_bytes = int((ks * ks).sum() * elt + 4 * len(ks) + ks.sum() * 4 + n * Rb * 8 + ks.sum() * Rb * 4)
+        bsym = pcb._tc_sym_ok(Rb, pcb._tc_terms(Rb))
+        tiles = pcb._tile_store(bsym)
+        tc_blk = tiles.nbytes if bsym else int((ks * ks).sum() * elt)
+        tc_bytes = int(tc_blk + 4 * len(ks) + ks.sum() * 4 + n * Rb * 8 + ks.sum() * Rb * 4)
         tc_flops = float(2 * (ks * ks).sum() * Rb)
         batched = {"rhs": Rb, "ms_per_solve": bms, "ms_per_rhs": bms / Rb, "iterations": max(mb["iterations"]),
                    "rel_error_vs_fp64_checked_columns": ebs,
                    "speedup_vs_fp64_plain_per_rhs": None,
-                   "tc_kernel": {"name": "ddx_schwarz_local_apply_tc", "ms_per_launch": tc_ms,
+                   "tc_kernel": {"name": "ddx_schwarz_local_apply_tc_sym" if bsym else "ddx_schwarz_local_apply_tc",
+                                 "ms_per_launch": tc_ms,
                                  "algorithmic_bytes": tc_bytes, "tile_bytes": tiles.nbytes,
                                  "achieved_gbs": tc_bytes / (tc_ms * 1e-3) / 1e9,
                                  "achieved_tflops": tc_flops / (tc_ms * 1e-3) / 1e12}}
@@ -629,7 +637,8 @@ def run_ours(args, spec, rank: int, world: int):
         f64_ms = per_prec["f64"]["ms_per_rhs"]
         if batched is not None:
             batched["speedup_vs_fp64_plain_per_rhs"] = f64_ms / batched["ms_per_rhs"]
-        kname = "ddx_schwarz_local_apply_tc" if tc else "ddx_schwarz_local_apply"
+        kname = ("ddx_schwarz_local_apply_tc_sym" if tcsym else "ddx_schwarz_local_apply_tc") if tc else \
+            ("ddx_schwarz_local_apply_sym" if pc.store.layout == "sym" else "ddx_schwarz_local_apply")
         out = {
             "metric": "time per RHS to 1e-8 rel. error (mixed-precision Schwarz PCG), 1 B200",
             "value": ms_head / world,

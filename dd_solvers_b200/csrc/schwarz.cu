@@ -19,47 +19,84 @@ namespace ddx {
 // ---------------------------------------------------------------------------
 // combine
 // ---------------------------------------------------------------------------
+// R = 1: one DOF per thread and U DOFs in flight per step (index loads, the
+// first transpose-map entry, u and the prolongation of all U issued before
+// any store). Every combine kernel here sums an element in one fixed order:
+// the ylocal entries in ascending subdomain order, then u, then sign * (P yc).
 template <typename ACC>
 __global__ void __launch_bounds__(kThreads, 4)
-    k_combine(int64_t n, PcgState S, const int* __restrict__ dof_ptr, const int* __restrict__ dof_src,
-              const ACC* __restrict__ ylocal, const double* u, const int* __restrict__ p_ptr,
-              const int* __restrict__ p_col, const double* __restrict__ p_val,
-              const double* __restrict__ yc, double sign, double* z, int dots,
-              const double* __restrict__ r, const double* __restrict__ q, double* partials,
-              unsigned int* ticket) {
+    k_combine1(int64_t n, PcgState S, const int* __restrict__ dof_ptr, const int* __restrict__ dof_src,
+               const ACC* __restrict__ ylocal, const double* u, const int* __restrict__ p_ptr,
+               const int* __restrict__ p_col, const double* __restrict__ p_val,
+               const double* __restrict__ yc, double sign, double* z, int dots,
+               const double* __restrict__ r, const double* __restrict__ q, double* partials,
+               unsigned int* ticket) {
+  constexpr int U = 4;
   __shared__ double red[kThreads];
-  const int R = S.R;
-  if (S.ist != nullptr && n_active(S.ist, R) == 0) return;
-  const int64_t total = n * R;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  const int j = threadIdx.x % R;
+  if (S.ist != nullptr && n_active(S.ist, 1) == 0) return;
+  const int64_t pass = (int64_t)gridDim.x * blockDim.x;
   double acc[2] = {0.0, 0.0};
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
-    const int64_t d = e / R;
-    double v = 0.0;
+  for (int64_t d0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d0 < n; d0 += pass * U) {
+    int64_t d[U];
+    bool ok[U];
+    double v[U];
+#pragma unroll
+    for (int uu = 0; uu < U; ++uu) {
+      d[uu] = d0 + uu * pass;
+      ok[uu] = d[uu] < n;
+      v[uu] = 0.0;
+    }
     if (ylocal != nullptr) {
-      const int t0 = dof_ptr[d], t1 = dof_ptr[d + 1];
-      for (int t = t0; t < t1; ++t) v += (double)ylocal[(int64_t)dof_src[t] * R + j];
+      int t0[U], t1[U], s0[U];
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu) {
+        t0[uu] = ok[uu] ? __ldg(dof_ptr + d[uu]) : 0;
+        t1[uu] = ok[uu] ? __ldg(dof_ptr + d[uu] + 1) : 0;
+      }
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu) s0[uu] = t0[uu] < t1[uu] ? __ldg(dof_src + t0[uu]) : -1;
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu)
+        if (s0[uu] >= 0) v[uu] += (double)__ldg(ylocal + s0[uu]);
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu)
+        for (int t = t0[uu] + 1; t < t1[uu]; ++t) v[uu] += (double)__ldg(ylocal + __ldg(dof_src + t));
     }
-    if (u != nullptr) v += u[e];
+    if (u != nullptr) {
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu)
+        if (ok[uu]) v[uu] += u[d[uu]];
+    }
     if (p_ptr != nullptr) {
-      double c = 0.0;
-      const int k0 = p_ptr[d], k1 = p_ptr[d + 1];
-      for (int k = k0; k < k1; ++k) c = fma(p_val[k], yc[(int64_t)p_col[k] * R + j], c);
-      v = fma(sign, c, v);
+      int k0[U], k1[U];
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu) {
+        k0[uu] = ok[uu] ? __ldg(p_ptr + d[uu]) : 0;
+        k1[uu] = ok[uu] ? __ldg(p_ptr + d[uu] + 1) : 0;
+      }
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu) {
+        double c = 0.0;
+        for (int k = k0[uu]; k < k1[uu]; ++k) c = fma(__ldg(p_val + k), __ldg(yc + __ldg(p_col + k)), c);
+        if (ok[uu]) v[uu] = fma(sign, c, v[uu]);
+      }
     }
-    z[e] = v;
-    if (dots) {
-      acc[0] = fma(r[e], v, acc[0]);
-      if (q != nullptr) acc[1] = fma(v, q[e], acc[1]);
-    }
+#pragma unroll
+    for (int uu = 0; uu < U; ++uu)
+      if (ok[uu]) {
+        if (dots) {
+          acc[0] = fma(__ldg(r + d[uu]), v[uu], acc[0]);
+          if (q != nullptr) acc[1] = fma(v[uu], __ldg(q + d[uu]), acc[1]);
+        }
+        z[d[uu]] = v[uu];
+      }
   }
   if (!dots) return;
-  write_cta_partials<2>(acc, red, R, partials);
+  write_cta_partials<2>(acc, red, 1, partials);
   if (!last_cta_arrival(ticket)) return;
   double tot[2];
-  final_sums<2>(partials, R, red, tot, ticket);
-  if (threadIdx.x < R) fin_rz(S, threadIdx.x, tot[0], tot[1]);
+  final_sums<2>(partials, 1, red, tot, ticket);
+  if (threadIdx.x == 0) fin_rz(S, 0, tot[0], tot[1]);
 }
 
 template <typename ACC> __device__ __forceinline__ double2 load_pair(const ACC* p);
@@ -77,7 +114,8 @@ template <> __device__ __forceinline__ double2 load_pair<float>(const float* p) 
 // any store. (u may alias z, so a one-element loop cannot
 // start the next element's loads before the previous store: every element
 // then waits out a chain of three dependent loads.) Each element is summed in
-// the same order as k_combine, so z is bitwise the same.
+// the same order as in k_combine1, so every column of z has the bits of an
+// R = 1 combine.
 template <typename ACC>
 __global__ void __launch_bounds__(kThreads, 4)
     k_combine2(int64_t n, PcgState S, const int* __restrict__ dof_ptr, const int* __restrict__ dof_src,
@@ -308,7 +346,6 @@ int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src
   if (dots) DDX_REQUIRE(r && st && ist && partials && tickets, "ddx_schwarz_combine: dots need PCG state");
   PcgState S{st, ist, nullptr, R};
   cudaStream_t s = (cudaStream_t)stream;
-  const int grid = dots ? red_grid(n * R) : (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n * R, kThreads), 148 * 16));
   unsigned int* t = tickets ? tickets + 4 : nullptr;
   if (ylocal != nullptr && acc_dtype != DDX_F64 && acc_dtype != DDX_F32) {
     set_error("ddx_schwarz_combine: acc dtype %d", acc_dtype);
@@ -327,15 +364,14 @@ int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src
     else
       k_combine2<float><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const float*)ylocal, u, p_ptr,
                                                    p_col, p_val, yc, sign, z, dots, r, q, partials, t);
-  } else if (f64) {
-    k_combine<double><<<grid, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const double*)ylocal, u, p_ptr, p_col,
-                                                p_val, yc, sign, z, dots, r, q, partials, t);
-  } else if (acc_dtype == DDX_F32) {
-    k_combine<float><<<grid, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const float*)ylocal, u, p_ptr, p_col,
-                                               p_val, yc, sign, z, dots, r, q, partials, t);
   } else {
-    set_error("ddx_schwarz_combine: acc dtype %d", acc_dtype);
-    return DDX_ERR_ARG;
+    const int grid1 = red_grid(ceil_div(n, 4));
+    if (f64)
+      k_combine1<double><<<grid1, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const double*)ylocal, u, p_ptr,
+                                                    p_col, p_val, yc, sign, z, dots, r, q, partials, t);
+    else
+      k_combine1<float><<<grid1, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const float*)ylocal, u, p_ptr,
+                                                   p_col, p_val, yc, sign, z, dots, r, q, partials, t);
   }
   DDX_LAUNCH_CHECK("ddx_schwarz_combine");
   return DDX_OK;

@@ -44,6 +44,10 @@ constexpr int kThreads = 192;
 constexpr int kEpiThreads = 128;
 constexpr int kPanelSlack = 2048;
 
+// 64-row chunks per residual term of a subdomain's B panel in HBM: whole pairs
+// (128 rows), so the symmetric kernel's 128-row K steps stay inside the panel.
+__host__ __device__ __forceinline__ int panel_chunks(int k) { return 2 * ((k + 127) / 128); }
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
@@ -279,11 +283,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc(Args a) {
         if (!mbar_wait(b_empty, (sub_n & 1u) ^ 1u)) { abort_flag = 1; break; }
         ++sub_n;
         constexpr uint32_t chunk_bytes = (uint32_t)kK * 2u * N;  // 64 panel rows
-        const unsigned char* psrc = a.b16 + a.panel_off[i];
+        const int nKp = panel_chunks(k);                           // chunks per term in HBM
         mbar_expect_tx(b_full, (uint32_t)TERMS * (uint32_t)nK * chunk_bytes);
-        for (int tt = 0; tt < TERMS; ++tt)
+        for (int tt = 0; tt < TERMS; ++tt) {
+          const unsigned char* psrc = a.b16 + a.panel_off[i] + (size_t)tt * nKp * chunk_bytes;
           for (int t = 0; t < nK; ++t, psrc += chunk_bytes)
             bulk_g2s(bbuf + (size_t)tt * panel_bytes + (size_t)t * chunk_bytes, psrc, chunk_bytes, b_full);
+        }
         const unsigned char* src = a.tiles + a.tile_off[i];
         for (int m0 = 0; m0 < k; m0 += kM) {
           const int rows = (min(kM, k - m0) + 7) / 8 * 8;
@@ -404,6 +410,255 @@ static int launch(const Args& a, cudaStream_t s) {
   return DDX_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Symmetric blocks: upper-triangle 128 x 128 tiles
+// ---------------------------------------------------------------------------
+// Q_i (exactly symmetric) stored as its tiles (I, J), I <= J, of 128 x 128,
+// row-major order of (I, J), each as two 128 x 64 halves (columns 0-63, 64-127
+// of the tile) in the K-major 128-byte-swizzled layout of the full-block kernel,
+// zero beyond k: 32 KB per tile, one bulk copy per tile. Tile (I, J) serves
+//   D_I += T X_J   (A = the tile, K-major: rows along I, K along J) and, for I < J,
+//   D_J += T^T X_I (A = the same shared memory read MN-major: its 128-byte rows
+//                   run along J (M), its rows along I (K); the two halves are
+//                   M-atoms 16 KB apart (LBO), 8-row groups 1 KB apart (SBO)).
+// The swizzle is a function of the shared-memory address, so one layout serves
+// both readings. Every row-tile accumulator of a block lives in TMEM at once
+// (nt x N columns, nt = ceil(k / 128)); the epilogue drains them after the
+// block's last MMA.
+
+// MN-major 128-byte-swizzle descriptor: LBO = stride between 64-element
+// M-atoms, SBO = stride between 8-row K groups (1024 B), version 1, layout 2.
+__device__ __forceinline__ uint64_t sw128_mn_desc(uint32_t saddr, uint32_t lbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)(1024u >> 4) << 32) | ((uint64_t)1u << 46) | ((uint64_t)2u << 61);
+}
+
+// Instruction descriptor as idesc_f16 with A MN-major (bit 15).
+__host__ __device__ constexpr uint32_t idesc_f16_amn(int ab_fmt, int N) { return idesc_f16(ab_fmt, N) | (1u << 15); }
+
+constexpr int kSymTile = 128;
+constexpr int kSymTileBytes = kSymTile * kSymTile * 2;  // 32 KB
+constexpr int kHalfBytes = kSymTileBytes / 2;           // 16 KB
+
+template <typename T, int N, int TERMS, int STAGES>
+__global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* ring = smem;                                   // STAGES x 32 KB
+  unsigned char* bbuf = smem + (size_t)STAGES * kSymTileBytes;  // TERMS x panel
+  const int nt_max = (a.kmax + kSymTile - 1) / kSymTile;
+  const uint32_t panel_bytes = (uint32_t)panel_chunks(a.kmax) * N * 128;  // nt_max x 128 rows
+  uint64_t* bars = reinterpret_cast<uint64_t*>(bbuf + (size_t)TERMS * panel_bytes + kPanelSlack);
+  uint64_t* a_full = bars;
+  uint64_t* a_empty = bars + STAGES;
+  uint64_t* b_full = bars + 2 * STAGES;
+  uint64_t* b_empty = b_full + 1;
+  uint64_t* acc_full = b_full + 2;
+  uint64_t* acc_empty = b_full + 3;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(b_full + 4);
+  __shared__ int abort_flag_s;
+  volatile int& abort_flag = abort_flag_s;
+  __shared__ float rhs_unscale[64];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (a.ist != nullptr && n_active(a.ist, N) == 0) return;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&a_full[s], 1);
+      mbar_init(&a_empty[s], 1);
+    }
+    mbar_init(b_full, 1);
+    mbar_init(b_empty, 1);
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, kEpiThreads / 32);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (threadIdx.x < N) rhs_unscale[threadIdx.x] = 1.0f / rhs_scale<T>(a.st, N, threadIdx.x);
+  uint32_t cols = 32;
+  while (cols < (uint32_t)(nt_max * N)) cols <<= 1;  // power of two >= 32, <= 512 (checked at launch)
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------ producer ------------------------------
+    if (lane == 0) {
+      uint32_t g = 0, sub_n = 0;
+      for (int w = blockIdx.x; w < a.n_sub && !abort_flag; w += gridDim.x) {
+        const int i = a.order[w];
+        const int k = (int)(a.sub_ptr[i + 1] - a.sub_ptr[i]);
+        if (k == 0 || k > a.kmax) continue;
+        const int nKp = panel_chunks(k);  // all nt x 128 panel rows (zero beyond k)
+        const int nt = (k + kSymTile - 1) / kSymTile;
+        if (!mbar_wait(b_empty, (sub_n & 1u) ^ 1u)) { abort_flag = 1; break; }
+        ++sub_n;
+        constexpr uint32_t chunk_bytes = (uint32_t)kK * 2u * N;
+        const unsigned char* psrc = a.b16 + a.panel_off[i];
+        mbar_expect_tx(b_full, (uint32_t)TERMS * (uint32_t)nKp * chunk_bytes);
+        for (int tt = 0; tt < TERMS; ++tt)
+          for (int t = 0; t < nKp; ++t, psrc += chunk_bytes)
+            bulk_g2s(bbuf + (size_t)tt * panel_bytes + (size_t)t * chunk_bytes, psrc, chunk_bytes, b_full);
+        const unsigned char* src = a.tiles + a.tile_off[i];
+        const int ntiles = nt * (nt + 1) / 2;
+        for (int t = 0; t < ntiles; ++t, ++g) {
+          const int s = g % STAGES;
+          if (!mbar_wait(&a_empty[s], ((g / STAGES) & 1u) ^ 1u)) { abort_flag = 1; break; }
+          mbar_expect_tx(&a_full[s], (uint32_t)kSymTileBytes);
+          bulk_g2s(ring + (size_t)s * kSymTileBytes, src, (uint32_t)kSymTileBytes, &a_full[s]);
+          src += kSymTileBytes;
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------ MMA issuer -----------------------------
+    if (lane == 0) {
+      constexpr int fmt = std::is_same<T, __nv_bfloat16>::value ? 1 : 0;
+      constexpr uint32_t idesc_k = idesc_f16(fmt, N);
+      constexpr uint32_t idesc_mn = idesc_f16_amn(fmt, N);
+      uint32_t g = 0, sub_n = 0;
+      for (int w = blockIdx.x; w < a.n_sub && !abort_flag; w += gridDim.x) {
+        const int i = a.order[w];
+        const int k = (int)(a.sub_ptr[i + 1] - a.sub_ptr[i]);
+        if (k == 0 || k > a.kmax) continue;
+        const int nt = (k + kSymTile - 1) / kSymTile;
+        if (!mbar_wait(b_full, sub_n & 1u)) { abort_flag = 1; break; }
+        if (!mbar_wait(acc_empty, (sub_n & 1u) ^ 1u)) { abort_flag = 1; break; }
+        fence_after();
+        uint64_t touched = 0;  // row tiles whose accumulator already holds a partial sum
+        for (int I = 0; I < nt && !abort_flag; ++I) {
+          for (int J = I; J < nt; ++J, ++g) {
+            const int s = g % STAGES;
+            if (!mbar_wait(&a_full[s], (g / STAGES) & 1u)) { abort_flag = 1; break; }
+            fence_after();
+            const uint32_t sa = smem_u32(ring + (size_t)s * kSymTileBytes);
+            // D_I += T X_J: K runs over the 128 columns of J (two 64-column halves)
+            {
+              const uint32_t d = tmem + (uint32_t)(I * N);
+              const uint32_t acc0 = (touched >> I) & 1u;
+#pragma unroll
+              for (int kk = 0; kk < kSymTile / 16; ++kk) {
+                const uint32_t a_addr = sa + (uint32_t)(kk >> 2) * kHalfBytes + (uint32_t)(kk & 3) * 32u;
+                const int prow = J * kSymTile + kk * 16;  // panel row of this K step
+                const uint32_t sb = smem_u32(bbuf + (size_t)(prow / kK) * N * 128) + (uint32_t)(prow % kK) * 2u * N;
+#pragma unroll
+                for (int tt = 0; tt < TERMS; ++tt)
+                  mma_f16(d, sw128_desc(a_addr), mn_desc<N>(sb + tt * panel_bytes), idesc_k,
+                          (acc0 || kk > 0 || tt > 0) ? 1u : 0u);
+              }
+              touched |= 1ull << I;
+            }
+            // D_J += T^T X_I: K runs over the 128 rows of I (16 rows = 2 KB per step)
+            if (I != J) {
+              const uint32_t d = tmem + (uint32_t)(J * N);
+              const uint32_t acc0 = (touched >> J) & 1u;
+#pragma unroll
+              for (int kk = 0; kk < kSymTile / 16; ++kk) {
+                const uint32_t a_addr = sa + (uint32_t)kk * 2048u;
+                const int prow = I * kSymTile + kk * 16;
+                const uint32_t sb = smem_u32(bbuf + (size_t)(prow / kK) * N * 128) + (uint32_t)(prow % kK) * 2u * N;
+#pragma unroll
+                for (int tt = 0; tt < TERMS; ++tt)
+                  mma_f16(d, sw128_mn_desc(a_addr, (uint32_t)kHalfBytes), mn_desc<N>(sb + tt * panel_bytes), idesc_mn,
+                          (acc0 || kk > 0 || tt > 0) ? 1u : 0u);
+              }
+              touched |= 1ull << J;
+            }
+            mma_commit(&a_empty[s]);
+          }
+        }
+        if (abort_flag) break;
+        mma_commit(acc_full);
+        mma_commit(b_empty);
+        ++sub_n;
+      }
+    }
+  } else {
+    // ------------------------------ epilogue --------------------------------
+    const int e = threadIdx.x - 64;
+    const int quarter = warp & 3;
+    uint32_t sub_n = 0;
+    for (int w = blockIdx.x; w < a.n_sub && !abort_flag; w += gridDim.x) {
+      const int i = a.order[w];
+      const int64_t p0 = a.sub_ptr[i];
+      const int k = (int)(a.sub_ptr[i + 1] - p0);
+      if (k == 0) continue;
+      if (k > a.kmax) {
+        if (e == 0) atomicOr(&g_device_error, DEVERR_BAD_SIZE);
+        continue;
+      }
+      const int nt = (k + kSymTile - 1) / kSymTile;
+      if (!mbar_wait(acc_full, sub_n & 1u)) { abort_flag = 1; break; }
+      fence_after();
+      const float sc = a.scale ? a.scale[i] : 1.0f;
+      for (int m = 0; m < nt; ++m) {
+        float v[N];
+#pragma unroll
+        for (int c = 0; c < N; c += 16) tmem_ld16(tmem + (uint32_t)(m * N + c) + ((uint32_t)(quarter * 32) << 16), v + c);
+        const int row = m * kSymTile + quarter * 32 + lane;
+        if (row < k) {
+          float4* dst = reinterpret_cast<float4*>(a.ylocal + (p0 + row) * N);
+#pragma unroll
+          for (int c = 0; c < N; c += 4)
+            dst[c / 4] = make_float4(sc * rhs_unscale[c] * v[c], sc * rhs_unscale[c + 1] * v[c + 1],
+                                     sc * rhs_unscale[c + 2] * v[c + 2], sc * rhs_unscale[c + 3] * v[c + 3]);
+        }
+      }
+      fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acc_empty);
+      ++sub_n;
+    }
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols) : "memory");
+  }
+}
+
+template <typename T, int N, int TERMS>
+static int launch_sym(const Args& a, cudaStream_t s) {
+  const int nk_max = panel_chunks(a.kmax);
+  const int nt_max = (a.kmax + kSymTile - 1) / kSymTile;
+  if (nt_max * N > 512) {
+    set_error("ddx_schwarz_local_apply_tc_sym: %d row tiles x R=%d accumulators exceed 512 TMEM columns", nt_max, N);
+    return DDX_ERR_UNSUPPORTED;
+  }
+  const size_t fixed = 1024 + (size_t)TERMS * nk_max * N * 128 + kPanelSlack + 16 * 8 + 64;
+  // at least 120 KB of shared memory keeps one CTA per SM (its accumulators may take all 512 TMEM columns)
+  const size_t smem3 = std::max<size_t>(fixed + 3 * (size_t)kSymTileBytes, 120 * 1024);
+  const size_t smem2 = std::max<size_t>(fixed + 2 * (size_t)kSymTileBytes, 120 * 1024);
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::max(1, std::min(a.n_sub, nsm));
+  if (smem3 <= 227 * 1024) {
+    auto kern = k_apply_tc_sym<T, N, TERMS, 3>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
+    kern<<<grid, kThreads, smem3, s>>>(a);
+  } else if (smem2 <= 227 * 1024) {
+    auto kern = k_apply_tc_sym<T, N, TERMS, 2>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
+    kern<<<grid, kThreads, smem2, s>>>(a);
+  } else {
+    set_error("ddx_schwarz_local_apply_tc_sym: k=%d with R=%d and %d residual terms needs %zu bytes of shared memory",
+              a.kmax, N, TERMS, smem2);
+    return DDX_ERR_UNSUPPORTED;
+  }
+  DDX_LAUNCH_CHECK("ddx_schwarz_local_apply_tc_sym");
+  return DDX_OK;
+}
+
 }  // namespace umma
 }  // namespace ddx
 
@@ -439,14 +694,46 @@ extern "C" int ddx_schwarz_local_apply_tc(int n_sub, int R, const int64_t* sub_p
   return DDX_ERR_ARG;
 }
 
+template <typename T, int TERMS>
+static int launch_sym_r(int R, const umma::Args& a, cudaStream_t s) {
+  if (R == 16) return umma::launch_sym<T, 16, TERMS>(a, s);
+  if (R == 32) return umma::launch_sym<T, 32, TERMS>(a, s);
+  return umma::launch_sym<T, 64, TERMS>(a, s);
+}
+
+extern "C" int ddx_schwarz_local_apply_tc_sym(int n_sub, int R, const int64_t* sub_ptr, const int* order,
+                                              const int64_t* tile_off, const void* tiles, int block_dtype,
+                                              const float* scale, int kmax, const void* b16,
+                                              const int64_t* panel_off, int terms, float* ylocal, const int* ist,
+                                              const double* st, ddx_stream_t stream) {
+  DDX_REQUIRE(R == 16 || R == 32 || R == 64, "ddx_schwarz_local_apply_tc_sym: R must be 16, 32 or 64 (got %d)", R);
+  DDX_REQUIRE(terms == 1 || terms == 2, "ddx_schwarz_local_apply_tc_sym: terms must be 1 or 2 (got %d)", terms);
+  DDX_REQUIRE(n_sub >= 0 && kmax >= 0, "ddx_schwarz_local_apply_tc_sym: bad sizes");
+  if (n_sub == 0 || kmax == 0) return DDX_OK;
+  DDX_REQUIRE(sub_ptr && order && tile_off && tiles && b16 && panel_off && ylocal,
+              "ddx_schwarz_local_apply_tc_sym: null pointer");
+  DDX_REQUIRE(((uintptr_t)tiles & 15u) == 0 && ((uintptr_t)ylocal & 15u) == 0 && ((uintptr_t)b16 & 15u) == 0,
+              "ddx_schwarz_local_apply_tc_sym: tiles, b16 and ylocal must be 16-byte aligned");
+  umma::Args a{n_sub, sub_ptr, order, tile_off, (const unsigned char*)tiles, scale,
+               (const unsigned char*)b16, panel_off, ylocal, ist, st, kmax};
+  cudaStream_t s = (cudaStream_t)stream;
+  if (block_dtype == DDX_BF16)
+    return terms == 1 ? launch_sym_r<__nv_bfloat16, 1>(R, a, s) : launch_sym_r<__nv_bfloat16, 2>(R, a, s);
+  if (block_dtype == DDX_F16)
+    return terms == 1 ? launch_sym_r<__half, 1>(R, a, s) : launch_sym_r<__half, 2>(R, a, s);
+  set_error("ddx_schwarz_local_apply_tc_sym: block dtype must be BF16 or F16");
+  return DDX_ERR_ARG;
+}
+
 namespace ddx {
 namespace umma {
-// B panels of the tensor-core apply. Subdomain i (k rows, nK = ceil(k / 64)
-// chunks) occupies TERMS x nK x 64 x 2N bytes at panel_off[i], term-major;
+// B panels of the tensor-core apply. Subdomain i (k rows, nKp = panel_chunks(k)
+// = 2 ceil(k / 128) chunks of 64 rows) occupies TERMS x nKp x 64 x 2N bytes at
+// panel_off[i], term-major;
 // within a term, panel row c (= DOF sub_idx[sub_ptr[i] + c]) holds its N
 // 16-bit values at the MN-major swizzled offsets mn_offset<N>(c, q) (q = 16-byte
 // chunk), the layout the UMMA B descriptor reads. Term 0 = 16-bit(s_j r[d, j]),
-// term 1 = 16-bit(s_j r[d, j] - term 0), s_j = rhs_scale<T>. Rows k..64 nK - 1
+// term 1 = 16-bit(s_j r[d, j] - term 0), s_j = rhs_scale<T>. Rows k..64 nKp - 1
 // are never written (the caller zeroes them once). One CTA walks subdomains;
 // each thread converts one 16-byte chunk (8 RHS) of one row per step.
 template <typename T, int N, int TERMS>
@@ -462,9 +749,8 @@ __global__ void __launch_bounds__(256) k_pack_panels(int n_sub, const int64_t* _
   for (int i = blockIdx.x; i < n_sub; i += gridDim.x) {
     const int64_t p0 = sub_ptr[i];
     const int k = (int)(sub_ptr[i + 1] - p0);
-    const int nK = (k + kK - 1) / kK;
     unsigned char* base = out + panel_off[i];
-    const size_t term_bytes = (size_t)nK * kK * 2 * N;
+    const size_t term_bytes = (size_t)panel_chunks(k) * kK * 2 * N;
     for (int u = threadIdx.x; u < k * CPR; u += blockDim.x) {
       const int c = u / CPR, q = u % CPR;
       const double2* src = reinterpret_cast<const double2*>(r + (int64_t)sub_idx[p0 + c] * N + q * 8);

@@ -57,9 +57,11 @@ def bench_apply(args) -> dict:
     A, sub_ptr, sub_idx, R0 = _problem(args.n_el, args.parts)
     pc = dd.AdditiveSchwarz(torch.float64, dd.Inv(DT[args.precision]), None)
     pc.setup(dd.csr_to_torch(A).to(dev), subdomains=(sub_ptr, sub_idx))
+    torch.cuda.empty_cache()  # release setup temporaries: a profiler then saves/restores less device memory
     R = args.rhs
     pc.use_tensor_cores = not args.simt
     pc.rhs_terms = args.terms
+    pc.tc_symmetric = not args.tc_full
     pc.autotune = args.tune
     tune = None
     if args.tune:
@@ -71,9 +73,15 @@ def bench_apply(args) -> dict:
     n = A.shape[0]
     acc = 8 if pc.acc_dtype == torch.float64 else 4
     tc = pc._tc_ok(R) and pc.use_tensor_cores
-    blk_bytes = int((ks * ks).sum() * ELT[args.precision]) if tc else pc.store.nbytes
+    tcsym = tc and pc._tc_sym_ok(R, pc._tc_terms(R))
+    if tc:
+        blk_bytes = pc._tile_store(True).nbytes if tcsym else int((ks * ks).sum() * ELT[args.precision])
+    else:
+        blk_bytes = pc.store.nbytes
     nbytes = int(blk_bytes + 4 * len(ks) + ks.sum() * 4 + n * R * 8 + ks.sum() * R * acc)
-    return {"kernel": "ddx_schwarz_local_apply_tc" if tc else "ddx_schwarz_local_apply", "precision": args.precision,
+    kname = ("ddx_schwarz_local_apply_tc_sym" if tcsym else "ddx_schwarz_local_apply_tc") if tc else (
+        "ddx_schwarz_local_apply_sym" if pc.store.layout == "sym" else "ddx_schwarz_local_apply")
+    return {"kernel": kname, "precision": args.precision,
             "rhs": R, "rhs_terms": pc._tc_terms(R) if tc else None, "layout": pc.store.layout, "n_dofs": n, "subdomains": len(ks), "k_max": int(ks.max()), "ms_per_launch": ms,
             "algorithmic_bytes": nbytes, "achieved_gbs": nbytes / ms / 1e6, "frac_of_peak": nbytes / ms / 1e6 / _peak(),
             "tflops": 2.0 * float((ks * ks).sum()) * R / ms / 1e9, "config": pc._apply_config(R), "tune_ms": tune}
@@ -109,6 +117,7 @@ def main():
     ap.add_argument("--rhs", type=int, default=1)
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--simt", action="store_true", help="force the SIMT kernel for R >= 16")
+    ap.add_argument("--tc-full", action="store_true", help="tensor-core apply on full blocks (not the upper triangle)")
     ap.add_argument("--terms", type=int, default=None, choices=[1, 2],
                     help="16-bit residual terms of the tensor-core apply (default: automatic)")
     ap.add_argument("--tune", action="store_true", help="run the autotuner first and report every candidate")

@@ -336,6 +336,55 @@ class UmmaTileStore:
         return int(self.off_np[-1]) * 2
 
 
+class UmmaSymTileStore:
+    """16-bit symmetric inverse blocks as upper-triangle 128 x 128 tensor-core tiles.
+
+    Subdomain ``i`` (size ``k``, ``nt = ceil(k/128)``) holds its tiles ``(I, J),
+    I <= J`` in row-major order of (I, J) from byte ``tile_off[i]``; each tile
+    is two 128 x 64 halves (tile columns 0-63, then 64-127) in the K-major
+    128-byte-swizzled layout of ``UmmaTileStore``, zero beyond k: 32 KB per
+    tile, one bulk copy per tile. The tensor-core kernel uses each tile for
+    ``T X_J`` and ``T^T X_I``. Built from a ``BlockStore`` whose blocks are
+    exactly symmetric (``layout="sym"``).
+    """
+
+    TILE = 128
+
+    def __init__(self, src: "BlockStore"):
+        assert src.dtype in (torch.bfloat16, torch.float16) and src.layout == "sym"
+        dev = src.data.device
+        T = self.TILE
+        self.dtype = src.dtype
+        ks = src.ks
+        nt = (ks.astype(np.int64) + T - 1) // T
+        sizes = nt * (nt + 1) // 2 * T * T
+        off = np.zeros(len(ks) + 1, dtype=np.int64)
+        np.cumsum(sizes, out=off[1:])
+        self.off_np = off
+        self.data = torch.zeros(max(int(off[-1]), 8), dtype=src.dtype, device=dev)
+        self.tile_off = torch.as_tensor(off[:-1] * 2, device=dev)  # bytes
+        self.scale = src.scale
+        sw = swizzle128_index(dev)
+        for i, k in enumerate(ks):
+            k = int(k)
+            if k == 0:
+                continue
+            n = int(nt[i])
+            full = torch.zeros(n * T, n * T, dtype=src.dtype, device=dev)
+            full[:k, :k] = src.dense_q(i)
+            tiles = full.view(n, T, n, T).permute(0, 2, 1, 3)  # [I, J, r, c]
+            I, J = torch.triu_indices(n, n, device=dev)
+            up = tiles[I, J]  # (ntiles, 128, 128)
+            halves = up.view(-1, T, 2, UMMA_K).permute(0, 2, 1, 3).reshape(-1, 2, T * UMMA_K)  # [tile, half, r*64+c]
+            swz = torch.empty_like(halves)
+            swz[:, :, sw] = halves
+            self.data[off[i]:off[i + 1]] = swz.reshape(-1)
+
+    @property
+    def nbytes(self) -> int:
+        return int(self.off_np[-1]) * 2
+
+
 def invert_blocks(blocks: torch.Tensor, ks: torch.Tensor) -> torch.Tensor:
     """Inverse of each padded SPD block; padding rows/cols zeroed afterwards."""
     inv = torch.linalg.inv(blocks)

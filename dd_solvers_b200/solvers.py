@@ -275,6 +275,9 @@ class SchwarzOperator(SparseSolver):
         # BF16 blocks when both panels fit in shared memory, else 1): BF16's
         # 8-bit significand on r stalls PCG once cond(A_i) is large
         self.rhs_terms = None
+        # tensor-core apply on the upper-triangle 128 x 128 tiles when the
+        # blocks are stored symmetric and the accumulators fit in TMEM
+        self.tc_symmetric = True
         self.autotune = True
 
     # -- setup -------------------------------------------------------------
@@ -455,6 +458,16 @@ class SchwarzOperator(SparseSolver):
         nk = (self.kmax + so.UMMA_K - 1) // so.UMMA_K
         return 1024 + 4 * 16384 + terms * nk * R * 128 + 2048 + 192 <= 227 * 1024
 
+    def _tc_sym_ok(self, R: int, terms: int) -> bool:
+        """Symmetric tensor-core kernel: upper-triangle blocks, every row-tile
+        accumulator of the largest block in TMEM (ceil(kmax/128) R <= 512) and
+        two 32 KB tile stages plus the B panels in shared memory."""
+        if not self.tc_symmetric or self.store.layout != "sym":
+            return False
+        nt = (self.kmax + 127) // 128
+        panel = terms * 2 * nt * so.UMMA_K * R * 2
+        return nt * R <= 512 and 1024 + 2 * 32768 + panel + 2048 + 192 <= 227 * 1024
+
     def _tc_terms(self, R: int) -> int:
         """Residual terms of the tensor-core path for R right-hand sides; 0 = not usable.
 
@@ -473,10 +486,14 @@ class SchwarzOperator(SparseSolver):
         """The tensor-core path: BF16/FP16 blocks, R in {16, 32, 64}, B panels in shared memory."""
         return self._tc_terms(R) > 0
 
-    def _tile_store(self):
-        if getattr(self, "_tiles", None) is None:
-            self._tiles = so.UmmaTileStore(self.store)
-        return self._tiles
+    def _tile_store(self, sym: bool = False):
+        """Tensor-core tiles of the blocks (full, or upper-triangle for ``sym``), built on first use."""
+        tiles = getattr(self, "_tiles", None)
+        if tiles is None:
+            tiles = self._tiles = {}
+        if sym not in tiles:
+            tiles[sym] = so.UmmaSymTileStore(self.store) if sym else so.UmmaTileStore(self.store)
+        return tiles[sym]
 
     def scratch(self, R: int) -> dict:
         s = self._scratch.get(R)
@@ -496,14 +513,16 @@ class SchwarzOperator(SparseSolver):
         s = self.scratch(R)
         terms = self._tc_terms(R) if self.use_tensor_cores else 0
         if terms:
-            t = self._tile_store()
+            sym = self._tc_sym_ok(R, terms)
+            t = self._tile_store(sym)
             b16, panel_off = self._panels(R, terms)
             code = L.DTYPE_CODE[self.block_dtype]
             L.call("ddx_pack_panels16", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
                    L.ptr(panel_off), L.ptr(r), L.ptr(st), L.ptr(b16), code, terms, L.stream_ptr())
-            L.call("ddx_schwarz_local_apply_tc", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.order),
-                   L.ptr(t.tile_off), L.ptr(t.data), code, L.ptr(self.store.scale), self.kmax, L.ptr(b16),
-                   L.ptr(panel_off), terms, L.ptr(s["ylocal"]), L.ptr(ist), L.ptr(st), L.stream_ptr())
+            L.call("ddx_schwarz_local_apply_tc_sym" if sym else "ddx_schwarz_local_apply_tc", self.n_solvers, R,
+                   L.ptr(self.sub_ptr), L.ptr(self.order), L.ptr(t.tile_off), L.ptr(t.data), code,
+                   L.ptr(self.store.scale), self.kmax, L.ptr(b16), L.ptr(panel_off), terms, L.ptr(s["ylocal"]),
+                   L.ptr(ist), L.ptr(st), L.stream_ptr())
             return s["ylocal"]
         cfg = self._apply_config(R)
         self._simt_apply(r, s["ylocal"], R, ist, *cfg)
@@ -511,11 +530,11 @@ class SchwarzOperator(SparseSolver):
 
     def _panels(self, R: int, terms: int):
         """Zero-initialised B-panel buffer and per-subdomain byte offsets for the
-        tensor-core path: subdomain i takes terms * ceil(k_i / 64) * 64 * 2R bytes."""
+        tensor-core path: subdomain i takes terms * 2 ceil(k_i / 128) * 64 * 2R bytes."""
         key = ("panels", R, terms)
         got = self._scratch.get(key)
         if got is None:
-            nk = (self.ks.astype(np.int64) + so.UMMA_K - 1) // so.UMMA_K
+            nk = 2 * ((self.ks.astype(np.int64) + 127) // 128)  # whole 128-row pairs of 64-row chunks
             sizes = terms * nk * so.UMMA_K * 2 * R
             off = np.zeros(len(sizes) + 1, dtype=np.int64)
             np.cumsum(sizes, out=off[1:])

@@ -16,11 +16,12 @@ pytestmark = pytest.mark.gpu
 DT = {"bf16": torch.bfloat16, "f16": torch.float16}
 
 
+@pytest.mark.parametrize("variant", ["full", "sym"])
 @pytest.mark.parametrize("terms", [1, 2])
 @pytest.mark.parametrize("prec", ["bf16", "f16"])
 @pytest.mark.parametrize("R", [16, 32, 64])
 @pytest.mark.parametrize("case", ["q1_small", "q1_34sq", "p1_rcb"])
-def test_tc_local_apply_matches_oracle(cuda, prec, R, case, terms):
+def test_tc_local_apply_matches_oracle(cuda, prec, R, case, terms, variant):
     import dd_solvers_b200 as dd
     from oracle import restatement as orc
 
@@ -33,8 +34,11 @@ def test_tc_local_apply_matches_oracle(cuda, prec, R, case, terms):
     pc = dd.AdditiveSchwarz(torch.float64, dd.Inv(DT[prec]), dd.CUDSS())
     pc.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0)
     pc.rhs_terms = terms
+    pc.tc_symmetric = variant == "sym"
     if not pc._tc_ok(R):
         pytest.skip("subdomains too large for the shared-memory B panels at this R")
+    if variant == "sym" and not pc._tc_sym_ok(R, terms):
+        pytest.skip("accumulators of the largest block exceed TMEM, or full-block storage")
     rng = np.random.default_rng(R)
     r = rng.standard_normal((A.shape[0], R))
     rt = torch.as_tensor(r, device=cuda).contiguous()
@@ -130,3 +134,24 @@ def test_high_contrast_p1_tensor_cores_converge(cuda, prec):
         assert err.max() <= 1e-8, (p, err.max(), max(meta["iterations"]))
         its[p] = max(meta["iterations"])
     assert its[prec] <= 1.35 * its["f64"] + 2, its
+
+
+def test_tc_symmetric_equals_full_blocks(cuda):
+    """Symmetric-tile and full-block tensor-core kernels on the same blocks: same
+    product up to FP32 accumulation order, on uneven RCB subdomains (k not a
+    multiple of 128), in a multi-RHS PCG solve too."""
+    import dd_solvers_b200 as dd
+
+    P, A, owner, nparts, sub_ptr, sub_idx, R0 = p1_case(100, 8)
+    pc = dd.HybridSchwarz(torch.float64, dd.Inv(torch.float16), dd.CUDSS())
+    pc.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0)
+    assert pc._tc_sym_ok(16, 1) and int(pc.ks.max()) % 128 != 0
+    r = torch.randn(A.shape[0], 16, dtype=torch.float64, device=cuda)
+    ys = pc._local(r.view(-1), 16).clone()
+    pc.tc_symmetric = False
+    yf = pc._local(r.view(-1), 16).clone()
+    rel = float(torch.linalg.norm(ys - yf) / torch.linalg.norm(yf))
+    assert rel <= 1e-5, rel
+    from dd_solvers_b200 import _lib
+
+    assert _lib.device_error() == 0

@@ -243,3 +243,35 @@ def test_blockstore_symmetric_tiles(dtype):
                     assert sym.data[pos] == want, (i, I, J, r, c)
                 tau += 1
         assert int(sym.off_np[i + 1]) - int(sym.off_np[i]) == tau * 1024
+
+
+def test_umma_symmetric_tile_layout():
+    """Upper-triangle 128 x 128 tensor-core tiles: every element where the kernel reads it."""
+    ks = np.array([130, 0, 300])
+    rng = np.random.default_rng(2)
+    inv = torch.zeros(len(ks), 304, 304, dtype=torch.float64)
+    for i, k in enumerate(ks):
+        m = rng.standard_normal((k, k))
+        inv[i, :k, :k] = torch.as_tensor(m + m.T)
+    st = so.BlockStore(ks, torch.bfloat16, "cpu", layout="sym")
+    st.put(0, inv)
+    ut = so.UmmaSymTileStore(st)
+    data = ut.data
+    for i, k in enumerate(ks):
+        if k == 0:
+            continue
+        Q = st.dense_q(i)
+        nt = (k + 127) // 128
+        base = int(ut.off_np[i])
+        assert int(ut.tile_off[i]) == 2 * base
+        tau = 0
+        for I in range(nt):
+            for J in range(I, nt):
+                for r, c in ((0, 0), (5, 70), (127, 127), (64, 9), (3, 63)):
+                    h, cc = divmod(c, 64)
+                    pos = base + tau * 16384 + h * 8192 + r * 64 + ((cc // 8) ^ (r % 8)) * 8 + cc % 8
+                    gr, gc = I * 128 + r, J * 128 + c
+                    want = Q[gr, gc] if gr < k and gc < k else 0
+                    assert data[pos] == want, (i, I, J, r, c)
+                tau += 1
+        assert int(ut.off_np[i + 1]) - base == tau * 16384
