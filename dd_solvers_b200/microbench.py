@@ -3,6 +3,7 @@ experiments/benchmark_batched_gemv.py and experiments/benchmark_bsrmv.py).
 
     python -m dd_solvers_b200.microbench apply --n-el 64 --parts 8 --precision bf16 --rhs 1
     python -m dd_solvers_b200.microbench spmv --n-el 128 --rhs 1
+    python -m dd_solvers_b200.microbench spmv --problem p1 --n-el 2048 --rhs 16
 
 ``apply`` times the Schwarz local-inverse apply (SIMT streaming kernel for
 R < 16, tensor-core kernel for R in {16, 32, 64} with BF16/FP16 blocks) on the
@@ -95,7 +96,10 @@ def bench_spmv(args) -> dict:
     from . import problems
 
     dev = torch.device("cuda")
-    A = problems.diffusion3d_lognormal(args.n_el, 0).matrix
+    if args.problem == "p1":
+        A = problems.p1_jittered(args.n_el, 0.3, 1.0, 0).matrix  # n_el = nodes per side
+    else:
+        A = problems.diffusion3d_lognormal(args.n_el, 0).matrix
     M = _SellMatrix(dd.csr_to_torch(A).to(dev))
     R = args.rhs
     x = torch.randn(A.shape[0] * R, dtype=torch.float64, device=dev)
@@ -112,6 +116,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["apply", "spmv"])
     ap.add_argument("--n-el", type=int, default=64)
+    ap.add_argument("--problem", default="q1_3d", choices=["q1_3d", "p1"],
+                    help="spmv: 3D Q1 lognormal diffusion (n-el cells per side) or jittered P1 (n-el nodes per side)")
     ap.add_argument("--parts", type=int, default=8)
     ap.add_argument("--precision", default="bf16", choices=list(DT))
     ap.add_argument("--rhs", type=int, default=1)
