@@ -386,7 +386,8 @@ def run_grad(args, spec, rank: int, world: int):
                                "head_vs_fp64_blocks_grad_rel_diff": grad_rel},
             "e2e": {"value": ms_e2e / world, "unit": "ms/gradient", "h2d_bytes_per_step": (kappa.numel() + n) * 8,
                     "d2h_bytes_per_step": (kappa.numel() + n + 1) * 8},
-            "roofline": {"kernel": f"ddx_schwarz_local_apply ({head}, R=1)", "bound": "hbm", "achieved": ach,
+            "roofline": {"kernel": ("ddx_schwarz_local_apply_sym" if pc.store.layout == "sym" else
+                                    "ddx_schwarz_local_apply") + f" ({head}, R=1)", "bound": "hbm", "achieved": ach,
                          "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": ach / peaks["hbm_gbs"], "traffic": None,
                          "algorithmic_bytes": alg_bytes, "ms_per_launch": k_ms, "peak_source": peaks["source"]},
             "gpu_launches": launches, "clocks": clk,

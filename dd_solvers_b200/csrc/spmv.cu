@@ -276,46 +276,57 @@ __global__ void __launch_bounds__(kThreads)
 // BSR with column-major (bs x bs) blocks; one warp per block row. Lane l walks
 // the row's stored values e = l, l+32, ...; entry e of the block row is block
 // e / bs^2, column (e % bs^2) / bs, row e % bs.
+// BSR SpMV, row per lane: a warp covers G = floor(32 / BS) block rows, lane
+// (g, r) computes scalar row r of block row g:
+//   y[br BS + r] = sum_{blk in row br} sum_c vals[blk][c][r] * x[cols[blk] BS + c]
+// with column-major blocks, so the BS lanes of a block row read BS consecutive
+// values per column c (coalesced) and x[cols[blk] BS + c] is a broadcast; no
+// cross-lane reduction. The next block's column index is loaded ahead.
 template <typename T, int BS>
-__global__ void k_spmv_bsr(int64_t nbr, const int* __restrict__ row_ptr, const int* __restrict__ cols,
-                           const T* __restrict__ vals, const T* __restrict__ x, T* __restrict__ y) {
-  const int lane = threadIdx.x & 31;
-  const int64_t br = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (br >= nbr) return;
+__global__ void __launch_bounds__(256) k_spmv_bsr(int64_t nbr, const int* __restrict__ row_ptr,
+                                                  const int* __restrict__ cols, const T* __restrict__ vals,
+                                                  const T* __restrict__ x, T* __restrict__ y) {
+  constexpr int G = 32 / BS;
   constexpr int B2 = BS * BS;
-  T acc[BS];
+  const int lane = threadIdx.x & 31;
+  const int g = lane / BS, r = lane - g * BS;
+  const int64_t br = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * G + g;
+  if (g >= G || br >= nbr) return;
+  const int k0 = row_ptr[br], k1 = row_ptr[br + 1];
+  T acc0 = T(0), acc1 = T(0);
+  int col = k0 < k1 ? __ldg(cols + k0) : 0;
+  for (int k = k0; k < k1; ++k) {
+    const int next = k + 1 < k1 ? __ldg(cols + k + 1) : 0;
+    const T* vb = vals + (int64_t)k * B2 + r;
+    const T* xb = x + (int64_t)col * BS;
 #pragma unroll
-  for (int r = 0; r < BS; ++r) acc[r] = T(0);
-  const int64_t e0 = (int64_t)row_ptr[br] * B2, e1 = (int64_t)row_ptr[br + 1] * B2;
-  for (int64_t e = e0 + lane; e < e1; e += 32) {
-    const int64_t blk = e / B2;
-    const int w = (int)(e - blk * B2);
-    const int c = w / BS, r = w - c * BS;
-    const T v = vals[e] * x[(int64_t)cols[blk] * BS + c];
-#pragma unroll
-    for (int rr = 0; rr < BS; ++rr)
-      if (rr == r) acc[rr] += v;
+    for (int c = 0; c + 1 < BS; c += 2) {
+      acc0 = fma(__ldg(vb + c * BS), __ldg(xb + c), acc0);
+      acc1 = fma(__ldg(vb + (c + 1) * BS), __ldg(xb + c + 1), acc1);
+    }
+    if (BS & 1) acc0 = fma(__ldg(vb + (BS - 1) * BS), __ldg(xb + BS - 1), acc0);
+    col = next;
   }
-#pragma unroll
-  for (int r = 0; r < BS; ++r) {
-    T v = acc[r];
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-    if (lane == r) y[br * BS + r] = v;
-  }
+  y[br * BS + r] = acc0 + acc1;
 }
 
 template <typename T>
 static int launch_bsr(int64_t nbr, int bs, const int* rp, const int* ci, const T* v, const T* x, T* y,
                       cudaStream_t s) {
   const int wpb = 8;
-  const int grid = (int)ceil_div(nbr, wpb);
   switch (bs) {
-#define DDX_BSR_CASE(B) \
-  case B: k_spmv_bsr<T, B><<<grid, wpb * 32, 0, s>>>(nbr, rp, ci, v, x, y); break;
-    DDX_BSR_CASE(1) DDX_BSR_CASE(2) DDX_BSR_CASE(3) DDX_BSR_CASE(4)
-    DDX_BSR_CASE(5) DDX_BSR_CASE(6) DDX_BSR_CASE(7) DDX_BSR_CASE(8)
+#define DDX_BSR_CASE(B)                                                             \
+  case B: {                                                                         \
+    const int grid = (int)ceil_div(nbr, (int64_t)wpb * (32 / B));                  \
+    k_spmv_bsr<T, B><<<grid, wpb * 32, 0, s>>>(nbr, rp, ci, v, x, y);               \
+    break;                                                                          \
+  }
+    DDX_BSR_CASE(1) DDX_BSR_CASE(2) DDX_BSR_CASE(3) DDX_BSR_CASE(4) DDX_BSR_CASE(5) DDX_BSR_CASE(6)
+    DDX_BSR_CASE(7) DDX_BSR_CASE(8) DDX_BSR_CASE(9) DDX_BSR_CASE(10) DDX_BSR_CASE(11) DDX_BSR_CASE(12)
+    DDX_BSR_CASE(13) DDX_BSR_CASE(14) DDX_BSR_CASE(15) DDX_BSR_CASE(16) DDX_BSR_CASE(17) DDX_BSR_CASE(18)
+    DDX_BSR_CASE(19) DDX_BSR_CASE(20) DDX_BSR_CASE(21) DDX_BSR_CASE(22) DDX_BSR_CASE(23) DDX_BSR_CASE(24)
 #undef DDX_BSR_CASE
-    default: set_error("ddx_spmv_bsr: block size %d not in 1..8", bs); return DDX_ERR_UNSUPPORTED;
+    default: set_error("ddx_spmv_bsr: block size %d not in 1..24", bs); return DDX_ERR_UNSUPPORTED;
   }
   DDX_LAUNCH_CHECK("ddx_spmv_bsr");
   return DDX_OK;

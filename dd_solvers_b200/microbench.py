@@ -4,6 +4,7 @@ experiments/benchmark_batched_gemv.py and experiments/benchmark_bsrmv.py).
     python -m dd_solvers_b200.microbench apply --n-el 64 --parts 8 --precision bf16 --rhs 1
     python -m dd_solvers_b200.microbench spmv --n-el 128 --rhs 1
     python -m dd_solvers_b200.microbench spmv --problem p1 --n-el 2048 --rhs 16
+    python -m dd_solvers_b200.microbench bsr --n-el 2048 --p 1
 
 ``apply`` times the Schwarz local-inverse apply (SIMT streaming kernel for
 R < 16, tensor-core kernel for R in {16, 32, 64} with BF16/FP16 blocks) on the
@@ -112,9 +113,34 @@ def bench_spmv(args) -> dict:
             "frac_of_peak": nbytes / ms / 1e6 / _peak()}
 
 
+def bench_bsr(args) -> dict:
+    """BSR SpMV on the DG block structure of the reference's BSR benchmark
+    (2D: the 2 n^2 triangles of an n x n grid, P_p elements), FP64 values."""
+    from dd_solvers_b200 import FastBSR, problems
+
+    dev = torch.device("cuda")
+    bs = problems.dg_block_size(2, args.p)
+    crow, col = problems.dg_bsr_pattern_2d(args.n_el)
+    nbr, nnzb = len(crow) - 1, int(crow[-1])
+    g = torch.Generator(device=dev).manual_seed(0)
+    vals = torch.randn(nnzb, bs, bs, dtype=torch.float64, device=dev, generator=g)
+    m = torch.sparse_bsr_tensor(torch.as_tensor(crow, device=dev), torch.as_tensor(col, device=dev), vals,
+                                size=(nbr * bs, nbr * bs))
+    A = FastBSR(m)
+    del m, vals
+    torch.cuda.empty_cache()
+    x = torch.randn(nbr * bs, dtype=torch.float64, device=dev, generator=g)
+    ms = _time(lambda: A @ x, args.reps)
+    nbytes = nnzb * (bs * bs * 8 + 4) + (nbr + 1) * 4 + 2 * nbr * bs * 8
+    return {"kernel": "ddx_spmv_bsr", "dim": 2, "p": args.p, "bs": bs, "dofs": nbr * bs, "bsr_nnz": nnzb,
+            "ms_per_launch": ms, "algorithmic_bytes": nbytes, "achieved_gbs": nbytes / ms / 1e6,
+            "frac_of_peak": nbytes / ms / 1e6 / _peak()}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["apply", "spmv"])
+    ap.add_argument("what", choices=["apply", "spmv", "bsr"])
+    ap.add_argument("--p", type=int, default=1, help="bsr: DG polynomial degree (block size (p+1)(p+2)/2)")
     ap.add_argument("--n-el", type=int, default=64)
     ap.add_argument("--problem", default="q1_3d", choices=["q1_3d", "p1"],
                     help="spmv: 3D Q1 lognormal diffusion (n-el cells per side) or jittered P1 (n-el nodes per side)")
@@ -128,7 +154,7 @@ def main():
                     help="16-bit residual terms of the tensor-core apply (default: automatic)")
     ap.add_argument("--tune", action="store_true", help="run the autotuner first and report every candidate")
     args = ap.parse_args()
-    out = bench_apply(args) if args.what == "apply" else bench_spmv(args)
+    out = {"apply": bench_apply, "spmv": bench_spmv, "bsr": bench_bsr}[args.what](args)
     print(json.dumps(out))
 
 

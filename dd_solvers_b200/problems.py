@@ -279,3 +279,42 @@ def diffusion3d_lognormal(n_el: int, seed: int) -> GridProblem:
     rng = np.random.default_rng(seed)
     g = rng.standard_normal((n_el,) * 3)
     return q1_grid(3, n_el, np.exp(g))
+
+
+# ---------------------------------------------------------------------------
+# DG block structure (the reference's BSR benchmark meshes)
+# ---------------------------------------------------------------------------
+
+def dg_block_size(dim: int, p: int) -> int:
+    """DOFs per element of a P_p DG space on triangles (dim 2) or tetrahedra (dim 3)."""
+    return (p + 1) * (p + 2) // 2 if dim == 2 else (p + 1) * (p + 2) * (p + 3) // 6
+
+
+def dg_bsr_pattern_2d(n: int) -> tuple[np.ndarray, np.ndarray]:
+    """Block sparsity of a DG operator on the 2 n^2 triangles of an n x n grid of
+    squares, each cut by its (i, j)-(i+1, j+1) diagonal: block row e holds e
+    and its face neighbours (up to 3), column indices sorted. Triangle 2 (j n + i)
+    is the lower-right one of square (i, j), 2 (j n + i) + 1 the upper-left one;
+    lower-right (i, j) borders upper-left (i, j), (i, j - 1) and (i + 1, j).
+    Returns (crow, col) as int32.
+    """
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="xy")
+    i, j = i.ravel(), j.ravel()
+    sq = j * n + i
+    lo, up = 2 * sq, 2 * sq + 1
+    rows, cols = [lo, up], [lo, up]  # diagonal blocks
+    pairs = [(lo, up, np.ones_like(i, dtype=bool))]  # own diagonal
+    m = j > 0
+    pairs.append((lo[m], 2 * ((j[m] - 1) * n + i[m]) + 1, None))  # bottom edge
+    m = i < n - 1
+    pairs.append((lo[m], 2 * (j[m] * n + i[m] + 1) + 1, None))  # right edge
+    for a, b, _ in pairs:
+        rows += [a, b]
+        cols += [b, a]
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    order = np.lexsort((c, r))
+    r, c = r[order], c[order]
+    crow = np.zeros(2 * n * n + 1, dtype=np.int64)
+    np.add.at(crow, r + 1, 1)
+    return np.cumsum(crow).astype(np.int32), c.astype(np.int32)

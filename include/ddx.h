@@ -127,9 +127,11 @@ int ddx_spmv_csr_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols,
  * y[row, j] = sum_k vals[k] x[cols[k], j] (coarse restriction A_R y or R0 r). */
 int ddx_spmv_csr_rowblock_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols,
                               const double* vals, const double* x, double* y, ddx_stream_t stream);
-/* BSR, block size bs (1..8), blocks column-major (bs, bs) as produced by the
- * reference's csr_to_bsr (src/dd_solvers/cpp/cusparse.cpp:22-107); dtype F64
- * or F32 for vals/x/y. One warp per block row. */
+/* BSR, block size bs (1..24: DG P1..P5 triangles have 3..21 DOFs per
+ * element), blocks column-major (bs, bs) as produced by the reference's
+ * csr_to_bsr (src/dd_solvers/cpp/cusparse.cpp:22-107); dtype F64 or F32 for
+ * vals/x/y. Replaces FastBSR's RPT-I kernel (src/dd_solvers/dd_solvers/bsr.py:40-76):
+ * one lane per scalar row, floor(32 / bs) block rows per warp. */
 int ddx_spmv_bsr(int64_t n_block_rows, int bs, const int* row_ptr, const int* cols, const void* vals,
                  const void* x, void* y, int dtype, ddx_stream_t stream);
 

@@ -61,20 +61,24 @@ def test_bsr_small_fixture(cuda, dtype):
 
 
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
-@pytest.mark.parametrize("bs", [1, 2, 3, 4, 6, 8])
+@pytest.mark.parametrize("bs", [1, 2, 3, 4, 6, 8, 10, 11, 15, 16, 20, 21, 24])
 def test_bsr_random(cuda, dtype, bs):
     from dd_solvers_b200 import FastBSR
 
     torch.manual_seed(bs)
-    nbr, per = 1000, 3
+    nbr, per = 1001, 3  # not a multiple of the block rows per warp
     crow = torch.arange(0, nbr * per + 1, per)
     col = torch.randint(0, nbr, (nbr * per,))
     vals = torch.randn(nbr * per, bs, bs, dtype=dtype)
     m = torch.sparse_bsr_tensor(crow, col, vals, size=(nbr * bs, nbr * bs))
     x = torch.randn(nbr * bs, dtype=dtype)
-    expected = (m.to_dense() @ x).to(cuda)
+    # exact product of the same inputs; rounding bound ~ terms x eps x sum |a_ij x_j|
+    dense = m.to_dense().double()
+    expected = (dense @ x.double()).to(cuda)
+    scale = (dense.abs() @ x.double().abs()).to(cuda)
     y = FastBSR(m.to(cuda)) @ x.to(cuda)
-    assert _allclose(y, expected)
+    eps = 1e-5 if dtype == torch.float32 else 1e-13
+    assert torch.all((y.double() - expected).abs() <= eps * scale + 1e-300)
 
 
 def test_csr_to_bsr_layout(cuda):
@@ -310,3 +314,19 @@ def test_symmetric_tiles_apply_matches_fp64_product(cuda, prec):
     from dd_solvers_b200 import _lib
 
     assert _lib.device_error() == 0
+
+
+def test_bsr_dg_pattern(cuda):
+    """DG triangle block structure (P2, 6 DOFs per element) with uneven rows (2-4 blocks)."""
+    from dd_solvers_b200 import FastBSR, problems
+
+    crow, col = problems.dg_bsr_pattern_2d(9)
+    bs = problems.dg_block_size(2, 2)
+    nbr = len(crow) - 1
+    vals = torch.randn(int(crow[-1]), bs, bs, dtype=torch.float64, generator=torch.Generator().manual_seed(1))
+    m = torch.sparse_bsr_tensor(torch.as_tensor(crow.astype(np.int64)), torch.as_tensor(col.astype(np.int64)), vals,
+                                size=(nbr * bs, nbr * bs))
+    x = torch.randn(nbr * bs, dtype=torch.float64)
+    expected = (m.to_dense() @ x).to(cuda)
+    y = FastBSR(m.to(cuda)) @ x.to(cuda)
+    assert torch.allclose(y, expected, rtol=1e-12, atol=1e-12)
