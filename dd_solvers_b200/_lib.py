@@ -46,7 +46,7 @@ _SIGS = {
     "ddx_gemv_strided_batched": (_I, [_I64, _I, _P, _I, _P, _P, _I, _P]),
     "ddx_schwarz_local_apply": (_I, [_I, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _P]),
     "ddx_schwarz_local_apply_ex": (_I, [_I, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _I, _P]),
-    "ddx_schwarz_local_apply_sym": (_I, [_I, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _I, _P]),
+    "ddx_schwarz_local_apply_sym": (_I, [_I, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _I, _I, _P]),
     "ddx_schwarz_local_apply_tc_sym": (_I, [_I, _I, _P, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _P]),
     "ddx_schwarz_local_apply_tc": (_I, [_I, _I, _P, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _P]),
     "ddx_dot_noalloc": (_I, [_I64, _I, _P, _P, _P, _P]),

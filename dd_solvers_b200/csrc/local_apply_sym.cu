@@ -10,8 +10,12 @@
 // the row, see setup_ops.sym_tile_index). Tile (I, J) contributes
 //   y_I += T x_J                 and, for I < J,   y_J += T^T x_I.
 //
-// Persistent CTAs walk a size-sorted subdomain list. One producer thread
-// streams the tiles of each block through a ring of four shared-memory stages
+// Persistent CTAs walk a size-sorted list of work items (block, part): with
+// parts > 1 (few, large blocks: not enough blocks to fill the SMs) part s of a
+// block takes tiles [s T / parts, (s + 1) T / parts) of its T tiles and writes
+// its partial y to ylocal slice s (slices sum_i k_i x R apart; the combine adds
+// them). One producer thread streams the tiles through a ring of four
+// shared-memory stages
 // (cp.async.bulk + mbarriers). W consumer warps take the tiles round-robin; in
 // a warp, lane t loads row t of the tile (16-byte loads, conflict-free thanks
 // to the swizzle) for the row sum sum_c T[t, c] x_J[c] -> y_I[t], and the
@@ -209,7 +213,15 @@ struct SymArgs {
   int tiles_per_stage;
   int kpad_max;  // ceil(kmax / 32) * 32
   int kmax;
+  int parts;  // tile ranges per block (work items = blocks x parts); the ylocal
+             // slice of part s starts s * sub_ptr[n_sub] * R elements in
 };
+
+// Tile range [ta, tb) of part s of a block with ntiles tiles.
+__device__ __forceinline__ void part_range(int ntiles, int parts, int s, int& ta, int& tb) {
+  ta = (int)((int64_t)ntiles * s / parts);
+  tb = (int)((int64_t)ntiles * (s + 1) / parts);
+}
 
 template <typename TB, typename ACC, int W>
 __global__ void __launch_bounds__(W * 32 + 32) k_local_apply_sym(SymArgs a) {
@@ -244,19 +256,20 @@ __global__ void __launch_bounds__(W * 32 + 32) k_local_apply_sym(SymArgs a) {
     // ------------------------------ producer ------------------------------
     if (tid != NC) return;
     uint32_t g = 0;
-    for (int w = blockIdx.x; w < a.n_sub && !abort_flag; w += gridDim.x) {
-      const int i = a.order[w];
+    for (int w = blockIdx.x; w < a.n_sub * a.parts && !abort_flag; w += gridDim.x) {
+      const int i = a.order[w / a.parts];
       const int k = (int)(a.sub_ptr[i + 1] - a.sub_ptr[i]);
       if (k == 0 || k > a.kmax) continue;
       const int nt = (k + kT - 1) / kT;
-      const int ntiles = nt * (nt + 1) / 2;
-      const int nchunk = (ntiles + a.tiles_per_stage - 1) / a.tiles_per_stage;
+      int ta, tb;
+      part_range(nt * (nt + 1) / 2, a.parts, w % a.parts, ta, tb);
+      const int nchunk = (tb - ta + a.tiles_per_stage - 1) / a.tiles_per_stage;
       const TB* src = blocks + a.blk_off[i];
       for (int q = 0; q < nchunk; ++q, ++g) {
         const int s = g % kSymStages;
         if (!mbar_wait(&empty[s], ((g / kSymStages) & 1u) ^ 1u)) { abort_flag = 1; return; }
-        const int t0 = q * a.tiles_per_stage;
-        const int nt_here = min(a.tiles_per_stage, ntiles - t0);
+        const int t0 = ta + q * a.tiles_per_stage;
+        const int nt_here = min(a.tiles_per_stage, tb - t0);
         const uint32_t bytes = (uint32_t)nt_here * TILE_BYTES;
         mbar_arrive_expect_tx(&full[s], bytes);
         bulk_g2s(stage_base + (size_t)s * stage_bytes, src + (int64_t)t0 * kTE, bytes, &full[s]);
@@ -270,8 +283,9 @@ __global__ void __launch_bounds__(W * 32 + 32) k_local_apply_sym(SymArgs a) {
   const int R = a.R;
   ACC* yw = ys + (size_t)warp * a.kpad_max;
   uint32_t g = 0;
-  for (int w = blockIdx.x; w < a.n_sub; w += gridDim.x) {
-    const int i = a.order[w];
+  for (int w = blockIdx.x; w < a.n_sub * a.parts; w += gridDim.x) {
+    const int i = a.order[w / a.parts];
+    const int part = w % a.parts;
     const int64_t p0 = a.sub_ptr[i];
     const int k = (int)(a.sub_ptr[i + 1] - p0);
     if (k == 0) continue;
@@ -281,25 +295,31 @@ __global__ void __launch_bounds__(W * 32 + 32) k_local_apply_sym(SymArgs a) {
     }
     const int nt = (k + kT - 1) / kT;
     const int kp = nt * kT;
-    const int ntiles = nt * (nt + 1) / 2;
-    const int nchunk = (ntiles + a.tiles_per_stage - 1) / a.tiles_per_stage;
+    int ta, tb;
+    part_range(nt * (nt + 1) / 2, a.parts, part, ta, tb);
+    const int nchunk = (tb - ta + a.tiles_per_stage - 1) / a.tiles_per_stage;
     named_sync(1, NC);  // previous subdomain done with xs and ys
     if (abort_flag) break;
     for (int c = tid; c < kp; c += NC) xs[c] = c < k ? (ACC)a.r[(int64_t)a.sub_idx[p0 + c] * R + a.j0] : ACC(0);
     for (int e = tid; e < W * kp; e += NC) ys[(e / kp) * a.kpad_max + e % kp] = ACC(0);
     named_sync(1, NC);
 
-    // this warp's tiles: tau = warp, warp + W, ... in row-major (I, J >= I)
-    // order; row I holds J = I..nt-1, so stepping past its end continues at
-    // J - nt + I + 1 of row I + 1
-    int I = 0, J = warp;
-    while (J >= nt && I < nt) { ++I; J = J - nt + I; }
-    int tau = warp;
+    // this warp's tiles: tau = ta + warp, ta + warp + W, ... in row-major
+    // (I, J >= I) order; row I holds J = I..nt-1 and starts at tile
+    // I nt - I (I - 1) / 2, so stepping past its end continues at J - nt + I + 1
+    // of row I + 1
+    int tau = ta + warp;
+    int I = 0, row_start = 0;
+    while (I < nt && row_start + (nt - I) <= tau) {
+      row_start += nt - I;
+      ++I;
+    }
+    int J = I + (tau - row_start);
     for (int q = 0; q < nchunk; ++q) {
       const uint32_t gq = g + (uint32_t)q;
       const int s = gq % kSymStages;
-      const int t0 = q * a.tiles_per_stage;
-      const int t1 = min(t0 + a.tiles_per_stage, ntiles);
+      const int t0 = ta + q * a.tiles_per_stage;
+      const int t1 = min(t0 + a.tiles_per_stage, tb);
       if (abort_flag) break;
       // every warp waits for every stage before releasing it, with or without
       // tiles of its own there: a warp can then never arrive twice on one
@@ -325,7 +345,7 @@ __global__ void __launch_bounds__(W * 32 + 32) k_local_apply_sym(SymArgs a) {
     named_sync(1, NC);  // all warps' slices complete
     if (abort_flag) break;
     const ACC sc = a.scale ? (ACC)a.scale[i] : ACC(1);
-    ACC* y = reinterpret_cast<ACC*>(a.ylocal);
+    ACC* y = reinterpret_cast<ACC*>(a.ylocal) + (int64_t)part * a.sub_ptr[a.n_sub] * R;
     for (int row = tid; row < k; row += NC) {
       ACC sum = ACC(0);
 #pragma unroll
@@ -353,7 +373,7 @@ int launch_sym_w(SymArgs a, int stage_kb, cudaStream_t s) {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, W * 32 + 32, smem);
   per_sm = std::max(1, std::min(per_sm, 4));
-  const int grid = std::max(1, std::min(a.n_sub, nsm * per_sm));
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)a.n_sub * a.parts, (int64_t)nsm * per_sm));
   for (int j = 0; j < a.R; ++j) {
     a.j0 = j;
     kernel<<<grid, W * 32 + 32, smem, s>>>(a);
@@ -382,7 +402,7 @@ extern "C" int ddx_schwarz_local_apply_sym(int n_sub, int R, const int64_t* sub_
                                            const int* order, const int64_t* blk_off, const void* blocks,
                                            int block_dtype, const float* scale, int kmax, const double* r,
                                            void* ylocal, int acc_dtype, const int* ist, int warps, int stage_kb,
-                                           ddx_stream_t stream) {
+                                           int parts, ddx_stream_t stream) {
   DDX_REQUIRE(valid_rhs_count(R), "ddx_schwarz_local_apply_sym: unsupported R=%d", R);
   DDX_REQUIRE(n_sub >= 0 && kmax >= 0, "ddx_schwarz_local_apply_sym: bad sizes");
   if (n_sub == 0 || kmax == 0) return DDX_OK;
@@ -401,8 +421,10 @@ extern "C" int ddx_schwarz_local_apply_sym(int n_sub, int R, const int64_t* sub_
   a.r = r;
   a.ylocal = ylocal;
   a.ist = ist;
+  DDX_REQUIRE(parts >= 1 && parts <= 64, "ddx_schwarz_local_apply_sym: parts must be 1..64 (got %d)", parts);
   a.kmax = kmax;
   a.kpad_max = (kmax + kT - 1) / kT * kT;
+  a.parts = parts;
   cudaStream_t s = (cudaStream_t)stream;
   switch (block_dtype) {
     case DDX_F64:

@@ -379,6 +379,7 @@ class SchwarzOperator(SparseSolver):
             del inv
             i = j
         del order_np
+        self._set_parts()
         if self.collect_timings:
             events[3].record()
             torch.cuda.synchronize()
@@ -430,6 +431,28 @@ class SchwarzOperator(SparseSolver):
             i = j
         other.store = store
         return other
+
+    def _set_parts(self) -> None:
+        """Tile ranges per block for the SIMT apply on upper-triangle tiles: with
+        fewer blocks than twice the SM count, each block is split so that about
+        2 x SMs work items run at once; the parts' partial products land in
+        separate ylocal slices, listed by an extended transpose map (every entry
+        of DOF d once per slice, slice-major within a subdomain: a fixed order)."""
+        self.parts = 1
+        if self.store.layout == "sym" and self.n_solvers:
+            nsm = torch.cuda.get_device_properties(self.device).multi_processor_count
+            if self.n_solvers < 2 * nsm:
+                self.parts = int(min(8, -(-2 * nsm // self.n_solvers)))
+        self._ymap_one = (self.dof_ptr, self.dof_src)
+        if self.parts > 1:
+            S = self.parts
+            total = int(self.sub_idx.numel())
+            src = (self.dof_src.to(torch.int64)[:, None] + torch.arange(S, device=self.device)[None, :] * total)
+            self._ymap_parts = ((self.dof_ptr * S).to(torch.int32).contiguous(),
+                                src.reshape(-1).to(torch.int32).contiguous())
+        else:
+            self._ymap_parts = self._ymap_one
+        self._ymap = self._ymap_one
 
     def _layout(self, ks: np.ndarray) -> str:
         """Upper-triangle tiles when they take fewer elements than the full
@@ -500,7 +523,7 @@ class SchwarzOperator(SparseSolver):
         if s is None:
             dev = self.device
             nloc = int(self.sub_idx.numel())
-            s = {"ylocal": torch.empty(max(nloc, 1) * R, dtype=self.acc_dtype, device=dev),
+            s = {"ylocal": torch.zeros(max(nloc, 1) * R * getattr(self, "parts", 1), dtype=self.acc_dtype, device=dev),
                  "y": torch.empty(self.n * R, dtype=torch.float64, device=dev)}
             if self.n_coarse:
                 s["w"] = torch.empty(self.n_coarse * R, dtype=torch.float64, device=dev)
@@ -523,10 +546,20 @@ class SchwarzOperator(SparseSolver):
                    L.ptr(self.sub_ptr), L.ptr(self.order), L.ptr(t.tile_off), L.ptr(t.data), code,
                    L.ptr(self.store.scale), self.kmax, L.ptr(b16), L.ptr(panel_off), terms, L.ptr(s["ylocal"]),
                    L.ptr(ist), L.ptr(st), L.stream_ptr())
+            self._ymap = self._ymap_one  # one slice written
             return s["ylocal"]
         cfg = self._apply_config(R)
         self._simt_apply(r, s["ylocal"], R, ist, *cfg)
+        self._ymap = self._ymap_parts if self.store.layout == "sym" else self._ymap_one
         return s["ylocal"]
+
+    def _local_sum(self, r: torch.Tensor, R: int) -> torch.Tensor:
+        """Local products ``y_i = s_i Q_i r[idx_i]`` stacked subdomain-major as a
+        (sum k_i) x R FP64 tensor: the ylocal slices of a split apply added up."""
+        ylocal = self._local(r, R)
+        total = int(self.sub_idx.numel())
+        n_slices = self.parts if self._ymap is self._ymap_parts else 1
+        return ylocal[: n_slices * total * R].view(n_slices, total, R).double().sum(0)
 
     def _panels(self, R: int, terms: int):
         """Zero-initialised B-panel buffer and per-subdomain byte offsets for the
@@ -546,11 +579,14 @@ class SchwarzOperator(SparseSolver):
     def _simt_apply(self, r, ylocal, R, ist, groups: int, stage_kb: int) -> None:
         """SIMT local apply; ``groups`` is the consumer-group count of the full-block
         kernel or the consumer-warp count of the upper-triangle-tile kernel."""
-        entry = "ddx_schwarz_local_apply_sym" if self.store.layout == "sym" else "ddx_schwarz_local_apply_ex"
-        L.call(entry, self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
-               L.ptr(self.order), L.ptr(self.store.blk_off), L.ptr(self.store.data),
-               L.DTYPE_CODE[self.block_dtype], L.ptr(self.store.scale), self.kmax, L.ptr(r),
-               L.ptr(ylocal), L.DTYPE_CODE[self.acc_dtype], L.ptr(ist), groups, stage_kb, L.stream_ptr())
+        args = (self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx), L.ptr(self.order),
+                L.ptr(self.store.blk_off), L.ptr(self.store.data), L.DTYPE_CODE[self.block_dtype],
+                L.ptr(self.store.scale), self.kmax, L.ptr(r), L.ptr(ylocal), L.DTYPE_CODE[self.acc_dtype],
+                L.ptr(ist), groups, stage_kb)
+        if self.store.layout == "sym":
+            L.call("ddx_schwarz_local_apply_sym", *args, self.parts, L.stream_ptr())
+        else:
+            L.call("ddx_schwarz_local_apply_ex", *args, L.stream_ptr())
 
     # -- autotuner -------------------------------------------------------------
     # (consumer groups of 4 warps, KiB per shared-memory stage): full-block kernel;
@@ -631,7 +667,8 @@ class SchwarzOperator(SparseSolver):
         if pcg is not None:
             st, ist, partials, tickets = pcg.st, pcg.ist, pcg.partials, pcg.tickets
             dots = 1
-        L.call("ddx_schwarz_combine", self.n, R, L.ptr(self.dof_ptr), L.ptr(self.dof_src), L.ptr(ylocal),
+        dof_ptr, dof_src = self._ymap if ylocal is not None else (None, None)
+        L.call("ddx_schwarz_combine", self.n, R, L.ptr(dof_ptr), L.ptr(dof_src), L.ptr(ylocal),
                L.DTYPE_CODE[self.acc_dtype], L.ptr(u), L.ptr(p_ptr), L.ptr(p_col), L.ptr(p_val), L.ptr(yc),
                float(sign), L.ptr(z), dots, L.ptr(r), L.ptr(q), L.ptr(st), L.ptr(ist), L.ptr(partials),
                L.ptr(tickets), L.stream_ptr())

@@ -180,14 +180,19 @@ int ddx_schwarz_local_apply(int n_sub, int R, const int64_t* sub_ptr, const int*
  * zero beyond k. Tile (I, J) adds T x_J to rows I and, for I < J, T^T x_I to
  * rows J. `warps` (4, 8 or 16; 0 = 8) consumer warps per CTA, `stage_kb`
  * (0 = 16) KiB per shared-memory stage: run-time choices for the autotuner.
- * Accumulation and output types as ddx_schwarz_local_apply_ex. No counterpart
+ * `parts` (1..64) splits each block's tiles into that many contiguous ranges,
+ * processed by different CTAs (for few, large blocks); part s writes its
+ * partial product to ylocal slice s, at element offset s * sub_ptr[n_sub] * R,
+ * and the caller adds the slices (ddx_schwarz_combine with a transpose map
+ * listing every slice). Accumulation and output types as
+ * ddx_schwarz_local_apply_ex. No counterpart
  * in the reference, whose inverse blocks are stored in full
  * (src/dd_solvers/dd_solvers/solvers.py:343-359). */
 int ddx_schwarz_local_apply_sym(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
                                 const int* order, const int64_t* blk_off, const void* blocks,
                                 int block_dtype, const float* scale, int kmax, const double* r,
                                 void* ylocal, int acc_dtype, const int* ist, int warps, int stage_kb,
-                                ddx_stream_t stream);
+                                int parts, ddx_stream_t stream);
 /* Tensor-core variant for R in {16, 32, 64} right-hand sides and BF16/FP16
  * blocks: Y_i = Q_i X_i as tcgen05.mma (M = 128, N = R, K = 16, FP32
  * accumulators in TMEM). `tiles` holds each block cut into 128-row x 64-column
