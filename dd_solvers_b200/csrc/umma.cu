@@ -437,6 +437,7 @@ __device__ __forceinline__ uint64_t sw128_mn_desc(uint32_t saddr, uint32_t lbo) 
 __host__ __device__ constexpr uint32_t idesc_f16_amn(int ab_fmt, int N) { return idesc_f16(ab_fmt, N) | (1u << 15); }
 
 constexpr int kSymTile = 128;
+constexpr int kMaxRowTiles = 32;  // ceil(kmax / 128) * N <= 512 TMEM columns with N >= 16
 constexpr int kSymTileBytes = kSymTile * kSymTile * 2;  // 32 KB
 constexpr int kHalfBytes = kSymTileBytes / 2;           // 16 KB
 
@@ -453,9 +454,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
   uint64_t* a_empty = bars + STAGES;
   uint64_t* b_full = bars + 2 * STAGES;
   uint64_t* b_empty = b_full + 1;
-  uint64_t* acc_full = b_full + 2;
-  uint64_t* acc_empty = b_full + 3;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(b_full + 4);
+  uint64_t* acc_full = b_full + 2;                     // [kMaxRowTiles]: D_m complete
+  uint64_t* acc_empty = acc_full + kMaxRowTiles;      // [kMaxRowTiles]: D_m drained
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + kMaxRowTiles);
   __shared__ int abort_flag_s;
   volatile int& abort_flag = abort_flag_s;
   __shared__ float rhs_unscale[64];
@@ -470,8 +471,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
     }
     mbar_init(b_full, 1);
     mbar_init(b_empty, 1);
-    mbar_init(acc_full, 1);
-    mbar_init(acc_empty, kEpiThreads / 32);
+    for (int m = 0; m < kMaxRowTiles; ++m) {
+      mbar_init(&acc_full[m], 1);
+      mbar_init(&acc_empty[m], kEpiThreads / 32);
+    }
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -525,19 +528,28 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
       constexpr uint32_t idesc_k = idesc_f16(fmt, N);
       constexpr uint32_t idesc_mn = idesc_f16_amn(fmt, N);
       uint32_t g = 0, sub_n = 0;
+      uint32_t ph = 0;  // bit m: parity of the completed uses of accumulator D_m
       for (int w = blockIdx.x; w < a.n_sub && !abort_flag; w += gridDim.x) {
         const int i = a.order[w];
         const int k = (int)(a.sub_ptr[i + 1] - a.sub_ptr[i]);
         if (k == 0 || k > a.kmax) continue;
         const int nt = (k + kSymTile - 1) / kSymTile;
         if (!mbar_wait(b_full, sub_n & 1u)) { abort_flag = 1; break; }
-        if (!mbar_wait(acc_empty, (sub_n & 1u) ^ 1u)) { abort_flag = 1; break; }
         fence_after();
         uint64_t touched = 0;  // row tiles whose accumulator already holds a partial sum
+        // before the first MMA into D_m in this block, the epilogue must have
+        // drained D_m of the previous block
+        auto claim = [&](int m) -> bool {
+          if ((touched >> m) & 1u) return true;
+          if (!mbar_wait(&acc_empty[m], ((ph >> m) & 1u) ^ 1u)) return false;
+          fence_after();
+          return true;
+        };
         for (int I = 0; I < nt && !abort_flag; ++I) {
           for (int J = I; J < nt; ++J, ++g) {
             const int s = g % STAGES;
             if (!mbar_wait(&a_full[s], (g / STAGES) & 1u)) { abort_flag = 1; break; }
+            if (!claim(I) || (I != J && !claim(J))) { abort_flag = 1; break; }
             fence_after();
             const uint32_t sa = smem_u32(ring + (size_t)s * kSymTileBytes);
             // D_I += T X_J: K runs over the 128 columns of J (two 64-column halves)
@@ -574,10 +586,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
             }
             mma_commit(&a_empty[s]);
           }
+          // D_I is complete once row I is done: its other contributions (T^T X of
+          // tiles (I', I), I' < I) came from earlier rows
+          if (!abort_flag) mma_commit(&acc_full[I]);
         }
         if (abort_flag) break;
-        mma_commit(acc_full);
         mma_commit(b_empty);
+        ph ^= (nt >= 32) ? 0xffffffffu : ((1u << nt) - 1u);
         ++sub_n;
       }
     }
@@ -585,7 +600,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
     // ------------------------------ epilogue --------------------------------
     const int e = threadIdx.x - 64;
     const int quarter = warp & 3;
-    uint32_t sub_n = 0;
+    uint32_t ph = 0;  // bit m: parity of the completed uses of accumulator D_m
     for (int w = blockIdx.x; w < a.n_sub && !abort_flag; w += gridDim.x) {
       const int i = a.order[w];
       const int64_t p0 = a.sub_ptr[i];
@@ -596,10 +611,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
         continue;
       }
       const int nt = (k + kSymTile - 1) / kSymTile;
-      if (!mbar_wait(acc_full, sub_n & 1u)) { abort_flag = 1; break; }
-      fence_after();
       const float sc = a.scale ? a.scale[i] : 1.0f;
       for (int m = 0; m < nt; ++m) {
+        // drain D_m as soon as its row is done, while later rows still multiply
+        if (!mbar_wait(&acc_full[m], (ph >> m) & 1u)) { abort_flag = 1; break; }
+        fence_after();
         float v[N];
 #pragma unroll
         for (int c = 0; c < N; c += 16) tmem_ld16(tmem + (uint32_t)(m * N + c) + ((uint32_t)(quarter * 32) << 16), v + c);
@@ -611,11 +627,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
             dst[c / 4] = make_float4(sc * rhs_unscale[c] * v[c], sc * rhs_unscale[c + 1] * v[c + 1],
                                      sc * rhs_unscale[c + 2] * v[c + 2], sc * rhs_unscale[c + 3] * v[c + 3]);
         }
+        fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[m]);
       }
-      fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(acc_empty);
-      ++sub_n;
+      if (abort_flag) break;
+      ph ^= (nt >= 32) ? 0xffffffffu : ((1u << nt) - 1u);
     }
   }
   fence_before();
@@ -634,7 +651,7 @@ static int launch_sym(const Args& a, cudaStream_t s) {
     set_error("ddx_schwarz_local_apply_tc_sym: %d row tiles x R=%d accumulators exceed 512 TMEM columns", nt_max, N);
     return DDX_ERR_UNSUPPORTED;
   }
-  const size_t fixed = 1024 + (size_t)TERMS * nk_max * N * 128 + kPanelSlack + 16 * 8 + 64;
+  const size_t fixed = 1024 + (size_t)TERMS * nk_max * N * 128 + kPanelSlack + (2 * 3 + 2 + 2 * kMaxRowTiles) * 8 + 64;
   // at least 120 KB of shared memory keeps one CTA per SM (its accumulators may take all 512 TMEM columns)
   const size_t smem3 = std::max<size_t>(fixed + 3 * (size_t)kSymTileBytes, 120 * 1024);
   const size_t smem2 = std::max<size_t>(fixed + 2 * (size_t)kSymTileBytes, 120 * 1024);

@@ -332,7 +332,10 @@ class SchwarzOperator(SparseSolver):
 
         # coarse space
         if R0 is not None:
-            Ac = (R0 @ A_sp @ R0.T).tocsr()
+            AR = (R0 @ A_sp).tocsr()  # also the hybrid's A_R = R0 A
+            AR.sum_duplicates()
+            self._AR_sp = AR
+            Ac = (AR @ R0.T).tocsr()
             Ac.sort_indices()
             Ac_t = torch.sparse_csr_tensor(torch.as_tensor(Ac.indptr), torch.as_tensor(Ac.indices),
                                            torch.as_tensor(Ac.data), Ac.shape).to(self.device)
@@ -489,7 +492,7 @@ class SchwarzOperator(SparseSolver):
             return False
         nt = (self.kmax + 127) // 128
         panel = terms * 2 * nt * so.UMMA_K * R * 2
-        return nt * R <= 512 and 1024 + 2 * 32768 + panel + 2048 + 192 <= 227 * 1024
+        return nt * R <= 512 and 1024 + 2 * 32768 + panel + 2048 + 640 <= 227 * 1024
 
     def _tc_terms(self, R: int) -> int:
         """Residual terms of the tensor-core path for R right-hand sides; 0 = not usable.
@@ -728,10 +731,7 @@ class HybridSchwarz(SchwarzOperator):
     def setup(self, matrix, dofs_per_solver=None, solvers_per_coarse=None, *args, **kwargs):
         timings = super().setup(matrix, dofs_per_solver, solvers_per_coarse, *args, **kwargs)
         if self.n_coarse:
-            A_sp = so.scipy_csr(matrix)
-            AR = (self._R0_sp @ A_sp).tocsr()
-            AR.sum_duplicates()
-            self._AR = _csr_dev(AR, self.device)
+            self._AR = _csr_dev(self._AR_sp, self.device)
         return timings
 
     def T0(self, rhs: torch.Tensor) -> torch.Tensor:
