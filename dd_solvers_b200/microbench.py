@@ -5,6 +5,7 @@ experiments/benchmark_batched_gemv.py and experiments/benchmark_bsrmv.py).
     python -m dd_solvers_b200.microbench spmv --n-el 128 --rhs 1
     python -m dd_solvers_b200.microbench spmv --problem p1 --n-el 2048 --rhs 16
     python -m dd_solvers_b200.microbench bsr --n-el 2048 --p 1
+    python -m dd_solvers_b200.microbench solve --workload c5 --precision f16
 
 ``apply`` times the Schwarz local-inverse apply (SIMT streaming kernel for
 R < 16, tensor-core kernel for R in {16, 32, 64} with BF16/FP16 blocks) on the
@@ -60,7 +61,7 @@ def bench_apply(args) -> dict:
     pc = dd.AdditiveSchwarz(torch.float64, dd.Inv(DT[args.precision]), None)
     pc.setup(dd.csr_to_torch(A).to(dev), subdomains=(sub_ptr, sub_idx))
     torch.cuda.empty_cache()  # release setup temporaries: a profiler then saves/restores less device memory
-    R = args.rhs
+    R = args.rhs or 1
     pc.use_tensor_cores = not args.simt
     pc.rhs_terms = args.terms
     pc.tc_symmetric = not args.tc_full
@@ -102,7 +103,7 @@ def bench_spmv(args) -> dict:
     else:
         A = problems.diffusion3d_lognormal(args.n_el, 0).matrix
     M = _SellMatrix(dd.csr_to_torch(A).to(dev))
-    R = args.rhs
+    R = args.rhs or 1
     x = torch.randn(A.shape[0] * R, dtype=torch.float64, device=dev)
     y = torch.empty_like(x)
     ms = _time(lambda: M.launch(x, y, R, L.SPMV_PLAIN), args.reps)
@@ -137,16 +138,49 @@ def bench_bsr(args) -> dict:
             "frac_of_peak": nbytes / ms / 1e6 / _peak()}
 
 
+def bench_solve(args) -> dict:
+    """One solve of a benchmark workload (``--workload``, block precision
+    ``--precision``) inside a cudaProfilerStart/Stop window, after one warm-up
+    solve: for launch lists (ncu --profile-from-start off)."""
+    import dd_solvers_b200 as dd
+    from dd_solvers_b200.workloads import WORKLOADS, build_problem, rhs_for
+
+    spec = WORKLOADS[args.workload]
+    prob = build_problem(spec)
+    dev = torch.device("cuda")
+    At = dd.csr_to_torch(prob["A"]).to(dev)
+    cls = dd.HybridSchwarz if spec["method"] == "hybrid" else dd.AdditiveSchwarz
+    cg = dd.CG(cls(torch.float64, dd.Inv(DT[args.precision]), dd.CUDSS()), rtol=2.5e-9, maxiter=2000,
+               flexible=args.precision != "f64")
+    cg.setup(At, subdomains=(prob["sub_ptr"], prob["sub_idx"]), coarse_restriction=prob["R0"], block_size=1)
+    R = args.rhs or spec["R"]
+    B = torch.as_tensor(rhs_for(prob["A"].shape[0], 0, 1, spec, R), device=dev)
+    cg.solve(B)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.profiler.start()
+    e0.record()
+    _, meta = cg.solve(B)
+    e1.record()
+    torch.cuda.profiler.stop()
+    torch.cuda.synchronize()
+    its = meta["iterations"] if isinstance(meta["iterations"], int) else max(meta["iterations"])
+    ms = e0.elapsed_time(e1)
+    return {"workload": args.workload, "precision": args.precision, "rhs": R, "ms_per_solve": ms,
+            "iterations": its, "ms_per_iteration": ms / max(its, 1)}
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["apply", "spmv", "bsr"])
+    ap.add_argument("what", choices=["apply", "spmv", "bsr", "solve"])
+    ap.add_argument("--workload", default="c5", help="solve: workload name (c1..c5)")
     ap.add_argument("--p", type=int, default=1, help="bsr: DG polynomial degree (block size (p+1)(p+2)/2)")
     ap.add_argument("--n-el", type=int, default=64)
     ap.add_argument("--problem", default="q1_3d", choices=["q1_3d", "p1"],
                     help="spmv: 3D Q1 lognormal diffusion (n-el cells per side) or jittered P1 (n-el nodes per side)")
     ap.add_argument("--parts", type=int, default=8)
     ap.add_argument("--precision", default="bf16", choices=list(DT))
-    ap.add_argument("--rhs", type=int, default=1)
+    ap.add_argument("--rhs", type=int, default=None, help="right-hand sides (apply/spmv: 1; solve: the workload's)")
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--simt", action="store_true", help="force the SIMT kernel for R >= 16")
     ap.add_argument("--tc-full", action="store_true", help="tensor-core apply on full blocks (not the upper triangle)")
@@ -154,7 +188,7 @@ def main():
                     help="16-bit residual terms of the tensor-core apply (default: automatic)")
     ap.add_argument("--tune", action="store_true", help="run the autotuner first and report every candidate")
     args = ap.parse_args()
-    out = {"apply": bench_apply, "spmv": bench_spmv, "bsr": bench_bsr}[args.what](args)
+    out = {"apply": bench_apply, "spmv": bench_spmv, "bsr": bench_bsr, "solve": bench_solve}[args.what](args)
     print(json.dumps(out))
 
 
