@@ -116,12 +116,16 @@ def bench_spmv(args) -> dict:
 
 def bench_bsr(args) -> dict:
     """BSR SpMV on the DG block structure of the reference's BSR benchmark
-    (2D: the 2 n^2 triangles of an n x n grid, P_p elements), FP64 values."""
+    (2D: the 2 n^2 triangles of an n x n grid; 3D: the 6 n^3 tetrahedra of an
+    n^3 grid of cubes; P_p elements), FP64 values."""
     from dd_solvers_b200 import FastBSR, problems
 
     dev = torch.device("cuda")
-    bs = problems.dg_block_size(2, args.p)
-    crow, col = problems.dg_bsr_pattern_2d(args.n_el)
+    bs = problems.dg_block_size(args.dim, args.p)
+    if args.dim == 2:
+        crow, col = problems.dg_bsr_pattern_2d(args.n_el)
+    else:
+        crow, col = problems.dg_bsr_pattern_3d(args.n_el, device=dev)
     nbr, nnzb = len(crow) - 1, int(crow[-1])
     g = torch.Generator(device=dev).manual_seed(0)
     vals = torch.randn(nnzb, bs, bs, dtype=torch.float64, device=dev, generator=g)
@@ -133,7 +137,7 @@ def bench_bsr(args) -> dict:
     x = torch.randn(nbr * bs, dtype=torch.float64, device=dev, generator=g)
     ms = _time(lambda: A @ x, args.reps)
     nbytes = nnzb * (bs * bs * 8 + 4) + (nbr + 1) * 4 + 2 * nbr * bs * 8
-    return {"kernel": "ddx_spmv_bsr", "dim": 2, "p": args.p, "bs": bs, "dofs": nbr * bs, "bsr_nnz": nnzb,
+    return {"kernel": "ddx_spmv_bsr", "dim": args.dim, "p": args.p, "bs": bs, "dofs": nbr * bs, "bsr_nnz": nnzb,
             "ms_per_launch": ms, "algorithmic_bytes": nbytes, "achieved_gbs": nbytes / ms / 1e6,
             "frac_of_peak": nbytes / ms / 1e6 / _peak()}
 
@@ -174,7 +178,8 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("what", choices=["apply", "spmv", "bsr", "solve"])
     ap.add_argument("--workload", default="c5", help="solve: workload name (c1..c5)")
-    ap.add_argument("--p", type=int, default=1, help="bsr: DG polynomial degree (block size (p+1)(p+2)/2)")
+    ap.add_argument("--p", type=int, default=1, help="bsr: DG polynomial degree")
+    ap.add_argument("--dim", type=int, default=2, choices=[2, 3], help="bsr: triangles (2) or tetrahedra (3)")
     ap.add_argument("--n-el", type=int, default=64)
     ap.add_argument("--problem", default="q1_3d", choices=["q1_3d", "p1"],
                     help="spmv: 3D Q1 lognormal diffusion (n-el cells per side) or jittered P1 (n-el nodes per side)")

@@ -318,3 +318,50 @@ def dg_bsr_pattern_2d(n: int) -> tuple[np.ndarray, np.ndarray]:
     crow = np.zeros(2 * n * n + 1, dtype=np.int64)
     np.add.at(crow, r + 1, 1)
     return np.cumsum(crow).astype(np.int32), c.astype(np.int32)
+
+
+def dg_bsr_pattern_3d(n: int, device="cpu") -> tuple[np.ndarray, np.ndarray]:
+    """Block sparsity of a DG operator on the 6 n^3 tetrahedra of an n^3 grid
+    of cubes, each cut into the 6 tetrahedra along its (0,0,0)-(1,1,1)
+    diagonal (tetrahedron (cube, p) = {v000, v000 + e_a, v000 + e_a + e_b,
+    v111} for the p-th permutation (a, b, c) of the axes): block row t holds
+    t and the tetrahedra sharing a face with it (up to 4), columns sorted.
+    Faces are matched by sorting their vertex triples (on ``device``).
+    Returns (crow, col) as int32.
+    """
+    import torch
+
+    dev = torch.device(device)
+    m = n + 1
+    c = torch.arange(n ** 3, device=dev, dtype=torch.int64)
+    ci, cj, ck = c % n, (c // n) % n, c // (n * n)
+    base = (ck * m + cj) * m + ci
+    step = {0: 1, 1: m, 2: m * m}
+    perms = [(0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)]
+    tets = []
+    for a, b, _ in perms:
+        v0 = base
+        v1 = base + step[a]
+        v2 = v1 + step[b]
+        v3 = base + 1 + m + m * m
+        tets.append(torch.stack([v0, v1, v2, v3], dim=1))
+    T = torch.stack(tets, dim=1).reshape(-1, 4)  # tet id = 6 cube + p
+    nt = T.shape[0]
+    faces = torch.cat([T[:, [1, 2, 3]], T[:, [0, 2, 3]], T[:, [0, 1, 3]], T[:, [0, 1, 2]]], dim=0)
+    owner = torch.arange(nt, device=dev).repeat(4)
+    faces, _ = torch.sort(faces, dim=1)
+    k1 = faces[:, 0] * (m ** 3) + faces[:, 1]
+    k2 = faces[:, 2]
+    o = torch.sort(k2, stable=True).indices
+    o = o[torch.sort(k1[o], stable=True).indices]  # lexicographic (k1, k2)
+    k1, k2, owner = k1[o], k2[o], owner[o]
+    same = (k1[1:] == k1[:-1]) & (k2[1:] == k2[:-1])
+    a_, b_ = owner[:-1][same], owner[1:][same]
+    rows = torch.cat([torch.arange(nt, device=dev), a_, b_])
+    cols = torch.cat([torch.arange(nt, device=dev), b_, a_])
+    key = rows * nt + cols
+    key = torch.sort(key).values
+    rows, cols = key // nt, key % nt
+    crow = torch.zeros(nt + 1, dtype=torch.int64, device=dev)
+    crow[1:] = torch.cumsum(torch.bincount(rows, minlength=nt), 0)
+    return crow.cpu().numpy().astype(np.int32), cols.cpu().numpy().astype(np.int32)

@@ -405,6 +405,27 @@ def invert_blocks(blocks: torch.Tensor, ks: torch.Tensor) -> torch.Tensor:
     return inv * mask
 
 
+def csr_torch(M: sps.csr_matrix, device) -> torch.Tensor:
+    """SciPy CSR -> torch CSR on ``device`` (int64 indices, FP64 values)."""
+    M = sps.csr_matrix(M)
+    return torch.sparse_csr_tensor(torch.as_tensor(M.indptr.astype(np.int64), device=device),
+                                   torch.as_tensor(M.indices.astype(np.int64), device=device),
+                                   torch.as_tensor(M.data.astype(np.float64), device=device), M.shape)
+
+
+def spgemm_sorted(X: torch.Tensor, Y: torch.Tensor) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+    """``X @ Y`` of two torch CSR matrices on the device (cuSPARSE SpGEMM through
+    torch), returned as (crow, col, val) with the columns of every row sorted,
+    so the stored order does not depend on the product routine."""
+    Z = X @ Y
+    crow = Z.crow_indices().to(torch.int64)
+    col = Z.col_indices().to(torch.int64)
+    val = Z.values().to(torch.float64)
+    rows = torch.repeat_interleave(torch.arange(Z.shape[0], device=crow.device), crow[1:] - crow[:-1])
+    order = torch.argsort(rows * Z.shape[1] + col)
+    return crow, col[order], val[order]
+
+
 def scipy_csr(A) -> sps.csr_matrix:
     if isinstance(A, sps.spmatrix) or isinstance(A, sps.sparray):
         return sps.csr_matrix(A)

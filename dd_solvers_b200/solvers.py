@@ -292,7 +292,10 @@ class SchwarzOperator(SparseSolver):
         if self.collect_timings:
             events = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
             events[0].record()
-        A_sp = so.scipy_csr(matrix)
+        # the system matrix on the device, int64 indices / FP64 values
+        crow = matrix.crow_indices().to(torch.int64)
+        col = matrix.col_indices().to(torch.int64)
+        val = matrix.values().to(torch.float64)
         if subdomains is None:
             assert dofs_per_solver is not None and solvers_per_coarse is not None
             spc = solvers_per_coarse.to("cpu", torch.int64).numpy()
@@ -332,13 +335,16 @@ class SchwarzOperator(SparseSolver):
 
         # coarse space
         if R0 is not None:
-            AR = (R0 @ A_sp).tocsr()  # also the hybrid's A_R = R0 A
-            AR.sum_duplicates()
-            self._AR_sp = AR
-            Ac = (AR @ R0.T).tocsr()
-            Ac.sort_indices()
-            Ac_t = torch.sparse_csr_tensor(torch.as_tensor(Ac.indptr), torch.as_tensor(Ac.indices),
-                                           torch.as_tensor(Ac.data), Ac.shape).to(self.device)
+            # coarse products on the device: A_R = R0 A (also the hybrid's
+            # restriction), A_C = A_R R0^T
+            A_t = torch.sparse_csr_tensor(crow, col, val, matrix.shape)
+            R0_t = so.csr_torch(R0, self.device)
+            ar = so.spgemm_sorted(R0_t, A_t)
+            self._AR_dev = (ar[0].to(torch.int32), ar[1].to(torch.int32), ar[2])
+            AR_t = torch.sparse_csr_tensor(ar[0], ar[1], ar[2], (R0.shape[0], n))
+            ac = so.spgemm_sorted(AR_t, so.csr_torch(R0.T.tocsr(), self.device))
+            Ac_t = torch.sparse_csr_tensor(ac[0], ac[1], ac[2], (R0.shape[0], R0.shape[0]))
+            del A_t, R0_t, AR_t
             self.coarse_solver.setup(Ac_t)
             self._R0 = _csr_dev(R0, self.device)
             self._P = _csr_dev(R0.T.tocsr(), self.device)
@@ -362,9 +368,6 @@ class SchwarzOperator(SparseSolver):
         self.order = torch.as_tensor(np.argsort(-ks, kind="stable").astype(np.int32), device=dev)
         self.dof_ptr, self.dof_src = so.transpose_map(self.sub_idx, n)
         self.store = so.BlockStore(ks, block_dtype, dev, layout=self._layout(ks))
-        crow = torch.as_tensor(A_sp.indptr.astype(np.int64), device=dev)
-        col = torch.as_tensor(A_sp.indices.astype(np.int64), device=dev)
-        val = torch.as_tensor(A_sp.data, device=dev)
         kpad = so.round_up(max(self.kmax, 1), 16)
         # group subdomains of similar size to bound padding work
         order_np = np.argsort(ks, kind="stable")
@@ -731,7 +734,7 @@ class HybridSchwarz(SchwarzOperator):
     def setup(self, matrix, dofs_per_solver=None, solvers_per_coarse=None, *args, **kwargs):
         timings = super().setup(matrix, dofs_per_solver, solvers_per_coarse, *args, **kwargs)
         if self.n_coarse:
-            self._AR = _csr_dev(self._AR_sp, self.device)
+            self._AR = self._AR_dev
         return timings
 
     def T0(self, rhs: torch.Tensor) -> torch.Tensor:

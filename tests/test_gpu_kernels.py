@@ -331,3 +331,19 @@ def test_bsr_dg_pattern(cuda):
     expected = (m.to_dense() @ x).to(cuda)
     y = FastBSR(m.to(cuda)) @ x.to(cuda)
     assert torch.allclose(y, expected, rtol=1e-12, atol=1e-12)
+
+
+def test_bsr_dg_pattern_3d(cuda):
+    """DG tetrahedron block structure (P2, 10 DOFs per element, 3-5 blocks per row)."""
+    from dd_solvers_b200 import FastBSR, problems
+
+    crow, col = problems.dg_bsr_pattern_3d(3)
+    bs = problems.dg_block_size(3, 2)
+    nbr = len(crow) - 1
+    vals = torch.randn(int(crow[-1]), bs, bs, dtype=torch.float64, generator=torch.Generator().manual_seed(2))
+    m = torch.sparse_bsr_tensor(torch.as_tensor(crow.astype(np.int64)), torch.as_tensor(col.astype(np.int64)), vals,
+                                size=(nbr * bs, nbr * bs))
+    x = torch.randn(nbr * bs, dtype=torch.float64)
+    expected = (m.to_dense() @ x).to(cuda)
+    y = FastBSR(m.to(cuda)) @ x.to(cuda)
+    assert torch.allclose(y, expected, rtol=1e-12, atol=1e-12)

@@ -275,3 +275,15 @@ def test_umma_symmetric_tile_layout():
                     assert data[pos] == want, (i, I, J, r, c)
                 tau += 1
         assert int(ut.off_np[i + 1]) - base == tau * 16384
+
+
+def test_dg_block_patterns_match_the_reference_meshes():
+    """The synthetic DG block structures have the block counts of the reference's
+    BSR-benchmark meshes (results/benchmark_bsrmv.csv: S8 2D and S5 3D)."""
+    crow, col = problems.dg_bsr_pattern_2d(256)
+    assert len(crow) - 1 == 131072 and crow[-1] == 523264
+    crow3, col3 = problems.dg_bsr_pattern_3d(32)
+    assert len(crow3) - 1 == 196608 and crow3[-1] == 970752
+    n = len(crow3) - 1
+    M = sps.csr_matrix((np.ones(len(col3)), col3, crow3), shape=(n, n))
+    assert abs(M - M.T).nnz == 0 and np.diff(crow3).max() == 5
