@@ -1,0 +1,292 @@
+"""Symmetric interior-penalty DG (SIPG) discretisation of the reference's own experiments.
+
+The reference assembles its benchmark systems with DOLFINx
+(``src/experiments/experiments/discretization.py:32-96``) on a nested family of
+uniform triangle meshes (``src/experiments/experiments/meshing.py:204-263``)
+and solves them with its Schwarz-preconditioned CG
+(``src/experiments/experiments/experiments.py:175-300``). DOLFINx is not part of
+this package, so this module restates that discretisation for P1 on the 2D
+uniform family, in torch (CPU or CUDA), FP64:
+
+* ``uniform_mesh_2d(m)`` - the mesh ``S_m``: the unit square split into two
+  right isosceles triangles along the (0,0)-(1,1) diagonal
+  (``create_unit_square(1, 1)``, ``meshing.py:99-107``), refined ``m`` times.
+  Every refinement bisects each triangle's hypotenuse, joins its midpoint to
+  the right-angle vertex and to the two leg midpoints (four similar children),
+  which is what the uniform refinement of these meshes produces: after one
+  step every triangle has exactly two interior edges (the 24-DOF matrix of
+  ``src/dd_solvers/tests/test_solvers.py:25-98`` has nine entries in every
+  row). Child ``k`` of cell ``c`` is cell ``4 c + k``, so the cells of any
+  coarser level ``S_s`` are contiguous runs of ``4^(m-s)`` cells.
+* ``sipg_p1(mesh, case)`` - the exact SIPG form of ``discretization.py:43-76``
+  for ``p = 1``: ``rho grad u . grad v`` plus the penalty
+  ``delta p^2 / h_e * rho+ rho- / (rho+ + rho-) [u][v]`` on interior edges and
+  ``delta p^2 rho / h_e u v`` on boundary edges, minus the symmetrised flux
+  ``[u] n . (rho+ rho- / (rho+ + rho-)) (grad v+ + grad v-)`` (and
+  ``u n . rho grad v`` on the boundary). ``rho`` and ``f`` are interpolated
+  into the DG P1 space (vertex values); the load vector is ``int f_I v``.
+  DOF ``3 c + i`` is vertex ``i`` of cell ``c``. The matrix comes back as a
+  torch CSR tensor with sorted columns (element-major block rows of width
+  3: the cell, then its edge neighbours).
+* ``cell_mapping(m, to)`` - ``S_m`` cells to the cells of ``S_s`` (parents)
+  or of ``C_s`` (the ``2^s x 2^s`` quadrilateral grid, by centroid:
+  ``meshing.py:238-261``).
+
+All the formulas are exact for P1 (the integrands are polynomials of degree at
+most 3 on each edge), so they differ from DOLFINx's quadrature only by
+rounding.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import torch
+
+# test cases of src/experiments/experiments/problems.py:31-74 (2D)
+
+
+def _rho_continuous(x, y):
+    return x ** 2 + y ** 2 + 1
+
+
+def _f_continuous(x, y):
+    pi = math.pi
+    return (8 * pi) * (
+        4 * pi * (x ** 2 + y ** 2 + 1) * torch.sin(4 * x * pi) * torch.sin(4 * y * pi)
+        - x * torch.cos(4 * x * pi) * torch.sin(4 * y * pi)
+        - y * torch.sin(4 * x * pi) * torch.cos(4 * y * pi))
+
+
+def _rho_one(x, y):
+    return torch.ones_like(x)
+
+
+def _f_constant(x, y):
+    pi = math.pi
+    return 2 * pi ** 2 * torch.sin(x * pi) * torch.sin(y * pi)
+
+
+@dataclasses.dataclass(frozen=True)
+class TestCase:
+    """A scalar elliptic problem ``-div(rho grad u) = f`` on the unit square
+    (``problems.py:17-20``): penalty ``delta``, coefficient and source as
+    functions of the coordinate tensors."""
+
+    __test__ = False  # not a pytest class
+    name: str
+    delta: float
+    rho: object
+    f: object
+
+
+CONTINUOUS_COEFFICIENT_2D = TestCase("continuous coefficient 2D", 7.0, _rho_continuous, _f_continuous)
+CONSTANT_COEFFICIENT_2D = TestCase("constant coefficient 2D", 7.0, _rho_one, _f_constant)
+
+
+@dataclasses.dataclass
+class TriangleMesh:
+    """``cells[c] = (a, b, c)``: vertex ids with the right angle at ``b``;
+    vertex ``v`` sits at ``(v % (N + 1), v // (N + 1)) / N``, ``N = 2^m``."""
+
+    m: int
+    cells: torch.Tensor  # (n_cells, 3) int64
+    vertices: torch.Tensor  # (n_vertices, 2) float64
+
+    @property
+    def n_cells(self) -> int:
+        return int(self.cells.shape[0])
+
+
+def uniform_mesh_2d(m: int, device="cpu") -> TriangleMesh:
+    """The uniform mesh ``S_m`` (``2 * 4^m`` triangles), built on integer
+    coordinates so every midpoint is exact."""
+    # (n, 3, 2) integer corner coordinates at scale 2^level: (a, b, c)
+    tri = torch.tensor([[[0, 0], [1, 0], [1, 1]],
+                        [[0, 0], [0, 1], [1, 1]]], dtype=torch.int64, device=device)
+    for _ in range(m):
+        tri = tri * 2
+        a, b, c = tri[:, 0], tri[:, 1], tri[:, 2]
+        M = (a + c) // 2
+        m1 = (a + b) // 2
+        m2 = (b + c) // 2
+        kids = torch.stack([torch.stack([a, m1, M], 1), torch.stack([b, m1, M], 1),
+                            torch.stack([b, m2, M], 1), torch.stack([c, m2, M], 1)], 1)
+        tri = kids.reshape(-1, 3, 2)
+    N = 1 << m
+    ids = tri[..., 1] * (N + 1) + tri[..., 0]
+    g = torch.arange(N + 1, dtype=torch.float64, device=device) / N
+    vy, vx = torch.meshgrid(g, g, indexing="ij")
+    verts = torch.stack([vx.reshape(-1), vy.reshape(-1)], 1)
+    return TriangleMesh(m, ids, verts)
+
+
+def cell_mapping(mesh: TriangleMesh, to: str) -> torch.Tensor:
+    """Cells of ``S_m`` to cells of ``to`` = ``"S<s>"`` (the parent at level
+    ``s``) or ``"C<s>"`` (the ``2^s x 2^s`` quadrilateral containing the
+    centroid, x fastest: ``meshing.py:238-261``)."""
+    kind, s = to[0], int(to[1:])
+    dev = mesh.cells.device
+    c = torch.arange(mesh.n_cells, device=dev)
+    if kind == "S":
+        assert 0 <= s <= mesh.m
+        return c >> (2 * (mesh.m - s))
+    if kind == "C":
+        ctr = mesh.vertices[mesh.cells].mean(dim=1)
+        k = torch.floor(ctr * (1 << s)).to(torch.int64)
+        return k[:, 0] + k[:, 1] * (1 << s)
+    raise ValueError(f"unknown mesh id {to}")
+
+
+def _edge_tables(mesh: TriangleMesh):
+    """Every (cell, local edge) with its neighbour: local edge ``o`` is the
+    edge opposite vertex ``o``. Returns the interior pairs ``(c1, o1, c2, o2)``
+    with ``c1 < c2`` and the boundary ``(c, o)``."""
+    cells = mesh.cells
+    n = cells.shape[0]
+    nv = mesh.vertices.shape[0]
+    j = cells[:, [1, 2, 0]]
+    k = cells[:, [2, 0, 1]]
+    key = (torch.minimum(j, k) * nv + torch.maximum(j, k)).reshape(-1)
+    order = torch.argsort(key, stable=True)
+    ks = key[order]
+    same_next = torch.zeros_like(ks, dtype=torch.bool)
+    same_next[:-1] = ks[1:] == ks[:-1]
+    first = torch.nonzero(same_next).squeeze(1)
+    e1, e2 = order[first], order[first + 1]
+    paired = torch.zeros(3 * n, dtype=torch.bool, device=cells.device)
+    paired[e1] = True
+    paired[e2] = True
+    bnd = torch.nonzero(~paired).squeeze(1)
+    return (e1 // 3, e1 % 3, e2 // 3, e2 % 3), (bnd // 3, bnd % 3)
+
+
+def _cell_geometry(mesh: TriangleMesh, rho):
+    p = mesh.vertices[mesh.cells]  # (n, 3, 2)
+    d1 = p[:, 1] - p[:, 0]
+    d2 = p[:, 2] - p[:, 0]
+    det = d1[:, 0] * d2[:, 1] - d2[:, 0] * d1[:, 1]
+    g1 = torch.stack([d2[:, 1], -d2[:, 0]], 1) / det[:, None]
+    g2 = torch.stack([-d1[:, 1], d1[:, 0]], 1) / det[:, None]
+    g = torch.stack([-g1 - g2, g1, g2], 1)  # (n, 3, 2) gradients of the barycentrics
+    area = det.abs() / 2
+    rv = rho(p[..., 0], p[..., 1])  # (n, 3) interpolated coefficient
+    return p, g, area, rv
+
+
+def _edge_terms(p, rv, c, o):
+    """Endpoints (local ids), length, and the trace integrals on edge ``o`` of
+    cells ``c``: ``I1[e, i] = int_0^1 rho lambda_i`` for the two endpoints,
+    ``C[e, i, j] = int_0^1 rho lambda_i lambda_j`` (rho linear along the edge)."""
+    jl = (o + 1) % 3
+    kl = (o + 2) % 3
+    pj, pk = p[c, jl], p[c, kl]
+    h = torch.linalg.norm(pk - pj, dim=1)
+    rj, rk = rv[c, jl], rv[c, kl]
+    I1 = torch.stack([rj / 3 + rk / 6, rj / 6 + rk / 3], 1)
+    cjk = (rj + rk) / 12
+    C = torch.stack([torch.stack([rj / 4 + rk / 12, cjk], 1),
+                     torch.stack([cjk, rj / 12 + rk / 4], 1)], 1)
+    return jl, kl, h, I1, C
+
+
+def _trace_matrix(o, jl, kl):
+    """``T[e, i, q]`` = 1 when local DOF ``i`` is endpoint ``q`` of the edge."""
+    n = o.shape[0]
+    T = torch.zeros(n, 3, 2, dtype=torch.float64, device=o.device)
+    ar = torch.arange(n, device=o.device)
+    T[ar, jl, 0] = 1.0
+    T[ar, kl, 1] = 1.0
+    return T
+
+
+@dataclasses.dataclass
+class DGSystem:
+    """An assembled SIPG system: ``matrix`` (torch sparse CSR, FP64, int64
+    indices), ``load`` (n,), ``block_size`` = DOFs per cell, and the mesh."""
+
+    matrix: torch.Tensor
+    load: torch.Tensor
+    block_size: int
+    mesh: TriangleMesh
+
+
+def sipg_p1(mesh: TriangleMesh, case: TestCase = CONTINUOUS_COEFFICIENT_2D) -> DGSystem:
+    """Assemble ``discretization.py:43-76`` (exact form, ``p = 1``) on ``mesh``."""
+    dev = mesh.cells.device
+    n = mesh.n_cells
+    delta = case.delta * 1 ** 2
+    p, g, area, rv = _cell_geometry(mesh, case.rho)
+
+    # element stiffness: (g_i . g_j) int_K rho, rho linear -> area * mean
+    blocks_self = torch.einsum("nid,njd->nij", g, g) * (area * rv.mean(dim=1))[:, None, None]
+
+    (c1, o1, c2, o2), (cb, ob) = _edge_tables(mesh)
+
+    # interior edges: 6x6 over [DOFs of c1 (+), DOFs of c2 (-)]
+    jl1, kl1, h, I1, C = _edge_terms(p, rv, c1, o1)
+    T1 = _trace_matrix(o1, jl1, kl1)
+    # the same geometric endpoints in c2's local numbering
+    pj = p[c1, jl1]
+    a2 = (o2 + 1) % 3
+    b2 = (o2 + 2) % 3
+    same = (p[c2, a2] == pj).all(dim=1)
+    jl2 = torch.where(same, a2, b2)
+    kl2 = torch.where(same, b2, a2)
+    T2 = _trace_matrix(o2, jl2, kl2)
+    T = torch.cat([T1, T2], 1)  # (E, 6, 2)
+    sigma = torch.tensor([1.0, 1, 1, -1, -1, -1], dtype=torch.float64, device=dev)
+    n_plus = -g[c1, o1] / torch.linalg.norm(g[c1, o1], dim=1, keepdim=True)  # outward of c1
+    G = torch.cat([g[c1], g[c2]], 1)  # (E, 6, 2)
+    ng = torch.einsum("ed,eid->ei", n_plus, G)
+    t = torch.einsum("eiq,eq->ei", T, I1)
+    TCT = torch.einsum("eiq,eqr,ejr->eij", T, C, T)
+    pen = (delta / 2) * sigma[:, None] * sigma[None, :] * TCT
+    Fm = (h / 2)[:, None, None] * ng[:, :, None] * (sigma * t)[:, None, :]
+    M = pen - Fm - Fm.transpose(1, 2)
+
+    # boundary edges: 3x3 on the cell
+    jlb, klb, hb, I1b, Cb = _edge_terms(p, rv, cb, ob)
+    Tb = _trace_matrix(ob, jlb, klb)
+    nb = -g[cb, ob] / torch.linalg.norm(g[cb, ob], dim=1, keepdim=True)
+    ngb = torch.einsum("ed,eid->ei", nb, g[cb])
+    tb = torch.einsum("eiq,eq->ei", Tb, I1b)
+    Mb = delta * torch.einsum("eiq,eqr,ejr->eij", Tb, Cb, Tb) \
+        - hb[:, None, None] * (ngb[:, :, None] * tb[:, None, :] + tb[:, :, None] * ngb[:, None, :])
+
+    blocks_self = blocks_self.index_add(0, c1, M[:, :3, :3])
+    blocks_self = blocks_self.index_add(0, c2, M[:, 3:, 3:])
+    blocks_self = blocks_self.index_add(0, cb, Mb)
+
+    # block-sparse rows: the cell itself and its interior-edge neighbours
+    rows = torch.cat([torch.arange(n, device=dev), c1, c2])
+    cols = torch.cat([torch.arange(n, device=dev), c2, c1])
+    vals = torch.cat([blocks_self, M[:, :3, 3:], M[:, 3:, :3]])
+    order = torch.argsort(rows * n + cols)
+    rows, cols, vals = rows[order], cols[order], vals[order]
+    bs = 3
+    counts = torch.bincount(rows, minlength=n)
+    # scalar CSR: block row r, local row i -> the row's blocks in column order
+    per_row = (counts * bs).repeat_interleave(bs)
+    crow = torch.zeros(n * bs + 1, dtype=torch.int64, device=dev)
+    crow[1:] = torch.cumsum(per_row, 0)
+    bptr = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    bptr[1:] = torch.cumsum(counts, 0)
+    # entries ordered (block row, local row i, block, local col j)
+    blk_of_row = bptr[:-1].repeat_interleave(bs)  # first block of each scalar row
+    cnt_of_row = counts.repeat_interleave(bs)
+    rid = torch.arange(n * bs, device=dev)
+    ent_row = torch.repeat_interleave(rid, cnt_of_row * bs)
+    pos = torch.arange(ent_row.shape[0], device=dev) - crow[ent_row]
+    blk = blk_of_row[ent_row] + pos // bs
+    jj = pos % bs
+    ii = ent_row % bs
+    col = cols[blk] * bs + jj
+    val = vals[blk, ii, jj]
+    A = torch.sparse_csr_tensor(crow, col, val, (n * bs, n * bs))
+
+    # load vector: int f_I v with f interpolated at the vertices
+    fv = case.f(p[..., 0], p[..., 1])
+    mref = torch.tensor([[2.0, 1, 1], [1, 2, 1], [1, 1, 2]], dtype=torch.float64, device=dev)
+    load = ((area / 12)[:, None] * (fv @ mref)).reshape(-1)
+    return DGSystem(A, load, bs, mesh)

@@ -24,12 +24,19 @@ low-precision block storage with per-block power-of-two scales):
 * ``coarse_matrix``       - ``R0 A R0^T`` (``_construct_coarse_solver_matrix``, 721-771).
 * ``quantize``            - ``Inv.setup`` downcast (350-353) plus the per-block
                             power-of-two scale of this package's low-precision storage.
+* ``ContiguousSchwarz``   - the reference's own data layout (``SchwarzOperator.setup``,
+                            571-640): equal contiguous subdomains of ``dofs_per_solver``
+                            DOFs, contiguous runs of ``solvers_per_coarse`` solvers per P0
+                            coarse aggregate; batched local inverses; the coarse matrix
+                            ``R0 A R0^T`` factored by a sparse LU (SciPy SuperLU) where the
+                            reference uses cuDSS (85-113).
 """
 from __future__ import annotations
 
 import numpy as np
 import scipy.linalg as sla
 import scipy.sparse as sps
+import scipy.sparse.linalg as spla
 
 
 class ConvergenceNotAchieved(Exception):
@@ -276,3 +283,47 @@ def lanczos_condition(alphas, betas) -> float:
             L[i, i] += betas[i - 1] / alphas[i - 1]
             L[i - 1, i] = L[i, i - 1] = np.sqrt(betas[i - 1]) / alphas[i - 1]
     return float(np.linalg.cond(L, 2))
+
+
+class ContiguousSchwarz:
+    """Additive/hybrid Schwarz on the reference's contiguous layout.
+
+    ``AdditiveSchwarz.solve`` (``solvers.py:811-826``): ``y = sum_i R_i^T A_i^{-1}
+    R_i r + R0^T A_C^{-1} R0 r``; ``HybridSchwarz.solve`` (874-888): ``y - R0^T
+    A_C^{-1} (R0 A) y``; ``HybridSchwarz.T0`` (861-872). ``R0`` sums the DOFs
+    of each coarse aggregate. FP64 throughout (the plain path).
+    """
+
+    def __init__(self, A, dofs_per_solver: int, solvers_per_coarse):
+        A = sps.csr_matrix(A)
+        n = A.shape[0]
+        k = int(dofs_per_solver)
+        assert n % k == 0
+        self.A, self.k, self.N = A, k, n // k
+        coo = A.tocoo()
+        same = (coo.row // k) == (coo.col // k)
+        B = np.zeros((self.N, k, k))
+        B[coo.row[same] // k, coo.row[same] % k, coo.col[same] % k] = coo.data[same]
+        self.Binv = np.linalg.inv(B)
+        spc = np.asarray(solvers_per_coarse, dtype=np.int64)
+        owner = np.repeat(np.arange(len(spc)), spc * k)
+        self.R0 = sps.csr_matrix((np.ones(n), (owner, np.arange(n))), shape=(len(spc), n))
+        self.AR = (self.R0 @ A).tocsr()
+        self.Ac = (self.AR @ self.R0.T).tocsc()
+        self.lu = spla.splu(self.Ac)
+
+    def local(self, r):
+        return np.einsum("nij,nj->ni", self.Binv, r.reshape(self.N, self.k)).reshape(-1)
+
+    def coarse_solve(self, w):
+        return self.lu.solve(w)
+
+    def additive(self, r):
+        return self.local(r) + self.R0.T @ self.coarse_solve(self.R0 @ r)
+
+    def hybrid(self, r):
+        y = self.local(r)
+        return y - self.R0.T @ self.coarse_solve(self.AR @ y)
+
+    def T0(self, b):
+        return self.R0.T @ self.coarse_solve(self.R0 @ b)

@@ -1,0 +1,141 @@
+"""The DG-SIPG discretisation of the reference's experiments, pinned to its logs.
+
+``tests/golden/dg_experiments.json`` holds the residual histories that the
+reference logged for its own CG runs on the 2D P1 uniform-mesh problems
+(``results/experiment_precisions.csv``); the oracle run on this package's
+assembly must reproduce them.
+"""
+import json
+import math
+import os
+import sys
+
+import numpy as np
+import pytest
+import scipy.sparse as sps
+import torch
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+from dd_solvers_b200 import dg, problems  # noqa: E402
+from oracle import restatement as rs  # noqa: E402
+
+GOLDEN = os.path.join(ROOT, "tests", "golden", "dg_experiments.json")
+
+
+def golden_rows():
+    with open(GOLDEN) as fh:
+        return json.load(fh)
+
+
+def golden(fine, solvers, coarse, prefix):
+    for r in golden_rows():
+        if (r["fine"], r["solvers"], r["coarse"]) == (fine, solvers, coarse) and r["solver"].startswith(prefix):
+            return r
+    raise KeyError((fine, solvers, coarse, prefix))
+
+
+def scipy_csr(A):
+    return sps.csr_matrix((A.values().numpy(), A.col_indices().numpy(), A.crow_indices().numpy()),
+                          shape=tuple(A.shape))
+
+
+def test_s0_block_sums_match_reference_test():
+    """``src/experiments/tests/test_discretization.py:8-27``: rho = 1, delta = 7
+    on the two-triangle mesh."""
+    s = dg.sipg_p1(dg.uniform_mesh_2d(0), dg.CONSTANT_COEFFICIENT_2D)
+    A = s.matrix.to_dense().numpy()
+    delta = 7.0
+    assert A.shape == (6, 6)
+    assert np.isclose(A[:3, :3].sum(), delta * 5 / 2)
+    assert np.isclose(A[3:, :3].sum(), -delta / 2)
+    assert np.isclose(A[3:, 3:].sum(), delta * 5 / 2)
+    assert np.isclose(A[:3, 3:].sum(), -delta / 2)
+
+
+@pytest.mark.parametrize("m", [1, 2, 3])
+def test_matrix_symmetric_positive_definite(m):
+    A = dg.sipg_p1(dg.uniform_mesh_2d(m)).matrix.to_dense().numpy()
+    assert np.abs(A - A.T).max() < 1e-12 * np.abs(A).max()
+    assert np.linalg.eigvalsh(A).min() > 0
+
+
+@pytest.mark.parametrize("m", [1, 4])
+def test_block_structure_matches_bsr_benchmark_pattern(m):
+    """Cell c's block row holds c and its edge neighbours; the block count is
+    that of the reference's 2D BSR benchmark meshes."""
+    mesh = dg.uniform_mesh_2d(m)
+    A = dg.sipg_p1(mesh).matrix
+    n = mesh.n_cells
+    assert n == 2 * 4 ** m
+    crow, col = A.crow_indices(), A.col_indices()
+    rows3 = crow[1::3][: n] - crow[0:-1:3][: n]  # entries of each cell's first row
+    blocks = int(rows3.sum()) // 3
+    _, bcol = problems.dg_bsr_pattern_2d(1 << m)
+    assert blocks == len(bcol)
+    # every row has sorted columns
+    for r in range(0, 3 * n, max(1, 3 * n // 50)):
+        c = col[crow[r]:crow[r + 1]]
+        assert bool((c[1:] > c[:-1]).all())
+
+
+def test_cell_mappings():
+    """``src/experiments/tests/test_meshing.py:36-61``: S2 -> C2 by centroid,
+    S2 -> S1 four children per parent, S1 -> S1 the identity."""
+    mesh = dg.uniform_mesh_2d(2)
+    mp = dg.cell_mapping(mesh, "C2")
+    assert mp.shape == (32,)
+    ctr = mesh.vertices[mesh.cells].mean(dim=1)
+    qx, qy = mp % 4, mp // 4
+    assert bool(((qx / 4 < ctr[:, 0]) & (ctr[:, 0] < (qx + 1) / 4)).all())
+    assert bool(((qy / 4 < ctr[:, 1]) & (ctr[:, 1] < (qy + 1) / 4)).all())
+    mp = dg.cell_mapping(mesh, "S1")
+    assert torch.equal(torch.bincount(mp), torch.full((8,), 4))
+    # children sit inside their parent
+    m1 = dg.uniform_mesh_2d(1)
+    par = m1.vertices[m1.cells][mp]  # (32, 3, 2)
+    a, b, c = par[:, 0], par[:, 1], par[:, 2]
+    v0, v1 = b - a, c - a
+    d = ctr - a
+    det = v0[:, 0] * v1[:, 1] - v0[:, 1] * v1[:, 0]
+    l1 = (d[:, 0] * v1[:, 1] - d[:, 1] * v1[:, 0]) / det
+    l2 = (v0[:, 0] * d[:, 1] - v0[:, 1] * d[:, 0]) / det
+    assert bool(((l1 > 0) & (l2 > 0) & (l1 + l2 < 1)).all())
+    assert torch.equal(dg.cell_mapping(m1, "S1"), torch.arange(8))
+
+
+@pytest.fixture(scope="module")
+def s10():
+    return dg.sipg_p1(dg.uniform_mesh_2d(10))
+
+
+def test_s10_size_and_load_norm_match_reference_log(s10):
+    """The S10 system: the reference logged its size, nnz and (as the first
+    additive-Schwarz residual norm, x0 = 0) the load-vector norm."""
+    row = golden("S10", "S8", "S8", "CG(AdditiveSchwarz(torch.float64, Inv(), CUDSS")
+    assert s10.load.shape[0] == row["dofs"]
+    assert s10.matrix.values().shape[0] == row["nnz"]
+    b = float(torch.linalg.norm(s10.load))
+    assert math.isclose(b, row["residual_norms"][0], rel_tol=1e-13)
+
+
+@pytest.mark.parametrize("kind", ["additive", "hybrid"])
+def test_s10_oracle_residual_history_matches_reference_log(s10, kind):
+    """Fine S10, subdomains and P0 coarse aggregates S8 (48 DOFs each,
+    131,072 coarse DOFs), FP64: the first twelve residual norms of the
+    reference's logged run, reproduced to 1e-10."""
+    prefix = {"additive": "CG(AdditiveSchwarz(torch.float64, Inv(), CUDSS",
+              "hybrid": "CG(HybridSchwarz(torch.float64, Inv(), CUDSS"}[kind]
+    row = golden("S10", "S8", "S8", prefix)
+    A = scipy_csr(s10.matrix)
+    b = s10.load.numpy()
+    n_sol = 2 * 4 ** 8
+    P = rs.ContiguousSchwarz(A, 3 * 4 ** 2, np.ones(n_sol, dtype=np.int64))
+    M = P.additive if kind == "additive" else P.hybrid
+    T0 = P.T0 if kind == "hybrid" else None
+    _, meta = rs.pcg(A, b, M=M, T0=T0, rtol=1e-9, maxiter=12, raise_on_fail=False)
+    ours = np.array(meta["residual norms"])
+    ref = np.array(row["residual_norms"][: len(ours)])
+    assert len(ours) == 12
+    np.testing.assert_allclose(ours, ref, rtol=1e-10)
