@@ -54,6 +54,8 @@ _SIGS = {
     "ddx_schwarz_combine": (_I, [_I64, _I, _P, _P, _P, _I, _P, _P, _P, _P, _P, _D, _P, _I, _P, _P, _P, _P,
                                  _P, _P, _P]),
     "ddx_coarse_gemv_f64": (_I, [_I, _I, _P, _P, _P, _P, _P]),
+    "ddx_nd_order": (_I, [_I64, _P, _P, _I, _P, _P, _P, _P]),
+    "ddx_coarse_solve_nd": (_I, [_P, _I, _P, _P, _P, _P, _P, _P]),
     "ddx_elem_grad_q1": (_I, [_I, _I, _P, _P, _P, _P, _P]),
 }
 

@@ -1,0 +1,372 @@
+// Sparse SPD direct solve for large coarse problems: nested-dissection
+// ordering (host) and the per-level multifrontal solve kernels (device).
+//
+// Replaces the cuDSS factor/solve behind the reference's CUDSS coarse solver
+// (src/dd_solvers/dd_solvers/solvers.py:85-113, src/dd_solvers/cpp/cudss.cpp:64-105)
+// for coarse spaces too large for a dense inverse. The numeric factorisation
+// (dense fronts, batched Cholesky) runs in torch at setup; what it leaves for
+// every front t is G_t = [Linv; M] ((s+u) x s, row-major FP64) with
+// Linv = chol(F_SS)^-1 and M = F_US F_SS^-1, so both solve sweeps are dense
+// GEMVs with no triangular recurrences:
+//
+//   forward  (leaves -> root): f = [w_S; 0] + children's update vectors
+//            y_S = Linv f_S,  u_t = f_U - M f_S
+//   backward (root -> leaves): x_S = Linv^T y_S - M^T x_U
+//
+// One launch per tree level and sweep; large fronts are split into row
+// (forward) or column (backward) chunks. All sums run in a fixed order.
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+
+namespace ddx {
+namespace {
+
+constexpr int kNdThreads = 128;
+constexpr int kNdWarps = kNdThreads / 32;
+constexpr int kNdSmemMax = 96 * 1024;
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+struct NdArgs {
+  const int* items;
+  const int* front_s;
+  const int* front_u;
+  const int64_t* g_off;
+  const int64_t* idx_off;
+  const int64_t* upd_off;
+  const int* fidx;
+  const int64_t* gptr;
+  const int64_t* gsrc;
+  const double* G;
+};
+
+template <int RG>
+__global__ void __launch_bounds__(kNdThreads)
+    k_nd_fwd(NdArgs A, int64_t item0, int R, const double* __restrict__ w, double* __restrict__ y,
+             double* __restrict__ upd, const int* ist) {
+  if (ist != nullptr && n_active(ist, R) == 0) return;
+  extern __shared__ double fs[];
+  const int64_t it = item0 + blockIdx.x;
+  const int t = A.items[3 * it], row0 = A.items[3 * it + 1], nrows = A.items[3 * it + 2];
+  const int s = A.front_s[t];
+  const int64_t io = A.idx_off[t], go = A.g_off[t], uo = A.upd_off[t];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int r0 = 0; r0 < R; r0 += RG) {
+    const int ng = min(RG, R - r0);
+    // f_S = w_S + the children's contributions, in gather-map order
+    for (int p = threadIdx.x; p < s; p += kNdThreads) {
+      const int64_t v = A.fidx[io + p];
+      double acc[RG];
+#pragma unroll
+      for (int r = 0; r < RG; ++r) acc[r] = r < ng ? w[v * R + r0 + r] : 0.0;
+      for (int64_t q = A.gptr[io + p]; q < A.gptr[io + p + 1]; ++q) {
+        const int64_t src = A.gsrc[q] * R + r0;
+#pragma unroll
+        for (int r = 0; r < RG; ++r)
+          if (r < ng) acc[r] += upd[src + r];
+      }
+#pragma unroll
+      for (int r = 0; r < RG; ++r) fs[p * RG + r] = acc[r];
+    }
+    __syncthreads();
+    for (int p = row0 + warp; p < row0 + nrows; p += kNdWarps) {
+      const double* g = A.G + go + (int64_t)p * s;
+      double acc[RG];
+#pragma unroll
+      for (int r = 0; r < RG; ++r) acc[r] = 0.0;
+      for (int j = lane; j < s; j += 32) {
+        const double gv = __ldg(g + j);
+#pragma unroll
+        for (int r = 0; r < RG; ++r) acc[r] = fma(gv, fs[j * RG + r], acc[r]);
+      }
+#pragma unroll
+      for (int r = 0; r < RG; ++r) acc[r] = warp_sum_d(acc[r]);
+      if (p < s) {
+        const int64_t v = A.fidx[io + p];
+#pragma unroll
+        for (int r = 0; r < RG; ++r)
+          if (lane == r && r < ng) y[v * R + r0 + r] = acc[r];
+      } else {
+        // f_U of this row (children only), then u_t = f_U - M f_S
+        double f[RG];
+#pragma unroll
+        for (int r = 0; r < RG; ++r) f[r] = 0.0;
+        for (int64_t q = A.gptr[io + p]; q < A.gptr[io + p + 1]; ++q) {
+          const int64_t src = A.gsrc[q] * R + r0;
+#pragma unroll
+          for (int r = 0; r < RG; ++r)
+            if (r < ng) f[r] += upd[src + r];
+        }
+        const int64_t dst = (uo + p - s) * R + r0;
+#pragma unroll
+        for (int r = 0; r < RG; ++r)
+          if (lane == r && r < ng) upd[dst + r] = f[r] - acc[r];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int RG>
+__global__ void __launch_bounds__(kNdThreads)
+    k_nd_bwd(NdArgs A, int64_t item0, int R, const double* __restrict__ y, double* __restrict__ x,
+             const int* ist) {
+  if (ist != nullptr && n_active(ist, R) == 0) return;
+  extern __shared__ double vs[];
+  const int64_t it = item0 + blockIdx.x;
+  const int t = A.items[3 * it], col0 = A.items[3 * it + 1], ncols = A.items[3 * it + 2];
+  const int s = A.front_s[t], m = s + A.front_u[t];
+  const int64_t io = A.idx_off[t], go = A.g_off[t];
+  for (int r0 = 0; r0 < R; r0 += RG) {
+    const int ng = min(RG, R - r0);
+    // v = [y_S; -x_U]
+    for (int p = threadIdx.x; p < m; p += kNdThreads) {
+      const int64_t v = A.fidx[io + p];
+#pragma unroll
+      for (int r = 0; r < RG; ++r)
+        vs[p * RG + r] = r < ng ? (p < s ? y[v * R + r0 + r] : -x[v * R + r0 + r]) : 0.0;
+    }
+    __syncthreads();
+    const int c = threadIdx.x;
+    if (c < ncols) {
+      const int col = col0 + c;
+      const double* g = A.G + go + col;
+      double acc[RG];
+#pragma unroll
+      for (int r = 0; r < RG; ++r) acc[r] = 0.0;
+#pragma unroll 4
+      for (int p = 0; p < m; ++p) {
+        const double gv = __ldg(g + (int64_t)p * s);
+#pragma unroll
+        for (int r = 0; r < RG; ++r) acc[r] = fma(gv, vs[p * RG + r], acc[r]);
+      }
+      const int64_t v = A.fidx[io + col];
+#pragma unroll
+      for (int r = 0; r < RG; ++r)
+        if (r < ng) x[v * R + r0 + r] = acc[r];
+    }
+    __syncthreads();
+  }
+}
+
+template <int RG>
+int nd_sweeps(const ddx_nd_plan* P, const NdArgs& fa, const NdArgs& ba, int R, const double* w, double* x,
+              double* y, double* upd, const int* ist, cudaStream_t s) {
+  const size_t smem_cap = (size_t)kNdSmemMax;
+  cudaFuncSetAttribute(k_nd_fwd<RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap);
+  cudaFuncSetAttribute(k_nd_bwd<RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap);
+  for (int lv = 0; lv < P->n_levels; ++lv) {
+    const int64_t a = P->fwd_level_ptr[lv], b = P->fwd_level_ptr[lv + 1];
+    if (b == a) continue;
+    const size_t smem = (size_t)std::max(P->fwd_level_smax[lv], 1) * RG * sizeof(double);
+    k_nd_fwd<RG><<<(unsigned)(b - a), kNdThreads, smem, s>>>(fa, a, R, w, y, upd, ist);
+  }
+  for (int lv = 0; lv < P->n_levels; ++lv) {
+    const int64_t a = P->bwd_level_ptr[lv], b = P->bwd_level_ptr[lv + 1];
+    if (b == a) continue;
+    const size_t smem = (size_t)std::max(P->bwd_level_mmax[lv], 1) * RG * sizeof(double);
+    k_nd_bwd<RG><<<(unsigned)(b - a), kNdThreads, smem, s>>>(ba, a, R, y, x, ist);
+  }
+  DDX_LAUNCH_CHECK("ddx_coarse_solve_nd");
+  return DDX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// ordering: recursive BFS level-set bisection
+// ---------------------------------------------------------------------------
+struct NdOrder {
+  int64_t n;
+  std::vector<int64_t> ptr, adj;  // symmetric adjacency, no self loops
+  std::vector<int64_t> label;     // current subgraph label, -1 once eliminated
+  std::vector<int64_t> seen, level;
+  int64_t stamp = 0, next_label = 1;
+  int leaf;
+  int64_t* perm;
+  int64_t* node_first;
+  int64_t* node_parent;
+  int64_t n_nodes = 0, perm_len = 0;
+
+  // BFS over vertices with label == lab from src; returns the visit order
+  // and fills level[] for the visited vertices.
+  void bfs(int64_t src, int64_t lab, std::vector<int64_t>& order) {
+    ++stamp;
+    order.clear();
+    order.push_back(src);
+    seen[src] = stamp;
+    level[src] = 0;
+    for (size_t h = 0; h < order.size(); ++h) {
+      const int64_t v = order[h];
+      for (int64_t e = ptr[v]; e < ptr[v + 1]; ++e) {
+        const int64_t w = adj[e];
+        if (label[w] == lab && seen[w] != stamp) {
+          seen[w] = stamp;
+          level[w] = level[v] + 1;
+          order.push_back(w);
+        }
+      }
+    }
+  }
+
+  int64_t create(std::vector<int64_t>& S, const std::vector<int64_t>& kids) {
+    std::sort(S.begin(), S.end());
+    const int64_t id = n_nodes++;
+    node_first[id] = perm_len;
+    for (int64_t v : S) {
+      perm[perm_len++] = v;
+      label[v] = -1;
+    }
+    node_first[id + 1] = perm_len;
+    node_parent[id] = -1;
+    for (int64_t k : kids) node_parent[k] = id;
+    return id;
+  }
+
+  // Vertices V (all carrying label lab): returns the root nodes built for them.
+  std::vector<int64_t> process(std::vector<int64_t> V, int64_t lab) {
+    std::vector<int64_t> roots;
+    std::vector<std::vector<int64_t>> comps;
+    std::vector<int64_t> order;
+    for (int64_t v : V) {
+      if (label[v] != lab) continue;
+      bfs(v, lab, order);
+      const int64_t lc = next_label++;
+      for (int64_t u : order) label[u] = lc;
+      comps.push_back(order);
+    }
+    for (auto& C : comps) {
+      const int64_t lc = label[C[0]];
+      if ((int64_t)C.size() <= leaf) {
+        roots.push_back(create(C, {}));
+        continue;
+      }
+      bfs(C[0], lc, order);
+      const int64_t far = order.back();
+      bfs(far, lc, order);
+      const int64_t depth = level[order.back()];
+      if (depth < 2) {
+        roots.push_back(create(C, {}));
+        continue;
+      }
+      std::vector<int64_t> cnt(depth + 1, 0);
+      for (int64_t v : order) ++cnt[level[v]];
+      int64_t k = 0, cum = 0;
+      while (k <= depth && 2 * (cum + cnt[k]) < (int64_t)C.size()) cum += cnt[k++];
+      k = std::min(std::max(k, (int64_t)1), depth - 1);
+      std::vector<int64_t> S, Av, Bv;
+      for (int64_t v : order) {
+        if (level[v] == k) S.push_back(v);
+        else if (level[v] < k) Av.push_back(v);
+        else Bv.push_back(v);
+      }
+      const int64_t la = next_label++, lb = next_label++;
+      for (int64_t v : S) label[v] = -2;  // removed from both halves
+      for (int64_t v : Av) label[v] = la;
+      for (int64_t v : Bv) label[v] = lb;
+      std::vector<int64_t> kids = process(std::move(Av), la);
+      std::vector<int64_t> kb = process(std::move(Bv), lb);
+      kids.insert(kids.end(), kb.begin(), kb.end());
+      roots.push_back(create(S, kids));
+    }
+    return roots;
+  }
+};
+
+}  // namespace
+}  // namespace ddx
+
+using namespace ddx;
+
+extern "C" {
+
+int ddx_nd_order(int64_t n, const int64_t* indptr, const int64_t* indices, int leaf, int64_t* perm,
+                 int64_t* node_first, int64_t* node_parent, int64_t* n_nodes) {
+  DDX_REQUIRE(n >= 0 && indptr && indices && perm && node_first && node_parent && n_nodes && leaf >= 1,
+              "ddx_nd_order: bad arguments");
+  NdOrder o;
+  o.n = n;
+  o.leaf = leaf;
+  o.perm = perm;
+  o.node_first = node_first;
+  o.node_parent = node_parent;
+  // symmetrised adjacency without the diagonal
+  std::vector<int64_t> deg(n + 1, 0);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t e = indptr[i]; e < indptr[i + 1]; ++e) {
+      const int64_t j = indices[e];
+      DDX_REQUIRE(j >= 0 && j < n, "ddx_nd_order: column %lld out of range", (long long)j);
+      if (j != i) {
+        ++deg[i + 1];
+        ++deg[j + 1];
+      }
+    }
+  o.ptr.assign(n + 1, 0);
+  for (int64_t i = 0; i < n; ++i) o.ptr[i + 1] = o.ptr[i] + deg[i + 1];
+  o.adj.resize(o.ptr[n]);
+  std::vector<int64_t> fill(o.ptr.begin(), o.ptr.end() - 1);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t e = indptr[i]; e < indptr[i + 1]; ++e) {
+      const int64_t j = indices[e];
+      if (j != i) {
+        o.adj[fill[i]++] = j;
+        o.adj[fill[j]++] = i;
+      }
+    }
+  // sort and deduplicate each list (pattern given once or twice per pair)
+  std::vector<int64_t> nptr(n + 1, 0);
+  int64_t outp = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    auto b = o.adj.begin() + o.ptr[i], e = o.adj.begin() + o.ptr[i + 1];
+    std::sort(b, e);
+    auto u = std::unique(b, e);
+    nptr[i] = outp;
+    for (auto it = b; it != u; ++it) o.adj[outp++] = *it;
+  }
+  nptr[n] = outp;
+  o.adj.resize(outp);
+  o.ptr.swap(nptr);
+  o.label.assign(n, 0);
+  o.seen.assign(n, 0);
+  o.level.assign(n, 0);
+  std::vector<int64_t> all(n);
+  for (int64_t i = 0; i < n; ++i) all[i] = i;
+  node_first[0] = 0;
+  o.process(std::move(all), 0);
+  *n_nodes = o.n_nodes;
+  DDX_REQUIRE(o.perm_len == n, "ddx_nd_order: ordering incomplete (%lld of %lld)", (long long)o.perm_len,
+              (long long)n);
+  return DDX_OK;
+}
+
+int ddx_coarse_solve_nd(const ddx_nd_plan* P, int R, const double* w, double* x, double* y, double* upd,
+                        const int* ist, ddx_stream_t stream) {
+  DDX_REQUIRE(P && w && x && y && upd && R >= 1, "ddx_coarse_solve_nd: bad arguments");
+  DDX_REQUIRE(P->fwd_level_ptr && P->bwd_level_ptr && P->fwd_level_smax && P->bwd_level_mmax,
+              "ddx_coarse_solve_nd: plan without level tables");
+  if (P->n == 0) return DDX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  NdArgs fa{P->fwd_items, P->front_s, P->front_u, P->g_off, P->idx_off, P->upd_off, P->fidx, P->gptr,
+            P->gsrc, P->G};
+  NdArgs ba = fa;
+  ba.items = P->bwd_items;
+  const int64_t mmax = std::max<int64_t>(P->max_front, 1);
+  // widest RHS group whose shared-memory vector fits
+  int rg = 1;
+  while (rg < 16 && rg * 2 <= R && mmax * rg * 2 * (int64_t)sizeof(double) <= kNdSmemMax) rg *= 2;
+  DDX_REQUIRE(mmax * (int64_t)sizeof(double) <= kNdSmemMax, "ddx_coarse_solve_nd: front of %lld exceeds %d B",
+              (long long)mmax, kNdSmemMax);
+  switch (rg) {
+    case 1: return nd_sweeps<1>(P, fa, ba, R, w, x, y, upd, ist, s);
+    case 2: return nd_sweeps<2>(P, fa, ba, R, w, x, y, upd, ist, s);
+    case 4: return nd_sweeps<4>(P, fa, ba, R, w, x, y, upd, ist, s);
+    case 8: return nd_sweeps<8>(P, fa, ba, R, w, x, y, upd, ist, s);
+    default: return nd_sweeps<16>(P, fa, ba, R, w, x, y, upd, ist, s);
+  }
+}
+
+}  // extern "C"

@@ -1,17 +1,24 @@
 """SPD factorisation with the interface of ``dd_solvers.cudss``
 (src/dd_solvers/dd_solvers/cudss.py:1-44; src/dd_solvers/cpp/cudss.cpp:34-105).
 
-cuDSS is absent from this image. ``spd_factorize`` instead factors the (small,
-coarse) matrix densely in FP64 with cuSOLVER's Cholesky (``torch.linalg.cholesky``),
-forms the explicit symmetric inverse once, and ``solve`` applies it with the
-HBM-bound ``ddx_coarse_gemv_f64`` kernel. The batched variant factors each
-matrix of a block-diagonal batch the same way.
+cuDSS is absent from this image. ``spd_factorize`` replaces it in two ways:
+
+* up to ``DENSE_MAX`` rows, a dense FP64 Cholesky (cuSOLVER through
+  ``torch.linalg.cholesky``) turned once into the explicit symmetric inverse,
+  applied by the HBM-bound ``ddx_coarse_gemv_f64`` kernel;
+* above that, the nested-dissection multifrontal factorisation of ``nd.py``,
+  applied by ``ddx_coarse_solve_nd`` (two GEMV sweeps over the tree levels).
+
+The batched variant factors each matrix of a block-diagonal batch the same way.
 """
 from __future__ import annotations
 
 import torch
 
 from . import _lib as L
+from . import nd
+
+DENSE_MAX = 8192  # largest coarse size solved with a dense explicit inverse
 
 __all__ = ["CudssSolver", "spd_factorize", "CudssBatchSolver", "spd_batch_factorize"]
 
@@ -31,6 +38,11 @@ class CudssSolver:
         self.dtype = dtype
         self.n = inverse.shape[0]
 
+    def solve_into(self, w: torch.Tensor, y: torch.Tensor, R: int, ist=None) -> None:
+        """``y = A^-1 w`` for ``(n, R)`` FP64 device blocks, no allocation."""
+        L.call("ddx_coarse_gemv_f64", self.n, R, L.ptr(self.inverse), L.ptr(w), L.ptr(y), L.ptr(ist),
+               L.stream_ptr())
+
     def solve(self, rhs: torch.Tensor) -> torch.Tensor:
         L.require_cuda(rhs, "rhs")
         R = 1 if rhs.dim() == 1 else rhs.shape[1]
@@ -48,9 +60,13 @@ class CudssSolver:
         return y.to(rhs.dtype)
 
 
-def spd_factorize(A: torch.Tensor) -> CudssSolver:
+def spd_factorize(A: torch.Tensor):
+    """Factor an SPD CSR matrix on the device; the result has ``solve(rhs)``
+    and ``solve_into(w, y, R, ist)``."""
     L.require_cuda(A, "A")
-    return CudssSolver(_dense_inverse(A), A.dtype)
+    if A.shape[0] <= DENSE_MAX:
+        return CudssSolver(_dense_inverse(A), A.dtype)
+    return nd.NDSolver(A.to(torch.float64))
 
 
 class CudssBatchSolver:

@@ -1,0 +1,448 @@
+"""Sparse SPD direct solver for large coarse problems: nested dissection +
+multifrontal Cholesky, applied by per-level GEMV kernels.
+
+The reference factors its coarse matrix ``A_C = R0 A R0^T`` once with cuDSS
+(``src/dd_solvers/dd_solvers/solvers.py:85-113``, ``cpp/cudss.cpp:64-105``) and
+calls the cuDSS solve in every preconditioner application. Its experiments use
+coarse spaces of 65k-1M DOFs (P0 on the ``S8``-``S10`` / ``C8``-``C10`` meshes),
+far beyond a dense inverse. cuDSS is not in this image; this module is the
+replacement for those sizes.
+
+Setup (host symbolic phase, device numeric phase):
+
+1. *Ordering.* Recursive vertex bisection of the matrix graph: a BFS from a
+   pseudo-peripheral vertex, the median level set as the separator, each
+   connected component handled on its own, down to leaves of at most
+   ``leaf`` vertices. The separator tree in post-order is the elimination
+   order (subtrees first, then their separator).
+2. *Symbolic.* Front ``t`` holds its separator ``S_t`` followed by its update
+   set ``U_t`` = the later-eliminated vertices coupled to the subtree
+   (``adj(S_t)`` plus the children's update sets, restricted to ancestors).
+3. *Numeric.* Level by level from the leaves, a padded batch of dense fronts
+   is assembled from ``A`` and the children's update matrices (extend-add,
+   one child slot at a time so no two additions meet), then
+   ``L = chol(F_SS)``, ``Linv = L^-1``, ``M = F_US F_SS^-1`` and the update
+   ``F_UU - F_US F_SS^-1 F_SU``. The stored operator of front ``t`` is
+   ``G_t = [Linv; M]`` (``(s+u) x s``, row-major, FP64).
+
+Solve (``ddx_coarse_solve_nd``, one forward launch and one backward launch per
+tree level):
+
+* forward, leaves to root: ``f = [w_S; 0] + sum of the children's update
+  vectors`` (fixed order), ``y_S = Linv f_S``, ``u_t = f_U - M f_S``;
+* backward, root to leaves: ``x_S = Linv^T y_S - M^T x_U``.
+
+Both are dense GEMVs over ``G_t``, split into row (forward) or column
+(backward) chunks so that large fronts spread over many CTAs; every sum is in
+a fixed order, so results are deterministic.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+FWD_ROWS = 64    # rows of G per forward work item
+BWD_COLS = 128   # columns of G per backward work item
+
+
+# ---------------------------------------------------------------------------
+# ordering
+# ---------------------------------------------------------------------------
+
+def nested_dissection(indptr: np.ndarray, indices: np.ndarray, n: int, leaf: int = 128):
+    """Separator tree of the graph of an ``n x n`` symmetric pattern, from the
+    native ``ddx_nd_order``. Returns ``(S, parent)`` in post-order: ``S[t]``
+    the vertices node ``t`` eliminates, ``parent[t]`` its parent (-1: root)."""
+    indptr = np.ascontiguousarray(indptr, dtype=np.int64)
+    indices = np.ascontiguousarray(indices, dtype=np.int64)
+    perm = np.empty(max(n, 1), dtype=np.int64)
+    first = np.empty(n + 2, dtype=np.int64)
+    parent = np.empty(n + 1, dtype=np.int64)
+    count = np.zeros(1, dtype=np.int64)
+    L.call("ddx_nd_order", n, indptr.ctypes.data, indices.ctypes.data, int(leaf), perm.ctypes.data,
+           first.ctypes.data, parent.ctypes.data, count.ctypes.data)
+    nf = int(count[0])
+    S = [perm[first[t]:first[t + 1]].copy() for t in range(nf)]
+    return S, parent[:nf].copy()
+
+
+# ---------------------------------------------------------------------------
+# symbolic analysis
+# ---------------------------------------------------------------------------
+
+class NDSymbolic:
+    """Fronts in post-order with their index sets, levels and gather maps."""
+
+    def __init__(self, indptr, indices, n: int, leaf: int = 128):
+        S, parent = nested_dissection(indptr, indices, n, leaf)
+        indptr = np.asarray(indptr, dtype=np.int64)
+        indices = np.asarray(indices, dtype=np.int64)
+        nf = len(S)
+        children = [[] for _ in range(nf)]
+        for t in range(nf):
+            if parent[t] >= 0:
+                children[parent[t]].append(t)
+        perm = np.concatenate(S) if nf else np.zeros(0, dtype=np.int64)
+        pos = np.empty(n, dtype=np.int64)
+        pos[perm] = np.arange(n)
+        s_sizes = np.array([len(x) for x in S], dtype=np.int64)
+        s_first = np.concatenate([[0], np.cumsum(s_sizes)[:-1]])
+        s_last = s_first + s_sizes - 1
+        # subtree_last = last position in the subtree = own S last (post-order)
+        U: list = [None] * nf
+        for t in range(nf):
+            nb = [indices[indptr[v]:indptr[v + 1]] for v in S[t]]
+            cand = [np.concatenate(nb)] + [U[c] for c in children[t]]
+            c = np.unique(pos[np.concatenate(cand)]) if cand else np.zeros(0, dtype=np.int64)
+            U[t] = perm[c[c > s_last[t]]]
+        level = np.zeros(nf, dtype=np.int64)
+        for t in range(nf):
+            if children[t]:
+                level[t] = 1 + max(level[c] for c in children[t])
+        self.n, self.nf = n, nf
+        self.S, self.U, self.children, self.parent = S, U, children, parent
+        self.perm, self.pos = perm, pos
+        self.level = level
+        self.n_levels = int(level.max()) + 1 if nf else 0
+        self.s = s_sizes
+        self.u = np.array([len(x) for x in U], dtype=np.int64)
+        m = self.s + self.u
+        self.idx_off = np.concatenate([[0], np.cumsum(m)[:-1]]).astype(np.int64)
+        self.g_off = np.concatenate([[0], np.cumsum(m * self.s)[:-1]]).astype(np.int64)
+        self.upd_off = np.concatenate([[0], np.cumsum(self.u)[:-1]]).astype(np.int64)
+        self.g_total = int((m * self.s).sum())
+        self.upd_total = int(self.u.sum())
+        self.fidx = np.concatenate([np.concatenate([S[t], U[t]]) for t in range(nf)]).astype(np.int64)
+        # extend-add positions of each child's update set inside its parent's front
+        self.rel = [None] * nf
+        for t in range(nf):
+            p = parent[t]
+            if p < 0:
+                assert self.u[t] == 0
+                continue
+            fp = pos[np.concatenate([S[p], U[p]])]
+            r = np.searchsorted(fp, pos[U[t]])
+            assert np.array_equal(fp[r], pos[U[t]]), "update set not inside the parent front"
+            self.rel[t] = r
+        # gather map: per front position, the update-buffer entries to add (children in order)
+        gp, gs = [], []
+        for t in range(nf):
+            p = parent[t]
+            if p < 0:
+                continue
+            gp.append(self.idx_off[p] + self.rel[t])
+            gs.append(self.upd_off[t] + np.arange(self.u[t]))
+        total = int(m.sum())
+        if gp:
+            gp = np.concatenate(gp)
+            gs = np.concatenate(gs)
+            order = np.argsort(gp, kind="stable")
+            gp, gs = gp[order], gs[order]
+        else:
+            gp = gs = np.zeros(0, dtype=np.int64)
+        self.gptr = np.zeros(total + 1, dtype=np.int64)
+        np.add.at(self.gptr, gp + 1, 1)
+        self.gptr = np.cumsum(self.gptr)
+        self.gsrc = gs.astype(np.int64)
+        # per-level work items
+        fwd, bwd = [], []
+        self.fwd_level_ptr = np.zeros(self.n_levels + 1, dtype=np.int64)
+        self.bwd_level_ptr = np.zeros(self.n_levels + 1, dtype=np.int64)
+        by_level = [np.nonzero(level == lv)[0] for lv in range(self.n_levels)]
+        for lv in range(self.n_levels):
+            for t in by_level[lv]:
+                rows = int(m[t])
+                for r0 in range(0, max(rows, 1), FWD_ROWS):
+                    fwd.append((t, r0, min(FWD_ROWS, rows - r0)))
+            self.fwd_level_ptr[lv + 1] = len(fwd)
+        # backward runs the levels from the top; items are stored in that order
+        for j, lv in enumerate(range(self.n_levels - 1, -1, -1)):
+            for t in by_level[lv]:
+                cols = int(self.s[t])
+                for c0 in range(0, cols, BWD_COLS):
+                    bwd.append((t, c0, min(BWD_COLS, cols - c0)))
+            self.bwd_level_ptr[j + 1] = len(bwd)
+        m_all = self.s + self.u
+        self.fwd_level_smax = np.array([int(self.s[f].max()) if len(f) else 0 for f in by_level], dtype=np.int32)
+        self.bwd_level_mmax = np.array([int(m_all[f].max()) if len(f) else 0 for f in by_level[::-1]],
+                                       dtype=np.int32)
+        self.fwd_items = np.array(fwd, dtype=np.int32).reshape(-1, 3)
+        self.bwd_items = np.array(bwd, dtype=np.int32).reshape(-1, 3)
+        self.by_level = by_level
+
+
+# ---------------------------------------------------------------------------
+# numeric factorisation (torch, any device)
+# ---------------------------------------------------------------------------
+
+def factorize(sym: NDSymbolic, indptr, indices, values, device, max_batch_bytes: int = 1 << 30) -> torch.Tensor:
+    """The stored operators ``G_t = [Linv; M]`` of every front, concatenated."""
+    indptr = np.asarray(indptr, dtype=np.int64)
+    indices = np.asarray(indices, dtype=np.int64)
+    vals = torch.as_tensor(np.asarray(values, dtype=np.float64)) if not isinstance(values, torch.Tensor) \
+        else values.to(torch.float64)
+    vals = vals.to(device)
+    n = sym.n
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(indptr))
+    front_of = np.empty(n, dtype=np.int64)
+    for t in range(sym.nf):
+        front_of[sym.S[t]] = t
+    # original entries (i in S_t, j in S_t or U_t): kept where pos(j) >= first position of S_t
+    t_of = front_of[rows]
+    first = np.array([sym.pos[x[0]] for x in sym.S], dtype=np.int64)
+    keep = sym.pos[indices] >= first[t_of]
+    e_t = t_of[keep]
+    e_i, e_j = rows[keep], indices[keep]
+    e_v = np.nonzero(keep)[0]
+    # local index of each vertex inside front t: position in [S_t, U_t]
+    li = sym.pos[e_i] - first[e_t]
+    fpos_cache = {}
+
+    def local(t, verts_pos):
+        fp = fpos_cache.get(t)
+        if fp is None:
+            fp = sym.pos[np.concatenate([sym.S[t], sym.U[t]])]
+            fpos_cache[t] = fp
+        return np.searchsorted(fp, verts_pos)
+
+    # group entries by front for assembly
+    order = np.argsort(e_t, kind="stable")
+    e_t, e_i, e_j, e_v, li = e_t[order], e_i[order], e_j[order], e_v[order], li[order]
+    bounds = np.searchsorted(e_t, np.arange(sym.nf + 1))
+    lj = np.empty_like(li)
+    for t in range(sym.nf):
+        a, b = bounds[t], bounds[t + 1]
+        if b > a:
+            lj[a:b] = local(t, sym.pos[e_j[a:b]])
+    in_s = lj < sym.s[e_t]
+
+    G = torch.zeros(sym.g_total, dtype=torch.float64, device=device)
+    upd = {}  # front -> (batch tensor, batch index, S_MAX) of its pending update matrix
+    for lv in range(sym.n_levels):
+        fronts = sym.by_level[lv]
+        # chunk the level so a padded batch stays within max_batch_bytes
+        sz = sym.s[fronts] + sym.u[fronts]
+        chunks, cur, cur_max = [], [], 0
+        for t, z in zip(fronts, sz):
+            mm = max(cur_max, int(z))
+            if cur and (len(cur) + 1) * (mm + 1) ** 2 * 8 > max_batch_bytes:
+                chunks.append(cur)
+                cur, mm = [], int(z)
+            cur.append(int(t))
+            cur_max = mm
+        if cur:
+            chunks.append(cur)
+        for ch in chunks:
+            ch = np.array(ch, dtype=np.int64)
+            B = len(ch)
+            SM = int(sym.s[ch].max())
+            UM = int(sym.u[ch].max())
+            m = SM + UM
+            F = torch.zeros(B, m, m, dtype=torch.float64, device=device)
+            # identity on the padded separator diagonal
+            pad_b, pad_i = [], []
+            for b, t in enumerate(ch):
+                if sym.s[t] < SM:
+                    ii = np.arange(sym.s[t], SM)
+                    pad_b.append(np.full(len(ii), b))
+                    pad_i.append(ii)
+            if pad_b:
+                pb = torch.as_tensor(np.concatenate(pad_b), device=device)
+                pi = torch.as_tensor(np.concatenate(pad_i), device=device)
+                F[pb, pi, pi] = 1.0
+            # original entries
+            sel = np.concatenate([np.arange(bounds[t], bounds[t + 1]) for t in ch])
+            if len(sel):
+                bmap = np.empty(sym.nf, dtype=np.int64)
+                bmap[ch] = np.arange(B)
+                bb = bmap[e_t[sel]]
+                r = li[sel]
+                c = lj[sel]
+                c_pad = np.where(in_s[sel], c, SM + (c - sym.s[e_t[sel]]))
+                vv = vals[torch.as_tensor(e_v[sel], device=device)]
+                bbt = torch.as_tensor(bb, device=device)
+                rt = torch.as_tensor(r, device=device)
+                ct = torch.as_tensor(c_pad, device=device)
+                F[bbt, rt, ct] = vv
+                us = ~in_s[sel]
+                if us.any():
+                    F[bbt[torch.as_tensor(us, device=device)], ct[torch.as_tensor(us, device=device)],
+                      rt[torch.as_tensor(us, device=device)]] = vv[torch.as_tensor(us, device=device)]
+            # extend-add of the children's updates, one child slot at a time
+            nslots = max((len(sym.children[t]) for t in ch), default=0)
+            for slot in range(nslots):
+                groups = {}
+                for b, t in enumerate(ch):
+                    if slot < len(sym.children[t]):
+                        c = sym.children[t][slot]
+                        Ub, ub_i, USM = upd[c]
+                        groups.setdefault(id(Ub), (Ub, USM, []))[2].append((b, t, c, ub_i))
+                for Ub, USM, items in groups.values():
+                    dst, src = [], []
+                    for b, t, c, ub_i in items:
+                        uc = int(sym.u[c])
+                        if uc == 0:
+                            continue
+                        rel = sym.rel[c]
+                        rel_pad = np.where(rel < sym.s[t], rel, SM + (rel - sym.s[t]))
+                        ii, jj = np.meshgrid(rel_pad, rel_pad, indexing="ij")
+                        dst.append(b * m * m + ii.reshape(-1) * m + jj.reshape(-1))
+                        um = Ub.shape[1]
+                        a = np.arange(uc)
+                        si, sj = np.meshgrid(a, a, indexing="ij")
+                        src.append(ub_i * um * um + si.reshape(-1) * um + sj.reshape(-1))
+                    if dst:
+                        d = torch.as_tensor(np.concatenate(dst), device=device)
+                        s_ = torch.as_tensor(np.concatenate(src), device=device)
+                        F.view(-1).index_put_((d,), Ub.reshape(-1)[s_], accumulate=True)
+                for b, t in enumerate(ch):
+                    if slot < len(sym.children[t]):
+                        upd.pop(sym.children[t][slot], None)
+            Fss = F[:, :SM, :SM]
+            Lc, info = torch.linalg.cholesky_ex(Fss)
+            if int(info.abs().max()) != 0:
+                raise RuntimeError("coarse matrix is not positive definite")
+            eye = torch.eye(SM, dtype=torch.float64, device=device).expand(B, SM, SM)
+            Linv = torch.linalg.solve_triangular(Lc, eye, upper=False)
+            del Lc, eye
+            if UM:
+                Fus = F[:, SM:, :SM]
+                W = Fus @ Linv.transpose(1, 2)
+                M = W @ Linv
+                Upd = F[:, SM:, SM:] - W @ W.transpose(1, 2)
+                del W
+            else:
+                M = Upd = None
+            # store G_t = [Linv; M] (unpadded, row-major)
+            for b, t in enumerate(ch):
+                s_t, u_t = int(sym.s[t]), int(sym.u[t])
+                o = int(sym.g_off[t])
+                G[o:o + s_t * s_t] = Linv[b, :s_t, :s_t].reshape(-1)
+                if u_t:
+                    G[o + s_t * s_t:o + (s_t + u_t) * s_t] = M[b, :u_t, :s_t].reshape(-1)
+            if Upd is not None:
+                for b, t in enumerate(ch):
+                    if sym.parent[t] >= 0:
+                        upd[int(t)] = (Upd, b, SM)
+            del F, Linv, M
+    return G
+
+
+# ---------------------------------------------------------------------------
+# the plan handed to the kernels
+# ---------------------------------------------------------------------------
+
+class _Plan(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int), ("n_fronts", ctypes.c_int), ("n_levels", ctypes.c_int),
+        ("max_front", ctypes.c_int),
+        ("fwd_level_ptr", ctypes.c_void_p), ("bwd_level_ptr", ctypes.c_void_p),
+        ("fwd_level_smax", ctypes.c_void_p), ("bwd_level_mmax", ctypes.c_void_p),
+        ("fwd_items", ctypes.c_void_p), ("bwd_items", ctypes.c_void_p),
+        ("front_s", ctypes.c_void_p), ("front_u", ctypes.c_void_p),
+        ("g_off", ctypes.c_void_p), ("idx_off", ctypes.c_void_p), ("upd_off", ctypes.c_void_p),
+        ("fidx", ctypes.c_void_p), ("gptr", ctypes.c_void_p), ("gsrc", ctypes.c_void_p),
+        ("G", ctypes.c_void_p),
+    ]
+
+
+class NDSolver:
+    """Factor once (``A`` a torch CSR tensor on the device, FP64), then
+    ``solve_into(w, x, R)`` with ``w, x`` (n, R) row-major FP64 on the device."""
+
+    def __init__(self, A: torch.Tensor, leaf: int = 128):
+        dev = A.device
+        indptr = A.crow_indices().cpu().numpy()
+        indices = A.col_indices().cpu().numpy()
+        self.n = A.shape[0]
+        self.sym = sym = NDSymbolic(indptr, indices, self.n, leaf)
+        self.G = factorize(sym, indptr, indices, A.values(), dev)
+        i32 = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.int32, device=dev)  # noqa: E731
+        i64 = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.int64, device=dev)  # noqa: E731
+        self.t = {
+            "fwd_items": i32(sym.fwd_items.reshape(-1)), "bwd_items": i32(sym.bwd_items.reshape(-1)),
+            "front_s": i32(sym.s), "front_u": i32(sym.u),
+            "g_off": i64(sym.g_off), "idx_off": i64(sym.idx_off), "upd_off": i64(sym.upd_off),
+            "fidx": i32(sym.fidx), "gptr": i64(sym.gptr), "gsrc": i64(sym.gsrc),
+        }
+        self.fwd_level_ptr = np.ascontiguousarray(sym.fwd_level_ptr, dtype=np.int64)
+        self.bwd_level_ptr = np.ascontiguousarray(sym.bwd_level_ptr, dtype=np.int64)
+        self.fwd_level_smax = np.ascontiguousarray(sym.fwd_level_smax, dtype=np.int32)
+        self.bwd_level_mmax = np.ascontiguousarray(sym.bwd_level_mmax, dtype=np.int32)
+        self.max_front = int((sym.s + sym.u).max()) if sym.nf else 0
+        p = _Plan()
+        p.n, p.n_fronts, p.n_levels, p.max_front = self.n, sym.nf, sym.n_levels, self.max_front
+        p.fwd_level_ptr = self.fwd_level_ptr.ctypes.data
+        p.bwd_level_ptr = self.bwd_level_ptr.ctypes.data
+        p.fwd_level_smax = self.fwd_level_smax.ctypes.data
+        p.bwd_level_mmax = self.bwd_level_mmax.ctypes.data
+        for k, v in self.t.items():
+            setattr(p, k, v.data_ptr())
+        p.G = self.G.data_ptr()
+        self.plan = p
+        self._work = {}
+        self.factor_bytes = self.G.numel() * 8
+
+    def workspace(self, R: int, device):
+        w = self._work.get(R)
+        if w is None:
+            w = {"y": torch.empty(self.n * R, dtype=torch.float64, device=device),
+                 "upd": torch.empty(max(self.sym.upd_total, 1) * R, dtype=torch.float64, device=device)}
+            self._work[R] = w
+        return w
+
+    def solve_into(self, w: torch.Tensor, x: torch.Tensor, R: int, ist=None) -> None:
+        ws = self.workspace(R, w.device)
+        L.call("ddx_coarse_solve_nd", ctypes.addressof(self.plan), R, L.ptr(w), L.ptr(x), L.ptr(ws["y"]),
+               L.ptr(ws["upd"]), L.ptr(ist), L.stream_ptr())
+
+    def solve(self, rhs: torch.Tensor) -> torch.Tensor:
+        L.require_cuda(rhs, "rhs")
+        R = 1 if rhs.dim() == 1 else rhs.shape[1]
+        w = rhs.to(torch.float64).contiguous()
+        x = torch.empty_like(w)
+        self.solve_into(w, x, R)
+        return x.to(rhs.dtype)
+
+
+def emulate_solve(sym: NDSymbolic, G: np.ndarray, w: np.ndarray) -> np.ndarray:
+    """The kernels' arithmetic on the host, work item by work item (test use:
+    it follows the same index maps and level order as ``ddx_coarse_solve_nd``)."""
+    n = sym.n
+    w = np.asarray(w, dtype=np.float64).reshape(n, -1)
+    R = w.shape[1]
+    y = np.zeros((n, R))
+    x = np.zeros((n, R))
+    upd = np.zeros((max(sym.upd_total, 1), R))
+    for lv in range(sym.n_levels):
+        for it in range(sym.fwd_level_ptr[lv], sym.fwd_level_ptr[lv + 1]):
+            t, r0, nr = sym.fwd_items[it]
+            s, u = int(sym.s[t]), int(sym.u[t])
+            io, go = int(sym.idx_off[t]), int(sym.g_off[t])
+            f = np.zeros((s + u, R))
+            for p in range(s + u):
+                acc = w[sym.fidx[io + p]].copy() if p < s else np.zeros(R)
+                for q in range(sym.gptr[io + p], sym.gptr[io + p + 1]):
+                    acc = acc + upd[sym.gsrc[q]]
+                f[p] = acc
+            Gt = G[go:go + (s + u) * s].reshape(s + u, s)
+            for p in range(r0, r0 + nr):
+                out = Gt[p] @ f[:s] if s else np.zeros(R)
+                if p < s:
+                    y[sym.fidx[io + p]] = out
+                else:
+                    upd[sym.upd_off[t] + p - s] = f[p] - out
+    for j in range(sym.n_levels):
+        for it in range(sym.bwd_level_ptr[j], sym.bwd_level_ptr[j + 1]):
+            t, c0, nc = sym.bwd_items[it]
+            s, u = int(sym.s[t]), int(sym.u[t])
+            io, go = int(sym.idx_off[t]), int(sym.g_off[t])
+            v = np.concatenate([y[sym.fidx[io:io + s]], -x[sym.fidx[io + s:io + s + u]]])
+            Gt = G[go:go + (s + u) * s].reshape(s + u, s)
+            for c in range(c0, c0 + nc):
+                x[sym.fidx[io + c]] = Gt[:, c] @ v
+    return x

@@ -112,10 +112,13 @@ class SparseSolver(ABC):
 class CUDSS(SparseSolver):
     """SPD coarse solver with the reference's ``CUDSS`` interface (85-113).
 
-    cuDSS is not installed in this image, so the factorisation is a dense FP64
-    Cholesky (cuSOLVER through ``torch.linalg.cholesky``) turned once into the
-    explicit inverse; each solve is one HBM-bound ``ddx_coarse_gemv_f64``
-    launch (coarse sizes here are at most a few thousand).
+    cuDSS is not installed in this image. Up to ``cudss.DENSE_MAX`` rows the
+    factorisation is a dense FP64 Cholesky (cuSOLVER through
+    ``torch.linalg.cholesky``) turned once into the explicit inverse, and each
+    solve is one HBM-bound ``ddx_coarse_gemv_f64`` launch. Larger coarse
+    matrices (the reference's experiments use 65k-1M coarse DOFs) get the
+    nested-dissection multifrontal factorisation of ``nd.py``, solved by
+    ``ddx_coarse_solve_nd``.
     """
 
     def __str__(self):
@@ -132,10 +135,6 @@ class CUDSS(SparseSolver):
         assert rhs.is_cuda
         assert rhs.dtype == self.dtype
         return self.solver.solve(rhs), {}
-
-    @property
-    def inverse(self) -> torch.Tensor:
-        return self.solver.inverse
 
     def destroy(self):
         self.solver = None
@@ -655,8 +654,7 @@ class SchwarzOperator(SparseSolver):
 
     def _coarse(self, w, yc, R, ist=None):
         if self._fused_coarse:
-            L.call("ddx_coarse_gemv_f64", self.n_coarse, R, L.ptr(self.coarse_solver.inverse), L.ptr(w),
-                   L.ptr(yc), L.ptr(ist), L.stream_ptr())
+            self.coarse_solver.solver.solve_into(w, yc, R, ist)
         else:
             out, _ = self.coarse_solver.solve(w.view(self.n_coarse, R).squeeze(-1) if R == 1 else
                                               w.view(self.n_coarse, R))

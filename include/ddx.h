@@ -260,6 +260,60 @@ int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src
 int ddx_coarse_gemv_f64(int n_c, int R, const double* Ainv, const double* w, double* yc,
                         const int* ist, ddx_stream_t stream);
 
+/* ---- Sparse coarse solve (cuDSS replacement for large coarse spaces) ------
+ * Replaces cudssExecute(FACTORIZATION / SOLVE) behind CudssSolver
+ * (src/dd_solvers/cpp/cudss.cpp:64-105, called from solvers.py:85-113) when
+ * the coarse matrix is too large for a dense inverse.
+ *
+ * ddx_nd_order (host memory, host computation): nested-dissection ordering of
+ * the symmetric pattern (indptr, indices) of an n x n matrix by recursive BFS
+ * level-set bisection down to leaves of at most `leaf` vertices. Writes the
+ * separator tree in post-order: node t eliminates perm[node_first[t] ..
+ * node_first[t+1]), its parent is node_parent[t] (-1 for a root); *n_nodes
+ * receives the node count. perm holds n entries; node_first and node_parent
+ * need room for n + 1 entries. */
+int ddx_nd_order(int64_t n, const int64_t* indptr, const int64_t* indices, int leaf, int64_t* perm,
+                 int64_t* node_first, int64_t* node_parent, int64_t* n_nodes);
+
+/* Multifrontal solve plan. Front t owns the (s_t + u_t) coarse indices
+ * fidx[idx_off[t] ...] (its separator, then its update set) and the operator
+ * G[g_off[t] ...] = [chol(F_SS)^-1; F_US F_SS^-1] ((s_t+u_t) x s_t, row-major).
+ * Its update vector lives at upd[upd_off[t] ...] (u_t rows of R values).
+ * gptr/gsrc list, for every front position (idx_off numbering), the update
+ * rows of its children to add, in a fixed order. Work items are int triples
+ * (front, first row/column, count); fwd_level_ptr / bwd_level_ptr (HOST
+ * arrays, n_levels + 1 entries) delimit the items of each level (leaves first
+ * for the forward sweep, root first for the backward sweep), and
+ * fwd_level_smax / bwd_level_mmax (HOST) give each level's largest s and
+ * s + u. All other pointers are device memory. */
+typedef struct ddx_nd_plan {
+  int n;
+  int n_fronts;
+  int n_levels;
+  int max_front;
+  const int64_t* fwd_level_ptr;
+  const int64_t* bwd_level_ptr;
+  const int* fwd_level_smax;
+  const int* bwd_level_mmax;
+  const int* fwd_items;
+  const int* bwd_items;
+  const int* front_s;
+  const int* front_u;
+  const int64_t* g_off;
+  const int64_t* idx_off;
+  const int64_t* upd_off;
+  const int* fidx;
+  const int64_t* gptr;
+  const int64_t* gsrc;
+  const double* G;
+} ddx_nd_plan;
+
+/* x = A^-1 w for w, x of shape (n, R) (DOF-major, FP64). y (n*R doubles) and
+ * upd (sum_t u_t * R doubles) are caller-owned scratch. With ist (PCG state),
+ * nothing runs once every right-hand side has converged. Deterministic. */
+int ddx_coarse_solve_nd(const ddx_nd_plan* plan, int R, const double* w, double* x, double* y, double* upd,
+                        const int* ist, ddx_stream_t stream);
+
 /* ---- Differentiable solve -----------------------------------------------
  * No counterpart in the reference (it has no autograd). Per-cell coefficient
  * gradient of a Q1 diffusion solve on a uniform n_el^dim grid:

@@ -1,0 +1,105 @@
+"""Nested-dissection multifrontal coarse solver: ordering, symbolic analysis
+and numeric factorisation on the host, and the solve kernels' arithmetic
+emulated item by item (``nd.emulate_solve``) against SciPy's sparse LU."""
+import os
+import sys
+
+import numpy as np
+import pytest
+import scipy.sparse as sps
+import scipy.sparse.linalg as spla
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+from dd_solvers_b200 import dg, nd  # noqa: E402
+
+
+def lap2d(k, shift=0.01):
+    T = sps.diags([-1, 2, -1], [-1, 0, 1], shape=(k, k))
+    return (sps.kron(sps.eye(k), T) + sps.kron(T, sps.eye(k)) + shift * sps.eye(k * k)).tocsr()
+
+
+def random_spd(n, density, seed):
+    B = sps.random(n, n, density=density, random_state=seed)
+    return (B + B.T + 10 * sps.eye(n)).tocsr()
+
+
+def dg_p0_coarse(m, solver_level):
+    s = dg.sipg_p1(dg.uniform_mesh_2d(m))
+    A = sps.csr_matrix((s.matrix.values().numpy(), s.matrix.col_indices().numpy(),
+                        s.matrix.crow_indices().numpy()), shape=tuple(s.matrix.shape))
+    n = A.shape[0]
+    k = 3 * 4 ** (m - solver_level)
+    R0 = sps.csr_matrix((np.ones(n), (np.arange(n) // k, np.arange(n))), shape=(n // k, n))
+    return (R0 @ A @ R0.T).tocsr()
+
+
+CASES = {
+    "grid20": lambda: lap2d(20),
+    "grid45": lambda: lap2d(45),
+    "random_disconnected": lambda: random_spd(300, 0.01, 1),
+    "dg_p0_S7_on_S4": lambda: dg_p0_coarse(7, 4),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("leaf", [8, 64])
+def test_emulated_solve_matches_sparse_lu(case, leaf):
+    A = CASES[case]()
+    A.sort_indices()
+    sym = nd.NDSymbolic(A.indptr, A.indices, A.shape[0], leaf)
+    G = nd.factorize(sym, A.indptr, A.indices, A.data, "cpu").numpy()
+    w = np.random.default_rng(0).standard_normal((A.shape[0], 3))
+    x = nd.emulate_solve(sym, G, w)
+    ref = spla.splu(A.tocsc()).solve(w)
+    assert np.abs(x - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_ordering_is_a_postorder_separator_tree(case):
+    A = CASES[case]()
+    n = A.shape[0]
+    S, parent = nd.nested_dissection(A.indptr, A.indices, n, 16)
+    perm = np.concatenate(S)
+    assert np.array_equal(np.sort(perm), np.arange(n))
+    nf = len(S)
+    assert all(parent[t] == -1 or parent[t] > t for t in range(nf))  # children first
+    # no edge joins two different subtrees without passing an ancestor: an
+    # edge (i, j) is allowed only if one endpoint's node is an ancestor of
+    # (or equal to) the other's
+    node_of = np.empty(n, dtype=np.int64)
+    for t, s in enumerate(S):
+        node_of[s] = t
+
+    def ancestors(t):
+        out = set()
+        while t >= 0:
+            out.add(t)
+            t = parent[t]
+        return out
+
+    anc = [ancestors(t) for t in range(nf)]
+    coo = A.tocoo()
+    for i, j in zip(coo.row, coo.col):
+        a, b = node_of[i], node_of[j]
+        assert a in anc[b] or b in anc[a]
+
+
+def test_symbolic_front_sets():
+    A = lap2d(30)
+    sym = nd.NDSymbolic(A.indptr, A.indices, A.shape[0], 32)
+    for t in range(sym.nf):
+        assert len(sym.S[t]) >= 1
+        # the update set follows the separator in elimination order
+        if len(sym.U[t]):
+            assert sym.pos[sym.U[t]].min() > sym.pos[sym.S[t]].max()
+        if sym.parent[t] < 0:
+            assert len(sym.U[t]) == 0
+    # every forward item covers its front's rows exactly once
+    rows = {}
+    for t, r0, nr in sym.fwd_items:
+        rows.setdefault(int(t), []).append((int(r0), int(nr)))
+    for t in range(sym.nf):
+        cover = sorted(rows[t])
+        assert cover[0][0] == 0 and sum(nr for _, nr in cover) == sym.s[t] + sym.u[t]
