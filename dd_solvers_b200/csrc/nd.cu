@@ -23,9 +23,10 @@
 namespace ddx {
 namespace {
 
-constexpr int kNdThreads = 128;
+constexpr int kNdThreads = 256;
 constexpr int kNdWarps = kNdThreads / 32;
-constexpr int kNdSmemMax = 96 * 1024;
+constexpr int kNdSmemMax = 96 * 1024;  // the staged vector (front rows x RHS group)
+constexpr int kNdCols = 32;            // columns per backward work item (one per lane)
 
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
@@ -113,16 +114,20 @@ __global__ void __launch_bounds__(kNdThreads)
   }
 }
 
+// Backward item: up to 32 columns of G_t (one per lane); the 8 warps take the
+// rows p = warp, warp + 8, ... and their partial sums are added in warp order.
 template <int RG>
 __global__ void __launch_bounds__(kNdThreads)
     k_nd_bwd(NdArgs A, int64_t item0, int R, const double* __restrict__ y, double* __restrict__ x,
              const int* ist) {
   if (ist != nullptr && n_active(ist, R) == 0) return;
   extern __shared__ double vs[];
+  __shared__ double red[kNdWarps][RG][kNdCols];
   const int64_t it = item0 + blockIdx.x;
   const int t = A.items[3 * it], col0 = A.items[3 * it + 1], ncols = A.items[3 * it + 2];
   const int s = A.front_s[t], m = s + A.front_u[t];
   const int64_t io = A.idx_off[t], go = A.g_off[t];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int r0 = 0; r0 < R; r0 += RG) {
     const int ng = min(RG, R - r0);
     // v = [y_S; -x_U]
@@ -133,25 +138,35 @@ __global__ void __launch_bounds__(kNdThreads)
         vs[p * RG + r] = r < ng ? (p < s ? y[v * R + r0 + r] : -x[v * R + r0 + r]) : 0.0;
     }
     __syncthreads();
-    const int c = threadIdx.x;
-    if (c < ncols) {
-      const int col = col0 + c;
-      const double* g = A.G + go + col;
+    for (int cb = 0; cb < ncols; cb += kNdCols) {  // items normally hold one 32-column chunk
+      const int c = cb + lane;
       double acc[RG];
 #pragma unroll
       for (int r = 0; r < RG; ++r) acc[r] = 0.0;
+      if (c < ncols) {
+        const double* g = A.G + go + col0 + c;
 #pragma unroll 4
-      for (int p = 0; p < m; ++p) {
-        const double gv = __ldg(g + (int64_t)p * s);
+        for (int p = warp; p < m; p += kNdWarps) {
+          const double gv = __ldg(g + (int64_t)p * s);
 #pragma unroll
-        for (int r = 0; r < RG; ++r) acc[r] = fma(gv, vs[p * RG + r], acc[r]);
+          for (int r = 0; r < RG; ++r) acc[r] = fma(gv, vs[p * RG + r], acc[r]);
+        }
       }
-      const int64_t v = A.fidx[io + col];
 #pragma unroll
-      for (int r = 0; r < RG; ++r)
-        if (r < ng) x[v * R + r0 + r] = acc[r];
+      for (int r = 0; r < RG; ++r) red[warp][r][lane] = acc[r];
+      __syncthreads();
+      if (warp == 0 && c < ncols) {
+        const int64_t v = A.fidx[io + col0 + c];
+#pragma unroll
+        for (int r = 0; r < RG; ++r) {
+          double sum = red[0][r][lane];
+#pragma unroll
+          for (int w = 1; w < kNdWarps; ++w) sum += red[w][r][lane];
+          if (r < ng) x[v * R + r0 + r] = sum;
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
 }
 

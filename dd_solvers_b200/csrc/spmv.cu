@@ -273,6 +273,32 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// Rows of moderate length (R = 1): L lanes per row (L = 4..32), lane l sums
+// the entries k0 + l, k0 + l + L, ...; the L partial sums are combined by a
+// fixed xor tree, so the result does not depend on timing.
+template <int L>
+__global__ void __launch_bounds__(kThreads)
+    k_spmv_rowwarp(int64_t n_rows, const int* __restrict__ row_ptr, const int* __restrict__ cols,
+                   const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y) {
+  constexpr int RPW = 32 / L;  // rows per warp and step
+  const int lane = threadIdx.x & 31;
+  const int sub = lane % L;
+  const int64_t warps = (int64_t)gridDim.x * (kThreads / 32);
+  // the loop bound depends on the warp only, so every lane reaches the shuffles
+  for (int64_t base = ((int64_t)blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5)) * RPW; base < n_rows;
+       base += warps * RPW) {
+    const int64_t row = base + lane / L;
+    double sum = 0.0;
+    if (row < n_rows) {
+      const int k0 = row_ptr[row], k1 = row_ptr[row + 1];
+      for (int k = k0 + sub; k < k1; k += L) sum = fma(__ldg(vals + k), __ldg(x + __ldg(cols + k)), sum);
+    }
+#pragma unroll
+    for (int o = L / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o, L);
+    if (sub == 0 && row < n_rows) y[row] = sum;
+  }
+}
+
 // BSR with column-major (bs x bs) blocks; one warp per block row. Lane l walks
 // the row's stored values e = l, l+32, ...; entry e of the block row is block
 // e / bs^2, column (e % bs^2) / bs, row e % bs.
@@ -451,6 +477,25 @@ int ddx_spmv_csr_rowblock_f64(int64_t n_rows, int R, const int* row_ptr, const i
     k_spmv_rowblock<<<grid, kThreads, 0, (cudaStream_t)stream>>>(n_rows, R, row_ptr, cols, vals, x, y);
   }
   DDX_LAUNCH_CHECK("ddx_spmv_csr_rowblock_f64");
+  return DDX_OK;
+}
+
+int ddx_spmv_csr_lanes_f64(int64_t n_rows, int lanes, const int* row_ptr, const int* cols, const double* vals,
+                           const double* x, double* y, ddx_stream_t stream) {
+  DDX_REQUIRE(n_rows >= 0 && row_ptr && x && y, "ddx_spmv_csr_lanes_f64: bad arguments");
+  DDX_REQUIRE(lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32,
+              "ddx_spmv_csr_lanes_f64: lanes must be 4, 8, 16 or 32 (got %d)", lanes);
+  if (n_rows == 0) return DDX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  auto go = [&](auto kernel) {
+    const int grid = resident_grid(kernel, ceil_div(n_rows * lanes, kThreads), 1 << 20);
+    kernel<<<grid, kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y);
+  };
+  if (lanes == 4) go(k_spmv_rowwarp<4>);
+  else if (lanes == 8) go(k_spmv_rowwarp<8>);
+  else if (lanes == 16) go(k_spmv_rowwarp<16>);
+  else go(k_spmv_rowwarp<32>);
+  DDX_LAUNCH_CHECK("ddx_spmv_csr_lanes_f64");
   return DDX_OK;
 }
 

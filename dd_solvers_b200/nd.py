@@ -45,8 +45,8 @@ import torch
 
 from . import _lib as L
 
-FWD_ROWS = 64    # rows of G per forward work item
-BWD_COLS = 128   # columns of G per backward work item
+FWD_ROWS = 32    # rows of G per forward work item (8 warps, 4 rows each)
+BWD_COLS = 32    # columns of G per backward work item (one per lane; warps split the rows)
 
 
 # ---------------------------------------------------------------------------
@@ -179,6 +179,17 @@ class NDSymbolic:
 # numeric factorisation (torch, any device)
 # ---------------------------------------------------------------------------
 
+def _pairs(lengths: np.ndarray):
+    """All index pairs ``(g, a, b)`` with ``a, b < lengths[g]`` (row-major per g)."""
+    lengths = np.asarray(lengths, dtype=np.int64)
+    sq = lengths * lengths
+    g = np.repeat(np.arange(len(lengths)), sq)
+    start = np.cumsum(sq) - sq
+    p = np.arange(int(sq.sum()), dtype=np.int64) - start[g]
+    u = lengths[g]
+    return g, p // u, p % u
+
+
 def factorize(sym: NDSymbolic, indptr, indices, values, device, max_batch_bytes: int = 1 << 30) -> torch.Tensor:
     """The stored operators ``G_t = [Linv; M]`` of every front, concatenated."""
     indptr = np.asarray(indptr, dtype=np.int64)
@@ -186,42 +197,25 @@ def factorize(sym: NDSymbolic, indptr, indices, values, device, max_batch_bytes:
     vals = torch.as_tensor(np.asarray(values, dtype=np.float64)) if not isinstance(values, torch.Tensor) \
         else values.to(torch.float64)
     vals = vals.to(device)
-    n = sym.n
+    n, nf = sym.n, sym.nf
     rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(indptr))
     front_of = np.empty(n, dtype=np.int64)
-    for t in range(sym.nf):
-        front_of[sym.S[t]] = t
+    front_of[sym.perm] = np.repeat(np.arange(nf), sym.s)
+    first = np.cumsum(sym.s) - sym.s  # position of each front's first separator vertex
     # original entries (i in S_t, j in S_t or U_t): kept where pos(j) >= first position of S_t
     t_of = front_of[rows]
-    first = np.array([sym.pos[x[0]] for x in sym.S], dtype=np.int64)
     keep = sym.pos[indices] >= first[t_of]
     e_t = t_of[keep]
-    e_i, e_j = rows[keep], indices[keep]
+    e_j = indices[keep]
     e_v = np.nonzero(keep)[0]
-    # local index of each vertex inside front t: position in [S_t, U_t]
-    li = sym.pos[e_i] - first[e_t]
-    fpos_cache = {}
-
-    def local(t, verts_pos):
-        fp = fpos_cache.get(t)
-        if fp is None:
-            fp = sym.pos[np.concatenate([sym.S[t], sym.U[t]])]
-            fpos_cache[t] = fp
-        return np.searchsorted(fp, verts_pos)
-
-    # group entries by front for assembly
-    order = np.argsort(e_t, kind="stable")
-    e_t, e_i, e_j, e_v, li = e_t[order], e_i[order], e_j[order], e_v[order], li[order]
-    bounds = np.searchsorted(e_t, np.arange(sym.nf + 1))
-    lj = np.empty_like(li)
-    for t in range(sym.nf):
-        a, b = bounds[t], bounds[t + 1]
-        if b > a:
-            lj[a:b] = local(t, sym.pos[e_j[a:b]])
+    li = sym.pos[rows[keep]] - first[e_t]
+    # local index of j: its place in front t's list [S_t, U_t] (sorted by position)
+    key_all = np.repeat(np.arange(nf, dtype=np.int64), sym.s + sym.u) * (n + 1) + sym.pos[sym.fidx]
+    lj = np.searchsorted(key_all, e_t * (n + 1) + sym.pos[e_j]) - sym.idx_off[e_t]
     in_s = lj < sym.s[e_t]
 
     G = torch.zeros(sym.g_total, dtype=torch.float64, device=device)
-    upd = {}  # front -> (batch tensor, batch index, S_MAX) of its pending update matrix
+    upd = {}  # front -> (batch tensor, batch index) of its pending update matrix
     for lv in range(sym.n_levels):
         fronts = sym.by_level[lv]
         # chunk the level so a padded batch stays within max_batch_bytes
@@ -239,39 +233,31 @@ def factorize(sym: NDSymbolic, indptr, indices, values, device, max_batch_bytes:
         for ch in chunks:
             ch = np.array(ch, dtype=np.int64)
             B = len(ch)
-            SM = int(sym.s[ch].max())
-            UM = int(sym.u[ch].max())
+            sc, uc = sym.s[ch], sym.u[ch]
+            SM, UM = int(sc.max()), int(uc.max())
             m = SM + UM
             F = torch.zeros(B, m, m, dtype=torch.float64, device=device)
             # identity on the padded separator diagonal
-            pad_b, pad_i = [], []
-            for b, t in enumerate(ch):
-                if sym.s[t] < SM:
-                    ii = np.arange(sym.s[t], SM)
-                    pad_b.append(np.full(len(ii), b))
-                    pad_i.append(ii)
-            if pad_b:
-                pb = torch.as_tensor(np.concatenate(pad_b), device=device)
-                pi = torch.as_tensor(np.concatenate(pad_i), device=device)
-                F[pb, pi, pi] = 1.0
-            # original entries
-            sel = np.concatenate([np.arange(bounds[t], bounds[t + 1]) for t in ch])
+            npad = SM - sc
+            if npad.any():
+                pb = np.repeat(np.arange(B), npad)
+                pi = np.arange(int(npad.sum())) - np.repeat(np.cumsum(npad) - npad, npad) + np.repeat(sc, npad)
+                F[torch.as_tensor(pb, device=device), torch.as_tensor(pi, device=device),
+                  torch.as_tensor(pi, device=device)] = 1.0
+            # original entries (F_SS and F_US, mirrored into F_SU)
+            bmap = np.full(nf, -1, dtype=np.int64)
+            bmap[ch] = np.arange(B)
+            sel = np.nonzero(bmap[e_t] >= 0)[0]
             if len(sel):
-                bmap = np.empty(sym.nf, dtype=np.int64)
-                bmap[ch] = np.arange(B)
-                bb = bmap[e_t[sel]]
-                r = li[sel]
+                et = e_t[sel]
+                bb = torch.as_tensor(bmap[et], device=device)
+                rt = torch.as_tensor(li[sel], device=device)
                 c = lj[sel]
-                c_pad = np.where(in_s[sel], c, SM + (c - sym.s[e_t[sel]]))
+                ct = torch.as_tensor(np.where(in_s[sel], c, SM + (c - sym.s[et])), device=device)
                 vv = vals[torch.as_tensor(e_v[sel], device=device)]
-                bbt = torch.as_tensor(bb, device=device)
-                rt = torch.as_tensor(r, device=device)
-                ct = torch.as_tensor(c_pad, device=device)
-                F[bbt, rt, ct] = vv
-                us = ~in_s[sel]
-                if us.any():
-                    F[bbt[torch.as_tensor(us, device=device)], ct[torch.as_tensor(us, device=device)],
-                      rt[torch.as_tensor(us, device=device)]] = vv[torch.as_tensor(us, device=device)]
+                F[bb, rt, ct] = vv
+                us = torch.as_tensor(~in_s[sel], device=device)
+                F[bb[us], ct[us], rt[us]] = vv[us]
             # extend-add of the children's updates, one child slot at a time
             nslots = max((len(sym.children[t]) for t in ch), default=0)
             for slot in range(nslots):
@@ -279,56 +265,57 @@ def factorize(sym: NDSymbolic, indptr, indices, values, device, max_batch_bytes:
                 for b, t in enumerate(ch):
                     if slot < len(sym.children[t]):
                         c = sym.children[t][slot]
-                        Ub, ub_i, USM = upd[c]
-                        groups.setdefault(id(Ub), (Ub, USM, []))[2].append((b, t, c, ub_i))
-                for Ub, USM, items in groups.values():
-                    dst, src = [], []
-                    for b, t, c, ub_i in items:
-                        uc = int(sym.u[c])
-                        if uc == 0:
-                            continue
-                        rel = sym.rel[c]
-                        rel_pad = np.where(rel < sym.s[t], rel, SM + (rel - sym.s[t]))
-                        ii, jj = np.meshgrid(rel_pad, rel_pad, indexing="ij")
-                        dst.append(b * m * m + ii.reshape(-1) * m + jj.reshape(-1))
-                        um = Ub.shape[1]
-                        a = np.arange(uc)
-                        si, sj = np.meshgrid(a, a, indexing="ij")
-                        src.append(ub_i * um * um + si.reshape(-1) * um + sj.reshape(-1))
-                    if dst:
-                        d = torch.as_tensor(np.concatenate(dst), device=device)
-                        s_ = torch.as_tensor(np.concatenate(src), device=device)
-                        F.view(-1).index_put_((d,), Ub.reshape(-1)[s_], accumulate=True)
-                for b, t in enumerate(ch):
-                    if slot < len(sym.children[t]):
-                        upd.pop(sym.children[t][slot], None)
-            Fss = F[:, :SM, :SM]
-            Lc, info = torch.linalg.cholesky_ex(Fss)
+                        Ub, ub_i = upd.pop(c)
+                        groups.setdefault(id(Ub), (Ub, []))[1].append((b, t, c, ub_i))
+                for Ub, items in groups.values():
+                    it = np.array(items, dtype=np.int64).reshape(-1, 4)
+                    ucs = sym.u[it[:, 2]]
+                    if not ucs.any():
+                        continue
+                    g, a, bq = _pairs(ucs)
+                    rel = np.concatenate([sym.rel[c] for c in it[:, 2]])
+                    rs = np.cumsum(ucs) - ucs
+                    s_par = np.repeat(sym.s[it[:, 1]], ucs)
+                    rel_pad = np.where(rel < s_par, rel, SM + (rel - s_par))
+                    dst = it[g, 0] * m * m + rel_pad[rs[g] + a] * m + rel_pad[rs[g] + bq]
+                    um = Ub.shape[1]
+                    src = it[g, 3] * um * um + a * um + bq
+                    F.view(-1).index_put_((torch.as_tensor(dst, device=device),),
+                                          Ub.reshape(-1)[torch.as_tensor(src, device=device)], accumulate=True)
+            Lc, info = torch.linalg.cholesky_ex(F[:, :SM, :SM])
             if int(info.abs().max()) != 0:
                 raise RuntimeError("coarse matrix is not positive definite")
             eye = torch.eye(SM, dtype=torch.float64, device=device).expand(B, SM, SM)
             Linv = torch.linalg.solve_triangular(Lc, eye, upper=False)
             del Lc, eye
             if UM:
-                Fus = F[:, SM:, :SM]
-                W = Fus @ Linv.transpose(1, 2)
+                W = F[:, SM:, :SM] @ Linv.transpose(1, 2)
                 M = W @ Linv
                 Upd = F[:, SM:, SM:] - W @ W.transpose(1, 2)
                 del W
             else:
                 M = Upd = None
-            # store G_t = [Linv; M] (unpadded, row-major)
-            for b, t in enumerate(ch):
-                s_t, u_t = int(sym.s[t]), int(sym.u[t])
-                o = int(sym.g_off[t])
-                G[o:o + s_t * s_t] = Linv[b, :s_t, :s_t].reshape(-1)
-                if u_t:
-                    G[o + s_t * s_t:o + (s_t + u_t) * s_t] = M[b, :u_t, :s_t].reshape(-1)
+            del F
+            # store G_t = [Linv; M] (unpadded, row-major), one gather per chunk
+            dev_s = torch.as_tensor(sc, device=device)
+            dev_u = torch.as_tensor(uc, device=device)
+            cnt = (dev_s + dev_u) * dev_s
+            gb = torch.repeat_interleave(torch.arange(B, device=device), cnt)
+            e = torch.arange(int(cnt.sum()), device=device) - torch.repeat_interleave(torch.cumsum(cnt, 0) - cnt, cnt)
+            sb = dev_s[gb]
+            row, col = e // sb, e % sb
+            dst = torch.as_tensor(sym.g_off[ch], device=device)[gb] + e
+            top = row < sb
+            G[dst[top]] = Linv.reshape(-1)[(gb * SM * SM + row * SM + col)[top]]
+            if M is not None:
+                bot = ~top
+                G[dst[bot]] = M.reshape(-1)[(gb * UM * SM + (row - sb) * SM + col)[bot]]
+            del gb, e, sb, row, col, dst, top
             if Upd is not None:
                 for b, t in enumerate(ch):
                     if sym.parent[t] >= 0:
-                        upd[int(t)] = (Upd, b, SM)
-            del F, Linv, M
+                        upd[int(t)] = (Upd, b)
+            del Linv, M
     return G
 
 

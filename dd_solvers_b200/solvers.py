@@ -356,6 +356,8 @@ class SchwarzOperator(SparseSolver):
         ks = np.diff(sub_ptr)
         self.ks = ks
         self.kmax = int(ks.max()) if len(ks) else 0
+        self.k_equal = int(ks[0]) if len(ks) and ks[0] > 0 and bool((ks == ks[0]).all()) else -1
+        self.rows_total = int(ks.sum())
         block_dtype = (getattr(self.local_solver, "precision", None) or self.preconditioner_precision
                        or matrix.dtype)
         if not isinstance(self.local_solver, Inv):
@@ -584,6 +586,12 @@ class SchwarzOperator(SparseSolver):
     def _simt_apply(self, r, ylocal, R, ist, groups: int, stage_kb: int) -> None:
         """SIMT local apply; ``groups`` is the consumer-group count of the full-block
         kernel or the consumer-warp count of the upper-triangle-tile kernel."""
+        if groups == self.SMALL or (groups == 0 and self._small_default()):
+            L.call("ddx_schwarz_local_apply_small", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
+                   L.ptr(self.store.blk_off), L.ptr(self.store.data), L.DTYPE_CODE[self.block_dtype],
+                   L.ptr(self.store.scale), self.kmax, self.k_equal, self.rows_total, L.ptr(r), L.ptr(ylocal),
+                   L.DTYPE_CODE[self.acc_dtype], L.ptr(ist), L.stream_ptr())
+            return
         args = (self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx), L.ptr(self.order),
                 L.ptr(self.store.blk_off), L.ptr(self.store.data), L.DTYPE_CODE[self.block_dtype],
                 L.ptr(self.store.scale), self.kmax, L.ptr(r), L.ptr(ylocal), L.DTYPE_CODE[self.acc_dtype],
@@ -596,13 +604,23 @@ class SchwarzOperator(SparseSolver):
     # -- autotuner -------------------------------------------------------------
     # (consumer groups of 4 warps, KiB per shared-memory stage): full-block kernel;
     # (consumer warps, KiB per stage): upper-triangle-tile kernel
+    # SMALL: the one-thread-per-entry kernel for small subdomains (full layout)
     TUNE_CANDIDATES = [(g, kb) for g in (1, 2, 4) for kb in (12, 20, 32)]
     TUNE_CANDIDATES_SYM = [(w, kb) for w in (4, 8, 16) for kb in (8, 16, 32)]
+    SMALL = -1
+    SMALL_KMAX = 64   # the small-subdomain kernel is a tuning candidate up to this size
+    SMALL_DEFAULT_KMAX = 32  # and the untuned default up to this one
     _tuned: dict = {}
 
     @property
     def tune_candidates(self):
-        return self.TUNE_CANDIDATES_SYM if self.store.layout == "sym" else self.TUNE_CANDIDATES
+        if self.store.layout == "sym":
+            return self.TUNE_CANDIDATES_SYM
+        small = [(self.SMALL, 0)] if self.kmax <= self.SMALL_KMAX else []
+        return small + self.TUNE_CANDIDATES
+
+    def _small_default(self) -> bool:
+        return self.store.layout != "sym" and self.kmax <= self.SMALL_DEFAULT_KMAX
 
     def _tune_key(self):
         # The SIMT apply runs one right-hand side per launch, so one
@@ -648,9 +666,27 @@ class SchwarzOperator(SparseSolver):
         self.tune_timings = timings
         return best
 
+    @staticmethod
+    def _lanes_for(n_rows: int, nnz: int) -> int:
+        """Lanes per row for the restriction SpMV from the mean row length
+        (0: one CTA per row, for long rows)."""
+        mean = nnz / max(n_rows, 1)
+        if mean >= 512:
+            return 0
+        for lanes in (4, 8, 16):
+            if mean < 2 * lanes:
+                return lanes
+        return 32
+
     def _restrict(self, rowptr, col, val, x, out, R):
-        L.call("ddx_spmv_csr_rowblock_f64", rowptr.numel() - 1, R, L.ptr(rowptr), L.ptr(col), L.ptr(val),
-               L.ptr(x), L.ptr(out), L.stream_ptr())
+        n_rows = rowptr.numel() - 1
+        lanes = self._lanes_for(n_rows, col.numel()) if R == 1 else 0
+        if lanes:
+            L.call("ddx_spmv_csr_lanes_f64", n_rows, lanes, L.ptr(rowptr), L.ptr(col), L.ptr(val), L.ptr(x),
+                   L.ptr(out), L.stream_ptr())
+        else:
+            L.call("ddx_spmv_csr_rowblock_f64", n_rows, R, L.ptr(rowptr), L.ptr(col), L.ptr(val),
+                   L.ptr(x), L.ptr(out), L.stream_ptr())
 
     def _coarse(self, w, yc, R, ist=None):
         if self._fused_coarse:

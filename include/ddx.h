@@ -127,6 +127,12 @@ int ddx_spmv_csr_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols,
  * y[row, j] = sum_k vals[k] x[cols[k], j] (coarse restriction A_R y or R0 r). */
 int ddx_spmv_csr_rowblock_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols,
                               const double* vals, const double* x, double* y, ddx_stream_t stream);
+/* CSR, R = 1, `lanes` (4, 8, 16 or 32) lanes per row summed by a fixed xor
+ * tree: rows of moderate length, e.g. the coarse restriction A_R y when the
+ * coarse aggregates are small (the caller picks lanes from the mean row
+ * length). */
+int ddx_spmv_csr_lanes_f64(int64_t n_rows, int lanes, const int* row_ptr, const int* cols, const double* vals,
+                           const double* x, double* y, ddx_stream_t stream);
 /* BSR, block size bs (1..24: DG P1..P5 triangles have 3..21 DOFs per
  * element), blocks column-major (bs, bs) as produced by the reference's
  * csr_to_bsr (src/dd_solvers/cpp/cusparse.cpp:22-107); dtype F64 or F32 for
@@ -172,6 +178,15 @@ int ddx_schwarz_local_apply(int n_sub, int R, const int64_t* sub_ptr, const int*
                             const int* order, const int64_t* blk_off, const void* blocks,
                             int block_dtype, const float* scale, int kmax, const double* r,
                             void* ylocal, int acc_dtype, const int* ist, ddx_stream_t stream);
+/* Same product and block layout for small subdomains (the reference's DG
+ * layouts: equal blocks of a few to a few dozen DOFs), one thread per output
+ * entry. rows = sub_ptr[n_sub]; k_equal > 0 declares every subdomain to have
+ * k_equal DOFs (k_equal * n_sub == rows), otherwise each row finds its
+ * subdomain by binary search in sub_ptr. Any R >= 1. */
+int ddx_schwarz_local_apply_small(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
+                                  const int64_t* blk_off, const void* blocks, int block_dtype,
+                                  const float* scale, int kmax, int k_equal, int64_t rows, const double* r,
+                                  void* ylocal, int acc_dtype, const int* ist, ddx_stream_t stream);
 /* Same product for blocks stored as upper-triangle tiles (half the bytes):
  * Q_i exactly symmetric, only its 32 x 32 tiles (I, J), I <= J, kept, in
  * row-major order of (I, J) from element blk_off[i] (16-byte aligned); each

@@ -218,6 +218,64 @@ def test_simt_apply_every_tuning_candidate(cuda, prec, layout):
     assert _lib.device_error() == 0
 
 
+@pytest.mark.parametrize("lanes", [4, 8, 16, 32])
+def test_spmv_csr_lanes(cuda, lanes):
+    """Sub-warp CSR SpMV (coarse restriction): rows of 0..90 entries, a row
+    count that is not a multiple of the rows per warp."""
+    from dd_solvers_b200 import _lib as L
+
+    rng = np.random.default_rng(lanes)
+    n_rows, n_cols = 3001, 5000
+    lens = rng.integers(0, 91, n_rows)
+    crow = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    col = rng.integers(0, n_cols, int(crow[-1])).astype(np.int32)
+    val = rng.standard_normal(int(crow[-1]))
+    x = rng.standard_normal(n_cols)
+    ref = sps.csr_matrix((val, col, crow), shape=(n_rows, n_cols)) @ x
+    t = lambda a: torch.as_tensor(a, device=cuda)  # noqa: E731
+    y = torch.full((n_rows,), np.nan, dtype=torch.float64, device=cuda)
+    crow_t, col_t, val_t, x_t = t(crow), t(col), t(val), t(x)
+    L.call("ddx_spmv_csr_lanes_f64", n_rows, lanes, L.ptr(crow_t), L.ptr(col_t), L.ptr(val_t), L.ptr(x_t),
+           L.ptr(y), L.stream_ptr())
+    np.testing.assert_allclose(y.cpu().numpy(), ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32", "bf16", "f16"])
+@pytest.mark.parametrize("shape", ["equal", "uneven"])
+@pytest.mark.parametrize("R", [1, 3])
+def test_small_subdomain_apply(cuda, prec, shape, R):
+    """The one-thread-per-entry kernel: equal contiguous blocks of 12 DOFs (the
+    reference's DG layout, k_equal path) and overlapping subdomains of uneven
+    size (binary search path), against the FP64 product of the stored blocks."""
+    import dd_solvers_b200 as dd
+    from dd_solvers_b200 import problems
+
+    if shape == "equal":
+        P = problems.q1_grid(2, 48)
+        A = P.matrix
+        n = A.shape[0]
+        k = 12
+        m = n // k
+        A = A[: m * k][:, : m * k].tocsr()
+        sub_ptr = np.arange(m + 1, dtype=np.int64) * k
+        sub_idx = np.arange(m * k, dtype=np.int32)
+    else:
+        P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(2, 24, 6)
+    pc = dd.AdditiveSchwarz(torch.float64, dd.Inv(DT[prec]), None)
+    pc.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx))
+    assert pc.store.layout == "colmajor" and pc.kmax <= pc.SMALL_KMAX
+    assert (pc.k_equal > 0) == (shape == "equal")
+    assert (pc.SMALL, 0) in pc.tune_candidates
+    blocks = [pc.store.block(i).cpu().numpy() for i in range(pc.n_solvers)]
+    r = np.random.default_rng(7).standard_normal((A.shape[0], R))
+    ref = np.concatenate([blocks[i] @ r[sub_idx[sub_ptr[i]:sub_ptr[i + 1]]] for i in range(pc.n_solvers)])
+    s = pc.scratch(R)
+    pc._simt_apply(torch.as_tensor(r, device=cuda).reshape(-1), s["ylocal"], R, None, pc.SMALL, 0)
+    got = s["ylocal"][: len(sub_idx) * R].double().view(-1, R).cpu().numpy()
+    tol = 1e-13 if prec == "f64" else (1e-12 if prec == "f32" and pc.acc_dtype == torch.float64 else 2e-6)
+    assert np.linalg.norm(got - ref) <= tol * np.linalg.norm(ref)
+
+
 @pytest.mark.parametrize("prec", ["f32", "bf16", "f16"])
 def test_block_quantisation_matches_oracle(cuda, prec):
     """Stored blocks equal the oracle's power-of-two-scaled rounding of the FP64 inverse."""
