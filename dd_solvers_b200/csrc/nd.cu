@@ -13,8 +13,10 @@
 //            y_S = Linv f_S,  u_t = f_U - M f_S
 //   backward (root -> leaves): x_S = Linv^T y_S - M^T x_U
 //
-// One launch per tree level and sweep; large fronts are split into row
-// (forward) or column (backward) chunks. All sums run in a fixed order.
+// The backward sweep reads the transposed copy G_t^T, so both sweeps are
+// row-wise GEMVs (a warp per row, lanes along the row: coalesced, short
+// per-lane chains). One launch per tree level and sweep; every front is split
+// into work items of a few rows sized by bytes. All sums run in a fixed order.
 #include <algorithm>
 #include <vector>
 
@@ -26,7 +28,6 @@ namespace {
 constexpr int kNdThreads = 256;
 constexpr int kNdWarps = kNdThreads / 32;
 constexpr int kNdSmemMax = 96 * 1024;  // the staged vector (front rows x RHS group)
-constexpr int kNdCols = 32;            // columns per backward work item (one per lane)
 
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
@@ -44,7 +45,8 @@ struct NdArgs {
   const int* fidx;
   const int64_t* gptr;
   const int64_t* gsrc;
-  const double* G;
+  const double* G;   // forward operator, (s+u) x s row-major per front
+  const double* GT;  // its transpose, s x (s+u) row-major per front (backward sweep)
 };
 
 template <int RG>
@@ -114,23 +116,21 @@ __global__ void __launch_bounds__(kNdThreads)
   }
 }
 
-// Backward item: up to 32 columns of G_t (one per lane); the 8 warps take the
-// rows p = warp, warp + 8, ... and their partial sums are added in warp order.
+// Backward item: rows c0 .. c0+nc of G_t^T (columns of G_t); a warp per row,
+// lanes over the s+u entries, v = [y_S; -x_U] staged in shared memory.
 template <int RG>
 __global__ void __launch_bounds__(kNdThreads)
     k_nd_bwd(NdArgs A, int64_t item0, int R, const double* __restrict__ y, double* __restrict__ x,
              const int* ist) {
   if (ist != nullptr && n_active(ist, R) == 0) return;
   extern __shared__ double vs[];
-  __shared__ double red[kNdWarps][RG][kNdCols];
   const int64_t it = item0 + blockIdx.x;
-  const int t = A.items[3 * it], col0 = A.items[3 * it + 1], ncols = A.items[3 * it + 2];
+  const int t = A.items[3 * it], c0 = A.items[3 * it + 1], nc = A.items[3 * it + 2];
   const int s = A.front_s[t], m = s + A.front_u[t];
   const int64_t io = A.idx_off[t], go = A.g_off[t];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int r0 = 0; r0 < R; r0 += RG) {
     const int ng = min(RG, R - r0);
-    // v = [y_S; -x_U]
     for (int p = threadIdx.x; p < m; p += kNdThreads) {
       const int64_t v = A.fidx[io + p];
 #pragma unroll
@@ -138,35 +138,24 @@ __global__ void __launch_bounds__(kNdThreads)
         vs[p * RG + r] = r < ng ? (p < s ? y[v * R + r0 + r] : -x[v * R + r0 + r]) : 0.0;
     }
     __syncthreads();
-    for (int cb = 0; cb < ncols; cb += kNdCols) {  // items normally hold one 32-column chunk
-      const int c = cb + lane;
+    for (int c = c0 + warp; c < c0 + nc; c += kNdWarps) {
+      const double* g = A.GT + go + (int64_t)c * m;
       double acc[RG];
 #pragma unroll
       for (int r = 0; r < RG; ++r) acc[r] = 0.0;
-      if (c < ncols) {
-        const double* g = A.G + go + col0 + c;
-#pragma unroll 4
-        for (int p = warp; p < m; p += kNdWarps) {
-          const double gv = __ldg(g + (int64_t)p * s);
+      for (int p = lane; p < m; p += 32) {
+        const double gv = __ldg(g + p);
 #pragma unroll
-          for (int r = 0; r < RG; ++r) acc[r] = fma(gv, vs[p * RG + r], acc[r]);
-        }
+        for (int r = 0; r < RG; ++r) acc[r] = fma(gv, vs[p * RG + r], acc[r]);
       }
 #pragma unroll
-      for (int r = 0; r < RG; ++r) red[warp][r][lane] = acc[r];
-      __syncthreads();
-      if (warp == 0 && c < ncols) {
-        const int64_t v = A.fidx[io + col0 + c];
+      for (int r = 0; r < RG; ++r) acc[r] = warp_sum_d(acc[r]);
+      const int64_t v = A.fidx[io + c];
 #pragma unroll
-        for (int r = 0; r < RG; ++r) {
-          double sum = red[0][r][lane];
-#pragma unroll
-          for (int w = 1; w < kNdWarps; ++w) sum += red[w][r][lane];
-          if (r < ng) x[v * R + r0 + r] = sum;
-        }
-      }
-      __syncthreads();
+      for (int r = 0; r < RG; ++r)
+        if (lane == r && r < ng) x[v * R + r0 + r] = acc[r];
     }
+    __syncthreads();
   }
 }
 
@@ -365,8 +354,9 @@ int ddx_coarse_solve_nd(const ddx_nd_plan* P, int R, const double* w, double* x,
               "ddx_coarse_solve_nd: plan without level tables");
   if (P->n == 0) return DDX_OK;
   cudaStream_t s = (cudaStream_t)stream;
+  DDX_REQUIRE(P->G && P->GT, "ddx_coarse_solve_nd: plan without operators");
   NdArgs fa{P->fwd_items, P->front_s, P->front_u, P->g_off, P->idx_off, P->upd_off, P->fidx, P->gptr,
-            P->gsrc, P->G};
+            P->gsrc, P->G, P->GT};
   NdArgs ba = fa;
   ba.items = P->bwd_items;
   const int64_t mmax = std::max<int64_t>(P->max_front, 1);

@@ -45,8 +45,14 @@ import torch
 
 from . import _lib as L
 
-FWD_ROWS = 32    # rows of G per forward work item (8 warps, 4 rows each)
-BWD_COLS = 32    # columns of G per backward work item (one per lane; warps split the rows)
+LEAF = 128          # largest subgraph left undissected (a leaf front)
+ITEM_BYTES = 32768  # operator bytes per work item (rows of G or of G^T) ...
+ITEM_MAX_ROWS = 64  # ... between 8 and this many rows
+
+
+def _rows_per_item(row_len: int, item_bytes: int, max_rows: int) -> int:
+    r = item_bytes // (8 * max(row_len, 1))
+    return int(min(max_rows, max(8, r // 8 * 8)))
 
 
 # ---------------------------------------------------------------------------
@@ -148,31 +154,37 @@ class NDSymbolic:
         np.add.at(self.gptr, gp + 1, 1)
         self.gptr = np.cumsum(self.gptr)
         self.gsrc = gs.astype(np.int64)
-        # per-level work items
+        self.by_level = [np.nonzero(level == lv)[0] for lv in range(self.n_levels)]
+        m_all = self.s + self.u
+        self.fwd_level_smax = np.array([int(self.s[f].max()) if len(f) else 0 for f in self.by_level],
+                                       dtype=np.int32)
+        self.bwd_level_mmax = np.array([int(m_all[f].max()) if len(f) else 0 for f in self.by_level[::-1]],
+                                       dtype=np.int32)
+        self.build_items()
+
+    def build_items(self, item_bytes: int = ITEM_BYTES, max_rows: int = ITEM_MAX_ROWS) -> None:
+        """Per-level work items: (front, first row, rows) of G_t for the forward
+        sweep (leaves first), of G_t^T for the backward sweep (root first)."""
+        m = self.s + self.u
         fwd, bwd = [], []
         self.fwd_level_ptr = np.zeros(self.n_levels + 1, dtype=np.int64)
         self.bwd_level_ptr = np.zeros(self.n_levels + 1, dtype=np.int64)
-        by_level = [np.nonzero(level == lv)[0] for lv in range(self.n_levels)]
         for lv in range(self.n_levels):
-            for t in by_level[lv]:
+            for t in self.by_level[lv]:
                 rows = int(m[t])
-                for r0 in range(0, max(rows, 1), FWD_ROWS):
-                    fwd.append((t, r0, min(FWD_ROWS, rows - r0)))
+                step = _rows_per_item(int(self.s[t]), item_bytes, max_rows)
+                for r0 in range(0, max(rows, 1), step):
+                    fwd.append((t, r0, min(step, rows - r0)))
             self.fwd_level_ptr[lv + 1] = len(fwd)
-        # backward runs the levels from the top; items are stored in that order
         for j, lv in enumerate(range(self.n_levels - 1, -1, -1)):
-            for t in by_level[lv]:
+            for t in self.by_level[lv]:
                 cols = int(self.s[t])
-                for c0 in range(0, cols, BWD_COLS):
-                    bwd.append((t, c0, min(BWD_COLS, cols - c0)))
+                step = _rows_per_item(int(m[t]), item_bytes, max_rows)
+                for c0 in range(0, cols, step):
+                    bwd.append((t, c0, min(step, cols - c0)))
             self.bwd_level_ptr[j + 1] = len(bwd)
-        m_all = self.s + self.u
-        self.fwd_level_smax = np.array([int(self.s[f].max()) if len(f) else 0 for f in by_level], dtype=np.int32)
-        self.bwd_level_mmax = np.array([int(m_all[f].max()) if len(f) else 0 for f in by_level[::-1]],
-                                       dtype=np.int32)
         self.fwd_items = np.array(fwd, dtype=np.int32).reshape(-1, 3)
         self.bwd_items = np.array(bwd, dtype=np.int32).reshape(-1, 3)
-        self.by_level = by_level
 
 
 # ---------------------------------------------------------------------------
@@ -190,8 +202,9 @@ def _pairs(lengths: np.ndarray):
     return g, p // u, p % u
 
 
-def factorize(sym: NDSymbolic, indptr, indices, values, device, max_batch_bytes: int = 1 << 30) -> torch.Tensor:
-    """The stored operators ``G_t = [Linv; M]`` of every front, concatenated."""
+def factorize(sym: NDSymbolic, indptr, indices, values, device, max_batch_bytes: int = 1 << 30):
+    """The stored operators ``G_t = [Linv; M]`` of every front, concatenated,
+    and their transposes (same offsets)."""
     indptr = np.asarray(indptr, dtype=np.int64)
     indices = np.asarray(indices, dtype=np.int64)
     vals = torch.as_tensor(np.asarray(values, dtype=np.float64)) if not isinstance(values, torch.Tensor) \
@@ -215,6 +228,7 @@ def factorize(sym: NDSymbolic, indptr, indices, values, device, max_batch_bytes:
     in_s = lj < sym.s[e_t]
 
     G = torch.zeros(sym.g_total, dtype=torch.float64, device=device)
+    GT = torch.zeros(sym.g_total, dtype=torch.float64, device=device)
     upd = {}  # front -> (batch tensor, batch index) of its pending update matrix
     for lv in range(sym.n_levels):
         fronts = sym.by_level[lv]
@@ -304,19 +318,25 @@ def factorize(sym: NDSymbolic, indptr, indices, values, device, max_batch_bytes:
             e = torch.arange(int(cnt.sum()), device=device) - torch.repeat_interleave(torch.cumsum(cnt, 0) - cnt, cnt)
             sb = dev_s[gb]
             row, col = e // sb, e % sb
-            dst = torch.as_tensor(sym.g_off[ch], device=device)[gb] + e
+            goff = torch.as_tensor(sym.g_off[ch], device=device)[gb]
+            dst = goff + e
+            dstT = goff + col * (sb + dev_u[gb]) + row  # (col, row) of the s x (s+u) transpose
             top = row < sb
-            G[dst[top]] = Linv.reshape(-1)[(gb * SM * SM + row * SM + col)[top]]
+            vtop = Linv.reshape(-1)[(gb * SM * SM + row * SM + col)[top]]
+            G[dst[top]] = vtop
+            GT[dstT[top]] = vtop
             if M is not None:
                 bot = ~top
-                G[dst[bot]] = M.reshape(-1)[(gb * UM * SM + (row - sb) * SM + col)[bot]]
-            del gb, e, sb, row, col, dst, top
+                vbot = M.reshape(-1)[(gb * UM * SM + (row - sb) * SM + col)[bot]]
+                G[dst[bot]] = vbot
+                GT[dstT[bot]] = vbot
+            del gb, e, sb, row, col, dst, dstT, goff, top
             if Upd is not None:
                 for b, t in enumerate(ch):
                     if sym.parent[t] >= 0:
                         upd[int(t)] = (Upd, b)
             del Linv, M
-    return G
+    return G, GT
 
 
 # ---------------------------------------------------------------------------
@@ -333,7 +353,7 @@ class _Plan(ctypes.Structure):
         ("front_s", ctypes.c_void_p), ("front_u", ctypes.c_void_p),
         ("g_off", ctypes.c_void_p), ("idx_off", ctypes.c_void_p), ("upd_off", ctypes.c_void_p),
         ("fidx", ctypes.c_void_p), ("gptr", ctypes.c_void_p), ("gsrc", ctypes.c_void_p),
-        ("G", ctypes.c_void_p),
+        ("G", ctypes.c_void_p), ("GT", ctypes.c_void_p),
     ]
 
 
@@ -341,38 +361,56 @@ class NDSolver:
     """Factor once (``A`` a torch CSR tensor on the device, FP64), then
     ``solve_into(w, x, R)`` with ``w, x`` (n, R) row-major FP64 on the device."""
 
-    def __init__(self, A: torch.Tensor, leaf: int = 128):
+    def __init__(self, A: torch.Tensor, leaf: int | None = None):
+        leaf = LEAF if leaf is None else leaf
         dev = A.device
+        self.leaf = leaf
         indptr = A.crow_indices().cpu().numpy()
         indices = A.col_indices().cpu().numpy()
         self.n = A.shape[0]
         self.sym = sym = NDSymbolic(indptr, indices, self.n, leaf)
-        self.G = factorize(sym, indptr, indices, A.values(), dev)
+        self.G, self.GT = factorize(sym, indptr, indices, A.values(), dev)
         i32 = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.int32, device=dev)  # noqa: E731
         i64 = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.int64, device=dev)  # noqa: E731
         self.t = {
-            "fwd_items": i32(sym.fwd_items.reshape(-1)), "bwd_items": i32(sym.bwd_items.reshape(-1)),
             "front_s": i32(sym.s), "front_u": i32(sym.u),
             "g_off": i64(sym.g_off), "idx_off": i64(sym.idx_off), "upd_off": i64(sym.upd_off),
             "fidx": i32(sym.fidx), "gptr": i64(sym.gptr), "gsrc": i64(sym.gsrc),
         }
-        self.fwd_level_ptr = np.ascontiguousarray(sym.fwd_level_ptr, dtype=np.int64)
-        self.bwd_level_ptr = np.ascontiguousarray(sym.bwd_level_ptr, dtype=np.int64)
         self.fwd_level_smax = np.ascontiguousarray(sym.fwd_level_smax, dtype=np.int32)
         self.bwd_level_mmax = np.ascontiguousarray(sym.bwd_level_mmax, dtype=np.int32)
         self.max_front = int((sym.s + sym.u).max()) if sym.nf else 0
         p = _Plan()
         p.n, p.n_fronts, p.n_levels, p.max_front = self.n, sym.nf, sym.n_levels, self.max_front
-        p.fwd_level_ptr = self.fwd_level_ptr.ctypes.data
-        p.bwd_level_ptr = self.bwd_level_ptr.ctypes.data
         p.fwd_level_smax = self.fwd_level_smax.ctypes.data
         p.bwd_level_mmax = self.bwd_level_mmax.ctypes.data
         for k, v in self.t.items():
             setattr(p, k, v.data_ptr())
         p.G = self.G.data_ptr()
+        p.GT = self.GT.data_ptr()
         self.plan = p
+        if self.n > 1_000_000:
+            # measured on B200: fatter items pay off once the leaf levels hold >100k of them
+            sym.build_items(65536, 128)
+        self._set_items()
         self._work = {}
-        self.factor_bytes = self.G.numel() * 8
+        self.factor_bytes = 2 * self.G.numel() * 8
+
+    def _set_items(self) -> None:
+        sym, dev, p = self.sym, self.G.device, self.plan
+        self.t["fwd_items"] = torch.as_tensor(sym.fwd_items.reshape(-1), dtype=torch.int32, device=dev)
+        self.t["bwd_items"] = torch.as_tensor(sym.bwd_items.reshape(-1), dtype=torch.int32, device=dev)
+        self.fwd_level_ptr = np.ascontiguousarray(sym.fwd_level_ptr, dtype=np.int64)
+        self.bwd_level_ptr = np.ascontiguousarray(sym.bwd_level_ptr, dtype=np.int64)
+        p.fwd_items = self.t["fwd_items"].data_ptr()
+        p.bwd_items = self.t["bwd_items"].data_ptr()
+        p.fwd_level_ptr = self.fwd_level_ptr.ctypes.data
+        p.bwd_level_ptr = self.bwd_level_ptr.ctypes.data
+
+    def set_items(self, item_bytes: int, max_rows: int) -> None:
+        """Re-cut the work items (a tuning knob: bytes of operator per CTA)."""
+        self.sym.build_items(item_bytes, max_rows)
+        self._set_items()
 
     def workspace(self, R: int, device):
         w = self._work.get(R)
@@ -396,7 +434,7 @@ class NDSolver:
         return x.to(rhs.dtype)
 
 
-def emulate_solve(sym: NDSymbolic, G: np.ndarray, w: np.ndarray) -> np.ndarray:
+def emulate_solve(sym: NDSymbolic, G: np.ndarray, GT: np.ndarray, w: np.ndarray) -> np.ndarray:
     """The kernels' arithmetic on the host, work item by work item (test use:
     it follows the same index maps and level order as ``ddx_coarse_solve_nd``)."""
     n = sym.n
@@ -429,7 +467,7 @@ def emulate_solve(sym: NDSymbolic, G: np.ndarray, w: np.ndarray) -> np.ndarray:
             s, u = int(sym.s[t]), int(sym.u[t])
             io, go = int(sym.idx_off[t]), int(sym.g_off[t])
             v = np.concatenate([y[sym.fidx[io:io + s]], -x[sym.fidx[io + s:io + s + u]]])
-            Gt = G[go:go + (s + u) * s].reshape(s + u, s)
+            GTt = GT[go:go + s * (s + u)].reshape(s, s + u)
             for c in range(c0, c0 + nc):
-                x[sym.fidx[io + c]] = Gt[:, c] @ v
+                x[sym.fidx[io + c]] = GTt[c] @ v
     return x
