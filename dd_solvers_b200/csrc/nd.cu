@@ -28,6 +28,7 @@ namespace {
 constexpr int kNdThreads = 256;
 constexpr int kNdWarps = kNdThreads / 32;
 constexpr int kNdSmemMax = 96 * 1024;  // the staged vector (front rows x RHS group)
+constexpr int kNdItemRows = 256;       // forward rows whose f_U is gathered up front (items hold <= 128)
 
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
@@ -55,11 +56,14 @@ __global__ void __launch_bounds__(kNdThreads)
              double* __restrict__ upd, const int* ist) {
   if (ist != nullptr && n_active(ist, R) == 0) return;
   extern __shared__ double fs[];
+  __shared__ double fu[kNdItemRows * RG];
   const int64_t it = item0 + blockIdx.x;
   const int t = A.items[3 * it], row0 = A.items[3 * it + 1], nrows = A.items[3 * it + 2];
   const int s = A.front_s[t];
   const int64_t io = A.idx_off[t], go = A.g_off[t], uo = A.upd_off[t];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // update rows of this item whose f_U is gathered in the prologue
+  const int u0 = max(row0, s), u1 = min(row0 + nrows, row0 + kNdItemRows);
   for (int r0 = 0; r0 < R; r0 += RG) {
     const int ng = min(RG, R - r0);
     // f_S = w_S + the children's contributions, in gather-map order
@@ -76,6 +80,20 @@ __global__ void __launch_bounds__(kNdThreads)
       }
 #pragma unroll
       for (int r = 0; r < RG; ++r) fs[p * RG + r] = acc[r];
+    }
+    // f_U of this item's update rows (children only), same order
+    for (int p = u0 + threadIdx.x; p < u1; p += kNdThreads) {
+      double acc[RG];
+#pragma unroll
+      for (int r = 0; r < RG; ++r) acc[r] = 0.0;
+      for (int64_t q = A.gptr[io + p]; q < A.gptr[io + p + 1]; ++q) {
+        const int64_t src = A.gsrc[q] * R + r0;
+#pragma unroll
+        for (int r = 0; r < RG; ++r)
+          if (r < ng) acc[r] += upd[src + r];
+      }
+#pragma unroll
+      for (int r = 0; r < RG; ++r) fu[(p - row0) * RG + r] = acc[r];
     }
     __syncthreads();
     for (int p = row0 + warp; p < row0 + nrows; p += kNdWarps) {
@@ -96,15 +114,21 @@ __global__ void __launch_bounds__(kNdThreads)
         for (int r = 0; r < RG; ++r)
           if (lane == r && r < ng) y[v * R + r0 + r] = acc[r];
       } else {
-        // f_U of this row (children only), then u_t = f_U - M f_S
+        // f_U of this row (children only, gathered above unless the item is
+        // longer than kNdItemRows), then u_t = f_U - M f_S
         double f[RG];
+        if (p < u1) {
 #pragma unroll
-        for (int r = 0; r < RG; ++r) f[r] = 0.0;
-        for (int64_t q = A.gptr[io + p]; q < A.gptr[io + p + 1]; ++q) {
-          const int64_t src = A.gsrc[q] * R + r0;
+          for (int r = 0; r < RG; ++r) f[r] = fu[(p - row0) * RG + r];
+        } else {
 #pragma unroll
-          for (int r = 0; r < RG; ++r)
-            if (r < ng) f[r] += upd[src + r];
+          for (int r = 0; r < RG; ++r) f[r] = 0.0;
+          for (int64_t q = A.gptr[io + p]; q < A.gptr[io + p + 1]; ++q) {
+            const int64_t src = A.gsrc[q] * R + r0;
+#pragma unroll
+            for (int r = 0; r < RG; ++r)
+              if (r < ng) f[r] += upd[src + r];
+          }
         }
         const int64_t dst = (uo + p - s) * R + r0;
 #pragma unroll

@@ -180,9 +180,10 @@ int ddx_schwarz_local_apply(int n_sub, int R, const int64_t* sub_ptr, const int*
                             void* ylocal, int acc_dtype, const int* ist, ddx_stream_t stream);
 /* Same product and block layout for small subdomains (the reference's DG
  * layouts: equal blocks of a few to a few dozen DOFs), one thread per output
- * entry. rows = sub_ptr[n_sub]; k_equal > 0 declares every subdomain to have
- * k_equal DOFs (k_equal * n_sub == rows), otherwise each row finds its
- * subdomain by binary search in sub_ptr. Any R >= 1. */
+ * entry (equal subdomains: a thread per 16 bytes of block rows). rows =
+ * sub_ptr[n_sub]; k_equal > 0 declares every subdomain to have k_equal DOFs
+ * (k_equal * n_sub == rows), otherwise each row finds its subdomain by binary
+ * search in sub_ptr. Blocks and every block start 16-byte aligned. Any R >= 1. */
 int ddx_schwarz_local_apply_small(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
                                   const int64_t* blk_off, const void* blocks, int block_dtype,
                                   const float* scale, int kmax, int k_equal, int64_t rows, const double* r,
@@ -292,11 +293,12 @@ int ddx_nd_order(int64_t n, const int64_t* indptr, const int64_t* indices, int l
 
 /* Multifrontal solve plan. Front t owns the (s_t + u_t) coarse indices
  * fidx[idx_off[t] ...] (its separator, then its update set) and the operator
- * G[g_off[t] ...] = [chol(F_SS)^-1; F_US F_SS^-1] ((s_t+u_t) x s_t, row-major).
+ * G[g_off[t] ...] = [chol(F_SS)^-1; F_US F_SS^-1] ((s_t+u_t) x s_t, row-major),
+ * with its transpose at GT[g_off[t] ...] (s_t x (s_t+u_t), row-major).
  * Its update vector lives at upd[upd_off[t] ...] (u_t rows of R values).
  * gptr/gsrc list, for every front position (idx_off numbering), the update
  * rows of its children to add, in a fixed order. Work items are int triples
- * (front, first row/column, count); fwd_level_ptr / bwd_level_ptr (HOST
+ * (front, first row of G_t / of G_t^T, count); fwd_level_ptr / bwd_level_ptr (HOST
  * arrays, n_levels + 1 entries) delimit the items of each level (leaves first
  * for the forward sweep, root first for the backward sweep), and
  * fwd_level_smax / bwd_level_mmax (HOST) give each level's largest s and
@@ -321,6 +323,7 @@ typedef struct ddx_nd_plan {
   const int64_t* gptr;
   const int64_t* gsrc;
   const double* G;
+  const double* GT;
 } ddx_nd_plan;
 
 /* x = A^-1 w for w, x of shape (n, R) (DOF-major, FP64). y (n*R doubles) and
