@@ -116,7 +116,7 @@ template <> struct Unpack<__nv_bfloat16, float> {
 // 16-byte vector per column; a CTA owns floor(256 / (ld / V)) whole blocks and
 // stages their inputs in shared memory once per right-hand side.
 template <typename TB, typename ACC>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)
     k_local_apply_small_eq(int n_sub, int R, int k, const int* __restrict__ sub_idx,
                            const int64_t* __restrict__ blk_off, const TB* __restrict__ blocks,
                            const float* __restrict__ scale, const double* __restrict__ r, ACC* __restrict__ y,

@@ -50,8 +50,9 @@ struct NdArgs {
   const double* GT;  // its transpose, s x (s+u) row-major per front (backward sweep)
 };
 
+// 4 CTAs per SM for the narrow RHS groups (latency-bound sweeps want warps in flight)
 template <int RG>
-__global__ void __launch_bounds__(kNdThreads)
+__global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
     k_nd_fwd(NdArgs A, int64_t item0, int R, const double* __restrict__ w, double* __restrict__ y,
              double* __restrict__ upd, const int* ist) {
   if (ist != nullptr && n_active(ist, R) == 0) return;
@@ -143,7 +144,7 @@ __global__ void __launch_bounds__(kNdThreads)
 // Backward item: rows c0 .. c0+nc of G_t^T (columns of G_t); a warp per row,
 // lanes over the s+u entries, v = [y_S; -x_U] staged in shared memory.
 template <int RG>
-__global__ void __launch_bounds__(kNdThreads)
+__global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
     k_nd_bwd(NdArgs A, int64_t item0, int R, const double* __restrict__ y, double* __restrict__ x,
              const int* ist) {
   if (ist != nullptr && n_active(ist, R) == 0) return;
