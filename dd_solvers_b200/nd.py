@@ -99,12 +99,20 @@ class NDSymbolic:
         s_first = np.concatenate([[0], np.cumsum(s_sizes)[:-1]])
         s_last = s_first + s_sizes - 1
         # subtree_last = last position in the subtree = own S last (post-order)
+        # the rows of A in elimination order: a front's separator rows are one slice
+        deg = np.diff(indptr)[perm]
+        p_ptr = np.zeros(n + 1, dtype=np.int64)
+        np.cumsum(deg, out=p_ptr[1:])
+        p_idx = indices[np.repeat(indptr[perm] - p_ptr[:-1], deg) + np.arange(int(p_ptr[-1]))] if n else indices
+        p_pos = pos[p_idx]
         U: list = [None] * nf
+        upos: list = [None] * nf
         for t in range(nf):
-            nb = [indices[indptr[v]:indptr[v + 1]] for v in S[t]]
-            cand = [np.concatenate(nb)] + [U[c] for c in children[t]]
-            c = np.unique(pos[np.concatenate(cand)]) if cand else np.zeros(0, dtype=np.int64)
-            U[t] = perm[c[c > s_last[t]]]
+            a, b = p_ptr[s_first[t]], p_ptr[s_first[t] + s_sizes[t]]
+            cand = [p_pos[a:b]] + [upos[c] for c in children[t]]
+            c = np.unique(np.concatenate(cand))
+            upos[t] = c[c > s_last[t]]
+            U[t] = perm[upos[t]]
         level = np.zeros(nf, dtype=np.int64)
         for t in range(nf):
             if children[t]:

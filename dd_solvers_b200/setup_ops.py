@@ -233,13 +233,30 @@ class BlockStore:
                 self.data[self.off_np[i]:self.off_np[i + 1]] = sw.reshape(-1)
             return
         qt = q.transpose(1, 2)  # column-major: row c of qt is column c of q
-        for b in range(B):
-            i = first + b
-            k, ld = int(self.ks[i]), int(self.lds[i])
-            if k == 0:
+        ks_b = np.asarray(self.ks[first:first + B])
+        for kk in np.unique(ks_b):
+            kk = int(kk)
+            if kk == 0:
                 continue
-            dst = self.data[self.off_np[i]:self.off_np[i] + k * ld].view(k, ld)
-            dst[:, :k] = qt[b, :k, :k]
+            sel = np.nonzero(ks_b == kk)[0]
+            if kk > 64:  # few large blocks: one slice copy each
+                for b in sel:
+                    i = first + int(b)
+                    ld = int(self.lds[i])
+                    dst = self.data[self.off_np[i]:self.off_np[i] + kk * ld].view(kk, ld)
+                    dst[:, :kk] = qt[b, :kk, :kk]
+                continue
+            # many small blocks of one size: one scatter per group of <= 2^22 entries
+            ld = int(self.lds[first + int(sel[0])])
+            cr = (torch.arange(kk, device=q.device)[:, None] * ld
+                  + torch.arange(kk, device=q.device)[None, :]).reshape(-1)  # column c, row r
+            step = max(1, (1 << 22) // (kk * kk))
+            for a in range(0, len(sel), step):
+                part = sel[a:a + step]
+                offs = torch.as_tensor(self.off_np[first + part], device=q.device)
+                dst = (offs[:, None] + cr[None, :]).reshape(-1)
+                src = qt[torch.as_tensor(part, device=q.device), :kk, :kk].reshape(-1)
+                self.data[dst] = src
 
     def dense_q(self, i: int) -> torch.Tensor:
         """Stored (quantised, unscaled) block i as a dense [row, col] k x k tensor."""
