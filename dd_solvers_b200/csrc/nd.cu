@@ -48,6 +48,8 @@ struct NdArgs {
   const int64_t* gsrc;
   const double* G;   // forward operator, (s+u) x s row-major per front
   const double* GT;  // its transpose, s x (s+u) row-major per front (backward sweep)
+  const int64_t* s_first;  // elimination position of each front's first separator vertex
+  const int* fpos;         // elimination position of every front position
 };
 
 // 4 CTAs per SM for the narrow RHS groups (latency-bound sweeps want warps in flight)
@@ -110,10 +112,10 @@ __global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
 #pragma unroll
       for (int r = 0; r < RG; ++r) acc[r] = warp_sum_d(acc[r]);
       if (p < s) {
-        const int64_t v = A.fidx[io + p];
+        const int64_t e = A.s_first[t] + p;  // y is kept in elimination order
 #pragma unroll
         for (int r = 0; r < RG; ++r)
-          if (lane == r && r < ng) y[v * R + r0 + r] = acc[r];
+          if (lane == r && r < ng) y[e * R + r0 + r] = acc[r];
       } else {
         // f_U of this row (children only, gathered above unless the item is
         // longer than kNdItemRows), then u_t = f_U - M f_S
@@ -145,8 +147,8 @@ __global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
 // lanes over the s+u entries, v = [y_S; -x_U] staged in shared memory.
 template <int RG>
 __global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
-    k_nd_bwd(NdArgs A, int64_t item0, int R, const double* __restrict__ y, double* __restrict__ x,
-             const int* ist) {
+    k_nd_bwd(NdArgs A, int64_t item0, int R, const double* __restrict__ y, double* __restrict__ xe,
+             double* __restrict__ x, const int* ist) {
   if (ist != nullptr && n_active(ist, R) == 0) return;
   extern __shared__ double vs[];
   const int64_t it = item0 + blockIdx.x;
@@ -156,11 +158,14 @@ __global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int r0 = 0; r0 < R; r0 += RG) {
     const int ng = min(RG, R - r0);
+    // y and the solution are read in elimination order: the separator is one
+    // range, the update set a few ranges of ancestor separators
+    const int64_t sf = A.s_first[t];
     for (int p = threadIdx.x; p < m; p += kNdThreads) {
-      const int64_t v = A.fidx[io + p];
+      const int64_t e = p < s ? sf + p : (int64_t)A.fpos[io + p];
 #pragma unroll
       for (int r = 0; r < RG; ++r)
-        vs[p * RG + r] = r < ng ? (p < s ? y[v * R + r0 + r] : -x[v * R + r0 + r]) : 0.0;
+        vs[p * RG + r] = r < ng ? (p < s ? y[e * R + r0 + r] : -xe[e * R + r0 + r]) : 0.0;
     }
     __syncthreads();
     for (int c = c0 + warp; c < c0 + nc; c += kNdWarps) {
@@ -178,7 +183,10 @@ __global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
       const int64_t v = A.fidx[io + c];
 #pragma unroll
       for (int r = 0; r < RG; ++r)
-        if (lane == r && r < ng) x[v * R + r0 + r] = acc[r];
+        if (lane == r && r < ng) {
+          xe[(sf + c) * R + r0 + r] = acc[r];  // for the descendants
+          x[v * R + r0 + r] = acc[r];          // the result, in the caller's order
+        }
     }
     __syncthreads();
   }
@@ -186,7 +194,7 @@ __global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
 
 template <int RG>
 int nd_sweeps(const ddx_nd_plan* P, const NdArgs& fa, const NdArgs& ba, int R, const double* w, double* x,
-              double* y, double* upd, const int* ist, cudaStream_t s) {
+              double* y, double* xe, double* upd, const int* ist, cudaStream_t s) {
   const size_t smem_cap = (size_t)kNdSmemMax;
   cudaFuncSetAttribute(k_nd_fwd<RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap);
   cudaFuncSetAttribute(k_nd_bwd<RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap);
@@ -200,7 +208,7 @@ int nd_sweeps(const ddx_nd_plan* P, const NdArgs& fa, const NdArgs& ba, int R, c
     const int64_t a = P->bwd_level_ptr[lv], b = P->bwd_level_ptr[lv + 1];
     if (b == a) continue;
     const size_t smem = (size_t)std::max(P->bwd_level_mmax[lv], 1) * RG * sizeof(double);
-    k_nd_bwd<RG><<<(unsigned)(b - a), kNdThreads, smem, s>>>(ba, a, R, y, x, ist);
+    k_nd_bwd<RG><<<(unsigned)(b - a), kNdThreads, smem, s>>>(ba, a, R, y, xe, x, ist);
   }
   DDX_LAUNCH_CHECK("ddx_coarse_solve_nd");
   return DDX_OK;
@@ -372,16 +380,17 @@ int ddx_nd_order(int64_t n, const int64_t* indptr, const int64_t* indices, int l
   return DDX_OK;
 }
 
-int ddx_coarse_solve_nd(const ddx_nd_plan* P, int R, const double* w, double* x, double* y, double* upd,
-                        const int* ist, ddx_stream_t stream) {
-  DDX_REQUIRE(P && w && x && y && upd && R >= 1, "ddx_coarse_solve_nd: bad arguments");
+int ddx_coarse_solve_nd(const ddx_nd_plan* P, int R, const double* w, double* x, double* y, double* xe,
+                        double* upd, const int* ist, ddx_stream_t stream) {
+  DDX_REQUIRE(P && w && x && y && xe && upd && R >= 1, "ddx_coarse_solve_nd: bad arguments");
+  DDX_REQUIRE(P->s_first && P->fpos, "ddx_coarse_solve_nd: plan without elimination positions");
   DDX_REQUIRE(P->fwd_level_ptr && P->bwd_level_ptr && P->fwd_level_smax && P->bwd_level_mmax,
               "ddx_coarse_solve_nd: plan without level tables");
   if (P->n == 0) return DDX_OK;
   cudaStream_t s = (cudaStream_t)stream;
   DDX_REQUIRE(P->G && P->GT, "ddx_coarse_solve_nd: plan without operators");
   NdArgs fa{P->fwd_items, P->front_s, P->front_u, P->g_off, P->idx_off, P->upd_off, P->fidx, P->gptr,
-            P->gsrc, P->G, P->GT};
+            P->gsrc, P->G, P->GT, P->s_first, P->fpos};
   NdArgs ba = fa;
   ba.items = P->bwd_items;
   const int64_t mmax = std::max<int64_t>(P->max_front, 1);
@@ -391,11 +400,11 @@ int ddx_coarse_solve_nd(const ddx_nd_plan* P, int R, const double* w, double* x,
   DDX_REQUIRE(mmax * (int64_t)sizeof(double) <= kNdSmemMax, "ddx_coarse_solve_nd: front of %lld exceeds %d B",
               (long long)mmax, kNdSmemMax);
   switch (rg) {
-    case 1: return nd_sweeps<1>(P, fa, ba, R, w, x, y, upd, ist, s);
-    case 2: return nd_sweeps<2>(P, fa, ba, R, w, x, y, upd, ist, s);
-    case 4: return nd_sweeps<4>(P, fa, ba, R, w, x, y, upd, ist, s);
-    case 8: return nd_sweeps<8>(P, fa, ba, R, w, x, y, upd, ist, s);
-    default: return nd_sweeps<16>(P, fa, ba, R, w, x, y, upd, ist, s);
+    case 1: return nd_sweeps<1>(P, fa, ba, R, w, x, y, xe, upd, ist, s);
+    case 2: return nd_sweeps<2>(P, fa, ba, R, w, x, y, xe, upd, ist, s);
+    case 4: return nd_sweeps<4>(P, fa, ba, R, w, x, y, xe, upd, ist, s);
+    case 8: return nd_sweeps<8>(P, fa, ba, R, w, x, y, xe, upd, ist, s);
+    default: return nd_sweeps<16>(P, fa, ba, R, w, x, y, xe, upd, ist, s);
   }
 }
 

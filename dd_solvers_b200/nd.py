@@ -362,6 +362,7 @@ class _Plan(ctypes.Structure):
         ("g_off", ctypes.c_void_p), ("idx_off", ctypes.c_void_p), ("upd_off", ctypes.c_void_p),
         ("fidx", ctypes.c_void_p), ("gptr", ctypes.c_void_p), ("gsrc", ctypes.c_void_p),
         ("G", ctypes.c_void_p), ("GT", ctypes.c_void_p),
+        ("s_first", ctypes.c_void_p), ("fpos", ctypes.c_void_p),
     ]
 
 
@@ -384,6 +385,7 @@ class NDSolver:
             "front_s": i32(sym.s), "front_u": i32(sym.u),
             "g_off": i64(sym.g_off), "idx_off": i64(sym.idx_off), "upd_off": i64(sym.upd_off),
             "fidx": i32(sym.fidx), "gptr": i64(sym.gptr), "gsrc": i64(sym.gsrc),
+            "s_first": i64(np.cumsum(sym.s) - sym.s), "fpos": i32(sym.pos[sym.fidx]),
         }
         self.fwd_level_smax = np.ascontiguousarray(sym.fwd_level_smax, dtype=np.int32)
         self.bwd_level_mmax = np.ascontiguousarray(sym.bwd_level_mmax, dtype=np.int32)
@@ -424,6 +426,7 @@ class NDSolver:
         w = self._work.get(R)
         if w is None:
             w = {"y": torch.empty(self.n * R, dtype=torch.float64, device=device),
+                 "xe": torch.empty(self.n * R, dtype=torch.float64, device=device),
                  "upd": torch.empty(max(self.sym.upd_total, 1) * R, dtype=torch.float64, device=device)}
             self._work[R] = w
         return w
@@ -431,7 +434,7 @@ class NDSolver:
     def solve_into(self, w: torch.Tensor, x: torch.Tensor, R: int, ist=None) -> None:
         ws = self.workspace(R, w.device)
         L.call("ddx_coarse_solve_nd", ctypes.addressof(self.plan), R, L.ptr(w), L.ptr(x), L.ptr(ws["y"]),
-               L.ptr(ws["upd"]), L.ptr(ist), L.stream_ptr())
+               L.ptr(ws["xe"]), L.ptr(ws["upd"]), L.ptr(ist), L.stream_ptr())
 
     def solve(self, rhs: torch.Tensor) -> torch.Tensor:
         L.require_cuda(rhs, "rhs")
@@ -448,8 +451,11 @@ def emulate_solve(sym: NDSymbolic, G: np.ndarray, GT: np.ndarray, w: np.ndarray)
     n = sym.n
     w = np.asarray(w, dtype=np.float64).reshape(n, -1)
     R = w.shape[1]
-    y = np.zeros((n, R))
+    y = np.zeros((n, R))   # forward result, elimination order
+    xe = np.zeros((n, R))  # solution, elimination order
     x = np.zeros((n, R))
+    s_first = np.cumsum(sym.s) - sym.s
+    fpos = sym.pos[sym.fidx]
     upd = np.zeros((max(sym.upd_total, 1), R))
     for lv in range(sym.n_levels):
         for it in range(sym.fwd_level_ptr[lv], sym.fwd_level_ptr[lv + 1]):
@@ -466,7 +472,7 @@ def emulate_solve(sym: NDSymbolic, G: np.ndarray, GT: np.ndarray, w: np.ndarray)
             for p in range(r0, r0 + nr):
                 out = Gt[p] @ f[:s] if s else np.zeros(R)
                 if p < s:
-                    y[sym.fidx[io + p]] = out
+                    y[s_first[t] + p] = out
                 else:
                     upd[sym.upd_off[t] + p - s] = f[p] - out
     for j in range(sym.n_levels):
@@ -474,8 +480,9 @@ def emulate_solve(sym: NDSymbolic, G: np.ndarray, GT: np.ndarray, w: np.ndarray)
             t, c0, nc = sym.bwd_items[it]
             s, u = int(sym.s[t]), int(sym.u[t])
             io, go = int(sym.idx_off[t]), int(sym.g_off[t])
-            v = np.concatenate([y[sym.fidx[io:io + s]], -x[sym.fidx[io + s:io + s + u]]])
+            v = np.concatenate([y[s_first[t]:s_first[t] + s], -xe[fpos[io + s:io + s + u]]])
             GTt = GT[go:go + s * (s + u)].reshape(s, s + u)
             for c in range(c0, c0 + nc):
-                x[sym.fidx[io + c]] = GTt[c] @ v
+                xe[s_first[t] + c] = GTt[c] @ v
+                x[sym.fidx[io + c]] = xe[s_first[t] + c]
     return x

@@ -324,13 +324,16 @@ typedef struct ddx_nd_plan {
   const int64_t* gsrc;
   const double* G;
   const double* GT;
+  const int64_t* s_first; /* elimination position of front t's first separator vertex */
+  const int* fpos;        /* elimination position of every front position (idx_off numbering) */
 } ddx_nd_plan;
 
-/* x = A^-1 w for w, x of shape (n, R) (DOF-major, FP64). y (n*R doubles) and
+/* x = A^-1 w for w, x of shape (n, R) (DOF-major, FP64). y and xe (n*R
+ * doubles each: the forward result and the solution in elimination order) and
  * upd (sum_t u_t * R doubles) are caller-owned scratch. With ist (PCG state),
  * nothing runs once every right-hand side has converged. Deterministic. */
-int ddx_coarse_solve_nd(const ddx_nd_plan* plan, int R, const double* w, double* x, double* y, double* upd,
-                        const int* ist, ddx_stream_t stream);
+int ddx_coarse_solve_nd(const ddx_nd_plan* plan, int R, const double* w, double* x, double* y, double* xe,
+                        double* upd, const int* ist, ddx_stream_t stream);
 
 /* ---- Differentiable solve -----------------------------------------------
  * No counterpart in the reference (it has no autograd). Per-cell coefficient
