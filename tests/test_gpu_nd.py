@@ -46,7 +46,7 @@ def test_nd_solve_matches_host_emulation_and_is_deterministic():
     x1 = solver.solve(w)
     x2 = solver.solve(w)
     assert torch.equal(x1, x2)
-    xe = nd.emulate_solve(solver.sym, solver.G.cpu().numpy(), w.cpu().numpy())
+    xe = nd.emulate_solve(solver.sym, solver.G.cpu().numpy(), solver.GT.cpu().numpy(), w.cpu().numpy())
     np.testing.assert_allclose(x1.cpu().numpy(), xe, rtol=1e-12, atol=1e-12 * np.abs(xe).max())
 
 
@@ -76,3 +76,26 @@ def test_dg_experiment_reproduces_reference_log(method):
     assert out["history_max_rel_diff_first10"] < 1e-10
     # later norms drift only by rounding (hybrid converges to ~1e-10 of r0)
     assert out["history_max_rel_diff"] < 1e-2
+
+
+@pytest.mark.parametrize("precision,expected", [("f16", 61), ("bf16", 62), ("f32", 61)])
+def test_dg_experiment_mixed_precision_iterations(precision, expected):
+    """Low-precision blocks (FP64 preconditioner, plain CG as the reference
+    runs it): the reference's logged iteration counts for S10 / S8 / S8."""
+    log = json.load(open(LOG))
+    out = dg_experiments.run("S10", "S8", "S8", "hybrid", precision, reps=1, log=log)
+    assert out["reference_iterations"] == expected
+    assert abs(out["iterations"] - expected) <= 1
+    assert out["history_max_rel_diff_first10"] < 1e-5
+
+
+def test_dg_experiment_quadrilateral_cells():
+    """Solver and coarse cells on the C-level quadrilateral grids (the DOFs are
+    permuted into (coarse, solver) groups first): S9 fine, C8 solvers (24 DOFs
+    each), C6 coarse cells; the PCG converges and the grouping is consistent."""
+    A, b, kw = dg_experiments.build("S9", "C8", "C6")
+    assert kw["dofs_per_solver"] == 24
+    assert int(kw["solvers_per_coarse"].sum()) == 4 ** 8
+    assert bool((kw["solvers_per_coarse"] == 16).all())
+    out = dg_experiments.run("S9", "C8", "C6", "hybrid", "f64", reps=1)
+    assert out["iterations"] < 200
