@@ -23,6 +23,9 @@ divided by their number.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2]
 
+At N = 1 the c2 line also carries "reference_experiment": the reference's own DG-SIPG experiment S10 / S8 /
+S8 (hybrid, FP16 blocks) solved through this package, next to the reference's logged A100 time for it.
+
 --impl reference times the FP64 CPU restatement of the same algorithm on the
 host cores (the reference's own solver runs on GPUs only; its CPU behaviour is
 what the restatement reproduces) on a bounded sample of the workload.
@@ -38,6 +41,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -68,7 +72,9 @@ class Clocks:
     def __init__(self, device_index: int):
         self.idx = device_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        # raw samples go to DDX_CLOCKS_DIR (default: the system temp directory); the line carries the summary
+        self.path = os.path.join(os.environ.get("DDX_CLOCKS_DIR", tempfile.gettempdir()),
+                                 f"ddx_clocks_{os.getpid()}.csv")
 
     def start(self):
         try:
@@ -626,6 +632,33 @@ def run_ours(args, spec, rank: int, world: int):
     return out, prob, cal
 
 
+# The reference's own logged run of its DG-SIPG experiment S10 / S8 / S8 (6.29M DOFs, hybrid Schwarz, FP64
+# preconditioner with FP16 local blocks, CG rtol 1e-9) on an A100: results/experiment_precisions.csv, row
+# "CG(HybridSchwarz(torch.float64, Inv(torch.float16), CUDSS), bsr_matmul=True)", min over 10 solves.
+REFERENCE_EXPERIMENT = {"fine": "S10", "solvers": "S8", "coarse": "S8", "method": "hybrid", "precision": "f16",
+                        "reference_iterations": 61, "reference_a100_ms_per_solve": 183.0207977294922}
+
+
+def reference_experiment() -> dict:
+    """The same experiment through this package (its SIPG system restated by dd_solvers_b200.dg, solved
+    through the drop-in API, timed like the reference: CUDA events, min over repeated solves, setup
+    excluded)."""
+    import torch
+
+    from dd_solvers_b200 import dg_experiments
+
+    torch.cuda.empty_cache()
+    e = REFERENCE_EXPERIMENT
+    r = dg_experiments.run(e["fine"], e["solvers"], e["coarse"], e["method"], e["precision"], reps=5)
+    torch.cuda.empty_cache()
+    return {"experiment": "reference DG-SIPG P1, fine S10 (6,291,456 DOFs), 131,072 subdomains of 48 DOFs, "
+                          "131,072 P0 coarse DOFs, HybridSchwarz(float64, Inv(float16), CUDSS), CG rtol 1e-9",
+            "iterations": r["iterations"], "reference_iterations": e["reference_iterations"],
+            "ms_per_solve": r["solve_ms_min"], "reference_a100_ms_per_solve": e["reference_a100_ms_per_solve"],
+            "speedup_vs_reference_a100": e["reference_a100_ms_per_solve"] / r["solve_ms_min"],
+            "source": "results/experiment_precisions.csv (the reference's log)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -638,6 +671,8 @@ def main():
     ap.add_argument("--replace-every", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batched", type=int, default=64, help="also time R right-hand sides per solve (0: skip)")
+    ap.add_argument("--no-reference-experiment", action="store_true",
+                    help="skip the reference's own DG experiment (run after the c2 measurement at N = 1)")
     args = ap.parse_args()
     spec = WORKLOADS[args.workload]
 
@@ -668,6 +703,8 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     runner = run_grad if spec["kind"] == "grad" else run_ours
     out, prob, cal = runner(args, spec, rank, world)
+    if rank == 0 and world == 1 and args.workload == "c2" and not args.no_reference_experiment:
+        out["reference_experiment"] = reference_experiment()
     if rank == 0:
         if not args.no_cpu_baseline:
             cb = cpu_time_per_rhs(prob, cal["f64"]["iterations"])
