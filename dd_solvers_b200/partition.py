@@ -156,3 +156,57 @@ def q1_coarse_restriction(dim: int, n_el: int, parts_per_axis: int) -> sps.csr_m
     R = P.T.tocsr()
     R.sort_indices()
     return R
+
+
+# ---------------------------------------------------------------------------
+# the same decompositions on the device (torch; any device)
+# ---------------------------------------------------------------------------
+
+def rcb_owner_device(coords, n_parts: int):
+    """``rcb_owner`` on a torch ``(n, dim)`` FP64 tensor: per level, the parts'
+    bounding boxes by segmented min/max, the longest axis (first on ties, as
+    ``np.argmax``), the midpoint, and the side of every node. The arithmetic is
+    the same, so the owners are identical to ``rcb_owner``."""
+    import torch
+
+    assert n_parts & (n_parts - 1) == 0, "n_parts must be a power of two"
+    n, dim = coords.shape
+    dev = coords.device
+    owner = torch.zeros(n, dtype=torch.int64, device=dev)
+    ar = torch.arange(n, device=dev)
+    for lv in range(int(np.log2(n_parts))):
+        P = 1 << lv
+        idx = owner[:, None].expand(n, dim)
+        lo = torch.full((P, dim), float("inf"), dtype=coords.dtype, device=dev).scatter_reduce(
+            0, idx, coords, "amin", include_self=True)
+        hi = torch.full((P, dim), float("-inf"), dtype=coords.dtype, device=dev).scatter_reduce(
+            0, idx, coords, "amax", include_self=True)
+        axis = torch.argmax(hi - lo, dim=1)
+        mid = 0.5 * (lo + hi)[torch.arange(P, device=dev), axis]
+        side = (coords[ar, axis[owner]] >= mid[owner]).to(torch.int64)
+        owner = owner * 2 + side
+    return owner.to(torch.int32)
+
+
+def overlapping_subdomains_device(crow, col, owner, n_parts: int, overlap: int):
+    """``overlapping_subdomains`` from a device CSR pattern (``crow``, ``col``) and
+    owners: the part-by-DOF incidence grown by ``overlap`` sparse products with
+    the matrix graph (cuSPARSE SpGEMM through torch), columns sorted. Returns
+    ``(sub_ptr int64, sub_idx int32)`` torch tensors on the same device."""
+    import torch
+
+    from .setup_ops import spgemm_sorted
+
+    dev = crow.device
+    n = crow.numel() - 1
+    order = torch.argsort(owner.to(torch.int64), stable=True)
+    counts = torch.bincount(owner.to(torch.int64), minlength=n_parts)
+    ptr = torch.zeros(n_parts + 1, dtype=torch.int64, device=dev)
+    ptr[1:] = torch.cumsum(counts, 0)
+    S = torch.sparse_csr_tensor(ptr, order, torch.ones(n, dtype=torch.float64, device=dev), (n_parts, n))
+    G = torch.sparse_csr_tensor(crow.to(torch.int64), col.to(torch.int64),
+                                torch.ones(col.numel(), dtype=torch.float64, device=dev), (n, n))
+    for _ in range(overlap):
+        p, c, _v = spgemm_sorted(S, G)
+        S = torch.sparse_csr_tensor(p, c, torch.ones(c.numel(), dtype=torch.float64, device=dev), (n_parts, n))
+    return S.crow_indices().to(torch.int64), S.col_indices().to(torch.int32)

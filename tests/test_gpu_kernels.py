@@ -405,3 +405,18 @@ def test_bsr_dg_pattern_3d(cuda):
     expected = (m.to_dense() @ x).to(cuda)
     y = FastBSR(m.to(cuda)) @ x.to(cuda)
     assert torch.allclose(y, expected, rtol=1e-12, atol=1e-12)
+
+
+def test_device_partitioning_on_gpu(cuda):
+    """RCB owners and overlapping subdomains computed on the GPU equal the host
+    versions (C5-style jittered P1 nodes, 256 parts, one layer of overlap)."""
+    from dd_solvers_b200 import partition, problems
+
+    P = problems.p1_jittered(257, 0.3, 1.0, 11)
+    o_host = partition.rcb_owner(P.coords, 256)
+    o_dev = partition.rcb_owner_device(torch.as_tensor(P.coords, device=cuda), 256)
+    assert np.array_equal(o_host, o_dev.cpu().numpy())
+    sp, si = partition.overlapping_subdomains(P.matrix, o_host, 256, 1)
+    sp_t, si_t = partition.overlapping_subdomains_device(
+        torch.as_tensor(P.matrix.indptr, device=cuda), torch.as_tensor(P.matrix.indices, device=cuda), o_dev, 256, 1)
+    assert np.array_equal(sp, sp_t.cpu().numpy()) and np.array_equal(si, si_t.cpu().numpy())

@@ -287,3 +287,23 @@ def test_dg_block_patterns_match_the_reference_meshes():
     n = len(crow3) - 1
     M = sps.csr_matrix((np.ones(len(col3)), col3, crow3), shape=(n, n))
     assert abs(M - M.T).nnz == 0 and np.diff(crow3).max() == 5
+
+
+@pytest.mark.parametrize("parts", [8, 64])
+def test_device_partitioning_matches_host(parts):
+    """RCB owners and overlap growth in torch (here on CPU tensors; the GPU
+    test runs them on cuda) equal the numpy/SciPy versions exactly."""
+    import torch
+
+    from dd_solvers_b200 import partition, problems
+
+    P = problems.p1_jittered(97, 0.3, 1.0, 5)
+    o_host = partition.rcb_owner(P.coords, parts)
+    o_dev = partition.rcb_owner_device(torch.as_tensor(P.coords), parts).numpy()
+    assert np.array_equal(o_host, o_dev)
+    for overlap in (0, 1, 2):
+        sp, si = partition.overlapping_subdomains(P.matrix, o_host, parts, overlap)
+        sp_t, si_t = partition.overlapping_subdomains_device(
+            torch.as_tensor(P.matrix.indptr), torch.as_tensor(P.matrix.indices), torch.as_tensor(o_host), parts,
+            overlap)
+        assert np.array_equal(sp, sp_t.numpy()) and np.array_equal(si, si_t.numpy())
