@@ -30,6 +30,27 @@ constexpr int kNdWarps = kNdThreads / 32;
 constexpr int kNdSmemMax = 96 * 1024;  // the staged vector (front rows x RHS group)
 constexpr int kNdItemRows = 256;       // forward rows whose f_U is gathered up front (items hold <= 128)
 
+// Programmatic dependent launch: each level's kernel is launched so that it
+// may start while the previous one drains; it reads only the static plan
+// before griddepcontrol.wait, which returns once the previous grid's writes
+// are visible.
+__device__ __forceinline__ void wait_previous_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename Kernel, typename... Args>
+cudaError_t launch_after_previous(Kernel kernel, unsigned grid, size_t smem, cudaStream_t stream, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kNdThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -57,7 +78,6 @@ template <int RG>
 __global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
     k_nd_fwd(NdArgs A, int64_t item0, int R, const double* __restrict__ w, double* __restrict__ y,
              double* __restrict__ upd, const int* ist) {
-  if (ist != nullptr && n_active(ist, R) == 0) return;
   extern __shared__ double fs[];
   __shared__ double fu[kNdItemRows * RG];
   const int64_t it = item0 + blockIdx.x;
@@ -65,6 +85,8 @@ __global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
   const int s = A.front_s[t];
   const int64_t io = A.idx_off[t], go = A.g_off[t], uo = A.upd_off[t];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  wait_previous_grid();
+  if (ist != nullptr && n_active(ist, R) == 0) return;
   // update rows of this item whose f_U is gathered in the prologue
   const int u0 = max(row0, s), u1 = min(row0 + nrows, row0 + kNdItemRows);
   for (int r0 = 0; r0 < R; r0 += RG) {
@@ -149,13 +171,14 @@ template <int RG>
 __global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
     k_nd_bwd(NdArgs A, int64_t item0, int R, const double* __restrict__ y, double* __restrict__ xe,
              double* __restrict__ x, const int* ist) {
-  if (ist != nullptr && n_active(ist, R) == 0) return;
   extern __shared__ double vs[];
   const int64_t it = item0 + blockIdx.x;
   const int t = A.items[3 * it], c0 = A.items[3 * it + 1], nc = A.items[3 * it + 2];
   const int s = A.front_s[t], m = s + A.front_u[t];
   const int64_t io = A.idx_off[t], go = A.g_off[t];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  wait_previous_grid();
+  if (ist != nullptr && n_active(ist, R) == 0) return;
   for (int r0 = 0; r0 < R; r0 += RG) {
     const int ng = min(RG, R - r0);
     // y and the solution are read in elimination order: the separator is one
@@ -202,13 +225,13 @@ int nd_sweeps(const ddx_nd_plan* P, const NdArgs& fa, const NdArgs& ba, int R, c
     const int64_t a = P->fwd_level_ptr[lv], b = P->fwd_level_ptr[lv + 1];
     if (b == a) continue;
     const size_t smem = (size_t)std::max(P->fwd_level_smax[lv], 1) * RG * sizeof(double);
-    k_nd_fwd<RG><<<(unsigned)(b - a), kNdThreads, smem, s>>>(fa, a, R, w, y, upd, ist);
+    launch_after_previous(k_nd_fwd<RG>, (unsigned)(b - a), smem, s, fa, a, R, w, y, upd, ist);
   }
   for (int lv = 0; lv < P->n_levels; ++lv) {
     const int64_t a = P->bwd_level_ptr[lv], b = P->bwd_level_ptr[lv + 1];
     if (b == a) continue;
     const size_t smem = (size_t)std::max(P->bwd_level_mmax[lv], 1) * RG * sizeof(double);
-    k_nd_bwd<RG><<<(unsigned)(b - a), kNdThreads, smem, s>>>(ba, a, R, y, xe, x, ist);
+    launch_after_previous(k_nd_bwd<RG>, (unsigned)(b - a), smem, s, ba, a, R, (const double*)y, xe, x, ist);
   }
   DDX_LAUNCH_CHECK("ddx_coarse_solve_nd");
   return DDX_OK;
