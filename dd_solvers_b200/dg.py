@@ -58,8 +58,16 @@ def _f_continuous(x, y):
         - y * torch.sin(4 * x * pi) * torch.cos(4 * y * pi))
 
 
+def _u_continuous(x, y):
+    return torch.sin(4 * x * math.pi) * torch.sin(4 * y * math.pi)
+
+
 def _rho_one(x, y):
     return torch.ones_like(x)
+
+
+def _u_constant(x, y):
+    return torch.sin(x * math.pi) * torch.sin(y * math.pi)
 
 
 def _f_constant(x, y):
@@ -78,10 +86,37 @@ class TestCase:
     delta: float
     rho: object
     f: object
+    solution: object = None  # exact solution (problems.py:23-74)
 
 
-CONTINUOUS_COEFFICIENT_2D = TestCase("continuous coefficient 2D", 7.0, _rho_continuous, _f_continuous)
-CONSTANT_COEFFICIENT_2D = TestCase("constant coefficient 2D", 7.0, _rho_one, _f_constant)
+CONTINUOUS_COEFFICIENT_2D = TestCase("continuous coefficient 2D", 7.0, _rho_continuous, _f_continuous,
+                                     _u_continuous)
+CONSTANT_COEFFICIENT_2D = TestCase("constant coefficient 2D", 7.0, _rho_one, _f_constant, _u_constant)
+
+# 7-point degree-5 rule on the reference triangle (Dunavant 1985): barycentric points, weights summing to 1
+_Q7_A, _Q7_B = 0.059715871789770, 0.470142064105115
+_Q7_P = [(1 / 3, 1 / 3, 1 / 3),
+         (_Q7_A, (1 - _Q7_A) / 2, (1 - _Q7_A) / 2), ((1 - _Q7_A) / 2, _Q7_A, (1 - _Q7_A) / 2),
+         ((1 - _Q7_A) / 2, (1 - _Q7_A) / 2, _Q7_A),
+         (_Q7_B, (1 - _Q7_B) / 2, (1 - _Q7_B) / 2), ((1 - _Q7_B) / 2, _Q7_B, (1 - _Q7_B) / 2),
+         ((1 - _Q7_B) / 2, (1 - _Q7_B) / 2, _Q7_B)]
+_Q7_W = [0.225] + [0.132394152788506] * 3 + [0.125939180544827] * 3
+
+
+def l2_error(mesh: "TriangleMesh", u, solution) -> float:
+    """``||u_h - u||_L2`` of a DG P1 field (DOF ``3 c + i`` = vertex ``i`` of cell ``c``)
+    against an exact solution, by a degree-5 quadrature on every triangle (the
+    reference reports this norm as "error L2 norm", ``experiments.py:282-297``)."""
+    p = mesh.vertices[mesh.cells]
+    u = torch.as_tensor(u, dtype=torch.float64, device=p.device).reshape(-1, 3)
+    d1, d2 = p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]
+    area = (d1[:, 0] * d2[:, 1] - d2[:, 0] * d1[:, 1]).abs() / 2
+    err2 = torch.zeros_like(area)
+    for (l0, l1, l2), wq in zip(_Q7_P, _Q7_W):
+        q = l0 * p[:, 0] + l1 * p[:, 1] + l2 * p[:, 2]
+        uh = l0 * u[:, 0] + l1 * u[:, 1] + l2 * u[:, 2]
+        err2 += wq * (uh - solution(q[:, 0], q[:, 1])) ** 2
+    return float(torch.sqrt((err2 * area).sum()))
 
 
 @dataclasses.dataclass

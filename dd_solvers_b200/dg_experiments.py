@@ -58,10 +58,11 @@ def solvers_to_coarse(solvers: str, coarse: str, device) -> torch.Tensor:
     return _quad_of(cx, cy, int(coarse[1:]))
 
 
-def build(fine: str, solvers: str, coarse: str, device="cuda"):
+def build(fine: str, solvers: str, coarse: str, device="cuda", return_perm: bool = False):
     """Assemble ``S<fine>`` and group its DOFs by (coarse, solver) as the
     reference does (``experiments.py:205-236``). Returns the permuted system
-    and the setup keyword arguments."""
+    and the setup keyword arguments (and, with ``return_perm``, the permutation:
+    ``b_permuted = b[perm]``, so a solution maps back as ``x[inv(perm)]``)."""
     mesh = dg.uniform_mesh_2d(int(fine[1:]), device)
     system = dg.sipg_p1(mesh)
     f2s = dg.cell_mapping(mesh, solvers)
@@ -77,6 +78,8 @@ def build(fine: str, solvers: str, coarse: str, device="cuda"):
     kwargs = dict(dofs_per_solver=int((f2s == 0).sum()) * 3,
                   solvers_per_coarse=torch.bincount(s2c, minlength=n_coarse),
                   block_size=3)
+    if return_perm:
+        return A, b, kwargs, perm
     return A, b, kwargs
 
 

@@ -139,3 +139,20 @@ def test_s10_oracle_residual_history_matches_reference_log(s10, kind):
     ref = np.array(row["residual_norms"][: len(ours)])
     assert len(ours) == 12
     np.testing.assert_allclose(ours, ref, rtol=1e-10)
+
+
+@pytest.mark.parametrize("case", [dg.CONTINUOUS_COEFFICIENT_2D, dg.CONSTANT_COEFFICIENT_2D], ids=["continuous", "constant"])
+def test_sipg_converges_at_second_order(case):
+    """Direct solves on S3..S6: the L2 error against the exact solution of
+    ``problems.py:31-74`` falls by ~4x per refinement (P1, h -> h/2)."""
+    import scipy.sparse.linalg as spla
+
+    errs = []
+    for m in range(3, 7):
+        mesh = dg.uniform_mesh_2d(m)
+        s = dg.sipg_p1(mesh, case)
+        u = spla.spsolve(scipy_csr(s.matrix).tocsc(), s.load.numpy())
+        errs.append(dg.l2_error(mesh, u, case.solution))
+    assert errs[0] < 0.5  # the reference's bound at S3 (tests/test_experiments.py:37-41)
+    ratio = errs[-2] / errs[-1]
+    assert 3.7 < ratio < 4.3, errs

@@ -99,3 +99,30 @@ def test_dg_experiment_quadrilateral_cells():
     assert bool((kw["solvers_per_coarse"] == 16).all())
     out = dg_experiments.run("S9", "C8", "C6", "hybrid", "f64", reps=1)
     assert out["iterations"] < 200
+
+
+def test_reference_experiment_factory_case():
+    """``src/experiments/tests/test_experiments.py:10-41``: fine S3, the direct
+    coarse-solver interface on the whole system, and CG(AdditiveSchwarz(float32,
+    Inv(float16), CUDSS)) with C3 subdomains and one C0 coarse cell; both reach
+    a residual below 1e-6 and an L2 error below 0.5."""
+    import dd_solvers_b200 as dd
+    from dd_solvers_b200 import dg
+
+    A, b, kw, perm = dg_experiments.build("S3", "C3", "C0", return_perm=True)
+    inv = torch.empty_like(perm)
+    inv[perm] = torch.arange(perm.numel(), device=perm.device)
+    mesh = dg.uniform_mesh_2d(3)
+    case = dg.CONTINUOUS_COEFFICIENT_2D
+
+    direct = dd.CUDSS()
+    direct.setup(A)
+    x_direct, _ = direct.solve(b)
+    cg = dd.CG(dd.AdditiveSchwarz(torch.float32, dd.Inv(torch.float16), dd.CUDSS()))
+    cg.setup(A, **kw)
+    x_cg, meta = cg.solve(b)
+    for x in (x_direct, x_cg):
+        res = float(torch.linalg.norm(torch.sparse.mm(A, x[:, None])[:, 0] - b))
+        assert res < 1e-6, res
+        err = dg.l2_error(mesh, x[inv].cpu(), case.solution)
+        assert err < 0.5, err
