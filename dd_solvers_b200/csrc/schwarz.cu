@@ -46,7 +46,11 @@ __global__ void __launch_bounds__(kThreads, 4)
       ok[uu] = d[uu] < n;
       v[uu] = 0.0;
     }
-    if (ylocal != nullptr) {
+    if (ylocal != nullptr && dof_ptr == nullptr) {  // identity map: ylocal is DOF-ordered
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu)
+        if (ok[uu]) v[uu] += (double)__ldg(ylocal + d[uu]);
+    } else if (ylocal != nullptr) {
       int t0[U], t1[U], s0[U];
 #pragma unroll
       for (int uu = 0; uu < U; ++uu) {
@@ -67,7 +71,11 @@ __global__ void __launch_bounds__(kThreads, 4)
       for (int uu = 0; uu < U; ++uu)
         if (ok[uu]) v[uu] += u[d[uu]];
     }
-    if (p_ptr != nullptr) {
+    if (p_ptr == nullptr && p_col != nullptr) {  // one unit entry per DOF: P0 aggregates
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu)
+        if (ok[uu]) v[uu] = fma(sign, __ldg(yc + __ldg(p_col + d[uu])), v[uu]);
+    } else if (p_ptr != nullptr) {
       int k0[U], k1[U];
 #pragma unroll
       for (int uu = 0; uu < U; ++uu) {
@@ -142,7 +150,15 @@ __global__ void __launch_bounds__(kThreads, 4)
       ok[uu] = d[uu] < n;
       v[uu] = make_double2(0.0, 0.0);
     }
-    if (ylocal != nullptr) {
+    if (ylocal != nullptr && dof_ptr == nullptr) {  // identity map
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu)
+        if (ok[uu]) {
+          const double2 y = load_pair<ACC>(ylocal + d[uu] * R + jc);
+          v[uu].x += y.x;
+          v[uu].y += y.y;
+        }
+    } else if (ylocal != nullptr) {
       int t0[U], t1[U], s0[U];
 #pragma unroll
       for (int uu = 0; uu < U; ++uu) {
@@ -175,7 +191,15 @@ __global__ void __launch_bounds__(kThreads, 4)
           v[uu].y += uv.y;
         }
     }
-    if (p_ptr != nullptr) {
+    if (p_ptr == nullptr && p_col != nullptr) {  // one unit entry per DOF
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu)
+        if (ok[uu]) {
+          const double2 y = __ldg(reinterpret_cast<const double2*>(yc + (int64_t)__ldg(p_col + d[uu]) * R + jc));
+          v[uu].x = fma(sign, y.x, v[uu].x);
+          v[uu].y = fma(sign, y.y, v[uu].y);
+        }
+    } else if (p_ptr != nullptr) {
       int k0[U], k1[U];
 #pragma unroll
       for (int uu = 0; uu < U; ++uu) {
@@ -341,8 +365,9 @@ int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src
                         unsigned int* tickets, ddx_stream_t stream) {
   DDX_REQUIRE(valid_rhs_count(R), "ddx_schwarz_combine: unsupported R=%d", R);
   DDX_REQUIRE(n >= 0 && z, "ddx_schwarz_combine: bad arguments");
-  if (ylocal) DDX_REQUIRE(dof_ptr && dof_src, "ddx_schwarz_combine: ylocal needs the transpose map");
+  if (ylocal && dof_ptr) DDX_REQUIRE(dof_src, "ddx_schwarz_combine: transpose map without dof_src");
   if (p_ptr) DDX_REQUIRE(p_col && p_val && yc, "ddx_schwarz_combine: prolongation needs P and yc");
+  if (!p_ptr && p_col) DDX_REQUIRE(yc, "ddx_schwarz_combine: P0 prolongation needs yc");
   if (dots) DDX_REQUIRE(r && st && ist && partials && tickets, "ddx_schwarz_combine: dots need PCG state");
   PcgState S{st, ist, nullptr, R};
   cudaStream_t s = (cudaStream_t)stream;

@@ -346,7 +346,12 @@ class SchwarzOperator(SparseSolver):
             del A_t, R0_t, AR_t
             self.coarse_solver.setup(Ac_t)
             self._R0 = _csr_dev(R0, self.device)
-            self._P = _csr_dev(R0.T.tocsr(), self.device)
+            P = R0.T.tocsr()
+            if P.nnz == P.shape[0] and bool((np.diff(P.indptr) == 1).all()) and bool((P.data == 1.0).all()):
+                # P0 aggregates: one unit entry per DOF, passed as its column alone
+                self._P = (None, torch.as_tensor(P.indices.astype(np.int32), device=self.device), None)
+            else:
+                self._P = _csr_dev(P, self.device)
             self._fused_coarse = isinstance(self.coarse_solver, CUDSS)
         if self.collect_timings:
             events[2].record()
@@ -450,7 +455,11 @@ class SchwarzOperator(SparseSolver):
             nsm = torch.cuda.get_device_properties(self.device).multi_processor_count
             if self.n_solvers < 2 * nsm:
                 self.parts = int(min(8, -(-2 * nsm // self.n_solvers)))
-        self._ymap_one = (self.dof_ptr, self.dof_src)
+        # equal contiguous non-overlapping subdomains in DOF order (the reference's
+        # layout): ylocal is DOF-ordered and the combine needs no transpose map
+        identity = (int(self.sub_idx.numel()) == self.n and
+                    bool((self.sub_idx == torch.arange(self.n, device=self.device, dtype=self.sub_idx.dtype)).all()))
+        self._ymap_one = (None, None) if identity else (self.dof_ptr, self.dof_src)
         if self.parts > 1:
             S = self.parts
             total = int(self.sub_idx.numel())

@@ -265,7 +265,11 @@ int ddx_pack_panels16(int n_sub, int R, const int64_t* sub_ptr, const int* sub_i
  * where T(d) = dof_ptr[d]..dof_ptr[d+1] lists the positions of DOF d in the
  * subdomain-major ylocal (ascending subdomain order, so the sum order is
  * fixed). With dots != 0 it also forms rho = r.z (and z.q when flexible) and
- * beta on the device. u may alias z. */
+ * beta on the device. u may alias z. Shortcuts for the reference's own layout
+ * (equal contiguous non-overlapping subdomains, P0 coarse aggregates):
+ * dof_ptr == NULL with ylocal means the identity map (ylocal is DOF-ordered);
+ * p_ptr == NULL with p_col means P has one unit entry per DOF, in column
+ * p_col[d] (p_val unused). */
 int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src, const void* ylocal,
                         int acc_dtype, const double* u, const int* p_ptr, const int* p_col,
                         const double* p_val, const double* yc, double sign, double* z, int dots,
