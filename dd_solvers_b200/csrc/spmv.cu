@@ -10,6 +10,7 @@
 // served by L1/L2). The PCG epilogues (p.q, b - A x and its norms) are fused
 // with deterministic CTA partials and a last-CTA finalize.
 #include <algorithm>
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -276,10 +277,10 @@ __global__ void __launch_bounds__(kThreads)
 // Rows of moderate length (R = 1): L lanes per row (L = 4..32), lane l sums
 // the entries k0 + l, k0 + l + L, ...; the L partial sums are combined by a
 // fixed xor tree, so the result does not depend on timing.
-template <int L>
+template <int L, typename TX>
 __global__ void __launch_bounds__(kThreads)
     k_spmv_rowwarp(int64_t n_rows, const int* __restrict__ row_ptr, const int* __restrict__ cols,
-                   const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y) {
+                   const double* __restrict__ vals, const TX* __restrict__ x, double* __restrict__ y) {
   constexpr int RPW = 32 / L;  // rows per warp and step
   const int lane = threadIdx.x & 31;
   const int sub = lane % L;
@@ -291,7 +292,8 @@ __global__ void __launch_bounds__(kThreads)
     double sum = 0.0;
     if (row < n_rows) {
       const int k0 = row_ptr[row], k1 = row_ptr[row + 1];
-      for (int k = k0 + sub; k < k1; k += L) sum = fma(__ldg(vals + k), __ldg(x + __ldg(cols + k)), sum);
+      for (int k = k0 + sub; k < k1; k += L)
+        sum = fma(__ldg(vals + k), (double)__ldg(x + __ldg(cols + k)), sum);
     }
 #pragma unroll
     for (int o = L / 2; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o, L);
@@ -480,23 +482,34 @@ int ddx_spmv_csr_rowblock_f64(int64_t n_rows, int R, const int* row_ptr, const i
   return DDX_OK;
 }
 
-int ddx_spmv_csr_lanes_f64(int64_t n_rows, int lanes, const int* row_ptr, const int* cols, const double* vals,
-                           const double* x, double* y, ddx_stream_t stream) {
-  DDX_REQUIRE(n_rows >= 0 && row_ptr && x && y, "ddx_spmv_csr_lanes_f64: bad arguments");
+int ddx_spmv_csr_lanes(int64_t n_rows, int lanes, const int* row_ptr, const int* cols, const double* vals,
+                       const void* x, int x_dtype, double* y, ddx_stream_t stream) {
+  DDX_REQUIRE(n_rows >= 0 && row_ptr && x && y, "ddx_spmv_csr_lanes: bad arguments");
   DDX_REQUIRE(lanes == 4 || lanes == 8 || lanes == 16 || lanes == 32,
-              "ddx_spmv_csr_lanes_f64: lanes must be 4, 8, 16 or 32 (got %d)", lanes);
+              "ddx_spmv_csr_lanes: lanes must be 4, 8, 16 or 32 (got %d)", lanes);
+  DDX_REQUIRE(x_dtype == DDX_F64 || x_dtype == DDX_F32, "ddx_spmv_csr_lanes: x must be F64 or F32");
   if (n_rows == 0) return DDX_OK;
   cudaStream_t s = (cudaStream_t)stream;
-  auto go = [&](auto kernel) {
+  auto go = [&](auto kernel, auto* xt) {
     const int grid = resident_grid(kernel, ceil_div(n_rows * lanes, kThreads), 1 << 20);
-    kernel<<<grid, kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y);
+    kernel<<<grid, kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, xt, y);
   };
-  if (lanes == 4) go(k_spmv_rowwarp<4>);
-  else if (lanes == 8) go(k_spmv_rowwarp<8>);
-  else if (lanes == 16) go(k_spmv_rowwarp<16>);
-  else go(k_spmv_rowwarp<32>);
-  DDX_LAUNCH_CHECK("ddx_spmv_csr_lanes_f64");
+  auto by_lanes = [&](auto* xt) {
+    using TX = typename std::remove_const<typename std::remove_pointer<decltype(xt)>::type>::type;
+    if (lanes == 4) go(k_spmv_rowwarp<4, TX>, xt);
+    else if (lanes == 8) go(k_spmv_rowwarp<8, TX>, xt);
+    else if (lanes == 16) go(k_spmv_rowwarp<16, TX>, xt);
+    else go(k_spmv_rowwarp<32, TX>, xt);
+  };
+  if (x_dtype == DDX_F64) by_lanes((const double*)x);
+  else by_lanes((const float*)x);
+  DDX_LAUNCH_CHECK("ddx_spmv_csr_lanes");
   return DDX_OK;
+}
+
+int ddx_spmv_csr_lanes_f64(int64_t n_rows, int lanes, const int* row_ptr, const int* cols, const double* vals,
+                           const double* x, double* y, ddx_stream_t stream) {
+  return ddx_spmv_csr_lanes(n_rows, lanes, row_ptr, cols, vals, x, DDX_F64, y, stream);
 }
 
 int ddx_spmv_bsr(int64_t n_block_rows, int bs, const int* row_ptr, const int* cols, const void* vals,

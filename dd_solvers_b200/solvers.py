@@ -694,9 +694,10 @@ class SchwarzOperator(SparseSolver):
         n_rows = rowptr.numel() - 1
         lanes = self._lanes_for(n_rows, col.numel()) if R == 1 else 0
         if lanes:
-            L.call("ddx_spmv_csr_lanes_f64", n_rows, lanes, L.ptr(rowptr), L.ptr(col), L.ptr(val), L.ptr(x),
-                   L.ptr(out), L.stream_ptr())
+            L.call("ddx_spmv_csr_lanes", n_rows, lanes, L.ptr(rowptr), L.ptr(col), L.ptr(val), L.ptr(x),
+                   L.DTYPE_CODE[x.dtype], L.ptr(out), L.stream_ptr())
         else:
+            assert x.dtype == torch.float64
             L.call("ddx_spmv_csr_rowblock_f64", n_rows, R, L.ptr(rowptr), L.ptr(col), L.ptr(val),
                    L.ptr(x), L.ptr(out), L.stream_ptr())
 
@@ -806,6 +807,13 @@ class HybridSchwarz(SchwarzOperator):
         ylocal = self._local(r, R, ist, st)
         if not self.n_coarse:
             self._combine(z, R, ylocal=ylocal, pcg=pcg, r=r, q=q)
+            return
+        if self._ymap[0] is None and R == 1 and self._lanes_for(self.n_coarse, self._AR[1].numel()):
+            # the reference's layout: y is ylocal widened to FP64, read in place by
+            # the restriction and the combine (same values, one pass fewer)
+            self._restrict(*self._AR, ylocal[: self.n], s["w"], R)
+            self._coarse(s["w"], s["yc"], R, ist)
+            self._combine(z, R, ylocal=ylocal, prolong=True, sign=-1.0, pcg=pcg, r=r, q=q)
             return
         y = s["y"]
         self._combine(y, R, ylocal=ylocal)

@@ -133,6 +133,11 @@ int ddx_spmv_csr_rowblock_f64(int64_t n_rows, int R, const int* row_ptr, const i
  * length). */
 int ddx_spmv_csr_lanes_f64(int64_t n_rows, int lanes, const int* row_ptr, const int* cols, const double* vals,
                            const double* x, double* y, ddx_stream_t stream);
+/* Same with x in x_dtype (DDX_F64 or DDX_F32, widened to FP64 on load): the
+ * hybrid restriction A_R y reads the FP32 local products directly when the
+ * subdomains are the reference's contiguous non-overlapping blocks. */
+int ddx_spmv_csr_lanes(int64_t n_rows, int lanes, const int* row_ptr, const int* cols, const double* vals,
+                       const void* x, int x_dtype, double* y, ddx_stream_t stream);
 /* BSR, block size bs (1..24: DG P1..P5 triangles have 3..21 DOFs per
  * element), blocks column-major (bs, bs) as produced by the reference's
  * csr_to_bsr (src/dd_solvers/cpp/cusparse.cpp:22-107); dtype F64 or F32 for
