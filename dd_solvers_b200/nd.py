@@ -399,8 +399,8 @@ class NDSolver:
         p.G = self.G.data_ptr()
         p.GT = self.GT.data_ptr()
         self.plan = p
-        if self.n > 1_000_000:
-            # measured on B200: fatter items pay off once the leaf levels hold >100k of them
+        if self.n > 300_000:
+            # measured on B200: fatter items pay off from ~500k coarse DOFs (tens of thousands of leaf items)
             sym.build_items(65536, 128)
         self._set_items()
         self._work = {}
