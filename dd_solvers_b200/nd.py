@@ -443,46 +443,3 @@ class NDSolver:
         x = torch.empty_like(w)
         self.solve_into(w, x, R)
         return x.to(rhs.dtype)
-
-
-def emulate_solve(sym: NDSymbolic, G: np.ndarray, GT: np.ndarray, w: np.ndarray) -> np.ndarray:
-    """The kernels' arithmetic on the host, work item by work item (test use:
-    it follows the same index maps and level order as ``ddx_coarse_solve_nd``)."""
-    n = sym.n
-    w = np.asarray(w, dtype=np.float64).reshape(n, -1)
-    R = w.shape[1]
-    y = np.zeros((n, R))   # forward result, elimination order
-    xe = np.zeros((n, R))  # solution, elimination order
-    x = np.zeros((n, R))
-    s_first = np.cumsum(sym.s) - sym.s
-    fpos = sym.pos[sym.fidx]
-    upd = np.zeros((max(sym.upd_total, 1), R))
-    for lv in range(sym.n_levels):
-        for it in range(sym.fwd_level_ptr[lv], sym.fwd_level_ptr[lv + 1]):
-            t, r0, nr = sym.fwd_items[it]
-            s, u = int(sym.s[t]), int(sym.u[t])
-            io, go = int(sym.idx_off[t]), int(sym.g_off[t])
-            f = np.zeros((s + u, R))
-            for p in range(s + u):
-                acc = w[sym.fidx[io + p]].copy() if p < s else np.zeros(R)
-                for q in range(sym.gptr[io + p], sym.gptr[io + p + 1]):
-                    acc = acc + upd[sym.gsrc[q]]
-                f[p] = acc
-            Gt = G[go:go + (s + u) * s].reshape(s + u, s)
-            for p in range(r0, r0 + nr):
-                out = Gt[p] @ f[:s] if s else np.zeros(R)
-                if p < s:
-                    y[s_first[t] + p] = out
-                else:
-                    upd[sym.upd_off[t] + p - s] = f[p] - out
-    for j in range(sym.n_levels):
-        for it in range(sym.bwd_level_ptr[j], sym.bwd_level_ptr[j + 1]):
-            t, c0, nc = sym.bwd_items[it]
-            s, u = int(sym.s[t]), int(sym.u[t])
-            io, go = int(sym.idx_off[t]), int(sym.g_off[t])
-            v = np.concatenate([y[s_first[t]:s_first[t] + s], -xe[fpos[io + s:io + s + u]]])
-            GTt = GT[go:go + s * (s + u)].reshape(s, s + u)
-            for c in range(c0, c0 + nc):
-                xe[s_first[t] + c] = GTt[c] @ v
-                x[sym.fidx[io + c]] = xe[s_first[t] + c]
-    return x

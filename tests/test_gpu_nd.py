@@ -14,6 +14,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 from dd_solvers_b200 import cudss, dg_experiments, nd  # noqa: E402
+from nd_emulation import emulate_solve  # noqa: E402
 from test_nd import CASES, lap2d  # noqa: E402
 
 pytestmark = pytest.mark.gpu
@@ -46,7 +47,7 @@ def test_nd_solve_matches_host_emulation_and_is_deterministic():
     x1 = solver.solve(w)
     x2 = solver.solve(w)
     assert torch.equal(x1, x2)
-    xe = nd.emulate_solve(solver.sym, solver.G.cpu().numpy(), solver.GT.cpu().numpy(), w.cpu().numpy())
+    xe = emulate_solve(solver.sym, solver.G.cpu().numpy(), solver.GT.cpu().numpy(), w.cpu().numpy())
     np.testing.assert_allclose(x1.cpu().numpy(), xe, rtol=1e-12, atol=1e-12 * np.abs(xe).max())
 
 

@@ -1,6 +1,6 @@
 """Nested-dissection multifrontal coarse solver: ordering, symbolic analysis
 and numeric factorisation on the host, and the solve kernels' arithmetic
-emulated item by item (``nd.emulate_solve``) against SciPy's sparse LU."""
+emulated item by item (``tests/nd_emulation.py``) against SciPy's sparse LU."""
 import os
 import sys
 
@@ -13,6 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 
 from dd_solvers_b200 import dg, nd  # noqa: E402
+from nd_emulation import emulate_solve  # noqa: E402
 
 
 def lap2d(k, shift=0.01):
@@ -49,9 +50,9 @@ def test_emulated_solve_matches_sparse_lu(case, leaf):
     A = CASES[case]()
     A.sort_indices()
     sym = nd.NDSymbolic(A.indptr, A.indices, A.shape[0], leaf)
-    G = nd.factorize(sym, A.indptr, A.indices, A.data, "cpu").numpy()
+    G, GT = (t.numpy() for t in nd.factorize(sym, A.indptr, A.indices, A.data, "cpu"))
     w = np.random.default_rng(0).standard_normal((A.shape[0], 3))
-    x = nd.emulate_solve(sym, G, w)
+    x = emulate_solve(sym, G, GT, w)
     ref = spla.splu(A.tocsc()).solve(w)
     assert np.abs(x - ref).max() <= 1e-12 * np.abs(ref).max()
 
@@ -96,10 +97,13 @@ def test_symbolic_front_sets():
             assert sym.pos[sym.U[t]].min() > sym.pos[sym.S[t]].max()
         if sym.parent[t] < 0:
             assert len(sym.U[t]) == 0
-    # every forward item covers its front's rows exactly once
-    rows = {}
-    for t, r0, nr in sym.fwd_items:
-        rows.setdefault(int(t), []).append((int(r0), int(nr)))
-    for t in range(sym.nf):
-        cover = sorted(rows[t])
-        assert cover[0][0] == 0 and sum(nr for _, nr in cover) == sym.s[t] + sym.u[t]
+    # the forward items cover each front's rows, the backward items its columns, once
+    for items, total in ((sym.fwd_items, sym.s + sym.u), (sym.bwd_items, sym.s)):
+        rows = {}
+        for t, r0, nr in items:
+            rows.setdefault(int(t), []).append((int(r0), int(nr)))
+        for t in range(sym.nf):
+            cover = sorted(rows[t])
+            ends = [r0 + nr for r0, nr in cover]
+            assert cover[0][0] == 0 and ends[-1] == total[t]
+            assert all(cover[i + 1][0] == ends[i] for i in range(len(cover) - 1))
