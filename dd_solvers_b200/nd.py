@@ -46,6 +46,7 @@ import torch
 from . import _lib as L
 
 LEAF = 128          # largest subgraph left undissected (a leaf front)
+TOP_MERGE = 2048    # merge the top levels into one dense front while it holds at most this many vertices
 ITEM_BYTES = 32768  # operator bytes per work item (rows of G or of G^T) ...
 ITEM_MAX_ROWS = 64  # ... between 8 and this many rows
 
@@ -76,6 +77,46 @@ def nested_dissection(indptr: np.ndarray, indices: np.ndarray, n: int, leaf: int
     return S, parent[:nf].copy()
 
 
+def _merge_top(S: list, parent: np.ndarray, limit: int):
+    """Merge the top levels of the separator tree into one front while the
+    merged separators hold at most ``limit`` vertices: whole levels, from the
+    root(s) down. The other nodes keep their post-order (each remaining subtree
+    stays contiguous), the merged front comes last, and the children of merged
+    nodes become its children. Fewer levels means fewer latency-bound sweep
+    launches; the merged front is one dense factor."""
+    nf = len(S)
+    if limit <= 0 or nf < 2:
+        return S, parent
+    children = [[] for _ in range(nf)]
+    for t in range(nf):
+        if parent[t] >= 0:
+            children[parent[t]].append(t)
+    depth = np.zeros(nf, dtype=np.int64)  # distance from the root
+    for t in range(nf - 1, -1, -1):  # post-order: parents after children
+        if parent[t] >= 0:
+            depth[t] = depth[parent[t]] + 1
+    sizes = np.array([len(x) for x in S], dtype=np.int64)
+    top, total = None, 0
+    for d in range(int(depth.max()) + 1):
+        layer = np.nonzero(depth == d)[0]
+        if total + int(sizes[layer].sum()) > limit:
+            break
+        total += int(sizes[layer].sum())
+        top = d
+    if top is None or top == 0 and len(np.nonzero(depth == 0)[0]) == nf:
+        return S, parent
+    merged = depth <= top
+    keep = [t for t in range(nf) if not merged[t]]
+    new_id = {t: i for i, t in enumerate(keep)}
+    root = len(keep)
+    S2 = [S[t] for t in keep] + [np.concatenate([S[t] for t in range(nf) if merged[t]])]
+    parent2 = np.full(root + 1, -1, dtype=np.int64)
+    for t in keep:
+        p = parent[t]
+        parent2[new_id[t]] = root if merged[p] else new_id[p]
+    return S2, parent2
+
+
 # ---------------------------------------------------------------------------
 # symbolic analysis
 # ---------------------------------------------------------------------------
@@ -83,8 +124,9 @@ def nested_dissection(indptr: np.ndarray, indices: np.ndarray, n: int, leaf: int
 class NDSymbolic:
     """Fronts in post-order with their index sets, levels and gather maps."""
 
-    def __init__(self, indptr, indices, n: int, leaf: int = 128):
+    def __init__(self, indptr, indices, n: int, leaf: int = 128, top_merge: int | None = None):
         S, parent = nested_dissection(indptr, indices, n, leaf)
+        S, parent = _merge_top(S, parent, TOP_MERGE if top_merge is None else top_merge)
         indptr = np.asarray(indptr, dtype=np.int64)
         indices = np.asarray(indices, dtype=np.int64)
         nf = len(S)
@@ -370,14 +412,14 @@ class NDSolver:
     """Factor once (``A`` a torch CSR tensor on the device, FP64), then
     ``solve_into(w, x, R)`` with ``w, x`` (n, R) row-major FP64 on the device."""
 
-    def __init__(self, A: torch.Tensor, leaf: int | None = None):
+    def __init__(self, A: torch.Tensor, leaf: int | None = None, top_merge: int | None = None):
         leaf = LEAF if leaf is None else leaf
         dev = A.device
         self.leaf = leaf
         indptr = A.crow_indices().cpu().numpy()
         indices = A.col_indices().cpu().numpy()
         self.n = A.shape[0]
-        self.sym = sym = NDSymbolic(indptr, indices, self.n, leaf)
+        self.sym = sym = NDSymbolic(indptr, indices, self.n, leaf, top_merge)
         self.G, self.GT = factorize(sym, indptr, indices, A.values(), dev)
         i32 = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.int32, device=dev)  # noqa: E731
         i64 = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.int64, device=dev)  # noqa: E731
