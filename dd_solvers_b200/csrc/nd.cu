@@ -17,6 +17,16 @@
 // row-wise GEMVs (a warp per row, lanes along the row: coalesced, short
 // per-lane chains). One launch per tree level and sweep; every front is split
 // into work items of a few rows sized by bytes. All sums run in a fixed order.
+//
+// On levels whose fronts are cut into many forward items, a gather launch
+// first assembles each front's vector f = [w_S; 0] + children's updates once
+// (into fb, front-position order), so the forward items read it contiguously
+// instead of each repeating the index-chained gather of the whole f_S.
+//
+// The sweeps are latency-bound (a few hundred items per level, one level after
+// another), so each item copies its operator rows into shared memory and
+// reads its static index maps before waiting on the previous level: after the
+// wait only the right-hand-side reads remain on its critical path.
 #include <algorithm>
 #include <vector>
 
@@ -27,14 +37,30 @@ namespace {
 
 constexpr int kNdThreads = 256;
 constexpr int kNdWarps = kNdThreads / 32;
-constexpr int kNdSmemMax = 96 * 1024;  // the staged vector (front rows x RHS group)
-constexpr int kNdItemRows = 256;       // forward rows whose f_U is gathered up front (items hold <= 128)
+constexpr int kNdSmemMax = 96 * 1024;     // the staged vector (front rows x RHS group)
+constexpr int kNdSmemOptin = 227 * 1024;  // a CTA's shared memory on sm_100
+constexpr int kNdItemRows = 256;          // forward rows whose f_U is gathered up front (items hold <= 128)
 
 // Programmatic dependent launch: each level's kernel is launched so that it
-// may start while the previous one drains; it reads only the static plan
-// before griddepcontrol.wait, which returns once the previous grid's writes
-// are visible.
+// may start while the previous one runs. Before griddepcontrol.wait it reads
+// only the static plan and operators (staging its operator rows into shared
+// memory); the wait returns once the previous grid has finished and its writes
+// are visible. With `release`, each grid lets its successor launch right after
+// its own wait, so a successor's prologue overlaps at most this grid's
+// dependent phase; without it the successor launches when this grid ends.
 __device__ __forceinline__ void wait_previous_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void release_next_grid() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Operator rows global -> shared with cp.async (8 bytes each: the rows of a
+// front start at any double), all of a thread's copies in flight together.
+__device__ __forceinline__ void stage_operator(double* dst, const double* __restrict__ src, int n) {
+  for (int e = threadIdx.x; e < n; e += kNdThreads) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst + e);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src + e) : "memory");
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void staged_operator_ready() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 template <typename Kernel, typename... Args>
 cudaError_t launch_after_previous(Kernel kernel, unsigned grid, size_t smem, cudaStream_t stream, Args... args) {
@@ -73,63 +99,121 @@ struct NdArgs {
   const int* fpos;         // elimination position of every front position
 };
 
+// The static part of one front position's gather, read before the wait: its
+// right-hand-side row (separator positions), its range in the gather map and
+// the first two update rows it adds (a binary separator tree gives at most two).
+struct GatherSlot {
+  int64_t v = 0, q0 = 0, q1 = 0, g0 = 0, g1 = 0;
+  __device__ __forceinline__ void load(const NdArgs& A, int64_t io, int p, int s) {
+    if (p < s) v = A.fidx[io + p];
+    q0 = A.gptr[io + p];
+    q1 = A.gptr[io + p + 1];
+    if (q1 > q0) g0 = A.gsrc[q0];
+    if (q1 > q0 + 1) g1 = A.gsrc[q0 + 1];
+  }
+  // f[p] for right-hand sides r0 .. r0+ng: w (separator rows), then the
+  // update entries in gather-map order
+  template <int RG>
+  __device__ __forceinline__ void sum(const NdArgs& A, int p, int s, int R, int r0, int ng,
+                                      const double* __restrict__ w, const double* __restrict__ upd,
+                                      double (&acc)[RG]) const {
+#pragma unroll
+    for (int r = 0; r < RG; ++r) acc[r] = (p < s && r < ng) ? w[v * R + r0 + r] : 0.0;
+    if (q1 > q0) {
+#pragma unroll
+      for (int r = 0; r < RG; ++r)
+        if (r < ng) acc[r] += upd[g0 * R + r0 + r];
+    }
+    if (q1 > q0 + 1) {
+#pragma unroll
+      for (int r = 0; r < RG; ++r)
+        if (r < ng) acc[r] += upd[g1 * R + r0 + r];
+    }
+    for (int64_t q = q0 + 2; q < q1; ++q) {
+      const int64_t src = A.gsrc[q] * R + r0;
+#pragma unroll
+      for (int r = 0; r < RG; ++r)
+        if (r < ng) acc[r] += upd[src + r];
+    }
+  }
+};
+
+// Forward item: rows row0 .. row0+nrows of G_t; a warp per row, lanes along
+// the row. f_S (and f_U of the item's update rows) come from fb when the
+// level's gather launch assembled them, else they are gathered here. With
+// STAGE the item's operator rows (one contiguous range of G) are copied to
+// shared memory before the wait.
 // 4 CTAs per SM for the narrow RHS groups (latency-bound sweeps want warps in flight)
-template <int RG>
+template <int RG, bool STAGE>
 __global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
-    k_nd_fwd(NdArgs A, int64_t item0, int R, const double* __restrict__ w, double* __restrict__ y,
-             double* __restrict__ upd, const int* ist) {
-  extern __shared__ double fs[];
+    k_nd_fwd(NdArgs A, int64_t item0, int R, const double* __restrict__ w, const double* __restrict__ fb,
+             double* __restrict__ y, double* __restrict__ upd, const int* ist, int release) {
+  extern __shared__ __align__(16) double sm[];
   __shared__ double fu[kNdItemRows * RG];
   const int64_t it = item0 + blockIdx.x;
   const int t = A.items[3 * it], row0 = A.items[3 * it + 1], nrows = A.items[3 * it + 2];
   const int s = A.front_s[t];
   const int64_t io = A.idx_off[t], go = A.g_off[t], uo = A.upd_off[t];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  wait_previous_grid();
-  if (ist != nullptr && n_active(ist, R) == 0) return;
-  // update rows of this item whose f_U is gathered in the prologue
+  double* fs = sm;                   // f_S, s x RG
+  double* gs = sm + (int64_t)s * RG;  // the item's operator rows, nrows x s
+  if constexpr (STAGE) stage_operator(gs, A.G + go + (int64_t)row0 * s, nrows * s);
+  // gather slots: the s separator positions, then the item's update rows
+  // whose f_U goes to fu (u0 .. u1)
   const int u0 = max(row0, s), u1 = min(row0 + nrows, row0 + kNdItemRows);
+  const int nslots = s + max(u1 - u0, 0);
+  GatherSlot pre;
+  if (fb == nullptr && (int)threadIdx.x < nslots) {
+    const int k = threadIdx.x;
+    pre.load(A, io, k < s ? k : u0 + (k - s), s);
+  }
+  wait_previous_grid();
+  if (release) release_next_grid();
+  if (ist != nullptr && n_active(ist, R) == 0) {
+    if constexpr (STAGE) staged_operator_ready();
+    return;
+  }
   for (int r0 = 0; r0 < R; r0 += RG) {
     const int ng = min(RG, R - r0);
-    // f_S = w_S + the children's contributions, in gather-map order
-    for (int p = threadIdx.x; p < s; p += kNdThreads) {
-      const int64_t v = A.fidx[io + p];
+    for (int k = threadIdx.x; k < nslots; k += kNdThreads) {
+      const int p = k < s ? k : u0 + (k - s);
       double acc[RG];
+      if (fb != nullptr) {
 #pragma unroll
-      for (int r = 0; r < RG; ++r) acc[r] = r < ng ? w[v * R + r0 + r] : 0.0;
-      for (int64_t q = A.gptr[io + p]; q < A.gptr[io + p + 1]; ++q) {
-        const int64_t src = A.gsrc[q] * R + r0;
-#pragma unroll
-        for (int r = 0; r < RG; ++r)
-          if (r < ng) acc[r] += upd[src + r];
+        for (int r = 0; r < RG; ++r) acc[r] = r < ng ? fb[(io + p) * R + r0 + r] : 0.0;
+      } else if (k == (int)threadIdx.x) {
+        pre.sum<RG>(A, p, s, R, r0, ng, w, upd, acc);
+      } else {
+        GatherSlot g;
+        g.load(A, io, p, s);
+        g.sum<RG>(A, p, s, R, r0, ng, w, upd, acc);
       }
+      double* dst = k < s ? fs + k * RG : fu + (p - row0) * RG;
 #pragma unroll
-      for (int r = 0; r < RG; ++r) fs[p * RG + r] = acc[r];
+      for (int r = 0; r < RG; ++r) dst[r] = acc[r];
     }
-    // f_U of this item's update rows (children only), same order
-    for (int p = u0 + threadIdx.x; p < u1; p += kNdThreads) {
-      double acc[RG];
-#pragma unroll
-      for (int r = 0; r < RG; ++r) acc[r] = 0.0;
-      for (int64_t q = A.gptr[io + p]; q < A.gptr[io + p + 1]; ++q) {
-        const int64_t src = A.gsrc[q] * R + r0;
-#pragma unroll
-        for (int r = 0; r < RG; ++r)
-          if (r < ng) acc[r] += upd[src + r];
-      }
-#pragma unroll
-      for (int r = 0; r < RG; ++r) fu[(p - row0) * RG + r] = acc[r];
+    if constexpr (STAGE) {
+      if (r0 == 0) staged_operator_ready();
     }
     __syncthreads();
     for (int p = row0 + warp; p < row0 + nrows; p += kNdWarps) {
-      const double* g = A.G + go + (int64_t)p * s;
       double acc[RG];
 #pragma unroll
       for (int r = 0; r < RG; ++r) acc[r] = 0.0;
-      for (int j = lane; j < s; j += 32) {
-        const double gv = __ldg(g + j);
+      if constexpr (STAGE) {
+        const double* g = gs + (int64_t)(p - row0) * s;
+        for (int j = lane; j < s; j += 32) {
+          const double gv = g[j];
 #pragma unroll
-        for (int r = 0; r < RG; ++r) acc[r] = fma(gv, fs[j * RG + r], acc[r]);
+          for (int r = 0; r < RG; ++r) acc[r] = fma(gv, fs[j * RG + r], acc[r]);
+        }
+      } else {
+        const double* g = A.G + go + (int64_t)p * s;
+        for (int j = lane; j < s; j += 32) {
+          const double gv = __ldg(g + j);
+#pragma unroll
+          for (int r = 0; r < RG; ++r) acc[r] = fma(gv, fs[j * RG + r], acc[r]);
+        }
       }
 #pragma unroll
       for (int r = 0; r < RG; ++r) acc[r] = warp_sum_d(acc[r]);
@@ -139,21 +223,19 @@ __global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
         for (int r = 0; r < RG; ++r)
           if (lane == r && r < ng) y[e * R + r0 + r] = acc[r];
       } else {
-        // f_U of this row (children only, gathered above unless the item is
-        // longer than kNdItemRows), then u_t = f_U - M f_S
+        // f_U of this row (gathered above unless the item is longer than
+        // kNdItemRows), then u_t = f_U - M f_S
         double f[RG];
         if (p < u1) {
 #pragma unroll
           for (int r = 0; r < RG; ++r) f[r] = fu[(p - row0) * RG + r];
+        } else if (fb != nullptr) {
+#pragma unroll
+          for (int r = 0; r < RG; ++r) f[r] = r < ng ? fb[(io + p) * R + r0 + r] : 0.0;
         } else {
-#pragma unroll
-          for (int r = 0; r < RG; ++r) f[r] = 0.0;
-          for (int64_t q = A.gptr[io + p]; q < A.gptr[io + p + 1]; ++q) {
-            const int64_t src = A.gsrc[q] * R + r0;
-#pragma unroll
-            for (int r = 0; r < RG; ++r)
-              if (r < ng) f[r] += upd[src + r];
-          }
+          GatherSlot g;
+          g.load(A, io, p, s);
+          g.sum<RG>(A, p, s, R, r0, ng, w, upd, f);
         }
         const int64_t dst = (uo + p - s) * R + r0;
 #pragma unroll
@@ -165,41 +247,94 @@ __global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
   }
 }
 
+// Gather item (t, p0, np): f at positions p0 .. p0+np of front t, all R
+// right-hand sides, f[p] = (p < s ? w[fidx[p]] : 0) + the children's update
+// entries in gather-map order (the order the forward items use on their own).
+__global__ void __launch_bounds__(kNdThreads)
+    k_nd_gather(NdArgs A, const int* __restrict__ gitems, int64_t item0, int R, const double* __restrict__ w,
+                const double* __restrict__ upd, double* __restrict__ fb, const int* ist, int release) {
+  const int64_t it = item0 + blockIdx.x;
+  const int t = gitems[3 * it], p0 = gitems[3 * it + 1], np = gitems[3 * it + 2];
+  const int s = A.front_s[t];
+  const int64_t io = A.idx_off[t];
+  GatherSlot pre;
+  if ((int)threadIdx.x < np) pre.load(A, io, p0 + threadIdx.x, s);
+  wait_previous_grid();
+  if (release) release_next_grid();
+  if (ist != nullptr && n_active(ist, R) == 0) return;
+  for (int k = threadIdx.x; k < np; k += kNdThreads) {
+    const int p = p0 + k;
+    GatherSlot g = pre;
+    if (k != (int)threadIdx.x) g.load(A, io, p, s);
+    for (int r = 0; r < R; ++r) {
+      double acc[1];
+      g.sum<1>(A, p, s, R, r, 1, w, upd, acc);
+      fb[(io + p) * R + r] = acc[0];
+    }
+  }
+}
+
 // Backward item: rows c0 .. c0+nc of G_t^T (columns of G_t); a warp per row,
-// lanes over the s+u entries, v = [y_S; -x_U] staged in shared memory.
-template <int RG>
+// lanes over the s+u entries, v = [y_S; -x_U] staged in shared memory. With
+// STAGE the item's rows of G_t^T (one contiguous range) are copied to shared
+// memory before the wait.
+template <int RG, bool STAGE>
 __global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
     k_nd_bwd(NdArgs A, int64_t item0, int R, const double* __restrict__ y, double* __restrict__ xe,
-             double* __restrict__ x, const int* ist) {
-  extern __shared__ double vs[];
+             double* __restrict__ x, const int* ist, int release) {
+  extern __shared__ __align__(16) double sm[];
   const int64_t it = item0 + blockIdx.x;
   const int t = A.items[3 * it], c0 = A.items[3 * it + 1], nc = A.items[3 * it + 2];
   const int s = A.front_s[t], m = s + A.front_u[t];
   const int64_t io = A.idx_off[t], go = A.g_off[t];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* vs = sm;                   // v, m x RG
+  double* gs = sm + (int64_t)m * RG;  // the item's rows of G_t^T, nc x m
+  if constexpr (STAGE) stage_operator(gs, A.GT + go + (int64_t)c0 * m, nc * m);
+  // y and the solution are read in elimination order: the separator is one
+  // range, the update set a few ranges of ancestor separators
+  const int64_t sf = A.s_first[t];
+  int64_t pre_e = 0;
+  if ((int)threadIdx.x < m) {
+    const int p = threadIdx.x;
+    pre_e = p < s ? sf + p : (int64_t)A.fpos[io + p];
+  }
   wait_previous_grid();
-  if (ist != nullptr && n_active(ist, R) == 0) return;
+  if (release) release_next_grid();
+  if (ist != nullptr && n_active(ist, R) == 0) {
+    if constexpr (STAGE) staged_operator_ready();
+    return;
+  }
   for (int r0 = 0; r0 < R; r0 += RG) {
     const int ng = min(RG, R - r0);
-    // y and the solution are read in elimination order: the separator is one
-    // range, the update set a few ranges of ancestor separators
-    const int64_t sf = A.s_first[t];
     for (int p = threadIdx.x; p < m; p += kNdThreads) {
-      const int64_t e = p < s ? sf + p : (int64_t)A.fpos[io + p];
+      const int64_t e = p == (int)threadIdx.x ? pre_e : (p < s ? sf + p : (int64_t)A.fpos[io + p]);
 #pragma unroll
       for (int r = 0; r < RG; ++r)
         vs[p * RG + r] = r < ng ? (p < s ? y[e * R + r0 + r] : -xe[e * R + r0 + r]) : 0.0;
     }
+    if constexpr (STAGE) {
+      if (r0 == 0) staged_operator_ready();
+    }
     __syncthreads();
     for (int c = c0 + warp; c < c0 + nc; c += kNdWarps) {
-      const double* g = A.GT + go + (int64_t)c * m;
       double acc[RG];
 #pragma unroll
       for (int r = 0; r < RG; ++r) acc[r] = 0.0;
-      for (int p = lane; p < m; p += 32) {
-        const double gv = __ldg(g + p);
+      if constexpr (STAGE) {
+        const double* g = gs + (int64_t)(c - c0) * m;
+        for (int p = lane; p < m; p += 32) {
+          const double gv = g[p];
 #pragma unroll
-        for (int r = 0; r < RG; ++r) acc[r] = fma(gv, vs[p * RG + r], acc[r]);
+          for (int r = 0; r < RG; ++r) acc[r] = fma(gv, vs[p * RG + r], acc[r]);
+        }
+      } else {
+        const double* g = A.GT + go + (int64_t)c * m;
+        for (int p = lane; p < m; p += 32) {
+          const double gv = __ldg(g + p);
+#pragma unroll
+          for (int r = 0; r < RG; ++r) acc[r] = fma(gv, vs[p * RG + r], acc[r]);
+        }
       }
 #pragma unroll
       for (int r = 0; r < RG; ++r) acc[r] = warp_sum_d(acc[r]);
@@ -217,21 +352,49 @@ __global__ void __launch_bounds__(kNdThreads, RG <= 2 ? 4 : 1)
 
 template <int RG>
 int nd_sweeps(const ddx_nd_plan* P, const NdArgs& fa, const NdArgs& ba, int R, const double* w, double* x,
-              double* y, double* xe, double* upd, const int* ist, cudaStream_t s) {
-  const size_t smem_cap = (size_t)kNdSmemMax;
-  cudaFuncSetAttribute(k_nd_fwd<RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap);
-  cudaFuncSetAttribute(k_nd_bwd<RG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap);
+              double* y, double* xe, double* upd, double* fb, const int* ist, cudaStream_t s) {
+  // dynamic shared memory: the staged vector, plus (staging kernels) the
+  // operator rows where they fit
+  const int fwd_cap = kNdSmemOptin - kNdItemRows * RG * (int)sizeof(double);
+  const int bwd_cap = kNdSmemOptin;
+  cudaFuncSetAttribute(k_nd_fwd<RG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNdSmemMax);
+  cudaFuncSetAttribute(k_nd_bwd<RG, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kNdSmemMax);
+  cudaFuncSetAttribute(k_nd_fwd<RG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, fwd_cap);
+  cudaFuncSetAttribute(k_nd_bwd<RG, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bwd_cap);
+  const int rel = P->release_early;
   for (int lv = 0; lv < P->n_levels; ++lv) {
     const int64_t a = P->fwd_level_ptr[lv], b = P->fwd_level_ptr[lv + 1];
     if (b == a) continue;
     const size_t smem = (size_t)std::max(P->fwd_level_smax[lv], 1) * RG * sizeof(double);
-    launch_after_previous(k_nd_fwd<RG>, (unsigned)(b - a), smem, s, fa, a, R, w, y, upd, ist);
+    const int64_t gmax = P->fwd_level_gmax ? P->fwd_level_gmax[lv] : -1;
+    const bool stage = gmax >= 0 && (int64_t)smem + gmax <= fwd_cap;
+    const double* f = nullptr;
+    if (fb != nullptr && P->gat_level_ptr != nullptr) {
+      const int64_t ga = P->gat_level_ptr[lv], gb = P->gat_level_ptr[lv + 1];
+      if (gb > ga) {
+        launch_after_previous(k_nd_gather, (unsigned)(gb - ga), 0, s, fa, P->gat_items, ga, R, w,
+                              (const double*)upd, fb, ist, rel);
+        f = fb;
+      }
+    }
+    if (stage)
+      launch_after_previous(k_nd_fwd<RG, true>, (unsigned)(b - a), smem + (size_t)gmax, s, fa, a, R, w, f, y,
+                            upd, ist, rel);
+    else
+      launch_after_previous(k_nd_fwd<RG, false>, (unsigned)(b - a), smem, s, fa, a, R, w, f, y, upd, ist, rel);
   }
   for (int lv = 0; lv < P->n_levels; ++lv) {
     const int64_t a = P->bwd_level_ptr[lv], b = P->bwd_level_ptr[lv + 1];
     if (b == a) continue;
     const size_t smem = (size_t)std::max(P->bwd_level_mmax[lv], 1) * RG * sizeof(double);
-    launch_after_previous(k_nd_bwd<RG>, (unsigned)(b - a), smem, s, ba, a, R, (const double*)y, xe, x, ist);
+    const int64_t gmax = P->bwd_level_gmax ? P->bwd_level_gmax[lv] : -1;
+    const bool stage = gmax >= 0 && (int64_t)smem + gmax <= bwd_cap;
+    if (stage)
+      launch_after_previous(k_nd_bwd<RG, true>, (unsigned)(b - a), smem + (size_t)gmax, s, ba, a, R,
+                            (const double*)y, xe, x, ist, rel);
+    else
+      launch_after_previous(k_nd_bwd<RG, false>, (unsigned)(b - a), smem, s, ba, a, R, (const double*)y, xe, x,
+                            ist, rel);
   }
   DDX_LAUNCH_CHECK("ddx_coarse_solve_nd");
   return DDX_OK;
@@ -404,8 +567,11 @@ int ddx_nd_order(int64_t n, const int64_t* indptr, const int64_t* indices, int l
 }
 
 int ddx_coarse_solve_nd(const ddx_nd_plan* P, int R, const double* w, double* x, double* y, double* xe,
-                        double* upd, const int* ist, ddx_stream_t stream) {
+                        double* upd, double* fb, const int* ist, ddx_stream_t stream) {
   DDX_REQUIRE(P && w && x && y && xe && upd && R >= 1, "ddx_coarse_solve_nd: bad arguments");
+  DDX_REQUIRE(fb == nullptr || P->gat_level_ptr == nullptr || P->gat_level_ptr[P->n_levels] == 0 ||
+                  P->gat_items != nullptr,
+              "ddx_coarse_solve_nd: plan with gather levels but no gather items");
   DDX_REQUIRE(P->s_first && P->fpos, "ddx_coarse_solve_nd: plan without elimination positions");
   DDX_REQUIRE(P->fwd_level_ptr && P->bwd_level_ptr && P->fwd_level_smax && P->bwd_level_mmax,
               "ddx_coarse_solve_nd: plan without level tables");
@@ -423,11 +589,11 @@ int ddx_coarse_solve_nd(const ddx_nd_plan* P, int R, const double* w, double* x,
   DDX_REQUIRE(mmax * (int64_t)sizeof(double) <= kNdSmemMax, "ddx_coarse_solve_nd: front of %lld exceeds %d B",
               (long long)mmax, kNdSmemMax);
   switch (rg) {
-    case 1: return nd_sweeps<1>(P, fa, ba, R, w, x, y, xe, upd, ist, s);
-    case 2: return nd_sweeps<2>(P, fa, ba, R, w, x, y, xe, upd, ist, s);
-    case 4: return nd_sweeps<4>(P, fa, ba, R, w, x, y, xe, upd, ist, s);
-    case 8: return nd_sweeps<8>(P, fa, ba, R, w, x, y, xe, upd, ist, s);
-    default: return nd_sweeps<16>(P, fa, ba, R, w, x, y, xe, upd, ist, s);
+    case 1: return nd_sweeps<1>(P, fa, ba, R, w, x, y, xe, upd, fb, ist, s);
+    case 2: return nd_sweeps<2>(P, fa, ba, R, w, x, y, xe, upd, fb, ist, s);
+    case 4: return nd_sweeps<4>(P, fa, ba, R, w, x, y, xe, upd, fb, ist, s);
+    case 8: return nd_sweeps<8>(P, fa, ba, R, w, x, y, xe, upd, fb, ist, s);
+    default: return nd_sweeps<16>(P, fa, ba, R, w, x, y, xe, upd, fb, ist, s);
   }
 }
 

@@ -335,14 +335,24 @@ typedef struct ddx_nd_plan {
   const double* GT;
   const int64_t* s_first; /* elimination position of front t's first separator vertex */
   const int* fpos;        /* elimination position of every front position (idx_off numbering) */
+  const int64_t* gat_level_ptr; /* host, n_levels+1: gather items of each forward level (NULL: none) */
+  const int* gat_items;         /* (front, first position, positions) per gather item */
+  const int64_t* fwd_level_gmax; /* host, n_levels: largest operator range of a forward item, bytes
+                                    (NULL: no staging in shared memory) */
+  const int64_t* bwd_level_gmax; /* host, n_levels: the same for the backward items, root level first;
+                                    a negative entry leaves that level's operator in global memory */
+  int release_early;             /* 1: each level's kernel lets the next one launch right after its wait */
 } ddx_nd_plan;
 
 /* x = A^-1 w for w, x of shape (n, R) (DOF-major, FP64). y and xe (n*R
- * doubles each: the forward result and the solution in elimination order) and
- * upd (sum_t u_t * R doubles) are caller-owned scratch. With ist (PCG state),
- * nothing runs once every right-hand side has converged. Deterministic. */
+ * doubles each: the forward result and the solution in elimination order),
+ * upd (sum_t u_t * R doubles) and fb (sum_t (s_t+u_t) * R doubles: the
+ * assembled front vectors of the levels that have gather items; NULL gathers
+ * inside the forward items instead, same results) are caller-owned scratch.
+ * With ist (PCG state), nothing runs once every right-hand side has
+ * converged. Deterministic. */
 int ddx_coarse_solve_nd(const ddx_nd_plan* plan, int R, const double* w, double* x, double* y, double* xe,
-                        double* upd, const int* ist, ddx_stream_t stream);
+                        double* upd, double* fb, const int* ist, ddx_stream_t stream);
 
 /* ---- Differentiable solve -----------------------------------------------
  * No counterpart in the reference (it has no autograd). Per-cell coefficient

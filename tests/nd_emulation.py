@@ -1,7 +1,7 @@
 """Host emulation of the sparse coarse-solve kernels, for tests only.
 
-``emulate_solve`` re-runs the arithmetic of ``k_nd_fwd`` / ``k_nd_bwd``
-(``dd_solvers_b200/csrc/nd.cu``) work item by work item in NumPy, with the same
+``emulate_solve`` re-runs the arithmetic of ``k_nd_gather`` / ``k_nd_fwd`` /
+``k_nd_bwd`` (``dd_solvers_b200/csrc/nd.cu``) work item by work item in NumPy, with the same
 index maps, level order and elimination-order buffers, so that the plan built
 by ``dd_solvers_b200.nd`` can be checked without a GPU.
 """
@@ -21,17 +21,29 @@ def emulate_solve(sym: NDSymbolic, G: np.ndarray, GT: np.ndarray, w: np.ndarray)
     s_first = np.cumsum(sym.s) - sym.s
     fpos = sym.pos[sym.fidx]
     upd = np.zeros((max(sym.upd_total, 1), R))
+    fb = np.full((len(sym.fidx), R), np.nan)  # gathered front vectors; NaN where never written
+
+    def gather(t, p):
+        io = int(sym.idx_off[t])
+        acc = w[sym.fidx[io + p]].copy() if p < sym.s[t] else np.zeros(R)
+        for q in range(sym.gptr[io + p], sym.gptr[io + p + 1]):
+            acc = acc + upd[sym.gsrc[q]]
+        return acc
+
     for lv in range(sym.n_levels):
+        ga, gb = sym.gat_level_ptr[lv], sym.gat_level_ptr[lv + 1]
+        for it in range(ga, gb):
+            t, p0, npos = sym.gat_items[it]
+            for p in range(p0, p0 + npos):
+                fb[sym.idx_off[t] + p] = gather(t, p)
         for it in range(sym.fwd_level_ptr[lv], sym.fwd_level_ptr[lv + 1]):
             t, r0, nr = sym.fwd_items[it]
             s, u = int(sym.s[t]), int(sym.u[t])
             io, go = int(sym.idx_off[t]), int(sym.g_off[t])
-            f = np.zeros((s + u, R))
-            for p in range(s + u):
-                acc = w[sym.fidx[io + p]].copy() if p < s else np.zeros(R)
-                for q in range(sym.gptr[io + p], sym.gptr[io + p + 1]):
-                    acc = acc + upd[sym.gsrc[q]]
-                f[p] = acc
+            if gb > ga:
+                f = fb[io:io + s + u]
+            else:
+                f = np.array([gather(t, p) for p in range(s + u)]).reshape(s + u, R)
             Gt = G[go:go + (s + u) * s].reshape(s + u, s)
             for p in range(r0, r0 + nr):
                 out = Gt[p] @ f[:s] if s else np.zeros(R)

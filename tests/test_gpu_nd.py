@@ -30,13 +30,38 @@ def to_dev(A):
 
 @pytest.mark.parametrize("case", sorted(CASES))
 @pytest.mark.parametrize("R", [1, 3, 16])
-def test_nd_solve_matches_sparse_lu(case, R):
+@pytest.mark.parametrize("tree", ["merged", "full"])
+def test_nd_solve_matches_sparse_lu(case, R, tree):
+    """One merged front (the default for these small cases), or the full
+    separator tree cut into 8-row items, whose upper levels take the gather
+    launch."""
     A = CASES[case]()
-    solver = nd.NDSolver(to_dev(A), leaf=32)
+    solver = nd.NDSolver(to_dev(A), leaf=32 if tree == "merged" else 16, top_merge=None if tree == "merged" else 0)
+    if tree == "full":
+        solver.set_items(512, 8)
+        assert solver.sym.gat_level_ptr[-1] > 0
     w = np.random.default_rng(R).standard_normal((A.shape[0], R))
     x = solver.solve(torch.as_tensor(w, device="cuda")).cpu().numpy()
     ref = spla.splu(A.tocsc()).solve(w)
     assert np.abs(x - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def test_nd_sweep_variants_agree_bitwise(monkeypatch):
+    """Operator rows staged in shared memory or read from global memory, f
+    gathered by the gather launch or inside the forward items, early or late
+    release of the next level: the same sums in the same order, so the same
+    bits."""
+    A = lap2d(45)
+    solver = nd.NDSolver(to_dev(A), leaf=16, top_merge=0)
+    solver.set_items(512, 8)
+    assert solver.gather and solver.plan.release_early == 1 and (solver.fwd_level_gmax >= 0).any()
+    w = torch.randn(A.shape[0], 3, dtype=torch.float64, device="cuda")
+    ref = solver.solve(w)
+    for knob in ("STAGE", "GATHER", "RELEASE"):
+        monkeypatch.setattr(nd, knob, False)
+        solver.set_items(512, 8)
+        assert torch.equal(solver.solve(w), ref), knob
+    assert not solver.gather and solver.plan.release_early == 0 and (solver.fwd_level_gmax < 0).all()
 
 
 def test_nd_solve_matches_host_emulation_and_is_deterministic():

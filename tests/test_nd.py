@@ -45,11 +45,15 @@ CASES = {
 
 
 @pytest.mark.parametrize("case", sorted(CASES))
-@pytest.mark.parametrize("leaf", [8, 64])
-def test_emulated_solve_matches_sparse_lu(case, leaf):
+@pytest.mark.parametrize("leaf,top_merge,small_items", [(8, None, False), (64, None, False), (16, 0, True)])
+def test_emulated_solve_matches_sparse_lu(case, leaf, top_merge, small_items):
+    """The last variant keeps the whole separator tree and cuts 8-row items,
+    so the upper levels run the gather launch."""
     A = CASES[case]()
     A.sort_indices()
-    sym = nd.NDSymbolic(A.indptr, A.indices, A.shape[0], leaf)
+    sym = nd.NDSymbolic(A.indptr, A.indices, A.shape[0], leaf, top_merge)
+    if small_items:
+        sym.build_items(512, 8)
     G, GT = (t.numpy() for t in nd.factorize(sym, A.indptr, A.indices, A.data, "cpu"))
     w = np.random.default_rng(0).standard_normal((A.shape[0], 3))
     x = emulate_solve(sym, G, GT, w)
@@ -107,3 +111,34 @@ def test_symbolic_front_sets():
             ends = [r0 + nr for r0, nr in cover]
             assert cover[0][0] == 0 and ends[-1] == total[t]
             assert all(cover[i + 1][0] == ends[i] for i in range(len(cover) - 1))
+
+
+@pytest.mark.parametrize("case", ["grid45", "dg_p0_S7_on_S4"])
+def test_gather_items_cover_their_levels(case):
+    """Where a level has gather items, they cover every position of every
+    front of that level exactly once; levels whose fronts are cut into many
+    forward items get them."""
+    A = CASES[case]()
+    sym = nd.NDSymbolic(A.indptr, A.indices, A.shape[0], 16, top_merge=0)
+    sym.build_items(512, 8)
+    m = sym.s + sym.u
+    gathered = 0
+    for lv in range(sym.n_levels):
+        ga, gb = sym.gat_level_ptr[lv], sym.gat_level_ptr[lv + 1]
+        a, b = sym.fwd_level_ptr[lv], sym.fwd_level_ptr[lv + 1]
+        repeated = int(sym.s[sym.fwd_items[a:b, 0]].sum())
+        once = int(m[sym.by_level[lv]].sum())
+        assert (gb > ga) == (lv >= nd.GATHER_MIN_LEVEL and repeated >= nd.GATHER_MIN_RATIO * once)
+        if gb == ga:
+            continue
+        gathered += 1
+        cover = {}
+        for t, p0, npos in sym.gat_items[ga:gb]:
+            assert 0 < npos <= nd.GATHER_POSITIONS
+            cover.setdefault(int(t), []).append((int(p0), int(npos)))
+        assert sorted(cover) == sorted(int(t) for t in sym.by_level[lv])
+        for t, parts in cover.items():
+            parts.sort()
+            assert parts[0][0] == 0 and parts[-1][0] + parts[-1][1] == m[t]
+            assert all(parts[i][0] + parts[i][1] == parts[i + 1][0] for i in range(len(parts) - 1))
+    assert gathered >= 1
