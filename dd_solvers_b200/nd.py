@@ -41,7 +41,7 @@ a fixed order, so results are deterministic. The sweeps are latency-bound;
 up to ``OVERLAP_MAX_N`` rows each item stages its operator rows in shared
 memory before waiting on the previous level and releases the next level
 right after that wait (measured on B200: -10% PCG time at 131k coarse rows,
-no change at 1.05M and 2.1M).
+-9% at 524k, no change at 1.05M; above 1M rows it stays off).
 """
 from __future__ import annotations
 
@@ -56,6 +56,7 @@ LEAF = 128          # largest subgraph left undissected (a leaf front)
 TOP_MERGE = 2048    # merge the top levels into one dense front while it holds at most this many vertices
 ITEM_BYTES = 32768  # operator bytes per work item (rows of G or of G^T) ...
 ITEM_MAX_ROWS = 64  # ... between 8 and this many rows
+FAT_ITEMS_MIN_N = 1_000_000  # above this many rows: items of 64 KB and up to 128 rows
 GATHER_POSITIONS = 256  # front positions per gather item
 GATHER_MIN_RATIO = 2.0  # gather f once per front on levels whose items would gather >= this x its size
 GATHER_MIN_LEVEL = 1    # ... from this tree level up (leaf fronts have no children to add)
@@ -64,7 +65,7 @@ GATHER_MIN_LEVEL = 1    # ... from this tree level up (leaf fronts have no child
 # early release of the next level's kernel (RELEASE); all three for coarse
 # problems of up to OVERLAP_MAX_N rows, and staging only on levels of at most
 # STAGE_MAX_WAVES x (SMs x 4) items (None: every level).
-OVERLAP_MAX_N = 300_000
+OVERLAP_MAX_N = 1_000_000
 STAGE, GATHER, RELEASE = True, True, True
 STAGE_MAX_WAVES = None
 
@@ -486,8 +487,9 @@ class NDSolver:
         p.G = self.G.data_ptr()
         p.GT = self.GT.data_ptr()
         self.plan = p
-        if self.n > 300_000:
-            # measured on B200: fatter items pay off from ~500k coarse DOFs (tens of thousands of leaf items)
+        if self.n > FAT_ITEMS_MIN_N:
+            # measured on B200 (hybrid FP16 PCG, same box): with staging, 32 KB items are 9% faster at 524k
+            # coarse rows, equal at 1.05M; unstaged 64 KB items are 1% faster at 2.1M
             sym.build_items(65536, 128)
         self._set_items()
         self._work = {}
