@@ -142,3 +142,27 @@ def test_gather_items_cover_their_levels(case):
             assert parts[0][0] == 0 and parts[-1][0] + parts[-1][1] == m[t]
             assert all(parts[i][0] + parts[i][1] == parts[i + 1][0] for i in range(len(parts) - 1))
     assert gathered >= 1
+
+
+def test_plan_binding_matches_the_c_struct(tmp_path):
+    """``nd._Plan`` (ctypes) has the layout of ``ddx_nd_plan`` in
+    ``include/ddx.h``: every field at the same offset, the same size."""
+    import ctypes
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    names = [f[0] for f in nd._Plan._fields_]
+    src = tmp_path / "plan_layout.c"
+    body = "".join(f'  printf("{n} %zu\\n", offsetof(ddx_nd_plan, {n}));\n' for n in names)
+    src.write_text("#include <stddef.h>\n#include <stdio.h>\n#include \"ddx.h\"\nint main(void) {\n"
+                   + body + '  printf("sizeof %zu\\n", sizeof(ddx_nd_plan));\n  return 0;\n}\n')
+    exe = tmp_path / "plan_layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(line.split() for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                       text=True).stdout.splitlines())
+    for n in names:
+        assert int(out[n]) == getattr(nd._Plan, n).offset, n
+    assert int(out["sizeof"]) == ctypes.sizeof(nd._Plan)
