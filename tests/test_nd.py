@@ -166,3 +166,27 @@ def test_plan_binding_matches_the_c_struct(tmp_path):
     for n in names:
         assert int(out[n]) == getattr(nd._Plan, n).offset, n
     assert int(out["sizeof"]) == ctypes.sizeof(nd._Plan)
+
+
+def test_solver_size_switches(monkeypatch):
+    """The size rules of ``nd.NDSolver`` (built on the host here, no solve):
+    up to ``OVERLAP_MAX_N`` rows the sweeps stage their operator rows, gather
+    per front and release the next level early; above ``FAT_ITEMS_MIN_N``
+    the items are re-cut to 64 KB."""
+    import torch
+
+    A = lap2d(45)
+    A.sort_indices()
+    At = torch.sparse_csr_tensor(torch.as_tensor(A.indptr), torch.as_tensor(A.indices), torch.as_tensor(A.data),
+                                 A.shape)
+    s = nd.NDSolver(At, leaf=16, top_merge=0)
+    assert s.gather and s.plan.release_early == 1
+    assert np.array_equal(s.fwd_level_gmax, s.sym.fwd_level_gmax)
+    small = s.sym.fwd_items.shape[0]
+    monkeypatch.setattr(nd, "OVERLAP_MAX_N", 100)
+    monkeypatch.setattr(nd, "FAT_ITEMS_MIN_N", 100)
+    s = nd.NDSolver(At, leaf=16, top_merge=0)
+    assert not s.gather and s.plan.release_early == 0
+    assert (s.fwd_level_gmax < 0).all() and (s.bwd_level_gmax < 0).all()
+    assert s.sym.fwd_items.shape[0] <= small
+    assert int(s.sym.fwd_items[:, 2].max()) <= 128
