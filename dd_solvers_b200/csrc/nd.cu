@@ -101,7 +101,8 @@ struct NdArgs {
 
 // The static part of one front position's gather, read before the wait: its
 // right-hand-side row (separator positions), its range in the gather map and
-// the first two update rows it adds (a binary separator tree gives at most two).
+// the first two update rows it adds (the two children of a binary separator
+// tree; positions of the merged top front may add more, read after the wait).
 struct GatherSlot {
   int64_t v = 0, q0 = 0, q1 = 0, g0 = 0, g1 = 0;
   __device__ __forceinline__ void load(const NdArgs& A, int64_t io, int p, int s) {
