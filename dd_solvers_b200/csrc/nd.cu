@@ -28,6 +28,10 @@
 // reads its static index maps before waiting on the previous level: after the
 // wait only the right-hand-side reads remain on its critical path.
 #include <algorithm>
+#include <atomic>
+#include <cstdlib>
+#include <exception>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -404,32 +408,63 @@ int nd_sweeps(const ddx_nd_plan* P, const NdArgs& fa, const NdArgs& ba, int R, c
 // ---------------------------------------------------------------------------
 // ordering: recursive BFS level-set bisection
 // ---------------------------------------------------------------------------
+// The two halves below a separator are independent subgraphs, so they are
+// ordered on separate threads down to a few levels. The output does not
+// depend on the threads: every subtree owns a known slice of perm (its
+// vertices, in the sequential order: first half, second half, separator), and
+// its nodes are numbered after the parent joins the halves' node lists.
+
+constexpr int64_t kNdParMin = 20000;  // smallest pair of halves worth a thread
+
+// Nodes of one subtree in creation (post-)order: perm offset and size of each
+// node's vertex set, and its parent (index in this list; -1 for the roots).
+struct NodeList {
+  std::vector<int64_t> first, size, parent;
+  void append(const NodeList& o) {
+    const int64_t base = (int64_t)first.size();
+    for (size_t i = 0; i < o.first.size(); ++i) {
+      first.push_back(o.first[i]);
+      size.push_back(o.size[i]);
+      parent.push_back(o.parent[i] < 0 ? -1 : o.parent[i] + base);
+    }
+  }
+  void add(int64_t f, int64_t s) {
+    first.push_back(f);
+    size.push_back(s);
+    parent.push_back(-1);
+  }
+};
+
 struct NdOrder {
   int64_t n;
   std::vector<int64_t> ptr, adj;  // symmetric adjacency, no self loops
-  std::vector<int64_t> label;     // current subgraph label, -1 once eliminated
-  std::vector<int64_t> seen, level;
-  int64_t stamp = 0, next_label = 1;
-  int leaf;
-  int64_t* perm;
-  int64_t* node_first;
-  int64_t* node_parent;
-  int64_t n_nodes = 0, perm_len = 0;
+  // current subgraph label of each vertex (-1 eliminated, -2 separator being
+  // ordered below). A BFS reads the labels of neighbours that another thread
+  // may be relabelling, never to the BFS's own label: relaxed atomics.
+  std::vector<int64_t> label;
+  std::vector<int64_t> seen, level;  // written only by the thread ordering the vertex's subgraph
+  std::atomic<int64_t> stamp{0}, next_label{1};
+  int leaf = 128;
+  int par_depth = 0;  // recursion depth down to which the halves run on separate threads
+  int64_t* perm = nullptr;
 
-  // BFS over vertices with label == lab from src; returns the visit order
-  // and fills level[] for the visited vertices.
+  int64_t get_label(int64_t v) { return __atomic_load_n(&label[v], __ATOMIC_RELAXED); }
+  void set_label(int64_t v, int64_t l) { __atomic_store_n(&label[v], l, __ATOMIC_RELAXED); }
+
+  // BFS over vertices labelled lab from src; returns the visit order and
+  // fills level[] for the visited vertices.
   void bfs(int64_t src, int64_t lab, std::vector<int64_t>& order) {
-    ++stamp;
+    const int64_t st = stamp.fetch_add(1) + 1;
     order.clear();
     order.push_back(src);
-    seen[src] = stamp;
+    seen[src] = st;
     level[src] = 0;
     for (size_t h = 0; h < order.size(); ++h) {
       const int64_t v = order[h];
       for (int64_t e = ptr[v]; e < ptr[v + 1]; ++e) {
         const int64_t w = adj[e];
-        if (label[w] == lab && seen[w] != stamp) {
-          seen[w] = stamp;
+        if (get_label(w) == lab && seen[w] != st) {
+          seen[w] = st;
           level[w] = level[v] + 1;
           order.push_back(w);
         }
@@ -437,69 +472,105 @@ struct NdOrder {
     }
   }
 
-  int64_t create(std::vector<int64_t>& S, const std::vector<int64_t>& kids) {
+  // a node eliminating the vertices S (sorted) from perm[off]
+  void put(std::vector<int64_t>& S, int64_t off, NodeList& out) {
     std::sort(S.begin(), S.end());
-    const int64_t id = n_nodes++;
-    node_first[id] = perm_len;
-    for (int64_t v : S) {
-      perm[perm_len++] = v;
-      label[v] = -1;
+    for (size_t i = 0; i < S.size(); ++i) {
+      perm[off + (int64_t)i] = S[i];
+      set_label(S[i], -1);
     }
-    node_first[id + 1] = perm_len;
-    node_parent[id] = -1;
-    for (int64_t k : kids) node_parent[k] = id;
-    return id;
+    out.add(off, (int64_t)S.size());
   }
 
-  // Vertices V (all carrying label lab): returns the root nodes built for them.
-  std::vector<int64_t> process(std::vector<int64_t> V, int64_t lab) {
-    std::vector<int64_t> roots;
+  // Vertices V (all labelled lab), placed in perm from off: the nodes built for them.
+  NodeList process(std::vector<int64_t> V, int64_t lab, int64_t off, int depth) {
+    NodeList out;
     std::vector<std::vector<int64_t>> comps;
     std::vector<int64_t> order;
     for (int64_t v : V) {
-      if (label[v] != lab) continue;
+      if (get_label(v) != lab) continue;
       bfs(v, lab, order);
-      const int64_t lc = next_label++;
-      for (int64_t u : order) label[u] = lc;
+      const int64_t lc = next_label.fetch_add(1);
+      for (int64_t u : order) set_label(u, lc);
       comps.push_back(order);
     }
     for (auto& C : comps) {
-      const int64_t lc = label[C[0]];
-      if ((int64_t)C.size() <= leaf) {
-        roots.push_back(create(C, {}));
+      const int64_t lc = get_label(C[0]);
+      const int64_t csize = (int64_t)C.size();
+      if (csize <= leaf) {
+        put(C, off, out);
+        off += csize;
         continue;
       }
       bfs(C[0], lc, order);
       const int64_t far = order.back();
       bfs(far, lc, order);
-      const int64_t depth = level[order.back()];
-      if (depth < 2) {
-        roots.push_back(create(C, {}));
+      const int64_t depth_c = level[order.back()];
+      if (depth_c < 2) {
+        put(C, off, out);
+        off += csize;
         continue;
       }
-      std::vector<int64_t> cnt(depth + 1, 0);
+      std::vector<int64_t> cnt(depth_c + 1, 0);
       for (int64_t v : order) ++cnt[level[v]];
       int64_t k = 0, cum = 0;
-      while (k <= depth && 2 * (cum + cnt[k]) < (int64_t)C.size()) cum += cnt[k++];
-      k = std::min(std::max(k, (int64_t)1), depth - 1);
+      while (k <= depth_c && 2 * (cum + cnt[k]) < csize) cum += cnt[k++];
+      k = std::min(std::max(k, (int64_t)1), depth_c - 1);
       std::vector<int64_t> S, Av, Bv;
       for (int64_t v : order) {
         if (level[v] == k) S.push_back(v);
         else if (level[v] < k) Av.push_back(v);
         else Bv.push_back(v);
       }
-      const int64_t la = next_label++, lb = next_label++;
-      for (int64_t v : S) label[v] = -2;  // removed from both halves
-      for (int64_t v : Av) label[v] = la;
-      for (int64_t v : Bv) label[v] = lb;
-      std::vector<int64_t> kids = process(std::move(Av), la);
-      std::vector<int64_t> kb = process(std::move(Bv), lb);
-      kids.insert(kids.end(), kb.begin(), kb.end());
-      roots.push_back(create(S, kids));
+      const int64_t la = next_label.fetch_add(1), lb = next_label.fetch_add(1);
+      for (int64_t v : S) set_label(v, -2);  // removed from both halves
+      for (int64_t v : Av) set_label(v, la);
+      for (int64_t v : Bv) set_label(v, lb);
+      const int64_t na = (int64_t)Av.size(), nb = (int64_t)Bv.size();
+      NodeList A, B;
+      if (depth < par_depth && na + nb >= kNdParMin) {
+        std::exception_ptr err;
+        std::thread th([&] {
+          try {
+            A = process(std::move(Av), la, off, depth + 1);
+          } catch (...) {
+            err = std::current_exception();
+          }
+        });
+        try {
+          B = process(std::move(Bv), lb, off + na, depth + 1);
+        } catch (...) {
+          th.join();
+          throw;
+        }
+        th.join();
+        if (err) std::rethrow_exception(err);
+      } else {
+        A = process(std::move(Av), la, off, depth + 1);
+        B = process(std::move(Bv), lb, off + na, depth + 1);
+      }
+      const int64_t base = (int64_t)out.first.size();
+      out.append(A);
+      out.append(B);
+      const int64_t sid = (int64_t)out.first.size();
+      for (int64_t i = base; i < sid; ++i)
+        if (out.parent[i] < 0) out.parent[i] = sid;
+      put(S, off + na + nb, out);
+      off += csize;
     }
-    return roots;
+    return out;
   }
 };
+
+// threads for the ordering: DDX_ND_THREADS if set, else the host's
+int nd_order_threads() {
+  if (const char* e = std::getenv("DDX_ND_THREADS")) {
+    const int t = std::atoi(e);
+    if (t >= 1) return t;
+  }
+  const unsigned hw = std::thread::hardware_concurrency();
+  return hw ? (int)hw : 1;
+}
 
 }  // namespace
 }  // namespace ddx
@@ -516,8 +587,7 @@ int ddx_nd_order(int64_t n, const int64_t* indptr, const int64_t* indices, int l
   o.n = n;
   o.leaf = leaf;
   o.perm = perm;
-  o.node_first = node_first;
-  o.node_parent = node_parent;
+  for (int t = nd_order_threads(); t > 1 && o.par_depth < 6; t >>= 1) ++o.par_depth;
   // symmetrised adjacency without the diagonal
   std::vector<int64_t> deg(n + 1, 0);
   for (int64_t i = 0; i < n; ++i)
@@ -559,11 +629,24 @@ int ddx_nd_order(int64_t n, const int64_t* indptr, const int64_t* indices, int l
   o.level.assign(n, 0);
   std::vector<int64_t> all(n);
   for (int64_t i = 0; i < n; ++i) all[i] = i;
-  node_first[0] = 0;
-  o.process(std::move(all), 0);
-  *n_nodes = o.n_nodes;
-  DDX_REQUIRE(o.perm_len == n, "ddx_nd_order: ordering incomplete (%lld of %lld)", (long long)o.perm_len,
-              (long long)n);
+  NodeList nodes;
+  try {
+    nodes = o.process(std::move(all), 0, 0, 0);
+  } catch (const std::exception& ex) {
+    ::ddx::set_error("ddx_nd_order: %s", ex.what());
+    return DDX_ERR_ARG;
+  }
+  const int64_t nn = (int64_t)nodes.first.size();
+  int64_t end = 0;
+  for (int64_t i = 0; i < nn; ++i) {
+    DDX_REQUIRE(nodes.first[i] == end, "ddx_nd_order: node %lld out of order", (long long)i);
+    node_first[i] = nodes.first[i];
+    node_parent[i] = nodes.parent[i];
+    end += nodes.size[i];
+  }
+  node_first[nn] = end;
+  *n_nodes = nn;
+  DDX_REQUIRE(end == n, "ddx_nd_order: ordering incomplete (%lld of %lld)", (long long)end, (long long)n);
   return DDX_OK;
 }
 

@@ -296,7 +296,9 @@ int ddx_coarse_gemv_f64(int n_c, int R, const double* Ainv, const double* w, dou
  * separator tree in post-order: node t eliminates perm[node_first[t] ..
  * node_first[t+1]), its parent is node_parent[t] (-1 for a root); *n_nodes
  * receives the node count. perm holds n entries; node_first and node_parent
- * need room for n + 1 entries. */
+ * need room for n + 1 entries. The halves below large separators are ordered
+ * on host threads (the environment variable DDX_ND_THREADS caps them, default
+ * the host's hardware threads); the output is the same for any thread count. */
 int ddx_nd_order(int64_t n, const int64_t* indptr, const int64_t* indices, int leaf, int64_t* perm,
                  int64_t* node_first, int64_t* node_parent, int64_t* n_nodes);
 

@@ -190,3 +190,20 @@ def test_solver_size_switches(monkeypatch):
     assert (s.fwd_level_gmax < 0).all() and (s.bwd_level_gmax < 0).all()
     assert s.sym.fwd_items.shape[0] <= small
     assert int(s.sym.fwd_items[:, 2].max()) <= 128
+
+
+def test_threaded_ordering_matches_single_threaded(monkeypatch):
+    """The ordering runs the halves below large separators on separate
+    threads; the separator tree and permutation are the same for any thread
+    count (40,000 vertices: halves above the threading threshold)."""
+    A = lap2d(200)
+    A.sort_indices()
+    out = []
+    for threads in ("1", "2", "8"):
+        monkeypatch.setenv("DDX_ND_THREADS", threads)
+        S, parent = nd.nested_dissection(A.indptr, A.indices, A.shape[0], 64)
+        out.append((np.concatenate(S), np.array([len(x) for x in S]), parent))
+    for perm, sizes, parent in out[1:]:
+        assert np.array_equal(perm, out[0][0])
+        assert np.array_equal(sizes, out[0][1])
+        assert np.array_equal(parent, out[0][2])
