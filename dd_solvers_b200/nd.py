@@ -70,9 +70,31 @@ STAGE, GATHER, RELEASE = True, True, True
 STAGE_MAX_WAVES = None
 
 
-def _rows_per_item(row_len: int, item_bytes: int, max_rows: int) -> int:
-    r = item_bytes // (8 * max(row_len, 1))
-    return int(min(max_rows, max(8, r // 8 * 8)))
+def _rows_per_item(row_len, item_bytes: int, max_rows: int):
+    """Rows of ``row_len`` doubles per work item: about ``item_bytes`` of
+    operator, a multiple of 8 between 8 and ``max_rows`` (elementwise on arrays)."""
+    r = item_bytes // (8 * np.maximum(row_len, 1))
+    return np.minimum(max_rows, np.maximum(8, r // 8 * 8))
+
+
+def _cut_items(levels, length, width, item_bytes: int, max_rows: int):
+    """Work items (front, first row, rows) over the fronts of ``levels`` in
+    order: front t's ``length[t]`` rows of ``width[t]`` doubles cut into runs
+    of ``_rows_per_item(width[t])``. Returns the (k, 3) int32 items and the
+    per-level item pointer."""
+    sizes = np.array([len(f) for f in levels], dtype=np.int64)
+    fronts = np.concatenate([np.asarray(f, dtype=np.int64) for f in levels] + [np.zeros(0, dtype=np.int64)])
+    ln = np.maximum(length[fronts], 1)
+    step = _rows_per_item(width[fronts], item_bytes, max_rows)
+    count = -(-ln // step)
+    ccum = np.concatenate([[0], np.cumsum(count)]).astype(np.int64)
+    ptr = ccum[np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)]
+    t = np.repeat(fronts, count)
+    k = np.arange(int(count.sum())) - np.repeat(np.cumsum(count) - count, count)
+    st = np.repeat(step, count)
+    r0 = k * st
+    nr = np.minimum(st, np.repeat(length[fronts], count) - r0)
+    return np.stack([t, r0, nr], axis=1).astype(np.int32), ptr
 
 
 # ---------------------------------------------------------------------------
@@ -235,25 +257,8 @@ class NDSymbolic:
         """Per-level work items: (front, first row, rows) of G_t for the forward
         sweep (leaves first), of G_t^T for the backward sweep (root first)."""
         m = self.s + self.u
-        fwd, bwd = [], []
-        self.fwd_level_ptr = np.zeros(self.n_levels + 1, dtype=np.int64)
-        self.bwd_level_ptr = np.zeros(self.n_levels + 1, dtype=np.int64)
-        for lv in range(self.n_levels):
-            for t in self.by_level[lv]:
-                rows = int(m[t])
-                step = _rows_per_item(int(self.s[t]), item_bytes, max_rows)
-                for r0 in range(0, max(rows, 1), step):
-                    fwd.append((t, r0, min(step, rows - r0)))
-            self.fwd_level_ptr[lv + 1] = len(fwd)
-        for j, lv in enumerate(range(self.n_levels - 1, -1, -1)):
-            for t in self.by_level[lv]:
-                cols = int(self.s[t])
-                step = _rows_per_item(int(m[t]), item_bytes, max_rows)
-                for c0 in range(0, cols, step):
-                    bwd.append((t, c0, min(step, cols - c0)))
-            self.bwd_level_ptr[j + 1] = len(bwd)
-        self.fwd_items = np.array(fwd, dtype=np.int32).reshape(-1, 3)
-        self.bwd_items = np.array(bwd, dtype=np.int32).reshape(-1, 3)
+        self.fwd_items, self.fwd_level_ptr = _cut_items(self.by_level, m, self.s, item_bytes, max_rows)
+        self.bwd_items, self.bwd_level_ptr = _cut_items(self.by_level[::-1], self.s, m, item_bytes, max_rows)
         # largest operator range of an item per level (bytes): staged in shared memory where it fits
         self.fwd_level_gmax = np.zeros(self.n_levels, dtype=np.int64)
         self.bwd_level_gmax = np.zeros(self.n_levels, dtype=np.int64)
