@@ -214,29 +214,27 @@ class NDSymbolic:
         self.g_total = int((m * self.s).sum())
         self.upd_total = int(self.u.sum())
         self.fidx = np.concatenate([np.concatenate([S[t], U[t]]) for t in range(nf)]).astype(np.int64)
-        # extend-add positions of each child's update set inside its parent's front
-        self.rel = [None] * nf
-        for t in range(nf):
-            p = parent[t]
-            if p < 0:
-                assert self.u[t] == 0
-                continue
-            fp = pos[np.concatenate([S[p], U[p]])]
-            r = np.searchsorted(fp, pos[U[t]])
-            assert np.array_equal(fp[r], pos[U[t]]), "update set not inside the parent front"
-            self.rel[t] = r
-        # gather map: per front position, the update-buffer entries to add (children in order)
-        gp, gs = [], []
-        for t in range(nf):
-            p = parent[t]
-            if p < 0:
-                continue
-            gp.append(self.idx_off[p] + self.rel[t])
-            gs.append(self.upd_off[t] + np.arange(self.u[t]))
+        # extend-add positions of each child's update set inside its parent's front:
+        # one search over (front, elimination position) keys, sorted because each
+        # front lists its separator and then its update set in elimination order
+        assert (self.u[parent < 0] == 0).all(), "a root front with an update set"
         total = int(m.sum())
-        if gp:
-            gp = np.concatenate(gp)
-            gs = np.concatenate(gs)
+        front_of = np.repeat(np.arange(nf, dtype=np.int64), m)
+        within = np.arange(total, dtype=np.int64) - np.repeat(self.idx_off, m)
+        keys = front_of * (n + 1) + pos[self.fidx]
+        upd_v = self.fidx[within >= np.repeat(self.s, m)]  # U[0], U[1], ... (update-buffer order)
+        upd_front = np.repeat(np.arange(nf, dtype=np.int64), self.u)
+        query = parent[upd_front].astype(np.int64) * (n + 1) + pos[upd_v]
+        gp = np.searchsorted(keys, query)
+        assert (gp < total).all() and np.array_equal(keys[np.minimum(gp, total - 1)], query), \
+            "update set not inside the parent front"
+        rel_all = gp - self.idx_off[parent[upd_front]] if gp.size else gp
+        self.rel = [None] * nf
+        for t in np.nonzero(parent >= 0)[0]:
+            self.rel[t] = rel_all[self.upd_off[t]:self.upd_off[t] + self.u[t]]
+        # gather map: per front position, the update-buffer entries to add (children in order)
+        gs = np.arange(self.upd_total, dtype=np.int64)
+        if gp.size:
             order = np.argsort(gp, kind="stable")
             gp, gs = gp[order], gs[order]
         else:
