@@ -31,6 +31,7 @@
 #include <atomic>
 #include <cstdlib>
 #include <exception>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -528,15 +529,22 @@ struct NdOrder {
       for (int64_t v : Bv) set_label(v, lb);
       const int64_t na = (int64_t)Av.size(), nb = (int64_t)Bv.size();
       NodeList A, B;
+      std::exception_ptr err;
+      std::thread th;
       if (depth < par_depth && na + nb >= kNdParMin) {
-        std::exception_ptr err;
-        std::thread th([&] {
-          try {
-            A = process(std::move(Av), la, off, depth + 1);
-          } catch (...) {
-            err = std::current_exception();
-          }
-        });
+        try {
+          th = std::thread([&] {
+            try {
+              A = process(std::move(Av), la, off, depth + 1);
+            } catch (...) {
+              err = std::current_exception();
+            }
+          });
+        } catch (const std::system_error&) {
+          // no thread available: order this half here (same output)
+        }
+      }
+      if (th.joinable()) {
         try {
           B = process(std::move(Bv), lb, off + na, depth + 1);
         } catch (...) {
