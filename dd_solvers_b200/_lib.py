@@ -59,6 +59,7 @@ _SIGS = {
     "ddx_spmv_csr_lanes": (_I, [_I64, _I, _P, _P, _P, _P, _I, _P, _P]),
     "ddx_schwarz_local_apply_small": (_I, [_I, _I, _P, _P, _P, _P, _I, _P, _I, _I, _I64, _P, _P, _I, _P, _P]),
     "ddx_coarse_solve_nd": (_I, [_P, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "ddx_nd_update_sets": (_I, [_I64, _I64, _P, _P, _P, _P, _P, _P, _P, _I64, _P]),
     "ddx_elem_grad_q1": (_I, [_I, _I, _P, _P, _P, _P, _P]),
 }
 

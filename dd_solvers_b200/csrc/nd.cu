@@ -658,6 +658,63 @@ int ddx_nd_order(int64_t n, const int64_t* indptr, const int64_t* indices, int l
   return DDX_OK;
 }
 
+int ddx_nd_update_sets(int64_t n, int64_t n_fronts, const int64_t* s_first, const int64_t* s_size,
+                       const int64_t* p_ptr, const int64_t* p_pos, const int64_t* parent, int64_t* u_ptr,
+                       int64_t* u_pos, int64_t capacity, int64_t* u_total) {
+  DDX_REQUIRE(n >= 0 && n_fronts >= 0 && s_first && s_size && p_ptr && p_pos && parent && u_ptr && u_total &&
+                  (capacity == 0 || u_pos),
+              "ddx_nd_update_sets: bad arguments");
+  // children of each front, in front order (a front's children precede it)
+  std::vector<int64_t> cptr(n_fronts + 1, 0), cidx;
+  for (int64_t t = 0; t < n_fronts; ++t) {
+    DDX_REQUIRE(parent[t] < n_fronts && (parent[t] < 0 || parent[t] > t), "ddx_nd_update_sets: not a post-order");
+    if (parent[t] >= 0) ++cptr[parent[t] + 1];
+  }
+  for (int64_t t = 0; t < n_fronts; ++t) cptr[t + 1] += cptr[t];
+  cidx.resize(cptr[n_fronts]);
+  {
+    std::vector<int64_t> fill(cptr.begin(), cptr.end() - 1);
+    for (int64_t t = 0; t < n_fronts; ++t)
+      if (parent[t] >= 0) cidx[fill[parent[t]]++] = t;
+  }
+  // per front: its separator rows' positions and its children's update sets,
+  // later than its own separator, sorted and distinct
+  std::vector<int64_t> mark(n, -1), cand;
+  std::vector<int64_t> store;  // all sets, concatenated as in u_pos (which may be too small to read back)
+  u_ptr[0] = 0;
+  for (int64_t t = 0; t < n_fronts; ++t) {
+    const int64_t last = s_first[t] + s_size[t] - 1;
+    cand.clear();
+    for (int64_t e = p_ptr[s_first[t]]; e < p_ptr[s_first[t] + s_size[t]]; ++e) {
+      const int64_t q = p_pos[e];
+      DDX_REQUIRE(q >= 0 && q < n, "ddx_nd_update_sets: position %lld out of range", (long long)q);
+      if (q > last && mark[q] != t) {
+        mark[q] = t;
+        cand.push_back(q);
+      }
+    }
+    for (int64_t k = cptr[t]; k < cptr[t + 1]; ++k) {
+      const int64_t c = cidx[k];
+      for (int64_t i = u_ptr[c]; i < u_ptr[c + 1]; ++i) {
+        const int64_t q = store[i];
+        if (q > last && mark[q] != t) {
+          mark[q] = t;
+          cand.push_back(q);
+        }
+      }
+    }
+    std::sort(cand.begin(), cand.end());
+    store.insert(store.end(), cand.begin(), cand.end());
+    u_ptr[t + 1] = (int64_t)store.size();
+  }
+  const int64_t total = (int64_t)store.size();
+  *u_total = total;
+  DDX_REQUIRE(total <= capacity, "ddx_nd_update_sets: %lld update entries exceed the capacity %lld",
+              (long long)total, (long long)capacity);
+  std::copy(store.begin(), store.end(), u_pos);
+  return DDX_OK;
+}
+
 int ddx_coarse_solve_nd(const ddx_nd_plan* P, int R, const double* w, double* x, double* y, double* xe,
                         double* upd, double* fb, const int* ist, ddx_stream_t stream) {
   DDX_REQUIRE(P && w && x && y && xe && upd && R >= 1, "ddx_coarse_solve_nd: bad arguments");

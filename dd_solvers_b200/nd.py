@@ -118,6 +118,29 @@ def nested_dissection(indptr: np.ndarray, indices: np.ndarray, n: int, leaf: int
     return S, parent[:nf].copy()
 
 
+def _update_sets(n: int, s_first, s_size, p_ptr, p_pos, parent):
+    """Update sets of the separator tree (``ddx_nd_update_sets``): CSR
+    ``(u_ptr, u_pos)`` of elimination positions, front by front: the
+    positions after the front's separator that its rows or its children's
+    update sets reach, sorted and distinct."""
+    a = [np.ascontiguousarray(x, dtype=np.int64) for x in (s_first, s_size, p_ptr, p_pos, parent)]
+    nf = len(a[1])
+    u_ptr = np.empty(nf + 1, dtype=np.int64)
+    total = np.zeros(1, dtype=np.int64)
+    cap = 2 * len(a[3]) + n
+    for _ in range(2):
+        u_pos = np.empty(max(cap, 1), dtype=np.int64)
+        try:
+            L.call("ddx_nd_update_sets", n, nf, *(x.ctypes.data for x in a), u_ptr.ctypes.data, u_pos.ctypes.data,
+                   cap, total.ctypes.data)
+            return u_ptr, u_pos[:int(total[0])]
+        except L.DDXError:
+            if int(total[0]) <= cap:
+                raise
+            cap = int(total[0])
+    raise RuntimeError("ddx_nd_update_sets: capacity")
+
+
 def _merge_top(S: list, parent: np.ndarray, limit: int):
     """Merge the top levels of the separator tree into one front while the
     merged separators hold at most ``limit`` vertices: whole levels, from the
@@ -180,22 +203,14 @@ class NDSymbolic:
         pos[perm] = np.arange(n)
         s_sizes = np.array([len(x) for x in S], dtype=np.int64)
         s_first = np.concatenate([[0], np.cumsum(s_sizes)[:-1]])
-        s_last = s_first + s_sizes - 1
-        # subtree_last = last position in the subtree = own S last (post-order)
         # the rows of A in elimination order: a front's separator rows are one slice
         deg = np.diff(indptr)[perm]
         p_ptr = np.zeros(n + 1, dtype=np.int64)
         np.cumsum(deg, out=p_ptr[1:])
         p_idx = indices[np.repeat(indptr[perm] - p_ptr[:-1], deg) + np.arange(int(p_ptr[-1]))] if n else indices
         p_pos = pos[p_idx]
-        U: list = [None] * nf
-        upos: list = [None] * nf
-        for t in range(nf):
-            a, b = p_ptr[s_first[t]], p_ptr[s_first[t] + s_sizes[t]]
-            cand = [p_pos[a:b]] + [upos[c] for c in children[t]]
-            c = np.unique(np.concatenate(cand))
-            upos[t] = c[c > s_last[t]]
-            U[t] = perm[upos[t]]
+        u_ptr, u_pos = _update_sets(n, s_first, s_sizes, p_ptr, p_pos, parent)
+        U = [perm[u_pos[u_ptr[t]:u_ptr[t + 1]]] for t in range(nf)]
         level = np.zeros(nf, dtype=np.int64)
         for t in range(nf):
             if children[t]:

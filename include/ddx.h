@@ -302,6 +302,21 @@ int ddx_coarse_gemv_f64(int n_c, int R, const double* Ainv, const double* w, dou
 int ddx_nd_order(int64_t n, const int64_t* indptr, const int64_t* indices, int leaf, int64_t* perm,
                  int64_t* node_first, int64_t* node_parent, int64_t* n_nodes);
 
+/* ddx_nd_update_sets (host memory, host computation): the symbolic update
+ * sets of the separator tree, the analysis step of the same cuDSS
+ * replacement. Positions are elimination-order positions (0 .. n-1); front t
+ * eliminates positions s_first[t] .. s_first[t]+s_size[t]-1, fronts in
+ * post-order (parent[t] > t, or -1). p_ptr/p_pos hold, for every position,
+ * the positions of its matrix row's entries (n+1 pointers). U_t = the
+ * positions after front t's separator that its rows or its children's update
+ * sets reach, sorted and distinct, written to u_pos[u_ptr[t] .. u_ptr[t+1])
+ * (u_ptr: n_fronts+1 entries). *u_total receives the total; if it exceeds
+ * capacity the call returns DDX_ERR_ARG and writes no u_pos (call again with
+ * capacity >= *u_total). */
+int ddx_nd_update_sets(int64_t n, int64_t n_fronts, const int64_t* s_first, const int64_t* s_size,
+                       const int64_t* p_ptr, const int64_t* p_pos, const int64_t* parent, int64_t* u_ptr,
+                       int64_t* u_pos, int64_t capacity, int64_t* u_total);
+
 /* Multifrontal solve plan. Front t owns the (s_t + u_t) coarse indices
  * fidx[idx_off[t] ...] (its separator, then its update set) and the operator
  * G[g_off[t] ...] = [chol(F_SS)^-1; F_US F_SS^-1] ((s_t+u_t) x s_t, row-major),

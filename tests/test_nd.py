@@ -207,3 +207,22 @@ def test_threaded_ordering_matches_single_threaded(monkeypatch):
         assert np.array_equal(perm, out[0][0])
         assert np.array_equal(sizes, out[0][1])
         assert np.array_equal(parent, out[0][2])
+
+
+def test_update_sets_native_contract():
+    """``ddx_nd_update_sets`` on a two-front tree (a 2 x 2 full matrix, one
+    vertex per front): U_0 = {1}, U_1 = {}; a capacity below the total is
+    refused with the total reported, then the call succeeds."""
+    from dd_solvers_b200 import _lib as L
+
+    i64 = lambda *v: np.array(v, dtype=np.int64)  # noqa: E731
+    s_first, s_size, p_ptr, p_pos, parent = i64(0, 1), i64(1, 1), i64(0, 2, 4), i64(0, 1, 0, 1), i64(1, -1)
+    u_ptr = np.zeros(3, dtype=np.int64)
+    u_pos = np.zeros(1, dtype=np.int64)
+    total = np.zeros(1, dtype=np.int64)
+    args = [x.ctypes.data for x in (s_first, s_size, p_ptr, p_pos, parent, u_ptr, u_pos)]
+    with pytest.raises(L.DDXError):
+        L.call("ddx_nd_update_sets", 2, 2, *args, 0, total.ctypes.data)
+    assert total[0] == 1
+    L.call("ddx_nd_update_sets", 2, 2, *args, 1, total.ctypes.data)
+    assert list(u_ptr) == [0, 1, 1] and list(u_pos) == [1]
