@@ -6,9 +6,12 @@
   reference's FP64 iteration counts and solutions (tests/golden/c1r.npz),
 * overlapping / uneven / Q1-coarse / multi-RHS / low-precision cases against the
   FP64 oracle restatement.
-Bar: FP64 path equal iteration counts (+-1) and 1e-10 relative solution
-agreement at equal counts; mixed precision: relative error <= 1e-8 against a
-direct FP64 solve at rtol 1e-10.
+Bar: FP64 path equal iteration counts (+-1), and 1e-10 relative solution
+agreement at equal counts. The equal-count comparison always runs: the solver is
+run for exactly the reference's iteration count K (rtol = atol = 0, maxiter = K,
+the iterate returned through ``x0``), which is the reference's converged
+iterate (its loop stops on the norm test after K updates). Mixed precision:
+relative error <= 1e-8 against a direct FP64 solve at rtol 1e-10.
 """
 import numpy as np
 import pytest
@@ -19,6 +22,29 @@ from conftest import golden
 from helpers import p1_case, q1_case, torch_csr
 
 pytestmark = pytest.mark.gpu
+
+
+def fixed_iterate(cg, b, K):
+    """x_K: exactly K PCG iterations from x0 = 0 (rtol = atol = 0, maxiter = K).
+
+    The run ends in ``ConvergenceNotAchieved`` as the reference's does
+    (solvers.py:294-295); the iterate comes back in ``x0``, which the solve
+    updates in place like the reference's.
+    """
+    import dd_solvers_b200 as dd
+
+    saved = (cg.rtol, cg.atol, cg.maxiter)
+    cg.rtol, cg.atol, cg.maxiter = 0.0, 0.0, int(K)
+    x0 = torch.zeros_like(b)
+    try:
+        cg.solve(b, x0=x0)
+    except dd.ConvergenceNotAchieved as e:
+        assert e.metadata["iterations"] == K - 1
+    else:
+        raise AssertionError("a run with rtol = atol = 0 must end in ConvergenceNotAchieved")
+    finally:
+        cg.rtol, cg.atol, cg.maxiter = saved
+    return x0
 
 
 def _ref_setup(cuda, g, problem_dtype=torch.float64):
@@ -53,6 +79,10 @@ def test_fixture24_matches_reference(cuda, rhs_name, case):
     if meta["iterations"] == ref_it:
         tol = 1e-10 if "inv32" not in case else 1e-6
         assert np.linalg.norm(x.cpu().numpy() - xr) <= tol * np.linalg.norm(xr)
+    # equal iteration counts, unconditionally: the reference's iterate x_K
+    xk = fixed_iterate(cg, b, ref_it).cpu().numpy()
+    tol = 1e-10 if "inv32" not in case else 1e-6
+    assert np.linalg.norm(xk - xr) <= tol * np.linalg.norm(xr), np.linalg.norm(xk - xr) / np.linalg.norm(xr)
     # reference's own pin (test_solvers.py:176)
     inv_perm = dd.inverse_permutation(perm)
     Ad = A.to_dense()
@@ -145,19 +175,25 @@ def test_config1r_matches_reference(cuda, kind, layout):
         Ap = dd.permute_csr_tensor(torch_csr(A, cuda), torch.as_tensor(inv, device=cuda))
         cg.setup(Ap, dofs_per_solver=289, solvers_per_coarse=torch.ones(nparts, dtype=torch.int64, device=cuda),
                  block_size=1)
-        x, meta = cg.solve(torch.as_tensor(b[perm], device=cuda))
+        bt = torch.as_tensor(b[perm], device=cuda)
+        x, meta = cg.solve(bt)
         x = x.cpu().numpy()
+        xk = fixed_iterate(cg, bt, int(g[kind + "__iters"])).cpu().numpy()
     else:
         # natural ordering with index-set subdomains (overlap 0) and P0 owners: same operator
         sub_ptr, sub_idx = partition.overlapping_subdomains(A, owner, nparts, 0)
         cg.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), owner=owner, block_size=1)
-        xn, meta = cg.solve(torch.as_tensor(b, device=cuda))
+        bt = torch.as_tensor(b, device=cuda)
+        xn, meta = cg.solve(bt)
         x = xn.cpu().numpy()[perm]
+        xk = fixed_iterate(cg, bt, int(g[kind + "__iters"])).cpu().numpy()[perm]
     ref_it = int(g[kind + "__iters"])
     assert abs(meta["iterations"] - ref_it) <= 1
     xr = g[kind + "__x"]
     if meta["iterations"] == ref_it:
         assert np.linalg.norm(x - xr) <= 1e-10 * np.linalg.norm(xr)
+    # equal iteration counts, unconditionally
+    assert np.linalg.norm(xk - xr) <= 1e-10 * np.linalg.norm(xr), np.linalg.norm(xk - xr) / np.linalg.norm(xr)
     ref_norms = g[kind + "__norms"]
     k = min(len(ref_norms), len(meta["residual norms"])) - 1
     assert np.allclose(meta["residual norms"][:k], ref_norms[:k], rtol=1e-7)
@@ -180,7 +216,8 @@ def test_overlapping_fp64_matches_oracle(cuda, case, kind):
     cls = dd.AdditiveSchwarz if kind == "additive" else dd.HybridSchwarz
     cg = dd.CG(cls(torch.float64, dd.Inv(), dd.CUDSS()), rtol=1e-8)
     cg.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0, block_size=1)
-    x, meta = cg.solve(torch.as_tensor(b, device=cuda))
+    bt = torch.as_tensor(b, device=cuda)
+    x, meta = cg.solve(bt)
     if kind == "additive":
         xr, om = orc.pcg(A, b, M.additive, rtol=1e-8)
     else:
@@ -188,6 +225,9 @@ def test_overlapping_fp64_matches_oracle(cuda, case, kind):
     assert abs(meta["iterations"] - om["iterations"]) <= 1
     if meta["iterations"] == om["iterations"]:
         assert np.linalg.norm(x.cpu().numpy() - xr) <= 1e-10 * np.linalg.norm(xr)
+    # equal iteration counts, unconditionally: the oracle's converged iterate x_K
+    xk = fixed_iterate(cg, bt, om["iterations"]).cpu().numpy()
+    assert np.linalg.norm(xk - xr) <= 1e-10 * np.linalg.norm(xr), np.linalg.norm(xk - xr) / np.linalg.norm(xr)
 
 
 @pytest.mark.parametrize("prec", [torch.float32, torch.bfloat16, torch.float16])
