@@ -49,6 +49,7 @@ _SIGS = {
     "ddx_schwarz_local_apply_sym": (_I, [_I, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _I, _I, _P]),
     "ddx_schwarz_local_apply_tc_sym": (_I, [_I, _I, _P, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _P]),
     "ddx_schwarz_local_apply_tc": (_I, [_I, _I, _P, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _P]),
+    "ddx_schwarz_local_apply_tc_sym_ex": (_I, [_I, _I, _P, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _P, _P, _I, _P]),
     "ddx_dot_noalloc": (_I, [_I64, _I, _P, _P, _P, _P]),
     "ddx_pack_panels16": (_I, [_I, _I, _P, _P, _P, _P, _P, _P, _I, _I, _P]),
     "ddx_schwarz_combine": (_I, [_I64, _I, _P, _P, _P, _I, _P, _P, _P, _P, _P, _D, _P, _I, _P, _P, _P, _P,

@@ -437,52 +437,88 @@ __device__ __forceinline__ uint64_t sw128_mn_desc(uint32_t saddr, uint32_t lbo) 
 __host__ __device__ constexpr uint32_t idesc_f16_amn(int ab_fmt, int N) { return idesc_f16(ab_fmt, N) | (1u << 15); }
 
 constexpr int kSymTile = 128;
-constexpr int kMaxRowTiles = 32;  // ceil(kmax / 128) * N <= 512 TMEM columns with N >= 16
 constexpr int kSymTileBytes = kSymTile * kSymTile * 2;  // 32 KB
 constexpr int kHalfBytes = kSymTileBytes / 2;           // 16 KB
+constexpr int kSymMaxStages = 6;
+// Shared memory after the panels, never addressed by an operand descriptor
+// (a margin between the last panel byte and the end of the allocation).
+constexpr int kSymSlack = 1024;
 
+// Row tiles (128 rows) of the largest block: all their accumulators live in
+// TMEM at once (nt x N of the 512 columns); at most 24, so the barriers and
+// the per-RHS scales fit in the 1 KB control area.
+template <int N>
+__host__ __device__ constexpr int sym_max_row_tiles() { return 512 / N < 24 ? 512 / N : 24; }
+
+// Control area at the start of the (1024-byte aligned) dynamic shared memory:
+// a_full/a_empty per ring stage, p_full/p_empty per 128-row panel chunk,
+// acc_full/acc_empty per row-tile accumulator, the TMEM address, the abort flag
+// and the per-RHS unscale factors.
+template <int N>
+struct SymCtl {
+  static constexpr int MT = sym_max_row_tiles<N>();
+  uint64_t a_full[kSymMaxStages], a_empty[kSymMaxStages];
+  uint64_t p_full[MT], p_empty[MT];
+  uint64_t acc_full[MT], acc_empty[MT];
+  uint32_t tmem_slot;
+  int abort_flag;
+  float rhs_unscale[N];
+};
+static_assert(sizeof(SymCtl<16>) <= 1024 && sizeof(SymCtl<32>) <= 1024 && sizeof(SymCtl<64>) <= 1024,
+              "control area exceeds 1 KB");
+
+// Dynamic shared memory of the symmetric kernel: alignment margin, control
+// area, STAGES tiles of 32 KB, TERMS B panels of the largest block, slack.
+__host__ __device__ inline size_t sym_smem_bytes(int stages, int terms, int kmax, int N) {
+  return 1024 + 1024 + (size_t)stages * kSymTileBytes + (size_t)terms * panel_chunks(kmax) * N * 128 + kSymSlack;
+}
+
+// Per block (k rows, nt = ceil(k / 128) row tiles):
+//   producer  loads panel chunk J (rows 128 J .. 128 J + 127 of every residual
+//             term) just before tile (0, J), then the remaining tiles in
+//             row-major order of (I, J), I <= J, through the STAGES-deep ring;
+//   MMA       row I = 0 waits for each chunk J as its tile (0, J) comes up, so
+//             the first MMA needs only chunk 0; after row I, chunk I is read
+//             by no later row and is released (p_empty[I]) for the next
+//             block, whose panel therefore streams in while this block's
+//             last rows multiply;
+//   epilogue  drains D_I once row I is complete.
 template <typename T, int N, int TERMS, int STAGES>
 __global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
+  constexpr int MT = sym_max_row_tiles<N>();
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  unsigned char* ring = smem;                                   // STAGES x 32 KB
-  unsigned char* bbuf = smem + (size_t)STAGES * kSymTileBytes;  // TERMS x panel
+  SymCtl<N>& ctl = *reinterpret_cast<SymCtl<N>*>(smem);
+  unsigned char* ring = smem + 1024;                            // STAGES x 32 KB
+  unsigned char* bbuf = ring + (size_t)STAGES * kSymTileBytes;  // TERMS x panel
   const int nt_max = (a.kmax + kSymTile - 1) / kSymTile;
   const uint32_t panel_bytes = (uint32_t)panel_chunks(a.kmax) * N * 128;  // nt_max x 128 rows
-  uint64_t* bars = reinterpret_cast<uint64_t*>(bbuf + (size_t)TERMS * panel_bytes + kPanelSlack);
-  uint64_t* a_full = bars;
-  uint64_t* a_empty = bars + STAGES;
-  uint64_t* b_full = bars + 2 * STAGES;
-  uint64_t* b_empty = b_full + 1;
-  uint64_t* acc_full = b_full + 2;                     // [kMaxRowTiles]: D_m complete
-  uint64_t* acc_empty = acc_full + kMaxRowTiles;      // [kMaxRowTiles]: D_m drained
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(acc_empty + kMaxRowTiles);
-  __shared__ int abort_flag_s;
-  volatile int& abort_flag = abort_flag_s;
-  __shared__ float rhs_unscale[64];
+  constexpr uint32_t chunk_bytes = (uint32_t)kK * 2u * N;                  // 64 panel rows
+  constexpr uint32_t chunk128 = 2u * chunk_bytes;                          // 128 panel rows
+  volatile int& abort_flag = ctl.abort_flag;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (a.ist != nullptr && n_active(a.ist, N) == 0) return;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&a_full[s], 1);
-      mbar_init(&a_empty[s], 1);
+      mbar_init(&ctl.a_full[s], 1);
+      mbar_init(&ctl.a_empty[s], 1);
     }
-    mbar_init(b_full, 1);
-    mbar_init(b_empty, 1);
-    for (int m = 0; m < kMaxRowTiles; ++m) {
-      mbar_init(&acc_full[m], 1);
-      mbar_init(&acc_empty[m], kEpiThreads / 32);
+    for (int m = 0; m < MT; ++m) {
+      mbar_init(&ctl.p_full[m], 1);
+      mbar_init(&ctl.p_empty[m], 1);
+      mbar_init(&ctl.acc_full[m], 1);
+      mbar_init(&ctl.acc_empty[m], kEpiThreads / 32);
     }
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (threadIdx.x < N) rhs_unscale[threadIdx.x] = 1.0f / rhs_scale<T>(a.st, N, threadIdx.x);
+  if (threadIdx.x < N) ctl.rhs_unscale[threadIdx.x] = 1.0f / rhs_scale<T>(a.st, N, threadIdx.x);
   uint32_t cols = 32;
   while (cols < (uint32_t)(nt_max * N)) cols <<= 1;  // power of two >= 32, <= 512 (checked at launch)
   if (warp == 1) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&ctl.tmem_slot)),
                  "r"(cols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
@@ -490,33 +526,37 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
   fence_before();
   __syncthreads();
   fence_after();
-  const uint32_t tmem = *tmem_slot;
+  const uint32_t tmem = ctl.tmem_slot;
 
   if (warp == 0) {
     // ------------------------------ producer ------------------------------
     if (lane == 0) {
-      uint32_t g = 0, sub_n = 0;
+      uint32_t g = 0;
+      uint32_t pu = 0;  // bit c: parity of the loads into panel chunk c so far
       for (int w = blockIdx.x; w < a.n_sub && !abort_flag; w += gridDim.x) {
         const int i = a.order[w];
         const int k = (int)(a.sub_ptr[i + 1] - a.sub_ptr[i]);
         if (k == 0 || k > a.kmax) continue;
-        const int nKp = panel_chunks(k);  // all nt x 128 panel rows (zero beyond k)
+        const int nKp = panel_chunks(k);  // 64-row chunks per term in HBM (whole 128-row pairs, zero beyond k)
         const int nt = (k + kSymTile - 1) / kSymTile;
-        if (!mbar_wait(b_empty, (sub_n & 1u) ^ 1u)) { abort_flag = 1; break; }
-        ++sub_n;
-        constexpr uint32_t chunk_bytes = (uint32_t)kK * 2u * N;
-        const unsigned char* psrc = a.b16 + a.panel_off[i];
-        mbar_expect_tx(b_full, (uint32_t)TERMS * (uint32_t)nKp * chunk_bytes);
-        for (int tt = 0; tt < TERMS; ++tt)
-          for (int t = 0; t < nKp; ++t, psrc += chunk_bytes)
-            bulk_g2s(bbuf + (size_t)tt * panel_bytes + (size_t)t * chunk_bytes, psrc, chunk_bytes, b_full);
+        const unsigned char* pbase = a.b16 + a.panel_off[i];
         const unsigned char* src = a.tiles + a.tile_off[i];
         const int ntiles = nt * (nt + 1) / 2;
         for (int t = 0; t < ntiles; ++t, ++g) {
+          if (t < nt) {
+            // panel chunk J = t, needed from tile (0, J) on
+            if (!mbar_wait(&ctl.p_empty[t], ((pu >> t) & 1u) ^ 1u)) { abort_flag = 1; break; }
+            pu ^= 1u << t;
+            mbar_expect_tx(&ctl.p_full[t], (uint32_t)TERMS * chunk128);
+#pragma unroll
+            for (int tt = 0; tt < TERMS; ++tt)
+              bulk_g2s(bbuf + (size_t)tt * panel_bytes + (size_t)t * chunk128,
+                       pbase + ((size_t)tt * nKp * chunk_bytes + (size_t)t * chunk128), chunk128, &ctl.p_full[t]);
+          }
           const int s = g % STAGES;
-          if (!mbar_wait(&a_empty[s], ((g / STAGES) & 1u) ^ 1u)) { abort_flag = 1; break; }
-          mbar_expect_tx(&a_full[s], (uint32_t)kSymTileBytes);
-          bulk_g2s(ring + (size_t)s * kSymTileBytes, src, (uint32_t)kSymTileBytes, &a_full[s]);
+          if (!mbar_wait(&ctl.a_empty[s], ((g / STAGES) & 1u) ^ 1u)) { abort_flag = 1; break; }
+          mbar_expect_tx(&ctl.a_full[s], (uint32_t)kSymTileBytes);
+          bulk_g2s(ring + (size_t)s * kSymTileBytes, src, (uint32_t)kSymTileBytes, &ctl.a_full[s]);
           src += kSymTileBytes;
         }
       }
@@ -527,28 +567,31 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
       constexpr int fmt = std::is_same<T, __nv_bfloat16>::value ? 1 : 0;
       constexpr uint32_t idesc_k = idesc_f16(fmt, N);
       constexpr uint32_t idesc_mn = idesc_f16_amn(fmt, N);
-      uint32_t g = 0, sub_n = 0;
+      uint32_t g = 0;
       uint32_t ph = 0;  // bit m: parity of the completed uses of accumulator D_m
+      uint32_t pm = 0;  // bit c: parity of the completed loads of panel chunk c
       for (int w = blockIdx.x; w < a.n_sub && !abort_flag; w += gridDim.x) {
         const int i = a.order[w];
         const int k = (int)(a.sub_ptr[i + 1] - a.sub_ptr[i]);
         if (k == 0 || k > a.kmax) continue;
         const int nt = (k + kSymTile - 1) / kSymTile;
-        if (!mbar_wait(b_full, sub_n & 1u)) { abort_flag = 1; break; }
-        fence_after();
         uint64_t touched = 0;  // row tiles whose accumulator already holds a partial sum
         // before the first MMA into D_m in this block, the epilogue must have
         // drained D_m of the previous block
         auto claim = [&](int m) -> bool {
           if ((touched >> m) & 1u) return true;
-          if (!mbar_wait(&acc_empty[m], ((ph >> m) & 1u) ^ 1u)) return false;
+          if (!mbar_wait(&ctl.acc_empty[m], ((ph >> m) & 1u) ^ 1u)) return false;
           fence_after();
           return true;
         };
         for (int I = 0; I < nt && !abort_flag; ++I) {
           for (int J = I; J < nt; ++J, ++g) {
             const int s = g % STAGES;
-            if (!mbar_wait(&a_full[s], (g / STAGES) & 1u)) { abort_flag = 1; break; }
+            if (!mbar_wait(&ctl.a_full[s], (g / STAGES) & 1u)) { abort_flag = 1; break; }
+            if (I == 0) {
+              if (!mbar_wait(&ctl.p_full[J], (pm >> J) & 1u)) { abort_flag = 1; break; }
+              pm ^= 1u << J;
+            }
             if (!claim(I) || (I != J && !claim(J))) { abort_flag = 1; break; }
             fence_after();
             const uint32_t sa = smem_u32(ring + (size_t)s * kSymTileBytes);
@@ -584,16 +627,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
               }
               touched |= 1ull << J;
             }
-            mma_commit(&a_empty[s]);
+            mma_commit(&ctl.a_empty[s]);
           }
+          if (abort_flag) break;
           // D_I is complete once row I is done: its other contributions (T^T X of
-          // tiles (I', I), I' < I) came from earlier rows
-          if (!abort_flag) mma_commit(&acc_full[I]);
+          // tiles (I', I), I' < I) came from earlier rows; panel chunk I is read
+          // by no later row
+          mma_commit(&ctl.acc_full[I]);
+          mma_commit(&ctl.p_empty[I]);
         }
         if (abort_flag) break;
-        mma_commit(b_empty);
         ph ^= (nt >= 32) ? 0xffffffffu : ((1u << nt) - 1u);
-        ++sub_n;
       }
     }
   } else {
@@ -614,7 +658,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
       const float sc = a.scale ? a.scale[i] : 1.0f;
       for (int m = 0; m < nt; ++m) {
         // drain D_m as soon as its row is done, while later rows still multiply
-        if (!mbar_wait(&acc_full[m], (ph >> m) & 1u)) { abort_flag = 1; break; }
+        if (!mbar_wait(&ctl.acc_full[m], (ph >> m) & 1u)) { abort_flag = 1; break; }
         fence_after();
         float v[N];
 #pragma unroll
@@ -624,12 +668,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
           float4* dst = reinterpret_cast<float4*>(a.ylocal + (p0 + row) * N);
 #pragma unroll
           for (int c = 0; c < N; c += 4)
-            dst[c / 4] = make_float4(sc * rhs_unscale[c] * v[c], sc * rhs_unscale[c + 1] * v[c + 1],
-                                     sc * rhs_unscale[c + 2] * v[c + 2], sc * rhs_unscale[c + 3] * v[c + 3]);
+            dst[c / 4] = make_float4(sc * ctl.rhs_unscale[c] * v[c], sc * ctl.rhs_unscale[c + 1] * v[c + 1],
+                                     sc * ctl.rhs_unscale[c + 2] * v[c + 2], sc * ctl.rhs_unscale[c + 3] * v[c + 3]);
         }
         fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&acc_empty[m]);
+        if (lane == 0) mbar_arrive(&ctl.acc_empty[m]);
       }
       if (abort_flag) break;
       ph ^= (nt >= 32) ? 0xffffffffu : ((1u << nt) - 1u);
@@ -643,34 +687,53 @@ __global__ void __launch_bounds__(kThreads, 1) k_apply_tc_sym(Args a) {
   }
 }
 
+template <typename T, int N, int TERMS, int STAGES>
+static void launch_sym_stages(const Args& a, cudaStream_t s, size_t smem, int grid) {
+  auto kern = k_apply_tc_sym<T, N, TERMS, STAGES>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  kern<<<grid, kThreads, smem, s>>>(a);
+}
+
+// Ring depth of the symmetric kernel: the deepest ring (2..6 stages of 32 KB)
+// that fits next to the B panels of the largest block; 0 if none does.
+inline int sym_stages(int terms, int kmax, int N) {
+  for (int st = kSymMaxStages; st >= 2; --st)
+    if (sym_smem_bytes(st, terms, kmax, N) <= 227 * 1024) return st;
+  return 0;
+}
+
 template <typename T, int N, int TERMS>
-static int launch_sym(const Args& a, cudaStream_t s) {
-  const int nk_max = panel_chunks(a.kmax);
+static int launch_sym(const Args& a, cudaStream_t s, int stages_req) {
+  constexpr int MT = sym_max_row_tiles<N>();
   const int nt_max = (a.kmax + kSymTile - 1) / kSymTile;
-  if (nt_max * N > 512) {
-    set_error("ddx_schwarz_local_apply_tc_sym: %d row tiles x R=%d accumulators exceed 512 TMEM columns", nt_max, N);
+  if (nt_max > MT) {
+    set_error("ddx_schwarz_local_apply_tc_sym: %d row tiles of 128 with R=%d exceed the %d accumulators in TMEM",
+              nt_max, N, MT);
     return DDX_ERR_UNSUPPORTED;
   }
-  const size_t fixed = 1024 + (size_t)TERMS * nk_max * N * 128 + kPanelSlack + (2 * 3 + 2 + 2 * kMaxRowTiles) * 8 + 64;
+  const int max_st = sym_stages(TERMS, a.kmax, N);
+  if (max_st == 0) {
+    set_error("ddx_schwarz_local_apply_tc_sym: k=%d with R=%d and %d residual terms needs %zu bytes of shared memory",
+              a.kmax, N, TERMS, sym_smem_bytes(2, TERMS, a.kmax, N));
+    return DDX_ERR_UNSUPPORTED;
+  }
+  const int stages = stages_req > 0 ? std::min(stages_req, max_st) : max_st;
+  if (stages < 2) {
+    set_error("ddx_schwarz_local_apply_tc_sym: %d ring stages requested (at least 2)", stages_req);
+    return DDX_ERR_ARG;
+  }
   // at least 120 KB of shared memory keeps one CTA per SM (its accumulators may take all 512 TMEM columns)
-  const size_t smem3 = std::max<size_t>(fixed + 3 * (size_t)kSymTileBytes, 120 * 1024);
-  const size_t smem2 = std::max<size_t>(fixed + 2 * (size_t)kSymTileBytes, 120 * 1024);
+  const size_t smem = std::max<size_t>(sym_smem_bytes(stages, TERMS, a.kmax, N), 120 * 1024);
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   const int grid = std::max(1, std::min(a.n_sub, nsm));
-  if (smem3 <= 227 * 1024) {
-    auto kern = k_apply_tc_sym<T, N, TERMS, 3>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
-    kern<<<grid, kThreads, smem3, s>>>(a);
-  } else if (smem2 <= 227 * 1024) {
-    auto kern = k_apply_tc_sym<T, N, TERMS, 2>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
-    kern<<<grid, kThreads, smem2, s>>>(a);
-  } else {
-    set_error("ddx_schwarz_local_apply_tc_sym: k=%d with R=%d and %d residual terms needs %zu bytes of shared memory",
-              a.kmax, N, TERMS, smem2);
-    return DDX_ERR_UNSUPPORTED;
+  switch (stages) {
+    case 2: launch_sym_stages<T, N, TERMS, 2>(a, s, smem, grid); break;
+    case 3: launch_sym_stages<T, N, TERMS, 3>(a, s, smem, grid); break;
+    case 4: launch_sym_stages<T, N, TERMS, 4>(a, s, smem, grid); break;
+    case 5: launch_sym_stages<T, N, TERMS, 5>(a, s, smem, grid); break;
+    default: launch_sym_stages<T, N, TERMS, 6>(a, s, smem, grid); break;
   }
   DDX_LAUNCH_CHECK("ddx_schwarz_local_apply_tc_sym");
   return DDX_OK;
@@ -712,10 +775,10 @@ extern "C" int ddx_schwarz_local_apply_tc(int n_sub, int R, const int64_t* sub_p
 }
 
 template <typename T, int TERMS>
-static int launch_sym_r(int R, const umma::Args& a, cudaStream_t s) {
-  if (R == 16) return umma::launch_sym<T, 16, TERMS>(a, s);
-  if (R == 32) return umma::launch_sym<T, 32, TERMS>(a, s);
-  return umma::launch_sym<T, 64, TERMS>(a, s);
+static int launch_sym_r(int R, const umma::Args& a, cudaStream_t s, int stages) {
+  if (R == 16) return umma::launch_sym<T, 16, TERMS>(a, s, stages);
+  if (R == 32) return umma::launch_sym<T, 32, TERMS>(a, s, stages);
+  return umma::launch_sym<T, 64, TERMS>(a, s, stages);
 }
 
 extern "C" int ddx_schwarz_local_apply_tc_sym(int n_sub, int R, const int64_t* sub_ptr, const int* order,
@@ -723,6 +786,17 @@ extern "C" int ddx_schwarz_local_apply_tc_sym(int n_sub, int R, const int64_t* s
                                               const float* scale, int kmax, const void* b16,
                                               const int64_t* panel_off, int terms, float* ylocal, const int* ist,
                                               const double* st, ddx_stream_t stream) {
+  return ddx_schwarz_local_apply_tc_sym_ex(n_sub, R, sub_ptr, order, tile_off, tiles, block_dtype, scale, kmax, b16,
+                                           panel_off, terms, ylocal, ist, st, 0, stream);
+}
+
+extern "C" int ddx_schwarz_local_apply_tc_sym_ex(int n_sub, int R, const int64_t* sub_ptr, const int* order,
+                                                 const int64_t* tile_off, const void* tiles, int block_dtype,
+                                                 const float* scale, int kmax, const void* b16,
+                                                 const int64_t* panel_off, int terms, float* ylocal, const int* ist,
+                                                 const double* st, int stages, ddx_stream_t stream) {
+  DDX_REQUIRE(stages == 0 || (stages >= 2 && stages <= 6),
+              "ddx_schwarz_local_apply_tc_sym: stages must be 0 or 2..6 (got %d)", stages);
   DDX_REQUIRE(R == 16 || R == 32 || R == 64, "ddx_schwarz_local_apply_tc_sym: R must be 16, 32 or 64 (got %d)", R);
   DDX_REQUIRE(terms == 1 || terms == 2, "ddx_schwarz_local_apply_tc_sym: terms must be 1 or 2 (got %d)", terms);
   DDX_REQUIRE(n_sub >= 0 && kmax >= 0, "ddx_schwarz_local_apply_tc_sym: bad sizes");
@@ -735,9 +809,9 @@ extern "C" int ddx_schwarz_local_apply_tc_sym(int n_sub, int R, const int64_t* s
                (const unsigned char*)b16, panel_off, ylocal, ist, st, kmax};
   cudaStream_t s = (cudaStream_t)stream;
   if (block_dtype == DDX_BF16)
-    return terms == 1 ? launch_sym_r<__nv_bfloat16, 1>(R, a, s) : launch_sym_r<__nv_bfloat16, 2>(R, a, s);
+    return terms == 1 ? launch_sym_r<__nv_bfloat16, 1>(R, a, s, stages) : launch_sym_r<__nv_bfloat16, 2>(R, a, s, stages);
   if (block_dtype == DDX_F16)
-    return terms == 1 ? launch_sym_r<__half, 1>(R, a, s) : launch_sym_r<__half, 2>(R, a, s);
+    return terms == 1 ? launch_sym_r<__half, 1>(R, a, s, stages) : launch_sym_r<__half, 2>(R, a, s, stages);
   set_error("ddx_schwarz_local_apply_tc_sym: block dtype must be BF16 or F16");
   return DDX_ERR_ARG;
 }

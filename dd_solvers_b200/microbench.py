@@ -66,8 +66,13 @@ def bench_apply(args) -> dict:
     pc.rhs_terms = args.terms
     pc.tc_symmetric = not args.tc_full
     pc.autotune = args.tune
+    pc.tc_stages = args.stages or None
     tune = None
-    if args.tune:
+    tc = pc._tc_ok(R) and pc.use_tensor_cores
+    if args.tune and tc:
+        pc.tune_tc(R)
+        tune = {f"sym={sym},stages={st}": ms for (sym, st), ms in pc.tune_tc_timings[R].items()}
+    elif args.tune:
         pc.tune(R)
         tune = {f"groups={g},stage_kb={kb}": ms for (g, kb), ms in pc.tune_timings.items()}
     r = torch.randn(A.shape[0] * R, dtype=torch.float64, device=dev)
@@ -75,8 +80,8 @@ def bench_apply(args) -> dict:
     ks = pc.ks.astype(np.int64)
     n = A.shape[0]
     acc = 8 if pc.acc_dtype == torch.float64 else 4
-    tc = pc._tc_ok(R) and pc.use_tensor_cores
-    tcsym = tc and pc._tc_sym_ok(R, pc._tc_terms(R))
+    tc_cfg = pc._tc_config(R, pc._tc_terms(R)) if tc else (False, 0)
+    tcsym = tc and tc_cfg[0]
     if tc:
         blk_bytes = pc._tile_store(True).nbytes if tcsym else int((ks * ks).sum() * ELT[args.precision])
     else:
@@ -87,7 +92,8 @@ def bench_apply(args) -> dict:
     return {"kernel": kname, "precision": args.precision,
             "rhs": R, "rhs_terms": pc._tc_terms(R) if tc else None, "layout": pc.store.layout, "n_dofs": n, "subdomains": len(ks), "k_max": int(ks.max()), "ms_per_launch": ms,
             "algorithmic_bytes": nbytes, "achieved_gbs": nbytes / ms / 1e6, "frac_of_peak": nbytes / ms / 1e6 / _peak(),
-            "tflops": 2.0 * float((ks * ks).sum()) * R / ms / 1e9, "config": pc._apply_config(R), "tune_ms": tune}
+            "tflops": 2.0 * float((ks * ks).sum()) * R / ms / 1e9,
+            "config": ({"symmetric": tc_cfg[0], "stages": tc_cfg[1]} if tc else pc._apply_config(R)), "tune_ms": tune}
 
 
 def bench_spmv(args) -> dict:
@@ -192,6 +198,8 @@ def main():
     ap.add_argument("--terms", type=int, default=None, choices=[1, 2],
                     help="16-bit residual terms of the tensor-core apply (default: automatic)")
     ap.add_argument("--tune", action="store_true", help="run the autotuner first and report every candidate")
+    ap.add_argument("--stages", type=int, default=0, help="apply: ring depth of the symmetric tensor-core kernel "
+                                                          "(2..6; 0: deepest that fits)")
     args = ap.parse_args()
     out = {"apply": bench_apply, "spmv": bench_spmv, "bsr": bench_bsr, "solve": bench_solve}[args.what](args)
     print(json.dumps(out))

@@ -277,6 +277,9 @@ class SchwarzOperator(SparseSolver):
         # tensor-core apply on the upper-triangle 128 x 128 tiles when the
         # blocks are stored symmetric and the accumulators fit in TMEM
         self.tc_symmetric = True
+        # ring depth of the symmetric tensor-core kernel (None: autotuned, or
+        # the deepest ring that fits when autotuning is off)
+        self.tc_stages = None
         self.autotune = True
 
     # -- setup -------------------------------------------------------------
@@ -499,13 +502,24 @@ class SchwarzOperator(SparseSolver):
 
     def _tc_sym_ok(self, R: int, terms: int) -> bool:
         """Symmetric tensor-core kernel: upper-triangle blocks, every row-tile
-        accumulator of the largest block in TMEM (ceil(kmax/128) R <= 512) and
-        two 32 KB tile stages plus the B panels in shared memory."""
+        accumulator of the largest block in TMEM (nt = ceil(kmax/128) row tiles,
+        nt R <= 512, nt <= 24) and at least two 32 KB tile stages plus the B
+        panels in shared memory."""
         if not self.tc_symmetric or self.store.layout != "sym":
             return False
         nt = (self.kmax + 127) // 128
+        return nt * R <= 512 and nt <= 24 and self._tc_sym_max_stages(R, terms) >= 2
+
+    def _tc_sym_max_stages(self, R: int, terms: int) -> int:
+        """Deepest tile ring (2..6 stages of 32 KB) of the symmetric kernel that
+        fits in 227 KB next to the B panels (3 KB of alignment margin, control
+        area and slack); 0 if none does."""
+        nt = (self.kmax + 127) // 128
         panel = terms * 2 * nt * so.UMMA_K * R * 2
-        return nt * R <= 512 and 1024 + 2 * 32768 + panel + 2048 + 640 <= 227 * 1024
+        for st in range(6, 1, -1):
+            if 3 * 1024 + st * 32768 + panel <= 227 * 1024:
+                return st
+        return 0
 
     def _tc_terms(self, R: int) -> int:
         """Residual terms of the tensor-core path for R right-hand sides; 0 = not usable.
@@ -552,22 +566,87 @@ class SchwarzOperator(SparseSolver):
         s = self.scratch(R)
         terms = self._tc_terms(R) if self.use_tensor_cores else 0
         if terms:
-            sym = self._tc_sym_ok(R, terms)
-            t = self._tile_store(sym)
-            b16, panel_off = self._panels(R, terms)
-            code = L.DTYPE_CODE[self.block_dtype]
-            L.call("ddx_pack_panels16", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
-                   L.ptr(panel_off), L.ptr(r), L.ptr(st), L.ptr(b16), code, terms, L.stream_ptr())
-            L.call("ddx_schwarz_local_apply_tc_sym" if sym else "ddx_schwarz_local_apply_tc", self.n_solvers, R,
-                   L.ptr(self.sub_ptr), L.ptr(self.order), L.ptr(t.tile_off), L.ptr(t.data), code,
-                   L.ptr(self.store.scale), self.kmax, L.ptr(b16), L.ptr(panel_off), terms, L.ptr(s["ylocal"]),
-                   L.ptr(ist), L.ptr(st), L.stream_ptr())
+            sym, stages = self._tc_config(R, terms)
+            self._tc_apply(r, s["ylocal"], R, terms, sym, stages, ist, st)
             self._ymap = self._ymap_one  # one slice written
             return s["ylocal"]
         cfg = self._apply_config(R)
         self._simt_apply(r, s["ylocal"], R, ist, *cfg)
         self._ymap = self._ymap_parts if self.store.layout == "sym" else self._ymap_one
         return s["ylocal"]
+
+    def _tc_apply(self, r, ylocal, R, terms, sym, stages, ist=None, st=None) -> None:
+        """Pack the 16-bit B panels of r, then the tensor-core local apply
+        (upper-triangle tiles with a ``stages``-deep ring when ``sym``, else
+        full-block tiles)."""
+        t = self._tile_store(sym)
+        b16, panel_off = self._panels(R, terms)
+        code = L.DTYPE_CODE[self.block_dtype]
+        L.call("ddx_pack_panels16", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
+               L.ptr(panel_off), L.ptr(r), L.ptr(st), L.ptr(b16), code, terms, L.stream_ptr())
+        args = (self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.order), L.ptr(t.tile_off), L.ptr(t.data), code,
+                L.ptr(self.store.scale), self.kmax, L.ptr(b16), L.ptr(panel_off), terms, L.ptr(ylocal),
+                L.ptr(ist), L.ptr(st))
+        if sym:
+            L.call("ddx_schwarz_local_apply_tc_sym_ex", *args, int(stages), L.stream_ptr())
+        else:
+            L.call("ddx_schwarz_local_apply_tc", *args, L.stream_ptr())
+
+    def _tc_candidates(self, R: int, terms: int) -> list[tuple[bool, int]]:
+        """(symmetric tiles, ring stages) the tensor-core autotuner times: every
+        ring depth of the symmetric kernel that fits, and the full-block kernel."""
+        cands = []
+        if self._tc_sym_ok(R, terms):
+            cands += [(True, st) for st in range(self._tc_sym_max_stages(R, terms), 1, -1)]
+        cands.append((False, 0))
+        return cands
+
+    def _tc_config(self, R: int, terms: int) -> tuple[bool, int]:
+        """Tuned (symmetric, stages) for R right-hand sides; tunes on first eager
+        use, else the default: symmetric tiles with the deepest ring when they fit."""
+        default = (True, int(self.tc_stages or 0)) if self._tc_sym_ok(R, terms) else (False, 0)
+        if not self.autotune or self.tc_stages:
+            return default
+        cfg = SchwarzOperator._tuned.get(self._tc_tune_key(R, terms))
+        if cfg is not None:
+            return cfg
+        if torch.cuda.is_current_stream_capturing():
+            return default
+        return self.tune_tc(R)
+
+    def _tc_tune_key(self, R: int, terms: int):
+        return self._tune_key() + ("tc", R, terms, bool(self.tc_symmetric))
+
+    def tune_tc(self, R: int, reps: int = 3) -> tuple[bool, int]:
+        """Project autotuner for the tensor-core path: times the panel pack plus
+        the apply for every (symmetric / full tiles, ring depth) candidate on this
+        operator's own blocks (CUDA events, one warm-up launch each) and keeps the
+        fastest for R right-hand sides; cached per (precision, layout, sizes, R)."""
+        terms = self._tc_terms(R)
+        assert terms, "the tensor-core path needs BF16/FP16 blocks and R in {16, 32, 64}"
+        s = self.scratch(R)
+        r = torch.randn(self.n * R, dtype=torch.float64, device=self.device)
+        best, best_ms, timings = None, float("inf"), {}
+        for sym, st in self._tc_candidates(R, terms):
+            try:
+                self._tc_apply(r, s["ylocal"], R, terms, sym, st)
+            except L.DDXError:
+                continue  # e.g. this block size does not fit the candidate's shared memory
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
+                self._tc_apply(r, s["ylocal"], R, terms, sym, st)
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            timings[(sym, st)] = ms
+            if ms < best_ms:
+                best, best_ms = (sym, st), ms
+        assert best is not None, "no tensor-core candidate ran"
+        SchwarzOperator._tuned[self._tc_tune_key(R, terms)] = best
+        self.tune_tc_timings = getattr(self, "tune_tc_timings", {})
+        self.tune_tc_timings[R] = timings
+        return best
 
     def _local_sum(self, r: torch.Tensor, R: int) -> torch.Tensor:
         """Local products ``y_i = s_i Q_i r[idx_i]`` stacked subdomain-major as a

@@ -232,6 +232,36 @@ int ddx_schwarz_local_apply_tc(int n_sub, int R, const int64_t* sub_ptr, const i
                                const float* scale, int kmax, const void* b16, const int64_t* panel_off,
                                int terms, float* ylocal, const int* ist, const double* st,
                                ddx_stream_t stream);
+/* Tensor-core apply for symmetric blocks stored as upper-triangle 128 x 128
+ * tiles: tiles (I, J), I <= J, of Q_i in row-major order of (I, J) from byte
+ * tile_off[i] (16-byte aligned), each as two 128 x 64 halves (tile
+ * columns 0-63, then 64-127) in the K-major 128-byte-swizzled layout of
+ * ddx_schwarz_local_apply_tc, zero beyond k_i: 32 KB per tile, about 56% of
+ * the full block at k ~ 2000. Each tile is multiplied twice: D_I += T X_J and,
+ * for I < J, D_J += T^T X_I (the same shared memory read as an MN-major
+ * operand). The B panel of a block arrives in 128-row chunks, each with its
+ * own barrier: the first MMA waits for chunk 0 only, and chunk I is released
+ * for the next block once tile row I is done. Needs nt = ceil(kmax / 128) row
+ * tiles with nt * R <= 512 and nt <= 24 (all row-tile accumulators of a block
+ * in TMEM) and 3 KB + S * 32 KB + terms * 2 nt * 64 * 2R bytes of shared
+ * memory (<= 227 KB) for a ring of S >= 2 tile stages; the deepest ring that
+ * fits (at most 6) is used. Other arguments as ddx_schwarz_local_apply_tc.
+ * No counterpart in the reference (full inverse blocks,
+ * src/dd_solvers/dd_solvers/solvers.py:343-359). */
+int ddx_schwarz_local_apply_tc_sym(int n_sub, int R, const int64_t* sub_ptr, const int* order,
+                                   const int64_t* tile_off, const void* tiles, int block_dtype,
+                                   const float* scale, int kmax, const void* b16, const int64_t* panel_off,
+                                   int terms, float* ylocal, const int* ist, const double* st,
+                                   ddx_stream_t stream);
+/* ddx_schwarz_local_apply_tc_sym with the ring depth chosen by the caller
+ * (stages in 2..6, clamped to the deepest ring that fits; 0 = deepest), for an
+ * autotuner. Same results for every depth (the summation order does not
+ * depend on it). No counterpart in the reference. */
+int ddx_schwarz_local_apply_tc_sym_ex(int n_sub, int R, const int64_t* sub_ptr, const int* order,
+                                      const int64_t* tile_off, const void* tiles, int block_dtype,
+                                      const float* scale, int kmax, const void* b16, const int64_t* panel_off,
+                                      int terms, float* ylocal, const int* ist, const double* st, int stages,
+                                      ddx_stream_t stream);
 /* Gathers and packs the tensor-core B panels X_i = r[idx_i, :] (r FP64, (n, R),
  * R in {16, 32, 64}) to 16-bit dtype (BF16 or F16). Subdomain i (k_i DOFs,
  * P_i = 2 ceil(k_i / 128) chunks of 64 rows) occupies terms * P_i * 64 * 2R
@@ -244,23 +274,6 @@ int ddx_schwarz_local_apply_tc(int n_sub, int R, const int64_t* sub_ptr, const i
  * 2^14 for F16 and 1 for BF16, so residual entries stay in the normal 16-bit
  * range as the solve converges; the tensor-core apply divides s_j out again.
  * Rows k_i..64 P_i - 1 are not written: zero them once. */
-/* Tensor-core apply for symmetric blocks stored as upper-triangle 128 x 128
- * tiles: tiles (I, J), I <= J, of Q_i in row-major order of (I, J) from byte
- * tile_off[i] (16-byte aligned), each as two 128 x 64 halves (tile
- * columns 0-63, then 64-127) in the K-major 128-byte-swizzled layout of
- * ddx_schwarz_local_apply_tc, zero beyond k_i: 32 KB per tile, about 56% of
- * the full block at k ~ 2000. Each tile is multiplied twice: D_I += T X_J and,
- * for I < J, D_J += T^T X_I (the same shared memory read as an MN-major
- * operand). Needs ceil(kmax / 128) * R <= 512 (all row-tile accumulators of a
- * block in TMEM) and 66-98 KB + terms * 2 ceil(kmax / 128) * 64 * 2R bytes of
- * shared memory (<= 227 KB). Other arguments as ddx_schwarz_local_apply_tc.
- * No counterpart in the reference (full inverse blocks,
- * src/dd_solvers/dd_solvers/solvers.py:343-359). */
-int ddx_schwarz_local_apply_tc_sym(int n_sub, int R, const int64_t* sub_ptr, const int* order,
-                                   const int64_t* tile_off, const void* tiles, int block_dtype,
-                                   const float* scale, int kmax, const void* b16, const int64_t* panel_off,
-                                   int terms, float* ylocal, const int* ist, const double* st,
-                                   ddx_stream_t stream);
 int ddx_pack_panels16(int n_sub, int R, const int64_t* sub_ptr, const int* sub_idx,
                       const int64_t* panel_off, const double* r, const double* st, void* b16,
                       int dtype, int terms, ddx_stream_t stream);

@@ -35,6 +35,7 @@ def test_tc_local_apply_matches_oracle(cuda, prec, R, case, terms, variant):
     pc.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0)
     pc.rhs_terms = terms
     pc.tc_symmetric = variant == "sym"
+    pc.autotune = False  # the variant under test, not the tuner's choice
     if not pc._tc_ok(R):
         pytest.skip("subdomains too large for the shared-memory B panels at this R")
     if variant == "sym" and not pc._tc_sym_ok(R, terms):
@@ -145,6 +146,7 @@ def test_tc_symmetric_equals_full_blocks(cuda):
     P, A, owner, nparts, sub_ptr, sub_idx, R0 = p1_case(100, 8)
     pc = dd.HybridSchwarz(torch.float64, dd.Inv(torch.float16), dd.CUDSS())
     pc.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0)
+    pc.autotune = False
     assert pc._tc_sym_ok(16, 1) and int(pc.ks.max()) % 128 != 0
     r = torch.randn(A.shape[0], 16, dtype=torch.float64, device=cuda)
     ys = pc._local(r.view(-1), 16).clone()
@@ -155,3 +157,52 @@ def test_tc_symmetric_equals_full_blocks(cuda):
     from dd_solvers_b200 import _lib
 
     assert _lib.device_error() == 0
+
+
+@pytest.mark.parametrize("prec,terms", [("bf16", 1), ("bf16", 2), ("f16", 1)])
+@pytest.mark.parametrize("R", [16, 32, 64])
+def test_tc_every_tuning_candidate(cuda, prec, terms, R):
+    """Every (symmetric / full tiles, ring depth) the tensor-core autotuner may
+    pick, on uneven RCB subdomains (k not a multiple of 128, several row tiles)
+    and on a 3D Q1 case (blocks of up to 1000 DOFs: 8 row tiles, all 512 TMEM
+    columns at R = 64): each against the oracle, and the symmetric kernel bitwise
+    equal for every ring depth (the depth changes no summation order)."""
+    import dd_solvers_b200 as dd
+    from dd_solvers_b200 import _lib
+    from oracle import restatement as orc
+
+    for case in ("p1", "q1_3d"):
+        if case == "p1":
+            P, A, owner, nparts, sub_ptr, sub_idx, R0 = p1_case(100, 8)
+        else:
+            P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(3, 32, 4, kappa_seed=3)
+        pc = dd.AdditiveSchwarz(torch.float64, dd.Inv(DT[prec]), None)
+        pc.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx))
+        pc.rhs_terms = terms
+        if not pc._tc_ok(R):
+            continue
+        cands = pc._tc_candidates(R, terms)
+        rng = np.random.default_rng(R + terms)
+        r = rng.standard_normal((A.shape[0], R))
+        rt = torch.as_tensor(r, device=cuda).contiguous().view(-1)
+        rq = orc.rhs_terms(r, prec, terms)
+        s = pc.scratch(R)
+        sym_out = None
+        for sym, st in cands:
+            s["ylocal"].zero_()
+            pc._tc_apply(rt, s["ylocal"], R, terms, sym, st)
+            y = s["ylocal"][: int(sub_ptr[-1]) * R].view(-1, R).double().cpu().numpy()
+            for i in range(pc.n_solvers):
+                idx = sub_idx[sub_ptr[i]:sub_ptr[i + 1]]
+                ref = pc.store.block(i).cpu().numpy() @ rq[idx]
+                got = y[sub_ptr[i]:sub_ptr[i + 1]]
+                err = np.linalg.norm(got - ref) / max(np.linalg.norm(ref), 1e-300)
+                assert err <= 1e-5, (case, sym, st, i, err)
+            if sym:
+                if sym_out is None:
+                    sym_out = y.copy()
+                else:
+                    assert np.array_equal(y, sym_out), (case, st)
+        assert _lib.device_error() == 0
+        best = pc.tune_tc(R)
+        assert best in cands
