@@ -2,8 +2,10 @@
 (src/dd_solvers/dd_solvers/bsr.py:15-25, 237-244).
 
 The reference registers several numba kernels; here every backend name maps to
-the sm_100a ``ddx_spmv_bsr`` kernel (one warp per block row, coalesced reads of
-the row's column-major blocks, shuffle reduction per output row).
+the sm_100a ``ddx_spmv_bsr`` kernel: one scalar row per lane, floor(32 / bs)
+block rows per warp, so the bs lanes of a block row read each column of the
+column-major blocks as consecutive values and x is a broadcast; no cross-lane
+reduction.
 """
 from __future__ import annotations
 

@@ -585,10 +585,10 @@ int nd_order_threads() {
 
 using namespace ddx;
 
-extern "C" {
+namespace {
 
-int ddx_nd_order(int64_t n, const int64_t* indptr, const int64_t* indices, int leaf, int64_t* perm,
-                 int64_t* node_first, int64_t* node_parent, int64_t* n_nodes) {
+int nd_order_impl(int64_t n, const int64_t* indptr, const int64_t* indices, int leaf, int64_t* perm,
+                  int64_t* node_first, int64_t* node_parent, int64_t* n_nodes) {
   DDX_REQUIRE(n >= 0 && indptr && indices && perm && node_first && node_parent && n_nodes && leaf >= 1,
               "ddx_nd_order: bad arguments");
   NdOrder o;
@@ -658,12 +658,21 @@ int ddx_nd_order(int64_t n, const int64_t* indptr, const int64_t* indices, int l
   return DDX_OK;
 }
 
-int ddx_nd_update_sets(int64_t n, int64_t n_fronts, const int64_t* s_first, const int64_t* s_size,
-                       const int64_t* p_ptr, const int64_t* p_pos, const int64_t* parent, int64_t* u_ptr,
-                       int64_t* u_pos, int64_t capacity, int64_t* u_total) {
+int nd_update_sets_impl(int64_t n, int64_t n_fronts, const int64_t* s_first, const int64_t* s_size,
+                        const int64_t* p_ptr, const int64_t* p_pos, const int64_t* parent, int64_t* u_ptr,
+                        int64_t* u_pos, int64_t capacity, int64_t* u_total) {
   DDX_REQUIRE(n >= 0 && n_fronts >= 0 && s_first && s_size && p_ptr && p_pos && parent && u_ptr && u_total &&
                   (capacity == 0 || u_pos),
               "ddx_nd_update_sets: bad arguments");
+  // every front's separator range lies in [0, n), and p_ptr does not decrease over it
+  for (int64_t t = 0; t < n_fronts; ++t) {
+    DDX_REQUIRE(s_first[t] >= 0 && s_size[t] >= 0 && s_first[t] + s_size[t] <= n,
+                "ddx_nd_update_sets: front %lld covers rows [%lld, %lld) outside [0, %lld)", (long long)t,
+                (long long)s_first[t], (long long)(s_first[t] + s_size[t]), (long long)n);
+    DDX_REQUIRE(p_ptr[s_first[t]] >= 0, "ddx_nd_update_sets: negative p_ptr at row %lld", (long long)s_first[t]);
+    for (int64_t i = s_first[t]; i < s_first[t] + s_size[t]; ++i)
+      DDX_REQUIRE(p_ptr[i] <= p_ptr[i + 1], "ddx_nd_update_sets: p_ptr decreases at row %lld", (long long)i);
+  }
   // children of each front, in front order (a front's children precede it)
   std::vector<int64_t> cptr(n_fronts + 1, 0), cidx;
   for (int64_t t = 0; t < n_fronts; ++t) {
@@ -713,6 +722,33 @@ int ddx_nd_update_sets(int64_t n, int64_t n_fronts, const int64_t* s_first, cons
               (long long)total, (long long)capacity);
   std::copy(store.begin(), store.end(), u_pos);
   return DDX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Host entry points: a failed allocation (or any other exception) in the host
+// code comes back as a status code instead of crossing the C boundary.
+int ddx_nd_order(int64_t n, const int64_t* indptr, const int64_t* indices, int leaf, int64_t* perm,
+                 int64_t* node_first, int64_t* node_parent, int64_t* n_nodes) {
+  try {
+    return nd_order_impl(n, indptr, indices, leaf, perm, node_first, node_parent, n_nodes);
+  } catch (const std::exception& ex) {
+    ::ddx::set_error("ddx_nd_order: %s", ex.what());
+    return DDX_ERR_ARG;
+  }
+}
+
+int ddx_nd_update_sets(int64_t n, int64_t n_fronts, const int64_t* s_first, const int64_t* s_size,
+                       const int64_t* p_ptr, const int64_t* p_pos, const int64_t* parent, int64_t* u_ptr,
+                       int64_t* u_pos, int64_t capacity, int64_t* u_total) {
+  try {
+    return nd_update_sets_impl(n, n_fronts, s_first, s_size, p_ptr, p_pos, parent, u_ptr, u_pos, capacity, u_total);
+  } catch (const std::exception& ex) {
+    ::ddx::set_error("ddx_nd_update_sets: %s", ex.what());
+    return DDX_ERR_ARG;
+  }
 }
 
 int ddx_coarse_solve_nd(const ddx_nd_plan* P, int R, const double* w, double* x, double* y, double* xe,

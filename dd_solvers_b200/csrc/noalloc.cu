@@ -2,10 +2,9 @@
 //
 // ddx_pcg_dots_rz needs two caller-allocated scratch buffers (per-CTA partial
 // sums and an arrival ticket). Some callers cannot allocate device memory at
-// the point where they need a dot product: code that runs while a CUDA graph
-// is being captured (cudaMalloc is not allowed during capture), hosts that
-// reach this library through a plain C FFI with no device allocator of their
-// own, and real-time loops that must not touch the allocator after start-up.
+// the point where they need a dot product: hosts that reach this library
+// through a plain C FFI with no device allocator of their own, and real-time
+// loops that must not touch the allocator after start-up.
 // ddx_dot_noalloc gives them the same deterministic reduction with the scratch
 // in a fixed array inside this library instead.
 #include <atomic>
@@ -49,7 +48,9 @@ __global__ void __launch_bounds__(kThreads) k_dot_noalloc(int64_t n, int R, cons
 }
 
 // Device address of the scratch array for the current device, looked up once
-// per device (cudaGetSymbolAddress with that device current).
+// per device (cudaGetSymbolAddress with that device current) and kept for the
+// process: a cudaDeviceReset unloads the module, after which the process must
+// restart before calling ddx_dot_noalloc again.
 int scratch_for_current_device(DotScratch** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);

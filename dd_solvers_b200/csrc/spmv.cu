@@ -301,9 +301,6 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// BSR with column-major (bs x bs) blocks; one warp per block row. Lane l walks
-// the row's stored values e = l, l+32, ...; entry e of the block row is block
-// e / bs^2, column (e % bs^2) / bs, row e % bs.
 // BSR SpMV, row per lane: a warp covers G = floor(32 / BS) block rows, lane
 // (g, r) computes scalar row r of block row g:
 //   y[br BS + r] = sum_{blk in row br} sum_c vals[blk][c][r] * x[cols[blk] BS + c]

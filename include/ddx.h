@@ -90,14 +90,17 @@ int ddx_pcg_dots_rz(int64_t n, int R, const double* r, const double* z, const do
 /* out[j] = x_j . y_j for R right-hand sides in (n, R) layout, with the same
  * deterministic two-stage reduction as ddx_pcg_dots_rz, but without any
  * caller-provided scratch: for callers that cannot allocate device memory
- * when they need the product (during CUDA graph capture, through a C FFI with
- * no device allocator, in loops that must not allocate after start-up).
+ * when they need the product (through a C FFI with no device allocator, in
+ * loops that must not allocate after start-up).
  * No counterpart in the reference. The scratch lives in a fixed array inside
  * the library (~296 KiB, held by every GPU that loads it until exit), which
  * limits R to at most 64 (R a power of two); larger R is rejected with
  * DDX_ERR_ARG. The first call on a device looks the array up
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture. All calls share the array: calls that can run
+ * (cudaGetSymbolAddress) with that device current and keeps the address for
+ * the rest of the process; make that first call before any stream capture.
+ * A device reset (cudaDeviceReset) unloads the array, so after one the
+ * process must restart before calling this again. All calls share the array:
+ * calls that can run
  * at the same time on the GPU (other streams, other host threads) race and
  * must be serialised by the caller. Allocates nothing (no cudaMalloc or
  * cudaFree); it clears the array's ticket with cudaMemsetAsync on `stream`. */

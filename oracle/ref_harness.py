@@ -1,8 +1,9 @@
 """ORACLE (test infrastructure only): run the reference's own solver code on CPU.
 
 This loads ``src/dd_solvers/dd_solvers/solvers.py`` from a checkout of the
-reference (default ``/root/reference``; it exists only in the development
-container, never on the GPU machines) and runs its ``CG``, ``AdditiveSchwarz``,
+reference named by the environment variable ``DDX_REFERENCE_ROOT`` (required;
+the checkout is a development-time input, not part of this package) and runs
+its ``CG``, ``AdditiveSchwarz``,
 ``HybridSchwarz``, ``Inv``, ``asm_permutation``, ``permute_csr_tensor`` and
 ``inverse_permutation`` verbatim on CPU tensors. Only the pieces that need a
 GPU or an absent library are replaced by same-math CPU equivalents:
@@ -29,11 +30,13 @@ import os
 import sys
 import types
 
-REF_ROOT = os.environ.get("DDX_REFERENCE_ROOT", "/root/reference")
+REF_ROOT = os.environ.get("DDX_REFERENCE_ROOT")
 _SIM_MAX_ROWS = 2000
 
 
-def load(ref_root: str = REF_ROOT):
+def load(ref_root: str | None = REF_ROOT):
+    if not ref_root:
+        raise RuntimeError("set DDX_REFERENCE_ROOT to a checkout of the reference (mgr0dzicki/dd-solvers)")
     os.environ.setdefault("TORCHDYNAMO_DISABLE", "1")
     os.environ.setdefault("NUMBA_ENABLE_CUDASIM", "1")
     import numpy as np

@@ -1,7 +1,7 @@
 """Writes tests/golden/dg_experiments.json from the reference's published results.
 
-Run in a checkout that has the reference at $DDX_REFERENCE_ROOT (default
-/root/reference):  python tests/golden/make_dg_golden.py
+Run with DDX_REFERENCE_ROOT set to a checkout of the reference:
+    DDX_REFERENCE_ROOT=<reference checkout>  python tests/golden/make_dg_golden.py
 
 The reference logged every CG run of its DG-SIPG experiments, with the full
 residual history, in ``results/experiment_precisions.csv`` and
@@ -28,7 +28,9 @@ import os
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("DDX_REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("DDX_REFERENCE_ROOT")
+if not REF:
+    raise SystemExit("set DDX_REFERENCE_ROOT to a checkout of the reference (mgr0dzicki/dd-solvers)")
 
 csv.field_size_limit(sys.maxsize)
 

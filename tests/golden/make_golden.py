@@ -1,7 +1,7 @@
 """Writes the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a checkout that has the reference at $DDX_REFERENCE_ROOT (default
-/root/reference):  python tests/golden/make_golden.py
+Run with DDX_REFERENCE_ROOT set to a checkout of the reference:
+    DDX_REFERENCE_ROOT=<reference checkout>  python tests/golden/make_golden.py
 
 * fixture24.npz  - the 24-DOF DG-SIPG system of the reference's solver test
                    (src/dd_solvers/tests/test_solvers.py:25-108) and the

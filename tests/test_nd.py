@@ -226,3 +226,69 @@ def test_update_sets_native_contract():
     assert total[0] == 1
     L.call("ddx_nd_update_sets", 2, 2, *args, 1, total.ctypes.data)
     assert list(u_ptr) == [0, 1, 1] and list(u_pos) == [1]
+
+
+def _update_sets_numpy(s_first, s_size, p_ptr, p_pos, parent):
+    """The update-set rule restated with numpy, front by front: the positions
+    after the front's separator reached by its rows or by its children's update
+    sets, sorted and distinct (np.unique)."""
+    nf = len(s_size)
+    sets = []
+    children = [[] for _ in range(nf)]
+    for t in range(nf):
+        if parent[t] >= 0:
+            children[parent[t]].append(t)
+    for t in range(nf):
+        last = s_first[t] + s_size[t] - 1
+        parts = [p_pos[p_ptr[s_first[t]]:p_ptr[s_first[t] + s_size[t]]]] + [sets[c] for c in children[t]]
+        u = np.unique(np.concatenate(parts)) if parts else np.zeros(0, dtype=np.int64)
+        sets.append(u[u > last])
+    u_ptr = np.concatenate([[0], np.cumsum([len(x) for x in sets])]).astype(np.int64)
+    u_pos = np.concatenate(sets) if sets else np.zeros(0, dtype=np.int64)
+    return u_ptr, u_pos
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("top_merge", [0, 64])
+def test_update_sets_native_equal_numpy(name, top_merge):
+    """``ddx_nd_update_sets`` returns exactly the numpy restatement's sets
+    (same pointers, same sorted positions) on every ordering case, with and
+    without the merged top front."""
+    A = CASES[name]()
+    A = sps.csr_matrix(A)
+    A.sort_indices()
+    n = A.shape[0]
+    S, parent = nd.nested_dissection(A.indptr, A.indices, n, 16)
+    S, parent = nd._merge_top(S, parent, top_merge)
+    perm = np.concatenate(S)
+    pos = np.empty(n, dtype=np.int64)
+    pos[perm] = np.arange(n)
+    s_size = np.array([len(x) for x in S], dtype=np.int64)
+    s_first = np.concatenate([[0], np.cumsum(s_size)[:-1]]).astype(np.int64)
+    indptr = A.indptr.astype(np.int64)
+    deg = np.diff(indptr)[perm]
+    p_ptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(deg, out=p_ptr[1:])
+    p_idx = A.indices.astype(np.int64)[np.repeat(indptr[perm] - p_ptr[:-1], deg) + np.arange(int(p_ptr[-1]))]
+    p_pos = pos[p_idx]
+    u_ptr, u_pos = nd._update_sets(n, s_first, s_size, p_ptr, p_pos, parent)
+    r_ptr, r_pos = _update_sets_numpy(s_first, s_size, p_ptr, p_pos, parent)
+    assert np.array_equal(u_ptr, r_ptr)
+    assert np.array_equal(u_pos, r_pos)
+
+
+def test_update_sets_rejects_bad_fronts():
+    """A front table whose separator range leaves [0, n), or a decreasing
+    p_ptr, is refused with a status (no out-of-range host reads)."""
+    from dd_solvers_b200 import _lib as L
+
+    i64 = lambda *v: np.array(v, dtype=np.int64)  # noqa: E731
+    p_ptr, p_pos, parent = i64(0, 2, 4), i64(0, 1, 0, 1), i64(1, -1)
+    u_ptr = np.zeros(3, dtype=np.int64)
+    u_pos = np.zeros(4, dtype=np.int64)
+    total = np.zeros(1, dtype=np.int64)
+    for s_first, s_size, pp in ((i64(0, 1), i64(1, 2), p_ptr), (i64(-1, 1), i64(1, 1), p_ptr),
+                                (i64(0, 1), i64(1, 1), i64(0, 3, 2))):
+        args = [x.ctypes.data for x in (s_first, s_size, pp, p_pos, parent, u_ptr, u_pos)]
+        with pytest.raises(L.DDXError):
+            L.call("ddx_nd_update_sets", 2, 2, *args, 4, total.ctypes.data)

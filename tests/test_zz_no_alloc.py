@@ -1,8 +1,8 @@
 """ddx_dot_noalloc: the dot-product entry point that needs no caller scratch.
 
 It exists for callers that cannot allocate device memory when they need a dot
-product (inside CUDA graph capture, behind a plain C FFI without a device
-allocator, or in loops that must not allocate after start-up). This test
+product (behind a plain C FFI without a device allocator, or in loops that must
+not allocate after start-up). This test
 calls it through the C ABI twice in a row and checks each result against the
 existing entry point, ddx_pcg_dots_rz (which takes caller-allocated scratch),
 on the same inputs. It is collected last so a failure here cannot hide
@@ -65,3 +65,26 @@ def test_dot_noalloc_rejects_too_many_rhs(cuda):
     out = torch.zeros(128, dtype=torch.float64, device=cuda)
     assert f(1, 128, x.data_ptr(), x.data_ptr(), out.data_ptr(), L.stream_ptr()) == 1
     assert b"R=128" in L.lib().ddx_last_error()
+
+
+def test_dot_noalloc_rejects_bad_arguments_and_allocates_nothing(cuda):
+    """A null pointer or n < 0 is refused with status 1; after a first call on
+    the device, further calls leave torch's allocator and the device's free
+    memory unchanged."""
+    from dd_solvers_b200 import _lib as L
+
+    f = _noalloc()
+    x = torch.ones(1000, dtype=torch.float64, device=cuda)
+    out = torch.zeros(1, dtype=torch.float64, device=cuda)
+    assert f(1000, 1, None, x.data_ptr(), out.data_ptr(), L.stream_ptr()) == 1
+    assert f(-1, 1, x.data_ptr(), x.data_ptr(), out.data_ptr(), L.stream_ptr()) == 1
+    assert f(1000, 1, x.data_ptr(), x.data_ptr(), out.data_ptr(), L.stream_ptr()) == 0
+    torch.cuda.synchronize()
+    alloc, reserved = torch.cuda.memory_allocated(cuda), torch.cuda.memory_reserved(cuda)
+    free0 = torch.cuda.mem_get_info(cuda)[0]
+    for _ in range(3):
+        assert f(1000, 1, x.data_ptr(), x.data_ptr(), out.data_ptr(), L.stream_ptr()) == 0
+    torch.cuda.synchronize()
+    assert float(out[0]) == 1000.0
+    assert torch.cuda.memory_allocated(cuda) == alloc and torch.cuda.memory_reserved(cuda) == reserved
+    assert abs(torch.cuda.mem_get_info(cuda)[0] - free0) <= 1 << 20
