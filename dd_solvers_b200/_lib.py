@@ -41,6 +41,7 @@ _SIGS = {
     "ddx_pcg_dots_rz": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ddx_spmv_sell_f64": (_I, [_I64, _I64, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P]),
     "ddx_spmv_csr_f64": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P]),
+    "ddx_spmv_csr_rowblock_mapped": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P]),
     "ddx_spmv_csr_rowblock_f64": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P]),
     "ddx_spmv_bsr": (_I, [_I64, _I, _P, _P, _P, _P, _P, _I, _P]),
     "ddx_gemv_strided_batched": (_I, [_I64, _I, _P, _I, _P, _P, _I, _P]),

@@ -257,6 +257,81 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// k_spmv_rowblock2 with x = the sum of the local products through the
+// transpose map, x[d, :] = sum_{t in [dof_ptr[d], dof_ptr[d+1])} ylocal[src[t], :]
+// (identity map when dof_ptr is null), each x value summed in FP64 in ascending
+// t from 0.0, as ddx_schwarz_combine sums it: the result equals
+// ddx_spmv_csr_rowblock_f64 applied to the materialised x, bit for bit, without
+// writing and re-reading that vector (the hybrid Schwarz restriction A_R y).
+template <typename ACC>
+__device__ __forceinline__ double2 ypair(const ACC* p);
+template <> __device__ __forceinline__ double2 ypair<double>(const double* p) {
+  return __ldg(reinterpret_cast<const double2*>(p));
+}
+template <> __device__ __forceinline__ double2 ypair<float>(const float* p) {
+  const float2 f = __ldg(reinterpret_cast<const float2*>(p));
+  return make_double2((double)f.x, (double)f.y);
+}
+
+template <typename ACC>
+__device__ __forceinline__ double2 mapped_x(int64_t d, int R, int c2, const int* __restrict__ dof_ptr,
+                                            const int* __restrict__ dof_src, const ACC* __restrict__ ylocal) {
+  double2 v = make_double2(0.0, 0.0);
+  if (dof_ptr == nullptr) {
+    const double2 y = ypair<ACC>(ylocal + d * R + 2 * c2);
+    v.x += y.x;
+    v.y += y.y;
+    return v;
+  }
+  const int t0 = __ldg(dof_ptr + d), t1 = __ldg(dof_ptr + d + 1);
+  for (int t = t0; t < t1; ++t) {
+    const double2 y = ypair<ACC>(ylocal + (int64_t)__ldg(dof_src + t) * R + 2 * c2);
+    v.x += y.x;
+    v.y += y.y;
+  }
+  return v;
+}
+
+template <typename ACC>
+__global__ void __launch_bounds__(kThreads)
+    k_spmv_rowblock2_mapped(int64_t n_rows, int R, const int* __restrict__ row_ptr, const int* __restrict__ cols,
+                            const double* __restrict__ vals, const int* __restrict__ dof_ptr,
+                            const int* __restrict__ dof_src, const ACC* __restrict__ ylocal, double* __restrict__ y) {
+  __shared__ double red[kThreads];
+  const int tpr = R / 2;
+  const int c2 = threadIdx.x % tpr;
+  const int G = blockDim.x / tpr;  // entries per step
+  const int e0 = threadIdx.x / tpr;
+  for (int64_t row = blockIdx.x; row < n_rows; row += gridDim.x) {
+    const int k0 = row_ptr[row], k1 = row_ptr[row + 1];
+    double2 s = make_double2(0.0, 0.0);
+    int k = k0 + e0;
+    for (; k + 3 * G < k1; k += 4 * G) {
+      const int cA = __ldg(cols + k), cB = __ldg(cols + k + G), cC = __ldg(cols + k + 2 * G),
+                cD = __ldg(cols + k + 3 * G);
+      const double vA = __ldg(vals + k), vB = __ldg(vals + k + G), vC = __ldg(vals + k + 2 * G),
+                   vD = __ldg(vals + k + 3 * G);
+      const double2 xA = mapped_x<ACC>(cA, R, c2, dof_ptr, dof_src, ylocal);
+      const double2 xB = mapped_x<ACC>(cB, R, c2, dof_ptr, dof_src, ylocal);
+      const double2 xC = mapped_x<ACC>(cC, R, c2, dof_ptr, dof_src, ylocal);
+      const double2 xD = mapped_x<ACC>(cD, R, c2, dof_ptr, dof_src, ylocal);
+      s.x = fma(vA, xA.x, s.x); s.y = fma(vA, xA.y, s.y);
+      s.x = fma(vB, xB.x, s.x); s.y = fma(vB, xB.y, s.y);
+      s.x = fma(vC, xC.x, s.x); s.y = fma(vC, xC.y, s.y);
+      s.x = fma(vD, xD.x, s.x); s.y = fma(vD, xD.y, s.y);
+    }
+    for (; k < k1; k += G) {
+      const double v = __ldg(vals + k);
+      const double2 xv = mapped_x<ACC>(__ldg(cols + k), R, c2, dof_ptr, dof_src, ylocal);
+      s.x = fma(v, xv.x, s.x);
+      s.y = fma(v, xv.y, s.y);
+    }
+    const double se = block_sum_by_col(s.x, red, tpr);
+    const double so = block_sum_by_col(s.y, red, tpr);
+    if (threadIdx.x < tpr) reinterpret_cast<double2*>(y + row * R)[threadIdx.x] = make_double2(se, so);
+  }
+}
+
 // One CTA per (long) row; threads stride over the row's entries.
 __global__ void __launch_bounds__(kThreads)
     k_spmv_rowblock(int64_t n_rows, int R, const int* __restrict__ row_ptr, const int* __restrict__ cols,
@@ -476,6 +551,29 @@ int ddx_spmv_csr_rowblock_f64(int64_t n_rows, int R, const int* row_ptr, const i
     k_spmv_rowblock<<<grid, kThreads, 0, (cudaStream_t)stream>>>(n_rows, R, row_ptr, cols, vals, x, y);
   }
   DDX_LAUNCH_CHECK("ddx_spmv_csr_rowblock_f64");
+  return DDX_OK;
+}
+
+int ddx_spmv_csr_rowblock_mapped(int64_t n_rows, int R, const int* row_ptr, const int* cols, const double* vals,
+                                 const int* dof_ptr, const int* dof_src, const void* ylocal, int acc_dtype,
+                                 double* y, ddx_stream_t stream) {
+  DDX_REQUIRE(R >= 2 && valid_rhs_count(R), "ddx_spmv_csr_rowblock_mapped: R must be 2, 4, ..., 64 (got %d)", R);
+  DDX_REQUIRE(n_rows >= 0 && row_ptr && cols && vals && ylocal && y, "ddx_spmv_csr_rowblock_mapped: bad arguments");
+  DDX_REQUIRE((dof_ptr == nullptr) == (dof_src == nullptr),
+              "ddx_spmv_csr_rowblock_mapped: dof_ptr and dof_src are given together");
+  DDX_REQUIRE(acc_dtype == DDX_F64 || acc_dtype == DDX_F32, "ddx_spmv_csr_rowblock_mapped: ylocal must be F64 or F32");
+  DDX_REQUIRE(((uintptr_t)y & 15u) == 0 && ((uintptr_t)ylocal & 15u) == 0,
+              "ddx_spmv_csr_rowblock_mapped: ylocal and y must be 16-byte aligned");
+  if (n_rows == 0) return DDX_OK;
+  const int grid = (int)std::min<int64_t>(n_rows, 148 * 8);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (acc_dtype == DDX_F64)
+    k_spmv_rowblock2_mapped<double><<<grid, kThreads, 0, s>>>(n_rows, R, row_ptr, cols, vals, dof_ptr, dof_src,
+                                                              (const double*)ylocal, y);
+  else
+    k_spmv_rowblock2_mapped<float><<<grid, kThreads, 0, s>>>(n_rows, R, row_ptr, cols, vals, dof_ptr, dof_src,
+                                                             (const float*)ylocal, y);
+  DDX_LAUNCH_CHECK("ddx_spmv_csr_rowblock_mapped");
   return DDX_OK;
 }
 

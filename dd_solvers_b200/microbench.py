@@ -106,6 +106,8 @@ def bench_spmv(args) -> dict:
     dev = torch.device("cuda")
     if args.problem == "p1":
         A = problems.p1_jittered(args.n_el, 0.3, 1.0, 0).matrix  # n_el = nodes per side
+    elif args.problem == "q1_2d":
+        A = problems.poisson2d(args.n_el).matrix
     else:
         A = problems.diffusion3d_lognormal(args.n_el, 0).matrix
     M = _SellMatrix(dd.csr_to_torch(A).to(dev))
@@ -115,9 +117,9 @@ def bench_spmv(args) -> dict:
     ms = _time(lambda: M.launch(x, y, R, L.SPMV_PLAIN), args.reps)
     n = A.shape[0]
     nbytes = A.nnz * 12 + (n + 1) * 4 + n * R * 16
-    return {"kernel": "ddx_spmv_sell_f64" if R == 1 else "ddx_spmv_csr_f64", "rhs": R, "n_dofs": n, "nnz": A.nnz,
-            "ms_per_launch": ms, "algorithmic_bytes": nbytes, "achieved_gbs": nbytes / ms / 1e6,
-            "frac_of_peak": nbytes / ms / 1e6 / _peak()}
+    return {"kernel": "ddx_spmv_sell_f64" if R == 1 else "ddx_spmv_csr_f64", "problem": args.problem, "rhs": R,
+            "n_dofs": n, "nnz": A.nnz, "ms_per_launch": ms, "algorithmic_bytes": nbytes,
+            "achieved_gbs": nbytes / ms / 1e6, "frac_of_peak": nbytes / ms / 1e6 / _peak()}
 
 
 def bench_bsr(args) -> dict:
@@ -187,7 +189,7 @@ def main():
     ap.add_argument("--p", type=int, default=1, help="bsr: DG polynomial degree")
     ap.add_argument("--dim", type=int, default=2, choices=[2, 3], help="bsr: triangles (2) or tetrahedra (3)")
     ap.add_argument("--n-el", type=int, default=64)
-    ap.add_argument("--problem", default="q1_3d", choices=["q1_3d", "p1"],
+    ap.add_argument("--problem", default="q1_3d", choices=["q1_3d", "p1", "q1_2d"],
                     help="spmv: 3D Q1 lognormal diffusion (n-el cells per side) or jittered P1 (n-el nodes per side)")
     ap.add_argument("--parts", type=int, default=8)
     ap.add_argument("--precision", default="bf16", choices=list(DT))

@@ -280,6 +280,9 @@ class SchwarzOperator(SparseSolver):
         # ring depth of the symmetric tensor-core kernel (None: autotuned, or
         # the deepest ring that fits when autotuning is off)
         self.tc_stages = None
+        # hybrid, R >= 2: the restriction reads y through the transpose map
+        # instead of a materialised y (same result, one vector pass fewer)
+        self.mapped_restriction = True
         self.autotune = True
 
     # -- setup -------------------------------------------------------------
@@ -891,6 +894,16 @@ class HybridSchwarz(SchwarzOperator):
             # the reference's layout: y is ylocal widened to FP64, read in place by
             # the restriction and the combine (same values, one pass fewer)
             self._restrict(*self._AR, ylocal[: self.n], s["w"], R)
+            self._coarse(s["w"], s["yc"], R, ist)
+            self._combine(z, R, ylocal=ylocal, prolong=True, sign=-1.0, pcg=pcg, r=r, q=q)
+            return
+        if R > 1 and self.mapped_restriction:
+            # y = sum of the local products, read through the transpose map by the
+            # restriction and by the combine (same sums, same bits): y is never written
+            dof_ptr, dof_src = self._ymap
+            rp, rc, rv = self._AR
+            L.call("ddx_spmv_csr_rowblock_mapped", rp.numel() - 1, R, L.ptr(rp), L.ptr(rc), L.ptr(rv), L.ptr(dof_ptr),
+                   L.ptr(dof_src), L.ptr(ylocal), L.DTYPE_CODE[self.acc_dtype], L.ptr(s["w"]), L.stream_ptr())
             self._coarse(s["w"], s["yc"], R, ist)
             self._combine(z, R, ylocal=ylocal, prolong=True, sign=-1.0, pcg=pcg, r=r, q=q)
             return

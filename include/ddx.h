@@ -136,6 +136,18 @@ int ddx_spmv_csr_rowblock_f64(int64_t n_rows, int R, const int* row_ptr, const i
  * length). */
 int ddx_spmv_csr_lanes_f64(int64_t n_rows, int lanes, const int* row_ptr, const int* cols, const double* vals,
                            const double* x, double* y, ddx_stream_t stream);
+/* ddx_spmv_csr_rowblock_f64 (R in {2, 4, ..., 64}) with x given as the sum of
+ * local products through the transpose map:
+ *   x[d, j] = sum_{t in [dof_ptr[d], dof_ptr[d+1])} ylocal[dof_src[t], j]
+ * (dof_ptr = dof_src = NULL: x = ylocal), ylocal F64 or F32 (acc_dtype), each
+ * x value summed in FP64 from 0.0 in ascending t, exactly as
+ * ddx_schwarz_combine sums it. The result equals the product with the
+ * materialised x bit for bit; the vector is never written. Replaces, for a
+ * block of right-hand sides, HybridSchwarz.solve's y = sum_i R_i^T y_i
+ * followed by A_R y (src/dd_solvers/dd_solvers/solvers.py:878-884). */
+int ddx_spmv_csr_rowblock_mapped(int64_t n_rows, int R, const int* row_ptr, const int* cols, const double* vals,
+                                 const int* dof_ptr, const int* dof_src, const void* ylocal, int acc_dtype,
+                                 double* y, ddx_stream_t stream);
 /* Same with x in x_dtype (DDX_F64 or DDX_F32, widened to FP64 on load): the
  * hybrid restriction A_R y reads the FP32 local products directly when the
  * subdomains are the reference's contiguous non-overlapping blocks. */

@@ -121,7 +121,10 @@ def block_scale(amax: float, dtype: str) -> float:
 
 
 def quantize(B: np.ndarray, dtype: str) -> tuple[float, np.ndarray]:
-    """Returns ``(s, Q)`` with ``Q = round(B / s)`` in ``dtype`` (as FP64 values)."""
+    """Returns ``(s, Q)`` with ``Q = round(B / s)`` in ``dtype`` (as FP64 values).
+    FP64 blocks are returned as they are (scale 1, no copy)."""
+    if dtype == "f64":
+        return 1.0, np.asarray(B, dtype=np.float64)
     s = block_scale(float(np.max(np.abs(B))) if B.size else 0.0, dtype)
     return s, round_to(B / s, dtype)
 

@@ -307,3 +307,4 @@ def test_device_partitioning_matches_host(parts):
             torch.as_tensor(P.matrix.indptr), torch.as_tensor(P.matrix.indices), torch.as_tensor(o_host), parts,
             overlap)
         assert np.array_equal(sp, sp_t.numpy()) and np.array_equal(si, si_t.numpy())
+
