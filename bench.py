@@ -610,6 +610,7 @@ def run_ours(args, spec, rank: int, world: int):
             },
             "rel_error_vs_fp64": errs[head],
             "iterations": its_head[-1],
+            "blocks_shifted_to_stay_spd": len(pcs[head].store.shifted),
             "fp64_plain_ms_per_rhs": f64_ms,
             "speedup_vs_fp64_plain": f64_ms / ms_head,
             "per_precision": per_prec,

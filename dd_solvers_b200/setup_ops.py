@@ -203,6 +203,10 @@ class BlockStore:
         self.blk_off = torch.as_tensor(off[:-1], device=device)
         self.scale = torch.ones(len(ks), dtype=torch.float32, device=device)
         self._sw = sym_tile_index(ELEM_BYTES[dtype], device) if layout == "sym" else None
+        # 16-bit symmetric blocks whose rounding made them indefinite are
+        # re-rounded with a diagonal shift (see _guard_spd); {block: shift}
+        self.spd_guard = True
+        self.shifted: dict[int, float] = {}
 
     @property
     def nbytes(self) -> int:
@@ -215,6 +219,8 @@ class BlockStore:
             inv = 0.5 * (inv + inv.transpose(1, 2))
         sc = block_scales(inv, self.dtype)
         q = quantize(inv, sc, self.dtype)
+        if self.spd_guard and self.dtype in (torch.bfloat16, torch.float16) and self.layout == "sym":
+            q, sc = self._guard_spd(first, inv, q, sc)
         self.scale[first:first + B] = sc
         if self.layout == "sym":
             for b in range(B):
@@ -257,6 +263,61 @@ class BlockStore:
                 dst = (offs[:, None] + cr[None, :]).reshape(-1)
                 src = qt[torch.as_tensor(part, device=q.device), :kk, :kk].reshape(-1)
                 self.data[dst] = src
+
+    def _guard_spd(self, first: int, inv: torch.Tensor, q: torch.Tensor, sc: torch.Tensor):
+        """Keeps every rounded 16-bit block positive definite.
+
+        The inverse of a very ill-conditioned local block (cond ~1e5-1e6, the
+        lognormal-coefficient outliers among thousands of subdomains) has its
+        smallest eigenvalues below the 16-bit rounding error of its entries:
+        rounding can make it indefinite, and PCG with an indefinite
+        preconditioner stalls. Each rounded block is tested with a Cholesky
+        factorisation of its dequantised FP64 form. A block that fails gets
+        ``sigma I`` added before rounding again, with the smallest sigma (from
+        twice the gap between half the block's smallest exact eigenvalue lam
+        and the rounded block's smallest eigenvalue, doubled as needed) whose
+        rounded block has all eigenvalues above lam / 2: the shift moves only
+        the few eigenvalues the rounding pushed below zero, and little more.
+        Blocks that pass, and blocks that are not positive definite before
+        rounding either, are unchanged.
+        """
+        B, kb = inv.shape[0], inv.shape[-1]
+        ks = torch.as_tensor(self.ks[first:first + B], device=inv.device)
+        pad = (torch.arange(kb, device=inv.device)[None, :] >= ks[:, None]).to(torch.float64)
+
+        def deq(qb, sb):
+            return qb.to(torch.float64) * sb.to(torch.float64)[..., None, None]
+
+        def spd(D, padb):
+            D.diagonal(dim1=-2, dim2=-1).add_(padb)  # D is a fresh dequantised copy
+            return torch.linalg.cholesky_ex(D)[1] == 0
+
+        ok = spd(deq(q, sc), pad)
+        bad = torch.nonzero(~ok).flatten().tolist()
+        dev = inv.device
+        for b in bad:
+            k = int(ks[b])
+            Bk = inv[b, :k, :k]
+            lam = float(torch.linalg.eigvalsh(Bk)[0])
+            if not lam > 0.0:
+                continue  # not positive definite before rounding either: nothing to keep
+            lam_q = float(torch.linalg.eigvalsh(deq(q[b, :k, :k], sc[b]))[0])
+            eye = torch.eye(k, dtype=torch.float64, device=dev)
+            sigma = 2.0 * (0.5 * lam - lam_q)
+            for _ in range(20):
+                Bs = Bk + sigma * eye
+                ss = block_scales(Bs[None], self.dtype)
+                qs = quantize(Bs[None], ss, self.dtype)[0]
+                if bool(spd(deq(qs, ss[0]) - 0.5 * lam * eye, torch.zeros(k, dtype=torch.float64, device=dev))):
+                    break
+                sigma *= 2.0
+            else:
+                raise RuntimeError(f"block {first + b}: no positive-definite {self.dtype} rounding found")
+            q[b] = 0
+            q[b, :k, :k] = qs
+            sc[b] = ss[0]
+            self.shifted[first + b] = sigma
+        return q, sc
 
     def dense_q(self, i: int) -> torch.Tensor:
         """Stored (quantised, unscaled) block i as a dense [row, col] k x k tensor."""

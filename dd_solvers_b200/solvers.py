@@ -280,9 +280,14 @@ class SchwarzOperator(SparseSolver):
         # ring depth of the symmetric tensor-core kernel (None: autotuned, or
         # the deepest ring that fits when autotuning is off)
         self.tc_stages = None
+        # 16-bit symmetric blocks made indefinite by their rounding are
+        # re-rounded with a diagonal shift (BlockStore._guard_spd)
+        self.spd_guard = True
         # hybrid, R >= 2: the restriction reads y through the transpose map
-        # instead of a materialised y (same result, one vector pass fewer)
-        self.mapped_restriction = True
+        # instead of a materialised y (same result, one vector pass fewer);
+        # None: measured per R on first use, True / False: forced
+        self.mapped_restriction = None
+        self._mapped_choice = {}
         self.autotune = True
 
     # -- setup -------------------------------------------------------------
@@ -380,6 +385,7 @@ class SchwarzOperator(SparseSolver):
         self.order = torch.as_tensor(np.argsort(-ks, kind="stable").astype(np.int32), device=dev)
         self.dof_ptr, self.dof_src = so.transpose_map(self.sub_idx, n)
         self.store = so.BlockStore(ks, block_dtype, dev, layout=self._layout(ks))
+        self.store.spd_guard = self.spd_guard
         kpad = so.round_up(max(self.kmax, 1), 16)
         # group subdomains of similar size to bound padding work
         order_np = np.argsort(ks, kind="stable")
@@ -434,7 +440,9 @@ class SchwarzOperator(SparseSolver):
         other.acc_dtype = self._acc_for(dtype)
         other._tiles = None
         other._scratch = {}
+        other._mapped_choice = {}
         store = so.BlockStore(self.ks, dtype, self.device, layout=self.store.layout)
+        store.spd_guard = self.spd_guard
         N = self.n_solvers
         i = 0
         while i < N:
@@ -897,13 +905,10 @@ class HybridSchwarz(SchwarzOperator):
             self._coarse(s["w"], s["yc"], R, ist)
             self._combine(z, R, ylocal=ylocal, prolong=True, sign=-1.0, pcg=pcg, r=r, q=q)
             return
-        if R > 1 and self.mapped_restriction:
+        if R > 1 and self._use_mapped(R, ylocal):
             # y = sum of the local products, read through the transpose map by the
             # restriction and by the combine (same sums, same bits): y is never written
-            dof_ptr, dof_src = self._ymap
-            rp, rc, rv = self._AR
-            L.call("ddx_spmv_csr_rowblock_mapped", rp.numel() - 1, R, L.ptr(rp), L.ptr(rc), L.ptr(rv), L.ptr(dof_ptr),
-                   L.ptr(dof_src), L.ptr(ylocal), L.DTYPE_CODE[self.acc_dtype], L.ptr(s["w"]), L.stream_ptr())
+            self._restrict_mapped(ylocal, s["w"], R)
             self._coarse(s["w"], s["yc"], R, ist)
             self._combine(z, R, ylocal=ylocal, prolong=True, sign=-1.0, pcg=pcg, r=r, q=q)
             return
@@ -912,6 +917,44 @@ class HybridSchwarz(SchwarzOperator):
         self._restrict(*self._AR, y, s["w"], R)
         self._coarse(s["w"], s["yc"], R, ist)
         self._combine(z, R, u=y, prolong=True, sign=-1.0, pcg=pcg, r=r, q=q)
+
+    def _restrict_mapped(self, ylocal, w, R):
+        dof_ptr, dof_src = self._ymap
+        rp, rc, rv = self._AR
+        L.call("ddx_spmv_csr_rowblock_mapped", rp.numel() - 1, R, L.ptr(rp), L.ptr(rc), L.ptr(rv), L.ptr(dof_ptr),
+               L.ptr(dof_src), L.ptr(ylocal), L.DTYPE_CODE[self.acc_dtype], L.ptr(w), L.stream_ptr())
+
+    def _use_mapped(self, R: int, ylocal) -> bool:
+        """Whether the restriction reads y through the transpose map (no y pass)
+        or y is written first: measured once per R on this operator (both give
+        the same bits). Reading through the map wins when few DOFs lie in several
+        subdomains and the restriction's rows are short (C3: 2.99 vs 3.05 ms per
+        iteration); with much overlap and long coarse rows (3D Q1 coarse) the
+        extra map and local-product reads cost more than the y pass."""
+        mode = self.mapped_restriction
+        if mode is not None:
+            return bool(mode)
+        key = ("mapped", R, self._ymap[0] is None, str(self.acc_dtype))
+        got = self._mapped_choice.get(key)
+        if got is None:
+            if torch.cuda.is_current_stream_capturing():
+                return False
+            s = self.scratch(R)
+
+            def timed(fn):
+                fn()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(3):
+                    fn()
+                e1.record()
+                torch.cuda.synchronize()
+                return e0.elapsed_time(e1)
+
+            t_map = timed(lambda: self._restrict_mapped(ylocal, s["w"], R))
+            t_mat = timed(lambda: (self._combine(s["y"], R, ylocal=ylocal), self._restrict(*self._AR, s["y"], s["w"], R)))
+            got = self._mapped_choice[key] = t_map < t_mat
+        return got
 
 
 # ---------------------------------------------------------------------------

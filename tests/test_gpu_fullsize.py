@@ -181,8 +181,13 @@ def _check_lowprec(cuda, F, pcq, prec, R):
 
     workload = F["name"]
     p = F["prob"]
-    # (a) the store: per-block scale and rounding of the oracle's inverse
-    for i in F["pick"]:
+    # (a) the store: per-block scale and rounding of the oracle's inverse; a
+    # block re-rounded with a diagonal shift (its plain rounding was indefinite)
+    # is checked to be positive definite instead
+    for i in sorted(set(F["pick"].tolist()) | set(list(pcq.store.shifted)[:4])):
+        if i in pcq.store.shifted:
+            assert float(torch.linalg.eigvalsh(pcq.store.block(int(i))).min()) > 0, (workload, prec, int(i))
+            continue
         Bo = _oracle_inverse(F, i)
         s_o = orc.block_scale(float(np.abs(Bo).max()), prec)
         s_g = float(pcq.store.scale[i])

@@ -308,3 +308,25 @@ def test_device_partitioning_matches_host(parts):
             overlap)
         assert np.array_equal(sp, sp_t.numpy()) and np.array_equal(si, si_t.numpy())
 
+
+
+def test_spd_guard_keeps_rounded_blocks_positive_definite():
+    """A block whose BF16 rounding is indefinite (inverse of cond ~1e6) is
+    re-rounded with a diagonal shift and comes out positive definite; a
+    well-conditioned block in the same batch is stored exactly as without the
+    guard (same bits, same scale)."""
+    rng = np.random.default_rng(0)
+    k = 256
+    Qm, _ = np.linalg.qr(rng.standard_normal((k, k)))
+    bad = (Qm * np.geomspace(1e-6, 1.0, k)) @ Qm.T         # eigenvalues 1e-6 .. 1
+    good = (Qm * np.geomspace(0.5, 1.0, k)) @ Qm.T
+    inv = torch.as_tensor(np.stack([bad, good]))
+    plain = so.BlockStore(np.array([k, k]), torch.bfloat16, "cpu", layout="sym")
+    plain.spd_guard = False
+    plain.put(0, inv.clone())
+    assert np.linalg.eigvalsh(plain.block(0).numpy()).min() < 0  # the case the guard is for
+    st = so.BlockStore(np.array([k, k]), torch.bfloat16, "cpu", layout="sym")
+    st.put(0, inv.clone())
+    assert list(st.shifted) == [0] and st.shifted[0] > 0
+    assert np.linalg.eigvalsh(st.block(0).numpy()).min() > 0
+    assert torch.equal(st.dense_q(1), plain.dense_q(1)) and float(st.scale[1]) == float(plain.scale[1])
