@@ -38,6 +38,7 @@ _SIGS = {
     "ddx_pcg_reset": (_I, [_I, _P, _P, _I, _I, _D, _D, _P]),
     "ddx_pcg_update_p": (_I, [_I64, _I, _P, _P, _P, _P, _P]),
     "ddx_pcg_update_xr": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "ddx_pcg_update_xr_pack16": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ddx_pcg_dots_rz": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ddx_spmv_sell_f64": (_I, [_I64, _I64, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P]),
     "ddx_spmv_csr_f64": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P]),

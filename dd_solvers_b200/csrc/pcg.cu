@@ -79,6 +79,69 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(int64_t n, PcgState S, d
   publish_nactive(S, act);
 }
 
+// k_update_xr for R in {16, 32, 64} right-hand sides that also writes the
+// tensor-core B panels of the next local apply (BF16, one residual term, scale
+// 1). Same layout as the multi-RHS SpMM: R/2 threads per DOF, each owning two
+// adjacent columns (16-byte loads, a warp reads whole rows), so x, p, r, q
+// stream exactly as in the plain update; each thread then stores its two
+// columns of r rounded to BF16 (4 bytes) into every panel row that holds the
+// DOF (pan_row[e] for e in [pan_ptr[d], pan_ptr[d+1]): the row's byte offset in
+// b16), in 16-byte chunk (c2 / 4) ^ ((offset >> 7) & mask), the panel's row
+// swizzle (mask 7 / 3 / 1 for R = 64 / 32 / 16): the threads of a DOF write
+// its panel row whole. The pack pass and its re-read of r through the subdomain
+// index maps disappear. rr = ||r||^2 per column in a fixed order (CTA trees of
+// the even and odd columns, then the last CTA).
+template <int R>
+__global__ void __launch_bounds__(kThreads) k_update_xr_pack(int64_t n, PcgState S, double* __restrict__ x,
+                                                             double* __restrict__ r, const double* __restrict__ p,
+                                                             const double* __restrict__ q,
+                                                             const int* __restrict__ pan_ptr,
+                                                             const int64_t* __restrict__ pan_row,
+                                                             unsigned char* __restrict__ b16, double* partials,
+                                                             unsigned int* ticket) {
+  constexpr int TPR = R / 2;  // threads per DOF, two columns each
+  constexpr uint32_t kMask = R == 64 ? 7u : (R == 32 ? 3u : 1u);
+  __shared__ double red[kThreads];
+  if (n_active(S.ist, R) == 0) return;
+  const int c2 = threadIdx.x % TPR;  // the stride is a multiple of TPR
+  const double a0 = S.st[DDX_ST_ALPHA * R + 2 * c2], a1 = S.st[DDX_ST_ALPHA * R + 2 * c2 + 1];
+  const int inrow = ((c2 >> 2) << 4) | ((c2 & 3) << 2);  // byte of this thread's pair in an unswizzled row
+  double acc0 = 0.0, acc1 = 0.0;
+  const int64_t total = n * TPR;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+    const int64_t d = i / TPR;
+    const int64_t o = d * R + 2 * c2;
+    const double2 xv = *reinterpret_cast<const double2*>(x + o);
+    const double2 pv = *reinterpret_cast<const double2*>(p + o);
+    const double2 rv = *reinterpret_cast<const double2*>(r + o);
+    const double2 qv = *reinterpret_cast<const double2*>(q + o);
+    const double2 rn = make_double2(fma(-a0, qv.x, rv.x), fma(-a1, qv.y, rv.y));
+    *reinterpret_cast<double2*>(x + o) = make_double2(fma(a0, pv.x, xv.x), fma(a1, pv.y, xv.y));
+    *reinterpret_cast<double2*>(r + o) = rn;
+    acc0 = fma(rn.x, rn.x, acc0);
+    acc1 = fma(rn.y, rn.y, acc1);
+    const uint32_t bits = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn((float)rn.x)) |
+                          ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn((float)rn.y)) << 16);
+    const int e1 = __ldg(pan_ptr + d + 1);
+    for (int e = __ldg(pan_ptr + d); e < e1; ++e) {
+      const int64_t off = __ldg(pan_row + e);
+      *reinterpret_cast<uint32_t*>(b16 + off + (inrow ^ (int)(((off >> 7) & kMask) << 4))) = bits;
+    }
+  }
+  // CTA sums of each column, written as partials[cta * R + column]
+  const double s0 = block_sum_by_col(acc0, red, TPR);
+  if (threadIdx.x < TPR) partials[(size_t)blockIdx.x * R + 2 * threadIdx.x] = s0;
+  const double s1 = block_sum_by_col(acc1, red, TPR);
+  if (threadIdx.x < TPR) partials[(size_t)blockIdx.x * R + 2 * threadIdx.x + 1] = s1;
+  if (!last_cta_arrival(ticket)) return;
+  double tot[1];
+  final_sums<1>(partials, R, red, tot, ticket);
+  int act = 0;
+  if (threadIdx.x < R) act = fin_rr(S, threadIdx.x, tot[0]);
+  publish_nactive(S, act);
+}
+
 // rho = r.z, zq = z.q -> beta
 __global__ void __launch_bounds__(kThreads) k_dots_rz(int64_t n, PcgState S, const double* __restrict__ r,
                                                       const double* __restrict__ z,
@@ -163,6 +226,30 @@ int ddx_pcg_update_xr(int64_t n, int R, double* x, double* r, const double* p, c
   k_update_xr<<<red_grid(n * R), kThreads, 0, (cudaStream_t)stream>>>(n, S, x, r, p, q, partials,
                                                                        tickets + 0);
   DDX_LAUNCH_CHECK("ddx_pcg_update_xr");
+  return DDX_OK;
+}
+
+int ddx_pcg_update_xr_pack16(int64_t n, int R, double* x, double* r, const double* p, const double* q,
+                             const int* pan_ptr, const int64_t* pan_row, void* b16, double* st, int* ist,
+                             double* hist, double* partials, unsigned int* tickets, ddx_stream_t stream) {
+  DDX_REQUIRE(R == 16 || R == 32 || R == 64, "ddx_pcg_update_xr_pack16: R must be 16, 32 or 64 (got %d)", R);
+  DDX_REQUIRE(n >= 0 && x && r && p && q && pan_ptr && pan_row && b16 && st && ist && hist && partials && tickets,
+              "ddx_pcg_update_xr_pack16: bad arguments");
+  DDX_REQUIRE(((uintptr_t)x & 15u) == 0 && ((uintptr_t)r & 15u) == 0 && ((uintptr_t)p & 15u) == 0 &&
+                  ((uintptr_t)q & 15u) == 0 && ((uintptr_t)b16 & 15u) == 0,
+              "ddx_pcg_update_xr_pack16: x, r, p, q and b16 must be 16-byte aligned");
+  if (n == 0) return DDX_OK;
+  PcgState S{st, ist, hist, R};
+  const int grid = red_grid(n * (R / 2));
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char* b = (unsigned char*)b16;
+  if (R == 16)
+    k_update_xr_pack<16><<<grid, kThreads, 0, s>>>(n, S, x, r, p, q, pan_ptr, pan_row, b, partials, tickets + 0);
+  else if (R == 32)
+    k_update_xr_pack<32><<<grid, kThreads, 0, s>>>(n, S, x, r, p, q, pan_ptr, pan_row, b, partials, tickets + 0);
+  else
+    k_update_xr_pack<64><<<grid, kThreads, 0, s>>>(n, S, x, r, p, q, pan_ptr, pan_row, b, partials, tickets + 0);
+  DDX_LAUNCH_CHECK("ddx_pcg_update_xr_pack16");
   return DDX_OK;
 }
 

@@ -573,12 +573,14 @@ class SchwarzOperator(SparseSolver):
         return s
 
     def _local(self, r: torch.Tensor, R: int, ist: torch.Tensor | None = None,
-               st: torch.Tensor | None = None) -> torch.Tensor:
+               st: torch.Tensor | None = None, packed: bool = False) -> torch.Tensor:
+        """Local products of r. ``packed``: the B panels of r were already written
+        (by ``ddx_pcg_update_xr_pack16`` or ``pack_panels``, scale 1)."""
         s = self.scratch(R)
         terms = self._tc_terms(R) if self.use_tensor_cores else 0
         if terms:
             sym, stages = self._tc_config(R, terms)
-            self._tc_apply(r, s["ylocal"], R, terms, sym, stages, ist, st)
+            self._tc_apply(r, s["ylocal"], R, terms, sym, stages, ist, None if packed else st, pack=not packed)
             self._ymap = self._ymap_one  # one slice written
             return s["ylocal"]
         cfg = self._apply_config(R)
@@ -586,15 +588,16 @@ class SchwarzOperator(SparseSolver):
         self._ymap = self._ymap_parts if self.store.layout == "sym" else self._ymap_one
         return s["ylocal"]
 
-    def _tc_apply(self, r, ylocal, R, terms, sym, stages, ist=None, st=None) -> None:
-        """Pack the 16-bit B panels of r, then the tensor-core local apply
-        (upper-triangle tiles with a ``stages``-deep ring when ``sym``, else
-        full-block tiles)."""
+    def _tc_apply(self, r, ylocal, R, terms, sym, stages, ist=None, st=None, pack=True) -> None:
+        """Pack the 16-bit B panels of r (unless ``pack`` is False: panels already
+        written), then the tensor-core local apply (upper-triangle tiles with a
+        ``stages``-deep ring when ``sym``, else full-block tiles)."""
         t = self._tile_store(sym)
         b16, panel_off = self._panels(R, terms)
         code = L.DTYPE_CODE[self.block_dtype]
-        L.call("ddx_pack_panels16", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
-               L.ptr(panel_off), L.ptr(r), L.ptr(st), L.ptr(b16), code, terms, L.stream_ptr())
+        if pack:
+            L.call("ddx_pack_panels16", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx),
+                   L.ptr(panel_off), L.ptr(r), L.ptr(st), L.ptr(b16), code, terms, L.stream_ptr())
         args = (self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.order), L.ptr(t.tile_off), L.ptr(t.data), code,
                 L.ptr(self.store.scale), self.kmax, L.ptr(b16), L.ptr(panel_off), terms, L.ptr(ylocal),
                 L.ptr(ist), L.ptr(st))
@@ -602,6 +605,33 @@ class SchwarzOperator(SparseSolver):
             L.call("ddx_schwarz_local_apply_tc_sym_ex", *args, int(stages), L.stream_ptr())
         else:
             L.call("ddx_schwarz_local_apply_tc", *args, L.stream_ptr())
+
+    def fused_pack_ok(self, R: int) -> bool:
+        """The PCG update can write this operator's B panels itself: tensor-core
+        path with BF16 blocks and one residual term."""
+        return (self.use_tensor_cores and self.block_dtype == torch.bfloat16 and R in (16, 32, 64)
+                and self._tc_terms(R) == 1)
+
+    def panel_rows(self, R: int):
+        """(pan_ptr, pan_row): for DOF d, the byte offsets in the B-panel buffer of
+        the panel rows that hold it (subdomain i, local row c: panel_off[i] + 2R c),
+        in transpose-map order; built once per R."""
+        key = ("panrows", R)
+        got = self._scratch.get(key)
+        if got is None:
+            _, panel_off = self._panels(R, 1)
+            t = self.dof_src.to(torch.int64)
+            i = torch.searchsorted(self.sub_ptr, t, right=True) - 1
+            c = t - self.sub_ptr[i]
+            got = (self.dof_ptr, (panel_off[i] + 2 * R * c).contiguous())
+            self._scratch[key] = got
+        return got
+
+    def pack_panels(self, r: torch.Tensor, R: int) -> None:
+        """B panels of r with scale 1 (what ``ddx_pcg_update_xr_pack16`` writes)."""
+        b16, panel_off = self._panels(R, 1)
+        L.call("ddx_pack_panels16", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx), L.ptr(panel_off),
+               L.ptr(r), None, L.ptr(b16), L.DTYPE_CODE[self.block_dtype], 1, L.stream_ptr())
 
     def _tc_candidates(self, R: int, terms: int) -> list[tuple[bool, int]]:
         """(symmetric tiles, ring stages) the tensor-core autotuner times: every
@@ -816,8 +846,9 @@ class SchwarzOperator(SparseSolver):
                float(sign), L.ptr(z), dots, L.ptr(r), L.ptr(q), L.ptr(st), L.ptr(ist), L.ptr(partials),
                L.ptr(tickets), L.stream_ptr())
 
-    # Applied by the fused PCG loop: z = M r with rho = r.z (and z.q) -> beta.
-    def _apply_fused(self, r, z, R, pcg, q):
+    # Applied by the fused PCG loop: z = M r with rho = r.z (and z.q) -> beta;
+    # ``packed``: the B panels of r are already written (tensor-core path).
+    def _apply_fused(self, r, z, R, pcg, q, packed=False):
         raise NotImplementedError
 
     def _apply(self, rhs: torch.Tensor) -> torch.Tensor:
@@ -851,14 +882,14 @@ class AdditiveSchwarz(SchwarzOperator):
             self.dofs_per_coarse = dofs_per_solver * int(self.solvers_per_coarse[0].item())
         return timings
 
-    def _apply_fused(self, r, z, R, pcg, q):
+    def _apply_fused(self, r, z, R, pcg, q, packed=False):
         s = self.scratch(R)
         ist = None if pcg is None else pcg.ist
         st = None if pcg is None else pcg.st
         if self.n_coarse:
             self._restrict(*self._R0, r, s["w"], R)
             self._coarse(s["w"], s["yc"], R, ist)
-        ylocal = self._local(r, R, ist, st)
+        ylocal = self._local(r, R, ist, st, packed)
         self._combine(z, R, ylocal=ylocal, prolong=bool(self.n_coarse), sign=1.0, pcg=pcg, r=r, q=q)
 
 
@@ -890,11 +921,11 @@ class HybridSchwarz(SchwarzOperator):
         self._coarse(s["w"], s["yc"], R, ist)
         self._combine(x, R, u=x, prolong=True, sign=1.0)
 
-    def _apply_fused(self, r, z, R, pcg, q):
+    def _apply_fused(self, r, z, R, pcg, q, packed=False):
         s = self.scratch(R)
         ist = None if pcg is None else pcg.ist
         st = None if pcg is None else pcg.st
-        ylocal = self._local(r, R, ist, st)
+        ylocal = self._local(r, R, ist, st, packed)
         if not self.n_coarse:
             self._combine(z, R, ylocal=ylocal, pcg=pcg, r=r, q=q)
             return
@@ -982,6 +1013,7 @@ class _PcgWork:
         self.graphs = {}
         self.graph_calls = {}
         self.warm = False
+        self.fused_pack = False
 
 
 class _SellMatrix:
@@ -1050,6 +1082,8 @@ class CG(SparseSolver):
         self.replace_every = replace_every
         self.check_every = check_every
         self.use_graph = use_graph
+        # multi-RHS tensor-core path: the x/r update writes the next apply's B panels
+        self.fuse_panels = True
         self._work = {}
 
     def __str__(self):
@@ -1097,7 +1131,7 @@ class CG(SparseSolver):
                    L.ptr(w.partials), L.ptr(w.tickets), L.stream_ptr())
             return w.r
         if isinstance(pc, SchwarzOperator):
-            pc._apply_fused(w.r, w.z, R, w, w.q)
+            pc._apply_fused(w.r, w.z, R, w, w.q, packed=w.fused_pack)
             return w.z
         # generic preconditioner: Python-level solve, then the fused dots
         rr = w.r.view(self.n, R) if R > 1 else w.r
@@ -1112,10 +1146,20 @@ class CG(SparseSolver):
         z = self._precondition(w)
         L.call("ddx_pcg_update_p", self.n, R, L.ptr(z), L.ptr(w.p), L.ptr(w.st), L.ptr(w.ist), L.stream_ptr())
         self.matrix.launch(w.p, w.q, R, L.SPMV_PQ, w, use_sell=self.bsr_matmul)
-        L.call("ddx_pcg_update_xr", self.n, R, L.ptr(w.x), L.ptr(w.r), L.ptr(w.p), L.ptr(w.q), L.ptr(w.st),
-               L.ptr(w.ist), L.ptr(w.hist), L.ptr(w.partials), L.ptr(w.tickets), L.stream_ptr())
+        if w.fused_pack:
+            # x, r and the next local apply's B panels in one pass
+            pan_ptr, pan_row = self.preconditioner.panel_rows(R)
+            b16, _ = self.preconditioner._panels(R, 1)
+            L.call("ddx_pcg_update_xr_pack16", self.n, R, L.ptr(w.x), L.ptr(w.r), L.ptr(w.p), L.ptr(w.q),
+                   L.ptr(pan_ptr), L.ptr(pan_row), L.ptr(b16), L.ptr(w.st), L.ptr(w.ist), L.ptr(w.hist),
+                   L.ptr(w.partials), L.ptr(w.tickets), L.stream_ptr())
+        else:
+            L.call("ddx_pcg_update_xr", self.n, R, L.ptr(w.x), L.ptr(w.r), L.ptr(w.p), L.ptr(w.q), L.ptr(w.st),
+                   L.ptr(w.ist), L.ptr(w.hist), L.ptr(w.partials), L.ptr(w.tickets), L.stream_ptr())
         if replace:
             self.matrix.launch(w.x, w.r, R, L.SPMV_RES_REPLACE, w, b=w.b, use_sell=self.bsr_matmul)
+            if w.fused_pack:
+                self.preconditioner.pack_panels(w.r, R)
 
     def _chunk(self, w: _PcgWork, k: int, start: int):
         re = self.replace_every
@@ -1125,7 +1169,8 @@ class CG(SparseSolver):
             for rep in plan:
                 self._iteration(w, rep)
             return
-        g = w.graphs.get(plan)
+        key = (plan, w.fused_pack)
+        g = w.graphs.get(key)
         if g is None:
             if not w.warm:
                 # first chunk runs eagerly: kernel attributes and scratch buffers
@@ -1139,11 +1184,11 @@ class CG(SparseSolver):
             with torch.cuda.graph(g):
                 for rep in plan:
                     self._iteration(w, rep)
-            w.graph_calls[plan] = L.CALLS[0] - c0
+            w.graph_calls[key] = L.CALLS[0] - c0
             L.CALLS[0] = c0
-            w.graphs[plan] = g
+            w.graphs[key] = g
         g.replay()
-        L.CALLS[0] += w.graph_calls[plan]
+        L.CALLS[0] += w.graph_calls[key]
 
     # -- solve ---------------------------------------------------------------
     def solve(self, rhs: torch.Tensor, x0=None) -> Tuple[torch.Tensor, Metadata]:
@@ -1177,6 +1222,13 @@ class CG(SparseSolver):
             else:
                 xmat[:, :R] += pc.T0(rhs).view(n, R).to(torch.float64)
         self.matrix.launch(w.x, w.r, Rp, L.SPMV_RES_INIT, w, b=w.b, use_sell=self.bsr_matmul)
+        w.fused_pack = bool(self.fuse_panels and isinstance(pc, SchwarzOperator) and pc.fused_pack_ok(Rp))
+        if w.fused_pack:
+            # the tensor-core autotuner packs its own test panels into the same
+            # buffer: let it run first, then the panels of the initial residual
+            # (later ones come from the x/r update)
+            pc._tc_config(Rp, 1)
+            pc.pack_panels(w.r, Rp)
 
         alphas, betas = [], []
         done = 0

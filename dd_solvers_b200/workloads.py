@@ -34,7 +34,12 @@ WORKLOADS = {
 }
 
 
-def build_problem(spec: dict, seed: int = 0):
+def build_problem(spec: dict, seed: int = 0, device=None):
+    """Matrix, owners, overlapping subdomains and coarse restriction of a
+    workload (numpy / SciPy). With a CUDA ``device`` the RCB bisection and the
+    overlap growth run there (``partition.rcb_owner_device``,
+    ``overlapping_subdomains_device``: identical output, tested) and are copied
+    back."""
     from . import partition, problems
 
     t0 = time.time()
@@ -51,9 +56,22 @@ def build_problem(spec: dict, seed: int = 0):
     else:
         P = problems.p1_jittered(spec["n_nodes"], 0.3, 1.0, seed)
         nparts = spec["parts"]
-        owner = partition.rcb_owner(P.coords, nparts)
+        if device is not None:
+            import torch
+
+            owner = partition.rcb_owner_device(torch.as_tensor(P.coords, device=device), nparts).cpu().numpy()
+        else:
+            owner = partition.rcb_owner(P.coords, nparts)
     A = P.matrix
-    sub_ptr, sub_idx = partition.overlapping_subdomains(A, owner, nparts, 1)
+    if device is not None:
+        import torch
+
+        crow = torch.as_tensor(A.indptr.astype(np.int64), device=device)
+        col = torch.as_tensor(A.indices.astype(np.int64), device=device)
+        sp, si = partition.overlapping_subdomains_device(crow, col, torch.as_tensor(owner, device=device), nparts, 1)
+        sub_ptr, sub_idx = sp.cpu().numpy(), si.cpu().numpy()
+    else:
+        sub_ptr, sub_idx = partition.overlapping_subdomains(A, owner, nparts, 1)
     if spec["coarse"] == "q1":
         R0 = partition.q1_coarse_restriction(3, spec["n_el"], spec["parts"])
     else:

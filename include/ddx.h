@@ -83,6 +83,20 @@ int ddx_pcg_update_p(int64_t n, int R, const double* z, double* p, const double*
 int ddx_pcg_update_xr(int64_t n, int R, double* x, double* r, const double* p, const double* q,
                       double* st, int* ist, double* hist, double* partials, unsigned int* tickets,
                       ddx_stream_t stream);
+/* ddx_pcg_update_xr for R in {16, 32, 64} (16-byte aligned vectors) that also
+ * writes r, rounded to BF16 with scale 1, into the tensor-core B panels of the
+ * next local apply (ddx_pack_panels16's layout with one term): DOF d's row goes
+ * to every panel row that holds it, at byte offsets pan_row[e] of b16 for e in
+ * [pan_ptr[d], pan_ptr[d+1]) (offset = panel_off[i] + 2R c for DOF d at local
+ * row c of subdomain i), its 16-byte chunk q at q ^ ((offset >> 7) & mask),
+ * mask 7 / 3 / 1 for R = 64 / 32 / 16. The apply then runs without a pack and
+ * with st = NULL (scale 1). rr is summed per column in a fixed order (not the
+ * order of ddx_pcg_update_xr). Replaces the same reference updates as
+ * ddx_pcg_update_xr (solvers.py:265-267) plus the gather of r into the
+ * local solves (Inv.solve's input, solvers.py:355-359). */
+int ddx_pcg_update_xr_pack16(int64_t n, int R, double* x, double* r, const double* p, const double* q,
+                             const int* pan_ptr, const int64_t* pan_row, void* b16, double* st, int* ist,
+                             double* hist, double* partials, unsigned int* tickets, ddx_stream_t stream);
 /* rho = r.z (and z.q when flexible) -> beta; for preconditioners that write z
  * themselves (generic path). q may be NULL on the first iteration. */
 int ddx_pcg_dots_rz(int64_t n, int R, const double* r, const double* z, const double* q, double* st,
