@@ -142,29 +142,42 @@ def host_inverses(prob):
 
 def cpu_solve_per_rhs(prob, spec, rtol, inverse_blocks, repeats: int = 1):
     """CPU baseline: full FP64 Schwarz-PCG solves of one right-hand side of the
-    workload with the oracle restatement on the host cores (NumPy/SciPy, BLAS on
-    every core), timed like the reference times its solves: the minimum over
-    ``repeats`` solves, setup excluded (the FP64 inverse blocks are given)."""
+    workload with the oracle restatement on the host cores, run the way the
+    reference runs its solver on CPU tensors: the equal-size local blocks applied
+    by one batched matrix product per size and the sparse products through
+    torch's threaded CSR kernel, every host thread. Timed like the reference times
+    its solves: the minimum over ``repeats`` solves, setup excluded (the FP64
+    inverse blocks are given)."""
+    import torch
+    from threadpoolctl import threadpool_limits
+
     from oracle import restatement as orc
 
+    torch.set_num_threads(os.cpu_count())
     A, R0 = prob["A"], prob["R0"]
-    M = orc.Schwarz(A, prob["sub_ptr"], prob["sub_idx"], R0, inverse_blocks=inverse_blocks)
+    M = orc.Schwarz(A, prob["sub_ptr"], prob["sub_idx"], R0, inverse_blocks=inverse_blocks, batched=True)
+    Ah = orc.HostCSR(A)
     n = A.shape[0]
     b = rhs_for(n, 0, 1, spec)
     b = b if b.ndim == 1 else b[:, 0]
     times, its = [], None
-    for _ in range(max(1, repeats)):
-        t0 = time.perf_counter()
-        if spec["method"] == "hybrid":
-            _, m = orc.pcg(A, b, M.hybrid, rtol=rtol, T0=M.T0, maxiter=5000)
-        else:
-            _, m = orc.pcg(A, b, M.additive, rtol=rtol, maxiter=5000)
-        times.append(time.perf_counter() - t0)
-        its = m["iterations"]
+    # NumPy's BLAS pool kept to one thread: its spinning workers would otherwise
+    # contend with torch's for the same cores (measured 10x slower solves)
+    with threadpool_limits(1, user_api="blas"):
+        for _ in range(max(1, repeats)):
+            t0 = time.perf_counter()
+            if spec["method"] == "hybrid":
+                _, m = orc.pcg(Ah, b, M.hybrid, rtol=rtol, T0=M.T0, maxiter=5000)
+            else:
+                _, m = orc.pcg(Ah, b, M.additive, rtol=rtol, maxiter=5000)
+            times.append(time.perf_counter() - t0)
+            its = m["iterations"]
     return {"ms_per_rhs": min(times) * 1e3, "iterations": its, "cores": os.cpu_count(), "solves": len(times),
             "sample": (f"full FP64 {spec['method']} Schwarz-PCG solve of one right-hand side on the whole problem "
                        f"({n} DOFs, {len(prob['sub_ptr']) - 1} subdomains) with the oracle restatement to rtol "
-                       f"{rtol:g}, {its} iterations, min over {len(times)} solve(s), setup excluded")}
+                       f"{rtol:g} (local blocks by torch.bmm per block size, torch CSR products, "
+                       f"{torch.get_num_threads()} threads), {its} iterations, min over {len(times)} solve(s), "
+                       f"setup excluded")}
 
 
 def gpu_blocks_to_host(pc):
@@ -344,7 +357,7 @@ def run_ours(args, spec, rank: int, world: int):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     R = spec["R"]
-    prob = build_problem(spec)
+    prob = build_problem(spec, device=dev)
     A = prob["A"]
     n = A.shape[0]
     At = dd.csr_to_torch(A).to(dev)
@@ -544,19 +557,24 @@ def run_ours(args, spec, rank: int, world: int):
         bms = replicas.max_over_ranks(e0.elapsed_time(e1) / kb, dev)
         rb = torch.randn(n * Rb, dtype=torch.float64, device=dev)
         pcb = pcs[head]
+        # the solve's own form of the apply: without a pack pass when the x/r
+        # update writes the B panels
+        fused = cgb.fuse_panels and pcb.fused_pack_ok(Rb)
+        if fused:
+            pcb.pack_panels(rb, Rb)
         for _ in range(2):
-            pcb._local(rb, Rb)
+            pcb._local(rb, Rb, packed=fused)
         torch.cuda.synchronize()
         kev[0].record()
         for _ in range(reps):
-            pcb._local(rb, Rb)
+            pcb._local(rb, Rb, packed=fused)
         kev[1].record()
         torch.cuda.synchronize()
         tc_ms = kev[0].elapsed_time(kev[1]) / reps
         bsym, bstages = pcb._tc_config(Rb, pcb._tc_terms(Rb))
         tiles = pcb._tile_store(bsym)
         tc_blk = tiles.nbytes if bsym else int((ks * ks).sum() * elt)
-        tc_bytes = int(tc_blk + 4 * len(ks) + ks.sum() * 4 + n * Rb * 8 + ks.sum() * Rb * 4)
+        tc_bytes = tc_apply_bytes(pcb, Rb, tc_blk, n, fused)
         tc_flops = float(2 * (ks * ks).sum() * Rb)
         batched = {"rhs": Rb, "ms_per_solve": bms, "ms_per_rhs": bms / Rb, "iterations": max(mb["iterations"]),
                    "rel_error_vs_fp64_checked_columns": ebs,
@@ -571,7 +589,8 @@ def run_ours(args, spec, rank: int, world: int):
                                  "mma_tflops": tc_mma_flops(pcb, Rb, bsym) / (tc_ms * 1e-3) / 1e12,
                                  "tensor_frac_of_measured_bf16_peak": tc_mma_flops(pcb, Rb, bsym) / (tc_ms * 1e-3)
                                  / 1e12 / load_peaks()["bf16_tflops"],
-                                 "includes": "16-bit B-panel pack + tensor-core apply"}}
+                                 "includes": ("tensor-core apply (the B panels are written by the x/r update)" if fused
+                                              else "16-bit B-panel pack + tensor-core apply")}}
 
     peaks = load_peaks()
     out = None
@@ -675,6 +694,18 @@ def tc_mma_flops(pc, R: int, sym: bool) -> float:
     return float(2 * R * (rows * cols).sum())
 
 
+def tc_apply_bytes(pc, R: int, blk_bytes: int, n: int, fused: bool) -> int:
+    """Algorithmic bytes of one tensor-core local apply: the block tiles, the
+    per-subdomain scales and sizes, the r input (the B panels it reads when the
+    x/r update wrote them, else r itself, n R FP64 values) and the FP32 local
+    products written."""
+    ks = pc.ks.astype(np.int64)
+    if fused:
+        panels = int((2 * ((ks + 127) // 128) * 64 * 2 * R).sum())
+        return int(blk_bytes + 4 * len(ks) + ks.sum() * 4 + panels + ks.sum() * R * 4)
+    return int(blk_bytes + 4 * len(ks) + ks.sum() * 4 + n * R * 8 + ks.sum() * R * 4)
+
+
 def time_ms(fn, reps: int = 10) -> float:
     import torch
 
@@ -704,7 +735,7 @@ def multi_rhs_summary(args, name: str, prec: str) -> dict:
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     spec = WORKLOADS[name]
     t0 = time.time()
-    prob = build_problem(spec)
+    prob = build_problem(spec, device=dev)
     A = prob["A"]
     n, R = A.shape[0], spec["R"]
     At = dd.csr_to_torch(A).to(dev)
@@ -754,10 +785,13 @@ def multi_rhs_summary(args, name: str, prec: str) -> dict:
     r = torch.randn(n * R, dtype=torch.float64, device=dev)
     terms = pcq._tc_terms(R)
     sym, stages = pcq._tc_config(R, terms)
-    k_ms = time_ms(lambda: pcq._local(r, R), 10)
+    fused = cg.fuse_panels and pcq.fused_pack_ok(R)
+    if fused:
+        pcq.pack_panels(r, R)
+    k_ms = time_ms(lambda: pcq._local(r, R, packed=fused), 10)
     ks = pcq.ks.astype(np.int64)
     blk = pcq._tile_store(True).nbytes if sym else int((ks * ks).sum() * 2)
-    alg = int(blk + 4 * len(ks) + ks.sum() * 4 + n * R * 8 + ks.sum() * R * 4)
+    alg = tc_apply_bytes(pcq, R, blk, n, fused)
     flops = tc_mma_flops(pcq, R, sym)
     q = torch.empty_like(r)
     mat = base.matrix
@@ -772,7 +806,8 @@ def multi_rhs_summary(args, name: str, prec: str) -> dict:
                          "achieved_gbs": alg / (k_ms * 1e-3) / 1e9, "hbm_frac": alg / (k_ms * 1e-3) / 1e9 /
                          peaks["hbm_gbs"], "mma_tflops": flops / (k_ms * 1e-3) / 1e12,
                          "tensor_frac_of_measured_bf16_peak": flops / (k_ms * 1e-3) / 1e12 / peaks["bf16_tflops"],
-                         "includes": "16-bit B-panel pack + tensor-core apply"},
+                         "includes": ("tensor-core apply (the B panels are written by the x/r update)" if fused
+                                      else "16-bit B-panel pack + tensor-core apply")},
            "spmm": {"name": "ddx_spmv_csr_f64",
                     "ms_per_launch": s_ms, "algorithmic_bytes": s_bytes,
                     "hbm_frac": s_bytes / (s_ms * 1e-3) / 1e9 / peaks["hbm_gbs"]}}
@@ -788,8 +823,10 @@ REF_BUDGET_S = 150.0
 
 
 def _blocks_bytes(prob) -> int:
+    """Host bytes the CPU solve holds for its FP64 blocks: the per-block list and,
+    while it is stacked by block size, the stacked copy."""
     ks = np.diff(prob["sub_ptr"]).astype(np.int64)
-    return int((ks * ks).sum() * 8)
+    return int((ks * ks).sum() * 8) * 2
 
 
 def _host_ram() -> int:

@@ -18,6 +18,11 @@ low-precision block storage with per-block power-of-two scales):
 * ``Schwarz.local``       - ``sum_i R_i^T A_i^{-1} R_i r`` (``Inv.solve``, 355-359, on the
                             ``reshape(n_solvers, -1)`` blocks of 814/878, generalised to
                             index sets).
+                            ``batched=True``: the blocks of each size stacked and applied
+                            by one ``torch.bmm`` (as ``Inv.solve`` batches them), with
+                            ``HostCSR`` (torch's threaded CSR product, as ``CG.solve``'s
+                            ``self.matrix @ p``, 264) for the sparse products: the mode the
+                            timed CPU baseline runs, same results up to summation order.
 * ``Schwarz.additive``    - ``AdditiveSchwarz.solve`` (811-826).
 * ``Schwarz.hybrid``      - ``HybridSchwarz.solve`` (874-888): ``y - R0^T A_C^{-1} (R0 A) y``.
 * ``Schwarz.T0``          - ``HybridSchwarz.T0`` (861-872).
@@ -32,6 +37,8 @@ low-precision block storage with per-block power-of-two scales):
                             reference uses cuDSS (85-113).
 """
 from __future__ import annotations
+
+import warnings
 
 import numpy as np
 import scipy.linalg as sla
@@ -141,11 +148,43 @@ def coarse_matrix(A: sps.csr_matrix, R0: sps.csr_matrix) -> np.ndarray:
     return (R0 @ A @ R0.T).toarray()
 
 
+class HostCSR:
+    """A SciPy CSR matrix applied through torch's CPU sparse product (threaded),
+    the way the reference runs its ``CG`` on CPU tensors (``self.matrix @ p``,
+    ``solvers.py:264``). ``A @ v`` for NumPy vectors / (n, R) blocks."""
+
+    def __init__(self, A):
+        import torch
+
+        A = sps.csr_matrix(A)
+        self.shape = A.shape
+        self.sp = A
+        with warnings.catch_warnings():  # torch flags CSR tensors as beta
+            warnings.simplefilter("ignore")
+            self.t = torch.sparse_csr_tensor(torch.as_tensor(A.indptr.astype(np.int64)),
+                                             torch.as_tensor(A.indices.astype(np.int64)),
+                                             torch.as_tensor(A.data.astype(np.float64)), A.shape)
+
+    def __matmul__(self, v):
+        import torch
+
+        v = np.asarray(v, dtype=np.float64)
+        vt = torch.from_numpy(np.ascontiguousarray(v))
+        out = self.t @ (vt if vt.dim() == 2 else vt[:, None])
+        return out.numpy()[:, 0] if v.ndim == 1 else out.numpy()
+
+
 class Schwarz:
-    """Two-level Schwarz with explicit local inverses (reference ``Inv``)."""
+    """Two-level Schwarz with explicit local inverses (reference ``Inv``).
+
+    ``batched=True`` runs the local solves the way the reference does on CPU
+    tensors: the blocks of equal size stacked and applied by one batched matrix
+    product (``torch.bmm``, as ``gemv_strided_batched``'s CPU counterpart) per
+    size, and the sparse products through torch (``HostCSR``). Same values; the
+    sums run in another order."""
 
     def __init__(self, A, sub_ptr, sub_idx, R0=None, block_dtype="f64", vec_dtype="f64",
-                 inverse_blocks=None):
+                 inverse_blocks=None, batched=False):
         self.A = sps.csr_matrix(A)
         self.sub_ptr = np.asarray(sub_ptr, dtype=np.int64)
         self.sub_idx = np.asarray(sub_idx, dtype=np.int64)
@@ -169,6 +208,28 @@ class Schwarz:
             self.Ac = coarse_matrix(self.A, self.R0)
             self.Ac_cho = sla.cho_factor(self.Ac)
             self.AR = (self.R0 @ self.A).tocsr()
+        self.groups = None
+        if batched:
+            self._stack()
+
+    def _stack(self):
+        """Blocks grouped by size: (sizes, stacked blocks (G, k, k), their index
+        sets (G, k), scales (G)) as torch tensors; the per-block list is dropped."""
+        import torch
+
+        ks = np.diff(self.sub_ptr)
+        self.groups = []
+        for k in np.unique(ks):
+            if k == 0:
+                continue
+            sel = np.nonzero(ks == k)[0]
+            B = torch.from_numpy(np.stack([self.blocks[i] for i in sel]))
+            idx = torch.from_numpy(np.stack([self.sub_idx[self.sub_ptr[i]:self.sub_ptr[i + 1]] for i in sel]))
+            self.groups.append((B, idx, torch.from_numpy(self.scales[sel])))
+            for i in sel:
+                self.blocks[i] = None
+        if self.R0 is not None:
+            self.AR = HostCSR(self.AR)
 
     def _vec(self, r):
         return round_to(r, self.vec_dtype)
@@ -176,6 +237,17 @@ class Schwarz:
     def local(self, r: np.ndarray) -> np.ndarray:
         """``sum_i R_i^T (s_i Q_i) R_i r`` (columns of r are independent RHS)."""
         r = self._vec(r)
+        if self.groups is not None:
+            import torch
+
+            rt = torch.from_numpy(np.ascontiguousarray(r))
+            vec = rt.dim() == 1
+            rt2 = rt[:, None] if vec else rt
+            y = torch.zeros_like(rt2)
+            for B, idx, sc in self.groups:
+                Y = torch.bmm(B, rt2[idx]) * sc[:, None, None]   # (G, k, R)
+                y.index_add_(0, idx.reshape(-1), Y.reshape(-1, Y.shape[-1]))
+            return (y[:, 0] if vec else y).numpy()
         y = np.zeros_like(r, dtype=np.float64)
         for i in range(self.N):
             idx = self.sub_idx[self.sub_ptr[i]:self.sub_ptr[i + 1]]
@@ -210,8 +282,9 @@ class Schwarz:
 
 def pcg(A, b, M=None, rtol=1e-7, atol=0.0, maxiter=1000, x0=None, T0=None,
         flexible=False, record_iterates=False, raise_on_fail=True):
-    """Single-RHS PCG with the reference's control flow (``solvers.py:228-297``)."""
-    A = sps.csr_matrix(A)
+    """Single-RHS PCG with the reference's control flow (``solvers.py:228-297``).
+    ``A`` is a SciPy matrix or a ``HostCSR``."""
+    A = A if isinstance(A, HostCSR) else sps.csr_matrix(A)
     b = np.asarray(b, dtype=np.float64)
     atol = max(atol, rtol * float(np.linalg.norm(b)))
     n = len(b)
@@ -316,7 +389,11 @@ class ContiguousSchwarz:
         self.lu = spla.splu(self.Ac)
 
     def local(self, r):
-        return np.einsum("nij,nj->ni", self.Binv, r.reshape(self.N, self.k)).reshape(-1)
+        import torch
+
+        # one batched product over the equal blocks, as the reference's Inv.solve
+        Y = torch.bmm(torch.from_numpy(self.Binv), torch.from_numpy(np.ascontiguousarray(r)).reshape(self.N, self.k, 1))
+        return Y.reshape(-1).numpy()
 
     def coarse_solve(self, w):
         return self.lu.solve(w)
