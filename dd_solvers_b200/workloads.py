@@ -12,7 +12,8 @@ import numpy as np
 # fp64_iterations: PCG iterations of the FP64 method on the workload at the
 # tolerance that reaches 1e-8 error (measured on B200 by the GPU arm; the CPU
 # restatement reproduces it +-1; c4: forward + adjoint solve, from the
-# restatement), used to scale the per-iteration CPU sample of the reference arm.
+# restatement), the count the gradient workload reports for its FP64 solves.
+# overlap: layers of overlap grown around each owned part (default 1).
 WORKLOADS = {
     "c2": dict(kind="q1_3d", n_el=128, parts=16, coarse="q1", method="hybrid", rhs="uniform", R=1,
                fp64_iterations=31,
@@ -20,6 +21,10 @@ WORKLOADS = {
     "c1": dict(kind="q1_2d", n_el=256, parts=8, coarse="p0", method="additive", rhs="uniform", R=1,
                fp64_iterations=91,
                name="additive-schwarz q1-2d poisson 256^2 cells, 64 subdomains overlap 1, p0 coarse 64"),
+    "c1r": dict(kind="q1_2d", n_el=256, parts=15, overlap=0, coarse="p0", method="hybrid", rhs="uniform", R=1,
+                fp64_iterations=42,
+                name="hybrid-schwarz q1-2d poisson 256^2 cells, 225 subdomains of 17^2 DOFs without overlap, "
+                     "p0 coarse 225 (the reference's own layout: contiguous equal subdomains)"),
     "c3": dict(kind="q1_2d", n_el=1024, parts=32, coarse="p0", method="hybrid", rhs="normal", R=64,
                fp64_iterations=70,
                name="hybrid-schwarz q1-2d poisson 1024^2 cells, 1024 subdomains overlap 1, p0 coarse, 64 rhs"),
@@ -68,10 +73,11 @@ def build_problem(spec: dict, seed: int = 0, device=None):
 
         crow = torch.as_tensor(A.indptr.astype(np.int64), device=device)
         col = torch.as_tensor(A.indices.astype(np.int64), device=device)
-        sp, si = partition.overlapping_subdomains_device(crow, col, torch.as_tensor(owner, device=device), nparts, 1)
+        sp, si = partition.overlapping_subdomains_device(crow, col, torch.as_tensor(owner, device=device), nparts,
+                                                         spec.get("overlap", 1))
         sub_ptr, sub_idx = sp.cpu().numpy(), si.cpu().numpy()
     else:
-        sub_ptr, sub_idx = partition.overlapping_subdomains(A, owner, nparts, 1)
+        sub_ptr, sub_idx = partition.overlapping_subdomains(A, owner, nparts, spec.get("overlap", 1))
     if spec["coarse"] == "q1":
         R0 = partition.q1_coarse_restriction(3, spec["n_el"], spec["parts"])
     else:
