@@ -154,7 +154,9 @@ def cpu_solve_per_rhs(prob, spec, rtol, inverse_blocks, repeats: int = 1):
     from oracle import restatement as orc
 
     torch.set_num_threads(os.cpu_count())
-    A, R0 = prob["A"], prob["R0"]
+    from dd_solvers_b200.setup_ops import scipy_csr
+
+    A, R0 = prob["A"], scipy_csr(prob["R0"])
     M = orc.Schwarz(A, prob["sub_ptr"], prob["sub_idx"], R0, inverse_blocks=inverse_blocks, batched=True)
     Ah = orc.HostCSR(A)
     n = A.shape[0]

@@ -159,6 +159,19 @@ struct PcgState {
   __device__ __forceinline__ int& g(int slot) const { return ist[DDX_IST_COUNT * R + slot]; }
 };
 
+// A sharded solve (DDX_G_DEFER set): the last CTA of a fused reduction parks
+// its NV column totals (valid in threads tid < R) in st slots T0.. and leaves
+// the epilogue to ddx_pcg_finalize. True when parked (the caller returns).
+template <int NV>
+__device__ __forceinline__ bool park_totals(PcgState S, const double (&tot)[NV]) {
+  if (S.ist == nullptr || S.g(DDX_G_DEFER) == 0) return false;
+  if (threadIdx.x < S.R) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) S.s(DDX_ST_T0 + v, threadIdx.x) = tot[v];
+  }
+  return true;
+}
+
 __device__ __forceinline__ int n_active(const int* ist, int R) {
   return ist == nullptr ? 1 : *((volatile const int*)ist + DDX_IST_COUNT * R + DDX_G_NACTIVE);
 }

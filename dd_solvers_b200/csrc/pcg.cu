@@ -34,7 +34,24 @@ __global__ void k_pcg_reset(PcgState S, int maxiter, int flexible, double rtol, 
     S.g(DDX_G_MAXITER) = maxiter;
     S.g(DDX_G_FLEXIBLE) = flexible;
     S.g(DDX_G_BREAKDOWN) = 0;
+    S.g(DDX_G_DEFER) = 0;
   }
+}
+
+// Epilogue of a deferred reduction on the totals parked in T0 / T1 (summed
+// over the ranks by the caller): the same fin_* step as the fused kernels.
+__global__ void k_pcg_finalize(PcgState S, int kind) {
+  const int j = threadIdx.x;
+  int act = 0;
+  if (j < S.R) {
+    const double t0 = S.s(DDX_ST_T0, j), t1 = S.s(DDX_ST_T1, j);
+    if (kind == DDX_FIN_RZ) fin_rz(S, j, t0, t1);
+    else if (kind == DDX_FIN_PQ) act = fin_pq(S, j, t0);
+    else if (kind == DDX_FIN_RR) act = fin_rr(S, j, t0);
+    else if (kind == DDX_FIN_INIT) act = fin_init(S, j, t1, t0);
+    else act = fin_replace(S, j, t0);
+  }
+  if (kind != DDX_FIN_RZ) publish_nactive(S, act);
 }
 
 // p = z + beta p
@@ -74,6 +91,7 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(int64_t n, PcgState S, d
   if (!last_cta_arrival(ticket)) return;
   double tot[1];
   final_sums<1>(partials, R, red, tot, ticket);
+  if (park_totals<1>(S, tot)) return;
   int act = 0;
   if (threadIdx.x < R) act = fin_rr(S, threadIdx.x, tot[0]);
   publish_nactive(S, act);
@@ -137,6 +155,7 @@ __global__ void __launch_bounds__(kThreads) k_update_xr_pack(int64_t n, PcgState
   if (!last_cta_arrival(ticket)) return;
   double tot[1];
   final_sums<1>(partials, R, red, tot, ticket);
+  if (park_totals<1>(S, tot)) return;
   int act = 0;
   if (threadIdx.x < R) act = fin_rr(S, threadIdx.x, tot[0]);
   publish_nactive(S, act);
@@ -162,6 +181,7 @@ __global__ void __launch_bounds__(kThreads) k_dots_rz(int64_t n, PcgState S, con
   if (!last_cta_arrival(ticket)) return;
   double tot[2];
   final_sums<2>(partials, R, red, tot, ticket);
+  if (park_totals<2>(S, tot)) return;
   if (threadIdx.x < R) fin_rz(S, threadIdx.x, tot[0], tot[1]);
 }
 
@@ -202,6 +222,16 @@ int ddx_pcg_reset(int R, double* st, int* ist, int maxiter, int flexible, double
   PcgState S{st, ist, nullptr, R};
   k_pcg_reset<<<1, 64, 0, (cudaStream_t)stream>>>(S, maxiter, flexible, rtol, atol);
   DDX_LAUNCH_CHECK("ddx_pcg_reset");
+  return DDX_OK;
+}
+
+int ddx_pcg_finalize(int R, int kind, double* st, int* ist, double* hist, ddx_stream_t stream) {
+  DDX_REQUIRE(valid_rhs_count(R), "ddx_pcg_finalize: unsupported R=%d", R);
+  DDX_REQUIRE(st && ist && hist, "ddx_pcg_finalize: null state");
+  DDX_REQUIRE(kind >= DDX_FIN_RZ && kind <= DDX_FIN_REPLACE, "ddx_pcg_finalize: unknown kind %d", kind);
+  PcgState S{st, ist, hist, R};
+  k_pcg_finalize<<<1, 64, 0, (cudaStream_t)stream>>>(S, kind);
+  DDX_LAUNCH_CHECK("ddx_pcg_finalize");
   return DDX_OK;
 }
 

@@ -104,6 +104,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   if (!last_cta_arrival(ticket)) return;
   double tot[2];
   final_sums<2>(partials, 1, red, tot, ticket);
+  if (park_totals<2>(S, tot)) return;
   if (threadIdx.x == 0) fin_rz(S, 0, tot[0], tot[1]);
 }
 
@@ -249,6 +250,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   if (!last_cta_arrival(ticket)) return;
   double tot[2];
   final_sums<2>(partials, R, red, tot, ticket);
+  if (park_totals<2>(S, tot)) return;
   if (threadIdx.x < R) fin_rz(S, threadIdx.x, tot[0], tot[1]);
 }
 

@@ -73,6 +73,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   if (!last_cta_arrival(ticket)) return;
   double tot[NV];
   final_sums<NV>(partials, 1, red, tot, ticket);
+  if (park_totals<NV>(S, tot)) return;
   int act = 0;
   if (threadIdx.x == 0) {
     if (MODE == DDX_SPMV_PQ) act = fin_pq(S, 0, tot[0]);
@@ -123,6 +124,7 @@ __global__ void __launch_bounds__(kThreads)
   if (!last_cta_arrival(ticket)) return;
   double tot[NV];
   final_sums<NV>(partials, R, red, tot, ticket);
+  if (park_totals<NV>(S, tot)) return;
   int act = 0;
   if (threadIdx.x < R) {
     const int jj = threadIdx.x;
@@ -206,6 +208,7 @@ __global__ void __launch_bounds__(kThreads)
   if (!last_cta_arrival(ticket)) return;
   double tot[NV];
   final_sums<NV>(partials, R, red, tot, ticket);
+  if (park_totals<NV>(S, tot)) return;
   int act = 0;
   if (threadIdx.x < R) {
     const int jj = threadIdx.x;

@@ -6,6 +6,7 @@ experiments/benchmark_batched_gemv.py and experiments/benchmark_bsrmv.py).
     python -m dd_solvers_b200.microbench spmv --problem p1 --n-el 2048 --rhs 16
     python -m dd_solvers_b200.microbench bsr --n-el 2048 --p 1
     python -m dd_solvers_b200.microbench solve --workload c5 --precision f16
+    python -m dd_solvers_b200.microbench gemv --ks 2,16,64,149
 
 ``apply`` times the Schwarz local-inverse apply (SIMT streaming kernel for
 R < 16, tensor-core kernel for R in {16, 32, 64} with BF16/FP16 blocks) on the
@@ -103,13 +104,25 @@ def bench_spmv(args) -> dict:
 
     from . import problems
 
+    from . import partition
+
     dev = torch.device("cuda")
     if args.problem == "p1":
-        A = problems.p1_jittered(args.n_el, 0.3, 1.0, 0).matrix  # n_el = nodes per side
+        P = problems.p1_jittered(args.n_el, 0.3, 1.0, 0)  # n_el = nodes per side
+        owner = partition.rcb_owner(P.coords, args.parts) if args.order == "parts" else None
     elif args.problem == "q1_2d":
-        A = problems.poisson2d(args.n_el).matrix
+        P = problems.poisson2d(args.n_el)
     else:
-        A = problems.diffusion3d_lognormal(args.n_el, 0).matrix
+        P = problems.diffusion3d_lognormal(args.n_el, 0)
+    A = P.matrix
+    if args.order == "parts":
+        # DOFs numbered part by part (each part's DOFs keep their order): the
+        # rows a CTA takes in turn then share most of their x rows
+        if args.problem != "p1":
+            owner, _ = partition.box_owner(P.interior_shape, args.parts)
+        perm = np.argsort(owner, kind="stable")
+        A = A[perm][:, perm].tocsr()
+        A.sort_indices()
     M = _SellMatrix(dd.csr_to_torch(A).to(dev))
     R = args.rhs or 1
     x = torch.randn(A.shape[0] * R, dtype=torch.float64, device=dev)
@@ -118,6 +131,7 @@ def bench_spmv(args) -> dict:
     n = A.shape[0]
     nbytes = A.nnz * 12 + (n + 1) * 4 + n * R * 16
     return {"kernel": "ddx_spmv_sell_f64" if R == 1 else "ddx_spmv_csr_f64", "problem": args.problem, "rhs": R,
+            "order": args.order,
             "n_dofs": n, "nnz": A.nnz, "ms_per_launch": ms, "algorithmic_bytes": nbytes,
             "achieved_gbs": nbytes / ms / 1e6, "frac_of_peak": nbytes / ms / 1e6 / _peak()}
 
@@ -148,6 +162,32 @@ def bench_bsr(args) -> dict:
     return {"kernel": "ddx_spmv_bsr", "dim": args.dim, "p": args.p, "bs": bs, "dofs": nbr * bs, "bsr_nnz": nnzb,
             "ms_per_launch": ms, "algorithmic_bytes": nbytes, "achieved_gbs": nbytes / ms / 1e6,
             "frac_of_peak": nbytes / ms / 1e6 / _peak()}
+
+
+def bench_gemv(args) -> dict:
+    """The reference op ``gemv_strided_batched`` on its own benchmark's shapes
+    (``experiments/benchmark_batched_gemv.py``): N = 2^27 // k^2 column-major
+    k x k matrices with random entries, every (matrix, vector) dtype pair the
+    op supports, for the k values of ``--ks``; CUDA-event time per launch."""
+    from dd_solvers_b200 import gemv_strided_batched
+
+    dev = torch.device("cuda")
+    pairs = [("f32", "f32"), ("f16", "f32"), ("bf16", "f32"), ("f64", "f64"), ("f32", "f64"), ("f16", "f64"),
+             ("bf16", "f64")]
+    rows = []
+    for k in [int(v) for v in args.ks.split(",")]:
+        n = 2 ** 27 // (k * k)
+        for a_dt, b_dt in pairs:
+            g = torch.Generator(device=dev).manual_seed(k)
+            A = torch.randn((n, k, k), device=dev, dtype=DT[a_dt], generator=g).transpose(1, 2).contiguous()
+            A = A.transpose(1, 2)  # column-major, as the reference's benchmark builds it
+            b = torch.randn((n, k), device=dev, dtype=DT[b_dt], generator=g)
+            ms = _time(lambda: gemv_strided_batched(A, b, True), args.reps)
+            nbytes = n * k * k * ELT[a_dt] + 2 * n * k * ELT[b_dt]
+            rows.append({"k": k, "n": n, "A_dtype": a_dt, "b_dtype": b_dt, "ms": ms,
+                         "achieved_gbs": nbytes / ms / 1e6, "frac_of_peak": nbytes / ms / 1e6 / _peak()})
+            del A, b
+    return {"kernel": "ddx_gemv_strided_batched", "rows": rows}
 
 
 def bench_solve(args) -> dict:
@@ -184,7 +224,8 @@ def bench_solve(args) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["apply", "spmv", "bsr", "solve"])
+    ap.add_argument("what", choices=["apply", "spmv", "bsr", "solve", "gemv"])
+    ap.add_argument("--ks", default="2,4,8,16,24,32,48,64,100,128,149", help="gemv: block sizes")
     ap.add_argument("--workload", default="c5", help="solve: workload name (c1..c5)")
     ap.add_argument("--p", type=int, default=1, help="bsr: DG polynomial degree")
     ap.add_argument("--dim", type=int, default=2, choices=[2, 3], help="bsr: triangles (2) or tetrahedra (3)")
@@ -192,6 +233,8 @@ def main():
     ap.add_argument("--problem", default="q1_3d", choices=["q1_3d", "p1", "q1_2d"],
                     help="spmv: 3D Q1 lognormal diffusion (n-el cells per side) or jittered P1 (n-el nodes per side)")
     ap.add_argument("--parts", type=int, default=8)
+    ap.add_argument("--order", default="natural", choices=["natural", "parts"],
+                    help="spmv: DOF numbering (natural grid order, or part by part with --parts)")
     ap.add_argument("--precision", default="bf16", choices=list(DT))
     ap.add_argument("--rhs", type=int, default=None, help="right-hand sides (apply/spmv: 1; solve: the workload's)")
     ap.add_argument("--reps", type=int, default=20)
@@ -203,7 +246,8 @@ def main():
     ap.add_argument("--stages", type=int, default=0, help="apply: ring depth of the symmetric tensor-core kernel "
                                                           "(2..6; 0: deepest that fits)")
     args = ap.parse_args()
-    out = {"apply": bench_apply, "spmv": bench_spmv, "bsr": bench_bsr, "solve": bench_solve}[args.what](args)
+    out = {"apply": bench_apply, "spmv": bench_spmv, "bsr": bench_bsr, "solve": bench_solve,
+           "gemv": bench_gemv}[args.what](args)
     print(json.dumps(out))
 
 

@@ -210,3 +210,65 @@ def overlapping_subdomains_device(crow, col, owner, n_parts: int, overlap: int):
         p, c, _v = spgemm_sorted(S, G)
         S = torch.sparse_csr_tensor(p, c, torch.ones(c.numel(), dtype=torch.float64, device=dev), (n_parts, n))
     return S.crow_indices().to(torch.int64), S.col_indices().to(torch.int32)
+
+
+def p0_restriction_device(owner, n_parts: int):
+    """``p0_restriction`` on the device: a torch CSR ``(n_parts x n)`` with a unit
+    entry at (owner[j], j), rows in DOF order (a stable sort of the owners)."""
+    import torch
+
+    dev = owner.device
+    own = owner.to(torch.int64)
+    n = own.numel()
+    cols = torch.argsort(own, stable=True)
+    ptr = torch.zeros(n_parts + 1, dtype=torch.int64, device=dev)
+    ptr[1:] = torch.cumsum(torch.bincount(own, minlength=n_parts), 0)
+    return torch.sparse_csr_tensor(ptr, cols, torch.ones(n, dtype=torch.float64, device=dev), (n_parts, n))
+
+
+def q1_coarse_restriction_device(dim: int, n_el: int, parts_per_axis: int, device):
+    """``q1_coarse_restriction`` on the device: every fine interior node takes the
+    multilinear weights of the 2^dim coarse nodes around it (the zero weights and
+    the Dirichlet coarse nodes dropped); the weights are multiplied slowest axis
+    first, as the Kronecker product of the 1D interpolations does, so the entries
+    are identical. Returns a torch CSR ``((parts_per_axis - 1)^dim x (n_el - 1)^dim)``
+    with sorted columns."""
+    import torch
+
+    P_ax = parts_per_axis
+    assert n_el % P_ax == 0
+    H = n_el // P_ax
+    m = n_el - 1
+    mc = P_ax - 1
+    # 1D: fine node p = 1..m -> (coarse index, weight) for its two neighbours
+    p = torch.arange(1, m + 1, dtype=torch.int64, device=device)
+    c0 = p // H
+    t = (p - c0 * H).to(torch.float64) / H
+    c1d = torch.stack([c0, c0 + 1], 1)                  # (m, 2)
+    w1d = torch.stack([1.0 - t, t], 1)
+    ok1d = (c1d >= 1) & (c1d <= mc) & (w1d != 0.0)
+    n = m ** dim
+    fine = torch.arange(n, dtype=torch.int64, device=device)
+    # per axis (slowest first) the fine coordinate of every fine node
+    coords = [(fine // (m ** (dim - 1 - a))) % m for a in range(dim)]
+    combos = torch.cartesian_prod(*[torch.arange(2, device=device)] * dim).reshape(-1, dim)  # (2^dim, dim)
+    rows, cols, vals = [], [], []
+    for cmb in combos.tolist():
+        w = None
+        c = torch.zeros(n, dtype=torch.int64, device=device)
+        ok = torch.ones(n, dtype=torch.bool, device=device)
+        for a in range(dim):
+            wa = w1d[coords[a], cmb[a]]
+            w = wa if w is None else w * wa
+            c = c * mc + (c1d[coords[a], cmb[a]] - 1)
+            ok &= ok1d[coords[a], cmb[a]]
+        rows.append(c[ok])
+        cols.append(fine[ok])
+        vals.append(w[ok])
+    rows, cols, vals = torch.cat(rows), torch.cat(cols), torch.cat(vals)
+    order = torch.argsort(rows * n + cols)
+    rows, cols, vals = rows[order], cols[order], vals[order]
+    n_c = mc ** dim
+    ptr = torch.zeros(n_c + 1, dtype=torch.int64, device=device)
+    ptr[1:] = torch.cumsum(torch.bincount(rows, minlength=n_c), 0)
+    return torch.sparse_csr_tensor(ptr, cols, vals, (n_c, n))

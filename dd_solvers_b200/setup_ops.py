@@ -93,7 +93,8 @@ def extract_blocks(crow, col, val, sub_ptr, sub_idx, first: int, last: int, kpad
     Returns ``(last-first, kpad, kpad)`` FP64 with the identity in the padding
     rows/columns (so every block stays invertible). Entries are located with a
     sorted-key search, the vectorised form of the reference's per-row scan
-    (``solvers.py:407-423``).
+    (``solvers.py:407-423``); a subdomain's indices may come in any order (a
+    sharded rank numbers its owned DOFs before its ghosts).
     """
     dev = crow.device
     n = crow.numel() - 1
@@ -111,7 +112,9 @@ def extract_blocks(crow, col, val, sub_ptr, sub_idx, first: int, last: int, kpad
     s_loc = torch.repeat_interleave(torch.arange(B, device=dev), ks)
     lrow = pos - sub_ptr[first:last].to(torch.int64)[s_loc]
     g = sub_idx[p0:p1].to(torch.int64)
-    mkey = s_loc * n + g  # sorted ascending
+    mkey = s_loc * n + g
+    order = torch.argsort(mkey, stable=True)  # the identity for ascending index lists
+    mkey = mkey[order]
     rs = crow[g].to(torch.int64)
     cnt = crow[g + 1].to(torch.int64) - rs
     e_row = torch.repeat_interleave(torch.arange(p1 - p0, device=dev), cnt)
@@ -122,7 +125,7 @@ def extract_blocks(crow, col, val, sub_ptr, sub_idx, first: int, last: int, kpad
     hit = torch.searchsorted(mkey, key)
     hit_c = torch.clamp(hit, max=mkey.numel() - 1)
     ok = mkey[hit_c] == key
-    lcol = hit_c - (sub_ptr[first:last].to(torch.int64)[s_loc[e_row]] - p0)
+    lcol = order[hit_c] - (sub_ptr[first:last].to(torch.int64)[s_loc[e_row]] - p0)
     out[s_loc[e_row][ok], lrow[e_row][ok], lcol[ok]] = val[e_idx][ok].to(torch.float64)
     return out
 

@@ -46,6 +46,7 @@ from .bsr import FastBSR
 from .cusparse import csr_to_bsr, gather_csr, sort_csr
 from .gemv import gemv_strided_batched
 from . import cudss
+from . import partition
 
 Metadata = dict[str, Any]
 
@@ -228,23 +229,40 @@ class Inv(DenseBatchSolver):
 # Schwarz operators
 # ---------------------------------------------------------------------------
 
-def _to_scipy_R(R0, n: int) -> sps.csr_matrix:
-    if R0 is None:
-        return None
+def _restriction_dev(R0, n: int, device):
+    """A coarse restriction (SciPy, or torch CSR on any device) as a sorted
+    torch CSR ``(crow int64, col int64, val f64, n_c)`` on ``device``; a torch
+    input stays on the device (no host copy)."""
     if isinstance(R0, torch.Tensor):
-        R0 = so.scipy_csr(R0)
+        crow = R0.crow_indices().to(device, torch.int64)
+        col = R0.col_indices().to(device, torch.int64)
+        val = R0.values().to(device, torch.float64)
+        n_c = int(R0.shape[0])
+        assert int(R0.shape[1]) == n
+        # sort the columns of every row (a no-op for sorted input)
+        rows = torch.repeat_interleave(torch.arange(n_c, device=device), crow[1:] - crow[:-1])
+        order = torch.argsort(rows * n + col)
+        return crow, col[order], val[order], n_c
     R0 = sps.csr_matrix(R0, dtype=np.float64)
     R0.sort_indices()
     assert R0.shape[1] == n
-    return R0
+    return (torch.as_tensor(R0.indptr.astype(np.int64), device=device),
+            torch.as_tensor(R0.indices.astype(np.int64), device=device),
+            torch.as_tensor(R0.data, device=device), R0.shape[0])
 
 
-def _csr_dev(M: sps.csr_matrix, device):
-    M = sps.csr_matrix(M)
-    M.sort_indices()
-    return (torch.as_tensor(M.indptr.astype(np.int32), device=device),
-            torch.as_tensor(M.indices.astype(np.int32), device=device),
-            torch.as_tensor(M.data.astype(np.float64), device=device))
+def _transpose_dev(crow, col, val, n_rows: int, n_cols: int):
+    """CSR transpose on the device by a sort of (column, row): columns of every
+    row of the result ascending."""
+    rows = torch.repeat_interleave(torch.arange(n_rows, device=crow.device), crow[1:] - crow[:-1])
+    order = torch.argsort(col * n_rows + rows)
+    ptr = torch.zeros(n_cols + 1, dtype=torch.int64, device=crow.device)
+    ptr[1:] = torch.cumsum(torch.bincount(col, minlength=n_cols), 0)
+    return ptr, rows[order], val[order]
+
+
+def _i32(crow, col, val):
+    return crow.to(torch.int32), col.to(torch.int32), val
 
 
 class SchwarzOperator(SparseSolver):
@@ -289,6 +307,9 @@ class SchwarzOperator(SparseSolver):
         self.mapped_restriction = None
         self._mapped_choice = {}
         self.autotune = True
+        # SIMT apply on upper-triangle tiles with few blocks: at most this many
+        # ylocal slices per block (1 keeps ylocal one row per subdomain entry)
+        self.max_parts = 8
 
     # -- setup -------------------------------------------------------------
     def setup(self, matrix: torch.Tensor, dofs_per_solver: int | None = None,
@@ -316,53 +337,51 @@ class SchwarzOperator(SparseSolver):
             sub_ptr, sub_idx = np.arange(self.n_solvers + 1, dtype=np.int64) * self.dofs_per_solver, \
                 np.arange(n, dtype=np.int32)
             assert sub_ptr[-1] == n, "dofs_per_solver * n_solvers must equal the matrix size"
-            solvers_to_coarse = np.repeat(np.arange(self.n_coarse), spc)
-            owner_np = np.repeat(np.arange(self.n_solvers), self.dofs_per_solver)
-            R0 = sps.csr_matrix((np.ones(n), (solvers_to_coarse[owner_np], np.arange(n))),
-                                shape=(self.n_coarse, n))
-            R0.sort_indices()
+            # DOF j -> coarse group of its solver j // dofs_per_solver
+            solvers_to_coarse = torch.repeat_interleave(torch.arange(self.n_coarse, device=self.device),
+                                                        torch.as_tensor(spc, device=self.device))
+            grp = solvers_to_coarse[torch.arange(n, device=self.device) // self.dofs_per_solver]
+            R0 = partition.p0_restriction_device(grp, self.n_coarse)
         else:
             sub_ptr, sub_idx = (np.asarray(t.cpu() if isinstance(t, torch.Tensor) else t) for t in subdomains)
             sub_ptr = sub_ptr.astype(np.int64)
             sub_idx = sub_idx.astype(np.int32)
             self.n_solvers = len(sub_ptr) - 1
             if coarse_restriction is not None:
-                R0 = _to_scipy_R(coarse_restriction, n)
+                R0 = coarse_restriction
             elif owner is not None:
-                own = np.asarray(owner.cpu() if isinstance(owner, torch.Tensor) else owner)
-                R0 = sps.csr_matrix((np.ones(n), (own.astype(np.int64), np.arange(n))),
-                                    shape=(int(own.max()) + 1, n))
-                R0.sort_indices()
+                own = torch.as_tensor(owner, device=self.device).to(torch.int64)
+                R0 = partition.p0_restriction_device(own, int(own.max().item()) + 1)
             else:
                 R0 = None
-            self.n_coarse = 0 if R0 is None else R0.shape[0]
         if self.coarse_solver is None:
             R0 = None
-            self.n_coarse = 0
-        self._R0_sp = R0
+        R0 = None if R0 is None else _restriction_dev(R0, n, self.device)
+        self.n_coarse = 0 if R0 is None else R0[3]
         if self.collect_timings:
             events[1].record()
 
         # coarse space
         if R0 is not None:
-            # coarse products on the device: A_R = R0 A (also the hybrid's
-            # restriction), A_C = A_R R0^T
+            # coarse space on the device: R0, P = R0^T, A_R = R0 A (also the
+            # hybrid's restriction), A_C = A_R R0^T
+            r_crow, r_col, r_val, n_c = R0
+            p_crow, p_col, p_val = _transpose_dev(r_crow, r_col, r_val, n_c, n)
             A_t = torch.sparse_csr_tensor(crow, col, val, matrix.shape)
-            R0_t = so.csr_torch(R0, self.device)
+            R0_t = torch.sparse_csr_tensor(r_crow, r_col, r_val, (n_c, n))
             ar = so.spgemm_sorted(R0_t, A_t)
             self._AR_dev = (ar[0].to(torch.int32), ar[1].to(torch.int32), ar[2])
-            AR_t = torch.sparse_csr_tensor(ar[0], ar[1], ar[2], (R0.shape[0], n))
-            ac = so.spgemm_sorted(AR_t, so.csr_torch(R0.T.tocsr(), self.device))
-            Ac_t = torch.sparse_csr_tensor(ac[0], ac[1], ac[2], (R0.shape[0], R0.shape[0]))
+            AR_t = torch.sparse_csr_tensor(ar[0], ar[1], ar[2], (n_c, n))
+            ac = so.spgemm_sorted(AR_t, torch.sparse_csr_tensor(p_crow, p_col, p_val, (n, n_c)))
+            Ac_t = torch.sparse_csr_tensor(ac[0], ac[1], ac[2], (n_c, n_c))
             del A_t, R0_t, AR_t
             self.coarse_solver.setup(Ac_t)
-            self._R0 = _csr_dev(R0, self.device)
-            P = R0.T.tocsr()
-            if P.nnz == P.shape[0] and bool((np.diff(P.indptr) == 1).all()) and bool((P.data == 1.0).all()):
+            self._R0 = _i32(r_crow, r_col, r_val)
+            if p_col.numel() == n and bool(((p_crow[1:] - p_crow[:-1]) == 1).all()) and bool((p_val == 1.0).all()):
                 # P0 aggregates: one unit entry per DOF, passed as its column alone
-                self._P = (None, torch.as_tensor(P.indices.astype(np.int32), device=self.device), None)
+                self._P = (None, p_col.to(torch.int32), None)
             else:
-                self._P = _csr_dev(P, self.device)
+                self._P = _i32(p_crow, p_col, p_val)
             self._fused_coarse = isinstance(self.coarse_solver, CUDSS)
         if self.collect_timings:
             events[2].record()
@@ -468,7 +487,7 @@ class SchwarzOperator(SparseSolver):
         if self.store.layout == "sym" and self.n_solvers:
             nsm = torch.cuda.get_device_properties(self.device).multi_processor_count
             if self.n_solvers < 2 * nsm:
-                self.parts = int(min(8, -(-2 * nsm // self.n_solvers)))
+                self.parts = int(min(self.max_parts, -(-2 * nsm // self.n_solvers)))
         # equal contiguous non-overlapping subdomains in DOF order (the reference's
         # layout): ylocal is DOF-ordered and the combine needs no transpose map
         identity = (int(self.sub_idx.numel()) == self.n and

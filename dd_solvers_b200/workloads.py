@@ -44,7 +44,8 @@ def build_problem(spec: dict, seed: int = 0, device=None):
     workload (numpy / SciPy). With a CUDA ``device`` the RCB bisection and the
     overlap growth run there (``partition.rcb_owner_device``,
     ``overlapping_subdomains_device``: identical output, tested) and are copied
-    back."""
+    back, and the coarse restriction ``R0`` is built there and stays there (a
+    torch CSR; ``setup_ops.scipy_csr`` gives the SciPy copy)."""
     from . import partition, problems
 
     t0 = time.time()
@@ -78,7 +79,14 @@ def build_problem(spec: dict, seed: int = 0, device=None):
         sub_ptr, sub_idx = sp.cpu().numpy(), si.cpu().numpy()
     else:
         sub_ptr, sub_idx = partition.overlapping_subdomains(A, owner, nparts, spec.get("overlap", 1))
-    if spec["coarse"] == "q1":
+    if device is not None:
+        import torch
+
+        if spec["coarse"] == "q1":
+            R0 = partition.q1_coarse_restriction_device(3, spec["n_el"], spec["parts"], device)
+        else:
+            R0 = partition.p0_restriction_device(torch.as_tensor(owner, device=device), nparts)
+    elif spec["coarse"] == "q1":
         R0 = partition.q1_coarse_restriction(3, spec["n_el"], spec["parts"])
     else:
         R0 = partition.p0_restriction(owner, nparts)

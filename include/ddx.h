@@ -46,7 +46,9 @@ enum ddx_dtype { DDX_F64 = 0, DDX_F32 = 1, DDX_BF16 = 2, DDX_F16 = 3 };
  */
 enum {
   DDX_ST_RHO = 0, DDX_ST_RHO_PREV = 1, DDX_ST_ZQ = 2, DDX_ST_PQ = 3, DDX_ST_ALPHA = 4,
-  DDX_ST_BETA = 5, DDX_ST_RR = 6, DDX_ST_ATOL = 7, DDX_ST_BB = 8, DDX_ST_COUNT = 9
+  DDX_ST_BETA = 5, DDX_ST_RR = 6, DDX_ST_ATOL = 7, DDX_ST_BB = 8,
+  DDX_ST_T0 = 9, DDX_ST_T1 = 10, /* parked column totals (DDX_G_DEFER) */
+  DDX_ST_COUNT = 11
 };
 enum { DDX_IST_ACTIVE = 0, DDX_IST_ITERS = 1, DDX_IST_COUNT = 2 };
 enum {
@@ -54,7 +56,24 @@ enum {
   DDX_G_MAXITER = 1,   /* update limit per RHS */
   DDX_G_FLEXIBLE = 2,  /* 1: Polak-Ribiere beta, 0: Fletcher-Reeves */
   DDX_G_BREAKDOWN = 3, /* set when p.q <= 0 stopped a RHS */
-  DDX_G_COUNT = 4
+  DDX_G_DEFER = 4,     /* 1: reductions park their totals for ddx_pcg_finalize */
+  DDX_G_COUNT = 5
+};
+/* Deferred reductions (a solve sharded over ranks): with DDX_G_DEFER set (the
+ * caller writes 1 after ddx_pcg_reset, which clears it), every fused reduction
+ * of this header (SpMV modes PQ / RES_INIT / RES_REPLACE, ddx_pcg_update_xr,
+ * ddx_pcg_update_xr_pack16, ddx_pcg_dots_rz, ddx_schwarz_combine with dots)
+ * stores its column totals of this rank's rows in st slots DDX_ST_T0 (and
+ * DDX_ST_T1: r.r for RES_INIT's b.b, z.q for the r.z pair) instead of running
+ * the step-length / stop-test epilogue. The caller sums those 2R doubles over
+ * the ranks (one all-reduce) and then calls ddx_pcg_finalize with the kind of
+ * the reduction, which runs the same epilogue on the summed totals. */
+enum {
+  DDX_FIN_RZ = 0,      /* T0 = r.z, T1 = z.q      -> beta        */
+  DDX_FIN_PQ = 1,      /* T0 = p.q                -> alpha       */
+  DDX_FIN_RR = 2,      /* T0 = r.r                -> stop test   */
+  DDX_FIN_INIT = 3,    /* T0 = r.r, T1 = b.b      -> tolerance, first stop test */
+  DDX_FIN_REPLACE = 4  /* T0 = r.r (replaced r)   -> stop test   */
 };
 enum { DDX_TICKETS = 16 };
 
@@ -83,6 +102,13 @@ int ddx_pcg_update_p(int64_t n, int R, const double* z, double* p, const double*
 int ddx_pcg_update_xr(int64_t n, int R, double* x, double* r, const double* p, const double* q,
                       double* st, int* ist, double* hist, double* partials, unsigned int* tickets,
                       ddx_stream_t stream);
+/* The epilogue of a deferred reduction (DDX_G_DEFER) on the totals in st slots
+ * DDX_ST_T0 / DDX_ST_T1, after the caller summed them over the ranks: kind is a
+ * DDX_FIN_* value. One CTA; same arithmetic as the in-kernel epilogue, so every
+ * rank that holds the same totals reaches the same alpha, beta and stop
+ * decisions. Replaces the host-side scalar steps of CG.solve (solvers.py:244-267)
+ * for a solve whose vectors are split over ranks. */
+int ddx_pcg_finalize(int R, int kind, double* st, int* ist, double* hist, ddx_stream_t stream);
 /* ddx_pcg_update_xr for R in {16, 32, 64} (16-byte aligned vectors) that also
  * writes r, rounded to BF16 with scale 1, into the tensor-core B panels of the
  * next local apply (ddx_pack_panels16's layout with one term): DOF d's row goes

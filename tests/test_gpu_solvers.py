@@ -230,6 +230,30 @@ def test_overlapping_fp64_matches_oracle(cuda, case, kind):
     assert np.linalg.norm(xk - xr) <= 1e-10 * np.linalg.norm(xr), np.linalg.norm(xk - xr) / np.linalg.norm(xr)
 
 
+@pytest.mark.parametrize("coarse", ["p0", "q1"])
+def test_device_built_restriction_solves_bitwise_like_scipy(cuda, coarse):
+    """A coarse restriction built on the device (torch CSR, no host copy) gives
+    the same coarse products and the same solve, bit for bit, as the SciPy one."""
+    import dd_solvers_b200 as dd
+    from dd_solvers_b200 import partition
+
+    P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(3, 16, 4, kappa_seed=3, coarse=coarse)
+    R0_dev = (partition.q1_coarse_restriction_device(3, 16, 4, cuda) if coarse == "q1" else
+              partition.p0_restriction_device(torch.as_tensor(owner, device=cuda), nparts))
+    b = torch.as_tensor(np.random.default_rng(5).uniform(-1, 1, A.shape[0]), device=cuda)
+    out = []
+    for R in (R0, R0_dev):
+        cg = dd.CG(dd.HybridSchwarz(torch.float64, dd.Inv(), dd.CUDSS()), rtol=1e-9)
+        cg.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R, block_size=1)
+        x, meta = cg.solve(b)
+        pc = cg.preconditioner
+        out.append((x, meta["iterations"], pc._AR_dev, pc._P))
+    (x0, i0, ar0, p0), (x1, i1, ar1, p1) = out
+    assert i0 == i1 and torch.equal(x0, x1)
+    assert all(torch.equal(u, v) for u, v in zip(ar0, ar1))
+    assert all((u is None and v is None) or torch.equal(u, v) for u, v in zip(p0, p1))
+
+
 @pytest.mark.parametrize("prec", [torch.float32, torch.bfloat16, torch.float16])
 @pytest.mark.parametrize("kind", ["additive", "hybrid"])
 def test_mixed_precision_reaches_fp64_accuracy(cuda, prec, kind):

@@ -1,4 +1,5 @@
 """Host-side logic on CPU: assemblers, partitions, coarse spaces, setup layouts, C ABI."""
+import ctypes
 import itertools
 import os
 import re
@@ -131,8 +132,16 @@ def test_sell32_roundtrip():
     assert np.array_equal(D, A.toarray())
 
 
-def test_extract_blocks_matches_scipy():
+@pytest.mark.parametrize("shuffled", [False, True])
+def test_extract_blocks_matches_scipy(shuffled):
+    """Blocks A[idx][:, idx] for ascending index lists and for lists in any
+    order (a sharded rank's local numbering)."""
     P, A, owner, nparts, sub_ptr, sub_idx, R0 = p1_case(20, 4)
+    if shuffled:
+        rng = np.random.default_rng(3)
+        sub_idx = sub_idx.copy()
+        for i in range(nparts):
+            rng.shuffle(sub_idx[sub_ptr[i]:sub_ptr[i + 1]])
     crow = torch.as_tensor(A.indptr.astype(np.int64))
     col = torch.as_tensor(A.indices.astype(np.int64))
     val = torch.as_tensor(A.data)
@@ -199,6 +208,14 @@ def test_capi_argument_checks_without_gpu():
     assert lib.ddx_spmv_sell_f64(100, 3, None, None, None, None, None, None, None, 0, None, None, None, None,
                                  None, None) == 1
     assert lib.ddx_partials_len(64) == 592 * 4 * 64
+    # the deferred-reduction epilogue checks its arguments before any launch
+    assert lib.ddx_pcg_finalize(3, _lib.FIN_RR, None, None, None, None) == 1
+    assert lib.ddx_pcg_finalize(4, _lib.FIN_RR, None, None, None, None) == 1
+    assert b"null state" in lib.ddx_last_error()
+    one = ctypes.c_double(0.0)
+    flag = ctypes.c_int(0)
+    assert lib.ddx_pcg_finalize(4, 9, ctypes.byref(one), ctypes.byref(flag), ctypes.byref(one), None) == 1
+    assert b"unknown kind 9" in lib.ddx_last_error()
 
 
 def test_solver_rejects_cpu_tensors():
@@ -308,6 +325,35 @@ def test_device_partitioning_matches_host(parts):
             overlap)
         assert np.array_equal(sp, sp_t.numpy()) and np.array_equal(si, si_t.numpy())
 
+
+@pytest.mark.parametrize("dim,n_el,parts", [(2, 12, 3), (2, 30, 5), (3, 18, 3), (3, 32, 4)])
+def test_device_coarse_restrictions_match_host(dim, n_el, parts):
+    """The Q1 and P0 coarse restrictions built in torch (CPU tensors here, cuda
+    in the bench) equal the SciPy ones entry for entry, and the device CSR
+    transpose the Schwarz setup uses equals SciPy's."""
+    import torch
+
+    from dd_solvers_b200 import partition
+    from dd_solvers_b200 import solvers as S
+    from dd_solvers_b200.setup_ops import scipy_csr
+
+    a = partition.q1_coarse_restriction(dim, n_el, parts)
+    b = scipy_csr(partition.q1_coarse_restriction_device(dim, n_el, parts, "cpu"))
+    assert np.array_equal(a.indptr, b.indptr) and np.array_equal(a.indices, b.indices)
+    assert np.array_equal(a.data, b.data)
+    own = np.random.default_rng(dim * n_el).integers(0, parts * parts, (n_el - 1) ** dim)
+    a0 = partition.p0_restriction(own, parts * parts)
+    b0 = scipy_csr(partition.p0_restriction_device(torch.as_tensor(own), parts * parts))
+    assert np.array_equal(a0.indptr, b0.indptr) and np.array_equal(a0.indices, b0.indices)
+    assert np.array_equal(a0.data, b0.data)
+    crow, col, val, n_c = S._restriction_dev(partition.q1_coarse_restriction_device(dim, n_el, parts, "cpu"),
+                                             a.shape[1], "cpu")
+    assert n_c == a.shape[0]
+    pt_crow, pt_col, pt_val = S._transpose_dev(crow, col, val, n_c, a.shape[1])
+    At = a.T.tocsr()
+    At.sort_indices()
+    assert np.array_equal(pt_crow.numpy(), At.indptr) and np.array_equal(pt_col.numpy(), At.indices)
+    assert np.array_equal(pt_val.numpy(), At.data)
 
 
 def test_spd_guard_keeps_rounded_blocks_positive_definite():
