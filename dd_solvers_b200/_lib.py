@@ -19,7 +19,8 @@ F64, F32, BF16, F16 = 0, 1, 2, 3
 DTYPE_CODE = {torch.float64: F64, torch.float32: F32, torch.bfloat16: BF16, torch.float16: F16}
 
 # PCG state layout (ddx.h)
-ST_RHO, ST_RHO_PREV, ST_ZQ, ST_PQ, ST_ALPHA, ST_BETA, ST_RR, ST_ATOL, ST_BB, ST_T0, ST_T1, ST_COUNT = range(12)
+(ST_RHO, ST_RHO_PREV, ST_ZQ, ST_PQ, ST_ALPHA, ST_BETA, ST_RR, ST_ATOL, ST_BB, ST_T0, ST_T1, ST_ALPHA_X,
+ ST_COUNT) = range(13)
 IST_ACTIVE, IST_ITERS, IST_COUNT = range(3)
 G_NACTIVE, G_MAXITER, G_FLEXIBLE, G_BREAKDOWN, G_DEFER, G_COUNT = range(6)
 FIN_RZ, FIN_PQ, FIN_RR, FIN_INIT, FIN_REPLACE = range(5)
@@ -38,6 +39,8 @@ _SIGS = {
     "ddx_device_error": (_I, [C.POINTER(_I)]),
     "ddx_pcg_reset": (_I, [_I, _P, _P, _I, _I, _D, _D, _P]),
     "ddx_pcg_update_p": (_I, [_I64, _I, _P, _P, _P, _P, _P]),
+    "ddx_pcg_update_px": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P]),
+    "ddx_pcg_flush_x": (_I, [_I64, _I, _P, _P, _P, _P, _P]),
     "ddx_pcg_update_xr": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ddx_pcg_finalize": (_I, [_I, _I, _P, _P, _P, _P]),
     "ddx_pcg_update_xr_pack16": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
@@ -59,6 +62,8 @@ _SIGS = {
     "ddx_schwarz_combine": (_I, [_I64, _I, _P, _P, _P, _I, _P, _P, _P, _P, _P, _D, _P, _I, _P, _P, _P, _P,
                                  _P, _P, _P]),
     "ddx_coarse_gemv_f64": (_I, [_I, _I, _P, _P, _P, _P, _P]),
+    "ddx_schwarz_combine_update": (_I, [_I64, _I, _P, _P, _P, _I, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P, _P]),
+    "ddx_schwarz_restrict_sub": (_I, [_I64, _I64, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P]),
     "ddx_nd_order": (_I, [_I64, _P, _P, _I, _P, _P, _P, _P]),
     "ddx_spmv_csr_lanes_f64": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P]),
     "ddx_spmv_csr_lanes": (_I, [_I64, _I, _P, _P, _P, _P, _I, _P, _P]),

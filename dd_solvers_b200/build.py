@@ -10,6 +10,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -47,15 +48,19 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
     if up_to_date() and not extra:
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
-    objs = []
     cc = nvcc()
-    for src in sources():
-        obj = os.path.join(OUT_DIR, os.path.basename(src).replace(".cu", ".o"))
+    objs = [os.path.join(OUT_DIR, os.path.basename(src).replace(".cu", ".o")) for src in sources()]
+
+    def compile_one(src: str, obj: str) -> None:
         cmd = [cc, *ARCH, *FLAGS, *(extra or []), "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+
+    # the translation units compile independently: one nvcc per host core
+    with ThreadPoolExecutor(max_workers=max(1, min(len(objs), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(compile_one, src, obj) for src, obj in zip(sources(), objs)]:
+            f.result()
     cmd = [cc, *ARCH, "-rdc=true", "-shared", "-o", LIB + ".tmp", *objs, "-lcudart"]
     subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)

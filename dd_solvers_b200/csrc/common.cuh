@@ -204,6 +204,7 @@ __device__ __forceinline__ void fin_rz(PcgState S, int j, double rho, double zq)
 
 __device__ __forceinline__ int fin_pq(PcgState S, int j, double pq) {
   S.s(DDX_ST_PQ, j) = pq;
+  S.s(DDX_ST_ALPHA_X, j) = 0.0;  // a parked x step was applied by the p update before this product
   int act = S.a(DDX_IST_ACTIVE, j);
   double alpha = 0.0;
   if (act) {
@@ -220,7 +221,10 @@ __device__ __forceinline__ int fin_pq(PcgState S, int j, double pq) {
   return act;
 }
 
-__device__ __forceinline__ int fin_rr(PcgState S, int j, double rr) {
+// defer_x: x was not updated with this alpha; park it for the next p update
+// (inactive RHS have alpha = 0 here, so parking is harmless for them).
+__device__ __forceinline__ int fin_rr(PcgState S, int j, double rr, bool defer_x = false) {
+  if (defer_x) S.s(DDX_ST_ALPHA_X, j) = S.s(DDX_ST_ALPHA, j);
   int act = S.a(DDX_IST_ACTIVE, j);
   if (act) {
     const int it = ++S.a(DDX_IST_ITERS, j);

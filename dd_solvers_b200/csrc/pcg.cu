@@ -54,17 +54,43 @@ __global__ void k_pcg_finalize(PcgState S, int kind) {
   if (kind != DDX_FIN_RZ) publish_nactive(S, act);
 }
 
-// p = z + beta p
+// p = z + beta p; with x: first x += alpha_x p (a deferred x update)
 __global__ void k_update_p(int64_t n, int R, const double* __restrict__ z, double* __restrict__ p,
-                           const double* __restrict__ st, const int* __restrict__ ist) {
+                           double* __restrict__ x, const double* __restrict__ st, const int* __restrict__ ist) {
   if (n_active(ist, R) == 0) return;
   const int64_t total = n * R;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int j = threadIdx.x % R;  // stride is a multiple of R
   const double beta = st[DDX_ST_BETA * R + j];
+  if (x != nullptr) {
+    const double ax = st[DDX_ST_ALPHA_X * R + j];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+      const double pi = p[i];
+      x[i] = fma(ax, pi, x[i]);
+      p[i] = fma(beta, pi, z[i]);
+    }
+    return;
+  }
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
     p[i] = fma(beta, p[i], z[i]);
   }
+}
+
+// x += alpha_x p, the parked step of a deferred x update, then alpha_x = 0
+// (by the last CTA, after every CTA has read it). Runs even when no RHS is
+// active: it completes the solution after the last update.
+__global__ void __launch_bounds__(kThreads) k_flush_x(int64_t n, int R, double* __restrict__ x,
+                                                      const double* __restrict__ p, double* st,
+                                                      unsigned int* ticket) {
+  const int64_t total = n * R;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int j = threadIdx.x % R;
+  const double ax = st[DDX_ST_ALPHA_X * R + j];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
+    x[i] = fma(ax, p[i], x[i]);
+  if (!last_cta_arrival(ticket)) return;
+  if (threadIdx.x < R) st[DDX_ST_ALPHA_X * R + threadIdx.x] = 0.0;
+  if (threadIdx.x == 0) *ticket = 0u;
 }
 
 // x += alpha p; r -= alpha q; rr = ||r||^2 -> stop test
@@ -79,11 +105,11 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(int64_t n, PcgState S, d
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   const int j = threadIdx.x % R;
   const double alpha = S.st[DDX_ST_ALPHA * R + j];
+  const bool defer_x = x == nullptr;  // x += alpha p left to the next p update
   double acc[1] = {0.0};
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-    const double xi = fma(alpha, p[i], x[i]);
+    if (!defer_x) x[i] = fma(alpha, p[i], x[i]);
     const double ri = fma(-alpha, q[i], r[i]);
-    x[i] = xi;
     r[i] = ri;
     acc[0] = fma(ri, ri, acc[0]);
   }
@@ -93,7 +119,7 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(int64_t n, PcgState S, d
   final_sums<1>(partials, R, red, tot, ticket);
   if (park_totals<1>(S, tot)) return;
   int act = 0;
-  if (threadIdx.x < R) act = fin_rr(S, threadIdx.x, tot[0]);
+  if (threadIdx.x < R) act = fin_rr(S, threadIdx.x, tot[0], defer_x);
   publish_nactive(S, act);
 }
 
@@ -127,15 +153,18 @@ __global__ void __launch_bounds__(kThreads) k_update_xr_pack(int64_t n, PcgState
   double acc0 = 0.0, acc1 = 0.0;
   const int64_t total = n * TPR;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const bool defer_x = x == nullptr;  // x += alpha p left to the next p update
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
     const int64_t d = i / TPR;
     const int64_t o = d * R + 2 * c2;
-    const double2 xv = *reinterpret_cast<const double2*>(x + o);
-    const double2 pv = *reinterpret_cast<const double2*>(p + o);
+    if (!defer_x) {
+      const double2 xv = *reinterpret_cast<const double2*>(x + o);
+      const double2 pv = *reinterpret_cast<const double2*>(p + o);
+      *reinterpret_cast<double2*>(x + o) = make_double2(fma(a0, pv.x, xv.x), fma(a1, pv.y, xv.y));
+    }
     const double2 rv = *reinterpret_cast<const double2*>(r + o);
     const double2 qv = *reinterpret_cast<const double2*>(q + o);
     const double2 rn = make_double2(fma(-a0, qv.x, rv.x), fma(-a1, qv.y, rv.y));
-    *reinterpret_cast<double2*>(x + o) = make_double2(fma(a0, pv.x, xv.x), fma(a1, pv.y, xv.y));
     *reinterpret_cast<double2*>(r + o) = rn;
     acc0 = fma(rn.x, rn.x, acc0);
     acc1 = fma(rn.y, rn.y, acc1);
@@ -157,7 +186,7 @@ __global__ void __launch_bounds__(kThreads) k_update_xr_pack(int64_t n, PcgState
   final_sums<1>(partials, R, red, tot, ticket);
   if (park_totals<1>(S, tot)) return;
   int act = 0;
-  if (threadIdx.x < R) act = fin_rr(S, threadIdx.x, tot[0]);
+  if (threadIdx.x < R) act = fin_rr(S, threadIdx.x, tot[0], defer_x);
   publish_nactive(S, act);
 }
 
@@ -241,8 +270,28 @@ int ddx_pcg_update_p(int64_t n, int R, const double* z, double* p, const double*
   DDX_REQUIRE(n >= 0 && z && p && st && ist, "ddx_pcg_update_p: bad arguments");
   if (n == 0) return DDX_OK;
   int grid = (int)std::min<int64_t>(ceil_div(n * R, kThreads), 148 * 16);
-  k_update_p<<<grid, kThreads, 0, (cudaStream_t)stream>>>(n, R, z, p, st, ist);
+  k_update_p<<<grid, kThreads, 0, (cudaStream_t)stream>>>(n, R, z, p, nullptr, st, ist);
   DDX_LAUNCH_CHECK("ddx_pcg_update_p");
+  return DDX_OK;
+}
+
+int ddx_pcg_update_px(int64_t n, int R, const double* z, double* p, double* x, const double* st, const int* ist,
+                      ddx_stream_t stream) {
+  DDX_REQUIRE(valid_rhs_count(R), "ddx_pcg_update_px: unsupported R=%d", R);
+  DDX_REQUIRE(n >= 0 && z && p && x && st && ist, "ddx_pcg_update_px: bad arguments");
+  if (n == 0) return DDX_OK;
+  int grid = (int)std::min<int64_t>(ceil_div(n * R, kThreads), 148 * 16);
+  k_update_p<<<grid, kThreads, 0, (cudaStream_t)stream>>>(n, R, z, p, x, st, ist);
+  DDX_LAUNCH_CHECK("ddx_pcg_update_px");
+  return DDX_OK;
+}
+
+int ddx_pcg_flush_x(int64_t n, int R, double* x, const double* p, double* st, unsigned int* tickets,
+                    ddx_stream_t stream) {
+  DDX_REQUIRE(valid_rhs_count(R), "ddx_pcg_flush_x: unsupported R=%d", R);
+  DDX_REQUIRE(n >= 0 && x && p && st && tickets, "ddx_pcg_flush_x: bad arguments");
+  k_flush_x<<<red_grid(n * R), kThreads, 0, (cudaStream_t)stream>>>(n, R, x, p, st, tickets + 5);
+  DDX_LAUNCH_CHECK("ddx_pcg_flush_x");
   return DDX_OK;
 }
 
@@ -250,7 +299,7 @@ int ddx_pcg_update_xr(int64_t n, int R, double* x, double* r, const double* p, c
                       double* st, int* ist, double* hist, double* partials, unsigned int* tickets,
                       ddx_stream_t stream) {
   DDX_REQUIRE(valid_rhs_count(R), "ddx_pcg_update_xr: unsupported R=%d", R);
-  DDX_REQUIRE(n >= 0 && x && r && p && q && st && ist && hist && partials && tickets,
+  DDX_REQUIRE(n >= 0 && r && p && q && st && ist && hist && partials && tickets,
               "ddx_pcg_update_xr: bad arguments");
   PcgState S{st, ist, hist, R};
   k_update_xr<<<red_grid(n * R), kThreads, 0, (cudaStream_t)stream>>>(n, S, x, r, p, q, partials,
@@ -263,7 +312,7 @@ int ddx_pcg_update_xr_pack16(int64_t n, int R, double* x, double* r, const doubl
                              const int* pan_ptr, const int64_t* pan_row, void* b16, double* st, int* ist,
                              double* hist, double* partials, unsigned int* tickets, ddx_stream_t stream) {
   DDX_REQUIRE(R == 16 || R == 32 || R == 64, "ddx_pcg_update_xr_pack16: R must be 16, 32 or 64 (got %d)", R);
-  DDX_REQUIRE(n >= 0 && x && r && p && q && pan_ptr && pan_row && b16 && st && ist && hist && partials && tickets,
+  DDX_REQUIRE(n >= 0 && r && p && q && pan_ptr && pan_row && b16 && st && ist && hist && partials && tickets,
               "ddx_pcg_update_xr_pack16: bad arguments");
   DDX_REQUIRE(((uintptr_t)x & 15u) == 0 && ((uintptr_t)r & 15u) == 0 && ((uintptr_t)p & 15u) == 0 &&
                   ((uintptr_t)q & 15u) == 0 && ((uintptr_t)b16 & 15u) == 0,

@@ -125,13 +125,17 @@ template <> __device__ __forceinline__ double2 load_pair<float>(const float* p) 
 // then waits out a chain of three dependent loads.) Each element is summed in
 // the same order as in k_combine1, so every column of z has the bits of an
 // R = 1 combine.
-template <typename ACC>
+// MODE 0: store z (and reduce it when dots); MODE 1: reduce z without storing
+// it; MODE 2: the direction update on the recomputed z (same bits as MODE 0's
+// z): x += alpha_x p (x may be null), p = z + beta p, no reduction. In MODE 2
+// the `z` argument is p and `r` is x.
+template <typename ACC, int MODE>
 __global__ void __launch_bounds__(kThreads, 4)
     k_combine2(int64_t n, PcgState S, const int* __restrict__ dof_ptr, const int* __restrict__ dof_src,
                const ACC* __restrict__ ylocal, const double* u, const int* __restrict__ p_ptr,
                const int* __restrict__ p_col, const double* __restrict__ p_val,
                const double* __restrict__ yc, double sign, double* z, int dots,
-               const double* __restrict__ r, const double* __restrict__ q, double* partials,
+               const double* r, const double* __restrict__ q, double* partials,
                unsigned int* ticket) {
   constexpr int U = 3;
   __shared__ double red[kThreads];
@@ -139,6 +143,13 @@ __global__ void __launch_bounds__(kThreads, 4)
   if (S.ist != nullptr && n_active(S.ist, R) == 0) return;
   const int tpr = R / 2;
   const int jc = 2 * (threadIdx.x % tpr);  // first of this thread's two columns
+  double beta0 = 0.0, beta1 = 0.0, ax0 = 0.0, ax1 = 0.0;
+  if (MODE == 2) {
+    beta0 = S.st[DDX_ST_BETA * R + jc];
+    beta1 = S.st[DDX_ST_BETA * R + jc + 1];
+    ax0 = S.st[DDX_ST_ALPHA_X * R + jc];
+    ax1 = S.st[DDX_ST_ALPHA_X * R + jc + 1];
+  }
   const int64_t rows_per_pass = (int64_t)gridDim.x * (blockDim.x / tpr);
   double acc_rz[2] = {0.0, 0.0}, acc_zq[2] = {0.0, 0.0};
   for (int64_t d0 = (int64_t)blockIdx.x * (blockDim.x / tpr) + threadIdx.x / tpr; d0 < n; d0 += rows_per_pass * U) {
@@ -225,6 +236,17 @@ __global__ void __launch_bounds__(kThreads, 4)
 #pragma unroll
     for (int uu = 0; uu < U; ++uu)
       if (ok[uu]) {
+        if (MODE == 2) {
+          double* pp = z + d[uu] * R + jc;
+          const double2 pv = *reinterpret_cast<const double2*>(pp);
+          if (r != nullptr) {
+            double* xp = const_cast<double*>(r) + d[uu] * R + jc;
+            const double2 xv = *reinterpret_cast<const double2*>(xp);
+            *reinterpret_cast<double2*>(xp) = make_double2(fma(ax0, pv.x, xv.x), fma(ax1, pv.y, xv.y));
+          }
+          *reinterpret_cast<double2*>(pp) = make_double2(fma(beta0, pv.x, v[uu].x), fma(beta1, pv.y, v[uu].y));
+          continue;
+        }
         if (dots) {
           const double2 rv = __ldg(reinterpret_cast<const double2*>(r + d[uu] * R + jc));
           acc_rz[0] = fma(rv.x, v[uu].x, acc_rz[0]);
@@ -235,9 +257,10 @@ __global__ void __launch_bounds__(kThreads, 4)
             acc_zq[1] = fma(v[uu].y, qv.y, acc_zq[1]);
           }
         }
-        *reinterpret_cast<double2*>(z + d[uu] * R + jc) = v[uu];
+        if (MODE == 0) *reinterpret_cast<double2*>(z + d[uu] * R + jc) = v[uu];
       }
   }
+  if constexpr (MODE == 2) return;
   if (!dots) return;
   // CTA sums per column, partials[(cta * 2 + v) * R + column], v = 0: r.z, 1: z.q
 #pragma unroll
@@ -354,11 +377,114 @@ __global__ void __launch_bounds__(256) k_coarse_gemvT(int n_c, int R, const doub
   if (live && lane < G) yc[row * R + g0 + lane] = out;
 }
 
+// ---------------------------------------------------------------------------
+// hybrid restriction per subdomain: w = A_R y = sum_i (A_R R_i^T) y_i
+// ---------------------------------------------------------------------------
+// The nonzeros of A_R R_i^T, grouped by (subdomain i, coarse row c) pair q
+// (pairs in ascending (i, c), entries of a pair in ascending position):
+// e_pos[t] is a ylocal row of subdomain i, e_val[t] = A_R[c, sub_idx[e_pos[t]]]
+// for t in [pair_ptr[q], pair_ptr[q+1]). ylocal is read row by row inside the
+// pair's subdomain, with no transpose map: the rows of one subdomain come from
+// DRAM about once and are re-read by its other pairs from L2.
+//
+// Pass 1 (one CTA per pair, grid-stride): R/2 threads per entry, two columns
+// each; G = 256 / (R/2) entry groups, group g summing entries g, g + G, ... in
+// ascending order (four in flight), then a fixed tree over the groups:
+// partial[q, :] = sum_t e_val[t] ylocal[e_pos[t], :] in FP64.
+template <typename ACC>
+__global__ void __launch_bounds__(kThreads)
+    k_restrict_sub(int64_t n_pairs, int R, const int64_t* __restrict__ pair_ptr, const int* __restrict__ e_pos,
+                   const double* __restrict__ e_val, const ACC* __restrict__ ylocal, double* __restrict__ partial,
+                   const int* ist) {
+  __shared__ double red[kThreads];
+  if (ist != nullptr && n_active(ist, R) == 0) return;
+  const int tpr = R / 2;
+  const int c2 = threadIdx.x % tpr;
+  const int G = blockDim.x / tpr;
+  const int e0 = threadIdx.x / tpr;
+  const ACC* ycol = ylocal + 2 * c2;
+  for (int64_t q = blockIdx.x; q < n_pairs; q += gridDim.x) {
+    const int64_t k0 = pair_ptr[q], k1 = pair_ptr[q + 1];
+    double2 s = make_double2(0.0, 0.0);
+    int64_t k = k0 + e0;
+    for (; k + 3 * G < k1; k += 4 * G) {
+      const int pA = __ldg(e_pos + k), pB = __ldg(e_pos + k + G), pC = __ldg(e_pos + k + 2 * G),
+                pD = __ldg(e_pos + k + 3 * G);
+      const double vA = __ldg(e_val + k), vB = __ldg(e_val + k + G), vC = __ldg(e_val + k + 2 * G),
+                   vD = __ldg(e_val + k + 3 * G);
+      const double2 yA = load_pair<ACC>(ycol + (int64_t)pA * R), yB = load_pair<ACC>(ycol + (int64_t)pB * R),
+                    yC = load_pair<ACC>(ycol + (int64_t)pC * R), yD = load_pair<ACC>(ycol + (int64_t)pD * R);
+      s.x = fma(vA, yA.x, s.x); s.y = fma(vA, yA.y, s.y);
+      s.x = fma(vB, yB.x, s.x); s.y = fma(vB, yB.y, s.y);
+      s.x = fma(vC, yC.x, s.x); s.y = fma(vC, yC.y, s.y);
+      s.x = fma(vD, yD.x, s.x); s.y = fma(vD, yD.y, s.y);
+    }
+    for (; k < k1; k += G) {
+      const double v = __ldg(e_val + k);
+      const double2 yv = load_pair<ACC>(ycol + (int64_t)__ldg(e_pos + k) * R);
+      s.x = fma(v, yv.x, s.x);
+      s.y = fma(v, yv.y, s.y);
+    }
+    const double se = block_sum_by_col(s.x, red, tpr);
+    const double so = block_sum_by_col(s.y, red, tpr);
+    if (threadIdx.x < tpr) reinterpret_cast<double2*>(partial + q * R)[threadIdx.x] = make_double2(se, so);
+  }
+}
+
+// Pass 2: w[c, j] = sum of partial[q, j] over the pairs q of coarse row c in
+// ascending subdomain order (sum_pair[sum_ptr[c] .. sum_ptr[c+1])), one
+// thread per (c, j).
+__global__ void __launch_bounds__(kThreads)
+    k_restrict_sum(int64_t n_coarse, int R, const int* __restrict__ sum_ptr, const int* __restrict__ sum_pair,
+                   const double* __restrict__ partial, double* __restrict__ w, const int* ist) {
+  if (ist != nullptr && n_active(ist, R) == 0) return;
+  const int64_t total = n_coarse * R;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = t / R;
+    const int j = (int)(t % R);
+    double acc = 0.0;
+    for (int u = __ldg(sum_ptr + c); u < __ldg(sum_ptr + c + 1); ++u)
+      acc += __ldg(partial + (int64_t)__ldg(sum_pair + u) * R + j);
+    w[t] = acc;
+  }
+}
+
 }  // namespace ddx
 
 using namespace ddx;
 
 extern "C" {
+
+int ddx_schwarz_restrict_sub(int64_t n_pairs, int64_t n_coarse, int R, const int64_t* pair_ptr, const int* e_pos,
+                             const double* e_val, const void* ylocal, int acc_dtype, const int* sum_ptr,
+                             const int* sum_pair, double* partial, double* w, const int* ist, ddx_stream_t stream) {
+  DDX_REQUIRE(R >= 2 && R <= 64 && valid_rhs_count(R), "ddx_schwarz_restrict_sub: R must be 2, 4, ..., 64 (got %d)",
+              R);
+  DDX_REQUIRE(n_pairs >= 0 && n_coarse >= 0, "ddx_schwarz_restrict_sub: bad sizes");
+  DDX_REQUIRE(acc_dtype == DDX_F64 || acc_dtype == DDX_F32, "ddx_schwarz_restrict_sub: acc dtype %d", acc_dtype);
+  if (n_coarse == 0) return DDX_OK;
+  DDX_REQUIRE(sum_ptr && w && (n_pairs == 0 || (pair_ptr && e_pos && e_val && ylocal && sum_pair && partial)),
+              "ddx_schwarz_restrict_sub: null pointer");
+  DDX_REQUIRE(((uintptr_t)partial & 15u) == 0 && ((uintptr_t)ylocal & (acc_dtype == DDX_F64 ? 15u : 7u)) == 0,
+              "ddx_schwarz_restrict_sub: partial must be 16-byte aligned, ylocal aligned to two columns");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n_pairs > 0) {
+    if (acc_dtype == DDX_F64) {
+      const int grid = resident_grid(k_restrict_sub<double>, n_pairs, 1 << 20);
+      k_restrict_sub<double><<<grid, kThreads, 0, s>>>(n_pairs, R, pair_ptr, e_pos, e_val, (const double*)ylocal,
+                                                       partial, ist);
+    } else {
+      const int grid = resident_grid(k_restrict_sub<float>, n_pairs, 1 << 20);
+      k_restrict_sub<float><<<grid, kThreads, 0, s>>>(n_pairs, R, pair_ptr, e_pos, e_val, (const float*)ylocal,
+                                                      partial, ist);
+    }
+    DDX_LAUNCH_CHECK("ddx_schwarz_restrict_sub");
+  }
+  const int grid2 = (int)std::min<int64_t>(ceil_div(n_coarse * R, kThreads), 4096);
+  k_restrict_sum<<<grid2, kThreads, 0, s>>>(n_coarse, R, sum_ptr, sum_pair, partial, w, ist);
+  DDX_LAUNCH_CHECK("ddx_schwarz_restrict_sub");
+  return DDX_OK;
+}
 
 int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src, const void* ylocal,
                         int acc_dtype, const double* u, const int* p_ptr, const int* p_col,
@@ -366,7 +492,8 @@ int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src
                         const double* r, const double* q, double* st, int* ist, double* partials,
                         unsigned int* tickets, ddx_stream_t stream) {
   DDX_REQUIRE(valid_rhs_count(R), "ddx_schwarz_combine: unsupported R=%d", R);
-  DDX_REQUIRE(n >= 0 && z, "ddx_schwarz_combine: bad arguments");
+  DDX_REQUIRE(n >= 0 && (z || (dots && R >= 2)), "ddx_schwarz_combine: bad arguments (z is required unless "
+              "R >= 2 and the combine only reduces)");
   if (ylocal && dof_ptr) DDX_REQUIRE(dof_src, "ddx_schwarz_combine: transpose map without dof_src");
   if (p_ptr) DDX_REQUIRE(p_col && p_val && yc, "ddx_schwarz_combine: prolongation needs P and yc");
   if (!p_ptr && p_col) DDX_REQUIRE(yc, "ddx_schwarz_combine: P0 prolongation needs yc");
@@ -385,12 +512,21 @@ int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src
                     ((uintptr_t)ylocal & (f64 ? 15u : 7u)) == 0,
                 "ddx_schwarz_combine: vectors must be 16-byte aligned for R >= 2");
     const int grid2 = red_grid(ceil_div(n * (R / 2), 3));
-    if (f64)
-      k_combine2<double><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const double*)ylocal, u, p_ptr,
-                                                    p_col, p_val, yc, sign, z, dots, r, q, partials, t);
-    else
-      k_combine2<float><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const float*)ylocal, u, p_ptr,
-                                                   p_col, p_val, yc, sign, z, dots, r, q, partials, t);
+    if (z != nullptr) {
+      if (f64)
+        k_combine2<double, 0><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const double*)ylocal, u, p_ptr,
+                                                         p_col, p_val, yc, sign, z, dots, r, q, partials, t);
+      else
+        k_combine2<float, 0><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const float*)ylocal, u, p_ptr,
+                                                        p_col, p_val, yc, sign, z, dots, r, q, partials, t);
+    } else {
+      if (f64)
+        k_combine2<double, 1><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const double*)ylocal, u, p_ptr,
+                                                         p_col, p_val, yc, sign, z, dots, r, q, partials, t);
+      else
+        k_combine2<float, 1><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const float*)ylocal, u, p_ptr,
+                                                        p_col, p_val, yc, sign, z, dots, r, q, partials, t);
+    }
   } else {
     const int grid1 = red_grid(ceil_div(n, 4));
     if (f64)
@@ -401,6 +537,39 @@ int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src
                                                    p_col, p_val, yc, sign, z, dots, r, q, partials, t);
   }
   DDX_LAUNCH_CHECK("ddx_schwarz_combine");
+  return DDX_OK;
+}
+
+int ddx_schwarz_combine_update(int64_t n, int R, const int* dof_ptr, const int* dof_src, const void* ylocal,
+                               int acc_dtype, const double* u, const int* p_ptr, const int* p_col,
+                               const double* p_val, const double* yc, double sign, double* x, double* p,
+                               const double* st, const int* ist, ddx_stream_t stream) {
+  DDX_REQUIRE(R >= 2 && valid_rhs_count(R), "ddx_schwarz_combine_update: R must be 2, 4, ..., 64 (got %d)", R);
+  DDX_REQUIRE(n >= 0 && p && st && ist, "ddx_schwarz_combine_update: bad arguments");
+  if (ylocal && dof_ptr) DDX_REQUIRE(dof_src, "ddx_schwarz_combine_update: transpose map without dof_src");
+  if (p_ptr) DDX_REQUIRE(p_col && p_val && yc, "ddx_schwarz_combine_update: prolongation needs P and yc");
+  if (!p_ptr && p_col) DDX_REQUIRE(yc, "ddx_schwarz_combine_update: P0 prolongation needs yc");
+  if (ylocal != nullptr && acc_dtype != DDX_F64 && acc_dtype != DDX_F32) {
+    set_error("ddx_schwarz_combine_update: acc dtype %d", acc_dtype);
+    return DDX_ERR_ARG;
+  }
+  const bool f64 = ylocal == nullptr || acc_dtype == DDX_F64;
+  DDX_REQUIRE(((uintptr_t)p & 15u) == 0 && ((uintptr_t)x & 15u) == 0 && ((uintptr_t)u & 15u) == 0 &&
+                  ((uintptr_t)yc & 15u) == 0 && ((uintptr_t)ylocal & (f64 ? 15u : 7u)) == 0,
+              "ddx_schwarz_combine_update: vectors must be 16-byte aligned");
+  if (n == 0) return DDX_OK;
+  // same launch shape as ddx_schwarz_combine (the per-element arithmetic does
+  // not depend on it, but keeping it keeps the memory behaviour alike)
+  PcgState S{const_cast<double*>(st), const_cast<int*>(ist), nullptr, R};
+  cudaStream_t s = (cudaStream_t)stream;
+  const int grid2 = red_grid(ceil_div(n * (R / 2), 3));
+  if (f64)
+    k_combine2<double, 2><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const double*)ylocal, u, p_ptr, p_col,
+                                                     p_val, yc, sign, p, 0, x, nullptr, nullptr, nullptr);
+  else
+    k_combine2<float, 2><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const float*)ylocal, u, p_ptr, p_col,
+                                                    p_val, yc, sign, p, 0, x, nullptr, nullptr, nullptr);
+  DDX_LAUNCH_CHECK("ddx_schwarz_combine_update");
   return DDX_OK;
 }
 

@@ -205,6 +205,9 @@ def bench_solve(args) -> dict:
     cg = dd.CG(cls(torch.float64, dd.Inv(DT[args.precision]), dd.CUDSS()), rtol=2.5e-9, maxiter=2000,
                flexible=args.precision != "f64")
     cg.setup(At, subdomains=(prob["sub_ptr"], prob["sub_idx"]), coarse_restriction=prob["R0"], block_size=1)
+    if args.restriction != "auto":
+        cg.preconditioner.sub_restriction = args.restriction == "sub"
+    cg.fuse_updates = args.fuse_updates == "on"
     R = args.rhs or spec["R"]
     B = torch.as_tensor(rhs_for(prob["A"].shape[0], 0, 1, spec, R), device=dev)
     cg.solve(B)
@@ -218,7 +221,9 @@ def bench_solve(args) -> dict:
     torch.cuda.synchronize()
     its = meta["iterations"] if isinstance(meta["iterations"], int) else max(meta["iterations"])
     ms = e0.elapsed_time(e1)
-    return {"workload": args.workload, "precision": args.precision, "rhs": R, "ms_per_solve": ms,
+    return {"workload": args.workload, "precision": args.precision, "rhs": R, "restriction": args.restriction,
+            "fuse_updates": args.fuse_updates,
+            "ms_per_solve": ms,
             "iterations": its, "ms_per_iteration": ms / max(its, 1)}
 
 
@@ -243,6 +248,10 @@ def main():
     ap.add_argument("--terms", type=int, default=None, choices=[1, 2],
                     help="16-bit residual terms of the tensor-core apply (default: automatic)")
     ap.add_argument("--tune", action="store_true", help="run the autotuner first and report every candidate")
+    ap.add_argument("--restriction", default="auto", choices=["auto", "sub", "y"],
+                    help="solve: hybrid restriction for R >= 2 (per subdomain, or from y / the transpose map)")
+    ap.add_argument("--fuse-updates", default="on", choices=["on", "off"],
+                    help="solve: multi-RHS x update in the p update, unstored z (CG.fuse_updates)")
     ap.add_argument("--stages", type=int, default=0, help="apply: ring depth of the symmetric tensor-core kernel "
                                                           "(2..6; 0: deepest that fits)")
     args = ap.parse_args()

@@ -87,6 +87,66 @@ def transpose_map(sub_idx: torch.Tensor, n: int):
     return dof_ptr.to(torch.int32), order.to(torch.int32)
 
 
+def subdomain_restriction(ar_ptr, ar_col, ar_val, n_c: int, n: int, sub_ptr, sub_idx, slices: int = 1) -> dict:
+    """Per-subdomain form of the hybrid restriction ``A_R y = sum_i (A_R R_i^T) y_i``
+    (``ddx_schwarz_restrict_sub``): the nonzeros of ``A_R R_i^T`` grouped by
+    (subdomain i, coarse row c) pair, pairs in ascending (i, c), entries of a
+    pair in ascending position of the subdomain-major list; and, per coarse
+    row, its pairs in ascending subdomain order. Runs on the tensors' device.
+    With ``slices`` > 1 (a local apply that splits each block into parts, part s
+    writing its partial products to ylocal slice s at row offset s * sum k_i),
+    every entry is listed once per slice (slice after slice for each position).
+
+    Returns ``pair_ptr`` (int64, n_pairs + 1), ``e_pos`` (int32 positions),
+    ``e_val`` (FP64 ``A_R[c, sub_idx[pos]]``), ``sum_ptr`` / ``sum_pair``
+    (int32) and ``n_pairs``.
+    """
+    dev = ar_ptr.device
+    ptr = ar_ptr.to(torch.int64)
+    col = ar_col.to(torch.int64)
+    val = ar_val.to(torch.float64)
+    # A_R^T by DOF: the coarse rows c (ascending) and values of column d of A_R
+    rows = torch.repeat_interleave(torch.arange(n_c, device=dev), ptr[1:] - ptr[:-1])
+    order = torch.argsort(col * n_c + rows)
+    t_c, t_v = rows[order], val[order]
+    t_ptr = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    t_ptr[1:] = torch.cumsum(torch.bincount(col, minlength=n), 0)
+    sp = sub_ptr.to(dev, torch.int64)
+    d = sub_idx.to(dev, torch.int64)
+    total = int(d.numel())
+    pos = torch.arange(total, device=dev)
+    sub = torch.repeat_interleave(torch.arange(sp.numel() - 1, device=dev), sp[1:] - sp[:-1])
+    cnt = t_ptr[d + 1] - t_ptr[d]
+    n_e = int(cnt.sum())
+    first = torch.cumsum(cnt, 0) - cnt
+    e_pos = torch.repeat_interleave(pos, cnt)
+    src = torch.repeat_interleave(t_ptr[d] - first, cnt) + torch.arange(n_e, device=dev)
+    e_c = t_c[src]
+    e_val = t_v[src]
+    e_sub = sub[e_pos]
+    # entries by (subdomain, coarse row), positions ascending within a pair
+    # (they are generated ascending; the sort is stable)
+    pkey = e_sub * n_c + e_c
+    o = torch.argsort(pkey, stable=True)
+    e_pos, e_val, pkey = e_pos[o], e_val[o], pkey[o]
+    if slices > 1:
+        S = int(slices)
+        e_pos = (e_pos[:, None] + torch.arange(S, device=dev)[None, :] * total).reshape(-1)
+        e_val = e_val[:, None].expand(-1, S).reshape(-1)
+        pkey = pkey[:, None].expand(-1, S).reshape(-1)
+    pairs, counts = torch.unique_consecutive(pkey, return_counts=True)
+    n_pairs = int(pairs.numel())
+    pair_ptr = torch.zeros(n_pairs + 1, dtype=torch.int64, device=dev)
+    pair_ptr[1:] = torch.cumsum(counts, 0)
+    p_sub, p_c = pairs // n_c, pairs % n_c
+    # each coarse row's pairs in ascending subdomain order
+    o2 = torch.argsort(p_c * max(int(sp.numel()) - 1, 1) + p_sub)
+    sum_ptr = torch.zeros(n_c + 1, dtype=torch.int64, device=dev)
+    sum_ptr[1:] = torch.cumsum(torch.bincount(p_c, minlength=n_c), 0)
+    return {"pair_ptr": pair_ptr, "e_pos": e_pos.to(torch.int32).contiguous(), "e_val": e_val.contiguous(),
+            "sum_ptr": sum_ptr.to(torch.int32), "sum_pair": o2.to(torch.int32), "n_pairs": n_pairs}
+
+
 def extract_blocks(crow, col, val, sub_ptr, sub_idx, first: int, last: int, kpad: int) -> torch.Tensor:
     """Dense local matrices ``A[idx_i][:, idx_i]`` for subdomains ``first..last-1``.
 

@@ -306,6 +306,9 @@ class SchwarzOperator(SparseSolver):
         # None: measured per R on first use, True / False: forced
         self.mapped_restriction = None
         self._mapped_choice = {}
+        # hybrid, R >= 2: the restriction A_R y summed per subdomain from the
+        # local products (None / True: used; False: the y / transpose-map forms)
+        self.sub_restriction = None
         self.autotune = True
         # SIMT apply on upper-triangle tiles with few blocks: at most this many
         # ylocal slices per block (1 keeps ylocal one row per subdomain entry)
@@ -848,7 +851,7 @@ class SchwarzOperator(SparseSolver):
                                               w.view(self.n_coarse, R))
             yc.copy_(out.reshape(-1))
 
-    def _combine(self, z, R, ylocal=None, u=None, prolong=False, sign=1.0, pcg=None, r=None, q=None):
+    def _combine(self, z, R, ylocal=None, u=None, prolong=False, sign=1.0, pcg=None, r=None, q=None, store=True):
         s = self.scratch(R)
         p_ptr = p_col = p_val = yc = None
         if prolong:
@@ -860,14 +863,34 @@ class SchwarzOperator(SparseSolver):
             st, ist, partials, tickets = pcg.st, pcg.ist, pcg.partials, pcg.tickets
             dots = 1
         dof_ptr, dof_src = self._ymap if ylocal is not None else (None, None)
-        L.call("ddx_schwarz_combine", self.n, R, L.ptr(dof_ptr), L.ptr(dof_src), L.ptr(ylocal),
-               L.DTYPE_CODE[self.acc_dtype], L.ptr(u), L.ptr(p_ptr), L.ptr(p_col), L.ptr(p_val), L.ptr(yc),
-               float(sign), L.ptr(z), dots, L.ptr(r), L.ptr(q), L.ptr(st), L.ptr(ist), L.ptr(partials),
-               L.ptr(tickets), L.stream_ptr())
+        args = (L.ptr(dof_ptr), L.ptr(dof_src), L.ptr(ylocal), L.DTYPE_CODE[self.acc_dtype], L.ptr(u), L.ptr(p_ptr),
+                L.ptr(p_col), L.ptr(p_val), L.ptr(yc), float(sign))
+        if not store:
+            # z is only reduced here; update_direction recomputes it from the same inputs
+            assert dots and R >= 2
+            self._z_inputs = args
+        L.call("ddx_schwarz_combine", self.n, R, *args, L.ptr(z) if store else None, dots, L.ptr(r), L.ptr(q),
+               L.ptr(st), L.ptr(ist), L.ptr(partials), L.ptr(tickets), L.stream_ptr())
+
+    def recompute_z_ok(self, R: int) -> bool:
+        """Whether the PCG loop may leave z unstored and have ``update_direction``
+        recompute it (R >= 2): when re-reading the local products and the
+        coarse correction costs fewer bytes than writing z and reading it back,
+        i.e. with a P0 coarse prolongation (one column per DOF) or none."""
+        return R >= 2 and (not self.n_coarse or self._P[0] is None)
+
+    def update_direction(self, x, p, R: int, pcg) -> None:
+        """``p = z + beta p`` (after ``x += alpha_x p`` of a deferred x update, x
+        may be None) on the z of the last fused apply, which was reduced but not
+        stored: the combine's arithmetic repeated on the same inputs, so z has
+        the same bits as a stored one."""
+        L.call("ddx_schwarz_combine_update", self.n, R, *self._z_inputs, L.ptr(x), L.ptr(p), L.ptr(pcg.st),
+               L.ptr(pcg.ist), L.stream_ptr())
 
     # Applied by the fused PCG loop: z = M r with rho = r.z (and z.q) -> beta;
-    # ``packed``: the B panels of r are already written (tensor-core path).
-    def _apply_fused(self, r, z, R, pcg, q, packed=False):
+    # ``packed``: the B panels of r are already written (tensor-core path);
+    # ``store_z`` False: z is reduced but not written (see update_direction).
+    def _apply_fused(self, r, z, R, pcg, q, packed=False, store_z=True):
         raise NotImplementedError
 
     def _apply(self, rhs: torch.Tensor) -> torch.Tensor:
@@ -901,7 +924,7 @@ class AdditiveSchwarz(SchwarzOperator):
             self.dofs_per_coarse = dofs_per_solver * int(self.solvers_per_coarse[0].item())
         return timings
 
-    def _apply_fused(self, r, z, R, pcg, q, packed=False):
+    def _apply_fused(self, r, z, R, pcg, q, packed=False, store_z=True):
         s = self.scratch(R)
         ist = None if pcg is None else pcg.ist
         st = None if pcg is None else pcg.st
@@ -909,7 +932,7 @@ class AdditiveSchwarz(SchwarzOperator):
             self._restrict(*self._R0, r, s["w"], R)
             self._coarse(s["w"], s["yc"], R, ist)
         ylocal = self._local(r, R, ist, st, packed)
-        self._combine(z, R, ylocal=ylocal, prolong=bool(self.n_coarse), sign=1.0, pcg=pcg, r=r, q=q)
+        self._combine(z, R, ylocal=ylocal, prolong=bool(self.n_coarse), sign=1.0, pcg=pcg, r=r, q=q, store=store_z)
 
 
 class HybridSchwarz(SchwarzOperator):
@@ -940,13 +963,13 @@ class HybridSchwarz(SchwarzOperator):
         self._coarse(s["w"], s["yc"], R, ist)
         self._combine(x, R, u=x, prolong=True, sign=1.0)
 
-    def _apply_fused(self, r, z, R, pcg, q, packed=False):
+    def _apply_fused(self, r, z, R, pcg, q, packed=False, store_z=True):
         s = self.scratch(R)
         ist = None if pcg is None else pcg.ist
         st = None if pcg is None else pcg.st
         ylocal = self._local(r, R, ist, st, packed)
         if not self.n_coarse:
-            self._combine(z, R, ylocal=ylocal, pcg=pcg, r=r, q=q)
+            self._combine(z, R, ylocal=ylocal, pcg=pcg, r=r, q=q, store=store_z)
             return
         if self._ymap[0] is None and R == 1 and self._lanes_for(self.n_coarse, self._AR[1].numel()):
             # the reference's layout: y is ylocal widened to FP64, read in place by
@@ -955,18 +978,64 @@ class HybridSchwarz(SchwarzOperator):
             self._coarse(s["w"], s["yc"], R, ist)
             self._combine(z, R, ylocal=ylocal, prolong=True, sign=-1.0, pcg=pcg, r=r, q=q)
             return
+        if R > 1 and self._use_sub_restriction(R):
+            # A_R y summed per subdomain from the local products (no transpose-map
+            # gathers, ylocal streamed once); the combine reads ylocal for z
+            self._restrict_sub(ylocal, s["w"], R, ist)
+            self._coarse(s["w"], s["yc"], R, ist)
+            self._combine(z, R, ylocal=ylocal, prolong=True, sign=-1.0, pcg=pcg, r=r, q=q, store=store_z)
+            return
         if R > 1 and self._use_mapped(R, ylocal):
             # y = sum of the local products, read through the transpose map by the
             # restriction and by the combine (same sums, same bits): y is never written
             self._restrict_mapped(ylocal, s["w"], R)
             self._coarse(s["w"], s["yc"], R, ist)
-            self._combine(z, R, ylocal=ylocal, prolong=True, sign=-1.0, pcg=pcg, r=r, q=q)
+            self._combine(z, R, ylocal=ylocal, prolong=True, sign=-1.0, pcg=pcg, r=r, q=q, store=store_z)
             return
         y = s["y"]
         self._combine(y, R, ylocal=ylocal)
         self._restrict(*self._AR, y, s["w"], R)
         self._coarse(s["w"], s["yc"], R, ist)
-        self._combine(z, R, u=y, prolong=True, sign=-1.0, pcg=pcg, r=r, q=q)
+        self._combine(z, R, u=y, prolong=True, sign=-1.0, pcg=pcg, r=r, q=q, store=store_z)
+
+    def _slices(self) -> int:
+        """ylocal slices written by the last local apply (parts of split blocks)."""
+        return self.parts if (self._ymap is self._ymap_parts and self.parts > 1) else 1
+
+    def _use_sub_restriction(self, R: int) -> bool:
+        """Whether the restriction is summed per subdomain
+        (``ddx_schwarz_restrict_sub``): by default for every R >= 2 with a P0
+        coarse space (a fixed choice, so that the result's bits do not depend on
+        a timing); ``sub_restriction`` = True / False forces it on / off. With a
+        Q1 coarse space every DOF meets ~10 coarse rows of A_R, the per-subdomain
+        entries outnumber A_R's and the y form is faster (C2 at 64 RHS: 7.96 vs
+        9.53 ms per iteration)."""
+        if self.sub_restriction is False:
+            return False
+        if self.sub_restriction is None and self._P[0] is not None:
+            return False
+        # the plan is built on first use, which the solver makes eagerly
+        return self._slices() in getattr(self, "_subr", {}) or not torch.cuda.is_current_stream_capturing()
+
+    def _restrict_sub(self, ylocal, w, R, ist=None):
+        plans = getattr(self, "_subr", None)
+        if plans is None:
+            plans = self._subr = {}
+        S = self._slices()
+        plan = plans.get(S)
+        if plan is None:
+            rp, rc, rv = self._AR
+            plan = plans[S] = so.subdomain_restriction(rp, rc, rv, self.n_coarse, self.n, self.sub_ptr,
+                                                       self.sub_idx, slices=S)
+        key = ("subr_partial", R, S)
+        part = self._scratch.get(key)
+        if part is None:
+            part = self._scratch[key] = torch.empty(max(plan["n_pairs"], 1) * R, dtype=torch.float64,
+                                                    device=self.device)
+        L.call("ddx_schwarz_restrict_sub", plan["n_pairs"], self.n_coarse, R, L.ptr(plan["pair_ptr"]),
+               L.ptr(plan["e_pos"]), L.ptr(plan["e_val"]), L.ptr(ylocal), L.DTYPE_CODE[self.acc_dtype],
+               L.ptr(plan["sum_ptr"]), L.ptr(plan["sum_pair"]), L.ptr(part), L.ptr(w), L.ptr(ist),
+               L.stream_ptr())
 
     def _restrict_mapped(self, ylocal, w, R):
         dof_ptr, dof_src = self._ymap
@@ -1033,6 +1102,8 @@ class _PcgWork:
         self.graph_calls = {}
         self.warm = False
         self.fused_pack = False
+        self.defer_x = False
+        self.recompute_z = False
 
 
 class _SellMatrix:
@@ -1103,6 +1174,10 @@ class CG(SparseSolver):
         self.use_graph = use_graph
         # multi-RHS tensor-core path: the x/r update writes the next apply's B panels
         self.fuse_panels = True
+        # multi-RHS Schwarz path: x += alpha p moves into the next p update (one
+        # read of p fewer) and, with a P0 or no coarse prolongation, z is reduced
+        # but not stored, the p update recomputing it (same bits either way)
+        self.fuse_updates = True
         self._work = {}
 
     def __str__(self):
@@ -1162,23 +1237,42 @@ class CG(SparseSolver):
 
     def _iteration(self, w: _PcgWork, replace: bool):
         R = w.R
-        z = self._precondition(w)
-        L.call("ddx_pcg_update_p", self.n, R, L.ptr(z), L.ptr(w.p), L.ptr(w.st), L.ptr(w.ist), L.stream_ptr())
+        if w.recompute_z:
+            # z reduced (r.z, z.q) but not stored; the direction update recomputes
+            # it and applies the parked x step
+            pc = self.preconditioner
+            pc._apply_fused(w.r, w.z, R, w, w.q, packed=w.fused_pack, store_z=False)
+            pc.update_direction(w.x, w.p, R, w)
+        elif w.defer_x:
+            z = self._precondition(w)
+            L.call("ddx_pcg_update_px", self.n, R, L.ptr(z), L.ptr(w.p), L.ptr(w.x), L.ptr(w.st), L.ptr(w.ist),
+                   L.stream_ptr())
+        else:
+            z = self._precondition(w)
+            L.call("ddx_pcg_update_p", self.n, R, L.ptr(z), L.ptr(w.p), L.ptr(w.st), L.ptr(w.ist), L.stream_ptr())
         self.matrix.launch(w.p, w.q, R, L.SPMV_PQ, w, use_sell=self.bsr_matmul)
+        x = None if w.defer_x else w.x  # deferred: x += alpha p waits for the next p update
         if w.fused_pack:
-            # x, r and the next local apply's B panels in one pass
+            # r (and x) and the next local apply's B panels in one pass
             pan_ptr, pan_row = self.preconditioner.panel_rows(R)
             b16, _ = self.preconditioner._panels(R, 1)
-            L.call("ddx_pcg_update_xr_pack16", self.n, R, L.ptr(w.x), L.ptr(w.r), L.ptr(w.p), L.ptr(w.q),
+            L.call("ddx_pcg_update_xr_pack16", self.n, R, L.ptr(x), L.ptr(w.r), L.ptr(w.p), L.ptr(w.q),
                    L.ptr(pan_ptr), L.ptr(pan_row), L.ptr(b16), L.ptr(w.st), L.ptr(w.ist), L.ptr(w.hist),
                    L.ptr(w.partials), L.ptr(w.tickets), L.stream_ptr())
         else:
-            L.call("ddx_pcg_update_xr", self.n, R, L.ptr(w.x), L.ptr(w.r), L.ptr(w.p), L.ptr(w.q), L.ptr(w.st),
+            L.call("ddx_pcg_update_xr", self.n, R, L.ptr(x), L.ptr(w.r), L.ptr(w.p), L.ptr(w.q), L.ptr(w.st),
                    L.ptr(w.ist), L.ptr(w.hist), L.ptr(w.partials), L.ptr(w.tickets), L.stream_ptr())
         if replace:
+            if w.defer_x:
+                self._flush_x(w)
             self.matrix.launch(w.x, w.r, R, L.SPMV_RES_REPLACE, w, b=w.b, use_sell=self.bsr_matmul)
             if w.fused_pack:
                 self.preconditioner.pack_panels(w.r, R)
+
+    def _flush_x(self, w: _PcgWork) -> None:
+        """Applies the parked step of a deferred x update (x += alpha_x p)."""
+        L.call("ddx_pcg_flush_x", self.n, w.R, L.ptr(w.x), L.ptr(w.p), L.ptr(w.st), L.ptr(w.tickets),
+               L.stream_ptr())
 
     def _chunk(self, w: _PcgWork, k: int, start: int):
         re = self.replace_every
@@ -1188,7 +1282,7 @@ class CG(SparseSolver):
             for rep in plan:
                 self._iteration(w, rep)
             return
-        key = (plan, w.fused_pack)
+        key = (plan, w.fused_pack, w.defer_x, w.recompute_z)
         g = w.graphs.get(key)
         if g is None:
             if not w.warm:
@@ -1242,6 +1336,8 @@ class CG(SparseSolver):
                 xmat[:, :R] += pc.T0(rhs).view(n, R).to(torch.float64)
         self.matrix.launch(w.x, w.r, Rp, L.SPMV_RES_INIT, w, b=w.b, use_sell=self.bsr_matmul)
         w.fused_pack = bool(self.fuse_panels and isinstance(pc, SchwarzOperator) and pc.fused_pack_ok(Rp))
+        w.defer_x = bool(self.fuse_updates and Rp >= 2 and isinstance(pc, SchwarzOperator))
+        w.recompute_z = bool(w.defer_x and pc.recompute_z_ok(Rp))
         if w.fused_pack:
             # the tensor-core autotuner packs its own test panels into the same
             # buffer: let it run first, then the panels of the initial residual
@@ -1270,6 +1366,8 @@ class CG(SparseSolver):
                 self._chunk(w, kk, done)
             done += kk
             active = int(w.ist[L.IST_COUNT * Rp + L.G_NACTIVE].item())
+        if w.defer_x:
+            self._flush_x(w)
 
         # results and reference-compatible metadata
         ist = w.ist[: L.IST_COUNT * Rp].view(L.IST_COUNT, Rp).cpu()

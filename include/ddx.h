@@ -48,7 +48,8 @@ enum {
   DDX_ST_RHO = 0, DDX_ST_RHO_PREV = 1, DDX_ST_ZQ = 2, DDX_ST_PQ = 3, DDX_ST_ALPHA = 4,
   DDX_ST_BETA = 5, DDX_ST_RR = 6, DDX_ST_ATOL = 7, DDX_ST_BB = 8,
   DDX_ST_T0 = 9, DDX_ST_T1 = 10, /* parked column totals (DDX_G_DEFER) */
-  DDX_ST_COUNT = 11
+  DDX_ST_ALPHA_X = 11,            /* step length still to be applied to x (deferred x update) */
+  DDX_ST_COUNT = 12
 };
 enum { DDX_IST_ACTIVE = 0, DDX_IST_ITERS = 1, DDX_IST_COUNT = 2 };
 enum {
@@ -98,10 +99,24 @@ int ddx_pcg_reset(int R, double* st, int* ist, int maxiter, int flexible, double
 /* p = z + beta p (beta = 0 on a RHS's first iteration). */
 int ddx_pcg_update_p(int64_t n, int R, const double* z, double* p, const double* st, const int* ist,
                      ddx_stream_t stream);
-/* x += alpha p; r -= alpha q; then rr = ||r||^2 per RHS, stop test, history. */
+/* x += alpha p; r -= alpha q; then rr = ||r||^2 per RHS, stop test, history.
+ * Deferred x update (x = NULL): only r is updated and alpha is parked in st
+ * slot DDX_ST_ALPHA_X; the next ddx_pcg_update_px / ddx_schwarz_combine_update,
+ * which read p anyway, apply it to x before p changes (one read of p fewer per
+ * iteration), and ddx_pcg_flush_x applies what is left after the last update
+ * or before a residual replacement. Same x bits as the undeferred update. */
 int ddx_pcg_update_xr(int64_t n, int R, double* x, double* r, const double* p, const double* q,
                       double* st, int* ist, double* hist, double* partials, unsigned int* tickets,
                       ddx_stream_t stream);
+/* p = z + beta p, after x += alpha_x p with the parked step length of a
+ * deferred x update (st slot DDX_ST_ALPHA_X, 0 when nothing is parked): the
+ * x update of solvers.py:265 moved into the p update of solvers.py:267. */
+int ddx_pcg_update_px(int64_t n, int R, const double* z, double* p, double* x, const double* st, const int* ist,
+                      ddx_stream_t stream);
+/* x += alpha_x p with the parked step length (DDX_ST_ALPHA_X), which is then
+ * cleared; runs whether or not any RHS is still active. */
+int ddx_pcg_flush_x(int64_t n, int R, double* x, const double* p, double* st, unsigned int* tickets,
+                    ddx_stream_t stream);
 /* The epilogue of a deferred reduction (DDX_G_DEFER) on the totals in st slots
  * DDX_ST_T0 / DDX_ST_T1, after the caller summed them over the ranks: kind is a
  * DDX_FIN_* value. One CTA; same arithmetic as the in-kernel epilogue, so every
@@ -120,6 +135,7 @@ int ddx_pcg_finalize(int R, int kind, double* st, int* ist, double* hist, ddx_st
  * order of ddx_pcg_update_xr). Replaces the same reference updates as
  * ddx_pcg_update_xr (solvers.py:265-267) plus the gather of r into the
  * local solves (Inv.solve's input, solvers.py:355-359). */
+/* x = NULL: deferred x update, as for ddx_pcg_update_xr. */
 int ddx_pcg_update_xr_pack16(int64_t n, int R, double* x, double* r, const double* p, const double* q,
                              const int* pan_ptr, const int64_t* pan_row, void* b16, double* st, int* ist,
                              double* hist, double* partials, unsigned int* tickets, ddx_stream_t stream);
@@ -342,12 +358,43 @@ int ddx_pack_panels16(int n_sub, int R, const int64_t* sub_ptr, const int* sub_i
  * (equal contiguous non-overlapping subdomains, P0 coarse aggregates):
  * dof_ptr == NULL with ylocal means the identity map (ylocal is DOF-ordered);
  * p_ptr == NULL with p_col means P has one unit entry per DOF, in column
- * p_col[d] (p_val unused). */
+ * p_col[d] (p_val unused). z = NULL (R >= 2, dots != 0): z is only reduced,
+ * not stored; ddx_schwarz_combine_update recomputes it where p needs it. */
 int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src, const void* ylocal,
                         int acc_dtype, const double* u, const int* p_ptr, const int* p_col,
                         const double* p_val, const double* yc, double sign, double* z, int dots,
                         const double* r, const double* q, double* st, int* ist, double* partials,
                         unsigned int* tickets, ddx_stream_t stream);
+/* The PCG direction update on a z that was reduced but not stored (R >= 2):
+ * recomputes z exactly as ddx_schwarz_combine does from the same inputs (same
+ * operations in the same order, so the same bits), then x += alpha_x p (x may
+ * be NULL; see ddx_pcg_update_px) and p = z + beta p. Instead of writing z and
+ * reading it back, the local products and the coarse correction are read a
+ * second time; fewer bytes when the prolongation is P0 (or absent). Replaces
+ * HybridSchwarz.solve's output (solvers.py:885-888) followed by CG.solve's
+ * fused_mul_add (solvers.py:267). */
+int ddx_schwarz_combine_update(int64_t n, int R, const int* dof_ptr, const int* dof_src, const void* ylocal,
+                               int acc_dtype, const double* u, const int* p_ptr, const int* p_col,
+                               const double* p_val, const double* yc, double sign, double* x, double* p,
+                               const double* st, const int* ist, ddx_stream_t stream);
+/* Hybrid restriction for a block of R in {2, 4, ..., 64} right-hand sides,
+ * computed per subdomain from the local products instead of from y:
+ *   w = A_R y = sum_i (A_R R_i^T) y_i.
+ * The nonzeros of A_R R_i^T are grouped by (subdomain i, coarse row c) pair q,
+ * pairs in ascending (i, c): for t in [pair_ptr[q], pair_ptr[q+1]), e_pos[t] is
+ * a row of the subdomain-major ylocal (F64 or F32, acc_dtype) inside
+ * subdomain i and e_val[t] = A_R[c, sub_idx[e_pos[t]]]. Pass 1 writes
+ * partial[q, :] (n_pairs x R FP64 scratch, 16-byte aligned) in a fixed order;
+ * pass 2 sums, for each coarse row c, the partials of its pairs listed in
+ * sum_pair[sum_ptr[c] .. sum_ptr[c+1]) in that order into w[c, :]. Deterministic
+ * (a fixed summation order, not the order of the transpose-map form, so the
+ * last bits can differ from ddx_spmv_csr_rowblock_mapped). Skipped when ist
+ * says no column is active. Replaces, for a block of right-hand sides,
+ * HybridSchwarz.solve's y = sum_i R_i^T y_i followed by A_R y
+ * (src/dd_solvers/dd_solvers/solvers.py:878-884). */
+int ddx_schwarz_restrict_sub(int64_t n_pairs, int64_t n_coarse, int R, const int64_t* pair_ptr, const int* e_pos,
+                             const double* e_val, const void* ylocal, int acc_dtype, const int* sum_ptr,
+                             const int* sum_pair, double* partial, double* w, const int* ist, ddx_stream_t stream);
 /* Dense coarse solve with the explicit FP64 inverse (row-major, symmetric):
  * yc[c, j] = sum_d Ainv[c, d] w[d, j]. */
 int ddx_coarse_gemv_f64(int n_c, int R, const double* Ainv, const double* w, double* yc,

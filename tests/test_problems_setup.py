@@ -376,3 +376,78 @@ def test_spd_guard_keeps_rounded_blocks_positive_definite():
     assert list(st.shifted) == [0] and st.shifted[0] > 0
     assert np.linalg.eigvalsh(st.block(0).numpy()).min() > 0
     assert torch.equal(st.dense_q(1), plain.dense_q(1)) and float(st.scale[1]) == float(plain.scale[1])
+
+
+@pytest.mark.parametrize("case", ["q1_2d_p0", "q1_3d_q1", "p1_rcb"])
+def test_subdomain_restriction_plan(case):
+    """The per-subdomain restriction plan (pairs of subdomain and coarse row,
+    built with torch on the CPU here): summing e_val * ylocal[e_pos] per pair and
+    the pairs per coarse row in the listed order gives A_R y with
+    y = sum_i R_i^T ylocal_i; pairs ascending in (subdomain, coarse row),
+    positions ascending and inside the pair's subdomain, each coarse row's
+    pairs in ascending subdomain order."""
+    if case == "q1_2d_p0":
+        P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(2, 24, 4)
+    elif case == "q1_3d_q1":
+        P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(3, 8, 2, kappa_seed=1, coarse="q1")
+    else:
+        P, A, owner, nparts, sub_ptr, sub_idx, R0 = p1_case(30, 8)
+    AR = sps.csr_matrix(R0 @ A)
+    AR.sort_indices()
+    n_c, n = AR.shape
+    plan = so.subdomain_restriction(torch.as_tensor(AR.indptr.astype(np.int64)),
+                                    torch.as_tensor(AR.indices.astype(np.int32)), torch.as_tensor(AR.data),
+                                    n_c, n, torch.as_tensor(sub_ptr), torch.as_tensor(sub_idx))
+    pp = plan["pair_ptr"].numpy()
+    pos = plan["e_pos"].numpy().astype(np.int64)
+    val = plan["e_val"].numpy()
+    sptr = plan["sum_ptr"].numpy()
+    spair = plan["sum_pair"].numpy()
+    n_pairs = plan["n_pairs"]
+    assert pp[0] == 0 and pp[-1] == len(pos) and len(pp) == n_pairs + 1
+    sub_of = np.searchsorted(sub_ptr, pos, side="right") - 1
+    # entries of a pair: one subdomain, ascending positions, the A_R values
+    pair_sub = np.empty(n_pairs, dtype=np.int64)
+    pair_c = np.full(n_pairs, -1, dtype=np.int64)
+    for c in range(n_c):
+        for t in range(sptr[c], sptr[c + 1]):
+            pair_c[spair[t]] = c
+    assert (pair_c >= 0).all()
+    for q in range(n_pairs):
+        s = sub_of[pp[q]:pp[q + 1]]
+        assert (s == s[0]).all()
+        pair_sub[q] = s[0]
+        assert (np.diff(pos[pp[q]:pp[q + 1]]) > 0).all()
+        np.testing.assert_array_equal(val[pp[q]:pp[q + 1]],
+                                      AR[pair_c[q], sub_idx[pos[pp[q]:pp[q + 1]]]].toarray().ravel())
+    keys = pair_sub * n_c + pair_c
+    assert (np.diff(keys) > 0).all()
+    for c in range(n_c):
+        assert (np.diff(pair_sub[spair[sptr[c]:sptr[c + 1]]]) > 0).all()
+    # every nonzero of A_R R_i^T appears once
+    expect = sum(int((AR[:, sub_idx[sub_ptr[i]:sub_ptr[i + 1]]] != 0).sum()) for i in range(len(sub_ptr) - 1))
+    assert len(pos) == expect
+    # the two passes reproduce A_R y
+    R = 3
+    ylocal = np.random.default_rng(0).standard_normal((int(sub_ptr[-1]), R))
+    partial = np.stack([val[pp[q]:pp[q + 1]] @ ylocal[pos[pp[q]:pp[q + 1]]] for q in range(n_pairs)])
+    w = np.stack([partial[spair[sptr[c]:sptr[c + 1]]].sum(0) for c in range(n_c)])
+    y = np.zeros((n, R))
+    np.add.at(y, sub_idx, ylocal)
+    ref = AR @ y
+    assert np.abs(w - ref).max() <= 1e-12 * np.abs(ref).max()
+    # split blocks: ylocal in 3 slices, every entry listed once per slice
+    S, total = 3, int(sub_ptr[-1])
+    p3 = so.subdomain_restriction(torch.as_tensor(AR.indptr.astype(np.int64)),
+                                  torch.as_tensor(AR.indices.astype(np.int32)), torch.as_tensor(AR.data),
+                                  n_c, n, torch.as_tensor(sub_ptr), torch.as_tensor(sub_idx), slices=S)
+    yl3 = np.random.default_rng(1).standard_normal((S * total, R))
+    pp3, pos3, val3 = p3["pair_ptr"].numpy(), p3["e_pos"].numpy().astype(np.int64), p3["e_val"].numpy()
+    assert p3["n_pairs"] == n_pairs and len(pos3) == S * len(pos)
+    part3 = np.stack([val3[pp3[q]:pp3[q + 1]] @ yl3[pos3[pp3[q]:pp3[q + 1]]] for q in range(n_pairs)])
+    sp3, sq3 = p3["sum_ptr"].numpy(), p3["sum_pair"].numpy()
+    w3 = np.stack([part3[sq3[sp3[c]:sp3[c + 1]]].sum(0) for c in range(n_c)])
+    y3 = np.zeros((n, R))
+    np.add.at(y3, sub_idx, yl3.reshape(S, total, R).sum(0))
+    ref3 = AR @ y3
+    assert np.abs(w3 - ref3).max() <= 1e-12 * np.abs(ref3).max()
