@@ -47,6 +47,8 @@ _SIGS = {
     "ddx_pcg_dots_rz": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ddx_spmv_sell_f64": (_I, [_I64, _I64, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P]),
     "ddx_spmv_csr_f64": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P]),
+    "ddx_spmv_csr_ordered_f64": (_I, [_I64, _I, _P, _P, _P, _P, _I, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P]),
+    "ddx_row_clusters": (_I, [_I64, _P, _P, _I, _P]),
     "ddx_spmv_csr_rowblock_mapped": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P]),
     "ddx_spmv_csr_rowblock_f64": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P]),
     "ddx_spmv_bsr": (_I, [_I64, _I, _P, _P, _P, _P, _P, _I, _P]),
@@ -62,8 +64,13 @@ _SIGS = {
     "ddx_schwarz_combine": (_I, [_I64, _I, _P, _P, _P, _I, _P, _P, _P, _P, _P, _D, _P, _I, _P, _P, _P, _P,
                                  _P, _P, _P]),
     "ddx_coarse_gemv_f64": (_I, [_I, _I, _P, _P, _P, _P, _P]),
-    "ddx_schwarz_combine_update": (_I, [_I64, _I, _P, _P, _P, _I, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P, _P]),
-    "ddx_schwarz_restrict_sub": (_I, [_I64, _I64, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P]),
+    "ddx_coarse_gemm_f64": (_I, [_I, _I, _P, _P, _P, _P, _I64, _P, _P]),
+    "ddx_schwarz_combine_update": (_I, [_I64, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _D, _P, _P, _P, _P,
+                                        _P]),
+    "ddx_schwarz_combine_ex": (_I, [_I64, _I, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _D, _P, _I, _P, _P, _P, _P,
+                                    _P, _P, _P]),
+    "ddx_schwarz_restrict_sub": (_I, [_I, _I64, _I64, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I64, _P,
+                                      _P, _P, _P, _P, _P]),
     "ddx_nd_order": (_I, [_I64, _P, _P, _I, _P, _P, _P, _P]),
     "ddx_spmv_csr_lanes_f64": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P]),
     "ddx_spmv_csr_lanes": (_I, [_I64, _I, _P, _P, _P, _P, _I, _P, _P]),

@@ -129,10 +129,14 @@ template <> __device__ __forceinline__ double2 load_pair<float>(const float* p) 
 // it; MODE 2: the direction update on the recomputed z (same bits as MODE 0's
 // z): x += alpha_x p (x may be null), p = z + beta p, no reduction. In MODE 2
 // the `z` argument is p and `r` is x.
+// dof_first (may be null): per DOF its only position (>= 0), -1 when it has
+// none, -2 when it has several; a DOF in one subdomain then costs a chain of
+// two dependent loads (dof_first, ylocal) instead of three (dof_ptr, dof_src,
+// ylocal). Same sums in the same order either way.
 template <typename ACC, int MODE>
 __global__ void __launch_bounds__(kThreads, 4)
     k_combine2(int64_t n, PcgState S, const int* __restrict__ dof_ptr, const int* __restrict__ dof_src,
-               const ACC* __restrict__ ylocal, const double* u, const int* __restrict__ p_ptr,
+               const int* __restrict__ dof_first, const ACC* __restrict__ ylocal, const double* u, const int* __restrict__ p_ptr,
                const int* __restrict__ p_col, const double* __restrict__ p_val,
                const double* __restrict__ yc, double sign, double* z, int dots,
                const double* r, const double* __restrict__ q, double* partials,
@@ -167,6 +171,30 @@ __global__ void __launch_bounds__(kThreads, 4)
       for (int uu = 0; uu < U; ++uu)
         if (ok[uu]) {
           const double2 y = load_pair<ACC>(ylocal + d[uu] * R + jc);
+          v[uu].x += y.x;
+          v[uu].y += y.y;
+        }
+    } else if (ylocal != nullptr && dof_first != nullptr) {
+      int f[U], t0[U], t1[U];
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu) f[uu] = ok[uu] ? __ldg(dof_first + d[uu]) : -1;
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu) {
+        const bool multi = f[uu] <= -2;
+        t0[uu] = multi ? __ldg(dof_ptr + d[uu]) : 0;
+        t1[uu] = multi ? __ldg(dof_ptr + d[uu] + 1) : 0;
+      }
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu)
+        if (f[uu] >= 0) {
+          const double2 y = load_pair<ACC>(ylocal + (int64_t)f[uu] * R + jc);
+          v[uu].x += y.x;
+          v[uu].y += y.y;
+        }
+#pragma unroll
+      for (int uu = 0; uu < U; ++uu)
+        for (int t = t0[uu]; t < t1[uu]; ++t) {
+          const double2 y = load_pair<ACC>(ylocal + (int64_t)__ldg(dof_src + t) * R + jc);
           v[uu].x += y.x;
           v[uu].y += y.y;
         }
@@ -377,57 +405,185 @@ __global__ void __launch_bounds__(256) k_coarse_gemvT(int n_c, int R, const doub
   if (live && lane < G) yc[row * R + g0 + lane] = out;
 }
 
+// R in {16, 32, 64}: yc = Ainv w as a tiled FP64 GEMM. A CTA of 256 threads
+// computes a tile of BM rows (64 for R = 64, else 128) x all R columns, each
+// thread an RM x 4 block (rows ty, ty + TR, ...; four adjacent columns), over
+// one K range of kc columns of Ainv, in 32-wide K steps staged in shared
+// memory (Ainv transposed into As[k][row], w as Bs[k][col]). Every Ainv entry is
+// read once per solve (not once per 16 columns), every w row once per row tile.
+// With more K ranges than one (few row tiles: n_c / BM CTAs would leave SMs
+// idle), each range writes its own partial tile and k_coarse_ksum adds them in
+// ascending range order. Each output is summed over k in ascending order, then
+// over the ranges in order: deterministic.
+template <int R>
+__global__ void __launch_bounds__(256) k_coarse_gemm(int n_c, const double* __restrict__ Ainv,
+                                                     const double* __restrict__ w, double* __restrict__ out,
+                                                     int kc, const int* ist) {
+  constexpr int BK = 32;
+  constexpr int TC = R / 4;          // thread columns
+  constexpr int TR = 256 / TC;       // thread rows
+  constexpr int RM = R == 16 ? 2 : 4;  // rows per thread
+  constexpr int BM = RM * TR;        // rows per tile
+  __shared__ double As[BK][BM + 1];
+  __shared__ __align__(16) double Bs[BK][R];
+  if (ist != nullptr && n_active(ist, R) == 0) return;
+  const int tx = threadIdx.x % TC, ty = threadIdx.x / TC;
+  const int row0 = blockIdx.x * BM;
+  const int k_begin = blockIdx.y * kc;
+  const int k_end = min(n_c, k_begin + kc);
+  double acc[RM][4];
+#pragma unroll
+  for (int i = 0; i < RM; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (int k0 = k_begin; k0 < k_end; k0 += BK) {
+    const int kt = min(BK, k_end - k0);
+    __syncthreads();  // previous tile consumed
+    // A tile: BM rows x kt columns of Ainv (row-major), lanes along k
+    for (int e = threadIdx.x; e < BM * BK; e += 256) {
+      const int r = e / BK, k = e % BK;
+      const int gr = row0 + r;
+      As[k][r] = (gr < n_c && k < kt) ? __ldg(Ainv + (int64_t)gr * n_c + k0 + k) : 0.0;
+    }
+    // B tile: kt rows of w, R columns each
+    for (int e = threadIdx.x; e < BK * R; e += 256) {
+      const int k = e / R, c = e % R;
+      Bs[k][c] = k < kt ? __ldg(w + (int64_t)(k0 + k) * R + c) : 0.0;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int k = 0; k < BK; ++k) {
+      double a[RM];
+#pragma unroll
+      for (int i = 0; i < RM; ++i) a[i] = As[k][ty + i * TR];
+      const double2 b01 = *reinterpret_cast<const double2*>(&Bs[k][4 * tx]);
+      const double2 b23 = *reinterpret_cast<const double2*>(&Bs[k][4 * tx + 2]);
+      const double b[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+      for (int i = 0; i < RM; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+  }
+  double* o = out + (int64_t)blockIdx.y * n_c * R;
+#pragma unroll
+  for (int i = 0; i < RM; ++i) {
+    const int gr = row0 + ty + i * TR;
+    if (gr < n_c) {
+      double2* d = reinterpret_cast<double2*>(o + (int64_t)gr * R + 4 * tx);
+      d[0] = make_double2(acc[i][0], acc[i][1]);
+      d[1] = make_double2(acc[i][2], acc[i][3]);
+    }
+  }
+}
+
+// yc = sum over the K ranges s = 0..S-1 of part[s], in that order.
+__global__ void __launch_bounds__(256) k_coarse_ksum(int64_t total, int S, const double* __restrict__ part,
+                                                     double* __restrict__ yc, const int* ist, int R) {
+  if (ist != nullptr && n_active(ist, R) == 0) return;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int s = 0; s < S; ++s) acc += __ldg(part + (int64_t)s * total + t);
+    yc[t] = acc;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // hybrid restriction per subdomain: w = A_R y = sum_i (A_R R_i^T) y_i
 // ---------------------------------------------------------------------------
-// The nonzeros of A_R R_i^T, grouped by (subdomain i, coarse row c) pair q
-// (pairs in ascending (i, c), entries of a pair in ascending position):
-// e_pos[t] is a ylocal row of subdomain i, e_val[t] = A_R[c, sub_idx[e_pos[t]]]
-// for t in [pair_ptr[q], pair_ptr[q+1]). ylocal is read row by row inside the
-// pair's subdomain, with no transpose map: the rows of one subdomain come from
-// DRAM about once and are re-read by its other pairs from L2.
+// The coarse rows that subdomain i touches (A_R[c, idx_i] != 0) are its slots
+// 0..n_slots[i]-1 (ascending c), the pairs q = slot_base[i] + slot. Row p of
+// the subdomain-major ylocal carries its entries (slot, A_R[c, sub_idx[p]]) in
+// ascending slot: the first two directly at p (f_slot[2p + e], f_val[2p + e],
+// e = 0, 1; slot 255: none), the others in [ov_ptr[p], ov_ptr[p+1]) of
+// ov_slot / ov_val (on a 2D P0 coarse space only the rows at an aggregate's
+// corner have more than two).
 //
-// Pass 1 (one CTA per pair, grid-stride): R/2 threads per entry, two columns
-// each; G = 256 / (R/2) entry groups, group g summing entries g, g + G, ... in
-// ascending order (four in flight), then a fixed tree over the groups:
-// partial[q, :] = sum_t e_val[t] ylocal[e_pos[t], :] in FP64.
+// Pass 1, one CTA per subdomain (grid-stride): R/2 threads per row, two columns
+// each, G = 512 / R row groups; group g takes the rows g, g + G, ... in order,
+// eight at a time with all their loads (ylocal, first entry, overflow range)
+// issued before any use, and adds val * ylocal[p, :] into its own
+// shared-memory accumulators acc[g][slot][:] (every thread touches only its
+// own columns of its own group: no atomics, no barrier while streaming); then
+// the groups are summed in ascending g into partial[q, :]. ylocal streams
+// once, row by row, with no transpose-map gathers.
+constexpr int kRestrictMaxSlots = 16;
 template <typename ACC>
 __global__ void __launch_bounds__(kThreads)
-    k_restrict_sub(int64_t n_pairs, int R, const int64_t* __restrict__ pair_ptr, const int* __restrict__ e_pos,
-                   const double* __restrict__ e_val, const ACC* __restrict__ ylocal, double* __restrict__ partial,
+    k_restrict_sub(int n_sub, int R, const int64_t* __restrict__ sub_ptr, const int* __restrict__ slot_base,
+                   const int* __restrict__ n_slots, const unsigned char* __restrict__ f_slot,
+                   const double* __restrict__ f_val, const int* __restrict__ ov_ptr,
+                   const unsigned char* __restrict__ ov_slot, const double* __restrict__ ov_val,
+                   const ACC* __restrict__ ylocal, int slices, int64_t slice_rows, double* __restrict__ partial,
                    const int* ist) {
-  __shared__ double red[kThreads];
+  constexpr int U = 8;
+  extern __shared__ double acc_sm[];  // [G][kRestrictMaxSlots][R]
   if (ist != nullptr && n_active(ist, R) == 0) return;
   const int tpr = R / 2;
   const int c2 = threadIdx.x % tpr;
   const int G = blockDim.x / tpr;
-  const int e0 = threadIdx.x / tpr;
-  const ACC* ycol = ylocal + 2 * c2;
-  for (int64_t q = blockIdx.x; q < n_pairs; q += gridDim.x) {
-    const int64_t k0 = pair_ptr[q], k1 = pair_ptr[q + 1];
-    double2 s = make_double2(0.0, 0.0);
-    int64_t k = k0 + e0;
-    for (; k + 3 * G < k1; k += 4 * G) {
-      const int pA = __ldg(e_pos + k), pB = __ldg(e_pos + k + G), pC = __ldg(e_pos + k + 2 * G),
-                pD = __ldg(e_pos + k + 3 * G);
-      const double vA = __ldg(e_val + k), vB = __ldg(e_val + k + G), vC = __ldg(e_val + k + 2 * G),
-                   vD = __ldg(e_val + k + 3 * G);
-      const double2 yA = load_pair<ACC>(ycol + (int64_t)pA * R), yB = load_pair<ACC>(ycol + (int64_t)pB * R),
-                    yC = load_pair<ACC>(ycol + (int64_t)pC * R), yD = load_pair<ACC>(ycol + (int64_t)pD * R);
-      s.x = fma(vA, yA.x, s.x); s.y = fma(vA, yA.y, s.y);
-      s.x = fma(vB, yB.x, s.x); s.y = fma(vB, yB.y, s.y);
-      s.x = fma(vC, yC.x, s.x); s.y = fma(vC, yC.y, s.y);
-      s.x = fma(vD, yD.x, s.x); s.y = fma(vD, yD.y, s.y);
+  const int g = threadIdx.x / tpr;
+  double* mine = acc_sm + (size_t)g * kRestrictMaxSlots * R + 2 * c2;
+  for (int i = blockIdx.x; i < n_sub; i += gridDim.x) {
+    const int ns = n_slots[i];
+    if (ns > kRestrictMaxSlots) {
+      if (threadIdx.x == 0) atomicOr(&g_device_error, DEVERR_BAD_SIZE);
+      continue;
     }
-    for (; k < k1; k += G) {
-      const double v = __ldg(e_val + k);
-      const double2 yv = load_pair<ACC>(ycol + (int64_t)__ldg(e_pos + k) * R);
-      s.x = fma(v, yv.x, s.x);
-      s.y = fma(v, yv.y, s.y);
+    for (int sl = 0; sl < ns; ++sl) *reinterpret_cast<double2*>(mine + sl * R) = make_double2(0.0, 0.0);
+    for (int sc = 0; sc < slices; ++sc)
+      for (int64_t p0 = sub_ptr[i] + sc * slice_rows, p1 = sub_ptr[i + 1] + sc * slice_rows, pb = p0 + g; pb < p1;
+           pb += (int64_t)U * G) {
+        double2 y[U], fv[U];
+        int fs[U], o0[U], o1[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int64_t p = pb + (int64_t)u * G;
+          const bool ok = p < p1;
+          y[u] = ok ? load_pair<ACC>(ylocal + p * R + 2 * c2) : make_double2(0.0, 0.0);
+          // both direct entries: a 2-byte slot pair, a 16-byte value pair
+          fs[u] = ok ? (int)__ldg(reinterpret_cast<const unsigned short*>(f_slot) + p) : 0xffff;
+          fv[u] = ok ? __ldg(reinterpret_cast<const double2*>(f_val) + p) : make_double2(0.0, 0.0);
+          o0[u] = ok ? __ldg(ov_ptr + p) : 0;
+          o1[u] = ok ? __ldg(ov_ptr + p + 1) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int s0 = fs[u] & 0xff, s1 = fs[u] >> 8;
+          if (s0 != 255) {
+            double2* a = reinterpret_cast<double2*>(mine + s0 * R);
+            double2 cur = *a;
+            cur.x = fma(fv[u].x, y[u].x, cur.x);
+            cur.y = fma(fv[u].x, y[u].y, cur.y);
+            *a = cur;
+          }
+          if (s1 != 255) {
+            double2* a = reinterpret_cast<double2*>(mine + s1 * R);
+            double2 cur = *a;
+            cur.x = fma(fv[u].y, y[u].x, cur.x);
+            cur.y = fma(fv[u].y, y[u].y, cur.y);
+            *a = cur;
+          }
+          for (int t = o0[u]; t < o1[u]; ++t) {
+            const double v = __ldg(ov_val + t);
+            double2* a = reinterpret_cast<double2*>(mine + (int)__ldg(ov_slot + t) * R);
+            double2 cur = *a;
+            cur.x = fma(v, y[u].x, cur.x);
+            cur.y = fma(v, y[u].y, cur.y);
+            *a = cur;
+          }
+        }
+      }
+    __syncthreads();
+    // groups summed in ascending order: thread t takes (slot, column) items
+    const int base = slot_base[i];
+    for (int it = threadIdx.x; it < ns * R; it += blockDim.x) {
+      const int sl = it / R, col = it % R;
+      double sum = 0.0;
+      for (int gg = 0; gg < G; ++gg) sum += acc_sm[((size_t)gg * kRestrictMaxSlots + sl) * R + col];
+      partial[(int64_t)(base + sl) * R + col] = sum;
     }
-    const double se = block_sum_by_col(s.x, red, tpr);
-    const double so = block_sum_by_col(s.y, red, tpr);
-    if (threadIdx.x < tpr) reinterpret_cast<double2*>(partial + q * R)[threadIdx.x] = make_double2(se, so);
+    __syncthreads();
   }
 }
 
@@ -455,29 +611,40 @@ using namespace ddx;
 
 extern "C" {
 
-int ddx_schwarz_restrict_sub(int64_t n_pairs, int64_t n_coarse, int R, const int64_t* pair_ptr, const int* e_pos,
-                             const double* e_val, const void* ylocal, int acc_dtype, const int* sum_ptr,
-                             const int* sum_pair, double* partial, double* w, const int* ist, ddx_stream_t stream) {
+int ddx_schwarz_restrict_sub(int n_sub, int64_t n_pairs, int64_t n_coarse, int R, const int64_t* sub_ptr,
+                             const int* slot_base, const int* n_slots, const unsigned char* f_slot,
+                             const double* f_val, const int* ov_ptr, const unsigned char* ov_slot,
+                             const double* ov_val, const void* ylocal, int acc_dtype, int slices, int64_t slice_rows,
+                             const int* sum_ptr, const int* sum_pair, double* partial, double* w, const int* ist,
+                             ddx_stream_t stream) {
   DDX_REQUIRE(R >= 2 && R <= 64 && valid_rhs_count(R), "ddx_schwarz_restrict_sub: R must be 2, 4, ..., 64 (got %d)",
               R);
-  DDX_REQUIRE(n_pairs >= 0 && n_coarse >= 0, "ddx_schwarz_restrict_sub: bad sizes");
+  DDX_REQUIRE(n_sub >= 0 && n_pairs >= 0 && n_coarse >= 0 && slices >= 1 && (slices == 1 || slice_rows >= 0),
+              "ddx_schwarz_restrict_sub: bad sizes");
   DDX_REQUIRE(acc_dtype == DDX_F64 || acc_dtype == DDX_F32, "ddx_schwarz_restrict_sub: acc dtype %d", acc_dtype);
   if (n_coarse == 0) return DDX_OK;
-  DDX_REQUIRE(sum_ptr && w && (n_pairs == 0 || (pair_ptr && e_pos && e_val && ylocal && sum_pair && partial)),
+  DDX_REQUIRE(sum_ptr && w && (n_pairs == 0 || (sub_ptr && slot_base && n_slots && f_slot && f_val && ov_ptr &&
+                                                ylocal && sum_pair && partial)),
               "ddx_schwarz_restrict_sub: null pointer");
-  DDX_REQUIRE(((uintptr_t)partial & 15u) == 0 && ((uintptr_t)ylocal & (acc_dtype == DDX_F64 ? 15u : 7u)) == 0,
-              "ddx_schwarz_restrict_sub: partial must be 16-byte aligned, ylocal aligned to two columns");
+  DDX_REQUIRE(((uintptr_t)partial & 15u) == 0 && ((uintptr_t)ylocal & (acc_dtype == DDX_F64 ? 15u : 7u)) == 0 &&
+                  ((uintptr_t)f_val & 15u) == 0 && ((uintptr_t)f_slot & 1u) == 0,
+              "ddx_schwarz_restrict_sub: partial and f_val must be 16-byte aligned, f_slot 2-byte aligned, ylocal "
+              "aligned to two columns");
   cudaStream_t s = (cudaStream_t)stream;
-  if (n_pairs > 0) {
-    if (acc_dtype == DDX_F64) {
-      const int grid = resident_grid(k_restrict_sub<double>, n_pairs, 1 << 20);
-      k_restrict_sub<double><<<grid, kThreads, 0, s>>>(n_pairs, R, pair_ptr, e_pos, e_val, (const double*)ylocal,
-                                                       partial, ist);
-    } else {
-      const int grid = resident_grid(k_restrict_sub<float>, n_pairs, 1 << 20);
-      k_restrict_sub<float><<<grid, kThreads, 0, s>>>(n_pairs, R, pair_ptr, e_pos, e_val, (const float*)ylocal,
-                                                      partial, ist);
-    }
+  if (n_pairs > 0 && n_sub > 0) {
+    const size_t smem = (size_t)(512 / R) * kRestrictMaxSlots * R * sizeof(double);  // 64 KB
+    auto go = [&](auto kern, const auto* yl) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      int dev = 0, nsm = 148, per = 1;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kThreads, smem) != cudaSuccess || per < 1) per = 1;
+      const int grid = (int)std::min<int64_t>(n_sub, (int64_t)per * nsm);
+      kern<<<grid, kThreads, smem, s>>>(n_sub, R, sub_ptr, slot_base, n_slots, f_slot, f_val, ov_ptr, ov_slot, ov_val,
+                                        yl, slices, slice_rows, partial, ist);
+    };
+    if (acc_dtype == DDX_F64) go(k_restrict_sub<double>, (const double*)ylocal);
+    else go(k_restrict_sub<float>, (const float*)ylocal);
     DDX_LAUNCH_CHECK("ddx_schwarz_restrict_sub");
   }
   const int grid2 = (int)std::min<int64_t>(ceil_div(n_coarse * R, kThreads), 4096);
@@ -491,10 +658,20 @@ int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src
                         const double* p_val, const double* yc, double sign, double* z, int dots,
                         const double* r, const double* q, double* st, int* ist, double* partials,
                         unsigned int* tickets, ddx_stream_t stream) {
+  return ddx_schwarz_combine_ex(n, R, dof_ptr, dof_src, nullptr, ylocal, acc_dtype, u, p_ptr, p_col, p_val, yc,
+                                sign, z, dots, r, q, st, ist, partials, tickets, stream);
+}
+
+int ddx_schwarz_combine_ex(int64_t n, int R, const int* dof_ptr, const int* dof_src, const int* dof_first,
+                           const void* ylocal, int acc_dtype, const double* u, const int* p_ptr, const int* p_col,
+                           const double* p_val, const double* yc, double sign, double* z, int dots,
+                           const double* r, const double* q, double* st, int* ist, double* partials,
+                           unsigned int* tickets, ddx_stream_t stream) {
   DDX_REQUIRE(valid_rhs_count(R), "ddx_schwarz_combine: unsupported R=%d", R);
   DDX_REQUIRE(n >= 0 && (z || (dots && R >= 2)), "ddx_schwarz_combine: bad arguments (z is required unless "
               "R >= 2 and the combine only reduces)");
   if (ylocal && dof_ptr) DDX_REQUIRE(dof_src, "ddx_schwarz_combine: transpose map without dof_src");
+  if (dof_first) DDX_REQUIRE(dof_ptr && dof_src, "ddx_schwarz_combine: dof_first needs the transpose map");
   if (p_ptr) DDX_REQUIRE(p_col && p_val && yc, "ddx_schwarz_combine: prolongation needs P and yc");
   if (!p_ptr && p_col) DDX_REQUIRE(yc, "ddx_schwarz_combine: P0 prolongation needs yc");
   if (dots) DDX_REQUIRE(r && st && ist && partials && tickets, "ddx_schwarz_combine: dots need PCG state");
@@ -514,17 +691,17 @@ int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src
     const int grid2 = red_grid(ceil_div(n * (R / 2), 3));
     if (z != nullptr) {
       if (f64)
-        k_combine2<double, 0><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const double*)ylocal, u, p_ptr,
+        k_combine2<double, 0><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, dof_first, (const double*)ylocal, u, p_ptr,
                                                          p_col, p_val, yc, sign, z, dots, r, q, partials, t);
       else
-        k_combine2<float, 0><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const float*)ylocal, u, p_ptr,
+        k_combine2<float, 0><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, dof_first, (const float*)ylocal, u, p_ptr,
                                                         p_col, p_val, yc, sign, z, dots, r, q, partials, t);
     } else {
       if (f64)
-        k_combine2<double, 1><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const double*)ylocal, u, p_ptr,
+        k_combine2<double, 1><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, dof_first, (const double*)ylocal, u, p_ptr,
                                                          p_col, p_val, yc, sign, z, dots, r, q, partials, t);
       else
-        k_combine2<float, 1><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const float*)ylocal, u, p_ptr,
+        k_combine2<float, 1><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, dof_first, (const float*)ylocal, u, p_ptr,
                                                         p_col, p_val, yc, sign, z, dots, r, q, partials, t);
     }
   } else {
@@ -540,13 +717,14 @@ int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src
   return DDX_OK;
 }
 
-int ddx_schwarz_combine_update(int64_t n, int R, const int* dof_ptr, const int* dof_src, const void* ylocal,
-                               int acc_dtype, const double* u, const int* p_ptr, const int* p_col,
+int ddx_schwarz_combine_update(int64_t n, int R, const int* dof_ptr, const int* dof_src, const int* dof_first,
+                               const void* ylocal, int acc_dtype, const double* u, const int* p_ptr, const int* p_col,
                                const double* p_val, const double* yc, double sign, double* x, double* p,
                                const double* st, const int* ist, ddx_stream_t stream) {
   DDX_REQUIRE(R >= 2 && valid_rhs_count(R), "ddx_schwarz_combine_update: R must be 2, 4, ..., 64 (got %d)", R);
   DDX_REQUIRE(n >= 0 && p && st && ist, "ddx_schwarz_combine_update: bad arguments");
   if (ylocal && dof_ptr) DDX_REQUIRE(dof_src, "ddx_schwarz_combine_update: transpose map without dof_src");
+  if (dof_first) DDX_REQUIRE(dof_ptr && dof_src, "ddx_schwarz_combine_update: dof_first needs the transpose map");
   if (p_ptr) DDX_REQUIRE(p_col && p_val && yc, "ddx_schwarz_combine_update: prolongation needs P and yc");
   if (!p_ptr && p_col) DDX_REQUIRE(yc, "ddx_schwarz_combine_update: P0 prolongation needs yc");
   if (ylocal != nullptr && acc_dtype != DDX_F64 && acc_dtype != DDX_F32) {
@@ -564,12 +742,49 @@ int ddx_schwarz_combine_update(int64_t n, int R, const int* dof_ptr, const int* 
   cudaStream_t s = (cudaStream_t)stream;
   const int grid2 = red_grid(ceil_div(n * (R / 2), 3));
   if (f64)
-    k_combine2<double, 2><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const double*)ylocal, u, p_ptr, p_col,
+    k_combine2<double, 2><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, dof_first, (const double*)ylocal, u, p_ptr, p_col,
                                                      p_val, yc, sign, p, 0, x, nullptr, nullptr, nullptr);
   else
-    k_combine2<float, 2><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, (const float*)ylocal, u, p_ptr, p_col,
+    k_combine2<float, 2><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, dof_first, (const float*)ylocal, u, p_ptr, p_col,
                                                     p_val, yc, sign, p, 0, x, nullptr, nullptr, nullptr);
   DDX_LAUNCH_CHECK("ddx_schwarz_combine_update");
+  return DDX_OK;
+}
+
+int ddx_coarse_gemm_f64(int n_c, int R, const double* Ainv, const double* w, double* yc, double* scratch,
+                        int64_t scratch_len, const int* ist, ddx_stream_t stream) {
+  DDX_REQUIRE(R == 16 || R == 32 || R == 64, "ddx_coarse_gemm_f64: R must be 16, 32 or 64 (got %d)", R);
+  DDX_REQUIRE(n_c >= 0 && Ainv && w && yc && scratch_len >= 0, "ddx_coarse_gemm_f64: bad arguments");
+  DDX_REQUIRE(scratch_len == 0 || scratch, "ddx_coarse_gemm_f64: scratch_len > 0 with a null scratch");
+  DDX_REQUIRE(((uintptr_t)yc & 15u) == 0 && ((uintptr_t)scratch & 15u) == 0,
+              "ddx_coarse_gemm_f64: yc and scratch must be 16-byte aligned");
+  if (n_c == 0) return DDX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int bm = (R == 16 ? 2 : 4) * (256 / (R / 4));
+  const int row_tiles = (int)ceil_div(n_c, bm);
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  // K ranges (multiples of 32 columns) so that about two CTAs per SM run, as
+  // many as the scratch holds (S x n_c x R doubles)
+  const int64_t k_tiles = ceil_div(n_c, 32);
+  int64_t S = std::min<int64_t>(k_tiles, std::max<int64_t>(1, ceil_div(2 * nsm, row_tiles)));
+  S = std::min<int64_t>(S, scratch_len / ((int64_t)n_c * R));
+  if (S < 1) S = 1;
+  const int kc = (int)(ceil_div(k_tiles, S) * 32);
+  S = ceil_div(n_c, kc);
+  double* out = S == 1 ? yc : scratch;
+  const dim3 grid((unsigned)row_tiles, (unsigned)S);
+  if (R == 16) k_coarse_gemm<16><<<grid, 256, 0, s>>>(n_c, Ainv, w, out, kc, ist);
+  else if (R == 32) k_coarse_gemm<32><<<grid, 256, 0, s>>>(n_c, Ainv, w, out, kc, ist);
+  else k_coarse_gemm<64><<<grid, 256, 0, s>>>(n_c, Ainv, w, out, kc, ist);
+  DDX_LAUNCH_CHECK("ddx_coarse_gemm_f64");
+  if (S > 1) {
+    const int64_t total = (int64_t)n_c * R;
+    k_coarse_ksum<<<(int)std::min<int64_t>(ceil_div(total, 256), 4096), 256, 0, s>>>(total, (int)S, scratch, yc,
+                                                                                       ist, R);
+    DDX_LAUNCH_CHECK("ddx_coarse_gemm_f64");
+  }
   return DDX_OK;
 }
 

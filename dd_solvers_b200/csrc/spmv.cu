@@ -10,6 +10,8 @@
 // served by L1/L2). The PCG epilogues (p.q, b - A x and its norms) are fused
 // with deterministic CTA partials and a last-CTA finalize.
 #include <algorithm>
+#include <exception>
+#include <vector>
 #include <type_traits>
 
 #include "common.cuh"
@@ -139,11 +141,19 @@ __global__ void __launch_bounds__(kThreads)
 // adjacent RHS columns (16-byte loads of x rows), entries walked four at a
 // time with independent loads. Column sums for the PCG epilogues are reduced
 // as even/odd halves and written in the standard partials layout.
-template <int MODE>
-__global__ void __launch_bounds__(kThreads)
+// Work order: with order == NULL, the rows in their own order, rpb = 256 /
+// (R/2) consecutive rows per CTA step and grid-stride steps. With a row order
+// (a permutation of the rows cut into clusters of `chunk` graph-adjacent
+// rows, ddx_row_clusters), a CTA takes a whole cluster at a time, its rows in
+// consecutive steps, so the x rows the cluster's neighbourhood shares are read
+// from L2 once and then hit in L1 (a stencil row is read by up to 27 rows in
+// 3D; in the natural order only the ~3 neighbours along a grid line share L1).
+template <int MODE, bool ORDERED>
+__global__ void __launch_bounds__(kThreads, 4)
     k_spmm_csr2(int64_t n, const int* __restrict__ row_ptr, const int* __restrict__ cols,
                 const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y,
-                const double* __restrict__ b, PcgState S, double* partials, unsigned int* ticket) {
+                const double* __restrict__ b, PcgState S, double* partials, unsigned int* ticket,
+                const int* __restrict__ order, int chunk) {
   __shared__ double red[kThreads];
   const int R = S.R;
   if (MODE != DDX_SPMV_PLAIN && n_active(S.ist, R) == 0) return;
@@ -151,7 +161,7 @@ __global__ void __launch_bounds__(kThreads)
   const int c2 = threadIdx.x % tpr;  // this thread's column pair
   const int rpb = blockDim.x / tpr;
   double acc0[2] = {0.0, 0.0}, acc1[2] = {0.0, 0.0};  // [even, odd] column partials
-  for (int64_t row = (int64_t)blockIdx.x * rpb + threadIdx.x / tpr; row < n; row += (int64_t)gridDim.x * rpb) {
+  auto do_row = [&](int64_t row) {
     const int k0 = row_ptr[row], k1 = row_ptr[row + 1];
     double2 sum = make_double2(0.0, 0.0);
     int k = k0;
@@ -192,6 +202,18 @@ __global__ void __launch_bounds__(kThreads)
       acc0[0] = fma(ri.x, ri.x, acc0[0]);
       acc0[1] = fma(ri.y, ri.y, acc0[1]);
     }
+  };
+  if constexpr (!ORDERED) {
+    for (int64_t row = (int64_t)blockIdx.x * rpb + threadIdx.x / tpr; row < n; row += (int64_t)gridDim.x * rpb)
+      do_row(row);
+  } else {
+    // chunk is a multiple of rpb: the CTA walks one cluster in consecutive steps
+    for (int64_t c0 = (int64_t)blockIdx.x * chunk; c0 < n; c0 += (int64_t)gridDim.x * chunk)
+      for (int st = 0; st < chunk; st += rpb) {
+        const int64_t t = c0 + st + threadIdx.x / tpr;
+        if (t >= n) break;
+        do_row((int64_t)__ldg(order + t));
+      }
   }
   if (MODE == DDX_SPMV_PLAIN) return;
   constexpr int NV = (MODE == DDX_SPMV_RES_INIT) ? 2 : 1;
@@ -435,6 +457,50 @@ static int launch_bsr(int64_t nbr, int bs, const int* rp, const int* ci, const T
   return DDX_OK;
 }
 
+// Launch of k_spmm_csr2 (grid-stride: one wave of resident CTAs).
+template <bool ORDERED>
+static int spmm2_launch_t(int64_t n_rows, int R, const int* row_ptr, const int* cols, const double* vals,
+                          const double* x, double* y, const double* b, int mode, PcgState S, double* partials,
+                          unsigned int* t, const int* order, int chunk, cudaStream_t s) {
+  const int rpb2 = kThreads / (R / 2);
+  const int64_t need2 = ORDERED ? ceil_div(n_rows, chunk) : ceil_div(n_rows, rpb2);
+  switch (mode) {
+    case DDX_SPMV_PLAIN: {
+      auto k = k_spmm_csr2<DDX_SPMV_PLAIN, ORDERED>;
+      k<<<resident_grid(k, need2, 1 << 20), kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S, partials, t,
+                                                              order, chunk);
+      break;
+    }
+    case DDX_SPMV_PQ: {
+      auto k = k_spmm_csr2<DDX_SPMV_PQ, ORDERED>;
+      k<<<resident_grid(k, need2, kRedCtas), kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S, partials, t,
+                                                               order, chunk);
+      break;
+    }
+    case DDX_SPMV_RES_INIT: {
+      auto k = k_spmm_csr2<DDX_SPMV_RES_INIT, ORDERED>;
+      k<<<resident_grid(k, need2, kRedCtas), kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S, partials, t,
+                                                               order, chunk);
+      break;
+    }
+    default: {
+      auto k = k_spmm_csr2<DDX_SPMV_RES_REPLACE, ORDERED>;
+      k<<<resident_grid(k, need2, kRedCtas), kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S, partials, t,
+                                                               order, chunk);
+    }
+  }
+  DDX_LAUNCH_CHECK("ddx_spmv_csr_f64");
+  return DDX_OK;
+}
+
+static int spmm2_launch(int64_t n_rows, int R, const int* row_ptr, const int* cols, const double* vals,
+                        const double* x, double* y, const double* b, int mode, PcgState S, double* partials,
+                        unsigned int* t, const int* order, int chunk, cudaStream_t s) {
+  if (order != nullptr)
+    return spmm2_launch_t<true>(n_rows, R, row_ptr, cols, vals, x, y, b, mode, S, partials, t, order, chunk, s);
+  return spmm2_launch_t<false>(n_rows, R, row_ptr, cols, vals, x, y, b, mode, S, partials, t, nullptr, 0, s);
+}
+
 }  // namespace ddx
 
 using namespace ddx;
@@ -494,28 +560,7 @@ int ddx_spmv_csr_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols,
   if (R >= 2) {
     DDX_REQUIRE(((uintptr_t)x & 15u) == 0 && ((uintptr_t)y & 15u) == 0 && (b == nullptr || ((uintptr_t)b & 15u) == 0),
                 "ddx_spmv_csr_f64: x, y and b must be 16-byte aligned for R >= 2");
-    // grid-stride kernels: one wave of resident CTAs
-    const int rpb2 = kThreads / (R / 2);
-    const int64_t need2 = ceil_div(n_rows, rpb2);
-    switch (mode) {
-      case DDX_SPMV_PLAIN:
-        k_spmm_csr2<DDX_SPMV_PLAIN><<<resident_grid(k_spmm_csr2<DDX_SPMV_PLAIN>, need2, 1 << 20), kThreads, 0, s>>>(
-            n_rows, row_ptr, cols, vals, x, y, b, S, partials, t);
-        break;
-      case DDX_SPMV_PQ:
-        k_spmm_csr2<DDX_SPMV_PQ><<<resident_grid(k_spmm_csr2<DDX_SPMV_PQ>, need2, kRedCtas), kThreads, 0, s>>>(
-            n_rows, row_ptr, cols, vals, x, y, b, S, partials, t);
-        break;
-      case DDX_SPMV_RES_INIT:
-        k_spmm_csr2<DDX_SPMV_RES_INIT><<<resident_grid(k_spmm_csr2<DDX_SPMV_RES_INIT>, need2, kRedCtas), kThreads,
-                                         0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S, partials, t);
-        break;
-      default:
-        k_spmm_csr2<DDX_SPMV_RES_REPLACE><<<resident_grid(k_spmm_csr2<DDX_SPMV_RES_REPLACE>, need2, kRedCtas),
-                                            kThreads, 0, s>>>(n_rows, row_ptr, cols, vals, x, y, b, S, partials, t);
-    }
-    DDX_LAUNCH_CHECK("ddx_spmv_csr_f64");
-    return DDX_OK;
+    return spmm2_launch(n_rows, R, row_ptr, cols, vals, x, y, b, mode, S, partials, t, nullptr, 0, s);
   }
   const int rpb = kThreads / R;
   const int64_t need = ceil_div(n_rows, rpb);
@@ -578,6 +623,77 @@ int ddx_spmv_csr_rowblock_mapped(int64_t n_rows, int R, const int* row_ptr, cons
                                                              (const float*)ylocal, y);
   DDX_LAUNCH_CHECK("ddx_spmv_csr_rowblock_mapped");
   return DDX_OK;
+}
+
+int ddx_spmv_csr_ordered_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols, const double* vals,
+                             const int* order, int chunk, const double* x, double* y, const double* b, int mode,
+                             double* st, int* ist, double* hist, double* partials, unsigned int* tickets,
+                             ddx_stream_t stream) {
+  DDX_REQUIRE(R >= 2 && valid_rhs_count(R), "ddx_spmv_csr_ordered_f64: R must be 2, 4, ..., 64 (got %d)", R);
+  DDX_REQUIRE(n_rows >= 0 && row_ptr && x && y && order, "ddx_spmv_csr_ordered_f64: bad arguments");
+  DDX_REQUIRE(chunk > 0 && chunk % (kThreads / (R / 2)) == 0,
+              "ddx_spmv_csr_ordered_f64: chunk %d must be a positive multiple of %d rows", chunk,
+              kThreads / (R / 2));
+  DDX_REQUIRE(mode >= 0 && mode <= 3, "ddx_spmv_csr_ordered_f64: bad mode %d", mode);
+  if (mode != DDX_SPMV_PLAIN)
+    DDX_REQUIRE(st && ist && hist && partials && tickets, "ddx_spmv_csr_ordered_f64: PCG mode needs state");
+  if (mode >= DDX_SPMV_RES_INIT) DDX_REQUIRE(b, "ddx_spmv_csr_ordered_f64: residual mode needs b");
+  DDX_REQUIRE(((uintptr_t)x & 15u) == 0 && ((uintptr_t)y & 15u) == 0 && (b == nullptr || ((uintptr_t)b & 15u) == 0),
+              "ddx_spmv_csr_ordered_f64: x, y and b must be 16-byte aligned");
+  if (n_rows == 0) return DDX_OK;
+  PcgState S{st, ist, hist, R};
+  return spmm2_launch(n_rows, R, row_ptr, cols, vals, x, y, b, mode, S, partials, tickets ? tickets + 3 : nullptr,
+                      order, chunk, (cudaStream_t)stream);
+}
+
+// Greedy breadth-first clusters of `cluster` rows: a BFS over the unassigned
+// rows of the (symmetric) pattern from the lowest unassigned row, cut every
+// `cluster` rows; when a BFS runs out before the cut, the next lowest
+// unassigned row seeds the rest of the same cluster. Every cluster but the
+// last has exactly `cluster` rows (so clusters line up with the SpMM's
+// chunks); each cluster's rows ascending. On a structured grid the clusters
+// are bricks (BFS balls of a 27- or 9-point stencil are cubes / squares).
+static int row_clusters_impl(int64_t n, const int64_t* indptr, const int64_t* indices, int cluster, int* order) {
+  DDX_REQUIRE(n >= 0 && n < (int64_t)1 << 31 && indptr && indices && order && cluster >= 1,
+              "ddx_row_clusters: bad arguments");
+  std::vector<unsigned char> taken((size_t)n, 0);
+  std::vector<int> queue;
+  queue.reserve((size_t)cluster);
+  int64_t out = 0, seed = 0;
+  while (out < n) {
+    queue.clear();
+    size_t head = 0;
+    while ((int)queue.size() < cluster) {
+      if (head == queue.size()) {  // BFS exhausted: next unassigned row
+        while (seed < n && taken[seed]) ++seed;
+        if (seed == n) break;
+        taken[seed] = 1;
+        queue.push_back((int)seed);
+      }
+      const int v = queue[head++];
+      DDX_REQUIRE(indptr[v] <= indptr[v + 1], "ddx_row_clusters: indptr decreases at row %d", v);
+      for (int64_t e = indptr[v]; e < indptr[v + 1] && (int)queue.size() < cluster; ++e) {
+        const int64_t u = indices[e];
+        DDX_REQUIRE(u >= 0 && u < n, "ddx_row_clusters: column %lld out of range", (long long)u);
+        if (!taken[u]) {
+          taken[u] = 1;
+          queue.push_back((int)u);
+        }
+      }
+    }
+    std::sort(queue.begin(), queue.end());
+    for (int v : queue) order[out++] = v;
+  }
+  return DDX_OK;
+}
+
+int ddx_row_clusters(int64_t n, const int64_t* indptr, const int64_t* indices, int cluster, int* order) {
+  try {
+    return row_clusters_impl(n, indptr, indices, cluster, order);
+  } catch (const std::exception& ex) {
+    set_error("ddx_row_clusters: %s", ex.what());
+    return DDX_ERR_ARG;
+  }
 }
 
 int ddx_spmv_csr_lanes(int64_t n_rows, int lanes, const int* row_ptr, const int* cols, const double* vals,

@@ -5,7 +5,8 @@ cuDSS is absent from this image. ``spd_factorize`` replaces it in two ways:
 
 * up to ``DENSE_MAX`` rows, a dense FP64 Cholesky (cuSOLVER through
   ``torch.linalg.cholesky``) turned once into the explicit symmetric inverse,
-  applied by the HBM-bound ``ddx_coarse_gemv_f64`` kernel;
+  applied by the HBM-bound ``ddx_coarse_gemv_f64`` kernel (a tiled GEMM,
+  ``ddx_coarse_gemm_f64``, for 16-64 right-hand sides);
 * above that, the nested-dissection multifrontal factorisation of ``nd.py``,
   applied by ``ddx_coarse_solve_nd`` (two GEMV sweeps over the tree levels).
 
@@ -32,14 +33,25 @@ def _dense_inverse(A: torch.Tensor) -> torch.Tensor:
     return 0.5 * (inv + inv.transpose(-1, -2))
 
 
+# K ranges the multi-RHS coarse GEMM may split its reduction into (scratch of
+# GEMM_SPLIT x n x 64 doubles per solver, allocated with the factor)
+GEMM_SPLIT = 16
+
+
 class CudssSolver:
     def __init__(self, inverse: torch.Tensor, dtype: torch.dtype):
         self.inverse = inverse.contiguous()
         self.dtype = dtype
         self.n = inverse.shape[0]
+        self.scratch = torch.empty(GEMM_SPLIT * self.n * 64, dtype=torch.float64, device=inverse.device)
 
     def solve_into(self, w: torch.Tensor, y: torch.Tensor, R: int, ist=None) -> None:
-        """``y = A^-1 w`` for ``(n, R)`` FP64 device blocks, no allocation."""
+        """``y = A^-1 w`` for ``(n, R)`` FP64 device blocks, no allocation: a GEMV
+        sweep for R < 16, the tiled GEMM (Ainv read once) for R in {16, 32, 64}."""
+        if R in (16, 32, 64):
+            L.call("ddx_coarse_gemm_f64", self.n, R, L.ptr(self.inverse), L.ptr(w), L.ptr(y), L.ptr(self.scratch),
+                   self.scratch.numel(), L.ptr(ist), L.stream_ptr())
+            return
         L.call("ddx_coarse_gemv_f64", self.n, R, L.ptr(self.inverse), L.ptr(w), L.ptr(y), L.ptr(ist),
                L.stream_ptr())
 
@@ -49,7 +61,7 @@ class CudssSolver:
         w = rhs.to(torch.float64).contiguous()
         y = torch.empty_like(w)
         if R in (1, 2, 4, 8, 16, 32, 64):
-            L.call("ddx_coarse_gemv_f64", self.n, R, L.ptr(self.inverse), L.ptr(w), L.ptr(y), None, L.stream_ptr())
+            self.solve_into(w, y, R)
         else:
             for j in range(R):
                 wj = w[:, j].contiguous()

@@ -124,13 +124,16 @@ def bench_spmv(args) -> dict:
         A = A[perm][:, perm].tocsr()
         A.sort_indices()
     M = _SellMatrix(dd.csr_to_torch(A).to(dev))
+    if args.cluster >= 0:
+        M.spmm_cluster = args.cluster
     R = args.rhs or 1
     x = torch.randn(A.shape[0] * R, dtype=torch.float64, device=dev)
     y = torch.empty_like(x)
     ms = _time(lambda: M.launch(x, y, R, L.SPMV_PLAIN), args.reps)
     n = A.shape[0]
     nbytes = A.nnz * 12 + (n + 1) * 4 + n * R * 16
-    return {"kernel": "ddx_spmv_sell_f64" if R == 1 else "ddx_spmv_csr_f64", "problem": args.problem, "rhs": R,
+    kern = "ddx_spmv_sell_f64" if R == 1 else ("ddx_spmv_csr_ordered_f64" if M._chunk_for(R) else "ddx_spmv_csr_f64")
+    return {"kernel": kern, "problem": args.problem, "rhs": R, "cluster": M._chunk_for(R),
             "order": args.order,
             "n_dofs": n, "nnz": A.nnz, "ms_per_launch": ms, "algorithmic_bytes": nbytes,
             "achieved_gbs": nbytes / ms / 1e6, "frac_of_peak": nbytes / ms / 1e6 / _peak()}
@@ -208,6 +211,8 @@ def bench_solve(args) -> dict:
     if args.restriction != "auto":
         cg.preconditioner.sub_restriction = args.restriction == "sub"
     cg.fuse_updates = args.fuse_updates == "on"
+    if args.cluster >= 0:
+        cg.matrix.spmm_cluster = args.cluster
     R = args.rhs or spec["R"]
     B = torch.as_tensor(rhs_for(prob["A"].shape[0], 0, 1, spec, R), device=dev)
     cg.solve(B)
@@ -222,7 +227,7 @@ def bench_solve(args) -> dict:
     its = meta["iterations"] if isinstance(meta["iterations"], int) else max(meta["iterations"])
     ms = e0.elapsed_time(e1)
     return {"workload": args.workload, "precision": args.precision, "rhs": R, "restriction": args.restriction,
-            "fuse_updates": args.fuse_updates,
+            "fuse_updates": args.fuse_updates, "cluster": cg.matrix._chunk_for(R),
             "ms_per_solve": ms,
             "iterations": its, "ms_per_iteration": ms / max(its, 1)}
 
@@ -250,6 +255,9 @@ def main():
     ap.add_argument("--tune", action="store_true", help="run the autotuner first and report every candidate")
     ap.add_argument("--restriction", default="auto", choices=["auto", "sub", "y"],
                     help="solve: hybrid restriction for R >= 2 (per subdomain, or from y / the transpose map)")
+    ap.add_argument("--cluster", type=int, default=-1,
+                    help="spmv / solve, R >= 2: rows per breadth-first cluster of the SpMM work order (0: row order; "
+                         "-1: the solver's default)")
     ap.add_argument("--fuse-updates", default="on", choices=["on", "off"],
                     help="solve: multi-RHS x update in the p update, unstored z (CG.fuse_updates)")
     ap.add_argument("--stages", type=int, default=0, help="apply: ring depth of the symmetric tensor-core kernel "

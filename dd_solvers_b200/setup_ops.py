@@ -87,19 +87,26 @@ def transpose_map(sub_idx: torch.Tensor, n: int):
     return dof_ptr.to(torch.int32), order.to(torch.int32)
 
 
+RESTRICT_MAX_SLOTS = 16  # coarse rows one subdomain may touch (ddx_schwarz_restrict_sub)
+
+
 def subdomain_restriction(ar_ptr, ar_col, ar_val, n_c: int, n: int, sub_ptr, sub_idx, slices: int = 1) -> dict:
     """Per-subdomain form of the hybrid restriction ``A_R y = sum_i (A_R R_i^T) y_i``
-    (``ddx_schwarz_restrict_sub``): the nonzeros of ``A_R R_i^T`` grouped by
-    (subdomain i, coarse row c) pair, pairs in ascending (i, c), entries of a
-    pair in ascending position of the subdomain-major list; and, per coarse
-    row, its pairs in ascending subdomain order. Runs on the tensors' device.
-    With ``slices`` > 1 (a local apply that splits each block into parts, part s
-    writing its partial products to ylocal slice s at row offset s * sum k_i),
-    every entry is listed once per slice (slice after slice for each position).
+    (``ddx_schwarz_restrict_sub``), built with torch on the tensors' device.
 
-    Returns ``pair_ptr`` (int64, n_pairs + 1), ``e_pos`` (int32 positions),
-    ``e_val`` (FP64 ``A_R[c, sub_idx[pos]]``), ``sum_ptr`` / ``sum_pair``
-    (int32) and ``n_pairs``.
+    The coarse rows c with ``A_R[c, idx_i] != 0`` are subdomain i's slots
+    (ascending c); pair ``q = slot_base[i] + slot`` (pairs ascending in (i, c)).
+    Position p of the subdomain-major list carries its entries (slot,
+    ``A_R[c, sub_idx[p]]``) in ascending c: the first two as
+    ``f_slot[2p + e]`` (uint8, 255 for none) and ``f_val[2p + e]``, the others
+    in ``ov_ptr[p] .. ov_ptr[p+1]`` of ``ov_slot`` / ``ov_val``. ``sum_ptr`` / ``sum_pair`` list, per coarse
+    row, its pairs in ascending subdomain order. With ``slices`` > 1 (a local
+    apply that splits each block into parts, part s writing ylocal slice s at
+    row offset s * sum k_i) the positions of every slice carry the same
+    entries (the per-position arrays cover ``slices * sum k_i`` rows).
+
+    ``max_slots`` is the largest slot count; the kernel takes at most
+    ``RESTRICT_MAX_SLOTS``.
     """
     dev = ar_ptr.device
     ptr = ar_ptr.to(torch.int64)
@@ -113,38 +120,51 @@ def subdomain_restriction(ar_ptr, ar_col, ar_val, n_c: int, n: int, sub_ptr, sub
     t_ptr[1:] = torch.cumsum(torch.bincount(col, minlength=n), 0)
     sp = sub_ptr.to(dev, torch.int64)
     d = sub_idx.to(dev, torch.int64)
+    n_sub = int(sp.numel()) - 1
     total = int(d.numel())
-    pos = torch.arange(total, device=dev)
-    sub = torch.repeat_interleave(torch.arange(sp.numel() - 1, device=dev), sp[1:] - sp[:-1])
+    sub = torch.repeat_interleave(torch.arange(n_sub, device=dev), sp[1:] - sp[:-1])
     cnt = t_ptr[d + 1] - t_ptr[d]
     n_e = int(cnt.sum())
     first = torch.cumsum(cnt, 0) - cnt
-    e_pos = torch.repeat_interleave(pos, cnt)
+    e_pos = torch.repeat_interleave(torch.arange(total, device=dev), cnt)
     src = torch.repeat_interleave(t_ptr[d] - first, cnt) + torch.arange(n_e, device=dev)
     e_c = t_c[src]
     e_val = t_v[src]
-    e_sub = sub[e_pos]
-    # entries by (subdomain, coarse row), positions ascending within a pair
-    # (they are generated ascending; the sort is stable)
-    pkey = e_sub * n_c + e_c
-    o = torch.argsort(pkey, stable=True)
-    e_pos, e_val, pkey = e_pos[o], e_val[o], pkey[o]
-    if slices > 1:
-        S = int(slices)
-        e_pos = (e_pos[:, None] + torch.arange(S, device=dev)[None, :] * total).reshape(-1)
-        e_val = e_val[:, None].expand(-1, S).reshape(-1)
-        pkey = pkey[:, None].expand(-1, S).reshape(-1)
-    pairs, counts = torch.unique_consecutive(pkey, return_counts=True)
+    pkey = sub[e_pos] * n_c + e_c
+    pairs, inv = torch.unique(pkey, sorted=True, return_inverse=True)
     n_pairs = int(pairs.numel())
-    pair_ptr = torch.zeros(n_pairs + 1, dtype=torch.int64, device=dev)
-    pair_ptr[1:] = torch.cumsum(counts, 0)
     p_sub, p_c = pairs // n_c, pairs % n_c
+    n_slots = torch.bincount(p_sub, minlength=n_sub)
+    slot_base = torch.cumsum(n_slots, 0) - n_slots
+    e_slot = inv - slot_base[sub[e_pos]]
+    # the first two entries of every position, stored directly (entries are
+    # grouped by position, c ascending); the rest in the overflow lists
+    f_slot = torch.full((total, 2), 255, dtype=torch.int64, device=dev)
+    f_val = torch.zeros(total, 2, dtype=torch.float64, device=dev)
+    rank = torch.arange(n_e, device=dev) - first[e_pos]  # entry's index within its position
+    direct = rank < 2
+    f_slot[e_pos[direct], rank[direct]] = e_slot[direct]
+    f_val[e_pos[direct], rank[direct]] = e_val[direct]
+    ov_slot, ov_val = e_slot[~direct], e_val[~direct]
+    ov_cnt = (cnt - 2).clamp(min=0)
+    f_slot, f_val = f_slot.reshape(-1), f_val.reshape(-1)
+    S = max(int(slices), 1)
+    if S > 1:
+        f_slot, f_val, ov_cnt = f_slot.repeat(S), f_val.repeat(S), ov_cnt.repeat(S)
+        ov_slot, ov_val = ov_slot.repeat(S), ov_val.repeat(S)
+    ov_ptr = torch.zeros(S * total + 1, dtype=torch.int64, device=dev)
+    ov_ptr[1:] = torch.cumsum(ov_cnt, 0)
     # each coarse row's pairs in ascending subdomain order
-    o2 = torch.argsort(p_c * max(int(sp.numel()) - 1, 1) + p_sub)
+    o2 = torch.argsort(p_c * max(n_sub, 1) + p_sub)
     sum_ptr = torch.zeros(n_c + 1, dtype=torch.int64, device=dev)
     sum_ptr[1:] = torch.cumsum(torch.bincount(p_c, minlength=n_c), 0)
-    return {"pair_ptr": pair_ptr, "e_pos": e_pos.to(torch.int32).contiguous(), "e_val": e_val.contiguous(),
-            "sum_ptr": sum_ptr.to(torch.int32), "sum_pair": o2.to(torch.int32), "n_pairs": n_pairs}
+    max_slots = int(n_slots.max()) if n_sub else 0
+    assert int(ov_ptr[-1]) < 2 ** 31, "restriction plan too large for 32-bit entry offsets"
+    u8 = lambda t: t.clamp(max=255).to(torch.uint8).contiguous()  # noqa: E731 (slots >= 255 are refused by max_slots)
+    return {"n_pairs": n_pairs, "max_slots": max_slots, "slot_base": slot_base.to(torch.int32),
+            "n_slots": n_slots.to(torch.int32), "f_slot": u8(f_slot), "f_val": f_val.contiguous(),
+            "ov_ptr": ov_ptr.to(torch.int32), "ov_slot": u8(ov_slot), "ov_val": ov_val.contiguous(),
+            "sum_ptr": sum_ptr.to(torch.int32), "sum_pair": o2.to(torch.int32), "slices": S}
 
 
 def extract_blocks(crow, col, val, sub_ptr, sub_idx, first: int, last: int, kpad: int) -> torch.Tensor:

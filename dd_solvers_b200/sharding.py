@@ -375,6 +375,7 @@ class _Shard:
         self.T = plan.n_local_rows
         self.n_recv = plan.n_recv_rows
         self.A = S._SellMatrix(_torch_csr(plan.A_own, device))
+        self.A.spmm_cluster = 0  # rectangular local block (ghost columns): rows in their own order
         pc = S.AdditiveSchwarz(torch.float64, S.Inv(block_dtype), None)
         pc.max_parts = 1  # one ylocal slice: rows are (subdomain, position) entries
         pc.setup(_torch_csr(plan.A_ext, device), subdomains=(plan.sub_ptr, plan.sub_idx), block_size=1)

@@ -182,6 +182,22 @@ int ddx_spmv_sell_f64(int64_t n, int64_t nslices, const int64_t* slice_ptr, cons
 int ddx_spmv_csr_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols, const double* vals,
                      const double* x, double* y, const double* b, int mode, double* st, int* ist,
                      double* hist, double* partials, unsigned int* tickets, ddx_stream_t stream);
+/* The CSR SpMM for R in {2, 4, ..., 64} with a row work order: order is a
+ * permutation of the rows cut into clusters of `chunk` rows (ddx_row_clusters;
+ * chunk a multiple of 256 / (R/2)), and one CTA computes a whole cluster before
+ * its next, so the x rows shared by a cluster's neighbourhood come from L2
+ * once. Same modes and results as ddx_spmv_csr_f64 up to the summation order
+ * of the fused dot products. Replaces, for a block of right-hand sides,
+ * FastBSR's y = A x (src/dd_solvers/dd_solvers/bsr.py:40-76). */
+int ddx_spmv_csr_ordered_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols, const double* vals,
+                             const int* order, int chunk, const double* x, double* y, const double* b, int mode,
+                             double* st, int* ist, double* hist, double* partials, unsigned int* tickets,
+                             ddx_stream_t stream);
+/* Host: the row order of ddx_spmv_csr_ordered_f64 from the matrix pattern
+ * (CSR indptr / indices, symmetric): greedy breadth-first clusters of
+ * `cluster` rows, each cluster ascending (order: n ints). No counterpart in
+ * the reference, whose SpMV walks the rows in order. */
+int ddx_row_clusters(int64_t n, const int64_t* indptr, const int64_t* indices, int cluster, int* order);
 /* CSR with long rows, one CTA per row, deterministic block reduction:
  * y[row, j] = sum_k vals[k] x[cols[k], j] (coarse restriction A_R y or R0 r). */
 int ddx_spmv_csr_rowblock_f64(int64_t n_rows, int R, const int* row_ptr, const int* cols,
@@ -216,7 +232,6 @@ int ddx_spmv_csr_lanes(int64_t n_rows, int lanes, const int* row_ptr, const int*
  * one lane per scalar row, floor(32 / bs) block rows per warp. */
 int ddx_spmv_bsr(int64_t n_block_rows, int bs, const int* row_ptr, const int* cols, const void* vals,
                  const void* x, void* y, int dtype, ddx_stream_t stream);
-
 /* ---- Batched GEMV (reference op) ----------------------------------------
  * Replaces dd_solvers_gemv::gemv_strided_batched
  * (src/dd_solvers/cpp/gemv.cpp:9-53, kernels gemv_kernels.cu:31-139):
@@ -365,40 +380,71 @@ int ddx_schwarz_combine(int64_t n, int R, const int* dof_ptr, const int* dof_src
                         const double* p_val, const double* yc, double sign, double* z, int dots,
                         const double* r, const double* q, double* st, int* ist, double* partials,
                         unsigned int* tickets, ddx_stream_t stream);
+/* ddx_schwarz_combine with dof_first (may be NULL): per DOF its only position
+ * in ylocal (>= 0), -1 when it has none, -2 when it has several. A DOF in one
+ * subdomain then costs two dependent loads (dof_first, ylocal) instead of
+ * three (dof_ptr, dof_src, ylocal); the transpose map is still read for the
+ * others. Same sums in the same order. Used for R >= 2 (R = 1 reads the map). */
+int ddx_schwarz_combine_ex(int64_t n, int R, const int* dof_ptr, const int* dof_src, const int* dof_first,
+                           const void* ylocal, int acc_dtype, const double* u, const int* p_ptr, const int* p_col,
+                           const double* p_val, const double* yc, double sign, double* z, int dots,
+                           const double* r, const double* q, double* st, int* ist, double* partials,
+                           unsigned int* tickets, ddx_stream_t stream);
 /* The PCG direction update on a z that was reduced but not stored (R >= 2):
- * recomputes z exactly as ddx_schwarz_combine does from the same inputs (same
+ * recomputes z exactly as ddx_schwarz_combine_ex does from the same inputs (same
  * operations in the same order, so the same bits), then x += alpha_x p (x may
  * be NULL; see ddx_pcg_update_px) and p = z + beta p. Instead of writing z and
  * reading it back, the local products and the coarse correction are read a
  * second time; fewer bytes when the prolongation is P0 (or absent). Replaces
  * HybridSchwarz.solve's output (solvers.py:885-888) followed by CG.solve's
  * fused_mul_add (solvers.py:267). */
-int ddx_schwarz_combine_update(int64_t n, int R, const int* dof_ptr, const int* dof_src, const void* ylocal,
-                               int acc_dtype, const double* u, const int* p_ptr, const int* p_col,
+int ddx_schwarz_combine_update(int64_t n, int R, const int* dof_ptr, const int* dof_src, const int* dof_first,
+                               const void* ylocal, int acc_dtype, const double* u, const int* p_ptr, const int* p_col,
                                const double* p_val, const double* yc, double sign, double* x, double* p,
                                const double* st, const int* ist, ddx_stream_t stream);
 /* Hybrid restriction for a block of R in {2, 4, ..., 64} right-hand sides,
  * computed per subdomain from the local products instead of from y:
  *   w = A_R y = sum_i (A_R R_i^T) y_i.
- * The nonzeros of A_R R_i^T are grouped by (subdomain i, coarse row c) pair q,
- * pairs in ascending (i, c): for t in [pair_ptr[q], pair_ptr[q+1]), e_pos[t] is
- * a row of the subdomain-major ylocal (F64 or F32, acc_dtype) inside
- * subdomain i and e_val[t] = A_R[c, sub_idx[e_pos[t]]]. Pass 1 writes
- * partial[q, :] (n_pairs x R FP64 scratch, 16-byte aligned) in a fixed order;
- * pass 2 sums, for each coarse row c, the partials of its pairs listed in
- * sum_pair[sum_ptr[c] .. sum_ptr[c+1]) in that order into w[c, :]. Deterministic
- * (a fixed summation order, not the order of the transpose-map form, so the
- * last bits can differ from ddx_spmv_csr_rowblock_mapped). Skipped when ist
- * says no column is active. Replaces, for a block of right-hand sides,
- * HybridSchwarz.solve's y = sum_i R_i^T y_i followed by A_R y
+ * The coarse rows c with A_R[c, idx_i] != 0 are subdomain i's slots
+ * 0..n_slots[i]-1 (ascending c, at most 16), the pairs q = slot_base[i] + slot
+ * ascending in (i, c). Row p of the subdomain-major ylocal (F64 or F32,
+ * acc_dtype) carries its entries (slot, A_R[c, sub_idx[p]]) in ascending slot:
+ * the first two as f_slot[2p + e] (255: none; 2-byte aligned) and f_val[2p + e]
+ * (16-byte aligned), e = 0, 1, the others in [ov_ptr[p], ov_ptr[p+1]) of
+ * ov_slot / ov_val. With slices > 1 (a local apply
+ * that splits blocks into parts), ylocal holds `slices` slices of slice_rows =
+ * sub_ptr[n_sub] rows each, subdomain i's rows of slice s at s * slice_rows +
+ * [sub_ptr[i], sub_ptr[i+1]), and the entry arrays cover all of them (every
+ * slice carrying the same entries). Pass 1 streams each subdomain's rows once
+ * and writes partial[q, :] (n_pairs x R FP64 scratch, 16-byte aligned) in a
+ * fixed order; pass 2 sums, for each coarse row c, the partials of its pairs
+ * listed in sum_pair[sum_ptr[c] .. sum_ptr[c+1]) in that order into w[c, :].
+ * Deterministic (a fixed summation order, not that of
+ * ddx_spmv_csr_rowblock_mapped, so the last bits can differ from it). Skipped
+ * when ist says no column is active. Replaces, for a block of right-hand
+ * sides, HybridSchwarz.solve's y = sum_i R_i^T y_i followed by A_R y
  * (src/dd_solvers/dd_solvers/solvers.py:878-884). */
-int ddx_schwarz_restrict_sub(int64_t n_pairs, int64_t n_coarse, int R, const int64_t* pair_ptr, const int* e_pos,
-                             const double* e_val, const void* ylocal, int acc_dtype, const int* sum_ptr,
-                             const int* sum_pair, double* partial, double* w, const int* ist, ddx_stream_t stream);
+int ddx_schwarz_restrict_sub(int n_sub, int64_t n_pairs, int64_t n_coarse, int R, const int64_t* sub_ptr,
+                             const int* slot_base, const int* n_slots, const unsigned char* f_slot,
+                             const double* f_val, const int* ov_ptr, const unsigned char* ov_slot,
+                             const double* ov_val, const void* ylocal, int acc_dtype, int slices, int64_t slice_rows,
+                             const int* sum_ptr, const int* sum_pair, double* partial, double* w, const int* ist,
+                             ddx_stream_t stream);
 /* Dense coarse solve with the explicit FP64 inverse (row-major, symmetric):
  * yc[c, j] = sum_d Ainv[c, d] w[d, j]. */
 int ddx_coarse_gemv_f64(int n_c, int R, const double* Ainv, const double* w, double* yc,
                         const int* ist, ddx_stream_t stream);
+/* The same for R in {16, 32, 64} as a tiled FP64 GEMM that reads Ainv once
+ * per call (ddx_coarse_gemv_f64 reads it once per 16 columns). scratch (16-byte
+ * aligned, scratch_len doubles, may be NULL / 0) lets the reduction over
+ * Ainv's columns be split into up to scratch_len / (n_c R) ranges, summed in a
+ * fixed order by a second pass, so that a coarse space of a few thousand rows
+ * still fills the GPU; results differ from ddx_coarse_gemv_f64 in the last
+ * bits (another summation order) but not from run to run. Replaces
+ * CudssSolver.solve (src/dd_solvers/cpp/cudss.cpp:98-101) for a block of
+ * right-hand sides. */
+int ddx_coarse_gemm_f64(int n_c, int R, const double* Ainv, const double* w, double* yc, double* scratch,
+                        int64_t scratch_len, const int* ist, ddx_stream_t stream);
 
 /* ---- Sparse coarse solve (cuDSS replacement for large coarse spaces) ------
  * Replaces cudssExecute(FACTORIZATION / SOLVE) behind CudssSolver

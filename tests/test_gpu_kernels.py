@@ -152,6 +152,45 @@ def test_spmv(cuda, case, R):
     assert np.max(np.abs(y - ref)) <= 1e-12 * np.max(np.abs(ref))
 
 
+@pytest.mark.parametrize("case", ["q1_2d", "q1_3d", "p1"])
+@pytest.mark.parametrize("R", [2, 16, 64])
+@pytest.mark.parametrize("cluster", [8, 64, 200])
+def test_spmm_cluster_order_same_rows(cuda, case, R, cluster):
+    """The SpMM in breadth-first cluster order (ddx_spmv_csr_ordered_f64) gives
+    every row of A x with the same bits as the row-order kernel (a row's sum
+    does not depend on the work order); its fused p.q (PQ mode) agrees to
+    rounding. The order is a permutation of the rows."""
+    from dd_solvers_b200 import _lib as L
+    from dd_solvers_b200.solvers import _PcgWork, _SellMatrix
+
+    if case == "q1_2d":
+        A = q1_case(2, 40)[1]
+    elif case == "q1_3d":
+        A = q1_case(3, 12, kappa_seed=1)[1]
+    else:
+        A = p1_case(40)[1]
+    n = A.shape[0]
+    M = _SellMatrix(torch_csr(A, cuda))
+    M.spmm_cluster = cluster
+    chunk = M._chunk_for(R)
+    assert chunk % (512 // R) == 0 and chunk >= cluster
+    order = M.row_order(chunk).cpu().numpy()
+    assert np.array_equal(np.sort(order), np.arange(n))
+    x = torch.randn(n * R, dtype=torch.float64, device=cuda)
+    outs, pq = [], []
+    for cl in (0, cluster):
+        M.spmm_cluster = cl
+        y = torch.full_like(x, float("nan"))
+        M.launch(x, y, R, L.SPMV_PLAIN)
+        outs.append(y)
+        w = _PcgWork(n, R, 4, cuda)
+        L.call("ddx_pcg_reset", R, L.ptr(w.st), L.ptr(w.ist), 4, 0, 1e-8, 0.0, L.stream_ptr())
+        M.launch(x, w.q, R, L.SPMV_PQ, w)
+        pq.append(w.st.view(L.ST_COUNT, R)[L.ST_PQ].clone())
+    assert torch.equal(outs[0], outs[1])
+    assert torch.allclose(pq[0], pq[1], rtol=1e-13, atol=0)
+
+
 @pytest.mark.parametrize("prec", ["f64", "bf16"])
 @pytest.mark.parametrize("R", [4, 16])
 def test_mapped_restriction_bitwise_equal(cuda, prec, R):
@@ -175,11 +214,12 @@ def test_mapped_restriction_bitwise_equal(cuda, prec, R):
 
 @pytest.mark.parametrize("case", ["q1_2d_p0", "q1_3d_q1", "p1_rcb"])
 @pytest.mark.parametrize("R", [2, 16, 64])
-def test_sub_restriction_kernel_matches_scipy(cuda, case, R):
+@pytest.mark.parametrize("slices", [1, 3])
+def test_sub_restriction_kernel_matches_scipy(cuda, case, R, slices):
     """ddx_schwarz_restrict_sub on FP32 and FP64 local products: A_R y with
-    y = sum_i R_i^T ylocal_i, against SciPy in FP64 (P0 and Q1 coarse spaces,
-    overlapping boxes and RCB parts); two calls in a row give the same bits."""
-    import dd_solvers_b200 as dd
+    y = sum_i R_i^T ylocal_i (summed over ylocal's slices), against SciPy in
+    FP64 (P0 and Q1 coarse spaces, overlapping boxes and RCB parts); two calls
+    in a row give the same bits."""
     from dd_solvers_b200 import _lib as L
     from dd_solvers_b200 import setup_ops as so
 
@@ -192,23 +232,27 @@ def test_sub_restriction_kernel_matches_scipy(cuda, case, R):
     AR = sps.csr_matrix(R0 @ A)
     AR.sort_indices()
     n_c, n = AR.shape
+    sp = torch.as_tensor(sub_ptr, device=cuda)
     plan = so.subdomain_restriction(torch.as_tensor(AR.indptr.astype(np.int64), device=cuda),
                                     torch.as_tensor(AR.indices.astype(np.int32), device=cuda),
-                                    torch.as_tensor(AR.data, device=cuda), n_c, n,
-                                    torch.as_tensor(sub_ptr, device=cuda), torch.as_tensor(sub_idx, device=cuda))
+                                    torch.as_tensor(AR.data, device=cuda), n_c, n, sp,
+                                    torch.as_tensor(sub_idx, device=cuda), slices=slices)
+    assert plan["max_slots"] <= so.RESTRICT_MAX_SLOTS
     total = int(sub_ptr[-1])
     for acc in (torch.float32, torch.float64):
-        yl = torch.randn(total, R, dtype=torch.float64, device=cuda).to(acc)
+        yl = torch.randn(slices * total, R, dtype=torch.float64, device=cuda).to(acc)
         part = torch.empty(plan["n_pairs"] * R, dtype=torch.float64, device=cuda)
         outs = []
         for _ in range(2):
             w = torch.full((n_c * R,), float("nan"), dtype=torch.float64, device=cuda)
-            L.call("ddx_schwarz_restrict_sub", plan["n_pairs"], n_c, R, L.ptr(plan["pair_ptr"]), L.ptr(plan["e_pos"]),
-                   L.ptr(plan["e_val"]), L.ptr(yl), L.DTYPE_CODE[acc], L.ptr(plan["sum_ptr"]),
-                   L.ptr(plan["sum_pair"]), L.ptr(part), L.ptr(w), None, L.stream_ptr())
+            L.call("ddx_schwarz_restrict_sub", len(sub_ptr) - 1, plan["n_pairs"], n_c, R, L.ptr(sp),
+                   L.ptr(plan["slot_base"]), L.ptr(plan["n_slots"]), L.ptr(plan["f_slot"]), L.ptr(plan["f_val"]),
+                   L.ptr(plan["ov_ptr"]), L.ptr(plan["ov_slot"]), L.ptr(plan["ov_val"]), L.ptr(yl),
+                   L.DTYPE_CODE[acc], slices, total, L.ptr(plan["sum_ptr"]), L.ptr(plan["sum_pair"]), L.ptr(part),
+                   L.ptr(w), None, L.stream_ptr())
             outs.append(w.view(n_c, R).cpu().numpy())
         y = np.zeros((n, R))
-        np.add.at(y, sub_idx, yl.double().cpu().numpy())
+        np.add.at(y, sub_idx, yl.double().cpu().numpy().reshape(slices, total, R).sum(0))
         ref = AR @ y
         assert np.abs(outs[0] - ref).max() <= 1e-13 * np.abs(ref).max()
         assert np.array_equal(outs[0], outs[1])
@@ -425,6 +469,29 @@ def test_coarse_gemv_matches_matmul(cuda, R, n_c):
     L.call("ddx_coarse_gemv_f64", n_c, R, L.ptr(Ainv), L.ptr(w), L.ptr(yc), None, L.stream_ptr())
     ref = Ainv @ w
     assert torch.allclose(yc, ref, rtol=1e-12, atol=1e-12 * float(ref.abs().max()))
+
+
+@pytest.mark.parametrize("R", [16, 32, 64])
+@pytest.mark.parametrize("n_c", [1, 33, 257, 1000, 3375])
+def test_coarse_gemm_matches_matmul(cuda, R, n_c):
+    """Tiled coarse GEMM with and without a split of Ainv's columns (scratch),
+    against torch's FP64 product; a repeated call gives the same bits."""
+    from dd_solvers_b200 import _lib as L
+
+    g = torch.Generator(device=cuda).manual_seed(R * 7 + n_c)
+    Ainv = torch.randn(n_c, n_c, dtype=torch.float64, device=cuda, generator=g)
+    w = torch.randn(n_c, R, dtype=torch.float64, device=cuda, generator=g)
+    ref = Ainv @ w
+    scratch = torch.empty(16 * n_c * R, dtype=torch.float64, device=cuda)
+    for sc, n_sc in ((None, 0), (scratch, scratch.numel())):
+        outs = []
+        for _ in range(2):
+            yc = torch.full((n_c, R), float("nan"), dtype=torch.float64, device=cuda)
+            L.call("ddx_coarse_gemm_f64", n_c, R, L.ptr(Ainv), L.ptr(w), L.ptr(yc), L.ptr(sc), n_sc, None,
+                   L.stream_ptr())
+            outs.append(yc)
+        assert torch.allclose(outs[0], ref, rtol=1e-12, atol=1e-12 * float(ref.abs().max()))
+        assert torch.equal(outs[0], outs[1])
 
 
 @pytest.mark.parametrize("prec", ["f64", "f32", "bf16", "f16"])

@@ -378,14 +378,40 @@ def test_spd_guard_keeps_rounded_blocks_positive_definite():
     assert torch.equal(st.dense_q(1), plain.dense_q(1)) and float(st.scale[1]) == float(plain.scale[1])
 
 
+def _entries(plan, p):
+    """(slot, value) entries of ylocal row p in a restriction plan."""
+    out = []
+    for e in range(2):
+        if int(plan["f_slot"][2 * p + e]) != 255:
+            out.append((int(plan["f_slot"][2 * p + e]), float(plan["f_val"][2 * p + e])))
+    for t in range(int(plan["ov_ptr"][p]), int(plan["ov_ptr"][p + 1])):
+        out.append((int(plan["ov_slot"][t]), float(plan["ov_val"][t])))
+    return out
+
+
+def _restrict_with_plan(plan, sub_ptr, ylocal, n_c, R):
+    """The two passes of ddx_schwarz_restrict_sub in numpy (any fixed order)."""
+    S = plan["slices"]
+    total = int(sub_ptr[-1])
+    base, nsl = plan["slot_base"].numpy(), plan["n_slots"].numpy()
+    partial = np.zeros((plan["n_pairs"], R))
+    for i in range(len(sub_ptr) - 1):
+        for sc in range(S):
+            for p in range(sub_ptr[i] + sc * total, sub_ptr[i + 1] + sc * total):
+                for sl, v in _entries(plan, p):
+                    assert sl < nsl[i]
+                    partial[base[i] + sl] += v * ylocal[p]
+    sp, sq = plan["sum_ptr"].numpy(), plan["sum_pair"].numpy()
+    return np.stack([partial[sq[sp[c]:sp[c + 1]]].sum(0) for c in range(n_c)])
+
+
 @pytest.mark.parametrize("case", ["q1_2d_p0", "q1_3d_q1", "p1_rcb"])
 def test_subdomain_restriction_plan(case):
-    """The per-subdomain restriction plan (pairs of subdomain and coarse row,
-    built with torch on the CPU here): summing e_val * ylocal[e_pos] per pair and
-    the pairs per coarse row in the listed order gives A_R y with
-    y = sum_i R_i^T ylocal_i; pairs ascending in (subdomain, coarse row),
-    positions ascending and inside the pair's subdomain, each coarse row's
-    pairs in ascending subdomain order."""
+    """The per-subdomain restriction plan (slots of the coarse rows each
+    subdomain touches, per-position entries; built with torch on the CPU):
+    the two passes reproduce A_R y with y = sum_i R_i^T ylocal_i, also with
+    ylocal split into slices; slots ascending in the coarse row, each coarse
+    row's pairs in ascending subdomain order, every nonzero of A_R R_i^T once."""
     if case == "q1_2d_p0":
         P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(2, 24, 4)
     elif case == "q1_3d_q1":
@@ -395,59 +421,63 @@ def test_subdomain_restriction_plan(case):
     AR = sps.csr_matrix(R0 @ A)
     AR.sort_indices()
     n_c, n = AR.shape
-    plan = so.subdomain_restriction(torch.as_tensor(AR.indptr.astype(np.int64)),
-                                    torch.as_tensor(AR.indices.astype(np.int32)), torch.as_tensor(AR.data),
-                                    n_c, n, torch.as_tensor(sub_ptr), torch.as_tensor(sub_idx))
-    pp = plan["pair_ptr"].numpy()
-    pos = plan["e_pos"].numpy().astype(np.int64)
-    val = plan["e_val"].numpy()
-    sptr = plan["sum_ptr"].numpy()
-    spair = plan["sum_pair"].numpy()
-    n_pairs = plan["n_pairs"]
-    assert pp[0] == 0 and pp[-1] == len(pos) and len(pp) == n_pairs + 1
-    sub_of = np.searchsorted(sub_ptr, pos, side="right") - 1
-    # entries of a pair: one subdomain, ascending positions, the A_R values
-    pair_sub = np.empty(n_pairs, dtype=np.int64)
-    pair_c = np.full(n_pairs, -1, dtype=np.int64)
+    args = (torch.as_tensor(AR.indptr.astype(np.int64)), torch.as_tensor(AR.indices.astype(np.int32)),
+            torch.as_tensor(AR.data), n_c, n, torch.as_tensor(sub_ptr), torch.as_tensor(sub_idx))
+    plan = so.subdomain_restriction(*args)
+    nsub = len(sub_ptr) - 1
+    # slots: the coarse rows each subdomain touches, ascending; pairs per coarse row
+    pairs = []
+    for i in range(nsub):
+        cs = np.unique(AR[:, sub_idx[sub_ptr[i]:sub_ptr[i + 1]]].nonzero()[0])
+        assert plan["n_slots"][i] == len(cs) and plan["slot_base"][i] == len(pairs)
+        pairs += [(i, c) for c in cs]
+    assert plan["n_pairs"] == len(pairs) and plan["max_slots"] == int(plan["n_slots"].max())
+    sp, sq = plan["sum_ptr"].numpy(), plan["sum_pair"].numpy()
     for c in range(n_c):
-        for t in range(sptr[c], sptr[c + 1]):
-            pair_c[spair[t]] = c
-    assert (pair_c >= 0).all()
-    for q in range(n_pairs):
-        s = sub_of[pp[q]:pp[q + 1]]
-        assert (s == s[0]).all()
-        pair_sub[q] = s[0]
-        assert (np.diff(pos[pp[q]:pp[q + 1]]) > 0).all()
-        np.testing.assert_array_equal(val[pp[q]:pp[q + 1]],
-                                      AR[pair_c[q], sub_idx[pos[pp[q]:pp[q + 1]]]].toarray().ravel())
-    keys = pair_sub * n_c + pair_c
-    assert (np.diff(keys) > 0).all()
-    for c in range(n_c):
-        assert (np.diff(pair_sub[spair[sptr[c]:sptr[c + 1]]]) > 0).all()
-    # every nonzero of A_R R_i^T appears once
-    expect = sum(int((AR[:, sub_idx[sub_ptr[i]:sub_ptr[i + 1]]] != 0).sum()) for i in range(len(sub_ptr) - 1))
-    assert len(pos) == expect
-    # the two passes reproduce A_R y
+        subs = [pairs[q][0] for q in sq[sp[c]:sp[c + 1]]]
+        assert all(pairs[q][1] == c for q in sq[sp[c]:sp[c + 1]]) and subs == sorted(subs)
+    # per-position entries: the A_R values of the position's DOF, slots ascending
+    for i in range(nsub):
+        for p in range(sub_ptr[i], sub_ptr[i + 1]):
+            ent = _entries(plan, p)
+            sl = np.array([e[0] for e in ent], dtype=np.int64)
+            assert (np.diff(sl) > 0).all()
+            cs = [pairs[int(plan["slot_base"][i]) + k][1] for k in sl]
+            np.testing.assert_array_equal(np.array([e[1] for e in ent]), AR[cs, sub_idx[p]].toarray().ravel())
     R = 3
-    ylocal = np.random.default_rng(0).standard_normal((int(sub_ptr[-1]), R))
-    partial = np.stack([val[pp[q]:pp[q + 1]] @ ylocal[pos[pp[q]:pp[q + 1]]] for q in range(n_pairs)])
-    w = np.stack([partial[spair[sptr[c]:sptr[c + 1]]].sum(0) for c in range(n_c)])
-    y = np.zeros((n, R))
-    np.add.at(y, sub_idx, ylocal)
-    ref = AR @ y
-    assert np.abs(w - ref).max() <= 1e-12 * np.abs(ref).max()
-    # split blocks: ylocal in 3 slices, every entry listed once per slice
-    S, total = 3, int(sub_ptr[-1])
-    p3 = so.subdomain_restriction(torch.as_tensor(AR.indptr.astype(np.int64)),
-                                  torch.as_tensor(AR.indices.astype(np.int32)), torch.as_tensor(AR.data),
-                                  n_c, n, torch.as_tensor(sub_ptr), torch.as_tensor(sub_idx), slices=S)
-    yl3 = np.random.default_rng(1).standard_normal((S * total, R))
-    pp3, pos3, val3 = p3["pair_ptr"].numpy(), p3["e_pos"].numpy().astype(np.int64), p3["e_val"].numpy()
-    assert p3["n_pairs"] == n_pairs and len(pos3) == S * len(pos)
-    part3 = np.stack([val3[pp3[q]:pp3[q + 1]] @ yl3[pos3[pp3[q]:pp3[q + 1]]] for q in range(n_pairs)])
-    sp3, sq3 = p3["sum_ptr"].numpy(), p3["sum_pair"].numpy()
-    w3 = np.stack([part3[sq3[sp3[c]:sp3[c + 1]]].sum(0) for c in range(n_c)])
-    y3 = np.zeros((n, R))
-    np.add.at(y3, sub_idx, yl3.reshape(S, total, R).sum(0))
-    ref3 = AR @ y3
-    assert np.abs(w3 - ref3).max() <= 1e-12 * np.abs(ref3).max()
+    for S in (1, 3):
+        pl = plan if S == 1 else so.subdomain_restriction(*args, slices=S)
+        yl = np.random.default_rng(S).standard_normal((S * int(sub_ptr[-1]), R))
+        w = _restrict_with_plan(pl, sub_ptr, yl, n_c, R)
+        y = np.zeros((n, R))
+        np.add.at(y, sub_idx, yl.reshape(S, -1, R).sum(0))
+        ref = AR @ y
+        assert np.abs(w - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("cluster", [1, 7, 64, 10_000])
+def test_row_clusters(cluster):
+    """ddx_row_clusters (host code of the library): a permutation of the rows,
+    cut into clusters of exactly `cluster` rows (but the last), each ascending
+    and, on a 3D grid, compact: a 64-row cluster's neighbourhood (distinct
+    columns) is well below that of 64 consecutive rows."""
+    from dd_solvers_b200 import _lib as L
+
+    A = sps.csr_matrix(q1_case(3, 24, 2)[1])
+    n = A.shape[0]
+    ip = torch.as_tensor(A.indptr.astype(np.int64))
+    ix = torch.as_tensor(A.indices.astype(np.int64))
+    order = torch.empty(n, dtype=torch.int32)
+    L.call("ddx_row_clusters", n, ip.data_ptr(), ix.data_ptr(), cluster, order.data_ptr())
+    o = order.numpy()
+    assert np.array_equal(np.sort(o), np.arange(n))
+    for i in range(0, n, cluster):
+        assert (np.diff(o[i:i + cluster]) > 0).all()
+    if cluster == 64:
+        nb = np.mean([len(np.unique(A[o[i:i + 64]].indices)) for i in range(0, n - 64, 64)])
+        nat = np.mean([len(np.unique(A[i:i + 64].indices)) for i in range(0, n - 64, 64)])
+        assert nb < 0.7 * nat, (nb, nat)
+    bad = torch.as_tensor(np.array([0, 1, 2], dtype=np.int64))
+    with pytest.raises(L.DDXError):
+        L.call("ddx_row_clusters", 2, bad.data_ptr(), torch.as_tensor([0, 5], dtype=torch.int64).data_ptr(), 4,
+               torch.empty(2, dtype=torch.int32).data_ptr())
