@@ -24,7 +24,8 @@ divided by their number.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2]
 
 At N = 1 the c2 line also carries "reference_experiment": the reference's own DG-SIPG experiment S10 / S8 /
-S8 (hybrid, FP16 blocks) solved through this package, next to the reference's logged A100 time for it.
+S8 (hybrid, FP16 blocks) solved through this package, next to the reference's logged A100 time for it;
+"multi_rhs": compact c3 and c5 results; "other_workloads": compact c1 and c4 results (short timing).
 
 --impl reference times the FP64 CPU restatement of the same algorithm on the
 host cores (the reference's own solver runs on GPUs only; its CPU behaviour is
@@ -901,6 +902,29 @@ def cpu_baseline(spec, prob, cal, unit) -> dict:
             "iterations": cb["iterations"]}
 
 
+def other_workload_summary(args, name: str) -> dict:
+    """Compact result of another configuration (c1: additive Schwarz on the 2D
+    Poisson problem; c4: the differentiable solve) in the c2 line at N = 1, so
+    that one default run records every configuration: its own runner with
+    short timing (3 steps after 2 warm-up steps) and no CPU baseline."""
+    import torch
+
+    sub = argparse.Namespace(**vars(args))
+    sub.workload, sub.steps, sub.warmup, sub.batched = name, 3, 2, 0
+    spec = WORKLOADS[name]
+    runner = run_grad if spec["kind"] == "grad" else run_ours
+    res, _, cal = runner(sub, spec, 0, 1)
+    torch.cuda.empty_cache()
+    keep = ("metric", "value", "unit", "ms_per_step", "dtype", "iterations", "rel_error_vs_fp64",
+            "fp64_plain_ms_per_rhs", "speedup_vs_fp64_plain", "fp64_blocks_ms_per_gradient",
+            "speedup_vs_fp64_blocks", "gradient_check", "clocks")
+    out = {k: res[k] for k in keep if k in res}
+    out["workload"] = res["config"]["workload"]
+    out["e2e"] = res["e2e"]["value"]
+    out["dominant_kernel"] = {k: res["roofline"][k] for k in ("kernel", "ms_per_launch", "frac")}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -917,6 +941,8 @@ def main():
                     help="skip the reference's own DG experiment (run after the c2 measurement at N = 1)")
     ap.add_argument("--no-multi-rhs", dest="multi_rhs", action="store_false",
                     help="skip the compact c3 / c5 sub-results of the c2 line")
+    ap.add_argument("--no-other-workloads", dest="other_workloads", action="store_false",
+                    help="skip the compact c1 / c4 sub-results of the c2 line")
     args = ap.parse_args()
     spec = WORKLOADS[args.workload]
 
@@ -947,6 +973,10 @@ def main():
             torch.cuda.empty_cache()
             out["multi_rhs"] = {name: multi_rhs_summary(args, name, prec) for name, prec in
                                 (("c3", "bf16"), ("c5", "f16"))}
+        if world == 1 and args.workload == "c2" and args.other_workloads:
+            cal.clear()
+            torch.cuda.empty_cache()
+            out["other_workloads"] = {name: other_workload_summary(args, name) for name in ("c1", "c4")}
         print(json.dumps(out))
     if world > 1:
         dist.barrier()

@@ -20,7 +20,7 @@ DTYPE_CODE = {torch.float64: F64, torch.float32: F32, torch.bfloat16: BF16, torc
 
 # PCG state layout (ddx.h)
 (ST_RHO, ST_RHO_PREV, ST_ZQ, ST_PQ, ST_ALPHA, ST_BETA, ST_RR, ST_ATOL, ST_BB, ST_T0, ST_T1, ST_ALPHA_X,
- ST_COUNT) = range(13)
+ ST_RR_PACK, ST_COUNT) = range(14)
 IST_ACTIVE, IST_ITERS, IST_COUNT = range(3)
 G_NACTIVE, G_MAXITER, G_FLEXIBLE, G_BREAKDOWN, G_DEFER, G_COUNT = range(6)
 FIN_RZ, FIN_PQ, FIN_RR, FIN_INIT, FIN_REPLACE = range(5)
@@ -44,6 +44,7 @@ _SIGS = {
     "ddx_pcg_update_xr": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ddx_pcg_finalize": (_I, [_I, _I, _P, _P, _P, _P]),
     "ddx_pcg_update_xr_pack16": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "ddx_pcg_update_xr_pack16_ex": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P]),
     "ddx_pcg_dots_rz": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
     "ddx_spmv_sell_f64": (_I, [_I64, _I64, _P, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P]),
     "ddx_spmv_csr_f64": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P]),

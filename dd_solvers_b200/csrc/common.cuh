@@ -6,6 +6,8 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <type_traits>
+
 #include "../../include/ddx.h"
 
 namespace ddx {
@@ -77,6 +79,41 @@ template <typename T> __device__ __forceinline__ float to_f32(T v);
 template <> __device__ __forceinline__ float to_f32<float>(float v) { return v; }
 template <> __device__ __forceinline__ float to_f32<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
 template <> __device__ __forceinline__ float to_f32<__half>(__half v) { return __half2float(v); }
+
+// 16-bit conversions of the tensor-core B panels (through FP32, round to nearest)
+template <typename T> __device__ __forceinline__ uint16_t to_bits(double v);
+template <> __device__ __forceinline__ uint16_t to_bits<__nv_bfloat16>(double v) {
+  return __bfloat16_as_ushort(__float2bfloat16_rn((float)v));
+}
+template <> __device__ __forceinline__ uint16_t to_bits<__half>(double v) {
+  return __half_as_ushort(__float2half_rn((float)v));
+}
+template <typename T> __device__ __forceinline__ double from_bits(uint16_t b);
+template <> __device__ __forceinline__ double from_bits<__nv_bfloat16>(uint16_t b) {
+  return (double)__bfloat162float(__ushort_as_bfloat16(b));
+}
+template <> __device__ __forceinline__ double from_bits<__half>(uint16_t b) {
+  return (double)__half2float(__ushort_as_half(b));
+}
+
+
+// Power-of-two scale applied to RHS j of r before the 16-bit conversion, from
+// the PCG's current ||r_j||^2 (1 without PCG state): ||s r_j|| lands in
+// [2^(top-1), 2^top) with top = 14 for FP16 (every entry stays below 2^14, far
+// from the FP16 maximum 65504, while entries down to ~2^-10 ||r_j|| keep full
+// precision instead of falling into FP16 subnormals) and top = 0 for BF16,
+// whose exponent range needs no help.
+template <typename T>
+__device__ __forceinline__ float rhs_scale(const double* st, int R, int j) {
+  if (st == nullptr) return 1.0f;
+  const double rr = st[DDX_ST_RR * R + j];
+  if (!(rr > 0.0) || !(rr < 1e300)) return 1.0f;
+  int e;
+  frexp(sqrt(rr), &e);  // sqrt(rr) in [2^(e-1), 2^e)
+  e = max(-100, min(100, e));
+  constexpr int top = std::is_same<T, __half>::value ? 14 : 0;
+  return ldexpf(1.0f, top - e);
+}
 
 // ---------------------------------------------------------------------------
 // Deterministic reductions.

@@ -50,6 +50,7 @@ __global__ void k_pcg_finalize(PcgState S, int kind) {
     else if (kind == DDX_FIN_RR) act = fin_rr(S, j, t0);
     else if (kind == DDX_FIN_INIT) act = fin_init(S, j, t1, t0);
     else act = fin_replace(S, j, t0);
+    if (kind == DDX_FIN_INIT || kind == DDX_FIN_REPLACE) S.s(DDX_ST_RR_PACK, j) = S.s(DDX_ST_RR, j);
   }
   if (kind != DDX_FIN_RZ) publish_nactive(S, act);
 }
@@ -135,7 +136,10 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(int64_t n, PcgState S, d
 // its panel row whole. The pack pass and its re-read of r through the subdomain
 // index maps disappear. rr = ||r||^2 per column in a fixed order (CTA trees of
 // the even and odd columns, then the last CTA).
-template <int R>
+// T16 = __half: the FP16 panels of ddx_pack_panels16 (per-RHS power-of-two
+// scale from the squared norm in st slot RR when the update starts, the norm
+// kept in slot RR_PACK for the apply); T16 = __nv_bfloat16: scale 1.
+template <typename T16, int R>
 __global__ void __launch_bounds__(kThreads) k_update_xr_pack(int64_t n, PcgState S, double* __restrict__ x,
                                                              double* __restrict__ r, const double* __restrict__ p,
                                                              const double* __restrict__ q,
@@ -149,6 +153,11 @@ __global__ void __launch_bounds__(kThreads) k_update_xr_pack(int64_t n, PcgState
   if (n_active(S.ist, R) == 0) return;
   const int c2 = threadIdx.x % TPR;  // the stride is a multiple of TPR
   const double a0 = S.st[DDX_ST_ALPHA * R + 2 * c2], a1 = S.st[DDX_ST_ALPHA * R + 2 * c2 + 1];
+  constexpr bool kF16 = std::is_same<T16, __half>::value;
+  // the 16-bit conversion scales (FP16), from the norm before this update
+  const double sc0 = kF16 ? (double)rhs_scale<T16>(S.st, R, 2 * c2) : 1.0;
+  const double sc1 = kF16 ? (double)rhs_scale<T16>(S.st, R, 2 * c2 + 1) : 1.0;
+  const double rr_old = threadIdx.x < R ? S.st[DDX_ST_RR * R + threadIdx.x] : 0.0;
   const int inrow = ((c2 >> 2) << 4) | ((c2 & 3) << 2);  // byte of this thread's pair in an unswizzled row
   double acc0 = 0.0, acc1 = 0.0;
   const int64_t total = n * TPR;
@@ -168,8 +177,7 @@ __global__ void __launch_bounds__(kThreads) k_update_xr_pack(int64_t n, PcgState
     *reinterpret_cast<double2*>(r + o) = rn;
     acc0 = fma(rn.x, rn.x, acc0);
     acc1 = fma(rn.y, rn.y, acc1);
-    const uint32_t bits = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn((float)rn.x)) |
-                          ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn((float)rn.y)) << 16);
+    const uint32_t bits = (uint32_t)to_bits<T16>(rn.x * sc0) | ((uint32_t)to_bits<T16>(rn.y * sc1) << 16);
     const int e1 = __ldg(pan_ptr + d + 1);
     for (int e = __ldg(pan_ptr + d); e < e1; ++e) {
       const int64_t off = __ldg(pan_row + e);
@@ -186,7 +194,10 @@ __global__ void __launch_bounds__(kThreads) k_update_xr_pack(int64_t n, PcgState
   final_sums<1>(partials, R, red, tot, ticket);
   if (park_totals<1>(S, tot)) return;
   int act = 0;
-  if (threadIdx.x < R) act = fin_rr(S, threadIdx.x, tot[0], defer_x);
+  if (threadIdx.x < R) {
+    if (kF16) S.s(DDX_ST_RR_PACK, threadIdx.x) = rr_old;  // the norm the panels were scaled with
+    act = fin_rr(S, threadIdx.x, tot[0], defer_x);
+  }
   publish_nactive(S, act);
 }
 
@@ -311,6 +322,15 @@ int ddx_pcg_update_xr(int64_t n, int R, double* x, double* r, const double* p, c
 int ddx_pcg_update_xr_pack16(int64_t n, int R, double* x, double* r, const double* p, const double* q,
                              const int* pan_ptr, const int64_t* pan_row, void* b16, double* st, int* ist,
                              double* hist, double* partials, unsigned int* tickets, ddx_stream_t stream) {
+  return ddx_pcg_update_xr_pack16_ex(n, R, x, r, p, q, pan_ptr, pan_row, b16, DDX_BF16, st, ist, hist, partials,
+                                     tickets, stream);
+}
+
+int ddx_pcg_update_xr_pack16_ex(int64_t n, int R, double* x, double* r, const double* p, const double* q,
+                                const int* pan_ptr, const int64_t* pan_row, void* b16, int dtype, double* st,
+                                int* ist, double* hist, double* partials, unsigned int* tickets,
+                                ddx_stream_t stream) {
+  DDX_REQUIRE(dtype == DDX_BF16 || dtype == DDX_F16, "ddx_pcg_update_xr_pack16: dtype must be BF16 or F16");
   DDX_REQUIRE(R == 16 || R == 32 || R == 64, "ddx_pcg_update_xr_pack16: R must be 16, 32 or 64 (got %d)", R);
   DDX_REQUIRE(n >= 0 && r && p && q && pan_ptr && pan_row && b16 && st && ist && hist && partials && tickets,
               "ddx_pcg_update_xr_pack16: bad arguments");
@@ -322,12 +342,17 @@ int ddx_pcg_update_xr_pack16(int64_t n, int R, double* x, double* r, const doubl
   const int grid = red_grid(n * (R / 2));
   cudaStream_t s = (cudaStream_t)stream;
   unsigned char* b = (unsigned char*)b16;
-  if (R == 16)
-    k_update_xr_pack<16><<<grid, kThreads, 0, s>>>(n, S, x, r, p, q, pan_ptr, pan_row, b, partials, tickets + 0);
-  else if (R == 32)
-    k_update_xr_pack<32><<<grid, kThreads, 0, s>>>(n, S, x, r, p, q, pan_ptr, pan_row, b, partials, tickets + 0);
-  else
-    k_update_xr_pack<64><<<grid, kThreads, 0, s>>>(n, S, x, r, p, q, pan_ptr, pan_row, b, partials, tickets + 0);
+  auto go = [&](auto t16) {
+    using T16 = decltype(t16);
+    if (R == 16)
+      k_update_xr_pack<T16, 16><<<grid, kThreads, 0, s>>>(n, S, x, r, p, q, pan_ptr, pan_row, b, partials, tickets);
+    else if (R == 32)
+      k_update_xr_pack<T16, 32><<<grid, kThreads, 0, s>>>(n, S, x, r, p, q, pan_ptr, pan_row, b, partials, tickets);
+    else
+      k_update_xr_pack<T16, 64><<<grid, kThreads, 0, s>>>(n, S, x, r, p, q, pan_ptr, pan_row, b, partials, tickets);
+  };
+  if (dtype == DDX_F16) go(__half());
+  else go(__nv_bfloat16());
   DDX_LAUNCH_CHECK("ddx_pcg_update_xr_pack16");
   return DDX_OK;
 }

@@ -81,6 +81,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     if (MODE == DDX_SPMV_PQ) act = fin_pq(S, 0, tot[0]);
     if (MODE == DDX_SPMV_RES_INIT) act = fin_init(S, 0, tot[NV - 1], tot[0]);
     if (MODE == DDX_SPMV_RES_REPLACE) act = fin_replace(S, 0, tot[0]);
+    if (MODE >= DDX_SPMV_RES_INIT) S.s(DDX_ST_RR_PACK, 0) = S.s(DDX_ST_RR, 0);  // panels packed from this r
   }
   if (MODE != DDX_SPMV_PQ) publish_nactive(S, act);
   else {
@@ -133,6 +134,7 @@ __global__ void __launch_bounds__(kThreads)
     if (MODE == DDX_SPMV_PQ) act = fin_pq(S, jj, tot[0]);
     if (MODE == DDX_SPMV_RES_INIT) act = fin_init(S, jj, tot[NV - 1], tot[0]);
     if (MODE == DDX_SPMV_RES_REPLACE) act = fin_replace(S, jj, tot[0]);
+    if (MODE >= DDX_SPMV_RES_INIT) S.s(DDX_ST_RR_PACK, jj) = S.s(DDX_ST_RR, jj);  // panels packed from this r
   }
   publish_nactive(S, act);
 }
@@ -237,6 +239,7 @@ __global__ void __launch_bounds__(kThreads, 4)
     if (MODE == DDX_SPMV_PQ) act = fin_pq(S, jj, tot[0]);
     if (MODE == DDX_SPMV_RES_INIT) act = fin_init(S, jj, tot[NV - 1], tot[0]);
     if (MODE == DDX_SPMV_RES_REPLACE) act = fin_replace(S, jj, tot[0]);
+    if (MODE >= DDX_SPMV_RES_INIT) S.s(DDX_ST_RR_PACK, jj) = S.s(DDX_ST_RR, jj);  // panels packed from this r
   }
   publish_nactive(S, act);
 }

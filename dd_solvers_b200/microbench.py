@@ -58,7 +58,17 @@ def bench_apply(args) -> dict:
     import dd_solvers_b200 as dd
 
     dev = torch.device("cuda")
-    A, sub_ptr, sub_idx, R0 = _problem(args.n_el, args.parts)
+    if args.problem == "p1":
+        # jittered P1 mesh of n-el x n-el nodes, RCB into `parts` subdomains (the
+        # C5 family; 724^2 nodes / 256 parts gives C5's block sizes, ~2200 DOFs)
+        from . import partition, problems
+
+        P = problems.p1_jittered(args.n_el, 0.3, 1.0, 0)
+        owner = partition.rcb_owner(P.coords, args.parts)
+        A = P.matrix
+        sub_ptr, sub_idx = partition.overlapping_subdomains(A, owner, args.parts, 1)
+    else:
+        A, sub_ptr, sub_idx, R0 = _problem(args.n_el, args.parts)
     pc = dd.AdditiveSchwarz(torch.float64, dd.Inv(DT[args.precision]), None)
     pc.setup(dd.csr_to_torch(A).to(dev), subdomains=(sub_ptr, sub_idx))
     torch.cuda.empty_cache()  # release setup temporaries: a profiler then saves/restores less device memory

@@ -610,7 +610,14 @@ class SchwarzOperator(SparseSolver):
         terms = self._tc_terms(R) if self.use_tensor_cores else 0
         if terms:
             sym, stages = self._tc_config(R, terms)
-            self._tc_apply(r, s["ylocal"], R, terms, sym, stages, ist, None if packed else st, pack=not packed)
+            st_apply = st
+            if packed:
+                # panels written by the x/r update: BF16 with scale 1; FP16 scaled
+                # with the squared norms in st slot RR_PACK, which the apply reads
+                # in place of slot RR (ddx_pcg_update_xr_pack16_ex)
+                st_apply = (st[(L.ST_RR_PACK - L.ST_RR) * R:]
+                            if (st is not None and self.block_dtype == torch.float16) else None)
+            self._tc_apply(r, s["ylocal"], R, terms, sym, stages, ist, st_apply, pack=not packed)
             self._ymap = self._ymap_one  # one slice written
             return s["ylocal"]
         cfg = self._apply_config(R)
@@ -638,8 +645,8 @@ class SchwarzOperator(SparseSolver):
 
     def fused_pack_ok(self, R: int) -> bool:
         """The PCG update can write this operator's B panels itself: tensor-core
-        path with BF16 blocks and one residual term."""
-        return (self.use_tensor_cores and self.block_dtype == torch.bfloat16 and R in (16, 32, 64)
+        path with BF16 or FP16 blocks and one residual term."""
+        return (self.use_tensor_cores and self.block_dtype in (torch.bfloat16, torch.float16) and R in (16, 32, 64)
                 and self._tc_terms(R) == 1)
 
     def panel_rows(self, R: int):
@@ -657,11 +664,14 @@ class SchwarzOperator(SparseSolver):
             self._scratch[key] = got
         return got
 
-    def pack_panels(self, r: torch.Tensor, R: int) -> None:
-        """B panels of r with scale 1 (what ``ddx_pcg_update_xr_pack16`` writes)."""
+    def pack_panels(self, r: torch.Tensor, R: int, st: torch.Tensor | None = None) -> None:
+        """B panels of r as ``ddx_pcg_update_xr_pack16_ex`` writes them: BF16 with
+        scale 1; FP16 scaled from the PCG state's squared norms ``st`` (slot RR,
+        which the residual SpMV has just copied to RR_PACK)."""
         b16, panel_off = self._panels(R, 1)
+        st_pack = st if self.block_dtype == torch.float16 else None
         L.call("ddx_pack_panels16", self.n_solvers, R, L.ptr(self.sub_ptr), L.ptr(self.sub_idx), L.ptr(panel_off),
-               L.ptr(r), None, L.ptr(b16), L.DTYPE_CODE[self.block_dtype], 1, L.stream_ptr())
+               L.ptr(r), L.ptr(st_pack), L.ptr(b16), L.DTYPE_CODE[self.block_dtype], 1, L.stream_ptr())
 
     def _tc_candidates(self, R: int, terms: int) -> list[tuple[bool, int]]:
         """(symmetric tiles, ring stages) the tensor-core autotuner times: every
@@ -1307,9 +1317,9 @@ class CG(SparseSolver):
             # r (and x) and the next local apply's B panels in one pass
             pan_ptr, pan_row = self.preconditioner.panel_rows(R)
             b16, _ = self.preconditioner._panels(R, 1)
-            L.call("ddx_pcg_update_xr_pack16", self.n, R, L.ptr(x), L.ptr(w.r), L.ptr(w.p), L.ptr(w.q),
-                   L.ptr(pan_ptr), L.ptr(pan_row), L.ptr(b16), L.ptr(w.st), L.ptr(w.ist), L.ptr(w.hist),
-                   L.ptr(w.partials), L.ptr(w.tickets), L.stream_ptr())
+            L.call("ddx_pcg_update_xr_pack16_ex", self.n, R, L.ptr(x), L.ptr(w.r), L.ptr(w.p), L.ptr(w.q),
+                   L.ptr(pan_ptr), L.ptr(pan_row), L.ptr(b16), L.DTYPE_CODE[self.preconditioner.block_dtype],
+                   L.ptr(w.st), L.ptr(w.ist), L.ptr(w.hist), L.ptr(w.partials), L.ptr(w.tickets), L.stream_ptr())
         else:
             L.call("ddx_pcg_update_xr", self.n, R, L.ptr(x), L.ptr(w.r), L.ptr(w.p), L.ptr(w.q), L.ptr(w.st),
                    L.ptr(w.ist), L.ptr(w.hist), L.ptr(w.partials), L.ptr(w.tickets), L.stream_ptr())
@@ -1318,7 +1328,7 @@ class CG(SparseSolver):
                 self._flush_x(w)
             self.matrix.launch(w.x, w.r, R, L.SPMV_RES_REPLACE, w, b=w.b, use_sell=self.bsr_matmul)
             if w.fused_pack:
-                self.preconditioner.pack_panels(w.r, R)
+                self.preconditioner.pack_panels(w.r, R, w.st)
 
     def _flush_x(self, w: _PcgWork) -> None:
         """Applies the parked step of a deferred x update (x += alpha_x p)."""
@@ -1394,7 +1404,7 @@ class CG(SparseSolver):
             # buffer: let it run first, then the panels of the initial residual
             # (later ones come from the x/r update)
             pc._tc_config(Rp, 1)
-            pc.pack_panels(w.r, Rp)
+            pc.pack_panels(w.r, Rp, w.st)
 
         alphas, betas = [], []
         done = 0

@@ -49,7 +49,8 @@ enum {
   DDX_ST_BETA = 5, DDX_ST_RR = 6, DDX_ST_ATOL = 7, DDX_ST_BB = 8,
   DDX_ST_T0 = 9, DDX_ST_T1 = 10, /* parked column totals (DDX_G_DEFER) */
   DDX_ST_ALPHA_X = 11,            /* step length still to be applied to x (deferred x update) */
-  DDX_ST_COUNT = 12
+  DDX_ST_RR_PACK = 12,            /* ||r||^2 the current 16-bit B panels were scaled with */
+  DDX_ST_COUNT = 13
 };
 enum { DDX_IST_ACTIVE = 0, DDX_IST_ITERS = 1, DDX_IST_COUNT = 2 };
 enum {
@@ -139,6 +140,19 @@ int ddx_pcg_finalize(int R, int kind, double* st, int* ist, double* hist, ddx_st
 int ddx_pcg_update_xr_pack16(int64_t n, int R, double* x, double* r, const double* p, const double* q,
                              const int* pan_ptr, const int64_t* pan_row, void* b16, double* st, int* ist,
                              double* hist, double* partials, unsigned int* tickets, ddx_stream_t stream);
+/* The same for BF16 (dtype DDX_BF16, scale 1, as above) or FP16 (DDX_F16)
+ * panels. FP16 panels hold s_j r[d, j] with the power-of-two scale s_j of
+ * ddx_pack_panels16 taken from the squared norm this update starts from
+ * (st slot DDX_ST_RR before it is replaced); that squared norm is left in slot
+ * DDX_ST_RR_PACK, and the tensor-core apply that reads these panels must
+ * take its scales from there: pass it st + (DDX_ST_RR_PACK - DDX_ST_RR) * R
+ * (the SpMV residual modes also copy RR to RR_PACK, for panels that
+ * ddx_pack_panels16 writes from a freshly computed residual). The scale is a
+ * power of two, so the products equal those of panels scaled with the new
+ * norm except where an entry over- or underflows the 16-bit range. */
+int ddx_pcg_update_xr_pack16_ex(int64_t n, int R, double* x, double* r, const double* p, const double* q,
+                                const int* pan_ptr, const int64_t* pan_row, void* b16, int dtype, double* st,
+                                int* ist, double* hist, double* partials, unsigned int* tickets, ddx_stream_t stream);
 /* rho = r.z (and z.q when flexible) -> beta; for preconditioners that write z
  * themselves (generic path). q may be NULL on the first iteration. */
 int ddx_pcg_dots_rz(int64_t n, int R, const double* r, const double* z, const double* q, double* st,

@@ -209,16 +209,20 @@ def test_tc_every_tuning_candidate(cuda, prec, terms, R):
 
 
 @pytest.mark.parametrize("R", [16, 32, 64])
-def test_update_xr_writes_the_packed_panels(cuda, R):
-    """ddx_pcg_update_xr_pack16: x and r as the plain update computes them, the
-    B panels bitwise equal to packing the new r (scale 1), ||r||^2 per column
-    to rounding; overlapping 3D subdomains (DOFs in up to 8 panels)."""
+@pytest.mark.parametrize("prec", ["bf16", "f16"])
+def test_update_xr_writes_the_packed_panels(cuda, R, prec):
+    """ddx_pcg_update_xr_pack16_ex: x and r as the plain update computes them,
+    the B panels bitwise equal to packing the new r (BF16: scale 1; FP16: the
+    per-RHS scale of the squared norm the update started from, which it leaves
+    in slot RR_PACK), ||r||^2 per column to rounding; overlapping 3D subdomains
+    (DOFs in up to 8 panels)."""
     import dd_solvers_b200 as dd
     from dd_solvers_b200 import _lib as L
     from dd_solvers_b200.solvers import _PcgWork
 
+    dt = torch.bfloat16 if prec == "bf16" else torch.float16
     P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(3, 24, 3, kappa_seed=2)
-    pc = dd.HybridSchwarz(torch.float64, dd.Inv(torch.bfloat16), dd.CUDSS())
+    pc = dd.HybridSchwarz(torch.float64, dd.Inv(dt), dd.CUDSS())
     pc.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0)
     pc.rhs_terms = 1
     assert pc.fused_pack_ok(R)
@@ -229,37 +233,50 @@ def test_update_xr_writes_the_packed_panels(cuda, R):
     L.call("ddx_pcg_reset", R, L.ptr(w.st), L.ptr(w.ist), 10, 0, 1e-8, 0.0, L.stream_ptr())
     alpha = torch.rand(R, dtype=torch.float64, device=cuda, generator=g)
     w.st.view(L.ST_COUNT, R)[L.ST_ALPHA] = alpha
+    # the squared norms the update starts from: spread over many binades
+    rr_old = torch.logspace(-30, 30, R, dtype=torch.float64, device=cuda)
+    w.st.view(L.ST_COUNT, R)[L.ST_RR] = rr_old
     x0, r0 = x.clone(), r.clone()
     b16, _ = pc._panels(R, 1)
     b16.zero_()
     pan_ptr, pan_row = pc.panel_rows(R)
-    L.call("ddx_pcg_update_xr_pack16", n, R, L.ptr(x), L.ptr(r), L.ptr(p), L.ptr(q), L.ptr(pan_ptr), L.ptr(pan_row),
-           L.ptr(b16), L.ptr(w.st), L.ptr(w.ist), L.ptr(w.hist), L.ptr(w.partials), L.ptr(w.tickets), L.stream_ptr())
+    L.call("ddx_pcg_update_xr_pack16_ex", n, R, L.ptr(x), L.ptr(r), L.ptr(p), L.ptr(q), L.ptr(pan_ptr),
+           L.ptr(pan_row), L.ptr(b16), L.DTYPE_CODE[dt], L.ptr(w.st), L.ptr(w.ist), L.ptr(w.hist), L.ptr(w.partials),
+           L.ptr(w.tickets), L.stream_ptr())
     fused = b16.clone()
     a = alpha.repeat(n)
     assert torch.allclose(x, x0 + a * p, rtol=1e-15, atol=1e-15)
     assert torch.allclose(r, r0 - a * q, rtol=1e-15, atol=1e-15)
-    rr = w.st.view(L.ST_COUNT, R)[L.ST_RR]
-    assert torch.allclose(rr, (r.view(n, R) ** 2).sum(0), rtol=1e-12, atol=0)
+    st = w.st.view(L.ST_COUNT, R)
+    assert torch.allclose(st[L.ST_RR], (r.view(n, R) ** 2).sum(0), rtol=1e-12, atol=0)
     b16.zero_()
-    pc.pack_panels(r, R)
+    if prec == "f16":
+        assert torch.equal(st[L.ST_RR_PACK], rr_old)
+        ref_st = torch.zeros_like(w.st)
+        ref_st.view(L.ST_COUNT, R)[L.ST_RR] = rr_old
+        pc.pack_panels(r, R, ref_st)
+    else:
+        pc.pack_panels(r, R)
     assert torch.equal(fused, b16)
     assert L.device_error() == 0
 
 
 @pytest.mark.parametrize("R", [16, 64])
-def test_fused_panel_solve_matches_unfused(cuda, R):
-    """Multi-RHS BF16 tensor-core PCG with the panels written by the x/r update
-    against the same solve with a pack pass: the same iterates (only the norms'
-    summation order differs), so the same iteration counts and solutions to
-    rounding; with residual replacement too."""
+@pytest.mark.parametrize("prec", ["bf16", "f16"])
+def test_fused_panel_solve_matches_unfused(cuda, R, prec):
+    """Multi-RHS BF16 / FP16 tensor-core PCG with the panels written by the x/r
+    update against the same solve with a pack pass: the same iterates (only the
+    norms' summation order differs; FP16 panels scaled by a power of two from
+    the previous norm, which changes no product), so the same iteration counts
+    and solutions to rounding; with residual replacement too."""
     import dd_solvers_b200 as dd
 
+    dt = torch.bfloat16 if prec == "bf16" else torch.float16
     P, A, owner, nparts, sub_ptr, sub_idx, R0 = q1_case(3, 24, 3, kappa_seed=4, coarse="q1")
     B = torch.as_tensor(np.random.default_rng(R).standard_normal((A.shape[0], R)), device=cuda)
     out = {}
     for fuse in (True, False):
-        cg = dd.CG(dd.HybridSchwarz(torch.float64, dd.Inv(torch.bfloat16), dd.CUDSS()), rtol=1e-9,
+        cg = dd.CG(dd.HybridSchwarz(torch.float64, dd.Inv(dt), dd.CUDSS()), rtol=1e-9,
                    replace_every=8)
         cg.fuse_panels = fuse
         cg.setup(torch_csr(A, cuda), subdomains=(sub_ptr, sub_idx), coarse_restriction=R0, block_size=1)
