@@ -133,8 +133,13 @@ template <> __device__ __forceinline__ double2 load_pair<float>(const float* p) 
 // none, -2 when it has several; a DOF in one subdomain then costs a chain of
 // two dependent loads (dof_first, ylocal) instead of three (dof_ptr, dof_src,
 // ylocal). Same sums in the same order either way.
+// CTAs per SM the multi-RHS combine is compiled for (5 or 6, which spill a few
+// registers, measured slower on C3 and C5)
+#ifndef DDX_COMBINE_MIN_CTAS
+#define DDX_COMBINE_MIN_CTAS 4
+#endif
 template <typename ACC, int MODE>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, DDX_COMBINE_MIN_CTAS)
     k_combine2(int64_t n, PcgState S, const int* __restrict__ dof_ptr, const int* __restrict__ dof_src,
                const int* __restrict__ dof_first, const ACC* __restrict__ ylocal, const double* u, const int* __restrict__ p_ptr,
                const int* __restrict__ p_col, const double* __restrict__ p_val,
@@ -508,15 +513,24 @@ __global__ void __launch_bounds__(256) k_coarse_ksum(int64_t total, int S, const
 // the groups are summed in ascending g into partial[q, :]. ylocal streams
 // once, row by row, with no transpose-map gathers.
 constexpr int kRestrictMaxSlots = 16;
+// rows in flight per row group, and CTAs per SM the kernel is compiled for:
+// eight rows took 142 registers (one CTA per SM); four rows at three CTAs (78
+// registers) measured C3 2.78 -> 2.61 ms and C5 4.17 -> 3.99 ms per iteration
+#ifndef DDX_RESTRICT_ROWS
+#define DDX_RESTRICT_ROWS 4
+#endif
+#ifndef DDX_RESTRICT_MIN_CTAS
+#define DDX_RESTRICT_MIN_CTAS 3
+#endif
 template <typename ACC>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, DDX_RESTRICT_MIN_CTAS)
     k_restrict_sub(int n_sub, int R, const int64_t* __restrict__ sub_ptr, const int* __restrict__ slot_base,
                    const int* __restrict__ n_slots, const unsigned char* __restrict__ f_slot,
                    const double* __restrict__ f_val, const int* __restrict__ ov_ptr,
                    const unsigned char* __restrict__ ov_slot, const double* __restrict__ ov_val,
                    const ACC* __restrict__ ylocal, int slices, int64_t slice_rows, double* __restrict__ partial,
                    const int* ist) {
-  constexpr int U = 8;
+  constexpr int U = DDX_RESTRICT_ROWS;
   extern __shared__ double acc_sm[];  // [G][kRestrictMaxSlots][R]
   if (ist != nullptr && n_active(ist, R) == 0) return;
   const int tpr = R / 2;

@@ -150,8 +150,16 @@ __global__ void __launch_bounds__(kThreads)
 // consecutive steps, so the x rows the cluster's neighbourhood shares are read
 // from L2 once and then hit in L1 (a stencil row is read by up to 27 rows in
 // 3D; in the natural order only the ~3 neighbours along a grid line share L1).
+// CTAs per SM the multi-RHS SpMM is compiled for (register cap 65536 / (256 x
+// this)): the kernel is latency-bound, so occupancy pays; 6 CTAs (40 registers,
+// no spills) measured 0.354 / 1.482 / 0.353 ms against 0.414 / 1.631 / 0.405
+// with 4 on C3's 9-point rows at 64 RHS, a 27-point 128^3 problem at 64 RHS
+// and C5's P1 mesh at 16 RHS (5 CTAs: no gain)
+#ifndef DDX_SPMM_MIN_CTAS
+#define DDX_SPMM_MIN_CTAS 6
+#endif
 template <int MODE, bool ORDERED>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, DDX_SPMM_MIN_CTAS)
     k_spmm_csr2(int64_t n, const int* __restrict__ row_ptr, const int* __restrict__ cols,
                 const double* __restrict__ vals, const double* __restrict__ x, double* __restrict__ y,
                 const double* __restrict__ b, PcgState S, double* partials, unsigned int* ticket,
@@ -410,8 +418,20 @@ __global__ void __launch_bounds__(kThreads)
 // with column-major blocks, so the BS lanes of a block row read BS consecutive
 // values per column c (coalesced) and x[cols[blk] BS + c] is a broadcast; no
 // cross-lane reduction. The next block's column index is loaded ahead.
+// CTAs per SM the BSR kernel is compiled for: the unrolled block columns took
+// up to ~180 registers at bs = 20 without a cap (one CTA per SM); with three
+// CTAs (at most 80 registers, no spills) the kernel measured 0.75 -> 0.88 of
+// the copy peak at bs = 6, 0.74 -> 1.04 at bs = 15, 0.69 -> 0.96 at bs = 20,
+// and with five for bs <= 4 (48 registers) 0.72 -> 0.79 at bs = 3 and
+// 0.76 -> 0.91 at bs = 4
+#ifndef DDX_BSR_MIN_CTAS
+#define DDX_BSR_MIN_CTAS 3
+#endif
+#ifndef DDX_BSR_MIN_CTAS_SMALL  // bs <= 4
+#define DDX_BSR_MIN_CTAS_SMALL 5
+#endif
 template <typename T, int BS>
-__global__ void __launch_bounds__(256) k_spmv_bsr(int64_t nbr, const int* __restrict__ row_ptr,
+__global__ void __launch_bounds__(256, BS <= 4 ? DDX_BSR_MIN_CTAS_SMALL : DDX_BSR_MIN_CTAS) k_spmv_bsr(int64_t nbr, const int* __restrict__ row_ptr,
                                                   const int* __restrict__ cols, const T* __restrict__ vals,
                                                   const T* __restrict__ x, T* __restrict__ y) {
   constexpr int G = 32 / BS;
