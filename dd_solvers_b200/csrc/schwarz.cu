@@ -118,7 +118,7 @@ template <> __device__ __forceinline__ double2 load_pair<float>(const float* p) 
 }
 
 // R >= 2: R/2 threads per DOF, each owning two adjacent RHS columns (8/16-byte
-// loads), and U DOFs per thread in flight per step: the index loads, the first
+// loads), and U (DDX_COMBINE_U) DOFs per thread in flight per step: the index loads, the first
 // transpose-map entry, u and the prolongation of all U DOFs are issued before
 // any store. (u may alias z, so a one-element loop cannot
 // start the next element's loads before the previous store: every element
@@ -134,9 +134,14 @@ template <> __device__ __forceinline__ double2 load_pair<float>(const float* p) 
 // two dependent loads (dof_first, ylocal) instead of three (dof_ptr, dof_src,
 // ylocal). Same sums in the same order either way.
 // CTAs per SM the multi-RHS combine is compiled for (5 or 6, which spill a few
-// registers, measured slower on C3 and C5)
+// registers, measured slower on C3 and C5), and DOFs in flight per thread (4:
+// C3 2.664 -> 2.645 ms per iteration against 3; 2, or 4 at three CTAs per SM,
+// slower)
 #ifndef DDX_COMBINE_MIN_CTAS
 #define DDX_COMBINE_MIN_CTAS 4
+#endif
+#ifndef DDX_COMBINE_U
+#define DDX_COMBINE_U 4
 #endif
 template <typename ACC, int MODE>
 __global__ void __launch_bounds__(kThreads, DDX_COMBINE_MIN_CTAS)
@@ -146,7 +151,7 @@ __global__ void __launch_bounds__(kThreads, DDX_COMBINE_MIN_CTAS)
                const double* __restrict__ yc, double sign, double* z, int dots,
                const double* r, const double* __restrict__ q, double* partials,
                unsigned int* ticket) {
-  constexpr int U = 3;
+  constexpr int U = DDX_COMBINE_U;
   __shared__ double red[kThreads];
   const int R = S.R;
   if (S.ist != nullptr && n_active(S.ist, R) == 0) return;
@@ -702,7 +707,7 @@ int ddx_schwarz_combine_ex(int64_t n, int R, const int* dof_ptr, const int* dof_
                     ((uintptr_t)q & 15u) == 0 && ((uintptr_t)yc & 15u) == 0 &&
                     ((uintptr_t)ylocal & (f64 ? 15u : 7u)) == 0,
                 "ddx_schwarz_combine: vectors must be 16-byte aligned for R >= 2");
-    const int grid2 = red_grid(ceil_div(n * (R / 2), 3));
+    const int grid2 = red_grid(ceil_div(n * (R / 2), DDX_COMBINE_U));
     if (z != nullptr) {
       if (f64)
         k_combine2<double, 0><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, dof_first, (const double*)ylocal, u, p_ptr,
@@ -754,7 +759,7 @@ int ddx_schwarz_combine_update(int64_t n, int R, const int* dof_ptr, const int* 
   // not depend on it, but keeping it keeps the memory behaviour alike)
   PcgState S{const_cast<double*>(st), const_cast<int*>(ist), nullptr, R};
   cudaStream_t s = (cudaStream_t)stream;
-  const int grid2 = red_grid(ceil_div(n * (R / 2), 3));
+  const int grid2 = red_grid(ceil_div(n * (R / 2), DDX_COMBINE_U));
   if (f64)
     k_combine2<double, 2><<<grid2, kThreads, 0, s>>>(n, S, dof_ptr, dof_src, dof_first, (const double*)ylocal, u, p_ptr, p_col,
                                                      p_val, yc, sign, p, 0, x, nullptr, nullptr, nullptr);
