@@ -966,7 +966,8 @@ def main():
     if rank == 0 and world == 1 and args.workload == "c2" and not args.no_reference_experiment:
         out["reference_experiment"] = reference_experiment()
     if rank == 0:
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:
+            # the CPU baseline is measured at N = 1 only (the other ranks would wait on it)
             out["cpu_baseline"] = cpu_baseline(spec, prob, cal, out["unit"])
         if world == 1 and args.workload == "c2" and args.multi_rhs:
             cal.clear()
