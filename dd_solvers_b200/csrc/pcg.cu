@@ -72,6 +72,17 @@ __global__ void k_update_p(int64_t n, int R, const double* __restrict__ z, doubl
     }
     return;
   }
+  if (R == 1 && (((uintptr_t)z | (uintptr_t)p) & 15u) == 0) {
+    // one right-hand side: element pairs with 16-byte loads
+    const int64_t npair = total / 2;
+    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int64_t i = t0; i < npair; i += stride) {
+      const double2 pv = reinterpret_cast<const double2*>(p)[i], zv = reinterpret_cast<const double2*>(z)[i];
+      reinterpret_cast<double2*>(p)[i] = make_double2(fma(beta, pv.x, zv.x), fma(beta, pv.y, zv.y));
+    }
+    if ((total & 1) && t0 == 0) p[total - 1] = fma(beta, p[total - 1], z[total - 1]);
+    return;
+  }
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
     p[i] = fma(beta, p[i], z[i]);
   }
@@ -108,11 +119,53 @@ __global__ void __launch_bounds__(kThreads) k_update_xr(int64_t n, PcgState S, d
   const double alpha = S.st[DDX_ST_ALPHA * R + j];
   const bool defer_x = x == nullptr;  // x += alpha p left to the next p update
   double acc[1] = {0.0};
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-    if (!defer_x) x[i] = fma(alpha, p[i], x[i]);
-    const double ri = fma(-alpha, q[i], r[i]);
-    r[i] = ri;
-    acc[0] = fma(ri, ri, acc[0]);
+  const bool aligned = (((uintptr_t)x | (uintptr_t)r | (uintptr_t)p | (uintptr_t)q) & 15u) == 0;
+  if (R == 1 && aligned) {
+    // one right-hand side: element pairs with 16-byte loads, two pairs in flight
+    const int64_t npair = total / 2;
+    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int64_t i = t0; i < npair; i += 2 * stride) {
+      const bool two = i + stride < npair;
+      const double2 qa = reinterpret_cast<const double2*>(q)[i], ra = reinterpret_cast<const double2*>(r)[i];
+      double2 qb = make_double2(0.0, 0.0), rb = qb;
+      if (two) {
+        qb = reinterpret_cast<const double2*>(q)[i + stride];
+        rb = reinterpret_cast<const double2*>(r)[i + stride];
+      }
+      if (!defer_x) {
+        const double2 pa = reinterpret_cast<const double2*>(p)[i], xa = reinterpret_cast<const double2*>(x)[i];
+        reinterpret_cast<double2*>(x)[i] = make_double2(fma(alpha, pa.x, xa.x), fma(alpha, pa.y, xa.y));
+        if (two) {
+          const double2 pb = reinterpret_cast<const double2*>(p)[i + stride];
+          const double2 xb = reinterpret_cast<const double2*>(x)[i + stride];
+          reinterpret_cast<double2*>(x)[i + stride] = make_double2(fma(alpha, pb.x, xb.x), fma(alpha, pb.y, xb.y));
+        }
+      }
+      const double2 na = make_double2(fma(-alpha, qa.x, ra.x), fma(-alpha, qa.y, ra.y));
+      reinterpret_cast<double2*>(r)[i] = na;
+      acc[0] = fma(na.x, na.x, acc[0]);
+      acc[0] = fma(na.y, na.y, acc[0]);
+      if (two) {
+        const double2 nb = make_double2(fma(-alpha, qb.x, rb.x), fma(-alpha, qb.y, rb.y));
+        reinterpret_cast<double2*>(r)[i + stride] = nb;
+        acc[0] = fma(nb.x, nb.x, acc[0]);
+        acc[0] = fma(nb.y, nb.y, acc[0]);
+      }
+    }
+    if ((total & 1) && t0 == 0) {  // an odd length: the last element
+      const int64_t i = total - 1;
+      if (!defer_x) x[i] = fma(alpha, p[i], x[i]);
+      const double ri = fma(-alpha, q[i], r[i]);
+      r[i] = ri;
+      acc[0] = fma(ri, ri, acc[0]);
+    }
+  } else {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+      if (!defer_x) x[i] = fma(alpha, p[i], x[i]);
+      const double ri = fma(-alpha, q[i], r[i]);
+      r[i] = ri;
+      acc[0] = fma(ri, ri, acc[0]);
+    }
   }
   write_cta_partials<1>(acc, red, R, partials);
   if (!last_cta_arrival(ticket)) return;

@@ -318,8 +318,8 @@ __global__ void __launch_bounds__(kThreads, DDX_COMBINE_MIN_CTAS)
 // ---------------------------------------------------------------------------
 // dense coarse solve: yc = Ainv w  (Ainv symmetric, row-major)
 // ---------------------------------------------------------------------------
-// R = 1: one warp per row, lanes stride the row in 16-byte pairs (four pairs
-// in flight per lane), shuffle-tree reduction. A row of odd length n_c starts
+// R = 1: one warp per row, lanes stride the row in 16-byte pairs (eight pairs
+// in flight per lane, then four), shuffle-tree reduction. A row of odd length n_c starts
 // 8 bytes off a 16-byte boundary on every other row: its first entry is
 // taken as a scalar head.
 __global__ void k_coarse_gemv1(int n_c, const double* __restrict__ Ainv, const double* __restrict__ w,
@@ -335,6 +335,17 @@ __global__ void k_coarse_gemv1(int n_c, const double* __restrict__ Ainv, const d
   const double* wh = w + head;
   double s0 = 0.0, s1 = 0.0;
   int c = lane;
+  // eight pairs in flight per lane
+  for (; c + 224 < m; c += 256) {
+    double2 v[8];
+#pragma unroll
+    for (int h = 0; h < 8; ++h) v[h] = __ldcs(a2 + c + 32 * h);
+#pragma unroll
+    for (int h = 0; h < 8; ++h) {
+      s0 = fma(v[h].x, __ldg(wh + 2 * c + 64 * h), s0);
+      s1 = fma(v[h].y, __ldg(wh + 2 * c + 64 * h + 1), s1);
+    }
+  }
   for (; c + 96 < m; c += 128) {
     const double2 v0 = __ldcs(a2 + c), v1 = __ldcs(a2 + c + 32), v2 = __ldcs(a2 + c + 64), v3 = __ldcs(a2 + c + 96);
     s0 = fma(v0.x, __ldg(wh + 2 * c), s0);
