@@ -500,10 +500,13 @@ class SchwarzOperator(SparseSolver):
         # multi-RHS combine's short path (one-slice ylocal)
         self._dof_first = None
         if not identity:
-            cnt = (self.dof_ptr[1:] - self.dof_ptr[:-1]).to(torch.int64)
-            first = self.dof_src.to(torch.int64)[self.dof_ptr[:-1].to(torch.int64).clamp(max=max(
-                int(self.dof_src.numel()) - 1, 0))] if self.dof_src.numel() else torch.zeros_like(cnt)
-            self._dof_first = torch.where(cnt == 1, first, torch.where(cnt == 0, -1, -2)).to(torch.int32)
+            starts = self.dof_ptr[:-1].to(torch.int64)
+            cnt = self.dof_ptr[1:].to(torch.int64) - starts
+            first = torch.full_like(cnt, -2)
+            first[cnt == 0] = -1
+            single = cnt == 1
+            first[single] = self.dof_src.to(torch.int64)[starts[single]]
+            self._dof_first = first.to(torch.int32)
         if self.parts > 1:
             S = self.parts
             total = int(self.sub_idx.numel())

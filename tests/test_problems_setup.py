@@ -477,7 +477,9 @@ def test_row_clusters(cluster):
         nb = np.mean([len(np.unique(A[o[i:i + 64]].indices)) for i in range(0, n - 64, 64)])
         nat = np.mean([len(np.unique(A[i:i + 64].indices)) for i in range(0, n - 64, 64)])
         assert nb < 0.7 * nat, (nb, nat)
-    bad = torch.as_tensor(np.array([0, 1, 2], dtype=np.int64))
+    # a column out of range is refused (the tensors stay referenced during the call)
+    bad_ptr = torch.as_tensor(np.array([0, 1, 2], dtype=np.int64))
+    bad_idx = torch.as_tensor([0, 5], dtype=torch.int64)
+    bad_out = torch.empty(2, dtype=torch.int32)
     with pytest.raises(L.DDXError):
-        L.call("ddx_row_clusters", 2, bad.data_ptr(), torch.as_tensor([0, 5], dtype=torch.int64).data_ptr(), 4,
-               torch.empty(2, dtype=torch.int32).data_ptr())
+        L.call("ddx_row_clusters", 2, bad_ptr.data_ptr(), bad_idx.data_ptr(), 4, bad_out.data_ptr())
