@@ -813,30 +813,36 @@ class SchwarzOperator(SparseSolver):
             return (0, 0)  # library defaults
         return self.tune()
 
-    def tune(self, R: int = 1, reps: int = 3) -> tuple[int, int]:
+    def tune(self, R: int = 1, reps: int = 3, rounds: int = 2) -> tuple[int, int]:
         """Project autotuner: times every candidate configuration of the SIMT
         local apply on this operator's own blocks (CUDA events, after one
-        warm-up launch, ``R`` right-hand sides per launch) and keeps the
-        fastest; results are cached per (precision, layout, sizes) for the
-        process and used for every R."""
+        warm-up launch, ``R`` right-hand sides per launch; ``rounds`` passes over
+        the candidates, the minimum per candidate kept, so that a clock ramp
+        during the first pass does not decide) and keeps the fastest; results
+        are cached per (precision, layout, sizes) for the process and used for
+        every R."""
         s = self.scratch(R)
         r = torch.randn(self.n * R, dtype=torch.float64, device=self.device)
-        best, best_ms, timings = (0, 0), float("inf"), {}
-        for g, kb in self.tune_candidates:
-            try:
-                self._simt_apply(r, s["ylocal"], R, None, g, kb)
-            except L.DDXError:
-                continue  # e.g. shared memory too small for this shape
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            for _ in range(reps):
-                self._simt_apply(r, s["ylocal"], R, None, g, kb)
-            e1.record()
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / reps
-            timings[(g, kb)] = ms
-            if ms < best_ms:
-                best, best_ms = (g, kb), ms
+        timings = {}
+        for _ in range(max(1, rounds)):
+            for g, kb in self.tune_candidates:
+                if timings.get((g, kb)) == float("inf"):
+                    continue
+                try:
+                    self._simt_apply(r, s["ylocal"], R, None, g, kb)
+                except L.DDXError:
+                    timings[(g, kb)] = float("inf")  # e.g. shared memory too small for this shape
+                    continue
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(reps):
+                    self._simt_apply(r, s["ylocal"], R, None, g, kb)
+                e1.record()
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / reps
+                timings[(g, kb)] = min(ms, timings.get((g, kb), float("inf")))
+        timings = {k: v for k, v in timings.items() if v < float("inf")}
+        best = min(timings, key=timings.get) if timings else (0, 0)
         SchwarzOperator._tuned[self._tune_key()] = best
         self.tune_timings = timings
         return best
