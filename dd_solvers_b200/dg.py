@@ -5,8 +5,9 @@ The reference assembles its benchmark systems with DOLFINx
 uniform triangle meshes (``src/experiments/experiments/meshing.py:204-263``)
 and solves them with its Schwarz-preconditioned CG
 (``src/experiments/experiments/experiments.py:175-300``). DOLFINx is not part of
-this package, so this module restates that discretisation for P1 on the 2D
-uniform family, in torch (CPU or CUDA), FP64:
+this package, so this module restates that discretisation on the 2D uniform
+family, in torch (CPU or CUDA), FP64, for the degrees of the reference's logged
+runs (p = 1, 3, 5; any p >= 1 works):
 
 * ``uniform_mesh_2d(m)`` - the mesh ``S_m``: the unit square split into two
   right isosceles triangles along the (0,0)-(1,1) diagonal
@@ -35,6 +36,12 @@ uniform family, in torch (CPU or CUDA), FP64:
 All the formulas are exact for P1 (the integrands are polynomials of degree at
 most 3 on each edge), so they differ from DOLFINx's quadrature only by
 rounding.
+
+* ``sipg(mesh, case, degree)`` - the same form in the degree-p space of
+  DOLFINx's ``("DG", p)`` (nodes: ``reference_nodes``, basix's GLL-warped
+  Lagrange points in its DOF order), assembled with the nodal basis and
+  quadrature rules exact for every integrand; ``load_vector`` and
+  ``l2_error_p`` for the same space.
 """
 from __future__ import annotations
 
@@ -292,14 +299,27 @@ def sipg_p1(mesh: TriangleMesh, case: TestCase = CONTINUOUS_COEFFICIENT_2D) -> D
     blocks_self = blocks_self.index_add(0, c1, M[:, :3, :3])
     blocks_self = blocks_self.index_add(0, c2, M[:, 3:, 3:])
     blocks_self = blocks_self.index_add(0, cb, Mb)
+    A = _block_csr(n, 3, blocks_self, c1, c2, M)
 
+    # load vector: int f_I v with f interpolated at the vertices
+    fv = case.f(p[..., 0], p[..., 1])
+    mref = torch.tensor([[2.0, 1, 1], [1, 2, 1], [1, 1, 2]], dtype=torch.float64, device=dev)
+    load = ((area / 12)[:, None] * (fv @ mref)).reshape(-1)
+    return DGSystem(A, load, 3, mesh)
+
+
+def _block_csr(n: int, bs: int, blocks_self, c1, c2, M) -> torch.Tensor:
+    """Scalar CSR (sorted columns) of the block matrix with diagonal blocks
+    ``blocks_self`` (n, bs, bs) and, for every interior edge ``e``, the
+    coupling blocks ``M[e, :bs, bs:]`` (row cell ``c1[e]``, column ``c2[e]``)
+    and ``M[e, bs:, :bs]`` (row ``c2[e]``, column ``c1[e]``)."""
+    dev = blocks_self.device
     # block-sparse rows: the cell itself and its interior-edge neighbours
     rows = torch.cat([torch.arange(n, device=dev), c1, c2])
     cols = torch.cat([torch.arange(n, device=dev), c2, c1])
-    vals = torch.cat([blocks_self, M[:, :3, 3:], M[:, 3:, :3]])
+    vals = torch.cat([blocks_self, M[:, :bs, bs:], M[:, bs:, :bs]])
     order = torch.argsort(rows * n + cols)
     rows, cols, vals = rows[order], cols[order], vals[order]
-    bs = 3
     counts = torch.bincount(rows, minlength=n)
     # scalar CSR: block row r, local row i -> the row's blocks in column order
     per_row = (counts * bs).repeat_interleave(bs)
@@ -318,10 +338,261 @@ def sipg_p1(mesh: TriangleMesh, case: TestCase = CONTINUOUS_COEFFICIENT_2D) -> D
     ii = ent_row % bs
     col = cols[blk] * bs + jj
     val = vals[blk, ii, jj]
-    A = torch.sparse_csr_tensor(crow, col, val, (n * bs, n * bs))
+    return torch.sparse_csr_tensor(crow, col, val, (n * bs, n * bs))
 
-    # load vector: int f_I v with f interpolated at the vertices
-    fv = case.f(p[..., 0], p[..., 1])
-    mref = torch.tensor([[2.0, 1, 1], [1, 2, 1], [1, 1, 2]], dtype=torch.float64, device=dev)
-    load = ((area / 12)[:, None] * (fv @ mref)).reshape(-1)
-    return DGSystem(A, load, bs, mesh)
+
+# ---------------------------------------------------------------------------
+# Higher degrees: DOLFINx's ("DG", p) space on triangles, p = 1..5
+# ---------------------------------------------------------------------------
+
+def _gll_points(n: int):
+    """The n + 1 Gauss-Lobatto-Legendre points on [0, 1], ascending: the
+    ends and the roots of P_n' (Newton-polished)."""
+    import numpy as np
+    from numpy.polynomial import legendre as leg
+
+    if n == 1:
+        return np.array([0.0, 1.0])
+    c = np.zeros(n + 1)
+    c[n] = 1.0
+    d1, d2 = leg.legder(c), leg.legder(c, 2)
+    r = np.sort(leg.legroots(d1).real)
+    for _ in range(4):
+        r = r - leg.legval(r, d1) / leg.legval(r, d2)
+    return np.concatenate([[0.0], (1.0 + r) / 2.0, [1.0]])
+
+
+def _warp(n: int, x):
+    """1D warp: the displacement of the GLL points from the equispaced ones,
+    interpolated at ``x`` by the degree-n Lagrange polynomial on the
+    equispaced points."""
+    import numpy as np
+
+    eq = np.arange(n + 1) / n
+    disp = _gll_points(n) - eq
+    out = np.zeros_like(x)
+    for k in range(n + 1):
+        lk = np.ones_like(x)
+        for m in range(n + 1):
+            if m != k:
+                lk = lk * (x - eq[m]) / (eq[k] - eq[m])
+        out = out + disp[k] * lk
+    return out
+
+
+def reference_nodes(degree: int):
+    """Nodes of the degree-p Lagrange element on the reference triangle
+    (0,0), (1,0), (0,1), in the DOF order of basix (the element library under
+    ``fem.functionspace(mesh, ("DG", p))``, ``discretization.py:38``):
+    the three vertices; the interior points of edge 0 (vertex 1 -> 2), edge 1
+    (0 -> 2) and edge 2 (0 -> 1); then the interior lattice points, row by
+    row. Its default variant for this space places them GLL-warped: edge
+    points at the GLL points, interior points by the warp-and-blend map of
+    Hesthaven and Warburton (Nodal Discontinuous Galerkin Methods, 2008,
+    sec. 6.1) without the optimised blend exponent - a point with barycentric
+    lattice coordinates (x, y, a) = (i, j, l) / p moves along each edge
+    direction by ``lambda_u lambda_v warp(r) / (r (1 - r))`` with
+    ``r = (1 + lambda_v - lambda_u) / 2``. For p <= 2 this is the equispaced
+    lattice. The choice is pinned by the load-vector norms that the reference
+    logged for its P3 and P5 runs."""
+    import numpy as np
+
+    n = int(degree)
+    if n < 1:
+        raise ValueError("degree must be >= 1")
+    g = _gll_points(n)[1:-1]
+    pts = [(0.0, 0.0), (1.0, 0.0), (0.0, 1.0)]
+    pts += [(1.0 - t, t) for t in g]
+    pts += [(0.0, t) for t in g]
+    pts += [(t, 0.0) for t in g]
+    r = np.linspace(0.0, 1.0, 2 * n + 1)
+    wbar = _warp(n, r)
+    wbar[1:-1] /= r[1:-1] * (1.0 - r[1:-1])
+    wbar[0] = wbar[-1] = 0.0
+    for j in range(1, n):
+        for i in range(1, n - j):
+            l = n - i - j
+            x, y, a = i / n, j / n, l / n
+            pts.append((x + x * (a * wbar[n + i - l] + y * wbar[n + i - j]),
+                        y + y * (a * wbar[n + j - l] + x * wbar[n + j - i])))
+    return np.array(pts, dtype=np.float64)
+
+
+def _legendre_basis(n: int, x, y):
+    """Values and x/y derivatives of L_a(2x-1) L_b(2y-1), a + b <= n: a
+    well-conditioned basis of P_n for the nodal interpolation."""
+    import numpy as np
+    from numpy.polynomial import legendre as leg
+
+    u, v = 2.0 * x - 1.0, 2.0 * y - 1.0
+    vals, dx, dy = [], [], []
+    for a in range(n + 1):
+        ca = np.zeros(a + 1)
+        ca[a] = 1.0
+        La, dLa = leg.legval(u, ca), 2.0 * leg.legval(u, leg.legder(ca))
+        for b in range(n + 1 - a):
+            cb = np.zeros(b + 1)
+            cb[b] = 1.0
+            Lb, dLb = leg.legval(v, cb), 2.0 * leg.legval(v, leg.legder(cb))
+            vals.append(La * Lb)
+            dx.append(dLa * Lb)
+            dy.append(La * dLb)
+    return np.stack(vals, -1), np.stack(dx, -1), np.stack(dy, -1)
+
+
+def nodal_basis(degree: int, x, y):
+    """Values and reference derivatives (each (..., n_b)) of the nodal basis
+    of ``reference_nodes(degree)`` at the points (x, y)."""
+    import numpy as np
+
+    P = reference_nodes(degree)
+    V, _, _ = _legendre_basis(degree, P[:, 0], P[:, 1])
+    Vi = np.linalg.inv(V)
+    v, dx, dy = _legendre_basis(degree, np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64))
+    return v @ Vi, dx @ Vi, dy @ Vi
+
+
+def _triangle_rule(q: int):
+    """Collapsed Gauss-Legendre rule on the reference triangle (q^2 points,
+    weights summing to 1/2): exact for polynomials of degree <= 2q - 2."""
+    import numpy as np
+    from numpy.polynomial import legendre as leg
+
+    t, w = leg.leggauss(q)
+    t, w = (t + 1.0) / 2.0, w / 2.0
+    u, v = np.meshgrid(t, t, indexing="ij")
+    wu, wv = np.meshgrid(w, w, indexing="ij")
+    return (u * (1.0 - v)).ravel(), v.ravel(), (wu * wv * (1.0 - v)).ravel()
+
+
+def sipg(mesh: TriangleMesh, case: TestCase = CONTINUOUS_COEFFICIENT_2D, degree: int = 1) -> DGSystem:
+    """Assemble ``discretization.py:43-76`` (exact form) in the degree-p DG
+    space on ``mesh``: DOF ``n_b c + i`` is node ``i`` (``reference_nodes``
+    order) of cell ``c``, ``n_b = (p + 1)(p + 2) / 2``. ``rho`` and ``f`` are
+    interpolated at the nodes as DOLFINx does; every integrand is then a
+    polynomial, integrated exactly (collapsed Gauss on the cells, Gauss on the
+    edges: ``rho_I grad u . grad v`` has degree <= 2p, the edge terms <= 3p;
+    on an interior edge both traces of ``rho_I`` interpolate the same points,
+    so the harmonic mean ``rho+ rho- / (rho+ + rho-)`` is the polynomial
+    ``rho_I / 2`` up to rounding). For p = 1 the closed form of ``sipg_p1``
+    is used."""
+    if int(degree) == 1:
+        return sipg_p1(mesh, case)
+    return _sipg_quadrature(mesh, case, int(degree))
+
+
+def _sipg_quadrature(mesh: TriangleMesh, case: TestCase, p_deg: int) -> DGSystem:
+    """``sipg`` by quadrature, for any degree (p = 1 included, where it agrees
+    with the closed form to rounding)."""
+    import numpy as np
+
+    dev = mesh.cells.device
+    f64 = dict(dtype=torch.float64, device=dev)
+    n = mesh.n_cells
+    delta = case.delta * p_deg ** 2
+    p, g, _, _ = _cell_geometry(mesh, case.rho)
+    xy, det = _nodes_physical(mesh, p_deg)
+    nb = xy.shape[1]
+    rho_n = case.rho(xy[..., 0], xy[..., 1])  # (n, nb) interpolated coefficient
+
+    # cells: rho_I grad phi_i . grad phi_j, grad = D_xi g1 + D_eta g2
+    X, Y, W = _triangle_rule(p_deg + 2)
+    Ph, Dx, Dy = (torch.tensor(a, **f64) for a in nodal_basis(p_deg, X, Y))
+    Wt = torch.tensor(W, **f64)
+    R = (rho_n @ Ph.T) * Wt * det[:, None]  # (n, Q)
+    g1, g2 = g[:, 1], g[:, 2]
+    Bxx = torch.einsum("qi,qj->qij", Dx, Dx).reshape(len(W), -1)
+    Byy = torch.einsum("qi,qj->qij", Dy, Dy).reshape(len(W), -1)
+    Bxy = (torch.einsum("qi,qj->qij", Dx, Dy) + torch.einsum("qi,qj->qij", Dy, Dx)).reshape(len(W), -1)
+    blocks_self = ((R @ Bxx) * (g1 * g1).sum(1, keepdim=True) + (R @ Byy) * (g2 * g2).sum(1, keepdim=True)
+                   + (R @ Bxy) * (g1 * g2).sum(1, keepdim=True)).reshape(n, nb, nb)
+    load = load_vector(mesh, case, p_deg)
+    del R
+
+    # edge traces: local edge o runs from vertex (o+1)%3 to (o+2)%3 (dir 0) or back (dir 1)
+    te, we = np.polynomial.legendre.leggauss(p_deg + 2)
+    te, we = (te + 1.0) / 2.0, torch.tensor(we / 2.0, **f64)
+    V = np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]])
+    tv, tdx, tdy = [], [], []
+    for o in range(3):
+        for d in range(2):
+            a, b = ((o + 1) % 3, (o + 2) % 3) if d == 0 else ((o + 2) % 3, (o + 1) % 3)
+            pt = V[a][None, :] + te[:, None] * (V[b] - V[a])[None, :]
+            v, dx, dy = nodal_basis(p_deg, pt[:, 0], pt[:, 1])
+            tv.append(v)
+            tdx.append(dx)
+            tdy.append(dy)
+    Tv, Tdx, Tdy = (torch.tensor(np.stack(a), **f64) for a in (tv, tdx, tdy))  # (6, qe, nb)
+
+    def side(c, o, d, nrm):
+        k = o * 2 + d
+        U = Tv[k]  # (E, qe, nb)
+        Gn = Tdx[k] * (nrm * g[c, 1]).sum(1)[:, None, None] + Tdy[k] * (nrm * g[c, 2]).sum(1)[:, None, None]
+        rho_e = torch.einsum("eti,ei->et", U, rho_n[c])
+        return U, Gn, rho_e
+
+    (c1, o1, c2, o2), (cb, ob) = _edge_tables(mesh)
+    a1 = (o1 + 1) % 3
+    same = (p[c2, (o2 + 1) % 3] == p[c1, a1]).all(dim=1)
+    n_plus = -g[c1, o1] / torch.linalg.norm(g[c1, o1], dim=1, keepdim=True)
+    h = torch.linalg.norm(p[c1, (o1 + 2) % 3] - p[c1, a1], dim=1)
+    U1, G1, r1 = side(c1, o1, torch.zeros_like(o1), n_plus)
+    U2, G2, r2 = side(c2, o2, (~same).to(torch.int64), n_plus)
+    wq = we * (r1 * r2 / (r1 + r2))  # (E, qe)
+    U = torch.cat([U1, -U2], 2)
+    G = torch.cat([G1, G2], 2)
+    del U1, U2, G1, G2
+    F = h[:, None, None] * torch.einsum("et,eti,etj->eij", wq, G, U)
+    M = delta * torch.einsum("et,eti,etj->eij", wq, U, U) - F - F.transpose(1, 2)
+    del F, U, G
+
+    nb_out = -g[cb, ob] / torch.linalg.norm(g[cb, ob], dim=1, keepdim=True)
+    hb = torch.linalg.norm(p[cb, (ob + 2) % 3] - p[cb, (ob + 1) % 3], dim=1)
+    Ub, Gb, rb = side(cb, ob, torch.zeros_like(ob), nb_out)
+    wb = we * rb
+    Fb = hb[:, None, None] * torch.einsum("et,eti,etj->eij", wb, Gb, Ub)
+    Mb = delta * torch.einsum("et,eti,etj->eij", wb, Ub, Ub) - Fb - Fb.transpose(1, 2)
+
+    blocks_self = blocks_self.index_add(0, c1, M[:, :nb, :nb])
+    blocks_self = blocks_self.index_add(0, c2, M[:, nb:, nb:])
+    blocks_self = blocks_self.index_add(0, cb, Mb)
+    A = _block_csr(n, nb, blocks_self, c1, c2, M)
+    return DGSystem(A, load, nb, mesh)
+
+
+def _nodes_physical(mesh: TriangleMesh, degree: int):
+    """(n, n_b, 2) node coordinates of every cell, the cell's area x 2."""
+    P = torch.tensor(reference_nodes(degree), dtype=torch.float64, device=mesh.cells.device)
+    p = mesh.vertices[mesh.cells]
+    d1, d2 = p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]
+    det = (d1[:, 0] * d2[:, 1] - d2[:, 0] * d1[:, 1]).abs()
+    return p[:, None, 0] + P[None, :, 0, None] * d1[:, None] + P[None, :, 1, None] * d2[:, None], det
+
+
+def load_vector(mesh: TriangleMesh, case: TestCase = CONTINUOUS_COEFFICIENT_2D, degree: int = 1) -> torch.Tensor:
+    """``int f_I v`` for every DOF of the degree-p space (``discretization.py:
+    90-92``): f interpolated at the nodes, times the exact reference mass
+    matrix."""
+    xy, det = _nodes_physical(mesh, degree)
+    X, Y, W = _triangle_rule(int(degree) + 2)
+    Ph = torch.tensor(nodal_basis(degree, X, Y)[0], dtype=torch.float64, device=xy.device)
+    Mref = torch.einsum("q,qi,qj->ij", torch.tensor(W, dtype=torch.float64, device=xy.device), Ph, Ph)
+    return (det[:, None] * (case.f(xy[..., 0], xy[..., 1]) @ Mref)).reshape(-1)
+
+
+def l2_error_p(mesh: TriangleMesh, u, solution, degree: int) -> float:
+    """``||u_h - u||_L2`` of a degree-p field (DOF ``n_b c + i`` = node ``i``
+    of cell ``c``) by a collapsed Gauss rule exact to degree 2p + 4."""
+    if int(degree) == 1:
+        return l2_error(mesh, u, solution)
+    p = mesh.vertices[mesh.cells]
+    d1, d2 = p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]
+    det = (d1[:, 0] * d2[:, 1] - d2[:, 0] * d1[:, 1]).abs()
+    X, Y, W = _triangle_rule(int(degree) + 3)
+    Ph = torch.tensor(nodal_basis(degree, X, Y)[0], dtype=torch.float64, device=p.device)
+    Xt = torch.tensor(X, dtype=torch.float64, device=p.device)
+    Yt = torch.tensor(Y, dtype=torch.float64, device=p.device)
+    q = p[:, None, 0] + Xt[None, :, None] * d1[:, None] + Yt[None, :, None] * d2[:, None]
+    u = torch.as_tensor(u, dtype=torch.float64, device=p.device).reshape(mesh.n_cells, -1)
+    err = u @ Ph.T - solution(q[..., 0], q[..., 1])
+    return float(torch.sqrt(((err ** 2) @ torch.tensor(W, dtype=torch.float64, device=p.device) * det).sum()))

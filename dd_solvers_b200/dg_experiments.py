@@ -5,12 +5,14 @@ run: permute the system so that DOFs are grouped by (coarse cell, solver
 cell), set up the solver with ``dofs_per_solver`` / ``solvers_per_coarse``,
 time ``solve`` with CUDA events, min over repetitions, setup excluded) for the
 configurations of ``experiments/precision_experiments.py`` and
-``experiments/parallelism_experiments.py``: 2D P1, continuous-coefficient test
-case, fine mesh ``S<m>``, solver and coarse cells on ``S<k>`` triangles or
-``C<k>`` quadrilaterals, ``CG(maxiter=2000, rtol=1e-9)``.
+``experiments/parallelism_experiments.py``: 2D, polynomial degree ``p`` = 1, 3
+or 5 (``--degree``), continuous-coefficient test case, fine mesh ``S<m>``,
+solver and coarse cells on ``S<k>`` triangles or ``C<k>`` quadrilaterals,
+``CG(maxiter=2000, rtol=1e-9)``.
 
     python -m dd_solvers_b200.dg_experiments --fine S10 --solvers S8 --coarse S8 \\
         --method hybrid --precision f16
+    python -m dd_solvers_b200.dg_experiments --degree 3 --fine S9 --solvers S8 --coarse S8
 
 prints one JSON line per run: iterations, the min / median solve time over the
 repetitions, and (when ``--log`` names the reference's logged results, e.g.
@@ -58,47 +60,52 @@ def solvers_to_coarse(solvers: str, coarse: str, device) -> torch.Tensor:
     return _quad_of(cx, cy, int(coarse[1:]))
 
 
-def build(fine: str, solvers: str, coarse: str, device="cuda", return_perm: bool = False):
-    """Assemble ``S<fine>`` and group its DOFs by (coarse, solver) as the
-    reference does (``experiments.py:205-236``). Returns the permuted system
-    and the setup keyword arguments (and, with ``return_perm``, the permutation:
-    ``b_permuted = b[perm]``, so a solution maps back as ``x[inv(perm)]``)."""
+def build(fine: str, solvers: str, coarse: str, device="cuda", return_perm: bool = False, degree: int = 1):
+    """Assemble ``S<fine>`` in the degree-p DG space and group its DOFs by
+    (coarse, solver) as the reference does (``experiments.py:205-236``).
+    Returns the permuted system and the setup keyword arguments (and, with
+    ``return_perm``, the permutation: ``b_permuted = b[perm]``, so a solution
+    maps back as ``x[inv(perm)]``)."""
     mesh = dg.uniform_mesh_2d(int(fine[1:]), device)
-    system = dg.sipg_p1(mesh)
+    system = dg.sipg(mesh, degree=degree)
+    nb = system.block_size
     f2s = dg.cell_mapping(mesh, solvers)
     s2c = solvers_to_coarse(solvers, coarse, device)
     n_cells = mesh.n_cells
-    f2d = torch.arange(3 * n_cells, device=device).view(n_cells, 3)
+    f2d = torch.arange(nb * n_cells, device=device).view(n_cells, nb)
     perm = asm_permutation(f2s, s2c, f2d)
     inv = torch.empty_like(perm)
     inv[perm] = torch.arange(perm.numel(), device=device)
+    load = system.load
     A = permute_csr_tensor(system.matrix, inv)
-    b = system.load[perm]
+    del system
+    b = load[perm]
     n_coarse = int(s2c.max()) + 1
-    kwargs = dict(dofs_per_solver=int((f2s == 0).sum()) * 3,
+    kwargs = dict(dofs_per_solver=int((f2s == 0).sum()) * nb,
                   solvers_per_coarse=torch.bincount(s2c, minlength=n_coarse),
-                  block_size=3)
+                  block_size=nb)
     if return_perm:
         return A, b, kwargs, perm
     return A, b, kwargs
 
 
-def reference_row(log, fine, solvers, coarse, method, pc_prec, block_prec):
+def reference_row(log, fine, solvers, coarse, method, pc_prec, block_prec, degree=1):
     if not log:
         return None
     name = "AdditiveSchwarz" if method == "additive" else "HybridSchwarz"
     inv = "Inv()" if block_prec == pc_prec else f"Inv({REF_NAME[block_prec]})"
     head = f"CG({name}({REF_NAME[pc_prec]}, {inv}, CUDSS"
     for r in log:
-        if (r["fine"], r["solvers"], r["coarse"]) == (fine, solvers, coarse) and r["solver"].startswith(head):
+        if ((r["fine"], r["solvers"], r["coarse"]) == (fine, solvers, coarse) and r.get("p", 1) == degree
+                and r["solver"].startswith(head)):
             return r
     return None
 
 
 def run(fine, solvers, coarse, method, precision, pc_precision="f64", reps=10, log=None, flexible=False,
-        device="cuda") -> dict:
+        device="cuda", degree=1) -> dict:
     t0 = time.perf_counter()
-    A, b, kw = build(fine, solvers, coarse, device)
+    A, b, kw = build(fine, solvers, coarse, device, degree=degree)
     torch.cuda.synchronize()
     t_build = time.perf_counter() - t0
     pc_dt, blk_dt = DT[pc_precision], DT[precision]
@@ -119,14 +126,14 @@ def run(fine, solvers, coarse, method, precision, pc_precision="f64", reps=10, l
         e1.record()
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
-    out = {"fine": fine, "solvers": solvers, "coarse": coarse, "method": method,
+    out = {"p": degree, "fine": fine, "solvers": solvers, "coarse": coarse, "method": method,
            "preconditioner_precision": pc_precision, "block_precision": precision,
            "flexible": bool(flexible), "dofs": int(A.shape[0]), "nnz": int(A.values().numel()),
            "dofs_per_solver": kw["dofs_per_solver"], "n_coarse": int(kw["solvers_per_coarse"].numel()),
            "iterations": meta["iterations"], "solve_ms_min": min(times),
            "solve_ms_median": float(np.median(times)), "setup_s": t_setup, "assembly_s": t_build,
            "residual_norms": meta["residual norms"]}
-    ref = reference_row(log, fine, solvers, coarse, method, pc_dt, blk_dt)
+    ref = reference_row(log, fine, solvers, coarse, method, pc_dt, blk_dt, degree)
     if ref is not None:
         out["reference_iterations"] = ref["iterations"]
         out["reference_a100_solve_ms_min"] = ref["solve_ms_min"]
@@ -143,6 +150,7 @@ def run(fine, solvers, coarse, method, precision, pc_precision="f64", reps=10, l
 
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--degree", type=int, default=1, help="polynomial degree p of the DG space")
     ap.add_argument("--fine", default="S10")
     ap.add_argument("--solvers", default="S8")
     ap.add_argument("--coarse", default="S8")
@@ -156,7 +164,7 @@ def main():
     args = ap.parse_args()
     log = json.load(open(args.log)) if args.log else None
     out = run(args.fine, args.solvers, args.coarse, args.method, args.precision, args.pc_precision,
-              args.reps, log, args.flexible)
+              args.reps, log, args.flexible, degree=args.degree)
     if not args.history:
         out.pop("residual_norms")
     print(json.dumps(out))

@@ -9,9 +9,10 @@ residual history, in ``results/experiment_precisions.csv`` and
 ``experiments/precision_experiments.py`` and
 ``experiments/parallelism_experiments.py`` through
 ``src/experiments/experiments/experiments.py:175-300``, on an A100). This
-script keeps, for the 2D P1 rows (continuous coefficient test case, uniform
-mesh family):
+script keeps, for the 2D rows (continuous coefficient test case, uniform mesh
+family, polynomial degrees 1, 3 and 5):
 
+* ``p``                              - polynomial degree of the DG space,
 * ``fine``, ``solvers``, ``coarse``  - mesh ids (``S<m>`` / ``C<m>``),
 * ``solver``                         - the reference's ``str(solver)``,
 * ``dofs``, ``nnz``                  - system size and matrix nnz,
@@ -39,7 +40,7 @@ def rows(name, keep_norms):
     out = []
     with open(os.path.join(REF, "results", name)) as fh:
         for r in csv.DictReader(fh):
-            if not r["solver"].startswith("CG(") or r["p"] != "1":
+            if not r["solver"].startswith("CG(") or r["p"] not in ("1", "3", "5"):
                 continue
             md = r["metadata"]
             it = norms = None
@@ -52,6 +53,7 @@ def rows(name, keep_norms):
             out.append({
                 "source": name,
                 "test_case": r["test case"],
+                "p": int(r["p"]),
                 "fine": r["fine m"], "solvers": r["solvers m"], "coarse": r["coarse m"],
                 "solver": r["solver"],
                 "dofs": int(r["DoFs"]), "nnz": int(r["matrix nnz"]),

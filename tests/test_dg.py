@@ -156,3 +156,106 @@ def test_sipg_converges_at_second_order(case):
     assert errs[0] < 0.5  # the reference's bound at S3 (tests/test_experiments.py:37-41)
     ratio = errs[-2] / errs[-1]
     assert 3.7 < ratio < 4.3, errs
+
+
+# ---------------------------------------------------------------------------
+# degrees p = 2..5 (the reference's P3 and P5 experiments)
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("m", [1, 3])
+@pytest.mark.parametrize("case", [dg.CONTINUOUS_COEFFICIENT_2D, dg.CONSTANT_COEFFICIENT_2D], ids=["continuous", "constant"])
+def test_quadrature_assembly_matches_p1_closed_form(m, case):
+    """The degree-p assembly (nodal basis, exact quadrature) at p = 1 against
+    the closed form that the S10 logs pin: same pattern, entries to rounding."""
+    mesh = dg.uniform_mesh_2d(m)
+    a, b = dg.sipg_p1(mesh, case), dg._sipg_quadrature(mesh, case, 1)
+    assert torch.equal(a.matrix.crow_indices(), b.matrix.crow_indices())
+    assert torch.equal(a.matrix.col_indices(), b.matrix.col_indices())
+    va, vb = a.matrix.values(), b.matrix.values()
+    assert float((va - vb).abs().max()) <= 1e-13 * float(va.abs().max())
+    assert float((a.load - b.load).abs().max()) <= 1e-13 * float(a.load.abs().max())
+
+
+def test_reference_nodes_layout():
+    """Vertices first, then each edge's interior points at the GLL points
+    (edge 0 from vertex 1 to 2, edge 1 from 0 to 2, edge 2 from 0 to 1), then
+    the interior; equispaced for p <= 2, the P3 interior point at the
+    centroid, and every node set invariant under the triangle's rotation."""
+    for p in range(1, 6):
+        P = dg.reference_nodes(p)
+        nb = (p + 1) * (p + 2) // 2
+        assert P.shape == (nb, 2)
+        np.testing.assert_array_equal(P[:3], [[0, 0], [1, 0], [0, 1]])
+        g = dg._gll_points(p)[1:-1]
+        k = p - 1
+        np.testing.assert_allclose(P[3:3 + k], np.stack([1 - g, g], 1), atol=1e-15)
+        np.testing.assert_allclose(P[3 + k:3 + 2 * k], np.stack([0 * g, g], 1), atol=1e-15)
+        np.testing.assert_allclose(P[3 + 2 * k:3 + 3 * k], np.stack([g, 0 * g], 1), atol=1e-15)
+        # rotation (x, y) -> (y, 1 - x - y) maps the node set onto itself
+        Q = np.stack([P[:, 1], 1 - P[:, 0] - P[:, 1]], 1)
+        d = np.abs(Q[:, None, :] - P[None, :, :]).sum(-1).min(1)
+        assert d.max() < 1e-14
+    np.testing.assert_allclose(dg.reference_nodes(2), [[0, 0], [1, 0], [0, 1], [.5, .5], [0, .5], [.5, 0]])
+    np.testing.assert_allclose(dg.reference_nodes(3)[-1], [1 / 3, 1 / 3], atol=1e-15)
+    # the nodal basis is the identity on the nodes
+    P = dg.reference_nodes(5)
+    v, _, _ = dg.nodal_basis(5, P[:, 0], P[:, 1])
+    np.testing.assert_allclose(v, np.eye(21), atol=1e-12)
+
+
+@pytest.mark.parametrize("p", [2, 3, 4, 5])
+def test_higher_degree_matrix_symmetric_positive_definite(p):
+    A = dg.sipg(dg.uniform_mesh_2d(2), degree=p).matrix.to_dense().numpy()
+    assert A.shape[0] == 32 * (p + 1) * (p + 2) // 2
+    assert np.abs(A - A.T).max() < 1e-13 * np.abs(A).max()
+    assert np.linalg.eigvalsh(A).min() > 0
+
+
+@pytest.mark.parametrize("p,fine", [(3, "S9"), (5, "S8")])
+def test_higher_degree_size_and_load_norm_match_reference_log(p, fine):
+    """The reference's P3 (S9) and P5 (S8) systems: DOFs and nnz from the
+    block structure, and the load-vector norm (its first additive-Schwarz
+    residual norm, x0 = 0), which depends on where the nodes sit: GLL-warped
+    nodes match to rounding, equispaced interior nodes would be 17% off at P5."""
+    row = next(r for r in golden_rows() if r.get("p") == p and r["fine"] == fine
+               and r["solver"].startswith("CG(AdditiveSchwarz(torch.float64, Inv(), CUDSS"))
+    mesh = dg.uniform_mesh_2d(int(fine[1:]))
+    nb = (p + 1) * (p + 2) // 2
+    (c1, _, _, _), _ = dg._edge_tables(mesh)
+    assert mesh.n_cells * nb == row["dofs"]
+    assert (mesh.n_cells + 2 * c1.numel()) * nb * nb == row["nnz"]
+    b = float(torch.linalg.norm(dg.load_vector(mesh, degree=p)))
+    assert math.isclose(b, row["residual_norms"][0], rel_tol=1e-12)
+
+
+@pytest.mark.parametrize("p,ratio", [(2, 8.0), (3, 16.0)])
+def test_higher_degree_converges_at_order_p_plus_one(p, ratio):
+    """Direct solves on S4..S6 (continuous coefficient): the L2 error falls by
+    ~2^(p+1) per refinement."""
+    import scipy.sparse.linalg as spla
+
+    case = dg.CONTINUOUS_COEFFICIENT_2D
+    errs = []
+    for m in range(4, 7):
+        mesh = dg.uniform_mesh_2d(m)
+        s = dg.sipg(mesh, case, p)
+        u = spla.spsolve(scipy_csr(s.matrix).tocsc(), s.load.numpy())
+        errs.append(dg.l2_error_p(mesh, u, case.solution, p))
+    r = errs[-2] / errs[-1]
+    assert 0.93 * ratio < r < 1.07 * ratio, errs
+
+
+def test_experiment_grouping_higher_degree():
+    """DOFs grouped by (coarse, solver) cells for p = 3: every solver holds
+    its cells' 10 DOFs each, in contiguous runs."""
+    from dd_solvers_b200 import dg_experiments
+
+    A, b, kw, perm = dg_experiments.build("S4", "S3", "S2", device="cpu", return_perm=True, degree=3)
+    assert A.shape == (512 * 10, 512 * 10) and b.shape == (5120,)
+    assert kw["block_size"] == 10 and kw["dofs_per_solver"] == 40
+    assert int(kw["solvers_per_coarse"].sum()) == 128
+    assert torch.equal(torch.sort(perm).values, torch.arange(5120))
+    cell = perm // 10
+    f2s = dg.cell_mapping(dg.uniform_mesh_2d(4), "S3")
+    sol = f2s[cell].view(-1, 40)
+    assert bool((sol == sol[:, :1]).all())

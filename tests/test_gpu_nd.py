@@ -115,6 +115,33 @@ def test_dg_experiment_mixed_precision_iterations(precision, expected):
     assert out["history_max_rel_diff_first10"] < 1e-5
 
 
+@pytest.mark.parametrize("p,fine,cells,method", [(3, "S9", "S8", "hybrid"), (3, "S9", "S8", "additive"),
+                                                  (5, "S8", "S7", "hybrid"), (5, "S8", "S7", "additive")])
+def test_dg_higher_degree_experiment_reproduces_reference_log(p, fine, cells, method):
+    """The reference's P3 (S9, 5.24M DOFs, 10 per cell) and P5 (S8, 2.75M
+    DOFs, 21 per cell) experiments, FP64: its logged size, iteration count and
+    residual history (GLL-warped nodes, exact quadrature)."""
+    log = json.load(open(LOG))
+    out = dg_experiments.run(fine, cells, cells, method, "f64", reps=1, log=log, degree=p)
+    size = {3: (5242880, 209510400), 5: (2752512, 230759424)}[p]
+    assert (out["dofs"], out["nnz"]) == size
+    assert abs(out["iterations"] - out["reference_iterations"]) <= 1
+    assert out["history_max_rel_diff_first10"] < 1e-10
+    # later norms drift only by rounding (the reference ran BSR products on an A100)
+    assert out["history_max_rel_diff"] < 1e-2
+
+
+@pytest.mark.parametrize("p,fine,precision,expected", [(3, "S9", "f16", 131), (5, "S8", "bf16", 152)])
+def test_dg_higher_degree_mixed_precision_iterations(p, fine, precision, expected):
+    """Low-precision blocks on the P3 / P5 problems with S8 subdomains and
+    coarse cells: the reference's logged iteration counts."""
+    log = json.load(open(LOG))
+    out = dg_experiments.run(fine, "S8", "S8", "hybrid", precision, reps=1, log=log, degree=p)
+    assert out["reference_iterations"] == expected
+    assert abs(out["iterations"] - expected) <= 1
+    assert out["history_max_rel_diff_first10"] < 1e-6
+
+
 def test_dg_experiment_quadrilateral_cells():
     """Solver and coarse cells on the C-level quadrilateral grids (the DOFs are
     permuted into (coarse, solver) groups first): S9 fine, C8 solvers (24 DOFs
