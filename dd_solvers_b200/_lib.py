@@ -53,6 +53,7 @@ _SIGS = {
     "ddx_spmv_csr_rowblock_mapped": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P, _I, _P, _P]),
     "ddx_spmv_csr_rowblock_f64": (_I, [_I64, _I, _P, _P, _P, _P, _P, _P]),
     "ddx_spmv_bsr": (_I, [_I64, _I, _P, _P, _P, _P, _P, _I, _P]),
+    "ddx_spmv_epilogue_f64": (_I, [_I64, _P, _P, _P, _I, _P, _P, _P, _P, _P, _P]),
     "ddx_gemv_strided_batched": (_I, [_I64, _I, _P, _I, _P, _P, _I, _P]),
     "ddx_schwarz_local_apply": (_I, [_I, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _P]),
     "ddx_schwarz_local_apply_ex": (_I, [_I, _I, _P, _P, _P, _P, _P, _I, _P, _I, _P, _P, _I, _P, _I, _I, _P]),

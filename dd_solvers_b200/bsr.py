@@ -5,8 +5,8 @@ The reference registers several numba kernels; here every backend name maps to
 the sm_100a ``ddx_spmv_bsr`` kernel: one scalar row per lane, floor(32 / bs)
 block rows per warp, so the bs lanes of a block row read each column of the
 column-major blocks as consecutive values and x is a broadcast; no cross-lane
-reduction. For bs <= 8 the warp first copies its block rows' values (one
-contiguous span) into shared memory with coalesced loads.
+reduction. ``CG(bsr_matmul=True)`` with a block size >= 2 runs its products
+through the same kernel.
 """
 from __future__ import annotations
 

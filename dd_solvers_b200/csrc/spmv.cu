@@ -90,6 +90,50 @@ __global__ void __launch_bounds__(kThreads, 4)
   }
 }
 
+// The PCG epilogue of a product that another kernel computed (the BSR product
+// for DG block matrices): y = A v is already in y. PQ: p.q -> alpha (x is p);
+// RES_*: y = b - y and its norms. Same partials, ticket and finalize as the
+// fused SELL kernel; grid-stride over rows with at most kRedCtas CTAs.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads)
+    k_spmv_epilogue(int64_t n, const double* __restrict__ x, double* __restrict__ y,
+                    const double* __restrict__ b, PcgState S, double* partials, unsigned int* ticket) {
+  __shared__ double red[kThreads];
+  if (n_active(S.ist, 1) == 0) return;
+  double acc[2] = {0.0, 0.0};
+  for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < n;
+       row += (int64_t)gridDim.x * blockDim.x) {
+    const double q = y[row];
+    if (MODE == DDX_SPMV_PQ) {
+      acc[0] = fma(x[row], q, acc[0]);
+    } else {
+      const double bi = b[row];
+      const double ri = bi - q;
+      y[row] = ri;
+      if (MODE == DDX_SPMV_RES_INIT) acc[1] = fma(bi, bi, acc[1]);
+      acc[0] = fma(ri, ri, acc[0]);
+    }
+  }
+  constexpr int NV = (MODE == DDX_SPMV_RES_INIT) ? 2 : 1;
+  double part[NV];
+  part[0] = acc[0];
+  if (NV == 2) part[NV - 1] = acc[1];
+  write_cta_partials<NV>(part, red, 1, partials);
+  if (!last_cta_arrival(ticket)) return;
+  double tot[NV];
+  final_sums<NV>(partials, 1, red, tot, ticket);
+  if (park_totals<NV>(S, tot)) return;
+  int act = 0;
+  if (threadIdx.x == 0) {
+    if (MODE == DDX_SPMV_PQ) act = fin_pq(S, 0, tot[0]);
+    if (MODE == DDX_SPMV_RES_INIT) act = fin_init(S, 0, tot[NV - 1], tot[0]);
+    if (MODE == DDX_SPMV_RES_REPLACE) act = fin_replace(S, 0, tot[0]);
+    if (MODE >= DDX_SPMV_RES_INIT) S.s(DDX_ST_RR_PACK, 0) = S.s(DDX_ST_RR, 0);
+  }
+  if (MODE != DDX_SPMV_PQ) publish_nactive(S, act);
+  else publish_nactive(S, threadIdx.x == 0 ? act : 0);
+}
+
 // CSR, R threads per row (R in {1..64}, power of two), (n, R) vector layout.
 template <int MODE>
 __global__ void __launch_bounds__(kThreads)
@@ -747,6 +791,32 @@ int ddx_spmv_csr_lanes(int64_t n_rows, int lanes, const int* row_ptr, const int*
 int ddx_spmv_csr_lanes_f64(int64_t n_rows, int lanes, const int* row_ptr, const int* cols, const double* vals,
                            const double* x, double* y, ddx_stream_t stream) {
   return ddx_spmv_csr_lanes(n_rows, lanes, row_ptr, cols, vals, x, DDX_F64, y, stream);
+}
+
+int ddx_spmv_epilogue_f64(int64_t n, const double* x, double* y, const double* b, int mode, double* st, int* ist,
+                          double* hist, double* partials, unsigned int* tickets, ddx_stream_t stream) {
+  DDX_REQUIRE(n >= 0 && y, "ddx_spmv_epilogue_f64: bad arguments");
+  DDX_REQUIRE(mode >= DDX_SPMV_PQ && mode <= DDX_SPMV_RES_REPLACE, "ddx_spmv_epilogue_f64: bad mode %d", mode);
+  DDX_REQUIRE(st && ist && hist && partials && tickets, "ddx_spmv_epilogue_f64: PCG mode needs state");
+  if (mode == DDX_SPMV_PQ) DDX_REQUIRE(x, "ddx_spmv_epilogue_f64: p.q needs p");
+  else DDX_REQUIRE(b, "ddx_spmv_epilogue_f64: residual mode needs b");
+  if (n == 0) return DDX_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  PcgState S{st, ist, hist, 1};
+  const int grid = (int)std::min<int64_t>(ceil_div(n, kThreads), kRedCtas);
+  unsigned int* t = tickets + 2;
+  switch (mode) {
+    case DDX_SPMV_PQ:
+      k_spmv_epilogue<DDX_SPMV_PQ><<<grid, kThreads, 0, s>>>(n, x, y, b, S, partials, t);
+      break;
+    case DDX_SPMV_RES_INIT:
+      k_spmv_epilogue<DDX_SPMV_RES_INIT><<<grid, kThreads, 0, s>>>(n, x, y, b, S, partials, t);
+      break;
+    default:
+      k_spmv_epilogue<DDX_SPMV_RES_REPLACE><<<grid, kThreads, 0, s>>>(n, x, y, b, S, partials, t);
+  }
+  DDX_LAUNCH_CHECK("ddx_spmv_epilogue_f64");
+  return DDX_OK;
 }
 
 int ddx_spmv_bsr(int64_t n_block_rows, int bs, const int* row_ptr, const int* cols, const void* vals,

@@ -1144,8 +1144,41 @@ class _PcgWork:
         self.recompute_z = False
 
 
+def _dense_blocks(crow: torch.Tensor, col: torch.Tensor, val: torch.Tensor, bs: int):
+    """BSR arrays ``(block_row_ptr, block_cols, vals)`` (int32, int32, blocks
+    column-major) of a scalar CSR matrix with sorted columns whose nonzeros
+    form dense ``bs x bs`` blocks (the DG matrices: every cell couples all of
+    its DOFs with all of its neighbours'), as ``csr_to_bsr``
+    (src/dd_solvers/cpp/cusparse.cpp:22-107) gives for them; None when the
+    pattern is not block-dense."""
+    n = crow.numel() - 1
+    if bs < 2 or n % bs:
+        return None
+    nbr = n // bs
+    dev = crow.device
+    crow = crow.to(torch.int64)
+    cnt = (crow[1:] - crow[:-1]).view(nbr, bs)
+    if not bool((cnt == cnt[:, :1]).all()) or bool((cnt[:, 0] % bs != 0).any()):
+        return None
+    per = cnt[:, 0] // bs
+    bptr = torch.zeros(nbr + 1, dtype=torch.int64, device=dev)
+    bptr[1:] = torch.cumsum(per, 0)
+    n_blocks = int(bptr[-1])
+    brow = torch.repeat_interleave(torch.arange(nbr, device=dev), per)
+    k = torch.arange(n_blocks, device=dev) - bptr[brow]
+    starts = crow[:-1].view(nbr, bs)[brow] + (k * bs)[:, None]  # (blocks, bs rows)
+    ar = torch.arange(bs, device=dev)
+    full = starts[:, :, None] + ar[None, None, :]  # (blocks, i, j)
+    bcol = col[starts[:, 0]].to(torch.int64) // bs
+    if not bool((col[full].to(torch.int64) == (bcol * bs)[:, None, None] + ar[None, None, :]).all()):
+        return None
+    vals = val[full].transpose(1, 2).contiguous()
+    return bptr.to(torch.int32), bcol.to(torch.int32), vals
+
+
 class _SellMatrix:
-    """The system matrix in SELL-32 (bsr_matmul=True) or CSR (R > 1) form."""
+    """The system matrix in SELL-32 (bsr_matmul=True), BSR (bsr_matmul=True
+    with a block size >= 2 on a block-dense pattern) or CSR (R > 1) form."""
 
     def __init__(self, matrix: torch.Tensor):
         crow = matrix.crow_indices()
@@ -1164,6 +1197,17 @@ class _SellMatrix:
         # 27-point stencil, 0.497 vs 0.404 ms on C5's P1 mesh)
         self.spmm_cluster = 0
         self._orders = {}
+        self.bsr = None  # (block_row_ptr, block_cols, column-major blocks, bs) for R = 1
+
+    def use_bsr(self, bs: int) -> bool:
+        """Multiply (R = 1) in BSR form with ``bs x bs`` blocks, as the
+        reference's ``CG(bsr_matmul=True)`` does (solvers.py:216-224): 8 bytes
+        per stored entry instead of SELL's 12, which pays on DG block rows. The
+        PCG epilogue then runs as a separate pass. Returns False (and keeps
+        SELL) when the pattern is not block-dense."""
+        got = _dense_blocks(self.crow32, self.col32, self.val, int(bs))
+        self.bsr = None if got is None else (*got, int(bs))
+        return self.bsr is not None
 
     def row_order(self, chunk: int) -> torch.Tensor:
         """The SpMM work order for ``chunk``-row clusters (``ddx_row_clusters``)."""
@@ -1190,12 +1234,21 @@ class _SellMatrix:
         v = vals.to(self.val.device, torch.float64)
         self.val.copy_(v)
         self.sell[3][self._sell_pos] = v
+        if self.bsr is not None:
+            self.use_bsr(self.bsr[3])
 
     def launch(self, x, y, R, mode, w: _PcgWork | None = None, b=None, use_sell=True):
         st = ist = hist = partials = tickets = None
         if w is not None:
             st, ist, hist, partials, tickets = w.st, w.ist, w.hist, w.partials, w.tickets
-        if R == 1 and use_sell:
+        if R == 1 and use_sell and self.bsr is not None:
+            bp, bc, bv, bs = self.bsr
+            L.call("ddx_spmv_bsr", bp.numel() - 1, bs, L.ptr(bp), L.ptr(bc), L.ptr(bv), L.ptr(x), L.ptr(y), L.F64,
+                   L.stream_ptr())
+            if mode != L.SPMV_PLAIN:
+                L.call("ddx_spmv_epilogue_f64", self.n, L.ptr(x), L.ptr(y), L.ptr(b), mode, L.ptr(st), L.ptr(ist),
+                       L.ptr(hist), L.ptr(partials), L.ptr(tickets), L.stream_ptr())
+        elif R == 1 and use_sell:
             sp, sw, sc, sv = self.sell
             L.call("ddx_spmv_sell_f64", self.n, sw.numel(), L.ptr(sp), L.ptr(sw), L.ptr(sc), L.ptr(sv), L.ptr(x),
                    L.ptr(y), L.ptr(b), mode, L.ptr(st), L.ptr(ist), L.ptr(hist), L.ptr(partials), L.ptr(tickets),
@@ -1264,6 +1317,8 @@ class CG(SparseSolver):
             raise ValueError("Unable to determine block size for BSR matrix multiplication.")
         self.block_size = kwargs.get("block_size", 1)
         self.matrix = _SellMatrix(matrix)
+        if self.bsr_matmul and self.block_size >= 2:
+            self.matrix.use_bsr(self.block_size)
         self.n = matrix.shape[0]
         self._work = {}
         return timings

@@ -246,6 +246,14 @@ int ddx_spmv_csr_lanes(int64_t n_rows, int lanes, const int* row_ptr, const int*
  * one lane per scalar row, floor(32 / bs) block rows per warp. */
 int ddx_spmv_bsr(int64_t n_block_rows, int bs, const int* row_ptr, const int* cols, const void* vals,
                  const void* x, void* y, int dtype, ddx_stream_t stream);
+/* PCG epilogue of a product computed by ddx_spmv_bsr (R = 1, F64), for the
+ * CG(bsr_matmul=True) path on DG block matrices (src/dd_solvers/dd_solvers/
+ * solvers.py:243-268 with the FastBSR product of bsr.py:24-25): y already holds
+ * A v. mode 1: x = p, y = q, p.q -> alpha; mode 2/3: y = b - y, then the norms
+ * and the stop test of ddx_spmv_sell_f64's modes 2/3. Same state, partials and
+ * ticket as ddx_spmv_sell_f64. */
+int ddx_spmv_epilogue_f64(int64_t n, const double* x, double* y, const double* b, int mode, double* st, int* ist,
+                          double* hist, double* partials, unsigned int* tickets, ddx_stream_t stream);
 /* ---- Batched GEMV (reference op) ----------------------------------------
  * Replaces dd_solvers_gemv::gemv_strided_batched
  * (src/dd_solvers/cpp/gemv.cpp:9-53, kernels gemv_kernels.cu:31-139):

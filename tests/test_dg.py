@@ -259,3 +259,25 @@ def test_experiment_grouping_higher_degree():
     f2s = dg.cell_mapping(dg.uniform_mesh_2d(4), "S3")
     sol = f2s[cell].view(-1, 40)
     assert bool((sol == sol[:, :1]).all())
+
+
+@pytest.mark.parametrize("p", [1, 3])
+def test_dense_blocks_match_torch_bsr(p):
+    """The BSR form that ``CG(bsr_matmul=True)`` multiplies with: the DG
+    matrix's dense cell blocks, column-major, as torch's own conversion gives
+    them; a pattern that is not block-dense is refused."""
+    from dd_solvers_b200.solvers import _dense_blocks
+
+    s = dg.sipg(dg.uniform_mesh_2d(2), degree=p)
+    A, bs = s.matrix, s.block_size
+    got = _dense_blocks(A.crow_indices(), A.col_indices(), A.values(), bs)
+    assert got is not None
+    bptr, bcol, vals = got
+    ref = A.to_sparse_bsr((bs, bs))
+    assert torch.equal(bptr.to(torch.int64), ref.crow_indices())
+    assert torch.equal(bcol.to(torch.int64), ref.col_indices())
+    assert torch.equal(vals, ref.values().transpose(1, 2).contiguous())
+    # 5-point Laplacian rows are not 2x2-block-dense
+    L = sps.diags([-1, -1, 4, -1, -1], [-8, -1, 0, 1, 8], shape=(64, 64), format="csr")
+    crow = torch.as_tensor(L.indptr, dtype=torch.int64)
+    assert _dense_blocks(crow, torch.as_tensor(L.indices), torch.as_tensor(L.data), 2) is None

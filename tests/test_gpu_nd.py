@@ -142,6 +142,42 @@ def test_dg_higher_degree_mixed_precision_iterations(p, fine, precision, expecte
     assert out["history_max_rel_diff_first10"] < 1e-6
 
 
+@pytest.mark.parametrize("p,fine", [(1, "S6"), (3, "S5"), (5, "S4")])
+def test_cg_bsr_products_match_csr(p, fine):
+    """``CG(bsr_matmul=True)`` on a DG matrix multiplies in BSR form (the cell
+    blocks, ``ddx_spmv_bsr``) with the PCG epilogue as a separate pass; the
+    same solve with ``bsr_matmul=False`` (CSR products with fused epilogues)
+    takes the same iterations and reaches the same solution. Residual
+    replacement exercises the r = b - A x epilogue."""
+    import dd_solvers_b200 as dd
+
+    A, b, kw = dg_experiments.build(fine, "S3", "S3", degree=p)
+    nb = (p + 1) * (p + 2) // 2
+    runs = {}
+    for name, opts in {"bsr": {}, "csr": {"bsr_matmul": False}, "bsr_replace": {"replace_every": 7}}.items():
+        cg = dd.CG(dd.HybridSchwarz(torch.float64, dd.Inv(), dd.CUDSS()), rtol=1e-10, **opts)
+        cg.setup(A, **kw)
+        assert (cg.matrix.bsr is not None) == (name != "csr")
+        x, meta = cg.solve(b)
+        runs[name] = (x, meta)
+        if name == "bsr":
+            v = torch.randn(A.shape[0], dtype=torch.float64, device="cuda")
+            ref = (A @ v[:, None])[:, 0]
+            got = cg.matrix @ v
+            assert float((got - ref).abs().max()) <= 1e-12 * float(ref.abs().max())
+            assert cg.matrix.bsr[3] == nb
+        cg.destroy()
+    xb, mb = runs["bsr"]
+    xc, mc = runs["csr"]
+    assert mb["iterations"] == mc["iterations"]
+    assert float(torch.linalg.norm(xb - xc)) <= 1e-9 * float(torch.linalg.norm(xc))
+    hb, hc = np.array(mb["residual norms"][:10]), np.array(mc["residual norms"][:10])
+    np.testing.assert_allclose(hb, hc, rtol=1e-11)
+    xr, mr = runs["bsr_replace"]
+    assert abs(mr["iterations"] - mc["iterations"]) <= 1
+    assert float(torch.linalg.norm(xr - xc)) <= 1e-8 * float(torch.linalg.norm(xc))
+
+
 def test_dg_experiment_quadrilateral_cells():
     """Solver and coarse cells on the C-level quadrilateral grids (the DOFs are
     permuted into (coarse, solver) groups first): S9 fine, C8 solvers (24 DOFs
