@@ -24,7 +24,8 @@ divided by their number.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2]
 
 At N = 1 the c2 line also carries "reference_experiment": the reference's own DG-SIPG experiment S10 / S8 /
-S8 (hybrid, FP16 blocks) solved through this package, next to the reference's logged A100 time for it;
+S8 (hybrid, FP16 blocks) solved through this package, next to the reference's logged A100 time for it (and
+the same experiment at P3 on S9 and P5 on S8 under "higher_degree");
 "multi_rhs": compact c3 and c5 results; "other_workloads": compact c1 and c4 results (short timing).
 
 --impl reference times the FP64 CPU restatement of the same algorithm on the
@@ -664,6 +665,14 @@ def run_ours(args, spec, rank: int, world: int):
 # "CG(HybridSchwarz(torch.float64, Inv(torch.float16), CUDSS), bsr_matmul=True)", min over 10 solves.
 REFERENCE_EXPERIMENT = {"fine": "S10", "solvers": "S8", "coarse": "S8", "method": "hybrid", "precision": "f16",
                         "reference_iterations": 61, "reference_a100_ms_per_solve": 183.0207977294922}
+# The same experiment at the higher degrees the reference logged (same file, same solver row): P3 on S9
+# (5,242,880 DOFs, 10 per cell) and P5 on S8 (2,752,512 DOFs, 21 per cell), S8 subdomains and coarse cells.
+REFERENCE_EXPERIMENTS_HIGHER_DEGREE = [
+    {"degree": 3, "fine": "S9", "solvers": "S8", "coarse": "S8", "method": "hybrid", "precision": "f16",
+     "reference_iterations": 131, "reference_a100_ms_per_solve": 457.8937683105469},
+    {"degree": 5, "fine": "S8", "solvers": "S8", "coarse": "S8", "method": "hybrid", "precision": "f16",
+     "reference_iterations": 151, "reference_a100_ms_per_solve": 451.76153564453125},
+]
 
 
 def reference_experiment() -> dict:
@@ -678,11 +687,26 @@ def reference_experiment() -> dict:
     e = REFERENCE_EXPERIMENT
     r = dg_experiments.run(e["fine"], e["solvers"], e["coarse"], e["method"], e["precision"], reps=5)
     torch.cuda.empty_cache()
+    higher = []
+    for h in REFERENCE_EXPERIMENTS_HIGHER_DEGREE:
+        try:
+            q = dg_experiments.run(h["fine"], h["solvers"], h["coarse"], h["method"], h["precision"], reps=5,
+                                   degree=h["degree"])
+        except Exception as exc:  # reported in the line; the headline metric does not depend on it
+            higher.append({"degree": h["degree"], "fine": h["fine"], "error": repr(exc)[:200]})
+            continue
+        finally:
+            torch.cuda.empty_cache()
+        higher.append({"degree": h["degree"], "fine": h["fine"], "dofs": q["dofs"], "iterations": q["iterations"],
+                       "reference_iterations": h["reference_iterations"], "ms_per_solve": q["solve_ms_min"],
+                       "reference_a100_ms_per_solve": h["reference_a100_ms_per_solve"],
+                       "speedup_vs_reference_a100": h["reference_a100_ms_per_solve"] / q["solve_ms_min"]})
     return {"experiment": "reference DG-SIPG P1, fine S10 (6,291,456 DOFs), 131,072 subdomains of 48 DOFs, "
                           "131,072 P0 coarse DOFs, HybridSchwarz(float64, Inv(float16), CUDSS), CG rtol 1e-9",
             "iterations": r["iterations"], "reference_iterations": e["reference_iterations"],
             "ms_per_solve": r["solve_ms_min"], "reference_a100_ms_per_solve": e["reference_a100_ms_per_solve"],
             "speedup_vs_reference_a100": e["reference_a100_ms_per_solve"] / r["solve_ms_min"],
+            "higher_degree": higher,
             "source": "results/experiment_precisions.csv (the reference's log)"}
 
 
