@@ -1,9 +1,9 @@
 """The DG-SIPG discretisation of the reference's experiments, pinned to its logs.
 
 ``tests/golden/dg_experiments.json`` holds the residual histories that the
-reference logged for its own CG runs on the 2D P1 uniform-mesh problems
-(``results/experiment_precisions.csv``); the oracle run on this package's
-assembly must reproduce them.
+reference logged for its own CG runs on the 2D uniform-mesh problems at P1, P3
+and P5 (``results/experiment_precisions.csv``); the oracle run on this
+package's assembly must reproduce them.
 """
 import json
 import math
@@ -281,3 +281,30 @@ def test_dense_blocks_match_torch_bsr(p):
     L = sps.diags([-1, -1, 4, -1, -1], [-8, -1, 0, 1, 8], shape=(64, 64), format="csr")
     crow = torch.as_tensor(L.indptr, dtype=torch.int64)
     assert _dense_blocks(crow, torch.as_tensor(L.indices), torch.as_tensor(L.data), 2) is None
+
+
+@pytest.fixture(scope="module")
+def p3_s9():
+    s = dg.sipg(dg.uniform_mesh_2d(9), degree=3)
+    A, b = scipy_csr(s.matrix), s.load.numpy()
+    del s
+    return A, b, rs.ContiguousSchwarz(A, 10 * 4, np.ones(2 * 4 ** 8, dtype=np.int64))
+
+
+@pytest.mark.parametrize("kind", ["additive", "hybrid"])
+def test_p3_oracle_residual_history_matches_reference_log(p3_s9, kind):
+    """The reference's P3 experiment on S9 (5,242,880 DOFs, 10 per cell), S8
+    subdomains of 40 DOFs and S8 P0 coarse cells, FP64: the oracle on this
+    package's higher-degree assembly reproduces the first ten logged residual
+    norms to 1e-10 (they depend on the GLL-warped nodes through the basis)."""
+    A, b, P = p3_s9
+    prefix = {"additive": "CG(AdditiveSchwarz(torch.float64, Inv(), CUDSS",
+              "hybrid": "CG(HybridSchwarz(torch.float64, Inv(), CUDSS"}[kind]
+    row = next(r for r in golden_rows() if r.get("p") == 3 and (r["fine"], r["solvers"], r["coarse"]) == ("S9", "S8", "S8")
+               and r["solver"].startswith(prefix))
+    M = P.additive if kind == "additive" else P.hybrid
+    T0 = P.T0 if kind == "hybrid" else None
+    _, meta = rs.pcg(A, b, M=M, T0=T0, rtol=1e-9, maxiter=10, raise_on_fail=False)
+    ours = np.array(meta["residual norms"])
+    assert len(ours) == 10
+    np.testing.assert_allclose(ours, np.array(row["residual_norms"][:10]), rtol=1e-10)
