@@ -48,7 +48,9 @@ from __future__ import annotations
 import dataclasses
 import math
 
+import numpy as np
 import torch
+from numpy.polynomial import legendre as leg
 
 # test cases of src/experiments/experiments/problems.py:31-74 (2D)
 
@@ -348,9 +350,6 @@ def _block_csr(n: int, bs: int, blocks_self, c1, c2, M) -> torch.Tensor:
 def _gll_points(n: int):
     """The n + 1 Gauss-Lobatto-Legendre points on [0, 1], ascending: the
     ends and the roots of P_n' (Newton-polished)."""
-    import numpy as np
-    from numpy.polynomial import legendre as leg
-
     if n == 1:
         return np.array([0.0, 1.0])
     c = np.zeros(n + 1)
@@ -366,8 +365,6 @@ def _warp(n: int, x):
     """1D warp: the displacement of the GLL points from the equispaced ones,
     interpolated at ``x`` by the degree-n Lagrange polynomial on the
     equispaced points."""
-    import numpy as np
-
     eq = np.arange(n + 1) / n
     disp = _gll_points(n) - eq
     out = np.zeros_like(x)
@@ -395,8 +392,6 @@ def reference_nodes(degree: int):
     ``r = (1 + lambda_v - lambda_u) / 2``. For p <= 2 this is the equispaced
     lattice. The choice is pinned by the load-vector norms that the reference
     logged for its P3 and P5 runs."""
-    import numpy as np
-
     n = int(degree)
     if n < 1:
         raise ValueError("degree must be >= 1")
@@ -421,9 +416,6 @@ def reference_nodes(degree: int):
 def _legendre_basis(n: int, x, y):
     """Values and x/y derivatives of L_a(2x-1) L_b(2y-1), a + b <= n: a
     well-conditioned basis of P_n for the nodal interpolation."""
-    import numpy as np
-    from numpy.polynomial import legendre as leg
-
     u, v = 2.0 * x - 1.0, 2.0 * y - 1.0
     vals, dx, dy = [], [], []
     for a in range(n + 1):
@@ -443,8 +435,6 @@ def _legendre_basis(n: int, x, y):
 def nodal_basis(degree: int, x, y):
     """Values and reference derivatives (each (..., n_b)) of the nodal basis
     of ``reference_nodes(degree)`` at the points (x, y)."""
-    import numpy as np
-
     P = reference_nodes(degree)
     V, _, _ = _legendre_basis(degree, P[:, 0], P[:, 1])
     Vi = np.linalg.inv(V)
@@ -455,9 +445,6 @@ def nodal_basis(degree: int, x, y):
 def _triangle_rule(q: int):
     """Collapsed Gauss-Legendre rule on the reference triangle (q^2 points,
     weights summing to 1/2): exact for polynomials of degree <= 2q - 2."""
-    import numpy as np
-    from numpy.polynomial import legendre as leg
-
     t, w = leg.leggauss(q)
     t, w = (t + 1.0) / 2.0, w / 2.0
     u, v = np.meshgrid(t, t, indexing="ij")
@@ -484,8 +471,6 @@ def sipg(mesh: TriangleMesh, case: TestCase = CONTINUOUS_COEFFICIENT_2D, degree:
 def _sipg_quadrature(mesh: TriangleMesh, case: TestCase, p_deg: int) -> DGSystem:
     """``sipg`` by quadrature, for any degree (p = 1 included, where it agrees
     with the closed form to rounding)."""
-    import numpy as np
-
     dev = mesh.cells.device
     f64 = dict(dtype=torch.float64, device=dev)
     n = mesh.n_cells
@@ -510,7 +495,7 @@ def _sipg_quadrature(mesh: TriangleMesh, case: TestCase, p_deg: int) -> DGSystem
     del R
 
     # edge traces: local edge o runs from vertex (o+1)%3 to (o+2)%3 (dir 0) or back (dir 1)
-    te, we = np.polynomial.legendre.leggauss(p_deg + 2)
+    te, we = leg.leggauss(p_deg + 2)
     te, we = (te + 1.0) / 2.0, torch.tensor(we / 2.0, **f64)
     V = np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]])
     tv, tdx, tdy = [], [], []
