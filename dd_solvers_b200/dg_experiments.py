@@ -13,6 +13,9 @@ solver and coarse cells on ``S<k>`` triangles or ``C<k>`` quadrilaterals,
     python -m dd_solvers_b200.dg_experiments --fine S10 --solvers S8 --coarse S8 \\
         --method hybrid --precision f16
     python -m dd_solvers_b200.dg_experiments --degree 3 --fine S9 --solvers S8 --coarse S8
+    python -m dd_solvers_b200.dg_experiments --all --log tests/golden/dg_experiments.json
+
+(``--all``: every converged configuration the reference logged, one JSON line each.)
 
 prints one JSON line per run: iterations, the min / median solve time over the
 repetitions, and (when ``--log`` names the reference's logged results, e.g.
@@ -102,6 +105,46 @@ def reference_row(log, fine, solvers, coarse, method, pc_prec, block_prec, degre
     return None
 
 
+_NAME_DT = {"torch.float64": "f64", "torch.float32": "f32", "torch.bfloat16": "bf16", "torch.float16": "f16"}
+
+
+def parse_solver(name: str) -> dict:
+    """(method, preconditioner precision, block precision) of a logged
+    ``str(CG(...))``, e.g. ``CG(HybridSchwarz(torch.float64,
+    Inv(torch.float16), CUDSS), bsr_matmul=True)`` (the formats of
+    ``solvers.py:209-210, 791-792, 844-845, 347-348``)."""
+    head = "CG(AdditiveSchwarz(" if name.startswith("CG(AdditiveSchwarz(") else "CG(HybridSchwarz("
+    if not name.startswith(head):
+        raise ValueError(f"not a Schwarz-preconditioned CG: {name}")
+    rest = name[len(head):]
+    pc, rest = rest.split(", ", 1)
+    if not rest.startswith("Inv("):
+        raise ValueError(f"local solver is not Inv: {name}")
+    blk = rest[len("Inv("):rest.index(")")]
+    return {"method": "additive" if "Additive" in head else "hybrid", "pc_precision": _NAME_DT[pc],
+            "precision": _NAME_DT[blk] if blk else _NAME_DT[pc]}
+
+
+def logged_runs(log, degree=None, include_failed=False):
+    """The converged runs of the reference's log (``make_dg_golden.py``
+    rows), one per configuration, in log order; ``include_failed`` adds the
+    ones that did not converge in 2000 iterations (they run to maxiter)."""
+    seen, out = set(), []
+    for r in log:
+        if degree is not None and r.get("p", 1) != degree:
+            continue
+        if r["exception"] and (r["iterations"] is None or not include_failed):
+            continue
+        if r["iterations"] is None or (r["iterations"] >= 1999 and not include_failed):
+            continue
+        cfg = (r.get("p", 1), r["fine"], r["solvers"], r["coarse"], r["solver"])
+        if cfg in seen:
+            continue
+        seen.add(cfg)
+        out.append(dict(degree=cfg[0], fine=cfg[1], solvers=cfg[2], coarse=cfg[3], **parse_solver(r["solver"])))
+    return out
+
+
 def run(fine, solvers, coarse, method, precision, pc_precision="f64", reps=10, log=None, flexible=False,
         device="cuda", degree=1) -> dict:
     t0 = time.perf_counter()
@@ -150,7 +193,7 @@ def run(fine, solvers, coarse, method, precision, pc_precision="f64", reps=10, l
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--degree", type=int, default=1, help="polynomial degree p of the DG space")
+    ap.add_argument("--degree", type=int, default=None, help="polynomial degree p of the DG space (default 1)")
     ap.add_argument("--fine", default="S10")
     ap.add_argument("--solvers", default="S8")
     ap.add_argument("--coarse", default="S8")
@@ -161,10 +204,25 @@ def main():
     ap.add_argument("--reps", type=int, default=10)
     ap.add_argument("--log", default=None, help="JSON of the reference's logged runs")
     ap.add_argument("--history", action="store_true", help="print the residual history too")
+    ap.add_argument("--all", action="store_true",
+                    help="run every converged configuration of --log (restricted to --degree if given)")
+    ap.add_argument("--include-failed", action="store_true",
+                    help="with --all: also the configurations that did not converge for the reference")
     args = ap.parse_args()
     log = json.load(open(args.log)) if args.log else None
+    if args.all:
+        if log is None:
+            ap.error("--all needs --log")
+        for c in logged_runs(log, args.degree, args.include_failed):
+            out = run(c["fine"], c["solvers"], c["coarse"], c["method"], c["precision"], c["pc_precision"],
+                      args.reps, log, args.flexible, degree=c["degree"])
+            if not args.history:
+                out.pop("residual_norms")
+            print(json.dumps(out), flush=True)
+            torch.cuda.empty_cache()
+        return
     out = run(args.fine, args.solvers, args.coarse, args.method, args.precision, args.pc_precision,
-              args.reps, log, args.flexible, degree=args.degree)
+              args.reps, log, args.flexible, degree=args.degree or 1)
     if not args.history:
         out.pop("residual_norms")
     print(json.dumps(out))

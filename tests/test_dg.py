@@ -308,3 +308,23 @@ def test_p3_oracle_residual_history_matches_reference_log(p3_s9, kind):
     ours = np.array(meta["residual norms"])
     assert len(ours) == 10
     np.testing.assert_allclose(ours, np.array(row["residual_norms"][:10]), rtol=1e-10)
+
+
+def test_logged_solver_strings_parse():
+    """The reference's ``str(CG(...))`` keys of its logs map to (method,
+    preconditioner precision, block precision); every converged logged
+    configuration is runnable by ``dg_experiments --all``."""
+    from dd_solvers_b200 import dg_experiments as de
+
+    assert de.parse_solver("CG(HybridSchwarz(torch.float64, Inv(torch.float16), CUDSS), bsr_matmul=True)") == \
+        {"method": "hybrid", "pc_precision": "f64", "precision": "f16"}
+    assert de.parse_solver("CG(AdditiveSchwarz(torch.float32, Inv(), CUDSS, const_dofs_per_coarse=False), "
+                           "bsr_matmul=True)") == {"method": "additive", "pc_precision": "f32", "precision": "f32"}
+    with pytest.raises(ValueError):
+        de.parse_solver("CG(AMGX(L1_TRUNC, None), bsr_matmul=True)")
+    runs = de.logged_runs(golden_rows())
+    assert {r["degree"] for r in runs} == {1, 3, 5}
+    assert len({tuple(sorted(r.items())) for r in runs}) == len(runs)
+    assert all(r["fine"] in ("S8", "S9", "S10", "S11") for r in runs)
+    p3 = de.logged_runs(golden_rows(), degree=3)
+    assert p3 and all(r["degree"] == 3 and r["fine"] == "S9" for r in p3)
