@@ -328,3 +328,20 @@ def test_logged_solver_strings_parse():
     assert all(r["fine"] in ("S8", "S9", "S10", "S11") for r in runs)
     p3 = de.logged_runs(golden_rows(), degree=3)
     assert p3 and all(r["degree"] == 3 and r["fine"] == "S9" for r in p3)
+
+
+def test_system_matrix_bsr_form():
+    """The PCG's matrix takes the BSR form only for a block size that tiles
+    the pattern densely, and keeps it in step with new values (the values of
+    the differentiable solve's ``set_matrix_values``)."""
+    from dd_solvers_b200.solvers import _SellMatrix, _dense_blocks
+
+    s = dg.sipg(dg.uniform_mesh_2d(2), degree=3)
+    M = _SellMatrix(s.matrix)
+    assert M.use_bsr(10) and M.bsr[3] == 10 and M.bsr[2].shape == (32 + 2 * 40, 10, 10)
+    assert not M.use_bsr(4) and M.bsr is None
+    assert M.use_bsr(10)
+    v = torch.randn(M.nnz, dtype=torch.float64, generator=torch.Generator().manual_seed(0))
+    M.set_values(v)
+    ref = _dense_blocks(M.crow32, M.col32, v, 10)
+    assert torch.equal(M.bsr[2], ref[2])
