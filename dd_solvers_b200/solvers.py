@@ -15,7 +15,8 @@ metadata keys follow ``src/dd_solvers/dd_solvers/solvers.py`` of mgr0dzicki/dd-s
 
 What runs where: every per-iteration operation is a kernel of ``libddx.so``
 (``include/ddx.h``) launched on the current torch stream: SELL-32 SpMV with the
-p.q / residual epilogues, the TMA-staged local-inverse apply, the transpose-map
+p.q / residual epilogues (BSR products plus an epilogue pass for DG block
+matrices), the TMA-staged local-inverse apply, the transpose-map
 prolongation with the coarse correction and the r.z dots, and the fused x/r/p
 updates. Step lengths, dot products and the stop test are evaluated on the
 device, so the loop needs no host synchronisation; the host polls the number
