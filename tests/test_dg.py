@@ -196,6 +196,11 @@ def test_reference_nodes_layout():
         d = np.abs(Q[:, None, :] - P[None, :, :]).sum(-1).min(1)
         assert d.max() < 1e-14
     np.testing.assert_allclose(dg.reference_nodes(2), [[0, 0], [1, 0], [0, 1], [.5, .5], [0, .5], [.5, 0]])
+    # GLL points in closed form: roots of P_3' at +-1/sqrt(5), of P_5' at +-sqrt(1/3 -+ 2 sqrt(7) / 21)
+    np.testing.assert_allclose(dg._gll_points(3), [0, .5 - 5 ** .5 / 10, .5 + 5 ** .5 / 10, 1], atol=1e-15)
+    r5 = sorted([-(1 / 3 + 2 * 7 ** .5 / 21) ** .5, -(1 / 3 - 2 * 7 ** .5 / 21) ** .5,
+                 (1 / 3 - 2 * 7 ** .5 / 21) ** .5, (1 / 3 + 2 * 7 ** .5 / 21) ** .5])
+    np.testing.assert_allclose(dg._gll_points(5)[1:-1], (1 + np.array(r5)) / 2, atol=1e-15)
     np.testing.assert_allclose(dg.reference_nodes(3)[-1], [1 / 3, 1 / 3], atol=1e-15)
     # the nodal basis is the identity on the nodes
     P = dg.reference_nodes(5)
