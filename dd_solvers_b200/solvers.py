@@ -1145,6 +1145,9 @@ class _PcgWork:
         self.recompute_z = False
 
 
+BSR_MAX_BLOCK = 24  # largest block size ddx_spmv_bsr is compiled for
+
+
 def _dense_blocks(crow: torch.Tensor, col: torch.Tensor, val: torch.Tensor, bs: int):
     """BSR arrays ``(block_row_ptr, block_cols, vals)`` (int32, int32, blocks
     column-major) of a scalar CSR matrix with sorted columns whose nonzeros
@@ -1205,7 +1208,11 @@ class _SellMatrix:
         reference's ``CG(bsr_matmul=True)`` does (solvers.py:216-224): 8 bytes
         per stored entry instead of SELL's 12, which pays on DG block rows. The
         PCG epilogue then runs as a separate pass. Returns False (and keeps
-        SELL) when the pattern is not block-dense."""
+        SELL) when the pattern is not block-dense or ``bs`` is outside the BSR
+        kernel's 2..24."""
+        if not 2 <= int(bs) <= BSR_MAX_BLOCK:
+            self.bsr = None
+            return False
         got = _dense_blocks(self.crow32, self.col32, self.val, int(bs))
         self.bsr = None if got is None else (*got, int(bs))
         return self.bsr is not None

@@ -345,6 +345,8 @@ def test_system_matrix_bsr_form():
     M = _SellMatrix(s.matrix)
     assert M.use_bsr(10) and M.bsr[3] == 10 and M.bsr[2].shape == (32 + 2 * 40, 10, 10)
     assert not M.use_bsr(4) and M.bsr is None
+    # block-dense at 28 x 28 (P6), but beyond the BSR kernel's block sizes: SELL stays
+    assert not _SellMatrix(dg.sipg(dg.uniform_mesh_2d(1), degree=6).matrix).use_bsr(28)
     assert M.use_bsr(10)
     v = torch.randn(M.nnz, dtype=torch.float64, generator=torch.Generator().manual_seed(0))
     M.set_values(v)
