@@ -145,6 +145,17 @@ def logged_runs(log, degree=None, include_failed=False):
     return out
 
 
+def summarize(outs) -> dict:
+    """Runs, how many reproduce the logged iteration count (exactly / within
+    1), and the range of speed-ups against the logged A100 times."""
+    ref = [o for o in outs if o.get("reference_iterations") is not None]
+    sp = [o["reference_a100_solve_ms_min"] / o["solve_ms_min"] for o in ref if o.get("reference_a100_solve_ms_min")]
+    return {"runs": len(outs), "with_reference": len(ref),
+            "iterations_equal": sum(o["iterations"] == o["reference_iterations"] for o in ref),
+            "iterations_within_1": sum(abs(o["iterations"] - o["reference_iterations"]) <= 1 for o in ref),
+            "speedup_min": min(sp) if sp else None, "speedup_max": max(sp) if sp else None}
+
+
 def run(fine, solvers, coarse, method, precision, pc_precision="f64", reps=10, log=None, flexible=False,
         device="cuda", degree=1) -> dict:
     t0 = time.perf_counter()
@@ -213,13 +224,16 @@ def main():
     if args.all:
         if log is None:
             ap.error("--all needs --log")
+        outs = []
         for c in logged_runs(log, args.degree, args.include_failed):
             out = run(c["fine"], c["solvers"], c["coarse"], c["method"], c["precision"], c["pc_precision"],
                       args.reps, log, args.flexible, degree=c["degree"])
             if not args.history:
                 out.pop("residual_norms")
             print(json.dumps(out), flush=True)
+            outs.append(out)
             torch.cuda.empty_cache()
+        print(json.dumps({"summary": summarize(outs)}), flush=True)
         return
     out = run(args.fine, args.solvers, args.coarse, args.method, args.precision, args.pc_precision,
               args.reps, log, args.flexible, degree=args.degree or 1)

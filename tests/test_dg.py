@@ -352,3 +352,13 @@ def test_system_matrix_bsr_form():
     M.set_values(v)
     ref = _dense_blocks(M.crow32, M.col32, v, 10)
     assert torch.equal(M.bsr[2], ref[2])
+
+
+def test_experiment_summary():
+    from dd_solvers_b200 import dg_experiments as de
+
+    outs = [{"iterations": 61, "reference_iterations": 61, "solve_ms_min": 40.0, "reference_a100_solve_ms_min": 160.0},
+            {"iterations": 76, "reference_iterations": 75, "solve_ms_min": 50.0, "reference_a100_solve_ms_min": 250.0},
+            {"iterations": 30, "solve_ms_min": 10.0}]
+    assert de.summarize(outs) == {"runs": 3, "with_reference": 2, "iterations_equal": 1, "iterations_within_1": 2,
+                                  "speedup_min": 4.0, "speedup_max": 5.0}
