@@ -216,6 +216,17 @@ def test_capi_argument_checks_without_gpu():
     flag = ctypes.c_int(0)
     assert lib.ddx_pcg_finalize(4, 9, ctypes.byref(one), ctypes.byref(flag), ctypes.byref(one), None) == 1
     assert b"unknown kind 9" in lib.ddx_last_error()
+    # the epilogue after a BSR product: y, a PCG mode and the state are required, checked before any launch
+    assert lib.ddx_spmv_epilogue_f64(10, None, None, None, 1, None, None, None, None, None, None) == 1
+    assert b"bad arguments" in lib.ddx_last_error()
+    y = ctypes.byref(one)
+    assert lib.ddx_spmv_epilogue_f64(10, y, y, None, 0, None, None, None, None, None, None) == 1
+    assert b"bad mode 0" in lib.ddx_last_error()
+    assert lib.ddx_spmv_epilogue_f64(10, y, y, None, 1, None, None, None, None, None, None) == 1
+    assert b"needs state" in lib.ddx_last_error()
+    st = (ctypes.byref(one), ctypes.byref(flag), ctypes.byref(one), ctypes.byref(one), ctypes.byref(flag))
+    assert lib.ddx_spmv_epilogue_f64(10, y, y, None, 2, *st, None) == 1
+    assert b"residual mode needs b" in lib.ddx_last_error()
 
 
 def test_solver_rejects_cpu_tensors():
