@@ -227,6 +227,11 @@ def test_capi_argument_checks_without_gpu():
     st = (ctypes.byref(one), ctypes.byref(flag), ctypes.byref(one), ctypes.byref(one), ctypes.byref(flag))
     assert lib.ddx_spmv_epilogue_f64(10, y, y, None, 2, *st, None) == 1
     assert b"residual mode needs b" in lib.ddx_last_error()
+    # the BSR kernel's block sizes end where the PCG's BSR form stops being used
+    from dd_solvers_b200.solvers import BSR_MAX_BLOCK
+    rp = ctypes.byref(flag)
+    assert lib.ddx_spmv_bsr(1, BSR_MAX_BLOCK + 1, rp, rp, y, y, y, _lib.F64, None) != 0
+    assert f"block size {BSR_MAX_BLOCK + 1} not in 1..{BSR_MAX_BLOCK}".encode() in lib.ddx_last_error()
 
 
 def test_solver_rejects_cpu_tensors():
