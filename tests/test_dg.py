@@ -362,3 +362,23 @@ def test_experiment_summary():
             {"iterations": 30, "solve_ms_min": 10.0}]
     assert de.summarize(outs) == {"runs": 3, "with_reference": 2, "iterations_equal": 1, "iterations_within_1": 2,
                                   "speedup_min": 4.0, "speedup_max": 5.0}
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 5])
+def test_sipg_consistency_with_constants(p):
+    """Exact identities of the form at every degree: a constant has no
+    gradient and no jumps, so A 1 vanishes on every cell away from the
+    boundary (only the boundary penalty and flux act), and with f = 1 the
+    load vector sums to the area of the unit square."""
+    mesh = dg.uniform_mesh_2d(3)
+    case = dg.TestCase("unit source", 7.0, dg._rho_continuous, lambda x, y: torch.ones_like(x))
+    s = dg.sipg(mesh, case, p)
+    nb = s.block_size
+    r = (s.matrix @ torch.ones(s.matrix.shape[0], dtype=torch.float64)).view(mesh.n_cells, nb)
+    _, (cb, _) = dg._edge_tables(mesh)
+    interior = torch.ones(mesh.n_cells, dtype=torch.bool)
+    interior[cb] = False
+    scale = float(s.matrix.values().abs().max())
+    assert float(r[interior].abs().max()) <= 1e-12 * scale
+    assert float(r[~interior].abs().max()) > 1e-3 * scale  # the boundary terms are there
+    assert math.isclose(float(s.load.sum()), 1.0, rel_tol=1e-13)
