@@ -54,6 +54,23 @@ def test_s0_block_sums_match_reference_test():
     assert np.isclose(A[:3, 3:].sum(), -delta / 2)
 
 
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 5])
+def test_s0_block_sums_at_every_degree(p):
+    """The same test at degree p: with rho = 1 a cell's constant has no
+    gradient, so a block sum is its penalty alone, delta p^2 times the jump
+    weights: 2 boundary edges + half the shared one (5/2) on the diagonal
+    blocks, -1/2 off them."""
+    s = dg.sipg(dg.uniform_mesh_2d(0), dg.CONSTANT_COEFFICIENT_2D, degree=p)
+    A = s.matrix.to_dense().numpy()
+    nb = s.block_size
+    dp2 = 7.0 * p * p
+    assert A.shape == (2 * nb, 2 * nb)
+    assert np.isclose(A[:nb, :nb].sum(), dp2 * 5 / 2)
+    assert np.isclose(A[nb:, :nb].sum(), -dp2 / 2)
+    assert np.isclose(A[nb:, nb:].sum(), dp2 * 5 / 2)
+    assert np.isclose(A[:nb, nb:].sum(), -dp2 / 2)
+
+
 @pytest.mark.parametrize("m", [1, 2, 3])
 def test_matrix_symmetric_positive_definite(m):
     A = dg.sipg_p1(dg.uniform_mesh_2d(m)).matrix.to_dense().numpy()
