@@ -305,24 +305,32 @@ def test_dense_blocks_match_torch_bsr(p):
     assert _dense_blocks(crow, torch.as_tensor(L.indices), torch.as_tensor(L.data), 2) is None
 
 
-@pytest.fixture(scope="module")
-def p3_s9():
-    s = dg.sipg(dg.uniform_mesh_2d(9), degree=3)
-    A, b = scipy_csr(s.matrix), s.load.numpy()
+# the reference's logged higher-degree runs with S8 subdomains and coarse cells:
+# degree -> (fine mesh level, cells per subdomain)
+HIGHER_DEGREE_RUNS = {3: (9, 4), 5: (8, 1)}
+
+
+@pytest.fixture(scope="module", params=sorted(HIGHER_DEGREE_RUNS))
+def higher_degree_system(request):
+    p = request.param
+    m, cells = HIGHER_DEGREE_RUNS[p]
+    s = dg.sipg(dg.uniform_mesh_2d(m), degree=p)
+    A, b, nb = scipy_csr(s.matrix), s.load.numpy(), s.block_size
     del s
-    return A, b, rs.ContiguousSchwarz(A, 10 * 4, np.ones(2 * 4 ** 8, dtype=np.int64))
+    return p, m, A, b, rs.ContiguousSchwarz(A, nb * cells, np.ones(2 * 4 ** 8, dtype=np.int64))
 
 
 @pytest.mark.parametrize("kind", ["additive", "hybrid"])
-def test_p3_oracle_residual_history_matches_reference_log(p3_s9, kind):
-    """The reference's P3 experiment on S9 (5,242,880 DOFs, 10 per cell), S8
-    subdomains of 40 DOFs and S8 P0 coarse cells, FP64: the oracle on this
-    package's higher-degree assembly reproduces the first ten logged residual
-    norms to 1e-10 (they depend on the GLL-warped nodes through the basis)."""
-    A, b, P = p3_s9
+def test_higher_degree_oracle_residual_history_matches_reference_log(higher_degree_system, kind):
+    """The reference's P3 experiment on S9 (5,242,880 DOFs, subdomains of 40)
+    and P5 experiment on S8 (2,752,512 DOFs, subdomains of 21), S8 P0 coarse
+    cells, FP64: the oracle on this package's higher-degree assembly
+    reproduces the first ten logged residual norms to 1e-10 (they depend on
+    the GLL-warped nodes through the basis)."""
+    p, m, A, b, P = higher_degree_system
     prefix = {"additive": "CG(AdditiveSchwarz(torch.float64, Inv(), CUDSS",
               "hybrid": "CG(HybridSchwarz(torch.float64, Inv(), CUDSS"}[kind]
-    row = next(r for r in golden_rows() if r.get("p") == 3 and (r["fine"], r["solvers"], r["coarse"]) == ("S9", "S8", "S8")
+    row = next(r for r in golden_rows() if r.get("p") == p and (r["fine"], r["solvers"], r["coarse"]) == (f"S{m}", "S8", "S8")
                and r["solver"].startswith(prefix))
     M = P.additive if kind == "additive" else P.hybrid
     T0 = P.T0 if kind == "hybrid" else None
